@@ -1,0 +1,336 @@
+"""Seeded synthetic C-alpha traces for the superposition-search workloads.
+
+No public dataset is used anywhere in this package.  Chains are built with the
+NeRF (natural extension reference frame) construction from virtual-bond
+internal coordinates:
+
+* every C-alpha to C-alpha virtual bond is 3.8 A long;
+* coil residues draw the virtual bond angle from N(105 deg, 10 deg) and the
+  torsion uniformly;
+* helix runs use a bond angle of 91 deg and a torsion of 50 deg, which gives
+  a rise of 1.5 A and 100 deg per residue;
+* strand runs use a bond angle of 120 deg and a torsion of -170 deg, which
+  gives a rise of about 3.3 A per residue;
+* helix and strand runs are 4-20 residues long.
+
+Homologs are copies of a template with 0..max indel fraction of random
+insertions/deletions, Gaussian coordinate noise of a chosen sigma, and a random
+rigid rotation and translation.
+
+Coordinates are rounded to the 3 decimals a PDB ATOM record carries and are
+converted to float32 the way ``std::stof`` does (``strtof``), so the arrays
+handed to the C-ABI and the PDB files read by the reference hold the same
+values.
+"""
+from __future__ import annotations
+
+import ctypes
+import math
+import os
+from dataclasses import dataclass, field
+from typing import List, Optional, Sequence
+
+import numpy as np
+
+AA = np.frombuffer(b"ACDEFGHIKLMNPQRSTVWY", dtype=np.uint8)
+AA3 = {
+    "A": "ALA", "C": "CYS", "D": "ASP", "E": "GLU", "F": "PHE", "G": "GLY",
+    "H": "HIS", "I": "ILE", "K": "LYS", "L": "LEU", "M": "MET", "N": "ASN",
+    "P": "PRO", "Q": "GLN", "R": "ARG", "S": "SER", "T": "THR", "V": "VAL",
+    "W": "TRP", "Y": "TYR",
+}
+
+_libc = ctypes.CDLL(None)
+_libc.strtof.restype = ctypes.c_float
+_libc.strtof.argtypes = [ctypes.c_char_p, ctypes.c_void_p]
+
+
+@dataclass
+class Chain:
+    """One structure: float32 SoA coordinates, residue letters, a name."""
+    xyz: np.ndarray            # (L, 3) float32
+    seq: np.ndarray            # (L,) uint8 residue letters
+    name: str = "chain"
+
+    @property
+    def length(self) -> int:
+        return int(self.xyz.shape[0])
+
+
+def _rot_random(rng: np.random.Generator) -> np.ndarray:
+    q = rng.normal(size=4)
+    q /= np.linalg.norm(q)
+    a, b, c, d = q
+    return np.array([
+        [a*a + b*b - c*c - d*d, 2*(b*c - a*d), 2*(b*d + a*c)],
+        [2*(b*c + a*d), a*a - b*b + c*c - d*d, 2*(c*d - a*b)],
+        [2*(b*d - a*c), 2*(c*d + a*b), a*a - b*b - c*c + d*d]])
+
+
+def _internal_coords(rng: np.random.Generator, L: int):
+    """Bond angles and torsions (radians) for a chain of L residues."""
+    theta = np.deg2rad(rng.normal(105.0, 10.0, size=L))
+    tau = rng.uniform(-np.pi, np.pi, size=L)
+    i = 0
+    while i < L:
+        r = rng.random()
+        run = int(rng.integers(4, 21))
+        if r < 0.35:          # helix run
+            theta[i:i+run] = np.deg2rad(91.0)
+            tau[i:i+run] = np.deg2rad(50.0)
+            i += run
+        elif r < 0.6:         # strand run
+            theta[i:i+run] = np.deg2rad(120.0)
+            tau[i:i+run] = np.deg2rad(-170.0)
+            i += run
+        else:                 # coil
+            i += int(rng.integers(2, 9))
+    return theta, tau
+
+
+def _nerf_batch(theta: np.ndarray, tau: np.ndarray, bond: float = 3.8) -> np.ndarray:
+    """NeRF over a batch: theta, tau of shape (B, L) -> coords (B, L, 3)."""
+    B, L = theta.shape
+    X = np.zeros((B, L, 3))
+    if L > 1:
+        X[:, 1, 0] = bond
+    if L > 2:
+        t = theta[:, 2]
+        X[:, 2, 0] = bond - bond * np.cos(t)
+        X[:, 2, 1] = bond * np.sin(t)
+    for i in range(3, L):
+        a, b, c = X[:, i-3], X[:, i-2], X[:, i-1]
+        bc = c - b
+        bc /= np.linalg.norm(bc, axis=1, keepdims=True)
+        n = np.cross(b - a, bc)
+        nn = np.linalg.norm(n, axis=1, keepdims=True)
+        nn[nn < 1e-9] = 1.0
+        n /= nn
+        m = np.cross(n, bc)
+        th, to = theta[:, i], tau[:, i]
+        d2 = np.stack([-bond * np.cos(th),
+                       bond * np.sin(th) * np.cos(to),
+                       bond * np.sin(th) * np.sin(to)], axis=1)
+        X[:, i] = c + d2[:, 0:1] * bc + d2[:, 1:2] * m + d2[:, 2:3] * n
+    return X
+
+
+def _pdb_round(x: np.ndarray) -> np.ndarray:
+    """Round to 3 decimals and convert each value as strtof would."""
+    x = np.round(np.asarray(x, dtype=np.float64), 3)
+    flat = x.ravel()
+    out = np.empty(flat.shape, dtype=np.float32)
+    for i, v in enumerate(flat):
+        out[i] = _libc.strtof(("%.3f" % v).encode(), None)
+    return out.reshape(x.shape)
+
+
+def _pdb_round_fast(x: np.ndarray) -> np.ndarray:
+    """Vectorised rounding: exact float32 of the 3-decimal value.
+
+    The 3-decimal value k/1000 with |k| < 2**24 is converted by dividing the
+    exact integer k by 1000 in float64 and rounding to float32.  Double
+    rounding (decimal -> float64 -> float32) can differ from a direct
+    decimal -> float32 conversion only when the float64 result lies within
+    2**-29 relative of a float32 rounding boundary; those values are re-done
+    with strtof.
+    """
+    k = np.round(np.asarray(x, dtype=np.float64) * 1000.0)
+    d = k / 1000.0
+    f = d.astype(np.float32)
+    # detect near-ties of the float64 -> float32 rounding
+    back = f.astype(np.float64)
+    ulp = np.abs(np.spacing(f).astype(np.float64))
+    frac = np.abs(d - back) / ulp
+    risky = np.abs(frac - 0.5) < 1e-6
+    if np.any(risky):
+        idx = np.nonzero(risky.ravel())[0]
+        ff = f.ravel()
+        dd = d.ravel()
+        for i in idx:
+            ff[i] = _libc.strtof(("%.3f" % dd[i]).encode(), None)
+        f = ff.reshape(f.shape)
+    return f
+
+
+def random_chains(rng: np.random.Generator, lengths: Sequence[int],
+                  prefix: str = "rnd") -> List[Chain]:
+    """Unrelated random-walk chains with helix/strand runs."""
+    lengths = list(int(l) for l in lengths)
+    out: List[Optional[Chain]] = [None] * len(lengths)
+    order = np.argsort(lengths, kind="stable")
+    # batch chains of equal length bucket (pad to the bucket max, then cut)
+    i = 0
+    while i < len(order):
+        j = min(i + 4096, len(order))
+        idx = order[i:j]
+        Lmax = max(lengths[k] for k in idx)
+        th = np.empty((len(idx), Lmax))
+        to = np.empty((len(idx), Lmax))
+        for r, k in enumerate(idx):
+            t1, t2 = _internal_coords(rng, Lmax)
+            th[r], to[r] = t1, t2
+        X = _nerf_batch(th, to)
+        for r, k in enumerate(idx):
+            L = lengths[k]
+            xyz = X[r, :L]
+            xyz = xyz - xyz.mean(axis=0) + rng.uniform(-20, 20, size=3)
+            seq = AA[rng.integers(0, len(AA), size=L)]
+            out[k] = Chain(_pdb_round_fast(xyz), seq.copy(), f"{prefix}{k:06d}")
+        i = j
+    return out  # type: ignore[return-value]
+
+
+def homolog(rng: np.random.Generator, tmpl: Chain, sigma: float,
+            indel_frac: float, name: str) -> Chain:
+    """A noisy, indel-bearing, rigidly moved copy of ``tmpl``."""
+    xyz = tmpl.xyz.astype(np.float64)
+    seq = tmpl.seq.copy()
+    L = xyz.shape[0]
+    nindel = int(round(indel_frac * L))
+    keep = np.ones(L, dtype=bool)
+    ins_after = {}
+    for _ in range(nindel):
+        p = int(rng.integers(0, L))
+        if rng.random() < 0.5:
+            keep[p] = False
+        else:
+            ins_after[p] = ins_after.get(p, 0) + int(rng.integers(1, 4))
+    pts, aas = [], []
+    for p in range(L):
+        if keep[p]:
+            pts.append(xyz[p])
+            aas.append(seq[p] if rng.random() < 0.6 else AA[rng.integers(0, 20)])
+        for _ in range(ins_after.get(p, 0)):
+            base = pts[-1] if pts else xyz[p]
+            step = rng.normal(size=3)
+            step *= 3.8 / np.linalg.norm(step)
+            pts.append(base + step)
+            aas.append(AA[rng.integers(0, 20)])
+    P = np.array(pts)
+    P = P + rng.normal(0.0, sigma, size=P.shape)
+    R = _rot_random(rng)
+    P = (P - P.mean(axis=0)) @ R.T + rng.uniform(-30, 30, size=3)
+    return Chain(_pdb_round_fast(P), np.array(aas, dtype=np.uint8), name)
+
+
+def write_pdb(ch: Chain, path: str) -> None:
+    """Write a C-alpha-only PDB file the reference reader accepts."""
+    lines = []
+    for i in range(ch.length):
+        x, y, z = (float(v) for v in ch.xyz[i])
+        res = AA3[chr(int(ch.seq[i]))]
+        lines.append("ATOM  %5d  CA  %3s A%4d    %8.3f%8.3f%8.3f  1.00  0.00           C\n"
+                     % (i + 1, res, i + 1, x, y, z))
+    lines.append("TER\nEND\n")
+    with open(path, "w") as f:
+        f.writelines(lines)
+
+
+# -------------------------------------------------------------------------
+# workload builders (seeded; sizes of the benchmark configurations)
+
+@dataclass
+class Workload:
+    queries: List[Chain]
+    refs: List[Chain]
+    seed: int
+    desc: str = ""
+    homolog_of: List[int] = field(default_factory=list)  # ref -> query or -1
+
+
+def config0(seed: int = 1, n_refs: int = 1000, qlen: int = 150,
+            lmin: int = 50, lmax: int = 500, homolog_frac: float = 0.2) -> Workload:
+    """One query of ``qlen`` residues against ``n_refs`` targets U(lmin,lmax);
+    ``homolog_frac`` of them homologs (sigma 1-3 A, 0-10% indels)."""
+    rng = np.random.default_rng(seed)
+    q = random_chains(rng, [qlen], "qry")[0]
+    refs: List[Chain] = []
+    hom: List[int] = []
+    lens = rng.integers(lmin, lmax + 1, size=n_refs)
+    rnd = random_chains(rng, lens, "ref")
+    for i in range(n_refs):
+        if rng.random() < homolog_frac:
+            refs.append(homolog(rng, q, float(rng.uniform(1.0, 3.0)),
+                                float(rng.uniform(0.0, 0.10)), f"hom{i:06d}"))
+            hom.append(0)
+        else:
+            refs.append(rnd[i])
+            hom.append(-1)
+    return Workload([q], refs, seed, f"config0 seed={seed}", hom)
+
+
+def config1(seed: int = 2, n_queries: int = 16, n_refs: int = 200_000,
+            family_frac: float = 0.05) -> Workload:
+    """16 queries U(80,800) against log-normal targets (median 250,
+    sigma_log 0.6, clipped to 30..2000); ``family_frac`` of the targets are
+    members of homolog families (10-50 members, sigma 0.5-4 A, <=15% indels)
+    seeded from the queries."""
+    rng = np.random.default_rng(seed)
+    qlens = rng.integers(80, 801, size=n_queries)
+    queries = random_chains(rng, qlens, "qry")
+    lens = np.clip(np.round(rng.lognormal(math.log(250.0), 0.6, size=n_refs)), 30, 2000).astype(int)
+    refs = random_chains(rng, lens, "ref")
+    hom = [-1] * n_refs
+    n_fam_members = int(family_frac * n_refs)
+    pos = rng.permutation(n_refs)
+    k = 0
+    while k < n_fam_members:
+        fsize = int(rng.integers(10, 51))
+        qi = int(rng.integers(0, n_queries))
+        for _ in range(fsize):
+            if k >= n_fam_members:
+                break
+            ri = int(pos[k])
+            refs[ri] = homolog(rng, queries[qi], float(rng.uniform(0.5, 4.0)),
+                               float(rng.uniform(0.0, 0.15)), f"fam{ri:06d}")
+            hom[ri] = qi
+            k += 1
+    return Workload(queries, refs, seed, f"config1 seed={seed}", hom)
+
+
+# -------------------------------------------------------------------------
+# SoA packing (the layout the C-ABI consumes)
+
+@dataclass
+class SoA:
+    """Structure-of-arrays block: lengths, prefix offsets, x/y/z, residues."""
+    lens: np.ndarray      # (n,) int32
+    offs: np.ndarray      # (n,) int32 exclusive prefix sums
+    x: np.ndarray         # (N,) float32
+    y: np.ndarray
+    z: np.ndarray
+    rsd: np.ndarray       # (N,) uint8 residue letters
+    mol: np.ndarray       # (n,) int32 molecule type (0 protein, 1 nucleic acid)
+
+    @property
+    def n(self) -> int:
+        return int(self.lens.shape[0])
+
+    @property
+    def total(self) -> int:
+        return int(self.x.shape[0])
+
+
+def pack(chains: Sequence[Chain]) -> SoA:
+    lens = np.array([c.length for c in chains], dtype=np.int32)
+    offs = np.zeros_like(lens)
+    if len(lens) > 1:
+        offs[1:] = np.cumsum(lens[:-1])
+    xyz = np.concatenate([c.xyz for c in chains], axis=0) if chains else np.zeros((0, 3), np.float32)
+    rsd = np.concatenate([c.seq for c in chains]) if chains else np.zeros(0, np.uint8)
+    return SoA(lens, offs,
+               np.ascontiguousarray(xyz[:, 0], dtype=np.float32),
+               np.ascontiguousarray(xyz[:, 1], dtype=np.float32),
+               np.ascontiguousarray(xyz[:, 2], dtype=np.float32),
+               np.ascontiguousarray(rsd, dtype=np.uint8),
+               np.zeros(len(lens), dtype=np.int32))
+
+
+def write_dirs(wl: Workload, qdir: str, rdir: str) -> None:
+    os.makedirs(qdir, exist_ok=True)
+    os.makedirs(rdir, exist_ok=True)
+    for c in wl.queries:
+        write_pdb(c, os.path.join(qdir, c.name + ".pdb"))
+    for c in wl.refs:
+        write_pdb(c, os.path.join(rdir, c.name + ".pdb"))

@@ -1,0 +1,1014 @@
+/*
+ * gtoracle.c -- CPU oracle (checker) for the GTalign superposition search.
+ *
+ * TEST INFRASTRUCTURE ONLY: loaded by tests/, __graft_entry__.smoke() and
+ * bench.py's cpu_baseline leg; never by the product.
+ *
+ * A sequential restatement, one query-reference pair at a time, of the
+ * reference's CPU stage sequence with --no-detailed-search semantics:
+ *   MpBatch::ProcessBlock           src/libmymp/mpbatch/MpBatch.cpp:208-470
+ *   MpStage1::Preinitialize1Kernel  src/libmymp/mpstage1/MpStage1.cpp:28-167
+ *   MpSecStr::ssk_kernel_helper     src/libmymp/mpss/MpSecStr.cpp:26-118,
+ *                                   AassignSecStr src/libmymp/mpss/MpSecStr.h:218-249
+ *   MpStage1::FindFragKernel        src/libmymp/mpstage1/MpStage1.cpp:289-440
+ *   MpStage1::RefineFragInitKernel  src/libmymp/mpstage1/MpStage1.cpp:548-736
+ *   MpStage1::DPRefine              src/libmymp/mpstage1/MpStage1.cpp:466-517
+ *   MpStage1::RefineFragDPKernel    src/libmymp/mpstage1/MpStage1.cpp:760-948
+ *   MpStage2::RunSpecialized/Align  src/libmymp/mpstage1/MpStage2.h:63-126
+ *   MpStageFin::Run                 src/libmymp/mpstage1/MpStageFin.h:63-96
+ *   MpDPHub::ExecDPwBtck128xKernel  src/libmymp/mpdp/MpDPHub.cpp:72-346 and
+ *     ExecDPTFMSSwBtck128xKernel    src/libmymp/mpdp/MpDPHub.cpp:686-940
+ *   MpDPHub::BtckToMatched128x      src/libmymp/mpdp/MpDPHub.cpp:1515-1660
+ *   MpDPHub::ConstrainedBtck...     src/libmymp/mpdp/MpDPHub.cpp:1699-1905
+ *   MpDPHub::ProductionMatchTo...   src/libmymp/mpdp/MpDPHub.cpp:1919-2125
+ *   MpStageFin production kernels   src/libmymp/mpstage1/MpStageFin.cpp:747-1525
+ *   constants (d0, d8, d0s)         src/libmycu/custages/stagecnsts.cuh:48-175
+ *   fragment rules                  src/libmycu/custages/fragment.cuh:30-110
+ *
+ * Numeric form (shared with the CUDA path so the two agree bit for bit):
+ *  - FP32 coordinates; transforms and squared distances written with explicit
+ *    fmaf at fixed places; nothing else contracted (-ffp-contract=off);
+ *  - every sum over positions is accumulated in forward position order in
+ *    FP32 blocks of GTB_BLK positions, each block folded into a Neumaier
+ *    compensated FP32 total;
+ *  - rotation solve in FP64 by the quaternion characteristic polynomial
+ *    (Horn 1987; Theobald 2005 "QCP"): Newton iteration for the largest
+ *    eigenvalue, eigenvector from the adjugate of (K - lambda I);
+ *  - the reported TM-scores and RMSD are recomputed in FP64 from the final
+ *    alignment and transform; |FP32 path - FP64| is reported per pair.
+ *  - d0 / d8 constants are FP32 values of the reference formulas
+ *    (cbrtf/powf of glibc), tabulated per length on the host.
+ */
+#include <math.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+#include "gtoracle.h"
+
+#define GTB_BLK 32
+#define LARGEDST 999999.9f
+#define LARGEDST_CMP 399999.9f
+#define RM_CONVEPS 1.e-5f
+#define SCORE_CONVEPS 1.e-6f
+#define FRAG_NSUB 6
+#define FRAG_STEP 40
+#define NMAXCONVIT 20
+#define FIN_MAXNPOS 128
+#define MINFRAGLEN 4
+
+#define CONV_SCOREDP 2
+#define CONV_LOWTMSC 8
+
+enum { BT_STOP = 0, BT_LEFT = 1, BT_UP = 2, BT_DIAG = 3 };
+
+/* ------------------------------------------------------------------------ */
+/* constants: stagecnsts.cuh:48-175                                          */
+static float c_d0(int lq, int lr) {
+    float l = (float)(lq < lr ? lq : lr);
+    float d0 = 0.168f;
+    if (l > 19.f) d0 = 1.24f * cbrtf(l - 15.f) - 1.8f;
+    return d0 + 0.8f;
+}
+static float c_d82(int lq, int lr) {
+    float l = (float)(lq < lr ? lq : lr);
+    float d8 = 1.5f * powf(l, 0.3f) + 3.5f;
+    return d8 * d8;
+}
+static float c_d0fin(int lq, int lr) {
+    float l = (float)(lq < lr ? lq : lr);
+    float d0 = 0.5f;
+    if (l > 21.f) d0 = 1.24f * cbrtf(l - 15.f) - 1.8f;
+    if (d0 < 0.5f) d0 = 0.5f;
+    return d0;
+}
+static float c_d0s(float d0) {
+    float d = d0;
+    d = d < 8.f ? d : 8.f;
+    d = d > 4.5f ? d : 4.5f;
+    return d;
+}
+void gto_constants(int lq, int lr, float* d0, float* d02, float* d82,
+                   float* d0fin, float* d02dpscan) {
+    float a = c_d0(lq, lr);
+    if (d0) *d0 = a;
+    if (d02) *d02 = a * a;
+    if (d82) *d82 = c_d82(lq, lr);
+    if (d0fin) *d0fin = c_d0fin(lq, lr);
+    if (d02dpscan) { float b = a + 1.5f; *d02dpscan = b * b; }
+}
+
+/* fragment.cuh:30-110 */
+static int frag_length(int alnlen, int sfragndx) {
+    if (alnlen < 4 && sfragndx == 0) return alnlen;
+    int a = alnlen >> sfragndx;
+    if (a == 2 && 0 < sfragndx && ((alnlen >> (sfragndx - 1)) & 1)) a = 4;
+    if (a < 3) return 0;
+    if (a < 4) a = 4;
+    if (sfragndx + 1 == FRAG_NSUB) a = 4;
+    return a;
+}
+static int max_nfrag_steps(int maxalnlen, int step, int fraglen) {
+    return (int)ceilf((float)(maxalnlen + step - fraglen) / step);
+}
+
+/* ------------------------------------------------------------------------ */
+/* geometry primitives (fixed FMA placement)                                 */
+static inline void xform(const float* t, float x, float y, float z,
+                         float* ox, float* oy, float* oz) {
+    *ox = fmaf(t[0], x, fmaf(t[1], y, fmaf(t[2], z, t[9])));
+    *oy = fmaf(t[3], x, fmaf(t[4], y, fmaf(t[5], z, t[10])));
+    *oz = fmaf(t[6], x, fmaf(t[7], y, fmaf(t[8], z, t[11])));
+}
+static inline float dist2_tf(const float* t, float qx, float qy, float qz,
+                             float rx, float ry, float rz) {
+    float x, y, z;
+    xform(t, qx, qy, qz, &x, &y, &z);
+    float dx = x - rx, dy = y - ry, dz = z - rz;
+    return fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+}
+
+/* ------------------------------------------------------------------------ */
+/* block-compensated sums                                                    */
+static inline void nfold(float* s, float* c, float* b) {
+    float t = *s + *b;
+    if (fabsf(*s) >= fabsf(*b)) *c += (*s - t) + *b;
+    else *c += (*b - t) + *s;
+    *s = t;
+    *b = 0.f;
+}
+
+typedef struct { float s[15], c[15], b[15]; int n; } ccacc;
+static void cc_init(ccacc* a) { memset(a, 0, sizeof(*a)); }
+static inline void cc_add(ccacc* a, float qx, float qy, float qz,
+                          float rx, float ry, float rz) {
+    a->b[0] = fmaf(qx, rx, a->b[0]); a->b[1] = fmaf(qx, ry, a->b[1]); a->b[2] = fmaf(qx, rz, a->b[2]);
+    a->b[3] = fmaf(qy, rx, a->b[3]); a->b[4] = fmaf(qy, ry, a->b[4]); a->b[5] = fmaf(qy, rz, a->b[5]);
+    a->b[6] = fmaf(qz, rx, a->b[6]); a->b[7] = fmaf(qz, ry, a->b[7]); a->b[8] = fmaf(qz, rz, a->b[8]);
+    a->b[9] += qx; a->b[10] += qy; a->b[11] += qz;
+    a->b[12] += rx; a->b[13] += ry; a->b[14] += rz;
+    a->n++;
+}
+static inline void cc_fold(ccacc* a) { for (int f = 0; f < 15; f++) nfold(&a->s[f], &a->c[f], &a->b[f]); }
+/* final: 16 values (15 sums + n) */
+static void cc_final(ccacc* a, float* v) {
+    cc_fold(a);
+    for (int f = 0; f < 15; f++) v[f] = a->s[f] + a->c[f];
+    v[15] = (float)a->n;
+}
+
+/* ------------------------------------------------------------------------ */
+/* FP64 rotation solve (quaternion characteristic polynomial)               */
+static double det3(double a, double b, double c, double d, double e, double f,
+                   double g, double h, double i) {
+    return a * (e * i - f * h) - b * (d * i - f * g) + c * (d * h - e * g);
+}
+/* cofactor (i,j) of symmetric 4x4 M */
+static double cof4(const double M[4][4], int i, int j) {
+    double m[9];
+    int k = 0;
+    for (int r = 0; r < 4; r++) {
+        if (r == i) continue;
+        for (int c = 0; c < 4; c++) {
+            if (c == j) continue;
+            m[k++] = M[r][c];
+        }
+    }
+    double d = det3(m[0], m[1], m[2], m[3], m[4], m[5], m[6], m[7], m[8]);
+    return ((i + j) & 1) ? -d : d;
+}
+
+/* Largest eigenvalue of Horn's key matrix for S (S[a][b] = sum x_a y_b,
+ * centred).  Returns lambda; fills N. */
+static double qcp_lambda(const double S[3][3], double N[4][4]) {
+    double Sxx = S[0][0], Sxy = S[0][1], Sxz = S[0][2];
+    double Syx = S[1][0], Syy = S[1][1], Syz = S[1][2];
+    double Szx = S[2][0], Szy = S[2][1], Szz = S[2][2];
+    N[0][0] = Sxx + Syy + Szz; N[0][1] = Syz - Szy; N[0][2] = Szx - Sxz; N[0][3] = Sxy - Syx;
+    N[1][1] = Sxx - Syy - Szz; N[1][2] = Sxy + Syx; N[1][3] = Szx + Sxz;
+    N[2][2] = -Sxx + Syy - Szz; N[2][3] = Syz + Szy;
+    N[3][3] = -Sxx - Syy + Szz;
+    N[1][0] = N[0][1]; N[2][0] = N[0][2]; N[3][0] = N[0][3];
+    N[2][1] = N[1][2]; N[3][1] = N[1][3]; N[3][2] = N[2][3];
+    double ss = 0.0;
+    for (int a = 0; a < 3; a++)
+        for (int b = 0; b < 3; b++) ss += S[a][b] * S[a][b];
+    double c2 = -2.0 * ss;
+    double c1 = -8.0 * det3(Sxx, Sxy, Sxz, Syx, Syy, Syz, Szx, Szy, Szz);
+    /* det(N) by cofactor expansion along row 0 */
+    double c0 = 0.0;
+    for (int j = 0; j < 4; j++) c0 += N[0][j] * cof4(N, 0, j);
+    double lam = sqrt(3.0 * ss);
+    double lam0 = lam;
+    for (int it = 0; it < 50; it++) {
+        double l2 = lam * lam;
+        double p = (l2 + c2) * l2 + c1 * lam + c0;
+        double dp = 4.0 * l2 * lam + 2.0 * c2 * lam + c1;
+        if (!(dp != 0.0)) break;
+        double step = p / dp;
+        lam -= step;
+        if (fabs(step) <= 1.e-13 * lam0) break;
+    }
+    return lam;
+}
+
+/* Rotation (row-major) rotating x onto y from S; returns 0 on degenerate. */
+static int qcp_rotation(const double S[3][3], double R[9], double* lamout) {
+    double N[4][4];
+    double lam = qcp_lambda(S, N);
+    if (lamout) *lamout = lam;
+    for (int i = 0; i < 4; i++) N[i][i] -= lam;
+    double dg[4];
+    int jm = 0;
+    for (int j = 0; j < 4; j++) {
+        dg[j] = cof4(N, j, j);
+        if (fabs(dg[j]) > fabs(dg[jm])) jm = j;
+    }
+    double l3 = fabs(lam) * lam * lam;
+    if (!(fabs(dg[jm]) > 1.e-14 * l3) || !(lam > 0.0)) return 0;
+    double q[4], qn = 0.0;
+    for (int i = 0; i < 4; i++) { q[i] = cof4(N, i, jm); qn += q[i] * q[i]; }
+    if (!(qn > 0.0)) return 0;
+    qn = 1.0 / sqrt(qn);
+    double a = q[0] * qn, b = q[1] * qn, c = q[2] * qn, d = q[3] * qn;
+    R[0] = a * a + b * b - c * c - d * d; R[1] = 2.0 * (b * c - a * d);     R[2] = 2.0 * (b * d + a * c);
+    R[3] = 2.0 * (b * c + a * d);     R[4] = a * a - b * b + c * c - d * d; R[5] = 2.0 * (c * d - a * b);
+    R[6] = 2.0 * (b * d - a * c);     R[7] = 2.0 * (c * d + a * b);     R[8] = a * a - b * b - c * c + d * d;
+    return 1;
+}
+
+/* sums: [0..8] sum q_i r_j, [9..11] sum q, [12..14] sum r; n.
+ * tfm rotates/translates the query onto the reference (row-major R, t). */
+static int solve_sums(const float* v, int n, int swap, float* tfm) {
+    double dn = (double)n;
+    double mq[3], mr[3], S[3][3];
+    for (int i = 0; i < 3; i++) { mq[i] = (double)v[9 + i] / dn; mr[i] = (double)v[12 + i] / dn; }
+    for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++)
+            S[i][j] = (double)v[3 * i + j] - dn * mq[i] * mr[j];
+    double R[9];
+    int ok;
+    if (!swap) {
+        ok = qcp_rotation(S, R, NULL);
+        if (!ok) { memset(R, 0, sizeof(R)); R[0] = R[4] = R[8] = 1.0; }
+        double t[3];
+        for (int i = 0; i < 3; i++) t[i] = mr[i] - (R[3*i] * mq[0] + R[3*i+1] * mq[1] + R[3*i+2] * mq[2]);
+        for (int k = 0; k < 9; k++) tfm[k] = (float)R[k];
+        for (int i = 0; i < 3; i++) tfm[9 + i] = (float)t[i];
+    } else {
+        /* rotate the reference onto the query, then invert */
+        double St[3][3];
+        for (int i = 0; i < 3; i++)
+            for (int j = 0; j < 3; j++) St[i][j] = S[j][i];
+        ok = qcp_rotation(St, R, NULL);
+        if (!ok) { memset(R, 0, sizeof(R)); R[0] = R[4] = R[8] = 1.0; }
+        double t[3];
+        for (int i = 0; i < 3; i++) t[i] = mq[i] - (R[3*i] * mr[0] + R[3*i+1] * mr[1] + R[3*i+2] * mr[2]);
+        /* inverse: R^T, -R^T t */
+        for (int i = 0; i < 3; i++)
+            for (int j = 0; j < 3; j++) tfm[3 * i + j] = (float)R[3 * j + i];
+        for (int i = 0; i < 3; i++)
+            tfm[9 + i] = (float)(-(R[i] * t[0] + R[3 + i] * t[1] + R[6 + i] * t[2]));
+    }
+    return ok;
+}
+
+int gto_solve(const float* sums15, int n, float* tfm12) {
+    return solve_sums(sums15, n, 0, tfm12);
+}
+
+/* ------------------------------------------------------------------------ */
+/* secondary structure: MpSecStr.cpp:26-118, MpSecStr.h:218-249              */
+static float ss_dst(const float* x, const float* y, const float* z, int i, int j) {
+    float dx = x[i] - x[j], dy = y[i] - y[j], dz = z[i] - z[j];
+    float a = dx * dx;
+    float b = dy * dy;
+    float c = dz * dz;
+    return sqrtf((a + b) + c);
+}
+void gto_secstr(int len, const float* x, const float* y, const float* z, char* ss) {
+    for (int p = 0; p < len; p++) ss[p] = ' ';
+    for (int p = 2; p + 2 < len; p++) {
+        float d13 = ss_dst(x, y, z, p - 2, p);
+        float d14 = ss_dst(x, y, z, p - 2, p + 1);
+        float d15 = ss_dst(x, y, z, p - 2, p + 2);
+        float d24 = ss_dst(x, y, z, p - 1, p + 1);
+        float d25 = ss_dst(x, y, z, p - 1, p + 2);
+        float d35 = ss_dst(x, y, z, p, p + 2);
+        float e = 2.1f;
+        char s = ' ';
+        if (fabsf(d15 - 6.37f) < e && fabsf(d14 - 5.18f) < e && fabsf(d25 - 5.18f) < e &&
+            fabsf(d13 - 5.45f) < e && fabsf(d24 - 5.45f) < e && fabsf(d35 - 5.45f) < e)
+            s = 'h';
+        else {
+            e = 1.42f;
+            if (fabsf(d15 - 13.0f) < e && fabsf(d14 - 10.4f) < e && fabsf(d25 - 10.4f) < e &&
+                fabsf(d13 - 6.1f) < e && fabsf(d24 - 6.1f) < e && fabsf(d35 - 6.1f) < e)
+                s = 'e';
+            else if (d15 < 8.0f)
+                s = 't';
+        }
+        ss[p] = s;
+    }
+}
+
+/* ------------------------------------------------------------------------ */
+/* pair context                                                              */
+typedef struct {
+    int lq, lr;
+    const float *qx, *qy, *qz, *rx, *ry, *rz;
+    const unsigned char *qa, *ra;
+    const char *qs, *rs;
+    int qmol, rmol;
+    /* chunk-level values */
+    int qmax, rmax, qmin, rmin;
+    const gto_opts* o;
+    /* state */
+    int flags;
+    float grand, best, best0;
+    int seedq, seedr;
+    int naln;
+    int sfndx, sfpos;           /* fragment of the final-phase-1 winner */
+    int sfndx_cur, sfpos_cur;
+    float tfm_ib[12], tfm_gr[12];
+    int *aq, *ar;               /* aligned pairs, forward order */
+    float *ad;                  /* constrained: dist2 */
+    unsigned char* bt;          /* traceback lq*lr */
+    float *h0, *h1;
+    float out[GTO_NOUT];
+    float err[GTO_NERR];
+    float d0, d02, d82, d0fin, d0s;
+} pairctx;
+
+static void tfm_identity(float* t) { memset(t, 0, 12 * sizeof(float)); t[0] = t[4] = t[8] = 1.f; }
+
+/* positions of k-space: 0 = gapless diagonal from (q0,r0); 1 = aligned pairs */
+typedef struct { int mode; int q0, r0; const int *aq, *ar; } kspace;
+static inline void kpos(const kspace* s, int k, int* q, int* r) {
+    if (s->mode == 0) { *q = s->q0 + k; *r = s->r0 + k; }
+    else { *q = s->aq[k]; *r = s->ar[k]; }
+}
+
+/* covariance over [k0,k1) (all positions) */
+static void cov_range(const pairctx* P, const kspace* s, int k0, int k1, float* v) {
+    ccacc a; cc_init(&a);
+    int blk = 0;
+    for (int k = k0; k < k1; k++) {
+        int q, r; kpos(s, k, &q, &r);
+        cc_add(&a, P->qx[q], P->qy[q], P->qz[q], P->rx[r], P->ry[r], P->rz[r]);
+        if (++blk == GTB_BLK) { cc_fold(&a); blk = 0; }
+    }
+    cc_final(&a, v);
+}
+/* covariance over [0,n) of positions with dist2(tfm) <= thr */
+static void cov_ext(const pairctx* P, const kspace* s, int n, const float* tfm,
+                    float thr, float* v) {
+    ccacc a; cc_init(&a);
+    int blk = 0;
+    for (int k = 0; k < n; k++) {
+        int q, r; kpos(s, k, &q, &r);
+        float qx = P->qx[q], qy = P->qy[q], qz = P->qz[q];
+        float rx = P->rx[r], ry = P->ry[r], rz = P->rz[r];
+        float d = dist2_tf(tfm, qx, qy, qz, rx, ry, rz);
+        if (d <= thr) cc_add(&a, qx, qy, qz, rx, ry, rz);
+        if (++blk == GTB_BLK) { cc_fold(&a); blk = 0; }
+    }
+    cc_final(&a, v);
+}
+
+/* score pass over [0,n); chk: only d<=d82 contribute;
+ * m3mode: 0 none, 1 distinct (findfrag), 2 multiset (refinement) */
+static float score_pass(const pairctx* P, const kspace* s, int n, const float* tfm,
+                        float d02, int chk, float d82, int m3mode, float* m3out) {
+    float ss = 0.f, sc = 0.f, sb = 0.f;
+    int blk = 0;
+    float m1 = LARGEDST, m2 = LARGEDST, m3 = LARGEDST;
+    for (int k = 0; k < n; k++) {
+        int q, r; kpos(s, k, &q, &r);
+        float d = dist2_tf(tfm, P->qx[q], P->qy[q], P->qz[q], P->rx[r], P->ry[r], P->rz[r]);
+        if (!chk || d <= d82) sb += d02 / (d02 + d);
+        if (m3mode == 2) {
+            if (d < m1) { m3 = m2; m2 = m1; m1 = d; }
+            else if (d < m2) { m3 = m2; m2 = d; }
+            else if (d < m3) m3 = d;
+        } else if (m3mode == 1) {
+            if (d < m1) { m3 = m2; m2 = m1; m1 = d; }
+            else if (d > m1 && d < m2) { m3 = m2; m2 = d; }
+            else if (d > m2 && d < m3) m3 = d;
+        }
+        if (++blk == GTB_BLK) { nfold(&ss, &sc, &sb); blk = 0; }
+    }
+    nfold(&ss, &sc, &sb);
+    if (m3out) *m3out = m3;
+    return ss + sc;
+}
+
+/* convergence of all 16 fields: MpStageBase.h:244-264 */
+static int converged16(const float* a, const float* b) {
+    int cnt = 0;
+    for (int f = 0; f < 16; f++) {
+        float x = a[f], y = b[f];
+        float m = fabsf(x) < fabsf(y) ? fabsf(x) : fabsf(y);
+        if (fabsf(x - y) < m * RM_CONVEPS) cnt++;
+    }
+    return cnt >= 16;
+}
+
+static int solve_pair(const pairctx* P, const float* v, float* tfm) {
+    int n = (int)v[15];
+    int swap = P->o->symmetric && (P->lq < P->lr);
+    return solve_sums(v, n, swap, tfm);
+}
+
+/* ------------------------------------------------------------------------ */
+/* stage 1: fragment seed, MpStage1.cpp:289-440 (per offset)                 */
+static float findfrag_variant(const pairctx* P, int qpos, int rpos, int n) {
+    kspace s = {0, qpos, rpos, NULL, NULL};
+    float v[16], tfm[12], m3, best = 0.f;
+    float d02s0 = P->d0s * P->d0s;
+    cov_range(P, &s, 0, n, v);
+    for (int it = 0; it < 3; it++) {
+        solve_pair(P, v, tfm);
+        int save = (it < 2);
+        float sc = score_pass(P, &s, n, tfm, P->d02, 0, 0.f, save ? 1 : 0, &m3);
+        if (best < sc) best = sc;
+        if (!save) break;
+        float d02s = d02s0 + (it == 1 ? 1.0f : 0.0f);
+        float dst32;
+        if (LARGEDST_CMP < m3 || m3 < d02s || n <= 3) dst32 = d02s;
+        else dst32 = d02s + ceilf((m3 - d02s) * 2.0f) * 0.5f;
+        cov_ext(P, &s, n, tfm, dst32, v);
+        if (v[15] < 1.0f) break;
+        if ((int)v[15] == n) break;
+    }
+    return best;
+}
+
+static void stage1_findfrag(pairctx* P) {
+    if (P->flags & CONV_LOWTMSC) return;
+    int minlenmin = P->qmin < P->rmin ? P->qmin : P->rmin;
+    int minalnmin = (minlenmin >> 1) > 5 ? (minlenmin >> 1) : 5;
+    int n1 = minalnmin - P->rmax;
+    int n2 = P->qmax - minalnmin;
+    int step = P->o->stepinit;
+    int nsteps = (n2 - n1) / step + 1;
+    int prv = (P->lq < P->lr ? P->lq : P->lr) >> 1;
+    if (prv < 5) prv = 5;
+    float best = 0.f;
+    int bq = 0, br = 0;
+    for (int si = 0; si < nsteps; si++) {
+        int ab = n1 + si * step;
+        int qpos = ab > 0 ? ab : 0;
+        int rpos = -ab > 0 ? -ab : 0;
+        if (P->lq <= qpos || P->lr <= rpos) continue;
+        if (P->lq - qpos < prv || P->lr - rpos < prv) continue;
+        int n = (P->lq - qpos) < (P->lr - rpos) ? (P->lq - qpos) : (P->lr - rpos);
+        float b = findfrag_variant(P, qpos, rpos, n);
+        if (b > 0.f && best < b) { best = b; bq = qpos; br = rpos; }
+    }
+    P->best = best;
+    P->seedq = bq;
+    P->seedr = br;
+}
+
+/* generic refinement loop: MpStage1.cpp:640-700 (and its copies) */
+static void refine_loop(const pairctx* P, const kspace* s, int nrange, int kf, int fraglen,
+                        float d0, float d02, int chk, float d82, float best_init,
+                        float* bestout, float* tfmbest) {
+    float v[16], last[16], tfm[12], m3 = LARGEDST, dst32 = LARGEDST;
+    float best = best_init;
+    float d0s = c_d0s(d0);
+    float thr2 = (d0s + 1.0f) * (d0s + 1.0f);
+    cov_range(P, s, kf, kf + fraglen, v);
+    float prev_tfm[12];
+    for (int cit = 0; cit < NMAXCONVIT + 2; cit++) {
+        if (cit > 0) {
+            cov_ext(P, s, nrange, prev_tfm, (cit < 2) ? dst32 : thr2, v);
+            if (converged16(v, last)) break;
+        }
+        if (v[15] < 1.0f) break;
+        memcpy(last, v, sizeof(last));
+        solve_pair(P, v, tfm);
+        float sc = score_pass(P, s, nrange, tfm, d02, chk, d82, cit < 1 ? 2 : 0, &m3);
+        if (cit < 1) {
+            float d0sm = d0s - 1.0f;
+            float d02s = d0sm * d0sm;
+            if (LARGEDST_CMP < m3 || m3 < d02s || nrange <= 3) dst32 = d02s;
+            else {
+                float t = d0sm + ceilf((sqrtf(m3) - d0sm) * 2.0f) * 0.5f;
+                dst32 = t * t;
+            }
+        }
+        if (best < sc) { best = sc; memcpy(tfmbest, tfm, sizeof(tfm)); }
+        memcpy(prev_tfm, tfm, sizeof(tfm));
+    }
+    *bestout = best;
+}
+
+/* variant enumeration of the 6-length x step-40 refinement */
+static int nlocsteps_refine(const pairctx* P) {
+    int maxalnmax = P->qmax < P->rmax ? P->qmax : P->rmax;
+    return max_nfrag_steps(maxalnmax, FRAG_STEP, MINFRAGLEN) * FRAG_NSUB;
+}
+
+/* RefineFragInit (dpmode 0) and RefineFragDP (dpmode 1) and FinalPhase1
+ * (dpmode 2): winner = max score > 0, lowest variant index on ties. */
+static void refine_stage(pairctx* P, int dpmode, float d0, float d02, int chk,
+                         float best_init, int grandupd, int writefrag) {
+    int nloc = nlocsteps_refine(P);
+    kspace s;
+    int nrange;
+    if (dpmode == 0) {
+        s.mode = 0; s.q0 = P->seedq; s.r0 = P->seedr; s.aq = s.ar = NULL;
+        if (P->lq <= P->seedq || P->lr <= P->seedr) nrange = 0;
+        else nrange = (P->lq - P->seedq) < (P->lr - P->seedr) ? (P->lq - P->seedq) : (P->lr - P->seedr);
+    } else {
+        s.mode = 1; s.aq = P->aq; s.ar = P->ar; s.q0 = s.r0 = 0;
+        nrange = P->naln;
+    }
+    float wbest = 0.f, wtfm[12];
+    int wsi = -1, wndx = 0, wpos = 0;
+    for (int si = 0; si < nloc && nrange > 0; si++) {
+        int sfragfct = si / FRAG_NSUB, sfragndx = si % FRAG_NSUB;
+        int fraglen = frag_length(nrange, sfragndx);
+        if (fraglen < 1) continue;
+        int sfragpos = sfragfct * FRAG_STEP;
+        if (nrange + FRAG_STEP <= sfragpos + fraglen) continue;
+        int delta = sfragpos + fraglen - nrange;
+        int kf = sfragpos - (delta > 0 ? delta : 0);
+        float best, tb[12];
+        refine_loop(P, &s, nrange, kf, fraglen, d0, d02, chk, P->d82, best_init, &best, tb);
+        if (best > 0.f && wbest < best) {
+            wbest = best; wsi = si; memcpy(wtfm, tb, sizeof(wtfm));
+            wndx = sfragndx; wpos = sfragpos;
+        }
+    }
+    P->best = wbest;
+    if (wsi >= 0) memcpy(P->tfm_ib, wtfm, sizeof(wtfm));
+    if (writefrag) {
+        if (wsi >= 0) { P->sfndx_cur = wndx; P->sfpos_cur = wpos; }
+        P->sfndx = P->sfndx_cur; P->sfpos = P->sfpos_cur;
+    }
+    if (grandupd && P->grand < wbest) {
+        P->grand = wbest;
+        memcpy(P->tfm_gr, wtfm, sizeof(wtfm));
+    }
+}
+
+/* Final phase 2, MpStageFin.cpp:270-480 */
+static void final_phase2(pairctx* P) {
+    int maxalnmax = P->qmax < P->rmax ? P->qmax : P->rmax;
+    int nf = 2 * maxalnmax < FIN_MAXNPOS ? 2 * maxalnmax : FIN_MAXNPOS;
+    kspace s = {1, 0, 0, P->aq, P->ar};
+    int n = P->naln;
+    float wbest = 0.f, wtfm[12];
+    int wsi = -1;
+    for (int si = 0; si < nf; si++) {
+        int sfragndx = P->sfndx;
+        int sfragpos = P->sfpos;
+        if (sfragndx == 0) sfragndx++;
+        sfragpos += (si - (nf >> 1));
+        int fraglen = frag_length(n, sfragndx);
+        if (fraglen < 1) continue;
+        if (sfragpos < 0 || n + 1 <= sfragpos + fraglen) continue;
+        float best, tb[12];
+        refine_loop(P, &s, n, sfragpos, fraglen, P->d0, P->d02, 1, P->d82, -1.0f, &best, tb);
+        if (best > 0.f && wbest < best) { wbest = best; wsi = si; memcpy(wtfm, tb, sizeof(wtfm)); }
+    }
+    P->best = wbest;
+    if (wsi >= 0) memcpy(P->tfm_ib, wtfm, sizeof(wtfm));
+    if (P->grand < wbest) { P->grand = wbest; memcpy(P->tfm_gr, wtfm, sizeof(wtfm)); }
+}
+
+/* ------------------------------------------------------------------------ */
+/* DP: MpDPHub.cpp:72-346 (plain) and :686-940 (grand tfm + SS)            */
+static void dp_run(pairctx* P, const float* tfm, int gap0, float gcost, int usess,
+                   float d02) {
+    int lq = P->lq, lr = P->lr;
+    float* prev = P->h0;   /* row i-1 */
+    float* cur = P->h1;
+    for (int j = 0; j < lr; j++) prev[j] = 0.f;
+    for (int i = 0; i < lq; i++) {
+        float tx, ty, tz;
+        xform(tfm, P->qx[i], P->qy[i], P->qz[i], &tx, &ty, &tz);
+        char qs = usess ? P->qs[i] : 0;
+        float left = 0.f;          /* H[i][j-1], boundary 0 */
+        for (int j = 0; j < lr; j++) {
+            float dx = tx - P->rx[j], dy = ty - P->ry[j], dz = tz - P->rz[j];
+            float d = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+            float v = d02 / (d02 + d);
+            if (usess) v += (float)(qs == P->rs[j]) * 0.5f;
+            float dg = (j > 0) ? prev[j - 1] : 0.f;
+            v += gap0 ? dg : fabsf(dg);
+            int bk = BT_DIAG;
+            float l = left;
+            if (!gap0 && l < 0.f) l = gcost - l;
+            if (v < l) { v = l; bk = BT_LEFT; }
+            float u = prev[j];
+            if (!gap0 && u < 0.f) u = gcost - u;
+            if (v < u) { v = u; bk = BT_UP; }
+            float w = (gap0 || bk != BT_DIAG) ? v : -v;
+            cur[j] = w;
+            left = w;
+            P->bt[(size_t)i * lr + j] = (unsigned char)bk;
+        }
+        float* t = prev; prev = cur; cur = t;
+    }
+}
+
+/* unconstrained traceback: MpDPHub.cpp:1515-1660 */
+static void btck_matched(pairctx* P) {
+    int y = P->lq - 1, x = P->lr - 1, n = 0;
+    while (x >= 0 && y >= 0) {
+        int b = P->bt[(size_t)y * P->lr + x];
+        if (b == BT_UP) { y--; continue; }
+        if (b == BT_LEFT) { x--; continue; }
+        P->aq[n] = y; P->ar[n] = x; n++;
+        x--; y--;
+    }
+    /* reverse to forward order */
+    for (int i = 0, j = n - 1; i < j; i++, j--) {
+        int t = P->aq[i]; P->aq[i] = P->aq[j]; P->aq[j] = t;
+        t = P->ar[i]; P->ar[i] = P->ar[j]; P->ar[j] = t;
+    }
+    P->naln = n;
+}
+
+/* constrained traceback: keep d2 <= d82 under the grand tfm */
+static void btck_constrained(pairctx* P) {
+    int y = P->lq - 1, x = P->lr - 1, n = 0;
+    while (x >= 0 && y >= 0) {
+        int b = P->bt[(size_t)y * P->lr + x];
+        if (b == BT_UP) { y--; continue; }
+        if (b == BT_LEFT) { x--; continue; }
+        float d = dist2_tf(P->tfm_gr, P->qx[y], P->qy[y], P->qz[y], P->rx[x], P->ry[x], P->rz[x]);
+        if (d <= P->d82) { P->aq[n] = y; P->ar[n] = x; P->ad[n] = d; n++; }
+        x--; y--;
+    }
+    for (int i = 0, j = n - 1; i < j; i++, j--) {
+        int t = P->aq[i]; P->aq[i] = P->aq[j]; P->aq[j] = t;
+        t = P->ar[i]; P->ar[i] = P->ar[j]; P->ar[j] = t;
+        float f = P->ad[i]; P->ad[i] = P->ad[j]; P->ad[j] = f;
+    }
+    P->naln = n;
+}
+
+/* DP + traceback with the iteration-best transform (DPRefine body) */
+static int dp_skip_plain(const pairctx* P) {
+    return (P->flags & CONV_LOWTMSC) || (P->flags & CONV_SCOREDP);
+}
+
+static void dprefine(pairctx* P, int gap0, int prescreen, int maxit) {
+    float gcost = gap0 ? 0.0f : -0.6f;
+    for (int dpi = 0; dpi < maxit; dpi++) {
+        if (!dp_skip_plain(P)) {
+            dp_run(P, P->tfm_ib, gap0, gcost, 0, P->d02);
+            btck_matched(P);
+        } else P->naln = 0;
+        if (P->flags) P->best = 0.f;   /* variants skipped: slot bests were reset */
+        else refine_stage(P, 1, P->d0, P->d02, 1, 0.f, 1, 0);
+        if (0 < dpi && !(P->flags & (CONV_SCOREDP | CONV_LOWTMSC)) &&
+            fabsf(P->best - P->best0) < SCORE_CONVEPS)
+            P->flags |= CONV_SCOREDP;
+        if (dpi + 1 < maxit && !(P->flags & (CONV_SCOREDP | CONV_LOWTMSC)))
+            P->best0 = P->best;
+        if (prescreen && maxit <= dpi + 1 && 0.0f < P->o->prescore) {
+            int ml = P->lq < P->lr ? P->lq : P->lr;
+            if (P->grand < P->o->prescore * (float)ml) P->flags |= CONV_LOWTMSC;
+        }
+    }
+    P->flags &= ~CONV_SCOREDP;
+}
+
+/* ------------------------------------------------------------------------ */
+/* production scores: MpStageFin.cpp:747-1000 and :1310-1525                 */
+typedef struct { float best, gbest; float tfm[12]; int ndx, pos; int si; } prodwin;
+
+static void prod_variant(const pairctx* P, const kspace* s, int n, int kf, int fraglen,
+                         float* best, float* gbest, float* tb) {
+    refine_loop(P, s, n, kf, fraglen, P->d0fin, P->d0fin * P->d0fin, 0, P->d82, -1.0f, best, tb);
+    if (*best < 0.f) { *gbest = *best; return; }   /* nothing computed */
+    if (P->lq != P->lr) {
+        int gl = P->lq > P->lr ? P->lq : P->lr;
+        float g0 = c_d0fin(gl, gl);
+        *gbest = score_pass(P, s, n, tb, g0 * g0, 0, P->d82, 0, NULL);
+    } else *gbest = *best;
+}
+
+static void prod_write(pairctx* P, const prodwin* w) {
+    float bs = w->best, gb = w->gbest;
+    if ((float)P->lr < (float)P->lq) { float t = bs; bs = gb; gb = t; }
+    P->out[GTO_SCOREQ] = bs / (float)P->lq;
+    P->out[GTO_SCORER] = gb / (float)P->lr;
+    P->out[GTO_D0Q] = c_d0fin(P->lq, P->lq);
+    P->out[GTO_D0R] = c_d0fin(P->lr, P->lr);
+    memcpy(P->tfm_gr, w->tfm, sizeof(w->tfm));
+}
+
+static double rmsd_from_sums(const double* v, double n) {
+    /* v: [0..8] sum q_i r_j, [9..11] sum q, [12..14] sum r, [15..17] sum q^2, [18..20] sum r^2 */
+    double mq[3], mr[3], S[3][3], E0 = 0.0;
+    for (int i = 0; i < 3; i++) { mq[i] = v[9 + i] / n; mr[i] = v[12 + i] / n; }
+    for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++) S[i][j] = v[3 * i + j] - n * mq[i] * mr[j];
+    for (int i = 0; i < 3; i++) E0 += (v[15 + i] - n * mq[i] * mq[i]) + (v[18 + i] - n * mr[i] * mr[i]);
+    double N[4][4];
+    double lam = qcp_lambda(S, N);
+    double e = (E0 - 2.0 * lam) / n;
+    return e > 0.0 ? sqrt(e) : 0.0;
+}
+
+static void production(pairctx* P) {
+    kspace s = {1, 0, 0, P->aq, P->ar};
+    int n = P->naln;
+    int nloc = nlocsteps_refine(P);
+    /* phase 1 */
+    prodwin w; w.best = 0.f; w.si = -1;
+    float rmsd32 = -1.f;
+    for (int si = 0; si < nloc && n > 0; si++) {
+        int sfragfct = si / FRAG_NSUB, sfragndx = si % FRAG_NSUB;
+        int fraglen = frag_length(n, sfragndx);
+        if (fraglen < 1) continue;
+        int sfragpos = sfragfct * FRAG_STEP;
+        if (n + FRAG_STEP <= sfragpos + fraglen) continue;
+        int delta = sfragpos + fraglen - n;
+        int kf = sfragpos - (delta > 0 ? delta : 0);
+        if (si == 0) {
+            /* RMSD over the full alignment from compensated FP32 sums */
+            float sq[6] = {0}, cq[6] = {0}, bq[6] = {0};
+            ccacc a; cc_init(&a);
+            int blk = 0;
+            for (int k = kf; k < kf + fraglen; k++) {
+                int q = P->aq[k], r = P->ar[k];
+                float qx = P->qx[q], qy = P->qy[q], qz = P->qz[q];
+                float rx = P->rx[r], ry = P->ry[r], rz = P->rz[r];
+                cc_add(&a, qx, qy, qz, rx, ry, rz);
+                bq[0] = fmaf(qx, qx, bq[0]); bq[1] = fmaf(qy, qy, bq[1]); bq[2] = fmaf(qz, qz, bq[2]);
+                bq[3] = fmaf(rx, rx, bq[3]); bq[4] = fmaf(ry, ry, bq[4]); bq[5] = fmaf(rz, rz, bq[5]);
+                if (++blk == GTB_BLK) {
+                    cc_fold(&a);
+                    for (int f = 0; f < 6; f++) nfold(&sq[f], &cq[f], &bq[f]);
+                    blk = 0;
+                }
+            }
+            float v[16];
+            cc_final(&a, v);
+            double dv[21];
+            for (int f = 0; f < 15; f++) dv[f] = v[f];
+            for (int f = 0; f < 6; f++) { nfold(&sq[f], &cq[f], &bq[f]); dv[15 + f] = (double)(sq[f] + cq[f]); }
+            rmsd32 = (float)rmsd_from_sums(dv, (double)fraglen);
+        }
+        float best, gbest, tb[12];
+        prod_variant(P, &s, n, kf, fraglen, &best, &gbest, tb);
+        if (best > 0.f && w.best < best) {
+            w.best = best; w.gbest = gbest; w.si = si; memcpy(w.tfm, tb, sizeof(tb));
+            w.ndx = sfragndx; w.pos = sfragpos;
+        }
+    }
+    if (w.si >= 0) {
+        P->grand = w.best;   /* unconditional production save */
+        prod_write(P, &w);
+        P->sfndx = w.ndx; P->sfpos = w.pos;
+    }
+    /* phase 2 (one-search and coarse) */
+    int maxalnmax = P->qmax < P->rmax ? P->qmax : P->rmax;
+    int nf = 2 * maxalnmax < FIN_MAXNPOS ? 2 * maxalnmax : FIN_MAXNPOS;
+    prodwin w2; w2.best = 0.f; w2.si = -1;
+    for (int si = 0; si < nf && n > 0; si++) {
+        int sfragndx = P->sfndx, sfragpos = P->sfpos;
+        sfragpos += (si - (nf >> 1));
+        if (sfragndx == 0) sfragndx++;
+        int fraglen = frag_length(n, sfragndx);
+        if (fraglen < 1) continue;
+        if (sfragpos < 0 || n + 1 <= sfragpos + fraglen) continue;
+        float best, gbest, tb[12];
+        prod_variant(P, &s, n, sfragpos, fraglen, &best, &gbest, tb);
+        if (best > 0.f && w2.best < best) {
+            w2.best = best; w2.gbest = gbest; w2.si = si; memcpy(w2.tfm, tb, sizeof(tb));
+        }
+    }
+    if (w2.si >= 0 && P->grand < w2.best) {
+        P->grand = w2.best;
+        prod_write(P, &w2);
+    }
+    /* FP64 recomputation of reported values */
+    if (n > 0) {
+        double d0q = c_d0fin(P->lq, P->lq), d0r = c_d0fin(P->lr, P->lr);
+        double d0q2 = d0q * d0q, d0r2 = d0r * d0r, tq = 0.0, tr = 0.0;
+        double dv[21];
+        memset(dv, 0, sizeof(dv));
+        const float* t = P->tfm_gr;
+        for (int k = 0; k < n; k++) {
+            int q = P->aq[k], r = P->ar[k];
+            double qx = P->qx[q], qy = P->qy[q], qz = P->qz[q];
+            double rx = P->rx[r], ry = P->ry[r], rz = P->rz[r];
+            double x = t[0] * qx + t[1] * qy + t[2] * qz + t[9];
+            double y = t[3] * qx + t[4] * qy + t[5] * qz + t[10];
+            double z = t[6] * qx + t[7] * qy + t[8] * qz + t[11];
+            double d = (x - rx) * (x - rx) + (y - ry) * (y - ry) + (z - rz) * (z - rz);
+            tq += d0q2 / (d0q2 + d);
+            tr += d0r2 / (d0r2 + d);
+            double qq[3] = {qx, qy, qz}, rr[3] = {rx, ry, rz};
+            for (int i = 0; i < 3; i++)
+                for (int j = 0; j < 3; j++) dv[3 * i + j] += qq[i] * rr[j];
+            for (int i = 0; i < 3; i++) {
+                dv[9 + i] += qq[i]; dv[12 + i] += rr[i];
+                dv[15 + i] += qq[i] * qq[i]; dv[18 + i] += rr[i] * rr[i];
+            }
+        }
+        double r64 = rmsd_from_sums(dv, (double)n);
+        if (rmsd32 >= 0.f) {
+            P->err[GTO_ERR_RMSD] = (float)fabs((double)rmsd32 - r64);
+            P->out[GTO_RMSD] = (float)r64;
+        }
+        if (P->out[GTO_SCOREQ] > 0.f || P->out[GTO_SCORER] > 0.f) {
+            double tmq = tq / P->lq, tmr = tr / P->lr;
+            P->err[GTO_ERR_TMQ] = (float)fabs((double)P->out[GTO_SCOREQ] - tmq);
+            P->err[GTO_ERR_TMR] = (float)fabs((double)P->out[GTO_SCORER] - tmr);
+            P->out[GTO_SCOREQ] = (float)tmq;
+            P->out[GTO_SCORER] = (float)tmr;
+        }
+    }
+}
+
+/* alignment strings: MpDPHub.cpp:1919-2125 */
+static void production_alignment(pairctx* P, char* dst) {
+    int W = P->lq + P->lr + 1;
+    char *rq = dst, *rm = dst + W, *rt = dst + 2 * W, *sq = dst + 3 * W, *st = dst + 4 * W;
+    int n = P->naln, col = 0, psts = 0, idts = 0, gaps = 0;
+    unsigned int bc = 0, ec = 0;
+    const float d2eq = 25.0f;
+    for (int k = 0; k < n; k++) {
+        int q = P->aq[k], r = P->ar[k];
+        float d = P->ad[k];
+        unsigned int cc = ((unsigned int)(r + 1) << 16) | (unsigned int)(q + 1);
+        if (k == 0) bc = cc;
+        ec = cc;
+        int eq = d < d2eq;
+        if (eq) psts++;
+        char a = (char)P->qa[q], b = (char)P->ra[r];
+        rq[col] = a; rt[col] = b; sq[col] = P->qs[q]; st[col] = P->rs[r];
+        char mc = eq ? '+' : ' ';
+        if (a != '-' && a == b) { idts++; mc = eq ? a : (char)(a | 32); }
+        rm[col] = mc;
+        col++;
+        if (k + 1 < n) {
+            int q1 = P->aq[k + 1], r1 = P->ar[k + 1];
+            for (int qq = q + 1; qq < q1; qq++) {
+                rq[col] = (char)P->qa[qq]; sq[col] = P->qs[qq];
+                rt[col] = '-'; st[col] = ' '; rm[col] = ' ';
+                col++; gaps++;
+            }
+            if (!P->o->nodeletions)
+                for (int rr = r + 1; rr < r1; rr++) {
+                    rt[col] = (char)P->ra[rr]; st[col] = P->rs[rr];
+                    rq[col] = '-'; sq[col] = ' '; rm[col] = ' ';
+                    col++; gaps++;
+                }
+        }
+    }
+    rq[col] = rm[col] = rt[col] = sq[col] = st[col] = 0;
+    union { unsigned int u; float f; } ub, ue;
+    ub.u = bc; ue.u = ec;
+    P->out[GTO_BEGCOORDS] = ub.f;
+    P->out[GTO_ENDCOORDS] = ue.f;
+    P->out[GTO_ALNLENGTH] = (float)col;
+    P->out[GTO_PSTVS] = (float)psts;
+    P->out[GTO_IDNTS] = (float)idts;
+    P->out[GTO_NGAPS] = (float)gaps;
+}
+
+/* ------------------------------------------------------------------------ */
+static void run_pair(pairctx* P, char* alndst) {
+    const gto_opts* o = P->o;
+    /* preinit: MpStage1.cpp:28-167 */
+    P->flags = (P->qmol != P->rmol) ? CONV_LOWTMSC : 0;
+    P->grand = P->best = P->best0 = 0.f;
+    P->seedq = P->seedr = 0;
+    P->naln = 0;
+    P->sfndx = P->sfpos = P->sfndx_cur = P->sfpos_cur = 0;
+    tfm_identity(P->tfm_ib);
+    tfm_identity(P->tfm_gr);
+    memset(P->out, 0, sizeof(P->out));
+    memset(P->err, 0, sizeof(P->err));
+    P->out[GTO_RMSD] = 9999.9f;
+    gto_constants(P->lq, P->lr, &P->d0, &P->d02, &P->d82, &P->d0fin, NULL);
+    P->d0s = c_d0s(P->d0);
+    float d02dpscan = (P->d0 + 1.5f) * (P->d0 + 1.5f);
+    if (alndst) alndst[0] = alndst[P->lq + P->lr + 1] = alndst[2 * (P->lq + P->lr + 1)] =
+        alndst[3 * (P->lq + P->lr + 1)] = alndst[4 * (P->lq + P->lr + 1)] = 0;
+
+    /* stage 1 */
+    stage1_findfrag(P);
+    if (!(P->flags & CONV_LOWTMSC))
+        refine_stage(P, 0, P->d0, P->d02, 1, 0.f, 1, 0);
+    else P->best = 0.f;
+    dprefine(P, 1, 1, 2);
+
+    /* stage 2, first call: MpStage2.h:63-83 with <false,true,DPSCAN> */
+    for (int call = 0; call < 2; call++) {
+        int gap0 = call == 1;
+        if (!(P->flags & CONV_LOWTMSC)) {
+            dp_run(P, P->tfm_gr, gap0, gap0 ? 0.0f : -1.0f, !gap0, gap0 ? P->d02 : d02dpscan);
+            if (!(P->flags & CONV_SCOREDP)) btck_matched(P);
+            else P->naln = 0;
+        } else P->naln = 0;
+        if (P->flags) P->best = 0.f;
+        else refine_stage(P, 1, P->d0, P->d02, 1, 0.f, 1, 0);
+        dprefine(P, 0, 0, 2);
+        dprefine(P, 1, 0, call == 0 ? 2 : o->convergence);
+        if (call == 1 && 0.0f < o->scorethld) {
+            int ml = P->lq < P->lr ? P->lq : P->lr;
+            if (P->grand < o->scorethld * (float)ml) P->flags |= CONV_LOWTMSC;
+        }
+    }
+
+    /* final stage: MpStageFin.h:63-96 */
+    if (P->flags & CONV_LOWTMSC) return;
+    dp_run(P, P->tfm_gr, 1, 0.f, 0, P->d02);
+    btck_matched(P);
+    refine_stage(P, 2, P->d0, P->d02, 1, -1.0f, 1, 1);
+    if (!(o->depth == 3 || o->refinement == 1))
+        final_phase2(P);
+    dp_run(P, P->tfm_gr, 1, 0.f, 0, P->d02);
+    btck_constrained(P);
+    if (alndst) production_alignment(P, alndst);
+    production(P);
+    if (o->referenced) {
+        float* t = P->tfm_gr;
+        float R[9];
+        memcpy(R, t, sizeof(R));
+        for (int i = 0; i < 3; i++)
+            for (int j = 0; j < 3; j++) t[3 * i + j] = R[3 * j + i];
+        float t0 = t[9], t1 = t[10], t2 = t[11];
+        t[9] = -(R[0] * t0 + R[3] * t1 + R[6] * t2);
+        t[10] = -(R[1] * t0 + R[4] * t1 + R[7] * t2);
+        t[11] = -(R[2] * t0 + R[5] * t1 + R[8] * t2);
+    }
+}
+
+int gto_process_block(const gto_opts* o,
+                      int nq, const int* qlen, const float* qx, const float* qy,
+                      const float* qz, const unsigned char* qrsd, const int* qmol,
+                      int nr, const int* rlen, const float* rx, const float* ry,
+                      const float* rz, const unsigned char* rrsd, const int* rmol,
+                      float* out, float* tfm, float* err,
+                      char* alns, const long long* aln_off,
+                      char* qss, char* rss, int nthreads) {
+    if (nq < 1 || nr < 1) return 1;
+    long long* qoff = (long long*)malloc(sizeof(long long) * (nq + 1));
+    long long* roff = (long long*)malloc(sizeof(long long) * (nr + 1));
+    qoff[0] = roff[0] = 0;
+    int qmax = 0, qmin = 1 << 30, rmax = 0, rmin = 1 << 30;
+    for (int i = 0; i < nq; i++) {
+        qoff[i + 1] = qoff[i] + qlen[i];
+        if (qlen[i] > qmax) qmax = qlen[i];
+        if (qlen[i] < qmin) qmin = qlen[i];
+    }
+    for (int i = 0; i < nr; i++) {
+        roff[i + 1] = roff[i] + rlen[i];
+        if (rlen[i] > rmax) rmax = rlen[i];
+        if (rlen[i] < rmin) rmin = rlen[i];
+    }
+    /* secondary structure (protein only) */
+    for (int i = 0; i < nq; i++) {
+        long long b = qoff[i];
+        if (!qmol || qmol[i] == 0) gto_secstr(qlen[i], qx + b, qy + b, qz + b, qss + b);
+        else memset(qss + b, ' ', qlen[i]);
+    }
+    for (int i = 0; i < nr; i++) {
+        long long b = roff[i];
+        if (!rmol || rmol[i] == 0) gto_secstr(rlen[i], rx + b, ry + b, rz + b, rss + b);
+        else memset(rss + b, ' ', rlen[i]);
+    }
+    long long npairs = (long long)nq * nr;
+    (void)nthreads;
+#pragma omp parallel for schedule(dynamic, 1) num_threads(nthreads > 0 ? nthreads : 1)
+    for (long long p = 0; p < npairs; p++) {
+        int qi = (int)(p / nr), ri = (int)(p % nr);
+        pairctx P;
+        memset(&P, 0, sizeof(P));
+        P.o = o;
+        P.lq = qlen[qi]; P.lr = rlen[ri];
+        P.qx = qx + qoff[qi]; P.qy = qy + qoff[qi]; P.qz = qz + qoff[qi];
+        P.rx = rx + roff[ri]; P.ry = ry + roff[ri]; P.rz = rz + roff[ri];
+        P.qa = qrsd + qoff[qi]; P.ra = rrsd + roff[ri];
+        P.qs = qss + qoff[qi]; P.rs = rss + roff[ri];
+        P.qmol = qmol ? qmol[qi] : 0; P.rmol = rmol ? rmol[ri] : 0;
+        P.qmax = qmax; P.qmin = qmin; P.rmax = rmax; P.rmin = rmin;
+        int mx = P.lq > P.lr ? P.lq : P.lr;
+        P.aq = (int*)malloc(sizeof(int) * (mx + 1));
+        P.ar = (int*)malloc(sizeof(int) * (mx + 1));
+        P.ad = (float*)malloc(sizeof(float) * (mx + 1));
+        P.bt = (unsigned char*)malloc((size_t)P.lq * P.lr);
+        P.h0 = (float*)malloc(sizeof(float) * P.lr);
+        P.h1 = (float*)malloc(sizeof(float) * P.lr);
+        run_pair(&P, alns ? alns + aln_off[p] : NULL);
+        memcpy(out + p * GTO_NOUT, P.out, sizeof(P.out));
+        memcpy(tfm + p * 12, P.tfm_gr, 12 * sizeof(float));
+        if (err) memcpy(err + p * GTO_NERR, P.err, sizeof(P.err));
+        free(P.aq); free(P.ar); free(P.ad); free(P.bt); free(P.h0); free(P.h1);
+    }
+    free(qoff);
+    free(roff);
+    return 0;
+}
