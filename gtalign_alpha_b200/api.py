@@ -1,0 +1,283 @@
+"""Host-side mirror of the reference's batch interface over the C ABI.
+
+``GTalignB200.process_block`` corresponds to the reference's
+``CuBatch::ProcessBlock`` (src/libmycu/cubatch/CuBatch.cuh:74-85): a block of
+query structures and a block of reference structures, packed structure-of-
+arrays exactly as ``PMBatchStrData`` packs them (field pointer arrays
+``pmbeg``/``pmend``, src/libgenp/gdats/PM2DVectorFields.h:220-239), go in;
+per-pair result records (gproc.h:148-168), 12-float transformation matrices
+and alignment rows come out.  Everything runs in the in-tree CUDA library
+``libgtb200.so``; there is no CPU fallback: a missing library is an error.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from dataclasses import dataclass, field
+from typing import List, Optional, Tuple
+
+import numpy as np
+
+from .synth import SoA
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+LIBPATH = os.path.join(PKG, "libgtb200.so")
+
+NOUT = 16
+NERR = 4
+NFIELDS = 10
+# result record fields (gproc.h:148-168)
+OUT_BEGCOORDS, OUT_ENDCOORDS, OUT_ALNLENGTH, OUT_PSTVS, OUT_IDNTS, OUT_NGAPS = 2, 3, 4, 5, 6, 7
+OUT_RMSD, OUT_SCOREQ, OUT_SCORER, OUT_D0Q, OUT_D0R = 8, 9, 10, 11, 12
+
+STATUS = {0: "GTB_OK", 1: "GTB_ERR_ARG", 2: "GTB_ERR_CUDA", 3: "GTB_ERR_NOMEM",
+          4: "GTB_ERR_UNSUPPORTED", 5: "GTB_ERR_TOO_LONG", 6: "GTB_ERR_NOT_BUILT"}
+
+
+class GTBError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        super().__init__("%s: %s" % (STATUS.get(status, str(status)), msg))
+        self.status = status
+
+
+class _COptions(ctypes.Structure):
+    _fields_ = [("refinement", ctypes.c_int), ("depth", ctypes.c_int),
+                ("convergence", ctypes.c_int), ("prescore", ctypes.c_float),
+                ("symmetric", ctypes.c_int), ("referenced", ctypes.c_int),
+                ("nodeletions", ctypes.c_int), ("nodetailedsearch", ctypes.c_int),
+                ("addsearchbyss", ctypes.c_int), ("twotmscore", ctypes.c_int)]
+
+
+class _CResults(ctypes.Structure):
+    _fields_ = [("alndata", ctypes.c_void_p), ("tfm", ctypes.c_void_p),
+                ("alns", ctypes.c_void_p), ("numerr", ctypes.c_void_p),
+                ("qss", ctypes.c_void_p), ("rss", ctypes.c_void_p)]
+
+
+@dataclass
+class Options:
+    """Per-pair computation options, with the gtalign command line's codes.
+
+    Defaults are the command line's defaults except ``nodetailedsearch``,
+    which must be 1 (the spatial-index search stage is not in this library).
+    """
+    refinement: int = 1
+    depth: int = 2
+    convergence: int = 18
+    prescore: float = 0.4
+    symmetric: int = 0
+    referenced: int = 0
+    nodeletions: int = 0
+    nodetailedsearch: int = 1
+    addsearchbyss: int = 0
+    twotmscore: int = 0
+
+    @classmethod
+    def speed(cls, level: int, **kw) -> "Options":
+        """The --speed presets that keep the detailed search off
+        (gtalign.cpp:833-867): 13 = --no-detailed-search --refinement=0
+        --convergence=2."""
+        if level != 13:
+            raise GTBError(4, "only --speed=13 runs without the detailed search")
+        o = cls(refinement=0, convergence=2, **kw)
+        return o
+
+    def _c(self) -> _COptions:
+        return _COptions(self.refinement, self.depth, self.convergence, self.prescore,
+                         self.symmetric, self.referenced, self.nodeletions,
+                         self.nodetailedsearch, self.addsearchbyss, self.twotmscore)
+
+
+_lib = None
+
+
+def load_library():
+    """Load the in-tree libgtb200.so; raises when it has not been built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIBPATH):
+        raise GTBError(6, "libgtb200.so not built (run gtalign_alpha_b200.build.build())")
+    L = ctypes.CDLL(LIBPATH)
+    vp, fp = ctypes.c_void_p, ctypes.POINTER(ctypes.c_float)
+    L.gtb_create.argtypes = [ctypes.c_int, ctypes.c_size_t, ctypes.POINTER(_COptions), ctypes.POINTER(vp)]
+    L.gtb_create.restype = ctypes.c_int
+    L.gtb_process_block.argtypes = [vp, ctypes.c_float, vp, vp, vp, vp, ctypes.POINTER(_CResults)]
+    L.gtb_process_block.restype = ctypes.c_int
+    L.gtb_alns_size.argtypes = [vp, vp, vp, vp]
+    L.gtb_alns_size.restype = ctypes.c_size_t
+    L.gtb_last_error.argtypes = [vp]
+    L.gtb_last_error.restype = ctypes.c_char_p
+    L.gtb_last_launch_count.argtypes = [vp]
+    L.gtb_last_launch_count.restype = ctypes.c_longlong
+    L.gtb_last_timings.argtypes = [vp, fp]
+    L.gtb_last_timings.restype = ctypes.c_int
+    L.gtb_destroy.argtypes = [vp]
+    L.gtb_destroy.restype = None
+    L.gtb_tm_adjoint.argtypes = [vp, ctypes.c_int, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp]
+    L.gtb_tm_adjoint.restype = ctypes.c_int
+    L.gtb_polish.argtypes = [vp, ctypes.c_int, vp, vp, vp, vp, vp, vp, ctypes.c_int, vp, vp, vp]
+    L.gtb_polish.restype = ctypes.c_int
+    _lib = L
+    return L
+
+
+@dataclass
+class PackedBlock:
+    """The 10 SoA field arrays of a block and their begin/end pointers."""
+    arrays: list
+    beg: ctypes.Array
+    end: ctypes.Array
+    n: int
+    npos: int
+
+
+def pack_fields(s: SoA) -> PackedBlock:
+    """Lay out a block the way PMBatchStrData does (one array per field)."""
+    n, N = s.n, s.total
+    insch = np.zeros(N, np.int32)
+    first = s.offs[s.mol > 0]
+    insch[first] = 1                      # sign of the first residue: > 0 = nucleic acid
+    arrays = [
+        np.ascontiguousarray(s.lens, np.int32),
+        np.ascontiguousarray(s.offs, np.uint32),
+        np.zeros(n, np.int32),
+        np.ascontiguousarray(s.x, np.float32),
+        np.ascontiguousarray(s.y, np.float32),
+        np.ascontiguousarray(s.z, np.float32),
+        insch,
+        np.arange(N, dtype=np.int32),
+        np.ascontiguousarray(s.rsd, np.uint8),
+        np.zeros(N, np.uint8),
+    ]
+    beg = (ctypes.c_void_p * NFIELDS)()
+    end = (ctypes.c_void_p * NFIELDS)()
+    for f, a in enumerate(arrays):
+        beg[f] = a.ctypes.data
+        end[f] = a.ctypes.data + a.nbytes
+    return PackedBlock(arrays, beg, end, n, N)
+
+
+@dataclass
+class BlockResult:
+    alndata: np.ndarray            # (nq, nr, 16)
+    tfm: np.ndarray                # (nq, nr, 12)
+    numerr: Optional[np.ndarray]   # (nq, nr, 4)
+    alns_raw: Optional[np.ndarray] # reference layout bytes
+    qlens: np.ndarray
+    rlens: np.ndarray
+    roffs: np.ndarray
+    qss: Optional[np.ndarray] = None
+    rss: Optional[np.ndarray] = None
+    launches: int = 0
+    timings_ms: np.ndarray = field(default_factory=lambda: np.zeros(7, np.float32))
+
+    @property
+    def tm_query(self) -> np.ndarray:
+        return self.alndata[..., OUT_SCOREQ]
+
+    @property
+    def tm_ref(self) -> np.ndarray:
+        return self.alndata[..., OUT_SCORER]
+
+    @property
+    def rmsd(self) -> np.ndarray:
+        return self.alndata[..., OUT_RMSD]
+
+    def alignment(self, qi: int, ri: int) -> Tuple[str, str, str, str, str]:
+        """(query row, middle row, target row, query SS, target SS)."""
+        if self.alns_raw is None:
+            raise ValueError("alignments were not requested")
+        nr = len(self.rlens)
+        Nr = int(self.rlens.sum())
+        base = 0
+        for k in range(qi):
+            base += 5 * (Nr + nr * (int(self.qlens[k]) + 1))
+        lq = int(self.qlens[qi])
+        rowlen = Nr + nr * (lq + 1)
+        col = int(self.roffs[ri]) + ri * (lq + 1)
+        W = lq + int(self.rlens[ri]) + 1
+        rows = []
+        for f in range(5):
+            seg = self.alns_raw[base + f * rowlen + col: base + f * rowlen + col + W].tobytes()
+            rows.append(seg.split(b"\0", 1)[0].decode("latin-1"))
+        return tuple(rows)
+
+
+class GTalignB200:
+    """One handle = one device area (the CuBatch analogue)."""
+
+    def __init__(self, device: int = 0, mem_bytes: int = 0, options: Optional[Options] = None):
+        self.lib = load_library()
+        self.options = options or Options()
+        self._h = ctypes.c_void_p()
+        copt = self.options._c()
+        st = self.lib.gtb_create(device, mem_bytes, ctypes.byref(copt), ctypes.byref(self._h))
+        if st != 0:
+            msg = self.lib.gtb_last_error(self._h).decode() if self._h else ""
+            if self._h:
+                self.lib.gtb_destroy(self._h)
+                self._h = ctypes.c_void_p()
+            raise GTBError(st, msg)
+
+    def close(self) -> None:
+        if self._h:
+            self.lib.gtb_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def handle(self):
+        return self._h
+
+    def process_block(self, queries: SoA, refs: SoA, scorethld: float = 0.5,
+                      alignments: bool = True, numerr: bool = True,
+                      secstr: bool = False) -> BlockResult:
+        qb, rb = pack_fields(queries), pack_fields(refs)
+        return self.process_packed(qb, rb, scorethld, alignments, numerr, secstr)
+
+    def process_packed(self, qb: PackedBlock, rb: PackedBlock, scorethld: float = 0.5,
+                       alignments: bool = True, numerr: bool = True,
+                       secstr: bool = False, out: Optional[dict] = None) -> BlockResult:
+        nq, nr = qb.n, rb.n
+        if out is None:
+            out = {}
+        aln = out.get("alndata")
+        if aln is None or aln.shape != (nq * nr, NOUT):
+            aln = np.zeros((nq * nr, NOUT), np.float32)
+        tfm = out.get("tfm")
+        if tfm is None or tfm.shape != (nq * nr, 12):
+            tfm = np.zeros((nq * nr, 12), np.float32)
+        err = np.zeros((nq * nr, NERR), np.float32) if numerr else None
+        alns = None
+        if alignments:
+            sz = self.lib.gtb_alns_size(qb.beg, qb.end, rb.beg, rb.end)
+            alns = np.zeros(sz, np.uint8)
+        qss = np.zeros(qb.npos, np.uint8) if secstr else None
+        rss = np.zeros(rb.npos, np.uint8) if secstr else None
+        res = _CResults(aln.ctypes.data, tfm.ctypes.data,
+                        alns.ctypes.data if alns is not None else None,
+                        err.ctypes.data if err is not None else None,
+                        qss.ctypes.data if qss is not None else None,
+                        rss.ctypes.data if rss is not None else None)
+        st = self.lib.gtb_process_block(self._h, float(scorethld), qb.beg, qb.end, rb.beg, rb.end,
+                                        ctypes.byref(res))
+        if st != 0:
+            raise GTBError(st, self.lib.gtb_last_error(self._h).decode())
+        tms = np.zeros(7, np.float32)
+        self.lib.gtb_last_timings(self._h, tms.ctypes.data_as(ctypes.POINTER(ctypes.c_float)))
+        return BlockResult(aln.reshape(nq, nr, NOUT), tfm.reshape(nq, nr, 12),
+                           err.reshape(nq, nr, NERR) if err is not None else None,
+                           alns, qb.arrays[0].copy(), rb.arrays[0].copy(), rb.arrays[1].copy(),
+                           qss, rss, int(self.lib.gtb_last_launch_count(self._h)), tms)

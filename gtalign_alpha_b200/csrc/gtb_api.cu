@@ -1,0 +1,484 @@
+// gtb_api.cu -- C ABI, device-memory plan and stage sequence of the search.
+//
+// The stage sequence is the reference's CuBatch::ProcessBlock with the
+// detailed (spatial-index) search off: stage 1 (CuBatch.cu:537-556 ->
+// custage1.cu:108-186), two stage-2 passes (CuBatch.cu:627-650 ->
+// custage2.cu:46-165), final stage (custage_fin.cu:45-128).  A block of
+// nq x nr pairs is processed in batches of consecutive pairs sized to the
+// device-memory budget; every kernel of a stage covers the whole batch.
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+#include <algorithm>
+#include <cuda_runtime.h>
+
+#include "gtb200.h"
+#include "gtb_kernels.cuh"
+
+using namespace gtb;
+
+struct gtb_handle {
+    int dev = 0;
+    size_t budget = 0;
+    gtb_options opts{};
+    cudaStream_t st = nullptr;
+    float *t_d0 = nullptr, *t_d82 = nullptr, *t_d0fin = nullptr;
+    char err[512] = {0};
+    long long launches = 0;
+    float timings[7] = {0};
+    cudaEvent_t ev[8] = {};
+};
+
+static const int TBL = 65536;
+
+#define CK(call)                                                                 \
+    do {                                                                         \
+        cudaError_t e_ = (call);                                                 \
+        if (e_ != cudaSuccess) {                                                 \
+            snprintf(h->err, sizeof(h->err), "%s: %s (%s:%d)", #call,            \
+                     cudaGetErrorString(e_), __FILE__, __LINE__);                \
+            return GTB_ERR_CUDA;                                                 \
+        }                                                                        \
+    } while (0)
+
+// Per-length constants; the FP32 formulas of stagecnsts.cuh:48-175.
+static void make_tables(std::vector<float>& d0, std::vector<float>& d82, std::vector<float>& d0fin) {
+    d0.resize(TBL); d82.resize(TBL); d0fin.resize(TBL);
+    for (int L = 0; L < TBL; L++) {
+        float l = (float)L;
+        float a = 0.168f;
+        if (l > 19.f) a = 1.24f * cbrtf(l - 15.f) - 1.8f;
+        d0[L] = a + 0.8f;
+        float d8 = 1.5f * powf(l, 0.3f) + 3.5f;
+        d82[L] = d8 * d8;
+        float f = 0.5f;
+        if (l > 21.f) f = 1.24f * cbrtf(l - 15.f) - 1.8f;
+        if (f < 0.5f) f = 0.5f;
+        d0fin[L] = f;
+    }
+}
+
+extern "C" gtb_status gtb_create(int device, size_t mem_bytes, const gtb_options* opts,
+                                 gtb_handle** out) {
+    if (!out || !opts) return GTB_ERR_ARG;
+    *out = nullptr;
+    gtb_handle* h = new gtb_handle();
+    h->dev = device;
+    h->opts = *opts;
+    cudaError_t e = cudaSetDevice(device);
+    if (e != cudaSuccess) {
+        snprintf(h->err, sizeof(h->err), "cudaSetDevice(%d): %s", device, cudaGetErrorString(e));
+        *out = h;
+        return GTB_ERR_CUDA;
+    }
+    size_t fr = 0, tot = 0;
+    CK(cudaMemGetInfo(&fr, &tot));
+    size_t avail = fr > ((size_t)256 << 20) ? fr - ((size_t)256 << 20) : fr / 2;
+    h->budget = (mem_bytes == 0 || mem_bytes > avail) ? avail : mem_bytes;
+    CK(cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking));
+    for (int k = 0; k < 8; k++) CK(cudaEventCreate(&h->ev[k]));
+    std::vector<float> a, b, c;
+    make_tables(a, b, c);
+    CK(cudaMalloc(&h->t_d0, TBL * sizeof(float)));
+    CK(cudaMalloc(&h->t_d82, TBL * sizeof(float)));
+    CK(cudaMalloc(&h->t_d0fin, TBL * sizeof(float)));
+    CK(cudaMemcpy(h->t_d0, a.data(), TBL * sizeof(float), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(h->t_d82, b.data(), TBL * sizeof(float), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(h->t_d0fin, c.data(), TBL * sizeof(float), cudaMemcpyHostToDevice));
+    *out = h;
+    return GTB_OK;
+}
+
+extern "C" void gtb_destroy(gtb_handle* h) {
+    if (!h) return;
+    cudaSetDevice(h->dev);
+    if (h->t_d0) cudaFree(h->t_d0);
+    if (h->t_d82) cudaFree(h->t_d82);
+    if (h->t_d0fin) cudaFree(h->t_d0fin);
+    for (int k = 0; k < 8; k++) if (h->ev[k]) cudaEventDestroy(h->ev[k]);
+    if (h->st) cudaStreamDestroy(h->st);
+    delete h;
+}
+
+extern "C" const char* gtb_last_error(const gtb_handle* h) { return h ? h->err : "null handle"; }
+extern "C" long long gtb_last_launch_count(const gtb_handle* h) { return h ? h->launches : -1; }
+extern "C" gtb_status gtb_last_timings(const gtb_handle* h, float* ms7) {
+    if (!h || !ms7) return GTB_ERR_ARG;
+    memcpy(ms7, h->timings, sizeof(h->timings));
+    return GTB_OK;
+}
+
+// ---------------------------------------------------------------------------
+static gtb_status check_options(gtb_handle* h) {
+    const gtb_options& o = h->opts;
+    if (!o.nodetailedsearch) {
+        snprintf(h->err, sizeof(h->err),
+                 "the spatial-index detailed search is not implemented: set nodetailedsearch=1");
+        return GTB_ERR_UNSUPPORTED;
+    }
+    if (o.addsearchbyss || o.twotmscore) {
+        snprintf(h->err, sizeof(h->err), "--add-search-by-ss and --2tm-score are not implemented");
+        return GTB_ERR_UNSUPPORTED;
+    }
+    if (o.refinement < 0 || o.refinement > 1) {
+        snprintf(h->err, sizeof(h->err), "--refinement %d not implemented (0 or 1)", o.refinement);
+        return GTB_ERR_UNSUPPORTED;
+    }
+    if (o.depth < 0 || o.depth > 3 || o.convergence < 1 || o.convergence > 30 ||
+        !(o.prescore >= 0.f && o.prescore < 1.f)) {
+        snprintf(h->err, sizeof(h->err), "option out of range");
+        return GTB_ERR_ARG;
+    }
+    return GTB_OK;
+}
+
+// Device-resident block description (inputs) for run_block.
+struct DevBlock {
+    int nq, nr;
+    const int *qlen, *rlen, *qoff, *roff, *qmol, *rmol;
+    const float *qx, *qy, *qz, *rx, *ry, *rz;
+    const unsigned char *qa, *ra;
+    char *qs, *rs;
+    std::vector<int> hqlen, hrlen;
+};
+
+// Results of one batch, device side.
+struct BatchBufs {
+    void* base = nullptr;
+    size_t cap = 0;
+};
+
+static size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+// Bytes of device scratch one pair needs.
+static size_t pair_bytes(int lq, int lr, bool strings) {
+    size_t nstrips = (size_t)(lq + 31) / 32;
+    size_t b = nstrips * (size_t)(lr + 31) * 8;       // traceback words
+    b += (size_t)lr * 4;                               // DP row buffer
+    b += (size_t)std::min(lq, lr) * 4;                 // aligned pairs
+    if (strings) b += (size_t)5 * (lq + lr + 1);       // alignment rows
+    b += 4 * 8 + 12 * 4 * 2 + 16 * 4 + 4 * 4 + 12 * 4 + 64;  // state + offsets
+    return b;
+}
+
+// Runs the whole stage sequence over a device-resident block.
+// Host outputs (may be null): alndata [nq*nr*16], tfm [nq*nr*12],
+// numerr [nq*nr*4]; strings: per pair compact rows copied to hstr (offsets
+// hstroff, 5*(lq+lr+1) bytes per pair) when non-null.
+static gtb_status run_block(gtb_handle* h, const DevBlock& D, float scorethld,
+                            float* h_alndata, float* h_tfm, float* h_err,
+                            char* hstr, const std::vector<long long>* hstroff) {
+    const gtb_options& o = h->opts;
+    cudaStream_t st = h->st;
+    const long long npairs = (long long)D.nq * D.nr;
+    Blk B{};
+    B.nq = D.nq; B.nr = D.nr;
+    B.qlen = D.qlen; B.rlen = D.rlen; B.qoff = D.qoff; B.roff = D.roff;
+    B.qx = D.qx; B.qy = D.qy; B.qz = D.qz; B.rx = D.rx; B.ry = D.ry; B.rz = D.rz;
+    B.qa = D.qa; B.ra = D.ra; B.qs = D.qs; B.rs = D.rs; B.qmol = D.qmol; B.rmol = D.rmol;
+    B.qmax = *std::max_element(D.hqlen.begin(), D.hqlen.end());
+    B.qmin = *std::min_element(D.hqlen.begin(), D.hqlen.end());
+    B.rmax = *std::max_element(D.hrlen.begin(), D.hrlen.end());
+    B.rmin = *std::min_element(D.hrlen.begin(), D.hrlen.end());
+    B.t_d0 = h->t_d0; B.t_d82 = h->t_d82; B.t_d0fin = h->t_d0fin;
+    B.stepinit = (o.depth == 3) ? 5 : 1;
+    B.refinement = o.refinement; B.depth = o.depth;
+    B.symmetric = o.symmetric; B.nodeletions = o.nodeletions;
+    const bool strings = hstr != nullptr;
+
+    size_t fr = 0, tot = 0;
+    CK(cudaMemGetInfo(&fr, &tot));
+    size_t budget = std::min(h->budget, fr > ((size_t)256 << 20) ? fr - ((size_t)256 << 20) : fr / 2);
+    // keep batches moderate so the pair-level state stays L2-friendly
+    const long long maxbatch = 1 << 20;
+
+    std::vector<long long> off_bt, off_row, off_aln, off_str;
+    float tsum[7] = {0, 0, 0, 0, 0, 0, 0};
+    h->launches = 0;
+
+    long long p0 = 0;
+    while (p0 < npairs) {
+        // choose the batch
+        size_t used = 0;
+        long long p1 = p0;
+        while (p1 < npairs && p1 - p0 < maxbatch) {
+            int lq = D.hqlen[p1 / D.nr], lr = D.hrlen[p1 % D.nr];
+            size_t b = pair_bytes(lq, lr, strings);
+            if (used + b > budget && p1 > p0) break;
+            used += b;
+            p1++;
+        }
+        if (used > budget) {
+            snprintf(h->err, sizeof(h->err), "pair (%lld) needs %zu bytes > budget %zu", p0, used, budget);
+            return GTB_ERR_NOMEM;
+        }
+        int np = (int)(p1 - p0);
+        off_bt.assign(np + 1, 0); off_row.assign(np + 1, 0);
+        off_aln.assign(np + 1, 0); off_str.assign(np + 1, 0);
+        for (int i = 0; i < np; i++) {
+            long long p = p0 + i;
+            int lq = D.hqlen[p / D.nr], lr = D.hrlen[p % D.nr];
+            off_bt[i + 1] = off_bt[i] + (long long)((lq + 31) / 32) * (lr + 31);
+            off_row[i + 1] = off_row[i] + lr;
+            off_aln[i + 1] = off_aln[i] + std::min(lq, lr);
+            off_str[i + 1] = off_str[i] + (strings ? 5LL * (lq + lr + 1) : 0);
+        }
+        // one allocation, carved
+        size_t sz = 0;
+        auto carve = [&](size_t bytes) { size_t o2 = sz; sz += align256(bytes); return o2; };
+        size_t o_ints = carve((size_t)np * 8 * sizeof(int));
+        size_t o_flts = carve((size_t)np * 4 * sizeof(float));
+        size_t o_tib = carve((size_t)np * 12 * sizeof(float));
+        size_t o_tgr = carve((size_t)np * 12 * sizeof(float));
+        size_t o_out = carve((size_t)np * 16 * sizeof(float));
+        size_t o_err = carve((size_t)np * 4 * sizeof(float));
+        size_t o_offs = carve((size_t)(np + 1) * 4 * sizeof(long long));
+        size_t o_bt = carve((size_t)off_bt[np] * sizeof(uint2));
+        size_t o_row = carve((size_t)off_row[np] * sizeof(float));
+        size_t o_aln = carve((size_t)off_aln[np] * sizeof(unsigned));
+        size_t o_str = carve((size_t)std::max<long long>(off_str[np], 1));
+        char* base = nullptr;
+        CK(cudaMallocAsync((void**)&base, sz, st));
+        Bat T{};
+        T.p0 = p0; T.np = np;
+        int* ints = (int*)(base + o_ints);
+        T.flags = ints; T.seedq = ints + np; T.seedr = ints + 2 * np; T.naln = ints + 3 * np;
+        T.sfndx = ints + 4 * np; T.sfpos = ints + 5 * np; T.sfndx_cur = ints + 6 * np; T.sfpos_cur = ints + 7 * np;
+        float* fl = (float*)(base + o_flts);
+        T.grand = fl; T.best = fl + np; T.best0 = fl + 2 * np; T.rmsd32 = fl + 3 * np;
+        T.tfm_ib = (float*)(base + o_tib); T.tfm_gr = (float*)(base + o_tgr);
+        T.out = (float*)(base + o_out); T.err = (float*)(base + o_err);
+        long long* offs = (long long*)(base + o_offs);
+        T.off_bt = offs; T.off_row = offs + (np + 1); T.off_aln = offs + 2 * (np + 1); T.off_str = offs + 3 * (np + 1);
+        T.bt = (uint2*)(base + o_bt); T.row = (float*)(base + o_row);
+        T.aln = (unsigned*)(base + o_aln); T.str = strings ? (base + o_str) : nullptr;
+        T.launches = &h->launches;
+        CK(cudaMemcpyAsync(offs, off_bt.data(), (np + 1) * sizeof(long long), cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(offs + (np + 1), off_row.data(), (np + 1) * sizeof(long long), cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(offs + 2 * (np + 1), off_aln.data(), (np + 1) * sizeof(long long), cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(offs + 3 * (np + 1), off_str.data(), (np + 1) * sizeof(long long), cudaMemcpyHostToDevice, st));
+
+        // ------------------------------------------------------------ stages
+        auto dprefine = [&](int gap0, int prescreen, int maxit) {
+            for (int dpi = 0; dpi < maxit; dpi++) {
+                launch_dp(B, T, DP_TFM_IBEST, gap0, gap0 ? 0.0f : -0.6f, 0, 0, 0, st);
+                launch_btck(B, T, 0, st);
+                launch_refine(RM_DP, B, T, st);
+                launch_post(B, T, dpi, maxit, prescreen, o.prescore, st);
+            }
+        };
+        CK(cudaEventRecord(h->ev[0], st));
+        launch_init(B, T, st);
+        launch_findfrag(B, T, st);
+        CK(cudaEventRecord(h->ev[1], st));
+        launch_refine(RM_INIT, B, T, st);
+        CK(cudaEventRecord(h->ev[2], st));
+        dprefine(1, 1, 2);
+        for (int call = 0; call < 2; call++) {
+            int gap0 = call == 1;
+            launch_dp(B, T, DP_TFM_GRAND, gap0, gap0 ? 0.0f : -1.0f, !gap0, !gap0, 1, st);
+            launch_btck(B, T, 0, st);
+            launch_refine(RM_DP, B, T, st);
+            dprefine(0, 0, 2);
+            dprefine(1, 0, call == 0 ? 2 : o.convergence);
+            if (call == 1 && 0.0f < scorethld) launch_lowscore(B, T, scorethld, st);
+        }
+        CK(cudaEventRecord(h->ev[3], st));
+        launch_dp(B, T, DP_TFM_GRAND, 1, 0.0f, 0, 0, 1, st);
+        launch_btck(B, T, 0, st);
+        launch_refine(RM_FIN1, B, T, st);
+        if (!(o.depth == 3 || o.refinement == 0)) launch_refine(RM_FIN2, B, T, st);
+        launch_dp(B, T, DP_TFM_GRAND, 1, 0.0f, 0, 0, 1, st);
+        launch_btck(B, T, 1, st);
+        launch_alnstr(B, T, st);
+        launch_refine(RM_PROD1, B, T, st);
+        launch_refine(RM_PROD2, B, T, st);
+        launch_final(B, T, o.referenced, st);
+        CK(cudaEventRecord(h->ev[4], st));
+        CK(cudaGetLastError());
+
+        // ------------------------------------------------------------ results
+        if (h_alndata)
+            CK(cudaMemcpyAsync(h_alndata + p0 * 16, T.out, (size_t)np * 16 * sizeof(float), cudaMemcpyDeviceToHost, st));
+        if (h_tfm)
+            CK(cudaMemcpyAsync(h_tfm + p0 * 12, T.tfm_gr, (size_t)np * 12 * sizeof(float), cudaMemcpyDeviceToHost, st));
+        if (h_err)
+            CK(cudaMemcpyAsync(h_err + p0 * 4, T.err, (size_t)np * 4 * sizeof(float), cudaMemcpyDeviceToHost, st));
+        if (strings)
+            CK(cudaMemcpyAsync(hstr + (*hstroff)[p0], T.str, (size_t)off_str[np], cudaMemcpyDeviceToHost, st));
+        CK(cudaFreeAsync(base, st));
+        CK(cudaStreamSynchronize(st));
+        float ms = 0.f;
+        CK(cudaEventElapsedTime(&ms, h->ev[0], h->ev[1])); tsum[0] += ms;
+        CK(cudaEventElapsedTime(&ms, h->ev[1], h->ev[2])); tsum[1] += ms;
+        CK(cudaEventElapsedTime(&ms, h->ev[2], h->ev[3])); tsum[2] += ms;
+        CK(cudaEventElapsedTime(&ms, h->ev[3], h->ev[4])); tsum[5] += ms;
+        CK(cudaEventElapsedTime(&ms, h->ev[0], h->ev[4])); tsum[6] += ms;
+        p0 = p1;
+    }
+    memcpy(h->timings, tsum, sizeof(tsum));
+    return GTB_OK;
+}
+
+// ---------------------------------------------------------------------------
+// The reference's SoA batch, read from host field pointers.
+struct HostSoA {
+    int n = 0;
+    long long npos = 0;
+    const int* len = nullptr;
+    const unsigned* dist = nullptr;
+    const float *x = nullptr, *y = nullptr, *z = nullptr;
+    const int* insch = nullptr;
+    const char* rsd = nullptr;
+    std::vector<int> mol, off;
+};
+
+static gtb_status parse_soa(gtb_handle* h, char* const* beg, char* const* end, HostSoA& S,
+                            const char* what) {
+    if (!beg || !end) { snprintf(h->err, sizeof(h->err), "%s: null field pointers", what); return GTB_ERR_ARG; }
+    for (int f = 0; f < GTB_NFIELDS; f++)
+        if ((f == GTB_FLD_LEN || f == GTB_FLD_DIST || f == GTB_FLD_X || f == GTB_FLD_Y ||
+             f == GTB_FLD_Z || f == GTB_FLD_INSCHORD || f == GTB_FLD_RSD) && !beg[f]) {
+            snprintf(h->err, sizeof(h->err), "%s: field %d is null", what, f);
+            return GTB_ERR_ARG;
+        }
+    S.n = (int)((end[GTB_FLD_LEN] - beg[GTB_FLD_LEN]) / (long)sizeof(int));
+    S.npos = (long long)(end[GTB_FLD_RSD] - beg[GTB_FLD_RSD]);
+    if (S.n < 1 || S.npos < 1) { snprintf(h->err, sizeof(h->err), "%s: empty block", what); return GTB_ERR_ARG; }
+    S.len = (const int*)beg[GTB_FLD_LEN];
+    S.dist = (const unsigned*)beg[GTB_FLD_DIST];
+    S.x = (const float*)beg[GTB_FLD_X]; S.y = (const float*)beg[GTB_FLD_Y]; S.z = (const float*)beg[GTB_FLD_Z];
+    S.insch = (const int*)beg[GTB_FLD_INSCHORD];
+    S.rsd = beg[GTB_FLD_RSD];
+    S.mol.resize(S.n); S.off.resize(S.n);
+    for (int i = 0; i < S.n; i++) {
+        int L = S.len[i];
+        long long d = S.dist[i];
+        if (L < 1 || d < 0 || d + L > S.npos) {
+            snprintf(h->err, sizeof(h->err), "%s: structure %d has invalid length/offset", what, i);
+            return GTB_ERR_ARG;
+        }
+        if (L > 65535) {
+            snprintf(h->err, sizeof(h->err), "%s: structure %d longer than 65535", what, i);
+            return GTB_ERR_TOO_LONG;
+        }
+        S.off[i] = (int)d;
+        S.mol[i] = (S.insch[d] > 0) ? 1 : 0;   // GetMoleculeType, PM2DVectorFields.h:98-102
+    }
+    return GTB_OK;
+}
+
+extern "C" size_t gtb_alns_size(char* const* qb, char* const* qe, char* const* rb, char* const* re) {
+    if (!qb || !qe || !rb || !re) return 0;
+    long long nq = (qe[GTB_FLD_LEN] - qb[GTB_FLD_LEN]) / (long)sizeof(int);
+    long long nr = (re[GTB_FLD_LEN] - rb[GTB_FLD_LEN]) / (long)sizeof(int);
+    long long Nr = re[GTB_FLD_RSD] - rb[GTB_FLD_RSD];
+    const int* ql = (const int*)qb[GTB_FLD_LEN];
+    size_t s = 0;
+    for (long long i = 0; i < nq; i++) s += (size_t)5 * (Nr + nr * ((long long)ql[i] + 1));
+    return s;
+}
+
+extern "C" gtb_status gtb_process_block(gtb_handle* h, float scorethld,
+                                        char* const* querypmbeg, char* const* querypmend,
+                                        char* const* bdbCpmbeg, char* const* bdbCpmend,
+                                        gtb_results* out) {
+    if (!h) return GTB_ERR_ARG;
+    h->err[0] = 0;
+    if (!out || !out->alndata || !out->tfm) { snprintf(h->err, sizeof(h->err), "null result buffers"); return GTB_ERR_ARG; }
+    if (!(scorethld >= 0.f && scorethld < 1.f)) { snprintf(h->err, sizeof(h->err), "scorethld out of [0,1)"); return GTB_ERR_ARG; }
+    gtb_status s = check_options(h);
+    if (s != GTB_OK) return s;
+    HostSoA Q, R;
+    if ((s = parse_soa(h, querypmbeg, querypmend, Q, "queries")) != GTB_OK) return s;
+    if ((s = parse_soa(h, bdbCpmbeg, bdbCpmend, R, "references")) != GTB_OK) return s;
+    CK(cudaSetDevice(h->dev));
+    cudaStream_t st = h->st;
+
+    // upload (SoA, one allocation)
+    size_t sz = 0;
+    auto carve = [&](size_t bytes) { size_t o2 = sz; sz += align256(bytes); return o2; };
+    size_t oql = carve(Q.n * 4), oqo = carve(Q.n * 4), oqm = carve(Q.n * 4);
+    size_t orl = carve(R.n * 4), oro = carve(R.n * 4), orm = carve(R.n * 4);
+    size_t oqx = carve(Q.npos * 4), oqy = carve(Q.npos * 4), oqz = carve(Q.npos * 4);
+    size_t orx = carve(R.npos * 4), ory = carve(R.npos * 4), orz = carve(R.npos * 4);
+    size_t oqa = carve(Q.npos), ora = carve(R.npos), oqs = carve(Q.npos), ors = carve(R.npos);
+    char* dbase = nullptr;
+    CK(cudaMallocAsync((void**)&dbase, sz, st));
+    CK(cudaMemcpyAsync(dbase + oql, Q.len, Q.n * 4, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(dbase + oqo, Q.off.data(), Q.n * 4, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(dbase + oqm, Q.mol.data(), Q.n * 4, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(dbase + orl, R.len, R.n * 4, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(dbase + oro, R.off.data(), R.n * 4, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(dbase + orm, R.mol.data(), R.n * 4, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(dbase + oqx, Q.x, Q.npos * 4, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(dbase + oqy, Q.y, Q.npos * 4, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(dbase + oqz, Q.z, Q.npos * 4, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(dbase + orx, R.x, R.npos * 4, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(dbase + ory, R.y, R.npos * 4, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(dbase + orz, R.z, R.npos * 4, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(dbase + oqa, Q.rsd, Q.npos, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(dbase + ora, R.rsd, R.npos, cudaMemcpyHostToDevice, st));
+
+    DevBlock D;
+    D.nq = Q.n; D.nr = R.n;
+    D.qlen = (int*)(dbase + oql); D.qoff = (int*)(dbase + oqo); D.qmol = (int*)(dbase + oqm);
+    D.rlen = (int*)(dbase + orl); D.roff = (int*)(dbase + oro); D.rmol = (int*)(dbase + orm);
+    D.qx = (float*)(dbase + oqx); D.qy = (float*)(dbase + oqy); D.qz = (float*)(dbase + oqz);
+    D.rx = (float*)(dbase + orx); D.ry = (float*)(dbase + ory); D.rz = (float*)(dbase + orz);
+    D.qa = (unsigned char*)(dbase + oqa); D.ra = (unsigned char*)(dbase + ora);
+    D.qs = dbase + oqs; D.rs = dbase + ors;
+    D.hqlen.assign(Q.len, Q.len + Q.n);
+    D.hrlen.assign(R.len, R.len + R.n);
+    long long ss_launch = 0;
+    launch_secstr(D.qs, D.qx, D.qy, D.qz, D.qlen, D.qoff, D.qmol, Q.n, st, &ss_launch);
+    launch_secstr(D.rs, D.rx, D.ry, D.rz, D.rlen, D.roff, D.rmol, R.n, st, &ss_launch);
+    CK(cudaGetLastError());
+
+    // compact per-pair alignment rows, scattered to the reference layout after
+    std::vector<long long> stroff;
+    std::vector<char> hstr;
+    if (out->alns) {
+        long long np = (long long)Q.n * R.n;
+        stroff.resize(np + 1);
+        stroff[0] = 0;
+        for (long long p = 0; p < np; p++)
+            stroff[p + 1] = stroff[p] + 5LL * (Q.len[p / R.n] + R.len[p % R.n] + 1);
+        hstr.assign((size_t)stroff[np], 0);
+    }
+    s = run_block(h, D, scorethld, out->alndata, out->tfm, out->numerr,
+                  out->alns ? hstr.data() : nullptr, out->alns ? &stroff : nullptr);
+    h->launches += ss_launch;
+    if (s != GTB_OK) { cudaFreeAsync(dbase, st); cudaStreamSynchronize(st); return s; }
+    if (out->qss) CK(cudaMemcpyAsync(out->qss, D.qs, Q.npos, cudaMemcpyDeviceToHost, st));
+    if (out->rss) CK(cudaMemcpyAsync(out->rss, D.rs, R.npos, cudaMemcpyDeviceToHost, st));
+    CK(cudaFreeAsync(dbase, st));
+    CK(cudaStreamSynchronize(st));
+
+    if (out->alns) {
+        // reference layout (MpDPHub.cpp:1975-1981)
+        long long Nr = R.npos;
+        long long base = 0;
+        for (int qi = 0; qi < Q.n; qi++) {
+            int lq = Q.len[qi];
+            long long rowlen = Nr + (long long)R.n * (lq + 1);
+            char* blk = out->alns + base;
+            for (int f = 0; f < 5; f++) memset(blk + f * rowlen, 0, (size_t)rowlen);
+            for (int ri = 0; ri < R.n; ri++) {
+                long long p = (long long)qi * R.n + ri;
+                int W = lq + R.len[ri] + 1;
+                const char* src = hstr.data() + stroff[p];
+                long long col = (long long)R.off[ri] + (long long)ri * (lq + 1);
+                for (int f = 0; f < 5; f++) {
+                    int n = 0;
+                    while (n < W && src[f * W + n]) n++;
+                    memcpy(blk + f * rowlen + col, src + f * W, (size_t)n);
+                }
+            }
+            base += 5 * rowlen;
+        }
+    }
+    return GTB_OK;
+}

@@ -1,0 +1,877 @@
+// gtb_kernels.cu -- sm_100a kernels of the per-pair superposition search.
+//
+// Work decomposition (one launch covers every pair of a batch):
+//  * seed (stage 1, fragment search): one CTA per pair, one thread per
+//    diagonal offset; each thread runs the whole covariance -> rotation ->
+//    score -> threshold loop of its offset sequentially and keeps its best;
+//    the CTA reduces (max score, lowest offset index).
+//  * refinement (every fragment-based superposition refinement): one CTA
+//    per pair, one thread per (fragment position, fragment length) variant,
+//    same reduction.  The distance-threshold covariance pass of iteration
+//    k+1 is fused into the scoring pass of iteration k.
+//  * DP: one warp per pair; the warp sweeps 32-row strips along
+//    anti-diagonals (lane = row), left/up/diagonal values move between lanes
+//    by shuffles, directions are packed 2 bits per cell with two ballots.
+//  * traceback, alignment rows, bookkeeping: one thread per pair.
+// All floating-point reductions are sequential per thread in forward position
+// order (blocks of BLK positions, Neumaier-compensated), so results do not
+// depend on the launch geometry.
+#include "gtb_device.cuh"
+#include "gtb_kernels.cuh"
+
+namespace gtb {
+
+#define GTB_LAUNCHED(T) do { if ((T).launches) (*(T).launches)++; } while (0)
+
+__device__ __forceinline__ int pair_qi(const Blk& B, const Bat& T, int i) {
+    return (int)((T.p0 + i) / B.nr);
+}
+__device__ __forceinline__ int pair_ri(const Blk& B, const Bat& T, int i) {
+    return (int)((T.p0 + i) % B.nr);
+}
+
+// ---------------------------------------------------------------------------
+// secondary structure: MpSecStr.cpp:26-118 / MpSecStr.h:218-249
+__device__ __forceinline__ float ss_dst(const float* x, const float* y, const float* z, int i, int j) {
+    float dx = __fsub_rn(x[i], x[j]), dy = __fsub_rn(y[i], y[j]), dz = __fsub_rn(z[i], z[j]);
+    float a = __fmul_rn(dx, dx), b = __fmul_rn(dy, dy), c = __fmul_rn(dz, dz);
+    return __fsqrt_rn(__fadd_rn(__fadd_rn(a, b), c));
+}
+
+__global__ void k_secstr(char* ss, const float* X, const float* Y, const float* Z,
+                         const int* len, const int* off, const int* mol, int nstr) {
+    int si = blockIdx.x;
+    if (si >= nstr) return;
+    int L = len[si];
+    const float* x = X + off[si];
+    const float* y = Y + off[si];
+    const float* z = Z + off[si];
+    char* s = ss + off[si];
+    int prot = mol ? (mol[si] == 0) : 1;
+    for (int p = threadIdx.x; p < L; p += blockDim.x) {
+        char c = ' ';
+        if (prot && p >= 2 && p + 2 < L) {
+            float d13 = ss_dst(x, y, z, p - 2, p);
+            float d14 = ss_dst(x, y, z, p - 2, p + 1);
+            float d15 = ss_dst(x, y, z, p - 2, p + 2);
+            float d24 = ss_dst(x, y, z, p - 1, p + 1);
+            float d25 = ss_dst(x, y, z, p - 1, p + 2);
+            float d35 = ss_dst(x, y, z, p, p + 2);
+            float e = 2.1f;
+            if (fabsf(d15 - 6.37f) < e && fabsf(d14 - 5.18f) < e && fabsf(d25 - 5.18f) < e &&
+                fabsf(d13 - 5.45f) < e && fabsf(d24 - 5.45f) < e && fabsf(d35 - 5.45f) < e)
+                c = 'h';
+            else {
+                e = 1.42f;
+                if (fabsf(d15 - 13.0f) < e && fabsf(d14 - 10.4f) < e && fabsf(d25 - 10.4f) < e &&
+                    fabsf(d13 - 6.1f) < e && fabsf(d24 - 6.1f) < e && fabsf(d35 - 6.1f) < e)
+                    c = 'e';
+                else if (d15 < 8.0f)
+                    c = 't';
+            }
+        }
+        s[p] = c;
+    }
+}
+
+void launch_secstr(char* ss, const float* x, const float* y, const float* z,
+                   const int* len, const int* off, const int* mol, int nstr,
+                   cudaStream_t st, long long* launches) {
+    if (nstr <= 0) return;
+    k_secstr<<<nstr, 128, 0, st>>>(ss, x, y, z, len, off, mol, nstr);
+    if (launches) (*launches)++;
+}
+
+// ---------------------------------------------------------------------------
+// pair initialisation: MpStage1.cpp:28-167
+__global__ void k_init(Blk B, Bat T) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= T.np) return;
+    int qi = pair_qi(B, T, i), ri = pair_ri(B, T, i);
+    T.flags[i] = (B.qmol[qi] != B.rmol[ri]) ? CONV_LOWTMSC : 0;
+    T.grand[i] = 0.f; T.best[i] = 0.f; T.best0[i] = 0.f; T.rmsd32[i] = -1.f;
+    T.seedq[i] = 0; T.seedr[i] = 0; T.naln[i] = 0;
+    T.sfndx[i] = T.sfpos[i] = T.sfndx_cur[i] = T.sfpos_cur[i] = 0;
+#pragma unroll
+    for (int f = 0; f < 12; f++) {
+        float v = (f == 0 || f == 4 || f == 8) ? 1.f : 0.f;
+        T.tfm_ib[i * 12 + f] = v;
+        T.tfm_gr[i * 12 + f] = v;
+    }
+#pragma unroll
+    for (int f = 0; f < 16; f++) T.out[i * 16 + f] = (f == 8) ? 9999.9f : 0.f;
+#pragma unroll
+    for (int f = 0; f < 4; f++) T.err[i * 4 + f] = 0.f;
+}
+
+void launch_init(const Blk& B, const Bat& T, cudaStream_t st) {
+    k_init<<<(T.np + 127) / 128, 128, 0, st>>>(B, T);
+    GTB_LAUNCHED(T);
+}
+
+// ---------------------------------------------------------------------------
+// position spaces: a gapless diagonal from (q0, r0), or DP-aligned pairs
+// stored in traceback (reverse) order.
+struct PairGeom {
+    const float *qx, *qy, *qz, *rx, *ry, *rz;
+    const unsigned* aln;  // reverse order; null for the diagonal space
+    int q0, r0, n;
+    __device__ __forceinline__ void at(int k, float& a, float& b, float& c,
+                                       float& d, float& e, float& f) const {
+        int q, r;
+        if (aln) {
+            unsigned w = aln[n - 1 - k];
+            q = (int)(w >> 16);
+            r = (int)(w & 0xffffu);
+        } else {
+            q = q0 + k;
+            r = r0 + k;
+        }
+        a = __ldg(qx + q); b = __ldg(qy + q); c = __ldg(qz + q);
+        d = __ldg(rx + r); e = __ldg(ry + r); f = __ldg(rz + r);
+    }
+};
+
+__device__ void cov_range(const PairGeom& G, int k0, int k1, float* v) {
+    CovAcc a;
+    a.init();
+    int blk = 0;
+    for (int k = k0; k < k1; k++) {
+        float qx, qy, qz, rx, ry, rz;
+        G.at(k, qx, qy, qz, rx, ry, rz);
+        a.add(qx, qy, qz, rx, ry, rz);
+        if (++blk == BLK) { a.fold(); blk = 0; }
+    }
+    a.final(v);
+}
+
+__device__ void cov_ext(const PairGeom& G, const float* tfm, float thr, float* v) {
+    CovAcc a;
+    a.init();
+    int blk = 0;
+    for (int k = 0; k < G.n; k++) {
+        float qx, qy, qz, rx, ry, rz;
+        G.at(k, qx, qy, qz, rx, ry, rz);
+        float d = dist2_tf(tfm, qx, qy, qz, rx, ry, rz);
+        if (d <= thr) a.add(qx, qy, qz, rx, ry, rz);
+        if (++blk == BLK) { a.fold(); blk = 0; }
+    }
+    a.final(v);
+}
+
+// score pass; m3mode 0 none, 1 distinct three smallest, 2 multiset
+__device__ float score_pass(const PairGeom& G, const float* tfm, float d02, int chk, float d82,
+                            int m3mode, float& m3out) {
+    float ss = 0.f, sc = 0.f, sb = 0.f;
+    int blk = 0;
+    float m1 = LARGEDST, m2 = LARGEDST, m3 = LARGEDST;
+    for (int k = 0; k < G.n; k++) {
+        float qx, qy, qz, rx, ry, rz;
+        G.at(k, qx, qy, qz, rx, ry, rz);
+        float d = dist2_tf(tfm, qx, qy, qz, rx, ry, rz);
+        if (!chk || d <= d82) sb = __fadd_rn(sb, tmterm(d02, d));
+        if (m3mode == 2) {
+            if (d < m1) { m3 = m2; m2 = m1; m1 = d; }
+            else if (d < m2) { m3 = m2; m2 = d; }
+            else if (d < m3) m3 = d;
+        } else if (m3mode == 1) {
+            if (d < m1) { m3 = m2; m2 = m1; m1 = d; }
+            else if (d > m1 && d < m2) { m3 = m2; m2 = d; }
+            else if (d > m2 && d < m3) m3 = d;
+        }
+        if (++blk == BLK) { nfold(ss, sc, sb); blk = 0; }
+    }
+    nfold(ss, sc, sb);
+    m3out = m3;
+    return __fadd_rn(ss, sc);
+}
+
+// fused: score under tfm (chk) and the covariance of positions within thr
+__device__ float score_and_ext(const PairGeom& G, const float* tfm, float d02, int chk, float d82,
+                               float thr, float* v) {
+    float ss = 0.f, sc = 0.f, sb = 0.f;
+    CovAcc a;
+    a.init();
+    int blk = 0;
+    for (int k = 0; k < G.n; k++) {
+        float qx, qy, qz, rx, ry, rz;
+        G.at(k, qx, qy, qz, rx, ry, rz);
+        float d = dist2_tf(tfm, qx, qy, qz, rx, ry, rz);
+        if (!chk || d <= d82) sb = __fadd_rn(sb, tmterm(d02, d));
+        if (d <= thr) a.add(qx, qy, qz, rx, ry, rz);
+        if (++blk == BLK) { nfold(ss, sc, sb); a.fold(); blk = 0; }
+    }
+    nfold(ss, sc, sb);
+    a.final(v);
+    return __fadd_rn(ss, sc);
+}
+
+__device__ __forceinline__ int converged16(const float* a, const float* b) {
+    int cnt = 0;
+#pragma unroll
+    for (int f = 0; f < 16; f++) {
+        float x = a[f], y = b[f];
+        float m = fabsf(x) < fabsf(y) ? fabsf(x) : fabsf(y);
+        if (fabsf(__fsub_rn(x, y)) < __fmul_rn(m, RM_CONVEPS)) cnt++;
+    }
+    return cnt >= 16;
+}
+
+// ---------------------------------------------------------------------------
+// stage 1 seed: MpStage1.cpp:289-440
+__device__ float findfrag_variant(const PairGeom& G, float d02, float d0s, int swap) {
+    float v[16], tfm[12], m3, best = 0.f;
+    float d02s0 = __fmul_rn(d0s, d0s);
+    cov_range(G, 0, G.n, v);
+    for (int it = 0; it < 3; it++) {
+        solve_sums(v, swap, tfm);
+        int save = (it < 2);
+        float sc = score_pass(G, tfm, d02, 0, 0.f, save ? 1 : 0, m3);
+        if (best < sc) best = sc;
+        if (!save) break;
+        float d02s = __fadd_rn(d02s0, (it == 1 ? 1.0f : 0.0f));
+        float dst32;
+        if (LARGEDST_CMP < m3 || m3 < d02s || G.n <= 3) dst32 = d02s;
+        else dst32 = __fadd_rn(d02s, __fmul_rn(ceilf(__fmul_rn(__fsub_rn(m3, d02s), 2.0f)), 0.5f));
+        cov_ext(G, tfm, dst32, v);
+        if (v[15] < 1.0f) break;
+        if ((int)v[15] == G.n) break;
+    }
+    return best;
+}
+
+__global__ void __launch_bounds__(128) k_findfrag(Blk B, Bat T) {
+    int i = blockIdx.x;
+    if (i >= T.np) return;
+    int flags = T.flags[i];
+    if (flags & CONV_LOWTMSC) return;
+    int qi = pair_qi(B, T, i), ri = pair_ri(B, T, i);
+    int lq = B.qlen[qi], lr = B.rlen[ri];
+    int minlenmin = B.qmin < B.rmin ? B.qmin : B.rmin;
+    int minalnmin = (minlenmin >> 1) > 5 ? (minlenmin >> 1) : 5;
+    int n1 = minalnmin - B.rmax;
+    int n2 = B.qmax - minalnmin;
+    int step = B.stepinit;
+    int nsteps = (n2 - n1) / step + 1;
+    int ml = lq < lr ? lq : lr;
+    int prv = (ml >> 1) > 5 ? (ml >> 1) : 5;
+    // per-pair admissible offsets: prv - lr <= ab <= lq - prv
+    int lo = prv - lr - n1;
+    int silo = lo <= 0 ? 0 : (lo + step - 1) / step;
+    int hi = lq - prv - n1;
+    int sihi = hi < 0 ? -1 : hi / step;
+    if (sihi > nsteps - 1) sihi = nsteps - 1;
+    float d0 = B.t_d0[ml];
+    float d02 = __fmul_rn(d0, d0);
+    float d0s = d0s_of(d0);
+    int swap = B.symmetric && (lq < lr);
+    PairGeom G;
+    G.qx = B.qx + B.qoff[qi]; G.qy = B.qy + B.qoff[qi]; G.qz = B.qz + B.qoff[qi];
+    G.rx = B.rx + B.roff[ri]; G.ry = B.ry + B.roff[ri]; G.rz = B.rz + B.roff[ri];
+    G.aln = nullptr;
+    float lbest = 0.f;
+    int lsi = 0x7fffffff;
+    for (int si = silo + (int)threadIdx.x; si <= sihi; si += blockDim.x) {
+        int ab = n1 + si * step;
+        int qpos = ab > 0 ? ab : 0;
+        int rpos = -ab > 0 ? -ab : 0;
+        if (lq <= qpos || lr <= rpos) continue;
+        if (lq - qpos < prv || lr - rpos < prv) continue;
+        G.q0 = qpos; G.r0 = rpos;
+        G.n = (lq - qpos) < (lr - rpos) ? (lq - qpos) : (lr - rpos);
+        float b = findfrag_variant(G, d02, d0s, swap);
+        if (b > 0.f && lbest < b) { lbest = b; lsi = si; }
+    }
+    __shared__ float sb[128];
+    __shared__ int ssi[128];
+    sb[threadIdx.x] = lbest;
+    ssi[threadIdx.x] = lsi;
+    __syncthreads();
+    for (int s = blockDim.x >> 1; s > 0; s >>= 1) {
+        if ((int)threadIdx.x < s) {
+            float o = sb[threadIdx.x + s];
+            int os = ssi[threadIdx.x + s];
+            if (o > sb[threadIdx.x] || (o == sb[threadIdx.x] && os < ssi[threadIdx.x])) {
+                sb[threadIdx.x] = o;
+                ssi[threadIdx.x] = os;
+            }
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        float b = sb[0];
+        T.best[i] = b;
+        if (b > 0.f) {
+            int ab = n1 + ssi[0] * step;
+            T.seedq[i] = ab > 0 ? ab : 0;
+            T.seedr[i] = -ab > 0 ? -ab : 0;
+        } else {
+            T.seedq[i] = 0;
+            T.seedr[i] = 0;
+        }
+    }
+}
+
+void launch_findfrag(const Blk& B, const Bat& T, cudaStream_t st) {
+    k_findfrag<<<T.np, 128, 0, st>>>(B, T);
+    GTB_LAUNCHED(T);
+}
+
+// ---------------------------------------------------------------------------
+// the refinement loop: MpStage1.cpp:640-700 and its copies in
+// RefineFragDPKernel and MpStageFin.cpp (one thread = one variant)
+__device__ void refine_loop(const PairGeom& G, int kf, int fraglen, float d0, float d02,
+                            int chk, float d82, float best_init, int swap,
+                            float& bestout, float* tb) {
+    float v[16], last[16], tfm[12], m3;
+    float best = best_init;
+    float d0s = d0s_of(d0);
+    float d0sp = __fadd_rn(d0s, 1.0f);
+    float thr2 = __fmul_rn(d0sp, d0sp);
+    float dst32 = LARGEDST;
+    cov_range(G, kf, kf + fraglen, v);
+    // iteration 0
+    if (v[15] < 1.0f) { bestout = best; return; }
+#pragma unroll
+    for (int f = 0; f < 16; f++) last[f] = v[f];
+    solve_sums(v, swap, tfm);
+    {
+        float sc = score_pass(G, tfm, d02, chk, d82, 2, m3);
+        float d0sm = __fsub_rn(d0s, 1.0f);
+        float d02s = __fmul_rn(d0sm, d0sm);
+        if (LARGEDST_CMP < m3 || m3 < d02s || G.n <= 3) dst32 = d02s;
+        else {
+            float t = __fadd_rn(d0sm, __fmul_rn(ceilf(__fmul_rn(__fsub_rn(__fsqrt_rn(m3), d0sm), 2.0f)), 0.5f));
+            dst32 = __fmul_rn(t, t);
+        }
+        if (best < sc) {
+            best = sc;
+#pragma unroll
+            for (int f = 0; f < 12; f++) tb[f] = tfm[f];
+        }
+    }
+    // iteration 1: threshold from iteration 0's three smallest distances
+    cov_ext(G, tfm, dst32, v);
+    for (int cit = 1; cit < NMAXCONVIT + 2; cit++) {
+        if (converged16(v, last)) break;
+        if (v[15] < 1.0f) break;
+#pragma unroll
+        for (int f = 0; f < 16; f++) last[f] = v[f];
+        solve_sums(v, swap, tfm);
+        // scoring pass of this iteration fused with the covariance of the next
+        float sc = score_and_ext(G, tfm, d02, chk, d82, thr2, v);
+        if (best < sc) {
+            best = sc;
+#pragma unroll
+            for (int f = 0; f < 12; f++) tb[f] = tfm[f];
+        }
+    }
+    bestout = best;
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(64) k_refine(Blk B, Bat T) {
+    int i = blockIdx.x;
+    if (i >= T.np) return;
+    int flags = T.flags[i];
+    if (MODE == RM_INIT) {
+        if (flags & CONV_LOWTMSC) { if (threadIdx.x == 0) T.best[i] = 0.f; return; }
+    } else if (MODE == RM_DP) {
+        if (flags) { if (threadIdx.x == 0) T.best[i] = 0.f; return; }
+    } else {
+        if (flags & CONV_LOWTMSC) return;
+    }
+    int qi = pair_qi(B, T, i), ri = pair_ri(B, T, i);
+    int lq = B.qlen[qi], lr = B.rlen[ri];
+    int ml = lq < lr ? lq : lr;
+    int swap = B.symmetric && (lq < lr);
+    PairGeom G;
+    G.qx = B.qx + B.qoff[qi]; G.qy = B.qy + B.qoff[qi]; G.qz = B.qz + B.qoff[qi];
+    G.rx = B.rx + B.roff[ri]; G.ry = B.ry + B.roff[ri]; G.rz = B.rz + B.roff[ri];
+    if (MODE == RM_INIT) {
+        int sq = T.seedq[i], sr = T.seedr[i];
+        G.aln = nullptr;
+        G.q0 = sq; G.r0 = sr;
+        if (lq <= sq || lr <= sr) G.n = 0;
+        else G.n = (lq - sq) < (lr - sr) ? (lq - sq) : (lr - sr);
+    } else {
+        G.aln = T.aln + T.off_aln[i];
+        G.q0 = G.r0 = 0;
+        G.n = T.naln[i];
+    }
+    const bool prod = (MODE == RM_PROD1 || MODE == RM_PROD2);
+    const bool phase2 = (MODE == RM_FIN2 || MODE == RM_PROD2);
+    float d0 = prod ? B.t_d0fin[ml] : B.t_d0[ml];
+    float d02 = __fmul_rn(d0, d0);
+    float d82 = B.t_d82[ml];
+    int chk = prod ? 0 : 1;
+    float best_init = (MODE == RM_INIT || MODE == RM_DP) ? 0.f : -1.f;
+    int maxalnmax = B.qmax < B.rmax ? B.qmax : B.rmax;
+    int nvar, nf = 0;
+    if (phase2) {
+        nf = 2 * maxalnmax < FIN_MAXNPOS ? 2 * maxalnmax : FIN_MAXNPOS;
+        nvar = nf;
+    } else {
+        nvar = (int)ceilf((float)(maxalnmax + FRAG_STEP - MINFRAGLEN) / FRAG_STEP) * FRAG_NSUB;
+    }
+    int nrange = G.n;
+    int sfndx0 = phase2 ? T.sfndx[i] : 0, sfpos0 = phase2 ? T.sfpos[i] : 0;
+    float lbest = 0.f, lgbest = 0.f, tbest[12];
+    int lsi = 0x7fffffff, lndx = 0, lpos = 0;
+    for (int si = threadIdx.x; si < nvar && nrange > 0; si += blockDim.x) {
+        int sfragndx, sfragpos, fraglen, kf;
+        if (phase2) {
+            sfragndx = sfndx0 == 0 ? 1 : sfndx0;
+            sfragpos = sfpos0 + (si - (nf >> 1));
+            fraglen = frag_length(nrange, sfragndx);
+            if (fraglen < 1) continue;
+            if (sfragpos < 0 || nrange + 1 <= sfragpos + fraglen) continue;
+            kf = sfragpos;
+        } else {
+            int sfragfct = si / FRAG_NSUB;
+            sfragndx = si - sfragfct * FRAG_NSUB;
+            fraglen = frag_length(nrange, sfragndx);
+            if (fraglen < 1) continue;
+            sfragpos = sfragfct * FRAG_STEP;
+            if (nrange + FRAG_STEP <= sfragpos + fraglen) continue;
+            int delta = sfragpos + fraglen - nrange;
+            kf = sfragpos - (delta > 0 ? delta : 0);
+        }
+        if (MODE == RM_PROD1 && si == 0) {
+            // RMSD over the whole alignment from compensated FP32 sums
+            CovAcc a;
+            a.init();
+            float sq[6], cq[6], bq[6];
+#pragma unroll
+            for (int f = 0; f < 6; f++) { sq[f] = 0.f; cq[f] = 0.f; bq[f] = 0.f; }
+            int blk = 0;
+            for (int k = kf; k < kf + fraglen; k++) {
+                float qx, qy, qz, rx, ry, rz;
+                G.at(k, qx, qy, qz, rx, ry, rz);
+                a.add(qx, qy, qz, rx, ry, rz);
+                bq[0] = __fmaf_rn(qx, qx, bq[0]); bq[1] = __fmaf_rn(qy, qy, bq[1]); bq[2] = __fmaf_rn(qz, qz, bq[2]);
+                bq[3] = __fmaf_rn(rx, rx, bq[3]); bq[4] = __fmaf_rn(ry, ry, bq[4]); bq[5] = __fmaf_rn(rz, rz, bq[5]);
+                if (++blk == BLK) {
+                    a.fold();
+#pragma unroll
+                    for (int f = 0; f < 6; f++) nfold(sq[f], cq[f], bq[f]);
+                    blk = 0;
+                }
+            }
+            float vv[16];
+            a.final(vv);
+            double dv[21];
+#pragma unroll
+            for (int f = 0; f < 15; f++) dv[f] = (double)vv[f];
+#pragma unroll
+            for (int f = 0; f < 6; f++) { nfold(sq[f], cq[f], bq[f]); dv[15 + f] = (double)__fadd_rn(sq[f], cq[f]); }
+            T.rmsd32[i] = (float)rmsd_from_sums(dv, (double)fraglen);
+        }
+        float best, tb[12];
+        refine_loop(G, kf, fraglen, d0, d02, chk, d82, best_init, swap, best, tb);
+        float gbest = best;
+        if (prod && best >= 0.f && lq != lr) {
+            int gl = lq > lr ? lq : lr;
+            float g0 = B.t_d0fin[gl];
+            float m3;
+            gbest = score_pass(G, tb, __fmul_rn(g0, g0), 0, d82, 0, m3);
+        }
+        if (best > 0.f && lbest < best) {
+            lbest = best; lgbest = gbest; lsi = si; lndx = sfragndx; lpos = sfragpos;
+#pragma unroll
+            for (int f = 0; f < 12; f++) tbest[f] = tb[f];
+        }
+    }
+    __shared__ float sb[64];
+    __shared__ int ssi[64];
+    sb[threadIdx.x] = lbest;
+    ssi[threadIdx.x] = lsi;
+    __syncthreads();
+    for (int s = blockDim.x >> 1; s > 0; s >>= 1) {
+        if ((int)threadIdx.x < s) {
+            float o = sb[threadIdx.x + s];
+            int os = ssi[threadIdx.x + s];
+            if (o > sb[threadIdx.x] || (o == sb[threadIdx.x] && os < ssi[threadIdx.x])) {
+                sb[threadIdx.x] = o;
+                ssi[threadIdx.x] = os;
+            }
+        }
+        __syncthreads();
+    }
+    float wb = sb[0];
+    int wsi = ssi[0];
+    bool havewin = wb > 0.f;
+    bool iamwin = havewin && lsi == wsi && lbest == wb;
+    if (MODE == RM_PROD1 || MODE == RM_PROD2) {
+        if (iamwin) {
+            float grand = T.grand[i];
+            bool write = (MODE == RM_PROD1) || (grand < wb);
+            if (write) {
+                T.grand[i] = wb;
+                float bs = wb, gb = lgbest;
+                if ((float)lr < (float)lq) { float t = bs; bs = gb; gb = t; }
+                T.out[i * 16 + 9] = __fdiv_rn(bs, (float)lq);
+                T.out[i * 16 + 10] = __fdiv_rn(gb, (float)lr);
+                T.out[i * 16 + 11] = B.t_d0fin[lq];
+                T.out[i * 16 + 12] = B.t_d0fin[lr];
+#pragma unroll
+                for (int f = 0; f < 12; f++) T.tfm_gr[i * 12 + f] = tbest[f];
+                if (MODE == RM_PROD1) { T.sfndx[i] = lndx; T.sfpos[i] = lpos; }
+            }
+        }
+        return;
+    }
+    if (threadIdx.x == 0) T.best[i] = havewin ? wb : 0.f;
+    if (iamwin) {
+#pragma unroll
+        for (int f = 0; f < 12; f++) T.tfm_ib[i * 12 + f] = tbest[f];
+        if (T.grand[i] < wb) {
+            T.grand[i] = wb;
+#pragma unroll
+            for (int f = 0; f < 12; f++) T.tfm_gr[i * 12 + f] = tbest[f];
+        }
+        if (MODE == RM_FIN1) { T.sfndx_cur[i] = lndx; T.sfpos_cur[i] = lpos; }
+    }
+    if (MODE == RM_FIN1) {
+        __syncthreads();
+        if (threadIdx.x == 0) { T.sfndx[i] = T.sfndx_cur[i]; T.sfpos[i] = T.sfpos_cur[i]; }
+    }
+}
+
+void launch_refine(int mode, const Blk& B, const Bat& T, cudaStream_t st) {
+    switch (mode) {
+        case RM_INIT:  k_refine<RM_INIT><<<T.np, 64, 0, st>>>(B, T); break;
+        case RM_DP:    k_refine<RM_DP><<<T.np, 64, 0, st>>>(B, T); break;
+        case RM_FIN1:  k_refine<RM_FIN1><<<T.np, 64, 0, st>>>(B, T); break;
+        case RM_FIN2:  k_refine<RM_FIN2><<<T.np, 64, 0, st>>>(B, T); break;
+        case RM_PROD1: k_refine<RM_PROD1><<<T.np, 64, 0, st>>>(B, T); break;
+        case RM_PROD2: k_refine<RM_PROD2><<<T.np, 64, 0, st>>>(B, T); break;
+    }
+    GTB_LAUNCHED(T);
+}
+
+// ---------------------------------------------------------------------------
+// DP: MpDPHub.cpp:72-346 and 686-940.  One warp per pair.
+__global__ void __launch_bounds__(128) k_dp(Blk B, Bat T, int tfmsrc, int gap0, float gcost,
+                                            int usess, int dpscan, int skipmode) {
+    int lane = threadIdx.x & 31;
+    int i = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    if (i >= T.np) return;
+    int flags = T.flags[i];
+    int skipmask = skipmode == 0 ? (CONV_LOWTMSC | CONV_SCOREDP) : CONV_LOWTMSC;
+    if (flags & skipmask) return;
+    int qi = pair_qi(B, T, i), ri = pair_ri(B, T, i);
+    int lq = B.qlen[qi], lr = B.rlen[ri];
+    int ml = lq < lr ? lq : lr;
+    const float* tsrc = (tfmsrc == DP_TFM_GRAND ? T.tfm_gr : T.tfm_ib) + i * 12;
+    float t[12];
+#pragma unroll
+    for (int f = 0; f < 12; f++) t[f] = tsrc[f];
+    float d0 = B.t_d0[ml];
+    float d02;
+    if (dpscan) { float a = __fadd_rn(d0, 1.5f); d02 = __fmul_rn(a, a); }
+    else d02 = __fmul_rn(d0, d0);
+    const float* qx = B.qx + B.qoff[qi];
+    const float* qy = B.qy + B.qoff[qi];
+    const float* qz = B.qz + B.qoff[qi];
+    const float* rx = B.rx + B.roff[ri];
+    const float* ry = B.ry + B.roff[ri];
+    const float* rz = B.rz + B.roff[ri];
+    const char* qs = B.qs + B.qoff[qi];
+    const char* rs = B.rs + B.roff[ri];
+    float* row = T.row + T.off_row[i];
+    uint2* bt = T.bt + T.off_bt[i];
+    const int W = lr + 31;
+    const int nstrips = (lq + 31) >> 5;
+    const unsigned FULL = 0xffffffffu;
+    for (int s = 0; s < nstrips; s++) {
+        int irow = (s << 5) + lane;
+        bool vrow = irow < lq;
+        float tx = 0.f, ty = 0.f, tz = 0.f;
+        char qss = 0;
+        if (vrow) {
+            xform(t, __ldg(qx + irow), __ldg(qy + irow), __ldg(qz + irow), tx, ty, tz);
+            if (usess) qss = qs[irow];
+        }
+        float hleft = 0.f, uplast = 0.f, rb = 0.f;
+        __syncwarp();
+        for (int tt = 0; tt < W; tt++) {
+            int j = tt - lane;
+            if ((tt & 31) == 0) {
+                int jj = tt + lane;
+                rb = (s > 0 && jj < lr) ? row[jj] : 0.f;
+            }
+            float upv = __shfl_up_sync(FULL, hleft, 1);
+            float up0 = __shfl_sync(FULL, rb, tt & 31);
+            if (lane == 0) upv = (j < lr) ? up0 : 0.f;
+            int bk = 0;
+            if (vrow && j >= 0 && j < lr) {
+                float d = dist2(tx, ty, tz, __ldg(rx + j), __ldg(ry + j), __ldg(rz + j));
+                float v = tmterm(d02, d);
+                if (usess) v = __fadd_rn(v, __fmul_rn((float)(qss == rs[j]), 0.5f));
+                float dg = uplast;
+                v = __fadd_rn(v, gap0 ? dg : fabsf(dg));
+                bk = BT_DIAG;
+                float l = hleft;
+                if (!gap0 && l < 0.f) l = __fsub_rn(gcost, l);
+                if (v < l) { v = l; bk = BT_LEFT; }
+                float u = upv;
+                if (!gap0 && u < 0.f) u = __fsub_rn(gcost, u);
+                if (v < u) { v = u; bk = BT_UP; }
+                float w = (gap0 || bk != BT_DIAG) ? v : -v;
+                hleft = w;
+                if (lane == 31) row[j] = w;
+            }
+            uplast = upv;
+            unsigned b0 = __ballot_sync(FULL, bk & 1);
+            unsigned b1 = __ballot_sync(FULL, (bk >> 1) & 1);
+            if (lane == 0) bt[(long long)s * W + tt] = make_uint2(b0, b1);
+        }
+        __syncwarp();
+    }
+}
+
+void launch_dp(const Blk& B, const Bat& T, int tfmsrc, int gap0, float gcost, int usess,
+               int dpscan, int skipmode, cudaStream_t st) {
+    k_dp<<<(T.np + 3) / 4, 128, 0, st>>>(B, T, tfmsrc, gap0, gcost, usess, dpscan, skipmode);
+    GTB_LAUNCHED(T);
+}
+
+// ---------------------------------------------------------------------------
+// traceback: MpDPHub.cpp:1515-1660 (plain) and 1699-1905 (constrained)
+__global__ void k_btck(Blk B, Bat T, int constrained) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= T.np) return;
+    int flags = T.flags[i];
+    if (constrained) {
+        if (flags & CONV_LOWTMSC) return;
+    } else if (flags & (CONV_LOWTMSC | CONV_SCOREDP)) {
+        T.naln[i] = 0;
+        return;
+    }
+    int qi = pair_qi(B, T, i), ri = pair_ri(B, T, i);
+    int lq = B.qlen[qi], lr = B.rlen[ri];
+    int ml = lq < lr ? lq : lr;
+    const uint2* bt = T.bt + T.off_bt[i];
+    unsigned* aln = T.aln + T.off_aln[i];
+    const int W = lr + 31;
+    float t[12];
+    float d82 = B.t_d82[ml];
+    const float *qx = B.qx + B.qoff[qi], *qy = B.qy + B.qoff[qi], *qz = B.qz + B.qoff[qi];
+    const float *rx = B.rx + B.roff[ri], *ry = B.ry + B.roff[ri], *rz = B.rz + B.roff[ri];
+    if (constrained) {
+#pragma unroll
+        for (int f = 0; f < 12; f++) t[f] = T.tfm_gr[i * 12 + f];
+    }
+    int y = lq - 1, x = lr - 1, n = 0;
+    while (x >= 0 && y >= 0) {
+        int l = y & 31;
+        uint2 w = bt[(long long)(y >> 5) * W + x + l];
+        int b = (int)((w.x >> l) & 1u) | ((int)((w.y >> l) & 1u) << 1);
+        if (b == BT_UP) { y--; continue; }
+        if (b == BT_LEFT) { x--; continue; }
+        if (constrained) {
+            float d = dist2_tf(t, qx[y], qy[y], qz[y], rx[x], ry[x], rz[x]);
+            if (d <= d82) aln[n++] = ((unsigned)y << 16) | (unsigned)x;
+        } else
+            aln[n++] = ((unsigned)y << 16) | (unsigned)x;
+        x--; y--;
+    }
+    T.naln[i] = n;
+}
+
+void launch_btck(const Blk& B, const Bat& T, int constrained, cudaStream_t st) {
+    k_btck<<<(T.np + 127) / 128, 128, 0, st>>>(B, T, constrained);
+    GTB_LAUNCHED(T);
+}
+
+// ---------------------------------------------------------------------------
+// per-iteration bookkeeping of DPRefine: MpStage1.cpp:495-513 and
+// CheckScoreConvergence / SaveLastScore0 / SetLowScoreConvergenceFlag
+__global__ void k_post(Blk B, Bat T, int dpi, int maxit, int prescreen, float prescore) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= T.np) return;
+    int flags = T.flags[i];
+    float best = T.best[i];
+    if (0 < dpi && !(flags & (CONV_SCOREDP | CONV_LOWTMSC)) &&
+        fabsf(__fsub_rn(best, T.best0[i])) < SCORE_CONVEPS)
+        flags |= CONV_SCOREDP;
+    if (dpi + 1 < maxit && !(flags & (CONV_SCOREDP | CONV_LOWTMSC)))
+        T.best0[i] = best;
+    if (prescreen && maxit <= dpi + 1 && 0.0f < prescore) {
+        int qi = pair_qi(B, T, i), ri = pair_ri(B, T, i);
+        int lq = B.qlen[qi], lr = B.rlen[ri];
+        int ml = lq < lr ? lq : lr;
+        if (T.grand[i] < __fmul_rn(prescore, (float)ml)) flags |= CONV_LOWTMSC;
+    }
+    if (dpi == maxit - 1) flags &= ~CONV_SCOREDP;
+    T.flags[i] = flags;
+}
+
+void launch_post(const Blk& B, const Bat& T, int dpi, int maxit, int prescreen, float prescore,
+                 cudaStream_t st) {
+    k_post<<<(T.np + 255) / 256, 256, 0, st>>>(B, T, dpi, maxit, prescreen, prescore);
+    GTB_LAUNCHED(T);
+}
+
+__global__ void k_lowscore(Blk B, Bat T, float thr) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= T.np) return;
+    int qi = pair_qi(B, T, i), ri = pair_ri(B, T, i);
+    int lq = B.qlen[qi], lr = B.rlen[ri];
+    int ml = lq < lr ? lq : lr;
+    if (T.grand[i] < __fmul_rn(thr, (float)ml)) T.flags[i] |= CONV_LOWTMSC;
+}
+
+void launch_lowscore(const Blk& B, const Bat& T, float thr, cudaStream_t st) {
+    k_lowscore<<<(T.np + 255) / 256, 256, 0, st>>>(B, T, thr);
+    GTB_LAUNCHED(T);
+}
+
+// ---------------------------------------------------------------------------
+// alignment rows: MpDPHub.cpp:1919-2125
+__global__ void k_alnstr(Blk B, Bat T) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= T.np) return;
+    if (T.flags[i] & CONV_LOWTMSC) return;
+    int qi = pair_qi(B, T, i), ri = pair_ri(B, T, i);
+    int lq = B.qlen[qi], lr = B.rlen[ri];
+    const unsigned* aln = T.aln + T.off_aln[i];
+    int n = T.naln[i];
+    float t[12];
+#pragma unroll
+    for (int f = 0; f < 12; f++) t[f] = T.tfm_gr[i * 12 + f];
+    const float *qx = B.qx + B.qoff[qi], *qy = B.qy + B.qoff[qi], *qz = B.qz + B.qoff[qi];
+    const float *rx = B.rx + B.roff[ri], *ry = B.ry + B.roff[ri], *rz = B.rz + B.roff[ri];
+    const unsigned char* qa = B.qa + B.qoff[qi];
+    const unsigned char* ra = B.ra + B.roff[ri];
+    const char* qs = B.qs + B.qoff[qi];
+    const char* rs = B.rs + B.roff[ri];
+    int W = lq + lr + 1;
+    char* dst = T.str ? T.str + T.off_str[i] : nullptr;
+    int col = 0, psts = 0, idts = 0, gaps = 0;
+    unsigned bc = 0, ec = 0;
+    for (int k = 0; k < n; k++) {
+        unsigned wv = aln[n - 1 - k];
+        int q = (int)(wv >> 16), r = (int)(wv & 0xffffu);
+        float d = dist2_tf(t, qx[q], qy[q], qz[q], rx[r], ry[r], rz[r]);
+        unsigned cc = ((unsigned)(r + 1) << 16) | (unsigned)(q + 1);
+        if (k == 0) bc = cc;
+        ec = cc;
+        int eq = d < 25.0f;
+        if (eq) psts++;
+        char a = (char)qa[q], b = (char)ra[r];
+        char mc = eq ? '+' : ' ';
+        if (a != '-' && a == b) { idts++; mc = eq ? a : (char)(a | 32); }
+        if (dst) { dst[col] = a; dst[2 * W + col] = b; dst[3 * W + col] = qs[q]; dst[4 * W + col] = rs[r]; dst[W + col] = mc; }
+        col++;
+        if (k + 1 < n) {
+            unsigned w1 = aln[n - 2 - k];
+            int q1 = (int)(w1 >> 16), r1 = (int)(w1 & 0xffffu);
+            for (int qq = q + 1; qq < q1; qq++) {
+                if (dst) { dst[col] = (char)qa[qq]; dst[3 * W + col] = qs[qq]; dst[2 * W + col] = '-'; dst[4 * W + col] = ' '; dst[W + col] = ' '; }
+                col++; gaps++;
+            }
+            if (!B.nodeletions)
+                for (int rr = r + 1; rr < r1; rr++) {
+                    if (dst) { dst[2 * W + col] = (char)ra[rr]; dst[4 * W + col] = rs[rr]; dst[col] = '-'; dst[3 * W + col] = ' '; dst[W + col] = ' '; }
+                    col++; gaps++;
+                }
+        }
+    }
+    if (dst) { dst[col] = 0; dst[W + col] = 0; dst[2 * W + col] = 0; dst[3 * W + col] = 0; dst[4 * W + col] = 0; }
+    T.out[i * 16 + 2] = __uint_as_float(bc);
+    T.out[i * 16 + 3] = __uint_as_float(ec);
+    T.out[i * 16 + 4] = (float)col;
+    T.out[i * 16 + 5] = (float)psts;
+    T.out[i * 16 + 6] = (float)idts;
+    T.out[i * 16 + 7] = (float)gaps;
+}
+
+void launch_alnstr(const Blk& B, const Bat& T, cudaStream_t st) {
+    k_alnstr<<<(T.np + 127) / 128, 128, 0, st>>>(B, T);
+    GTB_LAUNCHED(T);
+}
+
+// ---------------------------------------------------------------------------
+// FP64 recomputation of the reported TM-scores and RMSD, --referenced
+__global__ void k_final(Blk B, Bat T, int referenced) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= T.np) return;
+    if (T.flags[i] & CONV_LOWTMSC) return;
+    int qi = pair_qi(B, T, i), ri = pair_ri(B, T, i);
+    int lq = B.qlen[qi], lr = B.rlen[ri];
+    const unsigned* aln = T.aln + T.off_aln[i];
+    int n = T.naln[i];
+    float* t = T.tfm_gr + i * 12;
+    float* out = T.out + i * 16;
+    if (n > 0) {
+        const float *qx = B.qx + B.qoff[qi], *qy = B.qy + B.qoff[qi], *qz = B.qz + B.qoff[qi];
+        const float *rx = B.rx + B.roff[ri], *ry = B.ry + B.roff[ri], *rz = B.rz + B.roff[ri];
+        double d0q = (double)B.t_d0fin[lq], d0r = (double)B.t_d0fin[lr];
+        double d0q2 = __dmul_rn(d0q, d0q), d0r2 = __dmul_rn(d0r, d0r), tq = 0.0, tr = 0.0;
+        double dv[21];
+#pragma unroll
+        for (int f = 0; f < 21; f++) dv[f] = 0.0;
+        double td[12];
+#pragma unroll
+        for (int f = 0; f < 12; f++) td[f] = (double)t[f];
+        for (int k = 0; k < n; k++) {
+            unsigned wv = aln[n - 1 - k];
+            int q = (int)(wv >> 16), r = (int)(wv & 0xffffu);
+            double qq[3] = {(double)qx[q], (double)qy[q], (double)qz[q]};
+            double rr[3] = {(double)rx[r], (double)ry[r], (double)rz[r]};
+            double x = __dadd_rn(__dadd_rn(__dadd_rn(__dmul_rn(td[0], qq[0]), __dmul_rn(td[1], qq[1])), __dmul_rn(td[2], qq[2])), td[9]);
+            double y = __dadd_rn(__dadd_rn(__dadd_rn(__dmul_rn(td[3], qq[0]), __dmul_rn(td[4], qq[1])), __dmul_rn(td[5], qq[2])), td[10]);
+            double z = __dadd_rn(__dadd_rn(__dadd_rn(__dmul_rn(td[6], qq[0]), __dmul_rn(td[7], qq[1])), __dmul_rn(td[8], qq[2])), td[11]);
+            double dx = __dsub_rn(x, rr[0]), dy = __dsub_rn(y, rr[1]), dz = __dsub_rn(z, rr[2]);
+            double d = __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz));
+            tq = __dadd_rn(tq, __ddiv_rn(d0q2, __dadd_rn(d0q2, d)));
+            tr = __dadd_rn(tr, __ddiv_rn(d0r2, __dadd_rn(d0r2, d)));
+#pragma unroll
+            for (int a = 0; a < 3; a++)
+#pragma unroll
+                for (int b = 0; b < 3; b++) dv[3 * a + b] = __dadd_rn(dv[3 * a + b], __dmul_rn(qq[a], rr[b]));
+#pragma unroll
+            for (int a = 0; a < 3; a++) {
+                dv[9 + a] = __dadd_rn(dv[9 + a], qq[a]);
+                dv[12 + a] = __dadd_rn(dv[12 + a], rr[a]);
+                dv[15 + a] = __dadd_rn(dv[15 + a], __dmul_rn(qq[a], qq[a]));
+                dv[18 + a] = __dadd_rn(dv[18 + a], __dmul_rn(rr[a], rr[a]));
+            }
+        }
+        double r64 = rmsd_from_sums(dv, (double)n);
+        float r32 = T.rmsd32[i];
+        if (r32 >= 0.f) {
+            T.err[i * 4 + 2] = (float)fabs(__dsub_rn((double)r32, r64));
+            out[8] = (float)r64;
+        }
+        if (out[9] > 0.f || out[10] > 0.f) {
+            double tmq = __ddiv_rn(tq, (double)lq), tmr = __ddiv_rn(tr, (double)lr);
+            T.err[i * 4 + 0] = (float)fabs(__dsub_rn((double)out[9], tmq));
+            T.err[i * 4 + 1] = (float)fabs(__dsub_rn((double)out[10], tmr));
+            out[9] = (float)tmq;
+            out[10] = (float)tmr;
+        }
+    }
+    if (referenced) {
+        float R[9];
+#pragma unroll
+        for (int f = 0; f < 9; f++) R[f] = t[f];
+#pragma unroll
+        for (int a = 0; a < 3; a++)
+#pragma unroll
+            for (int b = 0; b < 3; b++) t[3 * a + b] = R[3 * b + a];
+        float t0 = t[9], t1 = t[10], t2 = t[11];
+        t[9] = -__fadd_rn(__fadd_rn(__fmul_rn(R[0], t0), __fmul_rn(R[3], t1)), __fmul_rn(R[6], t2));
+        t[10] = -__fadd_rn(__fadd_rn(__fmul_rn(R[1], t0), __fmul_rn(R[4], t1)), __fmul_rn(R[7], t2));
+        t[11] = -__fadd_rn(__fadd_rn(__fmul_rn(R[2], t0), __fmul_rn(R[5], t1)), __fmul_rn(R[8], t2));
+    }
+}
+
+void launch_final(const Blk& B, const Bat& T, int referenced, cudaStream_t st) {
+    k_final<<<(T.np + 127) / 128, 128, 0, st>>>(B, T, referenced);
+    GTB_LAUNCHED(T);
+}
+
+}  // namespace gtb

@@ -1,0 +1,56 @@
+// gtb_kernels.cuh -- kernel-side data layout and launchers of the search.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace gtb {
+
+// Block of queries x references (device pointers, SoA).
+struct Blk {
+    int nq, nr;
+    const int *qlen, *rlen;          // lengths
+    const int *qoff, *roff;          // first-residue offsets
+    const float *qx, *qy, *qz, *rx, *ry, *rz;
+    const unsigned char *qa, *ra;    // residue letters
+    const char *qs, *rs;             // secondary structure
+    const int *qmol, *rmol;          // molecule type per structure
+    int qmax, qmin, rmax, rmin;      // block-level length extremes
+    const float *t_d0, *t_d82, *t_d0fin;  // per-length constants
+    int stepinit, refinement, depth, symmetric, nodeletions;
+};
+
+// Batch of consecutive pairs p0 .. p0+np-1 of a block (pair = qi*nr + ri).
+struct Bat {
+    long long p0;
+    int np;
+    int *flags, *seedq, *seedr, *naln, *sfndx, *sfpos, *sfndx_cur, *sfpos_cur;
+    float *grand, *best, *best0, *rmsd32;
+    float *tfm_ib, *tfm_gr;          // [np][12]
+    float *out, *err;                // [np][16], [np][4]
+    const long long *off_bt;  uint2* bt;      // traceback words per pair
+    const long long *off_row; float* row;     // DP row buffer per pair
+    const long long *off_aln; unsigned* aln;  // aligned pairs, reverse order
+    const long long *off_str; char* str;      // alignment rows per pair
+    long long* launches;             // host counter of kernel launches
+};
+
+enum RefineMode { RM_INIT = 0, RM_DP = 1, RM_FIN1 = 2, RM_FIN2 = 3, RM_PROD1 = 4, RM_PROD2 = 5 };
+enum DpTfm { DP_TFM_IBEST = 0, DP_TFM_GRAND = 1 };
+
+void launch_secstr(char* ss, const float* x, const float* y, const float* z,
+                   const int* len, const int* off, const int* mol, int nstr,
+                   cudaStream_t st, long long* launches);
+void launch_init(const Blk& B, const Bat& T, cudaStream_t st);
+void launch_findfrag(const Blk& B, const Bat& T, cudaStream_t st);
+void launch_refine(int mode, const Blk& B, const Bat& T, cudaStream_t st);
+// skipmode 0: skip LOWTMSC|SCOREDP (plain), 1: skip LOWTMSC only
+void launch_dp(const Blk& B, const Bat& T, int tfmsrc, int gap0, float gcost, int usess,
+               int dpscan, int skipmode, cudaStream_t st);
+void launch_btck(const Blk& B, const Bat& T, int constrained, cudaStream_t st);
+void launch_post(const Blk& B, const Bat& T, int dpi, int maxit, int prescreen,
+                 float prescore, cudaStream_t st);
+void launch_lowscore(const Blk& B, const Bat& T, float thr, cudaStream_t st);
+void launch_alnstr(const Blk& B, const Bat& T, cudaStream_t st);
+void launch_final(const Blk& B, const Bat& T, int referenced, cudaStream_t st);
+
+}  // namespace gtb

@@ -1,0 +1,164 @@
+/*
+ * gtb200.h -- C ABI of the B200 (sm_100a) GTalign superposition-search library.
+ *
+ * Drop-in replacement for the stage sequence beneath CuBatch::ProcessBlock of
+ * the reference (src/libmycu/cubatch/CuBatch.cuh:74-85, defined at
+ * src/libmycu/cubatch/CuBatch.cu:339-717): the same SoA structure batches in,
+ * the same per-pair result records, 12-float transformation matrices and
+ * alignment rows out.  Plain C types only; errors are status codes (no C++
+ * exceptions cross this boundary).
+ *
+ * Threading: one handle per host thread / device area, as the reference's
+ * CuBatch (one stream per call, CuBatch.cu:420).  A handle is not reentrant.
+ */
+#ifndef GTB200_H
+#define GTB200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+    GTB_OK = 0,
+    GTB_ERR_ARG = 1,          /* invalid argument (null pointer, bad size) */
+    GTB_ERR_CUDA = 2,         /* CUDA runtime error; see gtb_last_error */
+    GTB_ERR_NOMEM = 3,        /* the block does not fit the device memory budget */
+    GTB_ERR_UNSUPPORTED = 4,  /* option combination not implemented */
+    GTB_ERR_TOO_LONG = 5,     /* structure longer than 65535 residues */
+    GTB_ERR_NOT_BUILT = 6     /* library built without device code */
+} gtb_status;
+
+/* Field indices of the reference's SoA batch (PM2DVectorFields.h:220-239):
+ * pmbeg[f]/pmend[f] delimit field f over all structures of a block. */
+enum {
+    GTB_FLD_LEN = 0,      /* int32 structure length (pps2DLen) */
+    GTB_FLD_DIST = 1,     /* uint32 offset of the structure's first residue (pps2DDist) */
+    GTB_FLD_TYPE = 2,     /* int32 (pps2DType, unused here) */
+    GTB_FLD_X = 3,        /* float x (pmv2DCoords+0) */
+    GTB_FLD_Y = 4,        /* float y */
+    GTB_FLD_Z = 5,        /* float z */
+    GTB_FLD_INSCHORD = 6, /* int32; sign of the first residue's value = molecule type:
+                             > 0 nucleic acid, <= 0 protein (GetMoleculeType) */
+    GTB_FLD_RESNUM = 7,   /* int32 residue number (unused here) */
+    GTB_FLD_RSD = 8,      /* char residue letter (pmv2Drsd) */
+    GTB_FLD_SS = 9,       /* char secondary structure (pmv2Dss; computed here) */
+    GTB_NFIELDS = 10
+};
+
+/* Per-pair output record (gproc.h:148-168, TDP2OutputAlnData) */
+enum {
+    GTB_OUT_ORGSTRNO = 0, GTB_OUT_STRNEWDST = 1, GTB_OUT_BEGCOORDS = 2,
+    GTB_OUT_ENDCOORDS = 3, GTB_OUT_ALNLENGTH = 4, GTB_OUT_PSTVS = 5,
+    GTB_OUT_IDNTS = 6, GTB_OUT_NGAPS = 7, GTB_OUT_RMSD = 8, GTB_OUT_SCOREQ = 9,
+    GTB_OUT_SCORER = 10, GTB_OUT_D0Q = 11, GTB_OUT_D0R = 12,
+    GTB_OUT_2SCOREQ = 13, GTB_OUT_2SCORER = 14, GTB_NOUT = 16
+};
+/* Per-pair numeric error record: |FP32 search path - FP64 recomputation| */
+enum { GTB_ERR_TMQ = 0, GTB_ERR_TMR = 1, GTB_ERR_RMSD = 2, GTB_NERR = 4 };
+
+/* Options the path reads (CuBatch.cu:353-366, custage_fin.cu:243-245,409),
+ * with the values of the gtalign command line. */
+typedef struct {
+    int   refinement;        /* --refinement 0 (coarse) or 1 (one search) */
+    int   depth;             /* --depth 0..3 (3 = shallow: seed step 5) */
+    int   convergence;       /* --convergence 1..30 */
+    float prescore;          /* --pre-score [0,1) */
+    int   symmetric;         /* --symmetric */
+    int   referenced;        /* --referenced */
+    int   nodeletions;       /* --no-deletions */
+    int   nodetailedsearch;  /* --no-detailed-search: must be 1 (the spatial-index
+                                search stage is not part of this library) */
+    int   addsearchbyss;     /* --add-search-by-ss: must be 0 */
+    int   twotmscore;        /* --2tm-score: must be 0 */
+} gtb_options;
+
+/* Result buffers (host memory), sizes for nq queries x nr references with
+ * total residue counts Nq, Nr:
+ *   alndata: nq*nr*GTB_NOUT floats    (record of pair (qi,ri) at (qi*nr+ri)*GTB_NOUT)
+ *   tfm:     nq*nr*12 floats          (row-major rotation, then translation;
+ *                                      transforms the query onto the reference,
+ *                                      or the reverse with --referenced)
+ *   alns:    sum over qi of 5*(Nr + nr*(lq_i+1)) bytes, the reference's layout
+ *            (MpDPHub.cpp:1975-1981): for query qi, 5 rows (query, middle,
+ *            target, query SS, target SS) of length Nr + nr*(lq_i+1); pair
+ *            (qi,ri) starts at column dist_ri + ri*(lq_i+1); NUL-terminated.
+ *            May be NULL.
+ *   numerr:  nq*nr*GTB_NERR floats; may be NULL.
+ *   qss/rss: Nq / Nr secondary-structure letters; may be NULL. */
+typedef struct {
+    float* alndata;
+    float* tfm;
+    char*  alns;
+    float* numerr;
+    char*  qss;
+    char*  rss;
+} gtb_results;
+
+typedef struct gtb_handle gtb_handle;
+
+/* Create a handle on CUDA device `device` with a device-memory budget of
+ * `mem_bytes` (0 = all free memory minus 256 MB; the --dev-mem analogue,
+ * Devices.cu:206-213).  Replaces the construction of CuDeviceMemory + CuBatch. */
+gtb_status gtb_create(int device, size_t mem_bytes, const gtb_options* opts,
+                      gtb_handle** out);
+
+/* Align every query of a block with every reference of a block.
+ * Replaces CuBatch::TransferQueryPMDataToDevice + TransferCPMDataToDevice +
+ * CuBatch::ProcessBlock (CuBatch.cuh:54-85).  querypmbeg/querypmend and
+ * bdbCpmbeg/bdbCpmend are arrays of GTB_NFIELDS host pointers delimiting each
+ * SoA field, exactly as PMBatchStrData hands them to the reference.
+ * scorethld is the -s threshold.  All buffers are host memory; the call
+ * copies inputs to the device and results back before returning. */
+gtb_status gtb_process_block(gtb_handle* h, float scorethld,
+                             char* const* querypmbeg, char* const* querypmend,
+                             char* const* bdbCpmbeg, char* const* bdbCpmend,
+                             gtb_results* out);
+
+/* Total bytes of the alns buffer for a block (GetSizeOfDP2Alns,
+ * CuMemoryBase.h:150-158). */
+size_t gtb_alns_size(char* const* querypmbeg, char* const* querypmend,
+                     char* const* bdbCpmbeg, char* const* bdbCpmend);
+
+/* Adjoint of the TM-score for fixed alignments (no reference counterpart:
+ * the superposition-polishing extension of this library).
+ * For npairs pairs, pair p has n_p aligned residue pairs at aln offset
+ * off[p] (arrays qxyz/rxyz hold 3*sum(n_p) floats, xyz interleaved per
+ * residue), a transform tfm[p*12..] and a d0 value d0[p].  Computes
+ * tm[p] = sum_i d0^2/(d0^2 + |R q_i + t - r_i|^2) and its gradient with
+ * respect to the rotation vector (omega, a left-multiplied infinitesimal
+ * rotation) and the translation: grad[p*6..] = (dTM/domega_xyz, dTM/dt_xyz).
+ * When gq is non-NULL the per-residue gradient with respect to the query
+ * coordinates is written to gq (3*sum(n_p)).  Device pointers, stream. */
+gtb_status gtb_tm_adjoint(gtb_handle* h, int npairs, const long long* off,
+                          const int* n, const float* qxyz, const float* rxyz,
+                          const float* tfm, const float* d0,
+                          float* tm, float* grad, float* gq, void* stream);
+
+/* Projected-gradient polishing of transforms on SO(3) x R^3 for fixed
+ * alignments: `steps` ascent steps with backtracking; a step is only
+ * accepted when it does not lower the TM-score.  Device pointers, stream.
+ * tm_before/tm_after receive the scores (may be NULL). */
+gtb_status gtb_polish(gtb_handle* h, int npairs, const long long* off,
+                      const int* n, const float* qxyz, const float* rxyz,
+                      float* tfm, const float* d0, int steps,
+                      float* tm_before, float* tm_after, void* stream);
+
+/* Message of the last error on this handle (static storage of the handle). */
+const char* gtb_last_error(const gtb_handle* h);
+
+/* Number of kernel launches issued by the last gtb_process_block call. */
+long long gtb_last_launch_count(const gtb_handle* h);
+
+/* Device time (ms) of the last gtb_process_block call, per stage:
+ * [0] stage 1 seed, [1] stage-1 refinement, [2] DP kernels, [3] traceback,
+ * [4] DP-alignment refinement, [5] final + production, [6] total. */
+gtb_status gtb_last_timings(const gtb_handle* h, float* ms7);
+
+void gtb_destroy(gtb_handle* h);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
