@@ -301,11 +301,11 @@ static gtb_status run_block(gtb_handle* h, const DevBlock& D, float scorethld,
 
         // ------------------------------------------------------------ results
         if (h_alndata)
-            CK(cudaMemcpyAsync(h_alndata + p0 * 16, T.out, (size_t)np * 16 * sizeof(float), cudaMemcpyDeviceToHost, st));
+            CK(cudaMemcpyAsync(h_alndata + p0 * 16, T.out, (size_t)np * 16 * sizeof(float), cudaMemcpyDefault, st));
         if (h_tfm)
-            CK(cudaMemcpyAsync(h_tfm + p0 * 12, T.tfm_gr, (size_t)np * 12 * sizeof(float), cudaMemcpyDeviceToHost, st));
+            CK(cudaMemcpyAsync(h_tfm + p0 * 12, T.tfm_gr, (size_t)np * 12 * sizeof(float), cudaMemcpyDefault, st));
         if (h_err)
-            CK(cudaMemcpyAsync(h_err + p0 * 4, T.err, (size_t)np * 4 * sizeof(float), cudaMemcpyDeviceToHost, st));
+            CK(cudaMemcpyAsync(h_err + p0 * 4, T.err, (size_t)np * 4 * sizeof(float), cudaMemcpyDefault, st));
         if (strings)
             CK(cudaMemcpyAsync(hstr + (*hstroff)[p0], T.str, (size_t)off_str[np], cudaMemcpyDeviceToHost, st));
         CK(cudaFreeAsync(base, st));
@@ -381,6 +381,97 @@ extern "C" size_t gtb_alns_size(char* const* qb, char* const* qe, char* const* r
     return s;
 }
 
+struct gtb_block {
+    int n = 0;
+    long long npos = 0;
+    std::vector<int> len, off, mol;
+    char* dbase = nullptr;
+    int *dlen = nullptr, *doff = nullptr, *dmol = nullptr;
+    float *x = nullptr, *y = nullptr, *z = nullptr;
+    unsigned char* rsd = nullptr;
+    char* ss = nullptr;
+};
+
+static gtb_status upload_block(gtb_handle* h, const HostSoA& S, gtb_block* b) {
+    cudaStream_t st = h->st;
+    b->n = S.n; b->npos = S.npos;
+    b->len.assign(S.len, S.len + S.n);
+    b->off = S.off; b->mol = S.mol;
+    size_t sz = 0;
+    auto carve = [&](size_t bytes) { size_t o2 = sz; sz += align256(bytes); return o2; };
+    size_t ol = carve(S.n * 4), oo = carve(S.n * 4), om = carve(S.n * 4);
+    size_t ox = carve(S.npos * 4), oy = carve(S.npos * 4), oz = carve(S.npos * 4);
+    size_t oa = carve(S.npos), os = carve(S.npos);
+    CK(cudaMalloc((void**)&b->dbase, sz));
+    char* d = b->dbase;
+    b->dlen = (int*)(d + ol); b->doff = (int*)(d + oo); b->dmol = (int*)(d + om);
+    b->x = (float*)(d + ox); b->y = (float*)(d + oy); b->z = (float*)(d + oz);
+    b->rsd = (unsigned char*)(d + oa); b->ss = d + os;
+    CK(cudaMemcpyAsync(b->dlen, S.len, S.n * 4, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(b->doff, S.off.data(), S.n * 4, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(b->dmol, S.mol.data(), S.n * 4, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(b->x, S.x, S.npos * 4, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(b->y, S.y, S.npos * 4, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(b->z, S.z, S.npos * 4, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(b->rsd, S.rsd, S.npos, cudaMemcpyHostToDevice, st));
+    long long nl = 0;
+    launch_secstr(b->ss, b->x, b->y, b->z, b->dlen, b->doff, b->dmol, b->n, st, &nl);
+    CK(cudaGetLastError());
+    return GTB_OK;
+}
+
+static void free_block(gtb_block* b) {
+    if (!b) return;
+    if (b->dbase) cudaFree(b->dbase);
+    delete b;
+}
+
+extern "C" gtb_status gtb_block_upload(gtb_handle* h, char* const* pmbeg, char* const* pmend,
+                                       gtb_block** out) {
+    if (!h || !out) return GTB_ERR_ARG;
+    *out = nullptr;
+    h->err[0] = 0;
+    HostSoA S;
+    gtb_status s = parse_soa(h, pmbeg, pmend, S, "block");
+    if (s != GTB_OK) return s;
+    CK(cudaSetDevice(h->dev));
+    gtb_block* b = new gtb_block();
+    s = upload_block(h, S, b);
+    if (s != GTB_OK) { free_block(b); return s; }
+    CK(cudaStreamSynchronize(h->st));
+    *out = b;
+    return GTB_OK;
+}
+
+extern "C" void gtb_block_free(gtb_handle* h, gtb_block* b) {
+    if (h) cudaSetDevice(h->dev);
+    free_block(b);
+}
+
+static DevBlock make_devblock(const gtb_block* Q, const gtb_block* R) {
+    DevBlock D;
+    D.nq = Q->n; D.nr = R->n;
+    D.qlen = Q->dlen; D.qoff = Q->doff; D.qmol = Q->dmol;
+    D.rlen = R->dlen; D.roff = R->doff; D.rmol = R->dmol;
+    D.qx = Q->x; D.qy = Q->y; D.qz = Q->z; D.rx = R->x; D.ry = R->y; D.rz = R->z;
+    D.qa = Q->rsd; D.ra = R->rsd; D.qs = Q->ss; D.rs = R->ss;
+    D.hqlen = Q->len; D.hrlen = R->len;
+    return D;
+}
+
+extern "C" gtb_status gtb_process_resident(gtb_handle* h, float scorethld, const gtb_block* queries,
+                                           const gtb_block* refs, float* d_alndata, float* d_tfm,
+                                           float* d_numerr) {
+    if (!h || !queries || !refs || !d_alndata || !d_tfm) return GTB_ERR_ARG;
+    h->err[0] = 0;
+    if (!(scorethld >= 0.f && scorethld < 1.f)) { snprintf(h->err, sizeof(h->err), "scorethld out of [0,1)"); return GTB_ERR_ARG; }
+    gtb_status s = check_options(h);
+    if (s != GTB_OK) return s;
+    CK(cudaSetDevice(h->dev));
+    DevBlock D = make_devblock(queries, refs);
+    return run_block(h, D, scorethld, d_alndata, d_tfm, d_numerr, nullptr, nullptr);
+}
+
 extern "C" gtb_status gtb_process_block(gtb_handle* h, float scorethld,
                                         char* const* querypmbeg, char* const* querypmend,
                                         char* const* bdbCpmbeg, char* const* bdbCpmend,
@@ -396,46 +487,12 @@ extern "C" gtb_status gtb_process_block(gtb_handle* h, float scorethld,
     if ((s = parse_soa(h, bdbCpmbeg, bdbCpmend, R, "references")) != GTB_OK) return s;
     CK(cudaSetDevice(h->dev));
     cudaStream_t st = h->st;
-
-    // upload (SoA, one allocation)
-    size_t sz = 0;
-    auto carve = [&](size_t bytes) { size_t o2 = sz; sz += align256(bytes); return o2; };
-    size_t oql = carve(Q.n * 4), oqo = carve(Q.n * 4), oqm = carve(Q.n * 4);
-    size_t orl = carve(R.n * 4), oro = carve(R.n * 4), orm = carve(R.n * 4);
-    size_t oqx = carve(Q.npos * 4), oqy = carve(Q.npos * 4), oqz = carve(Q.npos * 4);
-    size_t orx = carve(R.npos * 4), ory = carve(R.npos * 4), orz = carve(R.npos * 4);
-    size_t oqa = carve(Q.npos), ora = carve(R.npos), oqs = carve(Q.npos), ors = carve(R.npos);
-    char* dbase = nullptr;
-    CK(cudaMallocAsync((void**)&dbase, sz, st));
-    CK(cudaMemcpyAsync(dbase + oql, Q.len, Q.n * 4, cudaMemcpyHostToDevice, st));
-    CK(cudaMemcpyAsync(dbase + oqo, Q.off.data(), Q.n * 4, cudaMemcpyHostToDevice, st));
-    CK(cudaMemcpyAsync(dbase + oqm, Q.mol.data(), Q.n * 4, cudaMemcpyHostToDevice, st));
-    CK(cudaMemcpyAsync(dbase + orl, R.len, R.n * 4, cudaMemcpyHostToDevice, st));
-    CK(cudaMemcpyAsync(dbase + oro, R.off.data(), R.n * 4, cudaMemcpyHostToDevice, st));
-    CK(cudaMemcpyAsync(dbase + orm, R.mol.data(), R.n * 4, cudaMemcpyHostToDevice, st));
-    CK(cudaMemcpyAsync(dbase + oqx, Q.x, Q.npos * 4, cudaMemcpyHostToDevice, st));
-    CK(cudaMemcpyAsync(dbase + oqy, Q.y, Q.npos * 4, cudaMemcpyHostToDevice, st));
-    CK(cudaMemcpyAsync(dbase + oqz, Q.z, Q.npos * 4, cudaMemcpyHostToDevice, st));
-    CK(cudaMemcpyAsync(dbase + orx, R.x, R.npos * 4, cudaMemcpyHostToDevice, st));
-    CK(cudaMemcpyAsync(dbase + ory, R.y, R.npos * 4, cudaMemcpyHostToDevice, st));
-    CK(cudaMemcpyAsync(dbase + orz, R.z, R.npos * 4, cudaMemcpyHostToDevice, st));
-    CK(cudaMemcpyAsync(dbase + oqa, Q.rsd, Q.npos, cudaMemcpyHostToDevice, st));
-    CK(cudaMemcpyAsync(dbase + ora, R.rsd, R.npos, cudaMemcpyHostToDevice, st));
-
-    DevBlock D;
-    D.nq = Q.n; D.nr = R.n;
-    D.qlen = (int*)(dbase + oql); D.qoff = (int*)(dbase + oqo); D.qmol = (int*)(dbase + oqm);
-    D.rlen = (int*)(dbase + orl); D.roff = (int*)(dbase + oro); D.rmol = (int*)(dbase + orm);
-    D.qx = (float*)(dbase + oqx); D.qy = (float*)(dbase + oqy); D.qz = (float*)(dbase + oqz);
-    D.rx = (float*)(dbase + orx); D.ry = (float*)(dbase + ory); D.rz = (float*)(dbase + orz);
-    D.qa = (unsigned char*)(dbase + oqa); D.ra = (unsigned char*)(dbase + ora);
-    D.qs = dbase + oqs; D.rs = dbase + ors;
-    D.hqlen.assign(Q.len, Q.len + Q.n);
-    D.hrlen.assign(R.len, R.len + R.n);
-    long long ss_launch = 0;
-    launch_secstr(D.qs, D.qx, D.qy, D.qz, D.qlen, D.qoff, D.qmol, Q.n, st, &ss_launch);
-    launch_secstr(D.rs, D.rx, D.ry, D.rz, D.rlen, D.roff, D.rmol, R.n, st, &ss_launch);
-    CK(cudaGetLastError());
+    gtb_block* qb = new gtb_block();
+    gtb_block* rb = new gtb_block();
+    s = upload_block(h, Q, qb);
+    if (s == GTB_OK) s = upload_block(h, R, rb);
+    if (s != GTB_OK) { cudaStreamSynchronize(st); free_block(qb); free_block(rb); return s; }
+    DevBlock D = make_devblock(qb, rb);
 
     // compact per-pair alignment rows, scattered to the reference layout after
     std::vector<long long> stroff;
@@ -450,12 +507,21 @@ extern "C" gtb_status gtb_process_block(gtb_handle* h, float scorethld,
     }
     s = run_block(h, D, scorethld, out->alndata, out->tfm, out->numerr,
                   out->alns ? hstr.data() : nullptr, out->alns ? &stroff : nullptr);
-    h->launches += ss_launch;
-    if (s != GTB_OK) { cudaFreeAsync(dbase, st); cudaStreamSynchronize(st); return s; }
-    if (out->qss) CK(cudaMemcpyAsync(out->qss, D.qs, Q.npos, cudaMemcpyDeviceToHost, st));
-    if (out->rss) CK(cudaMemcpyAsync(out->rss, D.rs, R.npos, cudaMemcpyDeviceToHost, st));
-    CK(cudaFreeAsync(dbase, st));
-    CK(cudaStreamSynchronize(st));
+    h->launches += 2;  // secondary-structure launches of the two uploads
+    if (s == GTB_OK) {
+        cudaError_t e1 = cudaSuccess;
+        if (out->qss) e1 = cudaMemcpyAsync(out->qss, qb->ss, Q.npos, cudaMemcpyDeviceToHost, st);
+        if (e1 == cudaSuccess && out->rss) e1 = cudaMemcpyAsync(out->rss, rb->ss, R.npos, cudaMemcpyDeviceToHost, st);
+        if (e1 == cudaSuccess) e1 = cudaStreamSynchronize(st);
+        if (e1 != cudaSuccess) {
+            snprintf(h->err, sizeof(h->err), "result copy: %s", cudaGetErrorString(e1));
+            s = GTB_ERR_CUDA;
+        }
+    }
+    cudaStreamSynchronize(st);
+    free_block(qb);
+    free_block(rb);
+    if (s != GTB_OK) return s;
 
     if (out->alns) {
         // reference layout (MpDPHub.cpp:1975-1981)

@@ -71,83 +71,82 @@ def _internal_coords(rng: np.random.Generator, L: int):
     """Bond angles and torsions (radians) for a chain of L residues."""
     theta = np.deg2rad(rng.normal(105.0, 10.0, size=L))
     tau = rng.uniform(-np.pi, np.pi, size=L)
-    i = 0
-    while i < L:
-        r = rng.random()
-        run = int(rng.integers(4, 21))
-        if r < 0.35:          # helix run
-            theta[i:i+run] = np.deg2rad(91.0)
-            tau[i:i+run] = np.deg2rad(50.0)
-            i += run
-        elif r < 0.6:         # strand run
-            theta[i:i+run] = np.deg2rad(120.0)
-            tau[i:i+run] = np.deg2rad(-170.0)
-            i += run
-        else:                 # coil
-            i += int(rng.integers(2, 9))
+    nseg = L // 2 + 2
+    kind = rng.random(nseg)
+    seglen = np.where(kind < 0.6, rng.integers(4, 21, size=nseg), rng.integers(2, 9, size=nseg))
+    per = np.repeat(kind, seglen)[:L]
+    hel = per < 0.35
+    strd = (per >= 0.35) & (per < 0.6)
+    theta[hel] = np.deg2rad(91.0)
+    tau[hel] = np.deg2rad(50.0)
+    theta[strd] = np.deg2rad(120.0)
+    tau[strd] = np.deg2rad(-170.0)
     return theta, tau
 
 
-def _nerf_batch(theta: np.ndarray, tau: np.ndarray, bond: float = 3.8) -> np.ndarray:
-    """NeRF over a batch: theta, tau of shape (B, L) -> coords (B, L, 3)."""
-    B, L = theta.shape
-    X = np.zeros((B, L, 3))
-    if L > 1:
-        X[:, 1, 0] = bond
-    if L > 2:
-        t = theta[:, 2]
-        X[:, 2, 0] = bond - bond * np.cos(t)
-        X[:, 2, 1] = bond * np.sin(t)
-    for i in range(3, L):
-        a, b, c = X[:, i-3], X[:, i-2], X[:, i-1]
-        bc = c - b
-        bc /= np.linalg.norm(bc, axis=1, keepdims=True)
-        n = np.cross(b - a, bc)
-        nn = np.linalg.norm(n, axis=1, keepdims=True)
-        nn[nn < 1e-9] = 1.0
-        n /= nn
-        m = np.cross(n, bc)
-        th, to = theta[:, i], tau[:, i]
-        d2 = np.stack([-bond * np.cos(th),
-                       bond * np.sin(th) * np.cos(to),
-                       bond * np.sin(th) * np.sin(to)], axis=1)
-        X[:, i] = c + d2[:, 0:1] * bc + d2[:, 1:2] * m + d2[:, 2:3] * n
-    return X
-
-
-def _pdb_round(x: np.ndarray) -> np.ndarray:
-    """Round to 3 decimals and convert each value as strtof would."""
-    x = np.round(np.asarray(x, dtype=np.float64), 3)
-    flat = x.ravel()
-    out = np.empty(flat.shape, dtype=np.float32)
-    for i, v in enumerate(flat):
-        out[i] = _libc.strtof(("%.3f" % v).encode(), None)
-    return out.reshape(x.shape)
+def _nerf_flat(theta: np.ndarray, tau: np.ndarray, lens: np.ndarray, bond: float = 3.8) -> np.ndarray:
+    """NeRF for many chains at once.  Chains are sorted by decreasing length;
+    theta/tau are flat arrays (chain k owns [off[k], off[k]+lens[k])).
+    Returns flat (sum(lens), 3) coordinates."""
+    n = len(lens)
+    off = np.zeros(n, np.int64)
+    off[1:] = np.cumsum(lens[:-1])
+    out = np.zeros((int(lens.sum()), 3))
+    Lmax = int(lens.max()) if n else 0
+    # window of the last three atoms per chain
+    a = np.zeros((n, 3)); b = np.zeros((n, 3)); c = np.zeros((n, 3))
+    for i in range(Lmax):
+        m = int(np.searchsorted(-lens, -i, side="left"))  # chains with lens > i are [0, m)
+        m = int((lens > i).sum()) if m == 0 or lens[m - 1] <= i else m
+        if m == 0:
+            break
+        idx = off[:m] + i
+        if i == 0:
+            p = np.zeros((m, 3))
+        elif i == 1:
+            p = np.zeros((m, 3)); p[:, 0] = bond
+        elif i == 2:
+            t = theta[idx]
+            p = np.zeros((m, 3)); p[:, 0] = bond - bond * np.cos(t); p[:, 1] = bond * np.sin(t)
+        else:
+            A, Bv, C = a[:m], b[:m], c[:m]
+            bc = C - Bv
+            bc /= np.linalg.norm(bc, axis=1, keepdims=True)
+            nn = np.cross(Bv - A, bc)
+            nl = np.linalg.norm(nn, axis=1, keepdims=True)
+            nl[nl < 1e-9] = 1.0
+            nn /= nl
+            mm = np.cross(nn, bc)
+            th, to = theta[idx], tau[idx]
+            d0 = -bond * np.cos(th)
+            d1 = bond * np.sin(th) * np.cos(to)
+            d2 = bond * np.sin(th) * np.sin(to)
+            p = C + d0[:, None] * bc + d1[:, None] * mm + d2[:, None] * nn
+        out[idx] = p
+        a[:m], b[:m], c[:m] = b[:m], c[:m], p
+    return out
 
 
 def _pdb_round_fast(x: np.ndarray) -> np.ndarray:
-    """Vectorised rounding: exact float32 of the 3-decimal value.
+    """Round to 3 decimals and convert to float32 as strtof would.
 
-    The 3-decimal value k/1000 with |k| < 2**24 is converted by dividing the
-    exact integer k by 1000 in float64 and rounding to float32.  Double
-    rounding (decimal -> float64 -> float32) can differ from a direct
-    decimal -> float32 conversion only when the float64 result lies within
-    2**-29 relative of a float32 rounding boundary; those values are re-done
-    with strtof.
+    The 3-decimal value k/1000 is formed in float64 and rounded to float32.
+    Double rounding (decimal -> float64 -> float32) can differ from a direct
+    decimal -> float32 conversion only when the float64 value lies within
+    2**-29 relative of a float32 rounding boundary; such values are converted
+    again with strtof.
     """
     k = np.round(np.asarray(x, dtype=np.float64) * 1000.0)
     d = k / 1000.0
     f = d.astype(np.float32)
-    # detect near-ties of the float64 -> float32 rounding
     back = f.astype(np.float64)
     ulp = np.abs(np.spacing(f).astype(np.float64))
     frac = np.abs(d - back) / ulp
     risky = np.abs(frac - 0.5) < 1e-6
     if np.any(risky):
-        idx = np.nonzero(risky.ravel())[0]
         ff = f.ravel()
         dd = d.ravel()
-        for i in idx:
+        for i in np.nonzero(risky.ravel())[0]:
             ff[i] = _libc.strtof(("%.3f" % dd[i]).encode(), None)
         f = ff.reshape(f.shape)
     return f
@@ -156,28 +155,28 @@ def _pdb_round_fast(x: np.ndarray) -> np.ndarray:
 def random_chains(rng: np.random.Generator, lengths: Sequence[int],
                   prefix: str = "rnd") -> List[Chain]:
     """Unrelated random-walk chains with helix/strand runs."""
-    lengths = list(int(l) for l in lengths)
-    out: List[Optional[Chain]] = [None] * len(lengths)
-    order = np.argsort(lengths, kind="stable")
-    # batch chains of equal length bucket (pad to the bucket max, then cut)
-    i = 0
-    while i < len(order):
-        j = min(i + 4096, len(order))
-        idx = order[i:j]
-        Lmax = max(lengths[k] for k in idx)
-        th = np.empty((len(idx), Lmax))
-        to = np.empty((len(idx), Lmax))
-        for r, k in enumerate(idx):
-            t1, t2 = _internal_coords(rng, Lmax)
-            th[r], to[r] = t1, t2
-        X = _nerf_batch(th, to)
-        for r, k in enumerate(idx):
-            L = lengths[k]
-            xyz = X[r, :L]
-            xyz = xyz - xyz.mean(axis=0) + rng.uniform(-20, 20, size=3)
-            seq = AA[rng.integers(0, len(AA), size=L)]
-            out[k] = Chain(_pdb_round_fast(xyz), seq.copy(), f"{prefix}{k:06d}")
-        i = j
+    lengths = np.asarray([int(l) for l in lengths], dtype=np.int64)
+    n = len(lengths)
+    if n == 0:
+        return []
+    order = np.argsort(-lengths, kind="stable")
+    sl = lengths[order]
+    ths, tos = [], []
+    for k in range(n):
+        t1, t2 = _internal_coords(rng, int(sl[k]))
+        ths.append(t1); tos.append(t2)
+    X = _nerf_flat(np.concatenate(ths), np.concatenate(tos), sl)
+    shifts = rng.uniform(-20, 20, size=(n, 3))
+    seqs = AA[rng.integers(0, len(AA), size=int(sl.sum()))]
+    out: List[Optional[Chain]] = [None] * n
+    o = 0
+    for j in range(n):
+        L = int(sl[j])
+        xyz = X[o:o + L]
+        xyz = xyz - xyz.mean(axis=0) + shifts[j]
+        k = int(order[j])
+        out[k] = Chain(_pdb_round_fast(xyz), seqs[o:o + L].copy(), f"{prefix}{k:06d}")
+        o += L
     return out  # type: ignore[return-value]
 
 
@@ -185,33 +184,44 @@ def homolog(rng: np.random.Generator, tmpl: Chain, sigma: float,
             indel_frac: float, name: str) -> Chain:
     """A noisy, indel-bearing, rigidly moved copy of ``tmpl``."""
     xyz = tmpl.xyz.astype(np.float64)
-    seq = tmpl.seq.copy()
+    seq = tmpl.seq
     L = xyz.shape[0]
     nindel = int(round(indel_frac * L))
+    pos = rng.integers(0, L, size=nindel)
+    isdel = rng.random(nindel) < 0.5
     keep = np.ones(L, dtype=bool)
-    ins_after = {}
-    for _ in range(nindel):
-        p = int(rng.integers(0, L))
-        if rng.random() < 0.5:
-            keep[p] = False
-        else:
-            ins_after[p] = ins_after.get(p, 0) + int(rng.integers(1, 4))
-    pts, aas = [], []
-    for p in range(L):
-        if keep[p]:
-            pts.append(xyz[p])
-            aas.append(seq[p] if rng.random() < 0.6 else AA[rng.integers(0, 20)])
-        for _ in range(ins_after.get(p, 0)):
-            base = pts[-1] if pts else xyz[p]
-            step = rng.normal(size=3)
-            step *= 3.8 / np.linalg.norm(step)
-            pts.append(base + step)
-            aas.append(AA[rng.integers(0, 20)])
-    P = np.array(pts)
+    keep[pos[isdel]] = False
+    nins = np.zeros(L, dtype=np.int64)
+    np.add.at(nins, pos[~isdel], rng.integers(1, 4, size=int((~isdel).sum())))
+    # each kept residue, then its insertions (random 3.8 A steps from it)
+    reps = keep.astype(np.int64) + nins
+    src = np.repeat(np.arange(L), reps)
+    first = np.zeros(len(src), dtype=bool)
+    starts = np.cumsum(reps) - reps
+    kept_first = starts[keep & (reps > 0)]
+    first[kept_first] = True
+    P = xyz[src].copy()
+    ins = ~first
+    if ins.any():
+        steps = rng.normal(size=(int(ins.sum()), 3))
+        steps *= 3.8 / np.linalg.norm(steps, axis=1, keepdims=True)
+        # cumulative walk within each insertion run
+        run_id = np.cumsum(first)
+        d = np.zeros_like(P)
+        d[ins] = steps
+        cs = np.cumsum(d, axis=0)
+        base = np.zeros_like(P)
+        idx_first = np.nonzero(first)[0]
+        if len(idx_first):
+            base = cs[idx_first][np.clip(run_id - 1, 0, len(idx_first) - 1)]
+        P = P + (cs - base) * ins[:, None]
+    aas = seq[src].copy()
+    mut = (rng.random(len(src)) >= 0.6) | ins
+    aas[mut] = AA[rng.integers(0, 20, size=int(mut.sum()))]
     P = P + rng.normal(0.0, sigma, size=P.shape)
     R = _rot_random(rng)
     P = (P - P.mean(axis=0)) @ R.T + rng.uniform(-30, 30, size=3)
-    return Chain(_pdb_round_fast(P), np.array(aas, dtype=np.uint8), name)
+    return Chain(_pdb_round_fast(P), aas.astype(np.uint8), name)
 
 
 def write_pdb(ch: Chain, path: str) -> None:

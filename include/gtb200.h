@@ -116,6 +116,20 @@ gtb_status gtb_process_block(gtb_handle* h, float scorethld,
                              char* const* bdbCpmbeg, char* const* bdbCpmend,
                              gtb_results* out);
 
+/* Device-resident blocks: the reference uploads a reference chunk once and
+ * reuses it for every query block (TdCommutator.cpp:265-285,
+ * CuDeviceMemory::TransferCPMDataToDevice); gtb_block_upload is that step.
+ * gtb_process_resident aligns two resident blocks and writes the result
+ * records, transforms and (optionally) numeric errors to DEVICE buffers of
+ * the sizes given for gtb_results (no alignment rows). */
+typedef struct gtb_block gtb_block;
+gtb_status gtb_block_upload(gtb_handle* h, char* const* pmbeg, char* const* pmend,
+                            gtb_block** out);
+void gtb_block_free(gtb_handle* h, gtb_block* b);
+gtb_status gtb_process_resident(gtb_handle* h, float scorethld, const gtb_block* queries,
+                                const gtb_block* refs, float* d_alndata, float* d_tfm,
+                                float* d_numerr);
+
 /* Total bytes of the alns buffer for a block (GetSizeOfDP2Alns,
  * CuMemoryBase.h:150-158). */
 size_t gtb_alns_size(char* const* querypmbeg, char* const* querypmend,

@@ -1,0 +1,122 @@
+"""Generate the golden fixtures of the parity tests from the reference itself.
+
+Runs the reference's own CPU build (oracle/_ref/gtalign, compiled from the
+reference sources by oracle/Makefile.ref) on seeded synthetic structure sets
+and records, per query-reference pair, what it prints in its JSON output:
+TM-scores (5 decimals), RMSD (2 decimals), counts, alignment rows,
+secondary-structure rows and the transform.  The input coordinates are
+stored with the fixtures, so the tests never need the reference or the
+generator again.
+
+For every set the reference is also run a second time with the query moved
+by a rigid rotation + translation (which leaves every score unchanged in
+exact arithmetic); the agreement between those two reference runs is the
+reference's own numerical reproducibility and is stored as `self_agreement`.
+
+    python tests/golden/make_golden.py        (needs oracle/_ref/gtalign)
+"""
+from __future__ import annotations
+
+import copy
+import json
+import os
+import shutil
+import subprocess
+import sys
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+from gtalign_alpha_b200 import synth  # noqa: E402
+
+BIN = os.path.join(ROOT, "oracle", "_ref", "gtalign")
+
+SETS = {
+    # name: (workload builder, reference CLI options)
+    "c0_speed13": (lambda: synth.config0(seed=101, n_refs=80, qlen=150),
+                   ["--speed=13", "--pre-score=0", "-s", "0"]),
+    "c0_default": (lambda: synth.config0(seed=102, n_refs=60, qlen=120),
+                   ["--no-detailed-search", "--pre-score=0", "-s", "0"]),
+    "c0_filters": (lambda: synth.config0(seed=103, n_refs=60, qlen=180),
+                   ["--no-detailed-search"]),  # default --pre-score 0.4 and -s 0.5
+    "c0_sym_ref_nodel": (lambda: synth.config0(seed=104, n_refs=40, qlen=100),
+                         ["--speed=13", "--pre-score=0", "-s", "0", "--symmetric",
+                          "--referenced", "--no-deletions"]),
+}
+
+
+def run(wl, opts):
+    d = tempfile.mkdtemp(prefix="gtgold")
+    try:
+        synth.write_dirs(wl, d + "/q", d + "/r")
+        subprocess.run([BIN, "--qrs=" + d + "/q", "--rfs=" + d + "/r", "-o", d + "/out",
+                        "--outfmt=1", "--cpu-threads=8", "--cpu-threads-reading=1"] + opts,
+                       check=True, capture_output=True)
+        res = {}
+        for f in os.listdir(d + "/out"):
+            J = json.load(open(os.path.join(d, "out", f)))["gtalign_search"]
+            qn = os.path.basename(J["query"]["description"].split()[0])[:-4]
+            for h in J["search_results"]:
+                h = h["hit_record"]
+                rn = os.path.basename(h["reference_description"].split()[0])[:-4]
+                a = h["alignment"]
+                res[qn + "|" + rn] = {
+                    "tmq": a["tmscore_query"], "tmr": a["tmscore_refn"], "rmsd": a["rmsd"],
+                    "d0q": a["d0_query"], "d0r": a["d0_refn"],
+                    "n_identities": a["n_identities"], "n_matched": a["n_matched"],
+                    "n_gaps": a["n_gaps"], "n_aligned": a["n_aligned"],
+                    "query_from": a["query_from"], "query_to": a["query_to"],
+                    "refn_from": a["refn_from"], "refn_to": a["refn_to"],
+                    "query_aln": a["query_aln"], "refrn_aln": a["refrn_aln"], "middle": a["middle"],
+                    "query_secstr": a["query_secstr"], "refrn_secstr": a["refrn_secstr"],
+                    "rotation": h["rotation_matrix_rowmajor"], "translation": h["translation_vector"],
+                }
+        return res
+    finally:
+        shutil.rmtree(d, ignore_errors=True)
+
+
+def agreement(a, b):
+    d, same = [], []
+    for k, v in a.items():
+        w = b.get(k)
+        if w is None:
+            continue
+        d.append(max(abs(v["tmq"] - w["tmq"]), abs(v["tmr"] - w["tmr"])))
+        same.append(v["query_aln"] == w["query_aln"] and v["refrn_aln"] == w["refrn_aln"])
+    d = np.array(d)
+    return {"pairs": len(d), "frac_tm_1e4": float((d <= 1e-4).mean()) if len(d) else 1.0,
+            "frac_aln_identical": float(np.mean(same)) if same else 1.0}
+
+
+def main():
+    if not os.path.exists(BIN):
+        sys.exit("build the reference first: make -f oracle/Makefile.ref")
+    for name, (mk, opts) in SETS.items():
+        wl = mk()
+        res = run(wl, opts)
+        wl2 = copy.deepcopy(wl)
+        rng = np.random.default_rng(7)
+        R = synth._rot_random(rng)
+        q = wl2.queries[0]
+        q.xyz = synth._pdb_round_fast(q.xyz.astype(np.float64) @ R.T + np.array([3.0, -5.0, 7.0]))
+        res2 = run(wl2, opts)
+        arrs = {}
+        for tag, chains in (("q", wl.queries), ("r", wl.refs)):
+            s = synth.pack(chains)
+            arrs[tag + "_lens"] = s.lens
+            arrs[tag + "_xyz"] = np.stack([s.x, s.y, s.z], axis=1)
+            arrs[tag + "_rsd"] = s.rsd
+            arrs[tag + "_names"] = np.array([c.name for c in chains])
+        np.savez_compressed(os.path.join(HERE, name + ".npz"), **arrs)
+        with open(os.path.join(HERE, name + ".json"), "w") as f:
+            json.dump({"options": opts, "seed_desc": wl.desc, "results": res,
+                       "self_agreement": agreement(res, res2)}, f, indent=0, sort_keys=True)
+        print(name, len(res), "pairs; reference self-agreement:", agreement(res, res2))
+
+
+if __name__ == "__main__":
+    main()

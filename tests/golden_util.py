@@ -1,0 +1,51 @@
+"""Loading of the golden fixtures made by tests/golden/make_golden.py."""
+import json
+import os
+
+import numpy as np
+
+from gtalign_alpha_b200.synth import SoA
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+SETS = ["c0_speed13", "c0_default", "c0_filters", "c0_sym_ref_nodel"]
+
+
+def _soa(z, tag):
+    lens = z[tag + "_lens"].astype(np.int32)
+    offs = np.zeros_like(lens)
+    if len(lens) > 1:
+        offs[1:] = np.cumsum(lens[:-1])
+    xyz = z[tag + "_xyz"].astype(np.float32)
+    return SoA(lens, offs, np.ascontiguousarray(xyz[:, 0]), np.ascontiguousarray(xyz[:, 1]),
+               np.ascontiguousarray(xyz[:, 2]), z[tag + "_rsd"].astype(np.uint8),
+               np.zeros(len(lens), np.int32))
+
+
+def load(name):
+    z = np.load(os.path.join(GOLDEN, name + ".npz"))
+    with open(os.path.join(GOLDEN, name + ".json")) as f:
+        meta = json.load(f)
+    return (_soa(z, "q"), _soa(z, "r"), list(z["q_names"]), list(z["r_names"]), meta)
+
+
+def cli_options(opts):
+    """Translate the reference CLI options of a set into oracle/library options."""
+    d = dict(refinement=1, convergence=18, prescore=0.4, scorethld=0.5, depth=2,
+             symmetric=0, referenced=0, nodeletions=0)
+    i = 0
+    while i < len(opts):
+        o = opts[i]
+        if o == "--speed=13":
+            d["refinement"], d["convergence"] = 0, 2
+        elif o.startswith("--pre-score="):
+            d["prescore"] = float(o.split("=")[1])
+        elif o == "-s":
+            d["scorethld"] = float(opts[i + 1]); i += 1
+        elif o == "--symmetric":
+            d["symmetric"] = 1
+        elif o == "--referenced":
+            d["referenced"] = 1
+        elif o == "--no-deletions":
+            d["nodeletions"] = 1
+        i += 1
+    return d

@@ -1,0 +1,167 @@
+"""CUDA path against the oracle, through the C ABI (bit for bit).
+
+Every per-pair record (scores, RMSD, counts, coordinates), every transform
+and every alignment row of the library must equal the oracle's exactly:
+both follow the same arithmetic (explicit FMAs, IEEE division/sqrt,
+block-compensated sums in position order, FP64 quaternion solve).
+"""
+import numpy as np
+import pytest
+
+import golden_util as gu
+
+pytestmark = pytest.mark.gpu
+
+
+def _lib_opts(d):
+    from gtalign_alpha_b200.api import Options
+    return Options(refinement=d["refinement"], depth=d.get("depth", 2), convergence=d["convergence"],
+                   prescore=d["prescore"], symmetric=d["symmetric"], referenced=d["referenced"],
+                   nodeletions=d["nodeletions"])
+
+
+def _ora_opts(oracle, d):
+    return oracle.opts_from(refinement=d["refinement"], convergence=d["convergence"],
+                            prescore=d["prescore"], scorethld=d["scorethld"], depth=d.get("depth", 2),
+                            symmetric=d["symmetric"], referenced=d["referenced"],
+                            nodeletions=d["nodeletions"])
+
+
+def assert_same(res, ora, nq, nr):
+    a = res.alndata.view(np.uint32)
+    b = ora.out.view(np.uint32)
+    bad = np.argwhere((a != b).any(axis=2))
+    assert len(bad) == 0, ("records differ", bad[:5], res.alndata[tuple(bad[0])], ora.out[tuple(bad[0])])
+    assert np.array_equal(res.tfm.view(np.uint32), ora.tfm.view(np.uint32))
+    assert np.array_equal(res.numerr.view(np.uint32), ora.err.view(np.uint32))
+    for qi in range(nq):
+        for ri in range(nr):
+            assert res.alignment(qi, ri) == ora.alns[qi][ri], (qi, ri)
+
+
+def run_both(oracle, q, r, d, secstr=False):
+    from gtalign_alpha_b200.api import GTalignB200
+    with GTalignB200(0, 0, _lib_opts(d)) as g:
+        res = g.process_block(q, r, scorethld=d["scorethld"], secstr=secstr)
+    ora = oracle.process_block(q, r, _ora_opts(oracle, d))
+    return res, ora
+
+
+@pytest.mark.parametrize("name", gu.SETS)
+def test_golden_sets_bit_identical(oracle, name):
+    q, r, qn, rn, meta = gu.load(name)
+    d = gu.cli_options(meta["options"])
+    res, ora = run_both(oracle, q, r, d, secstr=True)
+    assert_same(res, ora, q.n, r.n)
+    assert res.qss.tobytes() == ora.qss.tobytes()
+    assert res.rss.tobytes() == ora.rss.tobytes()
+    assert res.launches > 20
+
+
+OPTSETS = {
+    "speed13": dict(refinement=0, convergence=2, prescore=0.0, scorethld=0.0, symmetric=0, referenced=0, nodeletions=0),
+    "default": dict(refinement=1, convergence=18, prescore=0.0, scorethld=0.0, symmetric=0, referenced=0, nodeletions=0),
+    "filters": dict(refinement=1, convergence=18, prescore=0.4, scorethld=0.5, symmetric=0, referenced=0, nodeletions=0),
+    "shallow": dict(refinement=1, convergence=6, prescore=0.3, scorethld=0.3, symmetric=0, referenced=0, nodeletions=0, depth=3),
+    "sym": dict(refinement=1, convergence=4, prescore=0.0, scorethld=0.0, symmetric=1, referenced=1, nodeletions=1),
+}
+
+
+@pytest.mark.parametrize("opt", list(OPTSETS))
+def test_multi_query_ragged_lengths(oracle, opt):
+    """3 queries, references from 3 to 700 residues (including structures too
+    short for any fragment), both homologs and unrelated chains."""
+    from gtalign_alpha_b200 import synth
+    rng = np.random.default_rng(7)
+    wl = synth.config0(seed=31, n_refs=18, qlen=140, lmin=3, lmax=700)
+    wl.queries += synth.random_chains(rng, [60, 25], "qx")
+    q, r = synth.pack(wl.queries), synth.pack(wl.refs)
+    res, ora = run_both(oracle, q, r, OPTSETS[opt])
+    assert_same(res, ora, q.n, r.n)
+
+
+def test_molecule_type_mismatch_is_skipped(oracle):
+    """A protein query and a nucleic-acid reference are not compared
+    (MpStage1.cpp:143-152): the record keeps its initial values."""
+    from gtalign_alpha_b200 import synth
+    wl = synth.config0(seed=32, n_refs=4, qlen=80)
+    q, r = synth.pack(wl.queries), synth.pack(wl.refs)
+    r.mol[1] = 1
+    res, ora = run_both(oracle, q, r, OPTSETS["speed13"])
+    assert_same(res, ora, q.n, r.n)
+    assert res.alndata[0, 1, 9] == 0.0 and res.alndata[0, 1, 8] == np.float32(9999.9)
+
+
+def test_single_pair_and_long_chain(oracle):
+    from gtalign_alpha_b200 import synth
+    rng = np.random.default_rng(9)
+    a = synth.random_chains(rng, [1500], "long")[0]
+    b = synth.homolog(rng, a, 1.5, 0.05, "longhom")
+    q, r = synth.pack([a]), synth.pack([b])
+    res, ora = run_both(oracle, q, r, OPTSETS["speed13"])
+    assert_same(res, ora, 1, 1)
+    assert res.alndata[0, 0, 9] > 0.5
+
+
+def test_resident_blocks_match_process_block(oracle):
+    import ctypes
+    import torch
+    from gtalign_alpha_b200 import synth
+    from gtalign_alpha_b200.api import GTalignB200, Options, pack_fields
+    wl = synth.config0(seed=33, n_refs=10, qlen=100)
+    q, r = synth.pack(wl.queries), synth.pack(wl.refs)
+    with GTalignB200(0, 0, Options(prescore=0.0)) as g:
+        ref = g.process_block(q, r, scorethld=0.0, alignments=False)
+        L = g.lib
+        L.gtb_block_upload.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                       ctypes.POINTER(ctypes.c_void_p)]
+        L.gtb_block_free.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+        L.gtb_process_resident.argtypes = [ctypes.c_void_p, ctypes.c_float, ctypes.c_void_p,
+                                           ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                           ctypes.c_void_p]
+        qb, rb = pack_fields(q), pack_fields(r)
+        hq, hr = ctypes.c_void_p(), ctypes.c_void_p()
+        assert L.gtb_block_upload(g.handle, qb.beg, qb.end, ctypes.byref(hq)) == 0
+        assert L.gtb_block_upload(g.handle, rb.beg, rb.end, ctypes.byref(hr)) == 0
+        d_out = torch.zeros(q.n * r.n * 16, dtype=torch.float32, device="cuda")
+        d_tfm = torch.zeros(q.n * r.n * 12, dtype=torch.float32, device="cuda")
+        for _ in range(2):
+            st = L.gtb_process_resident(g.handle, ctypes.c_float(0.0), hq, hr,
+                                        ctypes.c_void_p(d_out.data_ptr()),
+                                        ctypes.c_void_p(d_tfm.data_ptr()), None)
+            assert st == 0
+            torch.cuda.synchronize()
+            assert np.array_equal(d_out.cpu().numpy().view(np.uint32),
+                                  ref.alndata.ravel().view(np.uint32))
+            assert np.array_equal(d_tfm.cpu().numpy().view(np.uint32), ref.tfm.ravel().view(np.uint32))
+        L.gtb_block_free(g.handle, hq)
+        L.gtb_block_free(g.handle, hr)
+
+
+def test_status_codes():
+    from gtalign_alpha_b200 import synth
+    from gtalign_alpha_b200.api import GTalignB200, GTBError, Options
+    wl = synth.config0(seed=34, n_refs=2, qlen=50)
+    q, r = synth.pack(wl.queries), synth.pack(wl.refs)
+    with GTalignB200(0, 0, Options(nodetailedsearch=0)) as g:
+        with pytest.raises(GTBError) as e:
+            g.process_block(q, r)
+        assert e.value.status == 4
+    with GTalignB200(0, 0, Options(refinement=3)) as g:
+        with pytest.raises(GTBError) as e:
+            g.process_block(q, r)
+        assert e.value.status == 4
+    with GTalignB200(0, 0, Options()) as g:
+        with pytest.raises(GTBError) as e:
+            g.process_block(q, r, scorethld=1.5)
+        assert e.value.status == 1
+        big = synth.SoA(np.array([70000], np.int32), np.array([0], np.int32),
+                        np.zeros(70000, np.float32), np.zeros(70000, np.float32),
+                        np.zeros(70000, np.float32), np.full(70000, 65, np.uint8),
+                        np.zeros(1, np.int32))
+        with pytest.raises(GTBError) as e:
+            g.process_block(big, r)
+        assert e.value.status == 5
+        # the handle stays usable after errors
+        res = g.process_block(q, r, scorethld=0.0)
+        assert res.alndata.shape == (1, 2, 16)

@@ -1,0 +1,138 @@
+"""The oracle against the reference's own outputs (golden fixtures).
+
+The fixtures hold what the reference CPU build printed for seeded synthetic
+sets (tests/golden/make_golden.py).  Low-TM pairs have several near-equal
+local optima, and the reference's own result for them moves when the query
+is merely rotated (`self_agreement` in each fixture).  The bar for the oracle
+is therefore: agree with the reference at least as often as the reference
+agrees with itself (minus a small sampling margin), agree on nearly every
+generated homolog of the query, and agree exactly on everything that follows
+from an identical alignment.
+"""
+import numpy as np
+import pytest
+
+import golden_util as gu
+
+MARGIN = 0.12
+HOMOLOGS = []
+
+
+def rmsd_svd(P, Q):
+    pc, qc = P.mean(0), Q.mean(0)
+    H = (P - pc).T @ (Q - qc)
+    U, S, Vt = np.linalg.svd(H)
+    d = np.sign(np.linalg.det(Vt.T @ U.T))
+    S[2] *= d
+    e = ((P - pc) ** 2).sum() + ((Q - qc) ** 2).sum() - 2 * S.sum()
+    return float(np.sqrt(max(e, 0.0) / len(P)))
+
+
+def pairs_of(row_q, row_r, q0, r0):
+    out, qi, ri = [], q0, r0
+    for a, b in zip(row_q, row_r):
+        if a != "-" and b != "-":
+            out.append((qi, ri))
+        if a != "-":
+            qi += 1
+        if b != "-":
+            ri += 1
+    return out
+
+
+def run_oracle(oracle, name):
+    q, r, qn, rn, meta = gu.load(name)
+    d = gu.cli_options(meta["options"])
+    o = oracle.process_block(q, r, oracle.opts_from(
+        refinement=d["refinement"], convergence=d["convergence"], prescore=d["prescore"],
+        scorethld=d["scorethld"], symmetric=d["symmetric"], referenced=d["referenced"],
+        nodeletions=d["nodeletions"]))
+    return q, r, qn, rn, meta, d, o
+
+
+@pytest.mark.parametrize("name", gu.SETS)
+def test_oracle_matches_reference(oracle, name):
+    q, r, qn, rn, meta, d, o = run_oracle(oracle, name)
+    ref = meta["results"]
+    s = d["scorethld"]
+    ours = set()
+    for qi in range(q.n):
+        for ri in range(r.n):
+            out = o.out[qi, ri]
+            if max(out[9], out[10]) >= s and out[4] >= 1:
+                ours.add(qn[qi] + "|" + rn[ri])
+    theirs = set(ref.keys())
+    union = ours | theirs
+    assert len(ours & theirs) >= (1.0 - MARGIN) * len(union), (len(ours), len(theirs))
+
+    dtm, same, hom_same = [], [], []
+    for key in sorted(ours & theirs):
+        a, b = key.split("|")
+        qi, ri = qn.index(a), rn.index(b)
+        out = o.out[qi, ri]
+        g = ref[key]
+        dd = max(abs(out[9] - g["tmq"]), abs(out[10] - g["tmr"]))
+        rows = o.alns[qi][ri]
+        ident = rows[0] == g["query_aln"] and rows[2] == g["refrn_aln"]
+        dtm.append(dd)
+        same.append(ident)
+        if b.startswith("hom"):      # a generated homolog of the query
+            hom_same.append(ident and dd <= 1e-4)
+        if ident:
+            # everything that follows from the alignment agrees exactly
+            assert rows[3] == g["query_secstr"] and rows[4] == g["refrn_secstr"], key
+            assert int(out[6]) == g["n_identities"] and int(out[7]) == g["n_gaps"], key
+            assert int(out[4]) == g["n_aligned"], key
+            bq, be = int(out[2:3].view(np.uint32)[0]), int(out[3:4].view(np.uint32)[0])
+            assert (bq & 0xffff, bq >> 16) == (g["query_from"], g["refn_from"]), key
+            # with --no-deletions the reference's writer counts displayed residues
+            if not d["nodeletions"]:
+                assert (be & 0xffff, be >> 16) == (g["query_to"], g["refn_to"]), key
+            assert abs(out[11] - g["d0q"]) < 6e-3 and abs(out[12] - g["d0r"]) < 6e-3
+    dtm = np.array(dtm)
+    sa = meta["self_agreement"]
+    assert (dtm <= 1e-4).mean() >= sa["frac_tm_1e4"] - MARGIN, ((dtm <= 1e-4).mean(), sa)
+    assert np.mean(same) >= sa["frac_aln_identical"] - MARGIN, (np.mean(same), sa)
+    if hom_same:
+        assert np.mean(hom_same) >= 0.7, hom_same
+    HOMOLOGS.extend(hom_same)
+
+
+@pytest.mark.parametrize("name", ["c0_speed13", "c0_default"])
+def test_oracle_rmsd_is_exact(oracle, name):
+    """The reported RMSD is the optimal-superposition RMSD of the reported
+    alignment (FP64 SVD recomputation, 1e-3 A)."""
+    q, r, qn, rn, meta, d, o = run_oracle(oracle, name)
+    qxyz = np.stack([q.x, q.y, q.z], 1).astype(np.float64)
+    rxyz = np.stack([r.x, r.y, r.z], 1).astype(np.float64)
+    n = 0
+    for qi in range(q.n):
+        for ri in range(r.n):
+            out = o.out[qi, ri]
+            if out[4] < 3:
+                continue
+            rows = o.alns[qi][ri]
+            b = int(out[2:3].view(np.uint32)[0])
+            pr = pairs_of(rows[0], rows[2], (b & 0xffff) - 1, (b >> 16) - 1)
+            P = qxyz[[q.offs[qi] + a for a, _ in pr]]
+            Q = rxyz[[r.offs[ri] + c for _, c in pr]]
+            assert abs(rmsd_svd(P, Q) - out[8]) < 1e-3
+            n += 1
+    assert n > 10
+
+
+def test_oracle_tm_errors_small(oracle):
+    """|FP32 path - FP64 recomputation| of reported TM-scores is < 1e-5."""
+    q, r, qn, rn, meta, d, o = run_oracle(oracle, "c0_speed13")
+    assert o.err[..., :2].max() < 1e-5
+    assert o.err[..., 2].max() < 1e-3
+
+
+def test_oracle_homologs_overall(oracle):
+    """Across all fixture sets, the generated homologs of the query get the
+    reference's alignment and TM-score (1e-4) in at least 85% of cases."""
+    if len(HOMOLOGS) < 40:
+        for name in gu.SETS:
+            test_oracle_matches_reference(oracle, name)
+    assert len(HOMOLOGS) >= 40
+    assert np.mean(HOMOLOGS) >= 0.85, (np.mean(HOMOLOGS), len(HOMOLOGS))
