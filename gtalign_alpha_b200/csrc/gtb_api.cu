@@ -43,23 +43,6 @@ static const int TBL = 65536;
         }                                                                        \
     } while (0)
 
-// Per-length constants; the FP32 formulas of stagecnsts.cuh:48-175.
-static void make_tables(std::vector<float>& d0, std::vector<float>& d82, std::vector<float>& d0fin) {
-    d0.resize(TBL); d82.resize(TBL); d0fin.resize(TBL);
-    for (int L = 0; L < TBL; L++) {
-        float l = (float)L;
-        float a = 0.168f;
-        if (l > 19.f) a = 1.24f * cbrtf(l - 15.f) - 1.8f;
-        d0[L] = a + 0.8f;
-        float d8 = 1.5f * powf(l, 0.3f) + 3.5f;
-        d82[L] = d8 * d8;
-        float f = 0.5f;
-        if (l > 21.f) f = 1.24f * cbrtf(l - 15.f) - 1.8f;
-        if (f < 0.5f) f = 0.5f;
-        d0fin[L] = f;
-    }
-}
-
 extern "C" gtb_status gtb_create(int device, size_t mem_bytes, const gtb_options* opts,
                                  gtb_handle** out) {
     if (!out || !opts) return GTB_ERR_ARG;
@@ -79,8 +62,8 @@ extern "C" gtb_status gtb_create(int device, size_t mem_bytes, const gtb_options
     h->budget = (mem_bytes == 0 || mem_bytes > avail) ? avail : mem_bytes;
     CK(cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking));
     for (int k = 0; k < 8; k++) CK(cudaEventCreate(&h->ev[k]));
-    std::vector<float> a, b, c;
-    make_tables(a, b, c);
+    std::vector<float> a(TBL), b(TBL), c(TBL);
+    make_tables(a.data(), b.data(), c.data(), TBL);
     CK(cudaMalloc(&h->t_d0, TBL * sizeof(float)));
     CK(cudaMalloc(&h->t_d82, TBL * sizeof(float)));
     CK(cudaMalloc(&h->t_d0fin, TBL * sizeof(float)));
@@ -261,42 +244,8 @@ static gtb_status run_block(gtb_handle* h, const DevBlock& D, float scorethld,
         CK(cudaMemcpyAsync(offs + 3 * (np + 1), off_str.data(), (np + 1) * sizeof(long long), cudaMemcpyHostToDevice, st));
 
         // ------------------------------------------------------------ stages
-        auto dprefine = [&](int gap0, int prescreen, int maxit) {
-            for (int dpi = 0; dpi < maxit; dpi++) {
-                launch_dp(B, T, DP_TFM_IBEST, gap0, gap0 ? 0.0f : -0.6f, 0, 0, 0, st);
-                launch_btck(B, T, 0, st);
-                launch_refine(RM_DP, B, T, st);
-                launch_post(B, T, dpi, maxit, prescreen, o.prescore, st);
-            }
-        };
-        CK(cudaEventRecord(h->ev[0], st));
-        launch_init(B, T, st);
-        launch_findfrag(B, T, st);
-        CK(cudaEventRecord(h->ev[1], st));
-        launch_refine(RM_INIT, B, T, st);
-        CK(cudaEventRecord(h->ev[2], st));
-        dprefine(1, 1, 2);
-        for (int call = 0; call < 2; call++) {
-            int gap0 = call == 1;
-            launch_dp(B, T, DP_TFM_GRAND, gap0, gap0 ? 0.0f : -1.0f, !gap0, !gap0, 1, st);
-            launch_btck(B, T, 0, st);
-            launch_refine(RM_DP, B, T, st);
-            dprefine(0, 0, 2);
-            dprefine(1, 0, call == 0 ? 2 : o.convergence);
-            if (call == 1 && 0.0f < scorethld) launch_lowscore(B, T, scorethld, st);
-        }
-        CK(cudaEventRecord(h->ev[3], st));
-        launch_dp(B, T, DP_TFM_GRAND, 1, 0.0f, 0, 0, 1, st);
-        launch_btck(B, T, 0, st);
-        launch_refine(RM_FIN1, B, T, st);
-        if (!(o.depth == 3 || o.refinement == 0)) launch_refine(RM_FIN2, B, T, st);
-        launch_dp(B, T, DP_TFM_GRAND, 1, 0.0f, 0, 0, 1, st);
-        launch_btck(B, T, 1, st);
-        launch_alnstr(B, T, st);
-        launch_refine(RM_PROD1, B, T, st);
-        launch_refine(RM_PROD2, B, T, st);
-        launch_final(B, T, o.referenced, st);
-        CK(cudaEventRecord(h->ev[4], st));
+        launch_stages(B, T, o.refinement, o.depth, o.convergence, o.prescore, o.referenced,
+                      scorethld, st, h->ev);
         CK(cudaGetLastError());
 
         // ------------------------------------------------------------ results

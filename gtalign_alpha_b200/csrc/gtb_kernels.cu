@@ -874,4 +874,70 @@ void launch_final(const Blk& B, const Bat& T, int referenced, cudaStream_t st) {
     GTB_LAUNCHED(T);
 }
 
+// ---------------------------------------------------------------------------
+// Per-length constants; the FP32 formulas of stagecnsts.cuh:48-175 (host).
+void make_tables(float* d0, float* d82, float* d0fin, int n) {
+    for (int L = 0; L < n; L++) {
+        float l = (float)L;
+        float a = 0.168f;
+        if (l > 19.f) a = 1.24f * cbrtf(l - 15.f) - 1.8f;
+        d0[L] = a + 0.8f;
+        float d8 = 1.5f * powf(l, 0.3f) + 3.5f;
+        d82[L] = d8 * d8;
+        float f = 0.5f;
+        if (l > 21.f) f = 1.24f * cbrtf(l - 15.f) - 1.8f;
+        if (f < 0.5f) f = 0.5f;
+        d0fin[L] = f;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// The stage sequence of one batch: CuBatch::ProcessBlock (CuBatch.cu:537-700)
+// with the detailed search off.  ev (may be null): 5 events recorded at the
+// stage boundaries.
+void launch_stages(const Blk& B, const Bat& T, int refinement, int depth, int convergence,
+                   float prescore, int referenced, float scorethld, cudaStream_t st,
+                   cudaEvent_t* ev) {
+    auto mark = [&](int k) { if (ev) cudaEventRecord(ev[k], st); };
+    // DPRefine: MpStage1.cpp:466-517
+    auto dprefine = [&](int gap0, int prescreen, int maxit) {
+        for (int dpi = 0; dpi < maxit; dpi++) {
+            launch_dp(B, T, DP_TFM_IBEST, gap0, gap0 ? 0.0f : -0.6f, 0, 0, 0, st);
+            launch_btck(B, T, 0, st);
+            launch_refine(RM_DP, B, T, st);
+            launch_post(B, T, dpi, maxit, prescreen, prescore, st);
+        }
+    };
+    mark(0);
+    launch_init(B, T, st);
+    launch_findfrag(B, T, st);
+    mark(1);
+    launch_refine(RM_INIT, B, T, st);
+    mark(2);
+    dprefine(1, 1, 2);
+    // two stage-2 passes: MpStage2.h:63-83, CuBatch.cu:627-650
+    for (int call = 0; call < 2; call++) {
+        int gap0 = call == 1;
+        launch_dp(B, T, DP_TFM_GRAND, gap0, gap0 ? 0.0f : -1.0f, !gap0, !gap0, 1, st);
+        launch_btck(B, T, 0, st);
+        launch_refine(RM_DP, B, T, st);
+        dprefine(0, 0, 2);
+        dprefine(1, 0, call == 0 ? 2 : convergence);
+        if (call == 1 && 0.0f < scorethld) launch_lowscore(B, T, scorethld, st);
+    }
+    mark(3);
+    // final stage: MpStageFin.h:63-96
+    launch_dp(B, T, DP_TFM_GRAND, 1, 0.0f, 0, 0, 1, st);
+    launch_btck(B, T, 0, st);
+    launch_refine(RM_FIN1, B, T, st);
+    if (!(depth == 3 || refinement == 0)) launch_refine(RM_FIN2, B, T, st);
+    launch_dp(B, T, DP_TFM_GRAND, 1, 0.0f, 0, 0, 1, st);
+    launch_btck(B, T, 1, st);
+    launch_alnstr(B, T, st);
+    launch_refine(RM_PROD1, B, T, st);
+    launch_refine(RM_PROD2, B, T, st);
+    launch_final(B, T, referenced, st);
+    mark(4);
+}
+
 }  // namespace gtb
