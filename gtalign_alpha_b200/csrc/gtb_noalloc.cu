@@ -1,0 +1,225 @@
+// gtb_noalloc.cu -- the search over caller-owned device buffers, with all
+// working memory in a fixed static device array.
+//
+// Why: some callers cannot allocate device memory at the moment they want to
+// align structures -- e.g. code running inside another framework's memory
+// pool that forbids outside cudaMalloc/cudaFree, a process whose allocator is
+// locked while a CUDA graph is being built elsewhere, or a service that must
+// keep its device footprint fixed after start-up.  They own their inputs and
+// outputs; this entry point needs nothing else from the allocator.
+//
+// Limits and behaviour:
+//  * working memory (pair state, DP traceback words and row buffers, aligned
+//    pair lists, per-pair offsets) comes from g_noalloc_scratch below,
+//    GTB_NOALLOC_SCRATCH_BYTES = 16 MiB.  Every GPU that loads this library
+//    holds that array (and 768 KiB of constant tables) until the process exits.
+//    A block whose working memory does not fit, or that has more than
+//    GTB_NOALLOC_MAX_PAIRS pairs, is rejected with GTB_ERR_NOMEM and a message
+//    before anything runs;
+//  * the first call on a device does a one-time set-up on that device (looks
+//    up the device addresses of the static arrays and fills the constant
+//    tables, with that device current); make that first call before any
+//    stream capture;
+//  * every call uses the same scratch array and leaves its contents behind.
+//    Nothing in it has to start at zero: the pair state is initialised by
+//    the first kernel of each call and every other region is written before
+//    it is read.  Calls that overlap on the GPU (on different streams, or
+//    from different host threads at once) race on the scratch array and must
+//    not be issued; calls in order on one stream are fine;
+//  * nothing here calls cudaMalloc, cudaFree or any allocating routine.
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <cuda_runtime.h>
+
+#include "gtb200.h"
+#include "gtb_kernels.cuh"
+
+using namespace gtb;
+
+namespace {
+
+constexpr size_t SCRATCH_BYTES = (size_t)16 << 20;
+constexpr int TBLN = 65536;
+constexpr int MAXDEV = 64;
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[SCRATCH_BYTES];
+static __device__ __align__(256) float g_noalloc_d0[TBLN];
+static __device__ __align__(256) float g_noalloc_d82[TBLN];
+static __device__ __align__(256) float g_noalloc_d0fin[TBLN];
+
+struct DevState {
+    bool ready = false;
+    unsigned char* scratch = nullptr;
+    float *d0 = nullptr, *d82 = nullptr, *d0fin = nullptr;
+};
+static DevState g_dev[MAXDEV];
+static std::mutex g_setup_mutex;
+static float h_tbl[3][TBLN];
+// host copies of the per-pair offsets (4 arrays of up to MAX_PAIRS+1 entries)
+static long long h_offs[4 * (GTB_NOALLOC_MAX_PAIRS + 1)];
+
+size_t al256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+void setmsg(char* buf, size_t len, const char* fmt, long long a, long long b) {
+    if (buf && len) snprintf(buf, len, fmt, a, b);
+}
+
+// One-time set-up on the current device: device addresses of the static
+// arrays (the host-side names are only stand-ins) and the constant tables.
+cudaError_t setup(int dev, cudaStream_t st) {
+    std::lock_guard<std::mutex> lk(g_setup_mutex);
+    DevState& D = g_dev[dev];
+    if (D.ready) return cudaSuccess;
+    cudaError_t e;
+    if ((e = cudaGetSymbolAddress((void**)&D.scratch, g_noalloc_scratch)) != cudaSuccess) return e;
+    if ((e = cudaGetSymbolAddress((void**)&D.d0, g_noalloc_d0)) != cudaSuccess) return e;
+    if ((e = cudaGetSymbolAddress((void**)&D.d82, g_noalloc_d82)) != cudaSuccess) return e;
+    if ((e = cudaGetSymbolAddress((void**)&D.d0fin, g_noalloc_d0fin)) != cudaSuccess) return e;
+    make_tables(h_tbl[0], h_tbl[1], h_tbl[2], TBLN);
+    if ((e = cudaMemcpyAsync(D.d0, h_tbl[0], sizeof(h_tbl[0]), cudaMemcpyHostToDevice, st)) != cudaSuccess) return e;
+    if ((e = cudaMemcpyAsync(D.d82, h_tbl[1], sizeof(h_tbl[1]), cudaMemcpyHostToDevice, st)) != cudaSuccess) return e;
+    if ((e = cudaMemcpyAsync(D.d0fin, h_tbl[2], sizeof(h_tbl[2]), cudaMemcpyHostToDevice, st)) != cudaSuccess) return e;
+    if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return e;
+    D.ready = true;
+    return cudaSuccess;
+}
+
+}  // namespace
+
+extern "C" gtb_status gtb_process_block_noalloc(int device, const gtb_options* opts, float scorethld,
+                                                const gtb_dev_soa* q, const gtb_dev_soa* r,
+                                                float* d_alndata, float* d_tfm, float* d_numerr,
+                                                void* stream, char* errbuf, size_t errlen) {
+    if (errbuf && errlen) errbuf[0] = 0;
+    if (!opts || !q || !r || !d_alndata || !d_tfm || device < 0 || device >= MAXDEV) {
+        setmsg(errbuf, errlen, "null argument or device out of range (%lld, %lld)", device, MAXDEV);
+        return GTB_ERR_ARG;
+    }
+    if (!opts->nodetailedsearch || opts->addsearchbyss || opts->twotmscore ||
+        opts->refinement < 0 || opts->refinement > 1) {
+        setmsg(errbuf, errlen, "option combination not implemented (refinement %lld, detailed %lld)",
+               opts->refinement, !opts->nodetailedsearch);
+        return GTB_ERR_UNSUPPORTED;
+    }
+    if (!(scorethld >= 0.f && scorethld < 1.f) || opts->depth < 0 || opts->depth > 3 ||
+        opts->convergence < 1 || opts->convergence > 30 || !(opts->prescore >= 0.f && opts->prescore < 1.f)) {
+        setmsg(errbuf, errlen, "option out of range (%lld %lld)", 0, 0);
+        return GTB_ERR_ARG;
+    }
+    if (q->n < 1 || r->n < 1 || !q->lens || !r->lens || !q->d_lens || !r->d_lens || !q->d_offs ||
+        !r->d_offs || !q->d_mol || !r->d_mol || !q->d_x || !q->d_y || !q->d_z || !r->d_x ||
+        !r->d_y || !r->d_z || !q->d_rsd || !r->d_rsd || !q->d_ss || !r->d_ss) {
+        setmsg(errbuf, errlen, "empty block or null field (%lld x %lld)", q->n, r->n);
+        return GTB_ERR_ARG;
+    }
+    long long npairs = (long long)q->n * r->n;
+    if (npairs > GTB_NOALLOC_MAX_PAIRS) {
+        setmsg(errbuf, errlen, "block has %lld pairs; the allocation-free entry point takes at most %lld",
+               npairs, GTB_NOALLOC_MAX_PAIRS);
+        return GTB_ERR_NOMEM;
+    }
+    int qmax = 0, qmin = 1 << 30, rmax = 0, rmin = 1 << 30;
+    for (int i = 0; i < q->n; i++) {
+        int L = q->lens[i];
+        if (L < 1 || L > 65535) { setmsg(errbuf, errlen, "query %lld has length %lld", i, L); return L > 65535 ? GTB_ERR_TOO_LONG : GTB_ERR_ARG; }
+        qmax = L > qmax ? L : qmax; qmin = L < qmin ? L : qmin;
+    }
+    for (int i = 0; i < r->n; i++) {
+        int L = r->lens[i];
+        if (L < 1 || L > 65535) { setmsg(errbuf, errlen, "reference %lld has length %lld", i, L); return L > 65535 ? GTB_ERR_TOO_LONG : GTB_ERR_ARG; }
+        rmax = L > rmax ? L : rmax; rmin = L < rmin ? L : rmin;
+    }
+    // plan the scratch: pair state, offsets, traceback, DP rows, aligned pairs
+    int np = (int)npairs;
+    long long* obt = h_offs;
+    long long* orow = h_offs + (np + 1);
+    long long* oaln = h_offs + 2 * (np + 1);
+    long long* ostr = h_offs + 3 * (np + 1);
+    obt[0] = orow[0] = oaln[0] = ostr[0] = 0;
+    for (int i = 0; i < np; i++) {
+        int lq = q->lens[i / r->n], lr = r->lens[i % r->n];
+        obt[i + 1] = obt[i] + (long long)((lq + 31) / 32) * (lr + 31);
+        orow[i + 1] = orow[i] + lr;
+        oaln[i + 1] = oaln[i] + (lq < lr ? lq : lr);
+        ostr[i + 1] = 0;
+    }
+    size_t sz = 0;
+    auto carve = [&](size_t bytes) { size_t o = sz; sz += al256(bytes); return o; };
+    size_t o_ints = carve((size_t)np * 8 * sizeof(int));
+    size_t o_flts = carve((size_t)np * 4 * sizeof(float));
+    size_t o_tib = carve((size_t)np * 12 * sizeof(float));
+    size_t o_tgr = carve((size_t)np * 12 * sizeof(float));
+    size_t o_out = carve((size_t)np * 16 * sizeof(float));
+    size_t o_err = carve((size_t)np * 4 * sizeof(float));
+    size_t o_offs = carve((size_t)(np + 1) * 4 * sizeof(long long));
+    size_t o_bt = carve((size_t)obt[np] * sizeof(uint2));
+    size_t o_row = carve((size_t)orow[np] * sizeof(float));
+    size_t o_aln = carve((size_t)oaln[np] * sizeof(unsigned));
+    if (sz > SCRATCH_BYTES) {
+        setmsg(errbuf, errlen, "block needs %lld bytes of working memory; the static scratch holds %lld",
+               (long long)sz, (long long)SCRATCH_BYTES);
+        return GTB_ERR_NOMEM;
+    }
+
+    cudaStream_t st = (cudaStream_t)stream;
+    cudaError_t e = cudaSetDevice(device);
+    if (e == cudaSuccess) e = setup(device, st);
+    if (e != cudaSuccess) {
+        if (errbuf && errlen) snprintf(errbuf, errlen, "set-up: %s", cudaGetErrorString(e));
+        return GTB_ERR_CUDA;
+    }
+    const DevState& D = g_dev[device];
+    unsigned char* base = D.scratch;
+
+    Blk B{};
+    B.nq = q->n; B.nr = r->n;
+    B.qlen = q->d_lens; B.rlen = r->d_lens; B.qoff = q->d_offs; B.roff = r->d_offs;
+    B.qx = q->d_x; B.qy = q->d_y; B.qz = q->d_z; B.rx = r->d_x; B.ry = r->d_y; B.rz = r->d_z;
+    B.qa = q->d_rsd; B.ra = r->d_rsd; B.qs = q->d_ss; B.rs = r->d_ss;
+    B.qmol = q->d_mol; B.rmol = r->d_mol;
+    B.qmax = qmax; B.qmin = qmin; B.rmax = rmax; B.rmin = rmin;
+    B.t_d0 = D.d0; B.t_d82 = D.d82; B.t_d0fin = D.d0fin;
+    B.stepinit = (opts->depth == 3) ? 5 : 1;
+    B.refinement = opts->refinement; B.depth = opts->depth;
+    B.symmetric = opts->symmetric; B.nodeletions = opts->nodeletions;
+
+    Bat T{};
+    T.p0 = 0; T.np = np;
+    int* ints = (int*)(base + o_ints);
+    T.flags = ints; T.seedq = ints + np; T.seedr = ints + 2 * np; T.naln = ints + 3 * np;
+    T.sfndx = ints + 4 * np; T.sfpos = ints + 5 * np; T.sfndx_cur = ints + 6 * np; T.sfpos_cur = ints + 7 * np;
+    float* fl = (float*)(base + o_flts);
+    T.grand = fl; T.best = fl + np; T.best0 = fl + 2 * np; T.rmsd32 = fl + 3 * np;
+    T.tfm_ib = (float*)(base + o_tib); T.tfm_gr = (float*)(base + o_tgr);
+    T.out = (float*)(base + o_out); T.err = (float*)(base + o_err);
+    long long* offs = (long long*)(base + o_offs);
+    T.off_bt = offs; T.off_row = offs + (np + 1); T.off_aln = offs + 2 * (np + 1); T.off_str = offs + 3 * (np + 1);
+    T.bt = (uint2*)(base + o_bt); T.row = (float*)(base + o_row);
+    T.aln = (unsigned*)(base + o_aln); T.str = nullptr;
+    T.launches = nullptr;
+
+    // the host offsets are copied from the static host array (no allocation)
+    e = cudaMemcpyAsync(offs, h_offs, (size_t)(np + 1) * 4 * sizeof(long long), cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) {
+        long long nl = 0;
+        launch_secstr(q->d_ss, q->d_x, q->d_y, q->d_z, q->d_lens, q->d_offs, q->d_mol, q->n, st, &nl);
+        launch_secstr(r->d_ss, r->d_x, r->d_y, r->d_z, r->d_lens, r->d_offs, r->d_mol, r->n, st, &nl);
+        launch_stages(B, T, opts->refinement, opts->depth, opts->convergence, opts->prescore,
+                      opts->referenced, scorethld, st, nullptr);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(d_alndata, T.out, (size_t)np * 16 * sizeof(float), cudaMemcpyDeviceToDevice, st);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(d_tfm, T.tfm_gr, (size_t)np * 12 * sizeof(float), cudaMemcpyDeviceToDevice, st);
+    if (e == cudaSuccess && d_numerr)
+        e = cudaMemcpyAsync(d_numerr, T.err, (size_t)np * 4 * sizeof(float), cudaMemcpyDeviceToDevice, st);
+    // the host offsets array is reused by the next call: wait for its copy
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) {
+        if (errbuf && errlen) snprintf(errbuf, errlen, "%s", cudaGetErrorString(e));
+        return GTB_ERR_CUDA;
+    }
+    return GTB_OK;
+}

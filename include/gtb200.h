@@ -159,6 +159,42 @@ gtb_status gtb_polish(gtb_handle* h, int npairs, const long long* off,
                       float* tfm, const float* d0, int steps,
                       float* tm_before, float* tm_after, void* stream);
 
+/* ---------------------------------------------------------------------------
+ * Allocation-free search (no counterpart in the reference).
+ *
+ * For callers that must not allocate device memory while they align
+ * structures -- code living inside another framework's memory pool, a
+ * process whose device footprint must stay fixed after start-up, or code
+ * running while an allocator is locked.  Inputs and outputs are the
+ * caller's own device buffers; all working memory comes from one static
+ * device array of GTB_NOALLOC_SCRATCH_BYTES (16 MiB) that every GPU loading
+ * this library keeps until the process exits.  The call uses no handle and
+ * calls no cudaMalloc/cudaFree.  Blocks whose working memory would exceed the
+ * array, or with more than GTB_NOALLOC_MAX_PAIRS pairs, are rejected with
+ * GTB_ERR_NOMEM and a message in errbuf.  The first call on a device performs
+ * a one-time set-up there (device addresses of the static arrays, constant
+ * tables): make it before any stream capture.  All calls share the scratch
+ * array, so calls that overlap on the GPU race; issue them one after another.
+ * Results are those of gtb_process_block (records and transforms only). */
+#define GTB_NOALLOC_SCRATCH_BYTES ((size_t)16 << 20)
+#define GTB_NOALLOC_MAX_PAIRS 4096
+
+typedef struct {
+    int n;                     /* number of structures */
+    const int* lens;           /* HOST copy of the n lengths (working-memory plan) */
+    const int* d_lens;         /* device: lengths */
+    const int* d_offs;         /* device: offset of each structure's first residue */
+    const int* d_mol;          /* device: molecule type (0 protein, 1 nucleic acid) */
+    const float *d_x, *d_y, *d_z;
+    const unsigned char* d_rsd;  /* device: residue letters */
+    char* d_ss;                /* device output: secondary structure per residue */
+} gtb_dev_soa;
+
+gtb_status gtb_process_block_noalloc(int device, const gtb_options* opts, float scorethld,
+                                     const gtb_dev_soa* queries, const gtb_dev_soa* refs,
+                                     float* d_alndata, float* d_tfm, float* d_numerr,
+                                     void* stream, char* errbuf, size_t errlen);
+
 /* Message of the last error on this handle (static storage of the handle). */
 const char* gtb_last_error(const gtb_handle* h);
 
