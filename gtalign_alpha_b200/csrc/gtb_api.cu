@@ -61,6 +61,13 @@ extern "C" gtb_status gtb_create(int device, size_t mem_bytes, const gtb_options
     size_t avail = fr > ((size_t)256 << 20) ? fr - ((size_t)256 << 20) : fr / 2;
     h->budget = (mem_bytes == 0 || mem_bytes > avail) ? avail : mem_bytes;
     CK(cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking));
+    // keep freed batch memory in the device pool between calls instead of
+    // unmapping it at every synchronisation (each block reuses similar sizes)
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+        unsigned long long keep = ~0ull;
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    }
     for (int k = 0; k < 8; k++) CK(cudaEventCreate(&h->ev[k]));
     std::vector<float> a(TBL), b(TBL), c(TBL);
     make_tables(a.data(), b.data(), c.data(), TBL);

@@ -132,15 +132,21 @@ struct PairGeom {
     }
 };
 
+// Every pass below walks its range in blocks of BLK positions (folded into
+// the compensated totals after each block); the block boundaries count from
+// the start of the range, as in the oracle.
 __device__ void cov_range(const PairGeom& G, int k0, int k1, float* v) {
     CovAcc a;
     a.init();
-    int blk = 0;
-    for (int k = k0; k < k1; k++) {
-        float qx, qy, qz, rx, ry, rz;
-        G.at(k, qx, qy, qz, rx, ry, rz);
-        a.add(qx, qy, qz, rx, ry, rz);
-        if (++blk == BLK) { a.fold(); blk = 0; }
+    for (int b0 = k0; b0 < k1; b0 += BLK) {
+        int b1 = b0 + BLK < k1 ? b0 + BLK : k1;
+#pragma unroll 4
+        for (int k = b0; k < b1; k++) {
+            float qx, qy, qz, rx, ry, rz;
+            G.at(k, qx, qy, qz, rx, ry, rz);
+            a.add(qx, qy, qz, rx, ry, rz);
+        }
+        a.fold();
     }
     a.final(v);
 }
@@ -148,69 +154,90 @@ __device__ void cov_range(const PairGeom& G, int k0, int k1, float* v) {
 __device__ void cov_ext(const PairGeom& G, const float* tfm, float thr, float* v) {
     CovAcc a;
     a.init();
-    int blk = 0;
-    for (int k = 0; k < G.n; k++) {
-        float qx, qy, qz, rx, ry, rz;
-        G.at(k, qx, qy, qz, rx, ry, rz);
-        float d = dist2_tf(tfm, qx, qy, qz, rx, ry, rz);
-        if (d <= thr) a.add(qx, qy, qz, rx, ry, rz);
-        if (++blk == BLK) { a.fold(); blk = 0; }
+    for (int b0 = 0; b0 < G.n; b0 += BLK) {
+        int b1 = b0 + BLK < G.n ? b0 + BLK : G.n;
+#pragma unroll 4
+        for (int k = b0; k < b1; k++) {
+            float qx, qy, qz, rx, ry, rz;
+            G.at(k, qx, qy, qz, rx, ry, rz);
+            float d = dist2_tf(tfm, qx, qy, qz, rx, ry, rz);
+            if (d <= thr) a.add(qx, qy, qz, rx, ry, rz);
+        }
+        a.fold();
     }
     a.final(v);
 }
 
-// score pass; m3mode 0 none, 1 distinct three smallest, 2 multiset
+// three smallest distances; m3mode 0 none, 1 distinct values, 2 multiset
+__device__ __forceinline__ void track3(int m3mode, float d, float& m1, float& m2, float& m3) {
+    if (m3mode == 2) {
+        if (d < m1) { m3 = m2; m2 = m1; m1 = d; }
+        else if (d < m2) { m3 = m2; m2 = d; }
+        else if (d < m3) m3 = d;
+    } else if (m3mode == 1) {
+        if (d < m1) { m3 = m2; m2 = m1; m1 = d; }
+        else if (d > m1 && d < m2) { m3 = m2; m2 = d; }
+        else if (d > m2 && d < m3) m3 = d;
+    }
+}
+
+// score pass under tfm (chk: only distances within d82 count)
 __device__ float score_pass(const PairGeom& G, const float* tfm, float d02, int chk, float d82,
                             int m3mode, float& m3out) {
     float ss = 0.f, sc = 0.f, sb = 0.f;
-    int blk = 0;
     float m1 = LARGEDST, m2 = LARGEDST, m3 = LARGEDST;
-    for (int k = 0; k < G.n; k++) {
-        float qx, qy, qz, rx, ry, rz;
-        G.at(k, qx, qy, qz, rx, ry, rz);
-        float d = dist2_tf(tfm, qx, qy, qz, rx, ry, rz);
-        if (!chk || d <= d82) sb = __fadd_rn(sb, tmterm(d02, d));
-        if (m3mode == 2) {
-            if (d < m1) { m3 = m2; m2 = m1; m1 = d; }
-            else if (d < m2) { m3 = m2; m2 = d; }
-            else if (d < m3) m3 = d;
-        } else if (m3mode == 1) {
-            if (d < m1) { m3 = m2; m2 = m1; m1 = d; }
-            else if (d > m1 && d < m2) { m3 = m2; m2 = d; }
-            else if (d > m2 && d < m3) m3 = d;
+    for (int b0 = 0; b0 < G.n; b0 += BLK) {
+        int b1 = b0 + BLK < G.n ? b0 + BLK : G.n;
+#pragma unroll 4
+        for (int k = b0; k < b1; k++) {
+            float qx, qy, qz, rx, ry, rz;
+            G.at(k, qx, qy, qz, rx, ry, rz);
+            float d = dist2_tf(tfm, qx, qy, qz, rx, ry, rz);
+            if (!chk || d <= d82) sb = __fadd_rn(sb, tmterm(d02, d));
+            track3(m3mode, d, m1, m2, m3);
         }
-        if (++blk == BLK) { nfold(ss, sc, sb); blk = 0; }
+        nfold(ss, sc, sb);
     }
     nfold(ss, sc, sb);
     m3out = m3;
     return __fadd_rn(ss, sc);
 }
 
-// fused: score under tfm (chk) and the covariance of positions within thr
+// fused: score under tfm (chk, m3 tracking) and the covariance of the
+// positions with d <= thr (the next pass's threshold when it is known, or
+// its most likely value when it is not)
 __device__ float score_and_ext(const PairGeom& G, const float* tfm, float d02, int chk, float d82,
-                               float thr, float* v) {
+                               float thr, float* v, int m3mode, float& m3out) {
     float ss = 0.f, sc = 0.f, sb = 0.f;
+    float m1 = LARGEDST, m2 = LARGEDST, m3 = LARGEDST;
     CovAcc a;
     a.init();
-    int blk = 0;
-    for (int k = 0; k < G.n; k++) {
-        float qx, qy, qz, rx, ry, rz;
-        G.at(k, qx, qy, qz, rx, ry, rz);
-        float d = dist2_tf(tfm, qx, qy, qz, rx, ry, rz);
-        if (!chk || d <= d82) sb = __fadd_rn(sb, tmterm(d02, d));
-        if (d <= thr) a.add(qx, qy, qz, rx, ry, rz);
-        if (++blk == BLK) { nfold(ss, sc, sb); a.fold(); blk = 0; }
+    for (int b0 = 0; b0 < G.n; b0 += BLK) {
+        int b1 = b0 + BLK < G.n ? b0 + BLK : G.n;
+#pragma unroll 2
+        for (int k = b0; k < b1; k++) {
+            float qx, qy, qz, rx, ry, rz;
+            G.at(k, qx, qy, qz, rx, ry, rz);
+            float d = dist2_tf(tfm, qx, qy, qz, rx, ry, rz);
+            if (!chk || d <= d82) sb = __fadd_rn(sb, tmterm(d02, d));
+            track3(m3mode, d, m1, m2, m3);
+            if (d <= thr) a.add(qx, qy, qz, rx, ry, rz);
+        }
+        nfold(ss, sc, sb);
+        a.fold();
     }
     nfold(ss, sc, sb);
     a.final(v);
+    m3out = m3;
     return __fadd_rn(ss, sc);
 }
 
-__device__ __forceinline__ int converged16(const float* a, const float* b) {
+// every one of the 16 sums changed by less than RM_CONVEPS relative (b strided)
+__device__ __forceinline__ int converged16(const float* a, const float* b, int bstr) {
     int cnt = 0;
 #pragma unroll
     for (int f = 0; f < 16; f++) {
-        float x = a[f], y = b[f];
+        float x = a[f], y = b[f * bstr];
         float m = fabsf(x) < fabsf(y) ? fabsf(x) : fabsf(y);
         if (fabsf(__fsub_rn(x, y)) < __fmul_rn(m, RM_CONVEPS)) cnt++;
     }
@@ -225,15 +252,20 @@ __device__ float findfrag_variant(const PairGeom& G, float d02, float d0s, int s
     cov_range(G, 0, G.n, v);
     for (int it = 0; it < 3; it++) {
         solve_sums(v, swap, tfm);
-        int save = (it < 2);
-        float sc = score_pass(G, tfm, d02, 0, 0.f, save ? 1 : 0, m3);
-        if (best < sc) best = sc;
-        if (!save) break;
+        if (it == 2) {
+            float sc = score_pass(G, tfm, d02, 0, 0.f, 0, m3);
+            if (best < sc) best = sc;
+            break;
+        }
         float d02s = __fadd_rn(d02s0, (it == 1 ? 1.0f : 0.0f));
+        // the next threshold is d02s unless the third-smallest distance is
+        // above it: accumulate for d02s while scoring, redo in the rare case
+        float sc = score_and_ext(G, tfm, d02, 0, 0.f, d02s, v, 1, m3);
+        if (best < sc) best = sc;
         float dst32;
         if (LARGEDST_CMP < m3 || m3 < d02s || G.n <= 3) dst32 = d02s;
         else dst32 = __fadd_rn(d02s, __fmul_rn(ceilf(__fmul_rn(__fsub_rn(m3, d02s), 2.0f)), 0.5f));
-        cov_ext(G, tfm, dst32, v);
+        if (dst32 != d02s) cov_ext(G, tfm, dst32, v);
         if (v[15] < 1.0f) break;
         if ((int)v[15] == G.n) break;
     }
@@ -319,11 +351,13 @@ void launch_findfrag(const Blk& B, const Bat& T, cudaStream_t st) {
 
 // ---------------------------------------------------------------------------
 // the refinement loop: MpStage1.cpp:640-700 and its copies in
-// RefineFragDPKernel and MpStageFin.cpp (one thread = one variant)
+// RefineFragDPKernel and MpStageFin.cpp (one thread = one variant).
+// last/tb are this thread's slots in shared memory (stride `str`): the
+// previous iteration's sums (convergence test) and the best transform.
 __device__ void refine_loop(const PairGeom& G, int kf, int fraglen, float d0, float d02,
                             int chk, float d82, float best_init, int swap,
-                            float& bestout, float* tb) {
-    float v[16], last[16], tfm[12], m3;
+                            float& bestout, float* last, float* tb, int str) {
+    float v[16], tfm[12], m3;
     float best = best_init;
     float d0s = d0s_of(d0);
     float d0sp = __fadd_rn(d0s, 1.0f);
@@ -333,12 +367,14 @@ __device__ void refine_loop(const PairGeom& G, int kf, int fraglen, float d0, fl
     // iteration 0
     if (v[15] < 1.0f) { bestout = best; return; }
 #pragma unroll
-    for (int f = 0; f < 16; f++) last[f] = v[f];
+    for (int f = 0; f < 16; f++) last[f * str] = v[f];
     solve_sums(v, swap, tfm);
     {
-        float sc = score_pass(G, tfm, d02, chk, d82, 2, m3);
         float d0sm = __fsub_rn(d0s, 1.0f);
         float d02s = __fmul_rn(d0sm, d0sm);
+        // iteration 1's threshold is d02s unless the third-smallest distance
+        // is above it: accumulate for d02s while scoring, redo otherwise
+        float sc = score_and_ext(G, tfm, d02, chk, d82, d02s, v, 2, m3);
         if (LARGEDST_CMP < m3 || m3 < d02s || G.n <= 3) dst32 = d02s;
         else {
             float t = __fadd_rn(d0sm, __fmul_rn(ceilf(__fmul_rn(__fsub_rn(__fsqrt_rn(m3), d0sm), 2.0f)), 0.5f));
@@ -347,37 +383,122 @@ __device__ void refine_loop(const PairGeom& G, int kf, int fraglen, float d0, fl
         if (best < sc) {
             best = sc;
 #pragma unroll
-            for (int f = 0; f < 12; f++) tb[f] = tfm[f];
+            for (int f = 0; f < 12; f++) tb[f * str] = tfm[f];
         }
+        // iteration 1: threshold from iteration 0's three smallest distances
+        if (dst32 != d02s) cov_ext(G, tfm, dst32, v);
     }
-    // iteration 1: threshold from iteration 0's three smallest distances
-    cov_ext(G, tfm, dst32, v);
     for (int cit = 1; cit < NMAXCONVIT + 2; cit++) {
-        if (converged16(v, last)) break;
+        if (converged16(v, last, str)) break;
         if (v[15] < 1.0f) break;
 #pragma unroll
-        for (int f = 0; f < 16; f++) last[f] = v[f];
+        for (int f = 0; f < 16; f++) last[f * str] = v[f];
         solve_sums(v, swap, tfm);
         // scoring pass of this iteration fused with the covariance of the next
-        float sc = score_and_ext(G, tfm, d02, chk, d82, thr2, v);
+        float sc = score_and_ext(G, tfm, d02, chk, d82, thr2, v, 0, m3);
         if (best < sc) {
             best = sc;
 #pragma unroll
-            for (int f = 0; f < 12; f++) tb[f] = tfm[f];
+            for (int f = 0; f < 12; f++) tb[f * str] = tfm[f];
         }
     }
     bestout = best;
 }
 
+// Variant list of one pair, enumerated compactly (admissible variants only).
+// Modes with 6 fragment lengths x step 40: variant si = fct*6 + ndx is
+// admissible when frag_length(n, ndx) >= 1 and 40*fct + fraglen < n + 40
+// (MpStage1.cpp:635-641); phase-2 modes: si in [0, nf) with 0 <= pos and
+// pos + fraglen <= n (MpStageFin.cpp:380-396).
+struct VariantList {
+    int total;
+    int cnt[FRAG_NSUB], fl[FRAG_NSUB];
+    int lo, base, ndx2, fl2;  // phase 2
+};
+
+__device__ __forceinline__ void variants_init(VariantList& V, bool phase2, int n, int maxalnmax,
+                                              int sfndx0, int sfpos0) {
+    V.total = 0;
+    V.lo = V.base = V.ndx2 = V.fl2 = 0;
+#pragma unroll
+    for (int d = 0; d < FRAG_NSUB; d++) { V.cnt[d] = 0; V.fl[d] = 0; }
+    if (n <= 0) return;
+    if (phase2) {
+        int nf = 2 * maxalnmax < FIN_MAXNPOS ? 2 * maxalnmax : FIN_MAXNPOS;
+        V.ndx2 = sfndx0 == 0 ? 1 : sfndx0;
+        V.fl2 = frag_length(n, V.ndx2);
+        V.base = sfpos0 - (nf >> 1);            // pos = base + si
+        if (V.fl2 < 1) return;
+        int lo = -V.base > 0 ? -V.base : 0;     // pos >= 0
+        int hi = n - V.fl2 - V.base;            // pos + fl <= n
+        if (hi > nf - 1) hi = nf - 1;
+        V.lo = lo;
+        V.total = hi >= lo ? hi - lo + 1 : 0;
+    } else {
+        int NF = (int)ceilf((float)(maxalnmax + FRAG_STEP - MINFRAGLEN) / FRAG_STEP);
+#pragma unroll
+        for (int d = 0; d < FRAG_NSUB; d++) {
+            int fl = frag_length(n, d);
+            int c = 0;
+            if (fl >= 1) {
+                c = (n + FRAG_STEP - fl + FRAG_STEP - 1) / FRAG_STEP;
+                if (c > NF) c = NF;
+                if (c < 0) c = 0;
+            }
+            V.fl[d] = fl;
+            V.cnt[d] = c;
+            V.total += c;
+        }
+    }
+}
+
+// k-th admissible variant (0 <= k < total) -> (si, length index, position,
+// length, first position of the refined fragment)
+__device__ __forceinline__ void variants_get(const VariantList& V, bool phase2, int n, int k,
+                                             int& si, int& ndx, int& pos, int& fl, int& kf) {
+    if (phase2) {
+        si = V.lo + k;
+        ndx = V.ndx2;
+        pos = V.base + si;
+        fl = V.fl2;
+        kf = pos;
+        return;
+    }
+    int d = 0, fcl = V.fl[0], c = V.cnt[0];
+#pragma unroll
+    for (int e = 1; e < FRAG_NSUB; e++) {
+        if (k >= c) { k -= c; d = e; c = V.cnt[e]; fcl = V.fl[e]; }
+    }
+    si = k * FRAG_NSUB + d;
+    ndx = d;
+    fl = fcl;
+    pos = k * FRAG_STEP;
+    int delta = pos + fl - n;
+    kf = pos - (delta > 0 ? delta : 0);
+}
+
+// One warp per pair; the lanes take the pair's admissible variants in turn
+// and the warp reduces (max score, lowest variant index): the reference's
+// arg-max over fragment factors with strict comparisons
+// (MpStageBase.h:1192-1207).
+constexpr int RF_WARPS = 4;
+
 template <int MODE>
-__global__ void __launch_bounds__(64) k_refine(Blk B, Bat T) {
-    int i = blockIdx.x;
+__global__ void __launch_bounds__(RF_WARPS * 32) k_refine(Blk B, Bat T) {
+    __shared__ float s_last[16 * RF_WARPS * 32];
+    __shared__ float s_tb[12 * RF_WARPS * 32];
+    const unsigned FULL = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    const int i = blockIdx.x * RF_WARPS + (threadIdx.x >> 5);
     if (i >= T.np) return;
+    const int str = RF_WARPS * 32;
+    float* last = s_last + threadIdx.x;
+    float* tbs = s_tb + threadIdx.x;
     int flags = T.flags[i];
     if (MODE == RM_INIT) {
-        if (flags & CONV_LOWTMSC) { if (threadIdx.x == 0) T.best[i] = 0.f; return; }
+        if (flags & CONV_LOWTMSC) { if (lane == 0) T.best[i] = 0.f; return; }
     } else if (MODE == RM_DP) {
-        if (flags) { if (threadIdx.x == 0) T.best[i] = 0.f; return; }
+        if (flags) { if (lane == 0) T.best[i] = 0.f; return; }
     } else {
         if (flags & CONV_LOWTMSC) return;
     }
@@ -407,36 +528,17 @@ __global__ void __launch_bounds__(64) k_refine(Blk B, Bat T) {
     int chk = prod ? 0 : 1;
     float best_init = (MODE == RM_INIT || MODE == RM_DP) ? 0.f : -1.f;
     int maxalnmax = B.qmax < B.rmax ? B.qmax : B.rmax;
-    int nvar, nf = 0;
-    if (phase2) {
-        nf = 2 * maxalnmax < FIN_MAXNPOS ? 2 * maxalnmax : FIN_MAXNPOS;
-        nvar = nf;
-    } else {
-        nvar = (int)ceilf((float)(maxalnmax + FRAG_STEP - MINFRAGLEN) / FRAG_STEP) * FRAG_NSUB;
-    }
     int nrange = G.n;
-    int sfndx0 = phase2 ? T.sfndx[i] : 0, sfpos0 = phase2 ? T.sfpos[i] : 0;
-    float lbest = 0.f, lgbest = 0.f, tbest[12];
+    VariantList V;
+    variants_init(V, phase2, nrange, maxalnmax, phase2 ? T.sfndx[i] : 0, phase2 ? T.sfpos[i] : 0);
+    float lbest = 0.f, lgbest = 0.f;
     int lsi = 0x7fffffff, lndx = 0, lpos = 0;
-    for (int si = threadIdx.x; si < nvar && nrange > 0; si += blockDim.x) {
-        int sfragndx, sfragpos, fraglen, kf;
-        if (phase2) {
-            sfragndx = sfndx0 == 0 ? 1 : sfndx0;
-            sfragpos = sfpos0 + (si - (nf >> 1));
-            fraglen = frag_length(nrange, sfragndx);
-            if (fraglen < 1) continue;
-            if (sfragpos < 0 || nrange + 1 <= sfragpos + fraglen) continue;
-            kf = sfragpos;
-        } else {
-            int sfragfct = si / FRAG_NSUB;
-            sfragndx = si - sfragfct * FRAG_NSUB;
-            fraglen = frag_length(nrange, sfragndx);
-            if (fraglen < 1) continue;
-            sfragpos = sfragfct * FRAG_STEP;
-            if (nrange + FRAG_STEP <= sfragpos + fraglen) continue;
-            int delta = sfragpos + fraglen - nrange;
-            kf = sfragpos - (delta > 0 ? delta : 0);
-        }
+    float tbest[12];
+#pragma unroll
+    for (int f = 0; f < 12; f++) tbest[f] = 0.f;
+    for (int k = lane; k < V.total; k += 32) {
+        int si, sfragndx, sfragpos, fraglen, kf;
+        variants_get(V, phase2, nrange, k, si, sfragndx, sfragpos, fraglen, kf);
         if (MODE == RM_PROD1 && si == 0) {
             // RMSD over the whole alignment from compensated FP32 sums
             CovAcc a;
@@ -445,9 +547,9 @@ __global__ void __launch_bounds__(64) k_refine(Blk B, Bat T) {
 #pragma unroll
             for (int f = 0; f < 6; f++) { sq[f] = 0.f; cq[f] = 0.f; bq[f] = 0.f; }
             int blk = 0;
-            for (int k = kf; k < kf + fraglen; k++) {
+            for (int kk = kf; kk < kf + fraglen; kk++) {
                 float qx, qy, qz, rx, ry, rz;
-                G.at(k, qx, qy, qz, rx, ry, rz);
+                G.at(kk, qx, qy, qz, rx, ry, rz);
                 a.add(qx, qy, qz, rx, ry, rz);
                 bq[0] = __fmaf_rn(qx, qx, bq[0]); bq[1] = __fmaf_rn(qy, qy, bq[1]); bq[2] = __fmaf_rn(qz, qz, bq[2]);
                 bq[3] = __fmaf_rn(rx, rx, bq[3]); bq[4] = __fmaf_rn(ry, ry, bq[4]); bq[5] = __fmaf_rn(rz, rz, bq[5]);
@@ -467,41 +569,39 @@ __global__ void __launch_bounds__(64) k_refine(Blk B, Bat T) {
             for (int f = 0; f < 6; f++) { nfold(sq[f], cq[f], bq[f]); dv[15 + f] = (double)__fadd_rn(sq[f], cq[f]); }
             T.rmsd32[i] = (float)rmsd_from_sums(dv, (double)fraglen);
         }
-        float best, tb[12];
-        refine_loop(G, kf, fraglen, d0, d02, chk, d82, best_init, swap, best, tb);
+        float best;
+        refine_loop(G, kf, fraglen, d0, d02, chk, d82, best_init, swap, best, last, tbs, str);
         float gbest = best;
         if (prod && best >= 0.f && lq != lr) {
             int gl = lq > lr ? lq : lr;
             float g0 = B.t_d0fin[gl];
-            float m3;
+            float m3, tb[12];
+#pragma unroll
+            for (int f = 0; f < 12; f++) tb[f] = tbs[f * str];
             gbest = score_pass(G, tb, __fmul_rn(g0, g0), 0, d82, 0, m3);
         }
+        // a lane's variants come in increasing si: strict > keeps the lowest
         if (best > 0.f && lbest < best) {
             lbest = best; lgbest = gbest; lsi = si; lndx = sfragndx; lpos = sfragpos;
 #pragma unroll
-            for (int f = 0; f < 12; f++) tbest[f] = tb[f];
+            for (int f = 0; f < 12; f++) tbest[f] = tbs[f * str];
         }
     }
-    __shared__ float sb[64];
-    __shared__ int ssi[64];
-    sb[threadIdx.x] = lbest;
-    ssi[threadIdx.x] = lsi;
-    __syncthreads();
-    for (int s = blockDim.x >> 1; s > 0; s >>= 1) {
-        if ((int)threadIdx.x < s) {
-            float o = sb[threadIdx.x + s];
-            int os = ssi[threadIdx.x + s];
-            if (o > sb[threadIdx.x] || (o == sb[threadIdx.x] && os < ssi[threadIdx.x])) {
-                sb[threadIdx.x] = o;
-                ssi[threadIdx.x] = os;
-            }
-        }
-        __syncthreads();
+    // warp arg-max: larger score, then lower variant index
+    float wb = lbest;
+    int wsi = lsi;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        float ob = __shfl_xor_sync(FULL, wb, o);
+        int os = __shfl_xor_sync(FULL, wsi, o);
+        if (ob > wb || (ob == wb && os < wsi)) { wb = ob; wsi = os; }
     }
-    float wb = sb[0];
-    int wsi = ssi[0];
-    bool havewin = wb > 0.f;
-    bool iamwin = havewin && lsi == wsi && lbest == wb;
+    const bool havewin = wb > 0.f;
+    const unsigned wmask = __ballot_sync(FULL, havewin && lsi == wsi);
+    const int wl = wmask ? __ffs(wmask) - 1 : 0;
+    const bool iamwin = havewin && lane == wl;
+    const int wndx = __shfl_sync(FULL, lndx, wl);
+    const int wpos = __shfl_sync(FULL, lpos, wl);
     if (MODE == RM_PROD1 || MODE == RM_PROD2) {
         if (iamwin) {
             float grand = T.grand[i];
@@ -516,12 +616,12 @@ __global__ void __launch_bounds__(64) k_refine(Blk B, Bat T) {
                 T.out[i * 16 + 12] = B.t_d0fin[lr];
 #pragma unroll
                 for (int f = 0; f < 12; f++) T.tfm_gr[i * 12 + f] = tbest[f];
-                if (MODE == RM_PROD1) { T.sfndx[i] = lndx; T.sfpos[i] = lpos; }
+                if (MODE == RM_PROD1) { T.sfndx[i] = wndx; T.sfpos[i] = wpos; }
             }
         }
         return;
     }
-    if (threadIdx.x == 0) T.best[i] = havewin ? wb : 0.f;
+    if (lane == 0) T.best[i] = havewin ? wb : 0.f;
     if (iamwin) {
 #pragma unroll
         for (int f = 0; f < 12; f++) T.tfm_ib[i * 12 + f] = tbest[f];
@@ -530,22 +630,25 @@ __global__ void __launch_bounds__(64) k_refine(Blk B, Bat T) {
 #pragma unroll
             for (int f = 0; f < 12; f++) T.tfm_gr[i * 12 + f] = tbest[f];
         }
-        if (MODE == RM_FIN1) { T.sfndx_cur[i] = lndx; T.sfpos_cur[i] = lpos; }
     }
-    if (MODE == RM_FIN1) {
-        __syncthreads();
-        if (threadIdx.x == 0) { T.sfndx[i] = T.sfndx_cur[i]; T.sfpos[i] = T.sfpos_cur[i]; }
+    if (MODE == RM_FIN1 && lane == 0) {
+        // the winner's fragment, or the previous one when no variant scored
+        int nd = havewin ? wndx : T.sfndx_cur[i];
+        int np_ = havewin ? wpos : T.sfpos_cur[i];
+        T.sfndx_cur[i] = nd; T.sfpos_cur[i] = np_;
+        T.sfndx[i] = nd; T.sfpos[i] = np_;
     }
 }
 
 void launch_refine(int mode, const Blk& B, const Bat& T, cudaStream_t st) {
+    const int nb = (T.np + RF_WARPS - 1) / RF_WARPS, nt = RF_WARPS * 32;
     switch (mode) {
-        case RM_INIT:  k_refine<RM_INIT><<<T.np, 64, 0, st>>>(B, T); break;
-        case RM_DP:    k_refine<RM_DP><<<T.np, 64, 0, st>>>(B, T); break;
-        case RM_FIN1:  k_refine<RM_FIN1><<<T.np, 64, 0, st>>>(B, T); break;
-        case RM_FIN2:  k_refine<RM_FIN2><<<T.np, 64, 0, st>>>(B, T); break;
-        case RM_PROD1: k_refine<RM_PROD1><<<T.np, 64, 0, st>>>(B, T); break;
-        case RM_PROD2: k_refine<RM_PROD2><<<T.np, 64, 0, st>>>(B, T); break;
+        case RM_INIT:  k_refine<RM_INIT><<<nb, nt, 0, st>>>(B, T); break;
+        case RM_DP:    k_refine<RM_DP><<<nb, nt, 0, st>>>(B, T); break;
+        case RM_FIN1:  k_refine<RM_FIN1><<<nb, nt, 0, st>>>(B, T); break;
+        case RM_FIN2:  k_refine<RM_FIN2><<<nb, nt, 0, st>>>(B, T); break;
+        case RM_PROD1: k_refine<RM_PROD1><<<nb, nt, 0, st>>>(B, T); break;
+        case RM_PROD2: k_refine<RM_PROD2><<<nb, nt, 0, st>>>(B, T); break;
     }
     GTB_LAUNCHED(T);
 }
@@ -733,9 +836,17 @@ void launch_lowscore(const Blk& B, const Bat& T, float thr, cudaStream_t st) {
 __global__ void k_alnstr(Blk B, Bat T) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= T.np) return;
-    if (T.flags[i] & CONV_LOWTMSC) return;
     int qi = pair_qi(B, T, i), ri = pair_ri(B, T, i);
     int lq = B.qlen[qi], lr = B.rlen[ri];
+    if (T.flags[i] & CONV_LOWTMSC) {
+        // no alignment: five empty rows (the batch memory is reused between calls)
+        if (T.str) {
+            char* d = T.str + T.off_str[i];
+            int W = lq + lr + 1;
+            d[0] = 0; d[W] = 0; d[2 * W] = 0; d[3 * W] = 0; d[4 * W] = 0;
+        }
+        return;
+    }
     const unsigned* aln = T.aln + T.off_aln[i];
     int n = T.naln[i];
     float t[12];
