@@ -144,8 +144,7 @@ static size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 
 // Bytes of device scratch one pair needs.
 static size_t pair_bytes(int lq, int lr, bool strings) {
-    size_t nstrips = (size_t)(lq + 31) / 32;
-    size_t b = nstrips * (size_t)(lr + 31) * 8;       // traceback words
+    size_t b = (size_t)gtb::bt_words(lq, lr) * 4;     // traceback words
     b += (size_t)lr * 4;                               // DP row buffer
     b += (size_t)std::min(lq, lr) * 4;                 // aligned pairs
     if (strings) b += (size_t)5 * (lq + lr + 1);       // alignment rows
@@ -210,7 +209,7 @@ static gtb_status run_block(gtb_handle* h, const DevBlock& D, float scorethld,
         for (int i = 0; i < np; i++) {
             long long p = p0 + i;
             int lq = D.hqlen[p / D.nr], lr = D.hrlen[p % D.nr];
-            off_bt[i + 1] = off_bt[i] + (long long)((lq + 31) / 32) * (lr + 31);
+            off_bt[i + 1] = off_bt[i] + gtb::bt_words(lq, lr);
             off_row[i + 1] = off_row[i] + lr;
             off_aln[i + 1] = off_aln[i] + std::min(lq, lr);
             off_str[i + 1] = off_str[i] + (strings ? 5LL * (lq + lr + 1) : 0);
@@ -225,7 +224,7 @@ static gtb_status run_block(gtb_handle* h, const DevBlock& D, float scorethld,
         size_t o_out = carve((size_t)np * 16 * sizeof(float));
         size_t o_err = carve((size_t)np * 4 * sizeof(float));
         size_t o_offs = carve((size_t)(np + 1) * 4 * sizeof(long long));
-        size_t o_bt = carve((size_t)off_bt[np] * sizeof(uint2));
+        size_t o_bt = carve((size_t)off_bt[np] * sizeof(unsigned));
         size_t o_row = carve((size_t)off_row[np] * sizeof(float));
         size_t o_aln = carve((size_t)off_aln[np] * sizeof(unsigned));
         size_t o_str = carve((size_t)std::max<long long>(off_str[np], 1));
@@ -242,7 +241,7 @@ static gtb_status run_block(gtb_handle* h, const DevBlock& D, float scorethld,
         T.out = (float*)(base + o_out); T.err = (float*)(base + o_err);
         long long* offs = (long long*)(base + o_offs);
         T.off_bt = offs; T.off_row = offs + (np + 1); T.off_aln = offs + 2 * (np + 1); T.off_str = offs + 3 * (np + 1);
-        T.bt = (uint2*)(base + o_bt); T.row = (float*)(base + o_row);
+        T.bt = (unsigned*)(base + o_bt); T.row = (float*)(base + o_row);
         T.aln = (unsigned*)(base + o_aln); T.str = strings ? (base + o_str) : nullptr;
         T.launches = &h->launches;
         CK(cudaMemcpyAsync(offs, off_bt.data(), (np + 1) * sizeof(long long), cudaMemcpyHostToDevice, st));

@@ -5,13 +5,15 @@
 //    diagonal offset; each thread runs the whole covariance -> rotation ->
 //    score -> threshold loop of its offset sequentially and keeps its best;
 //    the CTA reduces (max score, lowest offset index).
-//  * refinement (every fragment-based superposition refinement): one CTA
-//    per pair, one thread per (fragment position, fragment length) variant,
-//    same reduction.  The distance-threshold covariance pass of iteration
-//    k+1 is fused into the scoring pass of iteration k.
-//  * DP: one warp per pair; the warp sweeps 32-row strips along
-//    anti-diagonals (lane = row), left/up/diagonal values move between lanes
-//    by shuffles, directions are packed 2 bits per cell with two ballots.
+//  * refinement (every fragment-based superposition refinement): one warp
+//    per pair, the lanes take the pair's admissible (fragment position,
+//    fragment length) variants in turn; the warp reduces (max score, lowest
+//    variant index) with shuffles.  The distance-threshold covariance pass
+//    of iteration k+1 is fused into the scoring pass of iteration k.
+//  * DP: one warp per pair; the warp sweeps strips of DP_ROWS rows along
+//    anti-diagonals (DP_R rows per lane, register-blocked), left/up/diagonal
+//    values move between lanes by shuffles, each lane packs the 2-bit
+//    directions of its cells into traceback words.
 //  * traceback, alignment rows, bookkeeping: one thread per pair.
 // All floating-point reductions are sequential per thread in forward position
 // order (blocks of BLK positions, Neumaier-compensated), so results do not
@@ -654,11 +656,18 @@ void launch_refine(int mode, const Blk& B, const Bat& T, cudaStream_t st) {
 }
 
 // ---------------------------------------------------------------------------
-// DP: MpDPHub.cpp:72-346 and 686-940.  One warp per pair.
+// DP: MpDPHub.cpp:72-346 and 686-940.  One warp per pair.  Lane l holds the
+// DP_R query rows DP_ROWS*s + DP_R*l + r of strip s and, at step t of the
+// strip, computes column j = t - l of those rows (one anti-diagonal of the
+// strip per step).  The value above a lane's first row comes from lane l-1
+// (its last row, previous step) or, for lane 0, from the previous strip's
+// last row kept in `row`.  Stored values are negated when the cell was
+// reached diagonally (the reference's state encoding, MpDPHub.cpp:246-262).
 __global__ void __launch_bounds__(128) k_dp(Blk B, Bat T, int tfmsrc, int gap0, float gcost,
                                             int usess, int dpscan, int skipmode) {
-    int lane = threadIdx.x & 31;
-    int i = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    const unsigned FULL = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    const int i = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
     if (i >= T.np) return;
     int flags = T.flags[i];
     int skipmask = skipmode == 0 ? (CONV_LOWTMSC | CONV_SCOREDP) : CONV_LOWTMSC;
@@ -683,52 +692,72 @@ __global__ void __launch_bounds__(128) k_dp(Blk B, Bat T, int tfmsrc, int gap0, 
     const char* qs = B.qs + B.qoff[qi];
     const char* rs = B.rs + B.roff[ri];
     float* row = T.row + T.off_row[i];
-    uint2* bt = T.bt + T.off_bt[i];
+    unsigned* bt = T.bt + T.off_bt[i];
     const int W = lr + 31;
-    const int nstrips = (lq + 31) >> 5;
-    const unsigned FULL = 0xffffffffu;
+    const long long sw = bt_strip_words(lr);
+    const int nstrips = (lq + DP_ROWS - 1) / DP_ROWS;
     for (int s = 0; s < nstrips; s++) {
-        int irow = (s << 5) + lane;
-        bool vrow = irow < lq;
-        float tx = 0.f, ty = 0.f, tz = 0.f;
-        char qss = 0;
-        if (vrow) {
-            xform(t, __ldg(qx + irow), __ldg(qy + irow), __ldg(qz + irow), tx, ty, tz);
-            if (usess) qss = qs[irow];
+        float tx[DP_R], ty[DP_R], tz[DP_R], h[DP_R];
+        char qss[DP_R];
+        int nv = 0;  // valid rows of this lane (a prefix of its DP_R rows)
+#pragma unroll
+        for (int r = 0; r < DP_R; r++) {
+            int irow = s * DP_ROWS + lane * DP_R + r;
+            tx[r] = ty[r] = tz[r] = 0.f;
+            qss[r] = 0;
+            h[r] = 0.f;
+            if (irow < lq) {
+                xform(t, __ldg(qx + irow), __ldg(qy + irow), __ldg(qz + irow), tx[r], ty[r], tz[r]);
+                if (usess) qss[r] = qs[irow];
+                nv = r + 1;
+            }
         }
-        float hleft = 0.f, uplast = 0.f, rb = 0.f;
+        float uplast = 0.f, rb = 0.f;
+        unsigned acc = 0u;
+        unsigned* bts = bt + s * sw + lane;
         __syncwarp();
         for (int tt = 0; tt < W; tt++) {
-            int j = tt - lane;
+            const int j = tt - lane;
             if ((tt & 31) == 0) {
                 int jj = tt + lane;
                 rb = (s > 0 && jj < lr) ? row[jj] : 0.f;
             }
-            float upv = __shfl_up_sync(FULL, hleft, 1);
+            float upv = __shfl_up_sync(FULL, h[DP_R - 1], 1);
             float up0 = __shfl_sync(FULL, rb, tt & 31);
             if (lane == 0) upv = (j < lr) ? up0 : 0.f;
-            int bk = 0;
-            if (vrow && j >= 0 && j < lr) {
-                float d = dist2(tx, ty, tz, __ldg(rx + j), __ldg(ry + j), __ldg(rz + j));
-                float v = tmterm(d02, d);
-                if (usess) v = __fadd_rn(v, __fmul_rn((float)(qss == rs[j]), 0.5f));
-                float dg = uplast;
-                v = __fadd_rn(v, gap0 ? dg : fabsf(dg));
-                bk = BT_DIAG;
-                float l = hleft;
-                if (!gap0 && l < 0.f) l = __fsub_rn(gcost, l);
-                if (v < l) { v = l; bk = BT_LEFT; }
-                float u = upv;
-                if (!gap0 && u < 0.f) u = __fsub_rn(gcost, u);
-                if (v < u) { v = u; bk = BT_UP; }
-                float w = (gap0 || bk != BT_DIAG) ? v : -v;
-                hleft = w;
-                if (lane == 31) row[j] = w;
+            unsigned bits = 0u;
+            if (j >= 0 && j < lr && nv > 0) {
+                float cx = __ldg(rx + j), cy = __ldg(ry + j), cz = __ldg(rz + j);
+                char css = usess ? rs[j] : 0;
+                float up = upv, dg = uplast;
+#pragma unroll
+                for (int r = 0; r < DP_R; r++) {
+                    if (r < nv) {
+                        float v = tmterm(d02, dist2(tx[r], ty[r], tz[r], cx, cy, cz));
+                        if (usess) v = __fadd_rn(v, __fmul_rn((float)(qss[r] == css), 0.5f));
+                        v = __fadd_rn(v, gap0 ? dg : fabsf(dg));
+                        int bk = BT_DIAG;
+                        float l = h[r];
+                        if (!gap0 && l < 0.f) l = __fsub_rn(gcost, l);
+                        if (v < l) { v = l; bk = BT_LEFT; }
+                        float u = up;
+                        if (!gap0 && u < 0.f) u = __fsub_rn(gcost, u);
+                        if (v < u) { v = u; bk = BT_UP; }
+                        float w = (gap0 || bk != BT_DIAG) ? v : -v;
+                        dg = h[r];   // (row r, j-1): the next row's diagonal
+                        up = w;      // (row r, j):   the next row's up
+                        h[r] = w;
+                        bits |= (unsigned)bk << (2 * r);
+                    }
+                }
+                if (lane == 31 && nv == DP_R) row[j] = h[DP_R - 1];
             }
             uplast = upv;
-            unsigned b0 = __ballot_sync(FULL, bk & 1);
-            unsigned b1 = __ballot_sync(FULL, (bk >> 1) & 1);
-            if (lane == 0) bt[(long long)s * W + tt] = make_uint2(b0, b1);
+            acc |= bits << (2 * DP_R * (tt % DP_SPW));
+            if (tt % DP_SPW == DP_SPW - 1 || tt == W - 1) {
+                bts[(tt / DP_SPW) * 32] = acc;
+                acc = 0u;
+            }
         }
         __syncwarp();
     }
@@ -755,9 +784,9 @@ __global__ void k_btck(Blk B, Bat T, int constrained) {
     int qi = pair_qi(B, T, i), ri = pair_ri(B, T, i);
     int lq = B.qlen[qi], lr = B.rlen[ri];
     int ml = lq < lr ? lq : lr;
-    const uint2* bt = T.bt + T.off_bt[i];
+    const unsigned* bt = T.bt + T.off_bt[i];
     unsigned* aln = T.aln + T.off_aln[i];
-    const int W = lr + 31;
+    const long long sw = bt_strip_words(lr);
     float t[12];
     float d82 = B.t_d82[ml];
     const float *qx = B.qx + B.qoff[qi], *qy = B.qy + B.qoff[qi], *qz = B.qz + B.qoff[qi];
@@ -768,9 +797,9 @@ __global__ void k_btck(Blk B, Bat T, int constrained) {
     }
     int y = lq - 1, x = lr - 1, n = 0;
     while (x >= 0 && y >= 0) {
-        int l = y & 31;
-        uint2 w = bt[(long long)(y >> 5) * W + x + l];
-        int b = (int)((w.x >> l) & 1u) | ((int)((w.y >> l) & 1u) << 1);
+        int yy = y % DP_ROWS, l = yy / DP_R, tt = x + l;
+        unsigned w = bt[(long long)(y / DP_ROWS) * sw + (tt / DP_SPW) * 32 + l];
+        int b = (int)((w >> (2 * DP_R * (tt % DP_SPW) + 2 * (yy % DP_R))) & 3u);
         if (b == BT_UP) { y--; continue; }
         if (b == BT_LEFT) { x--; continue; }
         if (constrained) {

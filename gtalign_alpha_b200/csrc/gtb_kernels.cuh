@@ -5,6 +5,21 @@
 
 namespace gtb {
 
+// DP traceback storage.  The DP sweeps strips of DP_ROWS query rows (DP_R
+// rows per lane of a warp) along anti-diagonals, lr + 31 steps per strip;
+// every lane packs the 2-bit directions of its DP_R rows for DP_SPW
+// consecutive steps into one 32-bit word, words of a strip stored
+// [step / DP_SPW][lane].
+constexpr int DP_R = 2;
+constexpr int DP_ROWS = 32 * DP_R;
+constexpr int DP_SPW = 16 / DP_R;
+__host__ __device__ inline long long bt_strip_words(int lr) {
+    return (long long)((lr + 31 + DP_SPW - 1) / DP_SPW) * 32;
+}
+__host__ __device__ inline long long bt_words(int lq, int lr) {
+    return (long long)((lq + DP_ROWS - 1) / DP_ROWS) * bt_strip_words(lr);
+}
+
 // Block of queries x references (device pointers, SoA).
 struct Blk {
     int nq, nr;
@@ -27,7 +42,7 @@ struct Bat {
     float *grand, *best, *best0, *rmsd32;
     float *tfm_ib, *tfm_gr;          // [np][12]
     float *out, *err;                // [np][16], [np][4]
-    const long long *off_bt;  uint2* bt;      // traceback words per pair
+    const long long *off_bt;  unsigned* bt;   // traceback words per pair
     const long long *off_row; float* row;     // DP row buffer per pair
     const long long *off_aln; unsigned* aln;  // aligned pairs, reverse order
     const long long *off_str; char* str;      // alignment rows per pair

@@ -139,7 +139,7 @@ extern "C" gtb_status gtb_process_block_noalloc(int device, const gtb_options* o
     obt[0] = orow[0] = oaln[0] = ostr[0] = 0;
     for (int i = 0; i < np; i++) {
         int lq = q->lens[i / r->n], lr = r->lens[i % r->n];
-        obt[i + 1] = obt[i] + (long long)((lq + 31) / 32) * (lr + 31);
+        obt[i + 1] = obt[i] + gtb::bt_words(lq, lr);
         orow[i + 1] = orow[i] + lr;
         oaln[i + 1] = oaln[i] + (lq < lr ? lq : lr);
         ostr[i + 1] = 0;
@@ -153,7 +153,7 @@ extern "C" gtb_status gtb_process_block_noalloc(int device, const gtb_options* o
     size_t o_out = carve((size_t)np * 16 * sizeof(float));
     size_t o_err = carve((size_t)np * 4 * sizeof(float));
     size_t o_offs = carve((size_t)(np + 1) * 4 * sizeof(long long));
-    size_t o_bt = carve((size_t)obt[np] * sizeof(uint2));
+    size_t o_bt = carve((size_t)obt[np] * sizeof(unsigned));
     size_t o_row = carve((size_t)orow[np] * sizeof(float));
     size_t o_aln = carve((size_t)oaln[np] * sizeof(unsigned));
     if (sz > SCRATCH_BYTES) {
@@ -195,7 +195,7 @@ extern "C" gtb_status gtb_process_block_noalloc(int device, const gtb_options* o
     T.out = (float*)(base + o_out); T.err = (float*)(base + o_err);
     long long* offs = (long long*)(base + o_offs);
     T.off_bt = offs; T.off_row = offs + (np + 1); T.off_aln = offs + 2 * (np + 1); T.off_str = offs + 3 * (np + 1);
-    T.bt = (uint2*)(base + o_bt); T.row = (float*)(base + o_row);
+    T.bt = (unsigned*)(base + o_bt); T.row = (float*)(base + o_row);
     T.aln = (unsigned*)(base + o_aln); T.str = nullptr;
     T.launches = nullptr;
 
