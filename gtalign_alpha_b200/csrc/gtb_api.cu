@@ -29,6 +29,11 @@ struct gtb_handle {
     long long launches = 0;
     float timings[7] = {0};
     cudaEvent_t ev[8] = {};
+    // sub-batches of a batch run concurrently on these streams (st first),
+    // so the short, narrow launches at the end of one overlap the others
+    static const int NSUB = 3;
+    cudaStream_t sub[NSUB] = {};
+    cudaEvent_t sev[NSUB][8] = {};
 };
 
 static const int TBL = 65536;
@@ -69,6 +74,11 @@ extern "C" gtb_status gtb_create(int device, size_t mem_bytes, const gtb_options
         cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
     }
     for (int k = 0; k < 8; k++) CK(cudaEventCreate(&h->ev[k]));
+    h->sub[0] = h->st;
+    for (int j = 1; j < gtb_handle::NSUB; j++)
+        CK(cudaStreamCreateWithFlags(&h->sub[j], cudaStreamNonBlocking));
+    for (int j = 0; j < gtb_handle::NSUB; j++)
+        for (int k = 0; k < 8; k++) CK(cudaEventCreate(&h->sev[j][k]));
     std::vector<float> a(TBL), b(TBL), c(TBL);
     make_tables(a.data(), b.data(), c.data(), TBL);
     CK(cudaMalloc(&h->t_d0, TBL * sizeof(float)));
@@ -88,6 +98,10 @@ extern "C" void gtb_destroy(gtb_handle* h) {
     if (h->t_d82) cudaFree(h->t_d82);
     if (h->t_d0fin) cudaFree(h->t_d0fin);
     for (int k = 0; k < 8; k++) if (h->ev[k]) cudaEventDestroy(h->ev[k]);
+    for (int j = 0; j < gtb_handle::NSUB; j++) {
+        for (int k = 0; k < 8; k++) if (h->sev[j][k]) cudaEventDestroy(h->sev[j][k]);
+        if (j > 0 && h->sub[j]) cudaStreamDestroy(h->sub[j]);
+    }
     if (h->st) cudaStreamDestroy(h->st);
     delete h;
 }
@@ -148,7 +162,7 @@ static size_t pair_bytes(int lq, int lr, bool strings) {
     b += (size_t)lr * 4;                               // DP row buffer
     b += (size_t)std::min(lq, lr) * 4;                 // aligned pairs
     if (strings) b += (size_t)5 * (lq + lr + 1);       // alignment rows
-    b += 4 * 8 + 12 * 4 * 2 + 16 * 4 + 4 * 4 + 12 * 4 + 64;  // state + offsets
+    b += 4 * 8 + 12 * 4 * 2 + 16 * 4 + 4 * 4 + 12 * 4 + 64 + 4;  // state, offsets, work list
     return b;
 }
 
@@ -160,7 +174,6 @@ static gtb_status run_block(gtb_handle* h, const DevBlock& D, float scorethld,
                             float* h_alndata, float* h_tfm, float* h_err,
                             char* hstr, const std::vector<long long>* hstroff) {
     const gtb_options& o = h->opts;
-    cudaStream_t st = h->st;
     const long long npairs = (long long)D.nq * D.nr;
     Blk B{};
     B.nq = D.nq; B.nr = D.nr;
@@ -183,38 +196,29 @@ static gtb_status run_block(gtb_handle* h, const DevBlock& D, float scorethld,
     // keep batches moderate so the pair-level state stays L2-friendly
     const long long maxbatch = 1 << 20;
 
-    std::vector<long long> off_bt, off_row, off_aln, off_str;
     float tsum[7] = {0, 0, 0, 0, 0, 0, 0};
     h->launches = 0;
+    // host offsets of the sub-batches in flight (kept until their copies ran)
+    std::vector<long long> offv[gtb_handle::NSUB];
 
-    long long p0 = 0;
-    while (p0 < npairs) {
-        // choose the batch
-        size_t used = 0;
-        long long p1 = p0;
-        while (p1 < npairs && p1 - p0 < maxbatch) {
-            int lq = D.hqlen[p1 / D.nr], lr = D.hrlen[p1 % D.nr];
-            size_t b = pair_bytes(lq, lr, strings);
-            if (used + b > budget && p1 > p0) break;
-            used += b;
-            p1++;
-        }
-        if (used > budget) {
-            snprintf(h->err, sizeof(h->err), "pair (%lld) needs %zu bytes > budget %zu", p0, used, budget);
-            return GTB_ERR_NOMEM;
-        }
-        int np = (int)(p1 - p0);
-        off_bt.assign(np + 1, 0); off_row.assign(np + 1, 0);
-        off_aln.assign(np + 1, 0); off_str.assign(np + 1, 0);
+    // One sub-batch [q0, q0 + np): plan, carve one allocation, upload the
+    // offsets, launch the stage sequence and the result copies on stream st.
+    auto launch_sub = [&](long long q0, int np, int j) -> gtb_status {
+        cudaStream_t st = h->sub[j];
+        std::vector<long long>& ov = offv[j];
+        ov.assign(4 * (size_t)(np + 1), 0);
+        long long* off_bt = ov.data();
+        long long* off_row = off_bt + (np + 1);
+        long long* off_aln = off_bt + 2 * (np + 1);
+        long long* off_str = off_bt + 3 * (np + 1);
         for (int i = 0; i < np; i++) {
-            long long p = p0 + i;
+            long long p = q0 + i;
             int lq = D.hqlen[p / D.nr], lr = D.hrlen[p % D.nr];
             off_bt[i + 1] = off_bt[i] + gtb::bt_words(lq, lr);
             off_row[i + 1] = off_row[i] + lr;
             off_aln[i + 1] = off_aln[i] + std::min(lq, lr);
             off_str[i + 1] = off_str[i] + (strings ? 5LL * (lq + lr + 1) : 0);
         }
-        // one allocation, carved
         size_t sz = 0;
         auto carve = [&](size_t bytes) { size_t o2 = sz; sz += align256(bytes); return o2; };
         size_t o_ints = carve((size_t)np * 8 * sizeof(int));
@@ -228,10 +232,12 @@ static gtb_status run_block(gtb_handle* h, const DevBlock& D, float scorethld,
         size_t o_row = carve((size_t)off_row[np] * sizeof(float));
         size_t o_aln = carve((size_t)off_aln[np] * sizeof(unsigned));
         size_t o_str = carve((size_t)std::max<long long>(off_str[np], 1));
+        size_t o_rl = carve((size_t)np * sizeof(int));
+        size_t o_rh = carve((size_t)4097 * sizeof(int));
         char* base = nullptr;
         CK(cudaMallocAsync((void**)&base, sz, st));
         Bat T{};
-        T.p0 = p0; T.np = np;
+        T.p0 = q0; T.np = np;
         int* ints = (int*)(base + o_ints);
         T.flags = ints; T.seedq = ints + np; T.seedr = ints + 2 * np; T.naln = ints + 3 * np;
         T.sfndx = ints + 4 * np; T.sfpos = ints + 5 * np; T.sfndx_cur = ints + 6 * np; T.sfpos_cur = ints + 7 * np;
@@ -243,34 +249,63 @@ static gtb_status run_block(gtb_handle* h, const DevBlock& D, float scorethld,
         T.off_bt = offs; T.off_row = offs + (np + 1); T.off_aln = offs + 2 * (np + 1); T.off_str = offs + 3 * (np + 1);
         T.bt = (unsigned*)(base + o_bt); T.row = (float*)(base + o_row);
         T.aln = (unsigned*)(base + o_aln); T.str = strings ? (base + o_str) : nullptr;
+        T.rlist = (int*)(base + o_rl); T.rhist = (int*)(base + o_rh);
         T.launches = &h->launches;
-        CK(cudaMemcpyAsync(offs, off_bt.data(), (np + 1) * sizeof(long long), cudaMemcpyHostToDevice, st));
-        CK(cudaMemcpyAsync(offs + (np + 1), off_row.data(), (np + 1) * sizeof(long long), cudaMemcpyHostToDevice, st));
-        CK(cudaMemcpyAsync(offs + 2 * (np + 1), off_aln.data(), (np + 1) * sizeof(long long), cudaMemcpyHostToDevice, st));
-        CK(cudaMemcpyAsync(offs + 3 * (np + 1), off_str.data(), (np + 1) * sizeof(long long), cudaMemcpyHostToDevice, st));
-
-        // ------------------------------------------------------------ stages
+        CK(cudaMemcpyAsync(offs, off_bt, 4 * (size_t)(np + 1) * sizeof(long long), cudaMemcpyHostToDevice, st));
         launch_stages(B, T, o.refinement, o.depth, o.convergence, o.prescore, o.referenced,
-                      scorethld, st, h->ev);
+                      scorethld, st, h->sev[j]);
         CK(cudaGetLastError());
-
-        // ------------------------------------------------------------ results
         if (h_alndata)
-            CK(cudaMemcpyAsync(h_alndata + p0 * 16, T.out, (size_t)np * 16 * sizeof(float), cudaMemcpyDefault, st));
+            CK(cudaMemcpyAsync(h_alndata + q0 * 16, T.out, (size_t)np * 16 * sizeof(float), cudaMemcpyDefault, st));
         if (h_tfm)
-            CK(cudaMemcpyAsync(h_tfm + p0 * 12, T.tfm_gr, (size_t)np * 12 * sizeof(float), cudaMemcpyDefault, st));
+            CK(cudaMemcpyAsync(h_tfm + q0 * 12, T.tfm_gr, (size_t)np * 12 * sizeof(float), cudaMemcpyDefault, st));
         if (h_err)
-            CK(cudaMemcpyAsync(h_err + p0 * 4, T.err, (size_t)np * 4 * sizeof(float), cudaMemcpyDefault, st));
+            CK(cudaMemcpyAsync(h_err + q0 * 4, T.err, (size_t)np * 4 * sizeof(float), cudaMemcpyDefault, st));
         if (strings)
-            CK(cudaMemcpyAsync(hstr + (*hstroff)[p0], T.str, (size_t)off_str[np], cudaMemcpyDeviceToHost, st));
+            CK(cudaMemcpyAsync(hstr + (*hstroff)[q0], T.str, (size_t)off_str[np], cudaMemcpyDeviceToHost, st));
         CK(cudaFreeAsync(base, st));
-        CK(cudaStreamSynchronize(st));
-        float ms = 0.f;
-        CK(cudaEventElapsedTime(&ms, h->ev[0], h->ev[1])); tsum[0] += ms;
-        CK(cudaEventElapsedTime(&ms, h->ev[1], h->ev[2])); tsum[1] += ms;
-        CK(cudaEventElapsedTime(&ms, h->ev[2], h->ev[3])); tsum[2] += ms;
-        CK(cudaEventElapsedTime(&ms, h->ev[3], h->ev[4])); tsum[5] += ms;
-        CK(cudaEventElapsedTime(&ms, h->ev[0], h->ev[4])); tsum[6] += ms;
+        return GTB_OK;
+    };
+
+    long long p0 = 0;
+    while (p0 < npairs) {
+        // choose the batch (fixed part: carve alignment and the work-list buckets)
+        size_t used = 32768 * gtb_handle::NSUB;
+        long long p1 = p0;
+        while (p1 < npairs && p1 - p0 < maxbatch) {
+            int lq = D.hqlen[p1 / D.nr], lr = D.hrlen[p1 % D.nr];
+            size_t b = pair_bytes(lq, lr, strings);
+            if (used + b > budget && p1 > p0) break;
+            used += b;
+            p1++;
+        }
+        if (used > budget) {
+            snprintf(h->err, sizeof(h->err), "pair (%lld) needs %zu bytes > budget %zu", p0, used, budget);
+            return GTB_ERR_NOMEM;
+        }
+        // split into concurrent sub-batches of at least 16k pairs
+        long long nb = p1 - p0;
+        int nsub = (int)std::min<long long>(gtb_handle::NSUB, std::max<long long>(1, nb / 16384));
+        long long q0 = p0;
+        for (int j = 0; j < nsub; j++) {
+            long long q1 = p0 + nb * (j + 1) / nsub;
+            gtb_status s = launch_sub(q0, (int)(q1 - q0), j);
+            if (s != GTB_OK) {
+                for (int k = 0; k < nsub; k++) cudaStreamSynchronize(h->sub[k]);
+                return s;
+            }
+            q0 = q1;
+        }
+        for (int j = 0; j < nsub; j++) {
+            CK(cudaStreamSynchronize(h->sub[j]));
+            cudaEvent_t* ev = h->sev[j];
+            float ms = 0.f;
+            CK(cudaEventElapsedTime(&ms, ev[0], ev[1])); tsum[0] += ms;
+            CK(cudaEventElapsedTime(&ms, ev[1], ev[2])); tsum[1] += ms;
+            CK(cudaEventElapsedTime(&ms, ev[2], ev[3])); tsum[2] += ms;
+            CK(cudaEventElapsedTime(&ms, ev[3], ev[4])); tsum[5] += ms;
+            CK(cudaEventElapsedTime(&ms, ev[0], ev[4])); tsum[6] += ms;
+        }
         p0 = p1;
     }
     memcpy(h->timings, tsum, sizeof(tsum));

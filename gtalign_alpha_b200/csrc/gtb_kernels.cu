@@ -352,59 +352,68 @@ void launch_findfrag(const Blk& B, const Bat& T, cudaStream_t st) {
 }
 
 // ---------------------------------------------------------------------------
-// the refinement loop: MpStage1.cpp:640-700 and its copies in
-// RefineFragDPKernel and MpStageFin.cpp (one thread = one variant).
-// last/tb are this thread's slots in shared memory (stride `str`): the
-// previous iteration's sums (convergence test) and the best transform.
-__device__ void refine_loop(const PairGeom& G, int kf, int fraglen, float d0, float d02,
-                            int chk, float d82, float best_init, int swap,
-                            float& bestout, float* last, float* tb, int str) {
-    float v[16], tfm[12], m3;
-    float best = best_init;
-    float d0s = d0s_of(d0);
-    float d0sp = __fadd_rn(d0s, 1.0f);
-    float thr2 = __fmul_rn(d0sp, d0sp);
-    float dst32 = LARGEDST;
-    cov_range(G, kf, kf + fraglen, v);
-    // iteration 0
-    if (v[15] < 1.0f) { bestout = best; return; }
-#pragma unroll
-    for (int f = 0; f < 16; f++) last[f * str] = v[f];
-    solve_sums(v, swap, tfm);
-    {
-        float d0sm = __fsub_rn(d0s, 1.0f);
-        float d02s = __fmul_rn(d0sm, d0sm);
-        // iteration 1's threshold is d02s unless the third-smallest distance
-        // is above it: accumulate for d02s while scoring, redo otherwise
-        float sc = score_and_ext(G, tfm, d02, chk, d82, d02s, v, 2, m3);
-        if (LARGEDST_CMP < m3 || m3 < d02s || G.n <= 3) dst32 = d02s;
-        else {
-            float t = __fadd_rn(d0sm, __fmul_rn(ceilf(__fmul_rn(__fsub_rn(__fsqrt_rn(m3), d0sm), 2.0f)), 0.5f));
-            dst32 = __fmul_rn(t, t);
-        }
-        if (best < sc) {
-            best = sc;
-#pragma unroll
-            for (int f = 0; f < 12; f++) tb[f * str] = tfm[f];
-        }
-        // iteration 1: threshold from iteration 0's three smallest distances
-        if (dst32 != d02s) cov_ext(G, tfm, dst32, v);
+// Refinement work list.  Before each refinement launch the pairs that take
+// part (mode's convergence flags clear, a non-empty position space) are
+// listed in decreasing order of their position count (buckets of 16), so
+// that the pairs sharing a warp have passes of about the same length and
+// finished pairs cost nothing.  Pairs left out get the mode's outputs for
+// "no variant scored" here.
+constexpr int RL_SHIFT = 4;
+constexpr int RL_NB = 65536 >> RL_SHIFT;   // buckets; rhist[RL_NB] = list length
+
+// position count of pair i in mode `mode`, or -1 when the pair is skipped
+__device__ __forceinline__ int refine_span(const Blk& B, const Bat& T, int mode, int i) {
+    int flags = T.flags[i];
+    if (mode == RM_DP ? flags != 0 : (flags & CONV_LOWTMSC) != 0) return -1;
+    if (mode != RM_INIT) return T.naln[i];
+    int qi = pair_qi(B, T, i), ri = pair_ri(B, T, i);
+    int lq = B.qlen[qi], lr = B.rlen[ri];
+    int sq = T.seedq[i], sr = T.seedr[i];
+    if (lq <= sq || lr <= sr) return 0;
+    return (lq - sq) < (lr - sr) ? (lq - sq) : (lr - sr);
+}
+
+__global__ void k_rlist_count(Blk B, Bat T, int mode) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= T.np) return;
+    int n = refine_span(B, T, mode, i);
+    if (n > 0) {
+        atomicAdd(&T.rhist[RL_NB - 1 - (n >> RL_SHIFT)], 1);
+        return;
     }
-    for (int cit = 1; cit < NMAXCONVIT + 2; cit++) {
-        if (converged16(v, last, str)) break;
-        if (v[15] < 1.0f) break;
+    // no variant: MpStage1.cpp:700-716 with nothing scored
+    bool skipped = n < 0;
+    if (mode == RM_INIT || mode == RM_DP || (!skipped && (mode == RM_FIN1 || mode == RM_FIN2)))
+        T.best[i] = 0.f;
+    if (!skipped && mode == RM_FIN1) { T.sfndx[i] = T.sfndx_cur[i]; T.sfpos[i] = T.sfpos_cur[i]; }
+}
+
+// exclusive scan of the bucket counts (one CTA of 1024 threads)
+__global__ void __launch_bounds__(1024) k_rlist_scan(Bat T) {
+    __shared__ int part[1024];
+    constexpr int PER = RL_NB / 1024;
+    int t = threadIdx.x, loc[PER], s = 0;
 #pragma unroll
-        for (int f = 0; f < 16; f++) last[f * str] = v[f];
-        solve_sums(v, swap, tfm);
-        // scoring pass of this iteration fused with the covariance of the next
-        float sc = score_and_ext(G, tfm, d02, chk, d82, thr2, v, 0, m3);
-        if (best < sc) {
-            best = sc;
-#pragma unroll
-            for (int f = 0; f < 12; f++) tb[f * str] = tfm[f];
-        }
+    for (int j = 0; j < PER; j++) { loc[j] = T.rhist[t * PER + j]; s += loc[j]; }
+    part[t] = s;
+    __syncthreads();
+    for (int o = 1; o < 1024; o <<= 1) {
+        int v = t >= o ? part[t - o] : 0;
+        __syncthreads();
+        part[t] += v;
+        __syncthreads();
     }
-    bestout = best;
+    int run = part[t] - s;
+#pragma unroll
+    for (int j = 0; j < PER; j++) { T.rhist[t * PER + j] = run; run += loc[j]; }
+    if (t == 1023) T.rhist[RL_NB] = part[1023];
+}
+
+__global__ void k_rlist_fill(Blk B, Bat T, int mode) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= T.np) return;
+    int n = refine_span(B, T, mode, i);
+    if (n > 0) T.rlist[atomicAdd(&T.rhist[RL_NB - 1 - (n >> RL_SHIFT)], 1)] = i;
 }
 
 // Variant list of one pair, enumerated compactly (admissible variants only).
@@ -479,31 +488,80 @@ __device__ __forceinline__ void variants_get(const VariantList& V, bool phase2, 
     kf = pos - (delta > 0 ? delta : 0);
 }
 
-// One warp per pair; the lanes take the pair's admissible variants in turn
-// and the warp reduces (max score, lowest variant index): the reference's
-// arg-max over fragment factors with strict comparisons
-// (MpStageBase.h:1192-1207).
+// ---------------------------------------------------------------------------
+// Refinement.  RF_LPP lanes share one pair and take the pair's admissible
+// variants from a pool in list order; a lane whose variant is done takes
+// the next one, so the lanes stay busy while variants last.  All lanes
+// advance together one pass at a time (a pass = one sweep of the pair's
+// positions); what a lane does in a pass depends on where its variant is
+// in the refinement loop of MpStage1.cpp:640-700 (and its copies in
+// RefineFragDPKernel and MpStageFin.cpp):
+enum PassKind {
+    PK_IDLE = 0,    // no variant left for this lane
+    PK_FRAG = 1,    // covariance of the fragment [k0, k1)
+    PK_SCORE = 2,   // score under tfm, fused with the covariance of d <= thr
+    PK_EXT = 3,     // covariance of d <= thr only (iteration 1's threshold
+                    // when it differs from the one fused into iteration 0)
+    PK_GSCORE = 4,  // score of the variant's best transform with another d0
+};
+
+// One pass of one lane.  Blocks of BLK positions are the absolute blocks
+// of the position space for every kind, so lanes fold together.
+__device__ __forceinline__ float lane_pass(const PairGeom& G, int kind, int k0, int k1,
+                                           const float* tfm, float d02, int chk, float d82,
+                                           float thr, int m3on, float* v, float& m3out) {
+    float ss = 0.f, sc = 0.f, sb = 0.f;
+    float m1 = LARGEDST, m2 = LARGEDST, m3 = LARGEDST;
+    const bool frag = kind == PK_FRAG;
+    const bool scr = kind == PK_SCORE || kind == PK_GSCORE;
+    const bool cov = kind == PK_SCORE || kind == PK_EXT;
+    const int n = kind == PK_IDLE ? 0 : (frag ? k1 : G.n);
+    CovAcc a;
+    a.init();
+    for (int b0 = frag ? (k0 & ~(BLK - 1)) : 0; b0 < n; b0 += BLK) {
+        int b1 = b0 + BLK < n ? b0 + BLK : n;
+#pragma unroll 2
+        for (int k = b0; k < b1; k++) {
+            float qx, qy, qz, rx, ry, rz;
+            G.at(k, qx, qy, qz, rx, ry, rz);
+            float d = dist2_tf(tfm, qx, qy, qz, rx, ry, rz);
+            if (scr) {
+                if (!chk || d <= d82) sb = __fadd_rn(sb, tmterm(d02, d));
+                if (m3on) track3(2, d, m1, m2, m3);
+            }
+            if (frag ? (k0 <= k) : (cov && d <= thr)) a.add(qx, qy, qz, rx, ry, rz);
+        }
+        nfold(ss, sc, sb);
+        a.fold();
+    }
+    nfold(ss, sc, sb);
+    a.final(v);
+    m3out = m3;
+    return __fadd_rn(ss, sc);
+}
+
+constexpr int RF_LPP = 16;                 // lanes per pair
+constexpr int RF_PPW = 32 / RF_LPP;        // pairs per warp
 constexpr int RF_WARPS = 4;
+constexpr int RF_PAIRS = RF_PPW * RF_WARPS;  // pairs per CTA
 
 template <int MODE>
 __global__ void __launch_bounds__(RF_WARPS * 32) k_refine(Blk B, Bat T) {
-    __shared__ float s_last[16 * RF_WARPS * 32];
-    __shared__ float s_tb[12 * RF_WARPS * 32];
+    __shared__ float s_last[16 * RF_WARPS * 32];   // previous iteration's sums
+    __shared__ float s_tb[12 * RF_WARPS * 32];     // best transform of the current variant
+    __shared__ float s_tbest[12 * RF_WARPS * 32];  // best transform over the lane's variants
     const unsigned FULL = 0xffffffffu;
     const int lane = threadIdx.x & 31;
-    const int i = blockIdx.x * RF_WARPS + (threadIdx.x >> 5);
-    if (i >= T.np) return;
+    const int sub = lane / RF_LPP;
+    const unsigned smask = ((1u << RF_LPP) - 1u) << (sub * RF_LPP);
+    const int slot = blockIdx.x * RF_PAIRS + (threadIdx.x >> 5) * RF_PPW + sub;
+    const bool valid = slot < T.rhist[RL_NB];
+    if (__ballot_sync(FULL, valid) == 0) return;
+    const int i = valid ? T.rlist[slot] : 0;
     const int str = RF_WARPS * 32;
     float* last = s_last + threadIdx.x;
     float* tbs = s_tb + threadIdx.x;
-    int flags = T.flags[i];
-    if (MODE == RM_INIT) {
-        if (flags & CONV_LOWTMSC) { if (lane == 0) T.best[i] = 0.f; return; }
-    } else if (MODE == RM_DP) {
-        if (flags) { if (lane == 0) T.best[i] = 0.f; return; }
-    } else {
-        if (flags & CONV_LOWTMSC) return;
-    }
+    float* tbest = s_tbest + threadIdx.x;
     int qi = pair_qi(B, T, i), ri = pair_ri(B, T, i);
     int lq = B.qlen[qi], lr = B.rlen[ri];
     int ml = lq < lr ? lq : lr;
@@ -522,88 +580,163 @@ __global__ void __launch_bounds__(RF_WARPS * 32) k_refine(Blk B, Bat T) {
         G.q0 = G.r0 = 0;
         G.n = T.naln[i];
     }
+    if (!valid) G.n = 0;
+    const int n = G.n;
     const bool prod = (MODE == RM_PROD1 || MODE == RM_PROD2);
     const bool phase2 = (MODE == RM_FIN2 || MODE == RM_PROD2);
-    float d0 = prod ? B.t_d0fin[ml] : B.t_d0[ml];
-    float d02 = __fmul_rn(d0, d0);
-    float d82 = B.t_d82[ml];
-    int chk = prod ? 0 : 1;
-    float best_init = (MODE == RM_INIT || MODE == RM_DP) ? 0.f : -1.f;
-    int maxalnmax = B.qmax < B.rmax ? B.qmax : B.rmax;
-    int nrange = G.n;
+    const float d0 = prod ? B.t_d0fin[ml] : B.t_d0[ml];
+    const float d02 = __fmul_rn(d0, d0);
+    const float d82 = B.t_d82[ml];
+    const int chk = prod ? 0 : 1;
+    const float best_init = (MODE == RM_INIT || MODE == RM_DP) ? 0.f : -1.f;
+    const int maxalnmax = B.qmax < B.rmax ? B.qmax : B.rmax;
+    const float d0s = d0s_of(d0);
+    const float d0sm = __fsub_rn(d0s, 1.0f);
+    const float d02s = __fmul_rn(d0sm, d0sm);       // iteration 1's usual threshold
+    const float d0sp = __fadd_rn(d0s, 1.0f);
+    const float thr2 = __fmul_rn(d0sp, d0sp);       // threshold of iterations >= 2
+    const bool gscore = prod && lq != lr;           // also scored by the longer length
+    float g02 = 0.f;
+    if (gscore) { float g0 = B.t_d0fin[lq > lr ? lq : lr]; g02 = __fmul_rn(g0, g0); }
     VariantList V;
-    variants_init(V, phase2, nrange, maxalnmax, phase2 ? T.sfndx[i] : 0, phase2 ? T.sfpos[i] : 0);
-    float lbest = 0.f, lgbest = 0.f;
+    variants_init(V, phase2, n, maxalnmax, phase2 ? T.sfndx[i] : 0, phase2 ? T.sfpos[i] : 0);
+    if (MODE == RM_PROD1 && (lane % RF_LPP) == 0 && V.total > 0) {
+        // RMSD over the whole alignment (variant 0: fragment [0, n)) from
+        // compensated FP32 sums, MpStageFin.cpp production phase 1
+        int s0, nd0, ps0, fl0, kf0;
+        variants_get(V, phase2, n, 0, s0, nd0, ps0, fl0, kf0);
+        CovAcc a;
+        a.init();
+        float sq[6], cq[6], bq[6];
+#pragma unroll
+        for (int f = 0; f < 6; f++) { sq[f] = 0.f; cq[f] = 0.f; bq[f] = 0.f; }
+        int blk = 0;
+        for (int kk = kf0; kk < kf0 + fl0; kk++) {
+            float qx, qy, qz, rx, ry, rz;
+            G.at(kk, qx, qy, qz, rx, ry, rz);
+            a.add(qx, qy, qz, rx, ry, rz);
+            bq[0] = __fmaf_rn(qx, qx, bq[0]); bq[1] = __fmaf_rn(qy, qy, bq[1]); bq[2] = __fmaf_rn(qz, qz, bq[2]);
+            bq[3] = __fmaf_rn(rx, rx, bq[3]); bq[4] = __fmaf_rn(ry, ry, bq[4]); bq[5] = __fmaf_rn(rz, rz, bq[5]);
+            if (++blk == BLK) {
+                a.fold();
+#pragma unroll
+                for (int f = 0; f < 6; f++) nfold(sq[f], cq[f], bq[f]);
+                blk = 0;
+            }
+        }
+        float vv[16];
+        a.final(vv);
+        double dv[21];
+#pragma unroll
+        for (int f = 0; f < 15; f++) dv[f] = (double)vv[f];
+#pragma unroll
+        for (int f = 0; f < 6; f++) { nfold(sq[f], cq[f], bq[f]); dv[15 + f] = (double)__fadd_rn(sq[f], cq[f]); }
+        T.rmsd32[i] = (float)rmsd_from_sums(dv, (double)fl0);
+    }
+    float lbest = 0.f, lgbest = 0.f;              // this lane's best variant so far
     int lsi = 0x7fffffff, lndx = 0, lpos = 0;
-    float tbest[12];
+    int kind = PK_IDLE, si = 0, vndx = 0, vpos = 0, k0 = 0, k1 = 0, cit = 0, m3mode = 0, pchk = chk;
+    float best = 0.f, thr = 0.f, pd02 = d02;
+    float tfm[12];
 #pragma unroll
-    for (int f = 0; f < 12; f++) tbest[f] = 0.f;
-    for (int k = lane; k < V.total; k += 32) {
-        int si, sfragndx, sfragpos, fraglen, kf;
-        variants_get(V, phase2, nrange, k, si, sfragndx, sfragpos, fraglen, kf);
-        if (MODE == RM_PROD1 && si == 0) {
-            // RMSD over the whole alignment from compensated FP32 sums
-            CovAcc a;
-            a.init();
-            float sq[6], cq[6], bq[6];
-#pragma unroll
-            for (int f = 0; f < 6; f++) { sq[f] = 0.f; cq[f] = 0.f; bq[f] = 0.f; }
-            int blk = 0;
-            for (int kk = kf; kk < kf + fraglen; kk++) {
-                float qx, qy, qz, rx, ry, rz;
-                G.at(kk, qx, qy, qz, rx, ry, rz);
-                a.add(qx, qy, qz, rx, ry, rz);
-                bq[0] = __fmaf_rn(qx, qx, bq[0]); bq[1] = __fmaf_rn(qy, qy, bq[1]); bq[2] = __fmaf_rn(qz, qz, bq[2]);
-                bq[3] = __fmaf_rn(rx, rx, bq[3]); bq[4] = __fmaf_rn(ry, ry, bq[4]); bq[5] = __fmaf_rn(rz, rz, bq[5]);
-                if (++blk == BLK) {
-                    a.fold();
-#pragma unroll
-                    for (int f = 0; f < 6; f++) nfold(sq[f], cq[f], bq[f]);
-                    blk = 0;
+    for (int f = 0; f < 12; f++) tfm[f] = 0.f;
+    bool need = true;
+    int nextk = 0;                                // the pair's next variant to hand out
+    for (;;) {
+        const unsigned nm = __ballot_sync(FULL, need) & smask;
+        if (nm) {
+            int kv = nextk + __popc(nm & ((1u << lane) - 1u));
+            nextk += __popc(nm);
+            if (need) {
+                need = false;
+                kind = PK_IDLE;
+                if (kv < V.total) {
+                    int fl, kf;
+                    variants_get(V, phase2, n, kv, si, vndx, vpos, fl, kf);
+                    kind = PK_FRAG; k0 = kf; k1 = kf + fl;
+                    best = best_init; cit = 0;
                 }
             }
-            float vv[16];
-            a.final(vv);
-            double dv[21];
-#pragma unroll
-            for (int f = 0; f < 15; f++) dv[f] = (double)vv[f];
-#pragma unroll
-            for (int f = 0; f < 6; f++) { nfold(sq[f], cq[f], bq[f]); dv[15 + f] = (double)__fadd_rn(sq[f], cq[f]); }
-            T.rmsd32[i] = (float)rmsd_from_sums(dv, (double)fraglen);
         }
-        float best;
-        refine_loop(G, kf, fraglen, d0, d02, chk, d82, best_init, swap, best, last, tbs, str);
-        float gbest = best;
-        if (prod && best >= 0.f && lq != lr) {
-            int gl = lq > lr ? lq : lr;
-            float g0 = B.t_d0fin[gl];
-            float m3, tb[12];
+        if (__ballot_sync(FULL, kind != PK_IDLE) == 0) break;
+        float v[16], m3;
+        const float sc = lane_pass(G, kind, k0, k1, tfm, pd02, pchk, d82, thr, m3mode, v, m3);
+        bool havev = false, done = false;
+        if (kind == PK_FRAG) {
+            if (v[15] < 1.0f) done = true;
+            else {
 #pragma unroll
-            for (int f = 0; f < 12; f++) tb[f] = tbs[f * str];
-            gbest = score_pass(G, tb, __fmul_rn(g0, g0), 0, d82, 0, m3);
+                for (int f = 0; f < 16; f++) last[f * str] = v[f];
+                solve_sums(v, swap, tfm);
+                kind = PK_SCORE; thr = d02s; m3mode = 2; cit = 0; pd02 = d02; pchk = chk;
+            }
+        } else if (kind == PK_SCORE) {
+            if (best < sc) {
+                best = sc;
+#pragma unroll
+                for (int f = 0; f < 12; f++) tbs[f * str] = tfm[f];
+            }
+            havev = true;
+            if (cit == 0) {
+                // iteration 1's threshold from iteration 0's three smallest distances
+                float dst32;
+                if (LARGEDST_CMP < m3 || m3 < d02s || n <= 3) dst32 = d02s;
+                else {
+                    float t = __fadd_rn(d0sm, __fmul_rn(ceilf(__fmul_rn(__fsub_rn(__fsqrt_rn(m3), d0sm), 2.0f)), 0.5f));
+                    dst32 = __fmul_rn(t, t);
+                }
+                if (dst32 != d02s) { kind = PK_EXT; thr = dst32; m3mode = 0; havev = false; }
+            }
+            cit++;
+        } else if (kind == PK_EXT) {
+            havev = true;
+        } else if (kind == PK_GSCORE) {
+            done = true;
         }
-        // a lane's variants come in increasing si: strict > keeps the lowest
-        if (best > 0.f && lbest < best) {
-            lbest = best; lgbest = gbest; lsi = si; lndx = sfragndx; lpos = sfragpos;
+        if (havev) {
+            if (cit >= NMAXCONVIT + 2 || converged16(v, last, str) || v[15] < 1.0f) done = true;
+            else {
 #pragma unroll
-            for (int f = 0; f < 12; f++) tbest[f] = tbs[f * str];
+                for (int f = 0; f < 16; f++) last[f * str] = v[f];
+                solve_sums(v, swap, tfm);
+                kind = PK_SCORE; thr = thr2; m3mode = 0;
+            }
+        }
+        if (done) {
+            if (kind != PK_GSCORE && gscore && best >= 0.f) {
+                // one more pass: the variant's best transform scored with the
+                // d0 of the longer structure
+#pragma unroll
+                for (int f = 0; f < 12; f++) tfm[f] = tbs[f * str];
+                kind = PK_GSCORE; pd02 = g02; pchk = 0; m3mode = 0;
+            } else {
+                const float gbest = kind == PK_GSCORE ? sc : best;
+                if (best > 0.f && (lbest < best || (lbest == best && si < lsi))) {
+                    lbest = best; lgbest = gbest; lsi = si; lndx = vndx; lpos = vpos;
+#pragma unroll
+                    for (int f = 0; f < 12; f++) tbest[f * str] = tbs[f * str];
+                }
+                need = true;
+                kind = PK_IDLE;
+            }
         }
     }
-    // warp arg-max: larger score, then lower variant index
+    // arg-max over the pair's lanes: larger score, then lower variant index
     float wb = lbest;
     int wsi = lsi;
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
+    for (int o = RF_LPP / 2; o > 0; o >>= 1) {
         float ob = __shfl_xor_sync(FULL, wb, o);
         int os = __shfl_xor_sync(FULL, wsi, o);
         if (ob > wb || (ob == wb && os < wsi)) { wb = ob; wsi = os; }
     }
     const bool havewin = wb > 0.f;
-    const unsigned wmask = __ballot_sync(FULL, havewin && lsi == wsi);
-    const int wl = wmask ? __ffs(wmask) - 1 : 0;
+    const unsigned wmask = __ballot_sync(FULL, havewin && lsi == wsi) & smask;
+    const int wl = wmask ? __ffs(wmask) - 1 : sub * RF_LPP;
     const bool iamwin = havewin && lane == wl;
     const int wndx = __shfl_sync(FULL, lndx, wl);
     const int wpos = __shfl_sync(FULL, lpos, wl);
+    if (!valid) return;
     if (MODE == RM_PROD1 || MODE == RM_PROD2) {
         if (iamwin) {
             float grand = T.grand[i];
@@ -617,23 +750,23 @@ __global__ void __launch_bounds__(RF_WARPS * 32) k_refine(Blk B, Bat T) {
                 T.out[i * 16 + 11] = B.t_d0fin[lq];
                 T.out[i * 16 + 12] = B.t_d0fin[lr];
 #pragma unroll
-                for (int f = 0; f < 12; f++) T.tfm_gr[i * 12 + f] = tbest[f];
+                for (int f = 0; f < 12; f++) T.tfm_gr[i * 12 + f] = tbest[f * str];
                 if (MODE == RM_PROD1) { T.sfndx[i] = wndx; T.sfpos[i] = wpos; }
             }
         }
         return;
     }
-    if (lane == 0) T.best[i] = havewin ? wb : 0.f;
+    if (lane == wl) T.best[i] = havewin ? wb : 0.f;
     if (iamwin) {
 #pragma unroll
-        for (int f = 0; f < 12; f++) T.tfm_ib[i * 12 + f] = tbest[f];
+        for (int f = 0; f < 12; f++) T.tfm_ib[i * 12 + f] = tbest[f * str];
         if (T.grand[i] < wb) {
             T.grand[i] = wb;
 #pragma unroll
-            for (int f = 0; f < 12; f++) T.tfm_gr[i * 12 + f] = tbest[f];
+            for (int f = 0; f < 12; f++) T.tfm_gr[i * 12 + f] = tbest[f * str];
         }
     }
-    if (MODE == RM_FIN1 && lane == 0) {
+    if (MODE == RM_FIN1 && lane == wl) {
         // the winner's fragment, or the previous one when no variant scored
         int nd = havewin ? wndx : T.sfndx_cur[i];
         int np_ = havewin ? wpos : T.sfpos_cur[i];
@@ -643,16 +776,21 @@ __global__ void __launch_bounds__(RF_WARPS * 32) k_refine(Blk B, Bat T) {
 }
 
 void launch_refine(int mode, const Blk& B, const Bat& T, cudaStream_t st) {
-    const int nb = (T.np + RF_WARPS - 1) / RF_WARPS, nt = RF_WARPS * 32;
+    cudaMemsetAsync(T.rhist, 0, (RL_NB + 1) * sizeof(int), st);
+    const int nb = (T.np + 255) / 256;
+    k_rlist_count<<<nb, 256, 0, st>>>(B, T, mode);
+    k_rlist_scan<<<1, 1024, 0, st>>>(T);
+    k_rlist_fill<<<nb, 256, 0, st>>>(B, T, mode);
+    const int ng = (T.np + RF_PAIRS - 1) / RF_PAIRS, nt = RF_WARPS * 32;
     switch (mode) {
-        case RM_INIT:  k_refine<RM_INIT><<<nb, nt, 0, st>>>(B, T); break;
-        case RM_DP:    k_refine<RM_DP><<<nb, nt, 0, st>>>(B, T); break;
-        case RM_FIN1:  k_refine<RM_FIN1><<<nb, nt, 0, st>>>(B, T); break;
-        case RM_FIN2:  k_refine<RM_FIN2><<<nb, nt, 0, st>>>(B, T); break;
-        case RM_PROD1: k_refine<RM_PROD1><<<nb, nt, 0, st>>>(B, T); break;
-        case RM_PROD2: k_refine<RM_PROD2><<<nb, nt, 0, st>>>(B, T); break;
+        case RM_INIT:  k_refine<RM_INIT><<<ng, nt, 0, st>>>(B, T); break;
+        case RM_DP:    k_refine<RM_DP><<<ng, nt, 0, st>>>(B, T); break;
+        case RM_FIN1:  k_refine<RM_FIN1><<<ng, nt, 0, st>>>(B, T); break;
+        case RM_FIN2:  k_refine<RM_FIN2><<<ng, nt, 0, st>>>(B, T); break;
+        case RM_PROD1: k_refine<RM_PROD1><<<ng, nt, 0, st>>>(B, T); break;
+        case RM_PROD2: k_refine<RM_PROD2><<<ng, nt, 0, st>>>(B, T); break;
     }
-    GTB_LAUNCHED(T);
+    if (T.launches) (*T.launches) += 4;
 }
 
 // ---------------------------------------------------------------------------

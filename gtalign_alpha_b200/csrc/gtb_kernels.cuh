@@ -46,6 +46,7 @@ struct Bat {
     const long long *off_row; float* row;     // DP row buffer per pair
     const long long *off_aln; unsigned* aln;  // aligned pairs, reverse order
     const long long *off_str; char* str;      // alignment rows per pair
+    int *rlist, *rhist;              // refinement work list [np], buckets [4097]
     long long* launches;             // host counter of kernel launches
 };
 

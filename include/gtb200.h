@@ -202,8 +202,10 @@ const char* gtb_last_error(const gtb_handle* h);
 long long gtb_last_launch_count(const gtb_handle* h);
 
 /* Device time (ms) of the last gtb_process_block call, per stage:
- * [0] stage 1 seed, [1] stage-1 refinement, [2] DP kernels, [3] traceback,
- * [4] DP-alignment refinement, [5] final + production, [6] total. */
+ * [0] stage-1 seed, [1] stage-1 fragment refinement, [2] the DP <->
+ * refinement loops (stage-1 DPRefine and both stage-2 passes), [3] and [4]
+ * unused (0), [5] final + production stages, [6] total.  A batch runs as up
+ * to three concurrent sub-batches; the times are summed over them. */
 gtb_status gtb_last_timings(const gtb_handle* h, float* ms7);
 
 void gtb_destroy(gtb_handle* h);

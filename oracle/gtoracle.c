@@ -29,8 +29,9 @@
  *  - FP32 coordinates; transforms and squared distances written with explicit
  *    fmaf at fixed places; nothing else contracted (-ffp-contract=off);
  *  - every sum over positions is accumulated in forward position order in
- *    FP32 blocks of GTB_BLK positions, each block folded into a Neumaier
- *    compensated FP32 total;
+ *    FP32 blocks of GTB_BLK positions (the absolute blocks [32m, 32m+32) of
+ *    the position space), each block folded into a Neumaier compensated
+ *    FP32 total;
  *  - rotation solve in FP64 by the quaternion characteristic polynomial
  *    (Horn 1987; Theobald 2005 "QCP"): Newton iteration for the largest
  *    eigenvalue, eigenvector from the adjugate of (K - lambda I);
@@ -349,13 +350,16 @@ static inline void kpos(const kspace* s, int k, int* q, int* r) {
 }
 
 /* covariance over [k0,k1) (all positions) */
+/* covariance over positions [k0,k1); the compensated blocks are the
+ * absolute position blocks [32m, 32m+32) of the position space (the first
+ * and last ones clipped to the range), so that every pass over a space
+ * folds at the same positions whatever range it covers */
 static void cov_range(const pairctx* P, const kspace* s, int k0, int k1, float* v) {
     ccacc a; cc_init(&a);
-    int blk = 0;
     for (int k = k0; k < k1; k++) {
         int q, r; kpos(s, k, &q, &r);
         cc_add(&a, P->qx[q], P->qy[q], P->qz[q], P->rx[r], P->ry[r], P->rz[r]);
-        if (++blk == GTB_BLK) { cc_fold(&a); blk = 0; }
+        if ((k + 1) % GTB_BLK == 0) cc_fold(&a);
     }
     cc_final(&a, v);
 }
