@@ -255,6 +255,12 @@ def run_ours(args):
     h2d = int(np.mean([sum(a.nbytes for a in qb.arrays) for qb in qbs])) + sum(a.nbytes for a in rb.arrays)
     d2h = int(np.mean(step_pairs)) * (16 + 12) * 4
 
+    # the plain form: the same kernels at one pair per call (1 query x 1
+    # reference through gtb_process_block with host buffers), on a sample
+    plain = plain_sample(g, L, q, r, args.plain_pairs, args.seed) if args.plain_pairs > 0 else None
+    if plain is not None:
+        plain["batched_vs_plain"] = value / plain["value"]
+
     # roofline of the dominant stage (fraction of the step per stage)
     hbm_peak, peak_kind = peaks()
     st_ms = stage_ms / args.steps
@@ -291,6 +297,7 @@ def run_ours(args):
             "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "gpu_launches": launches,
             "roofline": roof,
+            "plain": plain,
             "cpu_baseline": cpu,
             "clocks": clocks,
             "workload_gen_s": gen_s,
@@ -345,6 +352,40 @@ def run_reference_sample(wl, nq: int, nref: int, threads: int):
     return nq * nref, time.time() - t, "port"
 
 
+def plain_sample(g, L, q, r, npairs: int, seed: int):
+    """pairs/s of one gtb_process_block call per pair on a seeded sample of
+    the workload's pairs (blocks packed beforehand; the calls are timed)."""
+    import torch
+    from gtalign_alpha_b200.api import _CResults, pack_fields
+    from gtalign_alpha_b200.shard import subset
+    rng = np.random.default_rng(seed + 77)
+    qi = rng.integers(0, q.n, npairs)
+    ri = rng.integers(0, r.n, npairs)
+    blocks = [(pack_fields(subset(q, np.array([a]))), pack_fields(subset(r, np.array([b]))))
+              for a, b in zip(qi, ri)]
+    out = np.zeros(16, np.float32)
+    tfm = np.zeros(12, np.float32)
+    res = _CResults(out.ctypes.data, tfm.ctypes.data, None, None, None, None)
+
+    def one(qb, rb):
+        st = L.gtb_process_block(g.handle, ctypes.c_float(0.5), qb.beg, qb.end, rb.beg, rb.end,
+                                 ctypes.byref(res))
+        if st != 0:
+            raise RuntimeError(L.gtb_last_error(g.handle).decode())
+
+    for qb, rb in blocks[:3]:
+        one(qb, rb)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for qb, rb in blocks:
+        one(qb, rb)
+    torch.cuda.synchronize()
+    secs = time.perf_counter() - t0
+    return {"value": npairs / secs, "unit": UNIT,
+            "sample": "%d seeded pairs of the workload, one gtb_process_block call (1 query x "
+                      "1 reference, host buffers) per pair" % npairs}
+
+
 def cpu_baseline_sample(wl, args):
     threads = os.cpu_count() or 1
     nref = args.cpu_sample_refs
@@ -396,6 +437,8 @@ def main():
     ap.add_argument("--seed", type=int, default=2)
     ap.add_argument("--cpu-sample-refs", type=int, default=2000)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--plain-pairs", type=int, default=300,
+                    help="pairs timed in the one-pair-per-call form (0: skip)")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

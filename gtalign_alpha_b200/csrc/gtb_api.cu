@@ -160,7 +160,7 @@ static size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 static size_t pair_bytes(int lq, int lr, bool strings) {
     size_t b = (size_t)gtb::bt_words(lq, lr) * 4;     // traceback words
     b += (size_t)lr * 4;                               // DP row buffer
-    b += (size_t)std::min(lq, lr) * 4;                 // aligned pairs
+    b += (size_t)std::min(lq, lr) * 28;                // aligned pairs + coordinates
     if (strings) b += (size_t)5 * (lq + lr + 1);       // alignment rows
     b += 4 * 8 + 12 * 4 * 2 + 16 * 4 + 4 * 4 + 12 * 4 + 64 + 4;  // state, offsets, work list
     return b;
@@ -232,6 +232,7 @@ static gtb_status run_block(gtb_handle* h, const DevBlock& D, float scorethld,
         size_t o_row = carve((size_t)off_row[np] * sizeof(float));
         size_t o_aln = carve((size_t)off_aln[np] * sizeof(unsigned));
         size_t o_str = carve((size_t)std::max<long long>(off_str[np], 1));
+        size_t o_alc = carve((size_t)off_aln[np] * 6 * sizeof(float));
         size_t o_rl = carve((size_t)np * sizeof(int));
         size_t o_rh = carve((size_t)4097 * sizeof(int));
         char* base = nullptr;
@@ -249,6 +250,7 @@ static gtb_status run_block(gtb_handle* h, const DevBlock& D, float scorethld,
         T.off_bt = offs; T.off_row = offs + (np + 1); T.off_aln = offs + 2 * (np + 1); T.off_str = offs + 3 * (np + 1);
         T.bt = (unsigned*)(base + o_bt); T.row = (float*)(base + o_row);
         T.aln = (unsigned*)(base + o_aln); T.str = strings ? (base + o_str) : nullptr;
+        T.alc = (float*)(base + o_alc);
         T.rlist = (int*)(base + o_rl); T.rhist = (int*)(base + o_rh);
         T.launches = &h->launches;
         CK(cudaMemcpyAsync(offs, off_bt, 4 * (size_t)(np + 1) * sizeof(long long), cudaMemcpyHostToDevice, st));

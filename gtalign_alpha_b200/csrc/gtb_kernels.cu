@@ -114,23 +114,23 @@ void launch_init(const Blk& B, const Bat& T, cudaStream_t st) {
 // ---------------------------------------------------------------------------
 // position spaces: a gapless diagonal from (q0, r0), or DP-aligned pairs
 // stored in traceback (reverse) order.
+// (The aligned space is read from the coordinates the traceback stored
+// with each aligned pair, 6 floats per pair in traceback order.)
 struct PairGeom {
     const float *qx, *qy, *qz, *rx, *ry, *rz;
-    const unsigned* aln;  // reverse order; null for the diagonal space
+    const float2* alc;    // aligned coordinates, reverse order; null: diagonal
     int q0, r0, n;
     __device__ __forceinline__ void at(int k, float& a, float& b, float& c,
                                        float& d, float& e, float& f) const {
-        int q, r;
-        if (aln) {
-            unsigned w = aln[n - 1 - k];
-            q = (int)(w >> 16);
-            r = (int)(w & 0xffffu);
+        if (alc) {
+            const float2* p = alc + 3 * (n - 1 - k);
+            float2 u = __ldg(p), v = __ldg(p + 1), w = __ldg(p + 2);
+            a = u.x; b = u.y; c = v.x; d = v.y; e = w.x; f = w.y;
         } else {
-            q = q0 + k;
-            r = r0 + k;
+            int q = q0 + k, r = r0 + k;
+            a = __ldg(qx + q); b = __ldg(qy + q); c = __ldg(qz + q);
+            d = __ldg(rx + r); e = __ldg(ry + r); f = __ldg(rz + r);
         }
-        a = __ldg(qx + q); b = __ldg(qy + q); c = __ldg(qz + q);
-        d = __ldg(rx + r); e = __ldg(ry + r); f = __ldg(rz + r);
     }
 };
 
@@ -248,6 +248,84 @@ __device__ __forceinline__ int converged16(const float* a, const float* b, int b
 
 // ---------------------------------------------------------------------------
 // stage 1 seed: MpStage1.cpp:289-440
+
+// The seed's fused pass: score (no d8 check), the three smallest distinct
+// distances, the covariance of d <= thr, and the SEED_K smallest distances
+// with their positions (ascending; ties keep the earlier position first).
+// When the next threshold turns out to be above thr, the positions within
+// it are usually these few (three in almost every case), and their
+// covariance is rebuilt from the list instead of another pass.
+constexpr int SEED_K = 6;
+
+__device__ float seed_score_ext(const PairGeom& G, const float* tfm, float d02, float thr,
+                                float* v, float& m3out, float* kd, int* kk) {
+    float ss = 0.f, sc = 0.f, sb = 0.f;
+    float m1 = LARGEDST, m2 = LARGEDST, m3 = LARGEDST;
+#pragma unroll
+    for (int j = 0; j < SEED_K; j++) { kd[j] = LARGEDST; kk[j] = 0; }
+    CovAcc a;
+    a.init();
+    for (int b0 = 0; b0 < G.n; b0 += BLK) {
+        int b1 = b0 + BLK < G.n ? b0 + BLK : G.n;
+#pragma unroll 2
+        for (int k = b0; k < b1; k++) {
+            float qx, qy, qz, rx, ry, rz;
+            G.at(k, qx, qy, qz, rx, ry, rz);
+            float d = dist2_tf(tfm, qx, qy, qz, rx, ry, rz);
+            sb = __fadd_rn(sb, tmterm(d02, d));
+            track3(1, d, m1, m2, m3);
+            if (d < kd[SEED_K - 1]) {
+                // insert (d, k) keeping kd ascending
+                float cd = d;
+                int ck = k;
+#pragma unroll
+                for (int j = 0; j < SEED_K; j++) {
+                    bool sw = cd < kd[j];
+                    float td = kd[j];
+                    int tk = kk[j];
+                    kd[j] = sw ? cd : td; kk[j] = sw ? ck : tk;
+                    cd = sw ? td : cd; ck = sw ? tk : ck;
+                }
+            }
+            if (d <= thr) a.add(qx, qy, qz, rx, ry, rz);
+        }
+        nfold(ss, sc, sb);
+        a.fold();
+    }
+    nfold(ss, sc, sb);
+    a.final(v);
+    m3out = m3;
+    return __fadd_rn(ss, sc);
+}
+
+// covariance of the listed positions with kd <= thr, in position order
+// with the block folds of a full pass (folding an empty block changes
+// nothing); valid when every position with d <= thr is listed.
+__device__ void seed_cov_list(const PairGeom& G, const float* kd, const int* kk, float thr,
+                              float* v) {
+    int sel[SEED_K], m = 0;
+#pragma unroll
+    for (int j = 0; j < SEED_K; j++)
+        if (kd[j] <= thr) sel[m++] = kk[j];
+    for (int x = 1; x < m; x++) {            // position order
+        int y = sel[x], z = x - 1;
+        while (z >= 0 && sel[z] > y) { sel[z + 1] = sel[z]; z--; }
+        sel[z + 1] = y;
+    }
+    CovAcc a;
+    a.init();
+    int blk = -1;
+    for (int x = 0; x < m; x++) {
+        int k = sel[x];
+        if (blk >= 0 && k / BLK != blk) a.fold();
+        blk = k / BLK;
+        float qx, qy, qz, rx, ry, rz;
+        G.at(k, qx, qy, qz, rx, ry, rz);
+        a.add(qx, qy, qz, rx, ry, rz);
+    }
+    a.final(v);
+}
+
 __device__ float findfrag_variant(const PairGeom& G, float d02, float d0s, int swap) {
     float v[16], tfm[12], m3, best = 0.f;
     float d02s0 = __fmul_rn(d0s, d0s);
@@ -262,12 +340,17 @@ __device__ float findfrag_variant(const PairGeom& G, float d02, float d0s, int s
         float d02s = __fadd_rn(d02s0, (it == 1 ? 1.0f : 0.0f));
         // the next threshold is d02s unless the third-smallest distance is
         // above it: accumulate for d02s while scoring, redo in the rare case
-        float sc = score_and_ext(G, tfm, d02, 0, 0.f, d02s, v, 1, m3);
+        float kd[SEED_K];
+        int kk[SEED_K];
+        float sc = seed_score_ext(G, tfm, d02, d02s, v, m3, kd, kk);
         if (best < sc) best = sc;
         float dst32;
         if (LARGEDST_CMP < m3 || m3 < d02s || G.n <= 3) dst32 = d02s;
         else dst32 = __fadd_rn(d02s, __fmul_rn(ceilf(__fmul_rn(__fsub_rn(m3, d02s), 2.0f)), 0.5f));
-        if (dst32 != d02s) cov_ext(G, tfm, dst32, v);
+        if (dst32 != d02s) {
+            if (dst32 < kd[SEED_K - 1]) seed_cov_list(G, kd, kk, dst32, v);
+            else cov_ext(G, tfm, dst32, v);
+        }
         if (v[15] < 1.0f) break;
         if ((int)v[15] == G.n) break;
     }
@@ -302,7 +385,7 @@ __global__ void __launch_bounds__(128) k_findfrag(Blk B, Bat T) {
     PairGeom G;
     G.qx = B.qx + B.qoff[qi]; G.qy = B.qy + B.qoff[qi]; G.qz = B.qz + B.qoff[qi];
     G.rx = B.rx + B.roff[ri]; G.ry = B.ry + B.roff[ri]; G.rz = B.rz + B.roff[ri];
-    G.aln = nullptr;
+    G.alc = nullptr;
     float lbest = 0.f;
     int lsi = 0x7fffffff;
     for (int si = silo + (int)threadIdx.x; si <= sihi; si += blockDim.x) {
@@ -525,11 +608,17 @@ __device__ __forceinline__ float lane_pass(const PairGeom& G, int kind, int k0, 
             float qx, qy, qz, rx, ry, rz;
             G.at(k, qx, qy, qz, rx, ry, rz);
             float d = dist2_tf(tfm, qx, qy, qz, rx, ry, rz);
-            if (scr) {
-                if (!chk || d <= d82) sb = __fadd_rn(sb, tmterm(d02, d));
-                if (m3on) track3(2, d, m1, m2, m3);
-            }
-            if (frag ? (k0 <= k) : (cov && d <= thr)) a.add(qx, qy, qz, rx, ry, rz);
+            // branch-free: adding +0 and zero coordinates leaves the sums unchanged
+            float tm = tmterm(d02, d);
+            sb = __fadd_rn(sb, (scr && (!chk || d <= d82)) ? tm : 0.f);
+            bool c1 = m3on && d < m1, c2 = m3on && d < m2, c3 = m3on && d < m3;
+            m3 = c2 ? m2 : (c3 ? d : m3);
+            m2 = c1 ? m1 : (c2 ? d : m2);
+            m1 = c1 ? d : m1;
+            bool inc = frag ? (k0 <= k) : (cov && d <= thr);
+            a.add(inc ? qx : 0.f, inc ? qy : 0.f, inc ? qz : 0.f,
+                  inc ? rx : 0.f, inc ? ry : 0.f, inc ? rz : 0.f);
+            a.n += inc ? 0 : -1;
         }
         nfold(ss, sc, sb);
         a.fold();
@@ -571,12 +660,12 @@ __global__ void __launch_bounds__(RF_WARPS * 32) k_refine(Blk B, Bat T) {
     G.rx = B.rx + B.roff[ri]; G.ry = B.ry + B.roff[ri]; G.rz = B.rz + B.roff[ri];
     if (MODE == RM_INIT) {
         int sq = T.seedq[i], sr = T.seedr[i];
-        G.aln = nullptr;
+        G.alc = nullptr;
         G.q0 = sq; G.r0 = sr;
         if (lq <= sq || lr <= sr) G.n = 0;
         else G.n = (lq - sq) < (lr - sr) ? (lq - sq) : (lr - sr);
     } else {
-        G.aln = T.aln + T.off_aln[i];
+        G.alc = (const float2*)(T.alc + 6 * T.off_aln[i]);
         G.q0 = G.r0 = 0;
         G.n = T.naln[i];
     }
@@ -924,6 +1013,7 @@ __global__ void k_btck(Blk B, Bat T, int constrained) {
     int ml = lq < lr ? lq : lr;
     const unsigned* bt = T.bt + T.off_bt[i];
     unsigned* aln = T.aln + T.off_aln[i];
+    float* alc = T.alc + 6 * T.off_aln[i];
     const long long sw = bt_strip_words(lr);
     float t[12];
     float d82 = B.t_d82[ml];
@@ -940,11 +1030,15 @@ __global__ void k_btck(Blk B, Bat T, int constrained) {
         int b = (int)((w >> (2 * DP_R * (tt % DP_SPW) + 2 * (yy % DP_R))) & 3u);
         if (b == BT_UP) { y--; continue; }
         if (b == BT_LEFT) { x--; continue; }
-        if (constrained) {
-            float d = dist2_tf(t, qx[y], qy[y], qz[y], rx[x], ry[x], rz[x]);
-            if (d <= d82) aln[n++] = ((unsigned)y << 16) | (unsigned)x;
-        } else
-            aln[n++] = ((unsigned)y << 16) | (unsigned)x;
+        float cqx = qx[y], cqy = qy[y], cqz = qz[y], crx = rx[x], cry = ry[x], crz = rz[x];
+        bool keep = true;
+        if (constrained) keep = dist2_tf(t, cqx, cqy, cqz, crx, cry, crz) <= d82;
+        if (keep) {
+            aln[n] = ((unsigned)y << 16) | (unsigned)x;
+            float2* c2 = (float2*)(alc + 6 * (long long)n);
+            c2[0] = make_float2(cqx, cqy); c2[1] = make_float2(cqz, crx); c2[2] = make_float2(cry, crz);
+            n++;
+        }
         x--; y--;
     }
     T.naln[i] = n;

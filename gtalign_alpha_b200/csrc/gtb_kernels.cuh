@@ -45,6 +45,7 @@ struct Bat {
     const long long *off_bt;  unsigned* bt;   // traceback words per pair
     const long long *off_row; float* row;     // DP row buffer per pair
     const long long *off_aln; unsigned* aln;  // aligned pairs, reverse order
+    float* alc;                      // their coordinates, 6 floats each (offset 6*off_aln)
     const long long *off_str; char* str;      // alignment rows per pair
     int *rlist, *rhist;              // refinement work list [np], buckets [4097]
     long long* launches;             // host counter of kernel launches

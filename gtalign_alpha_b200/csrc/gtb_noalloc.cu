@@ -156,6 +156,7 @@ extern "C" gtb_status gtb_process_block_noalloc(int device, const gtb_options* o
     size_t o_bt = carve((size_t)obt[np] * sizeof(unsigned));
     size_t o_row = carve((size_t)orow[np] * sizeof(float));
     size_t o_aln = carve((size_t)oaln[np] * sizeof(unsigned));
+    size_t o_alc = carve((size_t)oaln[np] * 6 * sizeof(float));
     size_t o_rl = carve((size_t)np * sizeof(int));
     size_t o_rh = carve((size_t)4097 * sizeof(int));
     if (sz > SCRATCH_BYTES) {
@@ -199,6 +200,7 @@ extern "C" gtb_status gtb_process_block_noalloc(int device, const gtb_options* o
     T.off_bt = offs; T.off_row = offs + (np + 1); T.off_aln = offs + 2 * (np + 1); T.off_str = offs + 3 * (np + 1);
     T.bt = (unsigned*)(base + o_bt); T.row = (float*)(base + o_row);
     T.aln = (unsigned*)(base + o_aln); T.str = nullptr;
+    T.alc = (float*)(base + o_alc);
     T.rlist = (int*)(base + o_rl); T.rhist = (int*)(base + o_rh);
     T.launches = nullptr;
 
