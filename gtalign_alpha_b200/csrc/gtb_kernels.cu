@@ -890,8 +890,10 @@ void launch_refine(int mode, const Blk& B, const Bat& T, cudaStream_t st) {
 // (its last row, previous step) or, for lane 0, from the previous strip's
 // last row kept in `row`.  Stored values are negated when the cell was
 // reached diagonally (the reference's state encoding, MpDPHub.cpp:246-262).
-__global__ void __launch_bounds__(128) k_dp(Blk B, Bat T, int tfmsrc, int gap0, float gcost,
-                                            int usess, int dpscan, int skipmode) {
+template <int GAP0, int USESS>
+__global__ void __launch_bounds__(128) k_dp(Blk B, Bat T, int tfmsrc, float gcost, int dpscan,
+                                            int skipmode) {
+    constexpr bool gap0 = GAP0 != 0, usess = USESS != 0;
     const unsigned FULL = 0xffffffffu;
     const int lane = threadIdx.x & 31;
     const int i = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
@@ -992,7 +994,11 @@ __global__ void __launch_bounds__(128) k_dp(Blk B, Bat T, int tfmsrc, int gap0, 
 
 void launch_dp(const Blk& B, const Bat& T, int tfmsrc, int gap0, float gcost, int usess,
                int dpscan, int skipmode, cudaStream_t st) {
-    k_dp<<<(T.np + 3) / 4, 128, 0, st>>>(B, T, tfmsrc, gap0, gcost, usess, dpscan, skipmode);
+    const int nb = (T.np + 3) / 4;
+    if (gap0 && !usess) k_dp<1, 0><<<nb, 128, 0, st>>>(B, T, tfmsrc, gcost, dpscan, skipmode);
+    else if (!gap0 && !usess) k_dp<0, 0><<<nb, 128, 0, st>>>(B, T, tfmsrc, gcost, dpscan, skipmode);
+    else if (!gap0 && usess) k_dp<0, 1><<<nb, 128, 0, st>>>(B, T, tfmsrc, gcost, dpscan, skipmode);
+    else k_dp<1, 1><<<nb, 128, 0, st>>>(B, T, tfmsrc, gcost, dpscan, skipmode);
     GTB_LAUNCHED(T);
 }
 
