@@ -33,7 +33,7 @@ struct gtb_handle {
     // so the short, narrow launches at the end of one overlap the others
     static const int NSUB = 3;
     cudaStream_t sub[NSUB] = {};
-    cudaEvent_t sev[NSUB][8] = {};
+    cudaEvent_t sev[2 * NSUB][8] = {};  // stage events per sub-batch (two waves)
 };
 
 static const int TBL = 65536;
@@ -77,7 +77,7 @@ extern "C" gtb_status gtb_create(int device, size_t mem_bytes, const gtb_options
     h->sub[0] = h->st;
     for (int j = 1; j < gtb_handle::NSUB; j++)
         CK(cudaStreamCreateWithFlags(&h->sub[j], cudaStreamNonBlocking));
-    for (int j = 0; j < gtb_handle::NSUB; j++)
+    for (int j = 0; j < 2 * gtb_handle::NSUB; j++)
         for (int k = 0; k < 8; k++) CK(cudaEventCreate(&h->sev[j][k]));
     std::vector<float> a(TBL), b(TBL), c(TBL);
     make_tables(a.data(), b.data(), c.data(), TBL);
@@ -98,10 +98,10 @@ extern "C" void gtb_destroy(gtb_handle* h) {
     if (h->t_d82) cudaFree(h->t_d82);
     if (h->t_d0fin) cudaFree(h->t_d0fin);
     for (int k = 0; k < 8; k++) if (h->ev[k]) cudaEventDestroy(h->ev[k]);
-    for (int j = 0; j < gtb_handle::NSUB; j++) {
+    for (int j = 0; j < 2 * gtb_handle::NSUB; j++)
         for (int k = 0; k < 8; k++) if (h->sev[j][k]) cudaEventDestroy(h->sev[j][k]);
-        if (j > 0 && h->sub[j]) cudaStreamDestroy(h->sub[j]);
-    }
+    for (int j = 1; j < gtb_handle::NSUB; j++)
+        if (h->sub[j]) cudaStreamDestroy(h->sub[j]);
     if (h->st) cudaStreamDestroy(h->st);
     delete h;
 }
@@ -203,7 +203,7 @@ static gtb_status run_block(gtb_handle* h, const DevBlock& D, float scorethld,
 
     // One sub-batch [q0, q0 + np): plan, carve one allocation, upload the
     // offsets, launch the stage sequence and the result copies on stream st.
-    auto launch_sub = [&](long long q0, int np, int j) -> gtb_status {
+    auto launch_sub = [&](long long q0, int np, int j, int evset) -> gtb_status {
         cudaStream_t st = h->sub[j];
         std::vector<long long>& ov = offv[j];
         ov.assign(4 * (size_t)(np + 1), 0);
@@ -255,7 +255,7 @@ static gtb_status run_block(gtb_handle* h, const DevBlock& D, float scorethld,
         T.launches = &h->launches;
         CK(cudaMemcpyAsync(offs, off_bt, 4 * (size_t)(np + 1) * sizeof(long long), cudaMemcpyHostToDevice, st));
         launch_stages(B, T, o.refinement, o.depth, o.convergence, o.prescore, o.referenced,
-                      scorethld, st, h->sev[j]);
+                      scorethld, st, h->sev[evset]);
         CK(cudaGetLastError());
         if (h_alndata)
             CK(cudaMemcpyAsync(h_alndata + q0 * 16, T.out, (size_t)np * 16 * sizeof(float), cudaMemcpyDefault, st));
@@ -266,6 +266,17 @@ static gtb_status run_block(gtb_handle* h, const DevBlock& D, float scorethld,
         if (strings)
             CK(cudaMemcpyAsync(hstr + (*hstroff)[q0], T.str, (size_t)off_str[np], cudaMemcpyDeviceToHost, st));
         CK(cudaFreeAsync(base, st));
+        return GTB_OK;
+    };
+
+    auto add_times = [&](int j) -> gtb_status {
+        cudaEvent_t* ev = h->sev[j];
+        float ms = 0.f;
+        CK(cudaEventElapsedTime(&ms, ev[0], ev[1])); tsum[0] += ms;
+        CK(cudaEventElapsedTime(&ms, ev[1], ev[2])); tsum[1] += ms;
+        CK(cudaEventElapsedTime(&ms, ev[2], ev[3])); tsum[2] += ms;
+        CK(cudaEventElapsedTime(&ms, ev[3], ev[4])); tsum[5] += ms;
+        CK(cudaEventElapsedTime(&ms, ev[0], ev[4])); tsum[6] += ms;
         return GTB_OK;
     };
 
@@ -285,28 +296,25 @@ static gtb_status run_block(gtb_handle* h, const DevBlock& D, float scorethld,
             snprintf(h->err, sizeof(h->err), "pair (%lld) needs %zu bytes > budget %zu", p0, used, budget);
             return GTB_ERR_NOMEM;
         }
-        // split into concurrent sub-batches of at least 16k pairs
+        // split into sub-batches of at least 16k pairs, in up to two waves
+        // over the streams: the narrow stage-2 launches of the first wave
+        // overlap the wide stage-1 launches of the second
         long long nb = p1 - p0;
-        int nsub = (int)std::min<long long>(gtb_handle::NSUB, std::max<long long>(1, nb / 16384));
+        int nsub = (int)std::min<long long>(2 * gtb_handle::NSUB, std::max<long long>(1, nb / 16384));
         long long q0 = p0;
         for (int j = 0; j < nsub; j++) {
             long long q1 = p0 + nb * (j + 1) / nsub;
-            gtb_status s = launch_sub(q0, (int)(q1 - q0), j);
+            gtb_status s = launch_sub(q0, (int)(q1 - q0), j % gtb_handle::NSUB, j);
             if (s != GTB_OK) {
-                for (int k = 0; k < nsub; k++) cudaStreamSynchronize(h->sub[k]);
+                for (int k = 0; k < gtb_handle::NSUB; k++) cudaStreamSynchronize(h->sub[k]);
                 return s;
             }
             q0 = q1;
         }
+        for (int j = 0; j < std::min(nsub, gtb_handle::NSUB); j++) CK(cudaStreamSynchronize(h->sub[j]));
         for (int j = 0; j < nsub; j++) {
-            CK(cudaStreamSynchronize(h->sub[j]));
-            cudaEvent_t* ev = h->sev[j];
-            float ms = 0.f;
-            CK(cudaEventElapsedTime(&ms, ev[0], ev[1])); tsum[0] += ms;
-            CK(cudaEventElapsedTime(&ms, ev[1], ev[2])); tsum[1] += ms;
-            CK(cudaEventElapsedTime(&ms, ev[2], ev[3])); tsum[2] += ms;
-            CK(cudaEventElapsedTime(&ms, ev[3], ev[4])); tsum[5] += ms;
-            CK(cudaEventElapsedTime(&ms, ev[0], ev[4])); tsum[6] += ms;
+            gtb_status s = add_times(j);
+            if (s != GTB_OK) return s;
         }
         p0 = p1;
     }

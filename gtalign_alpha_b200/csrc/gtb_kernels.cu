@@ -629,13 +629,15 @@ __device__ __forceinline__ float lane_pass(const PairGeom& G, int kind, int k0, 
     return __fadd_rn(ss, sc);
 }
 
-constexpr int RF_LPP = 16;                 // lanes per pair
-constexpr int RF_PPW = 32 / RF_LPP;        // pairs per warp
+// RF_LPP lanes per pair: 16 (two pairs per warp) where most pairs of a
+// batch take part; 32 where few do (after the --pre-score filter), which
+// shortens the launches whose time is that of their slowest pair.
 constexpr int RF_WARPS = 4;
-constexpr int RF_PAIRS = RF_PPW * RF_WARPS;  // pairs per CTA
 
-template <int MODE>
+template <int MODE, int RF_LPP>
 __global__ void __launch_bounds__(RF_WARPS * 32) k_refine(Blk B, Bat T) {
+    constexpr int RF_PPW = 32 / RF_LPP;        // pairs per warp
+    constexpr int RF_PAIRS = RF_PPW * RF_WARPS;  // pairs per CTA
     __shared__ float s_last[16 * RF_WARPS * 32];   // previous iteration's sums
     __shared__ float s_tb[12 * RF_WARPS * 32];     // best transform of the current variant
     __shared__ float s_tbest[12 * RF_WARPS * 32];  // best transform over the lane's variants
@@ -864,21 +866,27 @@ __global__ void __launch_bounds__(RF_WARPS * 32) k_refine(Blk B, Bat T) {
     }
 }
 
-void launch_refine(int mode, const Blk& B, const Bat& T, cudaStream_t st) {
+template <int LPP>
+static void launch_refine_k(int mode, const Blk& B, const Bat& T, cudaStream_t st) {
+    const int ng = (T.np + (32 / LPP) * RF_WARPS - 1) / ((32 / LPP) * RF_WARPS), nt = RF_WARPS * 32;
+    switch (mode) {
+        case RM_INIT:  k_refine<RM_INIT, LPP><<<ng, nt, 0, st>>>(B, T); break;
+        case RM_DP:    k_refine<RM_DP, LPP><<<ng, nt, 0, st>>>(B, T); break;
+        case RM_FIN1:  k_refine<RM_FIN1, LPP><<<ng, nt, 0, st>>>(B, T); break;
+        case RM_FIN2:  k_refine<RM_FIN2, LPP><<<ng, nt, 0, st>>>(B, T); break;
+        case RM_PROD1: k_refine<RM_PROD1, LPP><<<ng, nt, 0, st>>>(B, T); break;
+        case RM_PROD2: k_refine<RM_PROD2, LPP><<<ng, nt, 0, st>>>(B, T); break;
+    }
+}
+
+void launch_refine(int mode, const Blk& B, const Bat& T, cudaStream_t st, bool few) {
     cudaMemsetAsync(T.rhist, 0, (RL_NB + 1) * sizeof(int), st);
     const int nb = (T.np + 255) / 256;
     k_rlist_count<<<nb, 256, 0, st>>>(B, T, mode);
     k_rlist_scan<<<1, 1024, 0, st>>>(T);
     k_rlist_fill<<<nb, 256, 0, st>>>(B, T, mode);
-    const int ng = (T.np + RF_PAIRS - 1) / RF_PAIRS, nt = RF_WARPS * 32;
-    switch (mode) {
-        case RM_INIT:  k_refine<RM_INIT><<<ng, nt, 0, st>>>(B, T); break;
-        case RM_DP:    k_refine<RM_DP><<<ng, nt, 0, st>>>(B, T); break;
-        case RM_FIN1:  k_refine<RM_FIN1><<<ng, nt, 0, st>>>(B, T); break;
-        case RM_FIN2:  k_refine<RM_FIN2><<<ng, nt, 0, st>>>(B, T); break;
-        case RM_PROD1: k_refine<RM_PROD1><<<ng, nt, 0, st>>>(B, T); break;
-        case RM_PROD2: k_refine<RM_PROD2><<<ng, nt, 0, st>>>(B, T); break;
-    }
+    if (few) launch_refine_k<32>(mode, B, T, st);
+    else launch_refine_k<16>(mode, B, T, st);
     if (T.launches) (*T.launches) += 4;
 }
 
@@ -1278,11 +1286,13 @@ void launch_stages(const Blk& B, const Bat& T, int refinement, int depth, int co
                    cudaEvent_t* ev) {
     auto mark = [&](int k) { if (ev) cudaEventRecord(ev[k], st); };
     // DPRefine: MpStage1.cpp:466-517
-    auto dprefine = [&](int gap0, int prescreen, int maxit) {
+    // after the stage-1 --pre-score filter only a small share of pairs is left
+    const bool few = 0.0f < prescore;
+    auto dprefine = [&](int gap0, int prescreen, int maxit, bool fewp) {
         for (int dpi = 0; dpi < maxit; dpi++) {
             launch_dp(B, T, DP_TFM_IBEST, gap0, gap0 ? 0.0f : -0.6f, 0, 0, 0, st);
             launch_btck(B, T, 0, st);
-            launch_refine(RM_DP, B, T, st);
+            launch_refine(RM_DP, B, T, st, fewp);
             launch_post(B, T, dpi, maxit, prescreen, prescore, st);
         }
     };
@@ -1290,30 +1300,30 @@ void launch_stages(const Blk& B, const Bat& T, int refinement, int depth, int co
     launch_init(B, T, st);
     launch_findfrag(B, T, st);
     mark(1);
-    launch_refine(RM_INIT, B, T, st);
+    launch_refine(RM_INIT, B, T, st, false);
     mark(2);
-    dprefine(1, 1, 2);
+    dprefine(1, 1, 2, false);
     // two stage-2 passes: MpStage2.h:63-83, CuBatch.cu:627-650
     for (int call = 0; call < 2; call++) {
         int gap0 = call == 1;
         launch_dp(B, T, DP_TFM_GRAND, gap0, gap0 ? 0.0f : -1.0f, !gap0, !gap0, 1, st);
         launch_btck(B, T, 0, st);
-        launch_refine(RM_DP, B, T, st);
-        dprefine(0, 0, 2);
-        dprefine(1, 0, call == 0 ? 2 : convergence);
+        launch_refine(RM_DP, B, T, st, few);
+        dprefine(0, 0, 2, few);
+        dprefine(1, 0, call == 0 ? 2 : convergence, few);
         if (call == 1 && 0.0f < scorethld) launch_lowscore(B, T, scorethld, st);
     }
     mark(3);
     // final stage: MpStageFin.h:63-96
     launch_dp(B, T, DP_TFM_GRAND, 1, 0.0f, 0, 0, 1, st);
     launch_btck(B, T, 0, st);
-    launch_refine(RM_FIN1, B, T, st);
-    if (!(depth == 3 || refinement == 0)) launch_refine(RM_FIN2, B, T, st);
+    launch_refine(RM_FIN1, B, T, st, few);
+    if (!(depth == 3 || refinement == 0)) launch_refine(RM_FIN2, B, T, st, few);
     launch_dp(B, T, DP_TFM_GRAND, 1, 0.0f, 0, 0, 1, st);
     launch_btck(B, T, 1, st);
     launch_alnstr(B, T, st);
-    launch_refine(RM_PROD1, B, T, st);
-    launch_refine(RM_PROD2, B, T, st);
+    launch_refine(RM_PROD1, B, T, st, few);
+    launch_refine(RM_PROD2, B, T, st, few);
     launch_final(B, T, referenced, st);
     mark(4);
 }

@@ -59,7 +59,8 @@ void launch_secstr(char* ss, const float* x, const float* y, const float* z,
                    cudaStream_t st, long long* launches);
 void launch_init(const Blk& B, const Bat& T, cudaStream_t st);
 void launch_findfrag(const Blk& B, const Bat& T, cudaStream_t st);
-void launch_refine(int mode, const Blk& B, const Bat& T, cudaStream_t st);
+// few: most pairs of the batch are already filtered out (32 lanes per pair)
+void launch_refine(int mode, const Blk& B, const Bat& T, cudaStream_t st, bool few);
 // skipmode 0: skip LOWTMSC|SCOREDP (plain), 1: skip LOWTMSC only
 void launch_dp(const Blk& B, const Bat& T, int tfmsrc, int gap0, float gcost, int usess,
                int dpscan, int skipmode, cudaStream_t st);
