@@ -143,6 +143,7 @@ struct DevBlock {
     int nq, nr;
     const int *qlen, *rlen, *qoff, *roff, *qmol, *rmol;
     const float *qx, *qy, *qz, *rx, *ry, *rz;
+    const float4 *q4, *r4;
     const unsigned char *qa, *ra;
     char *qs, *rs;
     std::vector<int> hqlen, hrlen;
@@ -179,6 +180,7 @@ static gtb_status run_block(gtb_handle* h, const DevBlock& D, float scorethld,
     B.nq = D.nq; B.nr = D.nr;
     B.qlen = D.qlen; B.rlen = D.rlen; B.qoff = D.qoff; B.roff = D.roff;
     B.qx = D.qx; B.qy = D.qy; B.qz = D.qz; B.rx = D.rx; B.ry = D.ry; B.rz = D.rz;
+    B.q4 = D.q4; B.r4 = D.r4; B.q4off = D.qoff; B.r4off = D.roff;
     B.qa = D.qa; B.ra = D.ra; B.qs = D.qs; B.rs = D.rs; B.qmol = D.qmol; B.rmol = D.rmol;
     B.qmax = *std::max_element(D.hqlen.begin(), D.hqlen.end());
     B.qmin = *std::min_element(D.hqlen.begin(), D.hqlen.end());
@@ -388,6 +390,7 @@ struct gtb_block {
     char* dbase = nullptr;
     int *dlen = nullptr, *doff = nullptr, *dmol = nullptr;
     float *x = nullptr, *y = nullptr, *z = nullptr;
+    float4* c4 = nullptr;
     unsigned char* rsd = nullptr;
     char* ss = nullptr;
 };
@@ -402,11 +405,13 @@ static gtb_status upload_block(gtb_handle* h, const HostSoA& S, gtb_block* b) {
     size_t ol = carve(S.n * 4), oo = carve(S.n * 4), om = carve(S.n * 4);
     size_t ox = carve(S.npos * 4), oy = carve(S.npos * 4), oz = carve(S.npos * 4);
     size_t oa = carve(S.npos), os = carve(S.npos);
+    size_t o4 = carve(S.npos * 16);
     CK(cudaMalloc((void**)&b->dbase, sz));
     char* d = b->dbase;
     b->dlen = (int*)(d + ol); b->doff = (int*)(d + oo); b->dmol = (int*)(d + om);
     b->x = (float*)(d + ox); b->y = (float*)(d + oy); b->z = (float*)(d + oz);
     b->rsd = (unsigned char*)(d + oa); b->ss = d + os;
+    b->c4 = (float4*)(d + o4);
     CK(cudaMemcpyAsync(b->dlen, S.len, S.n * 4, cudaMemcpyHostToDevice, st));
     CK(cudaMemcpyAsync(b->doff, S.off.data(), S.n * 4, cudaMemcpyHostToDevice, st));
     CK(cudaMemcpyAsync(b->dmol, S.mol.data(), S.n * 4, cudaMemcpyHostToDevice, st));
@@ -415,6 +420,7 @@ static gtb_status upload_block(gtb_handle* h, const HostSoA& S, gtb_block* b) {
     CK(cudaMemcpyAsync(b->z, S.z, S.npos * 4, cudaMemcpyHostToDevice, st));
     CK(cudaMemcpyAsync(b->rsd, S.rsd, S.npos, cudaMemcpyHostToDevice, st));
     long long nl = 0;
+    launch_pack4(b->c4, b->x, b->y, b->z, S.npos, st);
     launch_secstr(b->ss, b->x, b->y, b->z, b->dlen, b->doff, b->dmol, b->n, st, &nl);
     CK(cudaGetLastError());
     return GTB_OK;
@@ -454,6 +460,7 @@ static DevBlock make_devblock(const gtb_block* Q, const gtb_block* R) {
     D.qlen = Q->dlen; D.qoff = Q->doff; D.qmol = Q->dmol;
     D.rlen = R->dlen; D.roff = R->doff; D.rmol = R->dmol;
     D.qx = Q->x; D.qy = Q->y; D.qz = Q->z; D.rx = R->x; D.ry = R->y; D.rz = R->z;
+    D.q4 = Q->c4; D.r4 = R->c4;
     D.qa = Q->rsd; D.ra = R->rsd; D.qs = Q->ss; D.rs = R->ss;
     D.hqlen = Q->len; D.hrlen = R->len;
     return D;

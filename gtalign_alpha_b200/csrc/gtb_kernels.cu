@@ -85,6 +85,34 @@ void launch_secstr(char* ss, const float* x, const float* y, const float* z,
 }
 
 // ---------------------------------------------------------------------------
+__global__ void k_pack4(float4* out, const float* x, const float* y, const float* z, long long n) {
+    long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[i] = make_float4(x[i], y[i], z[i], 0.f);
+}
+
+void launch_pack4(float4* out, const float* x, const float* y, const float* z, long long n,
+                  cudaStream_t st) {
+    if (n <= 0) return;
+    k_pack4<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(out, x, y, z, n);
+}
+
+__global__ void k_pack4s(float4* out, const float* x, const float* y, const float* z,
+                         const int* off, const int* len, const int* coff, int n) {
+    int si = blockIdx.x;
+    if (si >= n) return;
+    int o = off[si], L = len[si], c = coff[si];
+    for (int p = threadIdx.x; p < L; p += blockDim.x)
+        out[c + p] = make_float4(x[o + p], y[o + p], z[o + p], 0.f);
+}
+
+void launch_pack4_structs(float4* out, const float* x, const float* y, const float* z,
+                          const int* off, const int* len, const int* coff, int n,
+                          cudaStream_t st) {
+    if (n <= 0) return;
+    k_pack4s<<<n, 128, 0, st>>>(out, x, y, z, off, len, coff, n);
+}
+
+// ---------------------------------------------------------------------------
 // pair initialisation: MpStage1.cpp:28-167
 __global__ void k_init(Blk B, Bat T) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -117,8 +145,8 @@ void launch_init(const Blk& B, const Bat& T, cudaStream_t st) {
 // (The aligned space is read from the coordinates the traceback stored
 // with each aligned pair, 6 floats per pair in traceback order.)
 struct PairGeom {
-    const float *qx, *qy, *qz, *rx, *ry, *rz;
-    const float2* alc;    // aligned coordinates, reverse order; null: diagonal
+    const float4 *q4, *r4;  // the pair's structures, (x, y, z, 0) per residue
+    const float2* alc;      // aligned coordinates, reverse order; null: diagonal
     int q0, r0, n;
     __device__ __forceinline__ void at(int k, float& a, float& b, float& c,
                                        float& d, float& e, float& f) const {
@@ -127,9 +155,8 @@ struct PairGeom {
             float2 u = __ldg(p), v = __ldg(p + 1), w = __ldg(p + 2);
             a = u.x; b = u.y; c = v.x; d = v.y; e = w.x; f = w.y;
         } else {
-            int q = q0 + k, r = r0 + k;
-            a = __ldg(qx + q); b = __ldg(qy + q); c = __ldg(qz + q);
-            d = __ldg(rx + r); e = __ldg(ry + r); f = __ldg(rz + r);
+            float4 u = __ldg(q4 + q0 + k), v = __ldg(r4 + r0 + k);
+            a = u.x; b = u.y; c = u.z; d = v.x; e = v.y; f = v.z;
         }
     }
 };
@@ -383,8 +410,7 @@ __global__ void __launch_bounds__(128) k_findfrag(Blk B, Bat T) {
     float d0s = d0s_of(d0);
     int swap = B.symmetric && (lq < lr);
     PairGeom G;
-    G.qx = B.qx + B.qoff[qi]; G.qy = B.qy + B.qoff[qi]; G.qz = B.qz + B.qoff[qi];
-    G.rx = B.rx + B.roff[ri]; G.ry = B.ry + B.roff[ri]; G.rz = B.rz + B.roff[ri];
+    G.q4 = B.q4 + B.q4off[qi]; G.r4 = B.r4 + B.r4off[ri];
     G.alc = nullptr;
     float lbest = 0.f;
     int lsi = 0x7fffffff;
@@ -658,8 +684,7 @@ __global__ void __launch_bounds__(RF_WARPS * 32) k_refine(Blk B, Bat T) {
     int ml = lq < lr ? lq : lr;
     int swap = B.symmetric && (lq < lr);
     PairGeom G;
-    G.qx = B.qx + B.qoff[qi]; G.qy = B.qy + B.qoff[qi]; G.qz = B.qz + B.qoff[qi];
-    G.rx = B.rx + B.roff[ri]; G.ry = B.ry + B.roff[ri]; G.rz = B.rz + B.roff[ri];
+    G.q4 = B.q4 + B.q4off[qi]; G.r4 = B.r4 + B.r4off[ri];
     if (MODE == RM_INIT) {
         int sq = T.seedq[i], sr = T.seedr[i];
         G.alc = nullptr;
@@ -923,9 +948,7 @@ __global__ void __launch_bounds__(128) k_dp(Blk B, Bat T, int tfmsrc, float gcos
     const float* qx = B.qx + B.qoff[qi];
     const float* qy = B.qy + B.qoff[qi];
     const float* qz = B.qz + B.qoff[qi];
-    const float* rx = B.rx + B.roff[ri];
-    const float* ry = B.ry + B.roff[ri];
-    const float* rz = B.rz + B.roff[ri];
+    const float4* r4 = B.r4 + B.r4off[ri];
     const char* qs = B.qs + B.qoff[qi];
     const char* rs = B.rs + B.roff[ri];
     float* row = T.row + T.off_row[i];
@@ -964,7 +987,8 @@ __global__ void __launch_bounds__(128) k_dp(Blk B, Bat T, int tfmsrc, float gcos
             if (lane == 0) upv = (j < lr) ? up0 : 0.f;
             unsigned bits = 0u;
             if (j >= 0 && j < lr && nv > 0) {
-                float cx = __ldg(rx + j), cy = __ldg(ry + j), cz = __ldg(rz + j);
+                float4 c4 = __ldg(r4 + j);
+                float cx = c4.x, cy = c4.y, cz = c4.z;
                 char css = usess ? rs[j] : 0;
                 float up = upv, dg = uplast;
 #pragma unroll
@@ -1031,8 +1055,8 @@ __global__ void k_btck(Blk B, Bat T, int constrained) {
     const long long sw = bt_strip_words(lr);
     float t[12];
     float d82 = B.t_d82[ml];
-    const float *qx = B.qx + B.qoff[qi], *qy = B.qy + B.qoff[qi], *qz = B.qz + B.qoff[qi];
-    const float *rx = B.rx + B.roff[ri], *ry = B.ry + B.roff[ri], *rz = B.rz + B.roff[ri];
+    const float4* q4 = B.q4 + B.q4off[qi];
+    const float4* r4 = B.r4 + B.r4off[ri];
     if (constrained) {
 #pragma unroll
         for (int f = 0; f < 12; f++) t[f] = T.tfm_gr[i * 12 + f];
@@ -1044,7 +1068,8 @@ __global__ void k_btck(Blk B, Bat T, int constrained) {
         int b = (int)((w >> (2 * DP_R * (tt % DP_SPW) + 2 * (yy % DP_R))) & 3u);
         if (b == BT_UP) { y--; continue; }
         if (b == BT_LEFT) { x--; continue; }
-        float cqx = qx[y], cqy = qy[y], cqz = qz[y], crx = rx[x], cry = ry[x], crz = rz[x];
+        float4 cq = __ldg(q4 + y), cr = __ldg(r4 + x);
+        float cqx = cq.x, cqy = cq.y, cqz = cq.z, crx = cr.x, cry = cr.y, crz = cr.z;
         bool keep = true;
         if (constrained) keep = dist2_tf(t, cqx, cqy, cqz, crx, cry, crz) <= d82;
         if (keep) {

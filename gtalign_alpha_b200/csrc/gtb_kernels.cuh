@@ -26,6 +26,8 @@ struct Blk {
     const int *qlen, *rlen;          // lengths
     const int *qoff, *roff;          // first-residue offsets
     const float *qx, *qy, *qz, *rx, *ry, *rz;
+    const float4 *q4, *r4;           // the same coordinates as (x, y, z, 0),
+    const int *q4off, *r4off;        // first residue of each structure in q4/r4
     const unsigned char *qa, *ra;    // residue letters
     const char *qs, *rs;             // secondary structure
     const int *qmol, *rmol;          // molecule type per structure
@@ -57,6 +59,14 @@ enum DpTfm { DP_TFM_IBEST = 0, DP_TFM_GRAND = 1 };
 void launch_secstr(char* ss, const float* x, const float* y, const float* z,
                    const int* len, const int* off, const int* mol, int nstr,
                    cudaStream_t st, long long* launches);
+// (x, y, z, 0) copies of n coordinates, for single 16-byte loads in the passes
+void launch_pack4(float4* out, const float* x, const float* y, const float* z, long long n,
+                  cudaStream_t st);
+// the same per structure into a back-to-back copy: structure i's residues
+// [off[i], off[i]+len[i]) go to out[coff[i] ...]
+void launch_pack4_structs(float4* out, const float* x, const float* y, const float* z,
+                          const int* off, const int* len, const int* coff, int n,
+                          cudaStream_t st);
 void launch_init(const Blk& B, const Bat& T, cudaStream_t st);
 void launch_findfrag(const Blk& B, const Bat& T, cudaStream_t st);
 // few: most pairs of the batch are already filtered out (32 lanes per pair)

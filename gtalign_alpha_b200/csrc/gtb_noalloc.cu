@@ -58,6 +58,8 @@ static std::mutex g_setup_mutex;
 static float h_tbl[3][TBLN];
 // host copies of the per-pair offsets (4 arrays of up to MAX_PAIRS+1 entries)
 static long long h_offs[4 * (GTB_NOALLOC_MAX_PAIRS + 1)];
+// host copies of the back-to-back residue offsets of the (x, y, z, 0) copies
+static int h_coff[2 * (GTB_NOALLOC_MAX_PAIRS + 1)];
 
 size_t al256(size_t x) { return (x + 255) & ~(size_t)255; }
 
@@ -157,6 +159,12 @@ extern "C" gtb_status gtb_process_block_noalloc(int device, const gtb_options* o
     size_t o_row = carve((size_t)orow[np] * sizeof(float));
     size_t o_aln = carve((size_t)oaln[np] * sizeof(unsigned));
     size_t o_alc = carve((size_t)oaln[np] * 6 * sizeof(float));
+    long long qres = 0, rres = 0;
+    for (int i = 0; i < q->n; i++) { h_coff[i] = (int)qres; qres += q->lens[i]; }
+    for (int i = 0; i < r->n; i++) { h_coff[q->n + i] = (int)rres; rres += r->lens[i]; }
+    size_t o_q4 = carve((size_t)qres * sizeof(float4));
+    size_t o_r4 = carve((size_t)rres * sizeof(float4));
+    size_t o_co = carve((size_t)(q->n + r->n) * sizeof(int));
     size_t o_rl = carve((size_t)np * sizeof(int));
     size_t o_rh = carve((size_t)4097 * sizeof(int));
     if (sz > SCRATCH_BYTES) {
@@ -179,6 +187,9 @@ extern "C" gtb_status gtb_process_block_noalloc(int device, const gtb_options* o
     B.nq = q->n; B.nr = r->n;
     B.qlen = q->d_lens; B.rlen = r->d_lens; B.qoff = q->d_offs; B.roff = r->d_offs;
     B.qx = q->d_x; B.qy = q->d_y; B.qz = q->d_z; B.rx = r->d_x; B.ry = r->d_y; B.rz = r->d_z;
+    int* coff = (int*)(base + o_co);
+    B.q4 = (const float4*)(base + o_q4); B.r4 = (const float4*)(base + o_r4);
+    B.q4off = coff; B.r4off = coff + q->n;
     B.qa = q->d_rsd; B.ra = r->d_rsd; B.qs = q->d_ss; B.rs = r->d_ss;
     B.qmol = q->d_mol; B.rmol = r->d_mol;
     B.qmax = qmax; B.qmin = qmin; B.rmax = rmax; B.rmin = rmin;
@@ -206,8 +217,12 @@ extern "C" gtb_status gtb_process_block_noalloc(int device, const gtb_options* o
 
     // the host offsets are copied from the static host array (no allocation)
     e = cudaMemcpyAsync(offs, h_offs, (size_t)(np + 1) * 4 * sizeof(long long), cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(coff, h_coff, (size_t)(q->n + r->n) * sizeof(int), cudaMemcpyHostToDevice, st);
     if (e == cudaSuccess) {
         long long nl = 0;
+        launch_pack4_structs((float4*)(base + o_q4), q->d_x, q->d_y, q->d_z, q->d_offs, q->d_lens, coff, q->n, st);
+        launch_pack4_structs((float4*)(base + o_r4), r->d_x, r->d_y, r->d_z, r->d_offs, r->d_lens, coff + q->n, r->n, st);
         launch_secstr(q->d_ss, q->d_x, q->d_y, q->d_z, q->d_lens, q->d_offs, q->d_mol, q->n, st, &nl);
         launch_secstr(r->d_ss, r->d_x, r->d_y, r->d_z, r->d_lens, r->d_offs, r->d_mol, r->n, st, &nl);
         launch_stages(B, T, opts->refinement, opts->depth, opts->convergence, opts->prescore,
