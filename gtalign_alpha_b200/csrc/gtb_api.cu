@@ -271,6 +271,11 @@ static gtb_status run_block(gtb_handle* h, const DevBlock& D, float scorethld,
         return GTB_OK;
     };
 
+    // the sub-batch streams start after everything queued on the handle's
+    // stream so far (block uploads, secondary structure, float4 copies)
+    CK(cudaEventRecord(h->ev[7], h->st));
+    for (int j = 1; j < gtb_handle::NSUB; j++) CK(cudaStreamWaitEvent(h->sub[j], h->ev[7], 0));
+
     auto add_times = [&](int j) -> gtb_status {
         cudaEvent_t* ev = h->sev[j];
         float ms = 0.f;
@@ -391,6 +396,7 @@ struct gtb_block {
     int *dlen = nullptr, *doff = nullptr, *dmol = nullptr;
     float *x = nullptr, *y = nullptr, *z = nullptr;
     float4* c4 = nullptr;
+    cudaStream_t st = nullptr;       // stream of the allocation and of the free
     unsigned char* rsd = nullptr;
     char* ss = nullptr;
 };
@@ -406,7 +412,9 @@ static gtb_status upload_block(gtb_handle* h, const HostSoA& S, gtb_block* b) {
     size_t ox = carve(S.npos * 4), oy = carve(S.npos * 4), oz = carve(S.npos * 4);
     size_t oa = carve(S.npos), os = carve(S.npos);
     size_t o4 = carve(S.npos * 16);
-    CK(cudaMalloc((void**)&b->dbase, sz));
+    // from the device's memory pool (kept between calls), in stream order
+    CK(cudaMallocAsync((void**)&b->dbase, sz, st));
+    b->st = st;
     char* d = b->dbase;
     b->dlen = (int*)(d + ol); b->doff = (int*)(d + oo); b->dmol = (int*)(d + om);
     b->x = (float*)(d + ox); b->y = (float*)(d + oy); b->z = (float*)(d + oz);
@@ -428,7 +436,7 @@ static gtb_status upload_block(gtb_handle* h, const HostSoA& S, gtb_block* b) {
 
 static void free_block(gtb_block* b) {
     if (!b) return;
-    if (b->dbase) cudaFree(b->dbase);
+    if (b->dbase) cudaFreeAsync(b->dbase, b->st);
     delete b;
 }
 

@@ -300,7 +300,12 @@ __device__ float seed_score_ext(const PairGeom& G, const float* tfm, float d02, 
             G.at(k, qx, qy, qz, rx, ry, rz);
             float d = dist2_tf(tfm, qx, qy, qz, rx, ry, rz);
             sb = __fadd_rn(sb, tmterm(d02, d));
-            track3(1, d, m1, m2, m3);
+            {   // three smallest distinct distances, branch-free
+                bool c1 = d < m1, c2 = d > m1 && d < m2, c3 = d > m2 && d < m3;
+                m3 = (c1 || c2) ? m2 : (c3 ? d : m3);
+                m2 = c1 ? m1 : (c2 ? d : m2);
+                m1 = c1 ? d : m1;
+            }
             if (d < kd[SEED_K - 1]) {
                 // insert (d, k) keeping kd ascending
                 float cd = d;

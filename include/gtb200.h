@@ -125,6 +125,7 @@ gtb_status gtb_process_block(gtb_handle* h, float scorethld,
 typedef struct gtb_block gtb_block;
 gtb_status gtb_block_upload(gtb_handle* h, char* const* pmbeg, char* const* pmend,
                             gtb_block** out);
+/* Free a block with the handle that uploaded it, before gtb_destroy. */
 void gtb_block_free(gtb_handle* h, gtb_block* b);
 gtb_status gtb_process_resident(gtb_handle* h, float scorethld, const gtb_block* queries,
                                 const gtb_block* refs, float* d_alndata, float* d_tfm,
