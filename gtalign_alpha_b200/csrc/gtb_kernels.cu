@@ -10,8 +10,8 @@
 //    fragment length) variants in turn; the warp reduces (max score, lowest
 //    variant index) with shuffles.  The distance-threshold covariance pass
 //    of iteration k+1 is fused into the scoring pass of iteration k.
-//  * DP: one warp per pair; the warp sweeps strips of DP_ROWS rows along
-//    anti-diagonals (DP_R rows per lane, register-blocked), left/up/diagonal
+//  * DP: one warp per pair; the warp sweeps strips of 32*R rows along
+//    anti-diagonals (R rows per lane, register-blocked), left/up/diagonal
 //    values move between lanes by shuffles, each lane packs the 2-bit
 //    directions of its cells into traceback words.
 //  * traceback, alignment rows, bookkeeping: one thread per pair.
@@ -621,13 +621,17 @@ enum PassKind {
 
 // One pass of one lane.  Blocks of BLK positions are the absolute blocks
 // of the position space for every kind, so lanes fold together.
-__device__ __forceinline__ float lane_pass(const PairGeom& G, int kind, int k0, int k1,
-                                           const float* tfm, float d02, int chk, float d82,
-                                           float thr, int m3on, float* v, float& m3out) {
+// M3 / FR / SC: whether any lane of the warp tracks the three smallest
+// distances, covers a fragment, or scores in this pass; the code for what
+// no lane does is left out.
+template <bool M3, bool FR, bool SC>
+__device__ __forceinline__ float lane_pass_t(const PairGeom& G, int kind, int k0, int k1,
+                                             const float* tfm, float d02, int chk, float d82,
+                                             float thr, int m3on, float* v, float& m3out) {
     float ss = 0.f, sc = 0.f, sb = 0.f;
     float m1 = LARGEDST, m2 = LARGEDST, m3 = LARGEDST;
-    const bool frag = kind == PK_FRAG;
-    const bool scr = kind == PK_SCORE || kind == PK_GSCORE;
+    const bool frag = FR && kind == PK_FRAG;
+    const bool scr = SC && (kind == PK_SCORE || kind == PK_GSCORE);
     const bool cov = kind == PK_SCORE || kind == PK_EXT;
     const int n = kind == PK_IDLE ? 0 : (frag ? k1 : G.n);
     CovAcc a;
@@ -640,13 +644,17 @@ __device__ __forceinline__ float lane_pass(const PairGeom& G, int kind, int k0, 
             G.at(k, qx, qy, qz, rx, ry, rz);
             float d = dist2_tf(tfm, qx, qy, qz, rx, ry, rz);
             // branch-free: adding +0 and zero coordinates leaves the sums unchanged
-            float tm = tmterm(d02, d);
-            sb = __fadd_rn(sb, (scr && (!chk || d <= d82)) ? tm : 0.f);
-            bool c1 = m3on && d < m1, c2 = m3on && d < m2, c3 = m3on && d < m3;
-            m3 = c2 ? m2 : (c3 ? d : m3);
-            m2 = c1 ? m1 : (c2 ? d : m2);
-            m1 = c1 ? d : m1;
-            bool inc = frag ? (k0 <= k) : (cov && d <= thr);
+            if (SC) {
+                float tm = tmterm(d02, d);
+                sb = __fadd_rn(sb, (scr && (!chk || d <= d82)) ? tm : 0.f);
+            }
+            if (M3) {
+                bool c1 = m3on && d < m1, c2 = m3on && d < m2, c3 = m3on && d < m3;
+                m3 = c2 ? m2 : (c3 ? d : m3);
+                m2 = c1 ? m1 : (c2 ? d : m2);
+                m1 = c1 ? d : m1;
+            }
+            bool inc = FR ? (frag ? (k0 <= k) : (cov && d <= thr)) : (cov && d <= thr);
             a.add(inc ? qx : 0.f, inc ? qy : 0.f, inc ? qz : 0.f,
                   inc ? rx : 0.f, inc ? ry : 0.f, inc ? rz : 0.f);
             a.n += inc ? 0 : -1;
@@ -658,6 +666,23 @@ __device__ __forceinline__ float lane_pass(const PairGeom& G, int kind, int k0, 
     a.final(v);
     m3out = m3;
     return __fadd_rn(ss, sc);
+}
+
+__device__ __forceinline__ float lane_pass(const PairGeom& G, int kind, int k0, int k1,
+                                           const float* tfm, float d02, int chk, float d82,
+                                           float thr, int m3on, float* v, float& m3out) {
+    const unsigned FULL = 0xffffffffu;
+    const bool sc = __any_sync(FULL, kind == PK_SCORE || kind == PK_GSCORE);
+    const bool m3 = __any_sync(FULL, kind == PK_SCORE && m3on);
+    const bool fr = __any_sync(FULL, kind == PK_FRAG);
+    if (m3)
+        return fr ? lane_pass_t<true, true, true>(G, kind, k0, k1, tfm, d02, chk, d82, thr, m3on, v, m3out)
+                  : lane_pass_t<true, false, true>(G, kind, k0, k1, tfm, d02, chk, d82, thr, m3on, v, m3out);
+    if (sc)
+        return fr ? lane_pass_t<false, true, true>(G, kind, k0, k1, tfm, d02, chk, d82, thr, m3on, v, m3out)
+                  : lane_pass_t<false, false, true>(G, kind, k0, k1, tfm, d02, chk, d82, thr, m3on, v, m3out);
+    return fr ? lane_pass_t<false, true, false>(G, kind, k0, k1, tfm, d02, chk, d82, thr, m3on, v, m3out)
+              : lane_pass_t<false, false, false>(G, kind, k0, k1, tfm, d02, chk, d82, thr, m3on, v, m3out);
 }
 
 // RF_LPP lanes per pair: 16 (two pairs per warp) where most pairs of a
@@ -922,17 +947,92 @@ void launch_refine(int mode, const Blk& B, const Bat& T, cudaStream_t st, bool f
 
 // ---------------------------------------------------------------------------
 // DP: MpDPHub.cpp:72-346 and 686-940.  One warp per pair.  Lane l holds the
-// DP_R query rows DP_ROWS*s + DP_R*l + r of strip s and, at step t of the
-// strip, computes column j = t - l of those rows (one anti-diagonal of the
-// strip per step).  The value above a lane's first row comes from lane l-1
-// (its last row, previous step) or, for lane 0, from the previous strip's
-// last row kept in `row`.  Stored values are negated when the cell was
-// reached diagonally (the reference's state encoding, MpDPHub.cpp:246-262).
+// R query rows 32*R*s + R*l + r of strip s and, at step t of the strip,
+// computes column j = t - l of those rows (one anti-diagonal of the strip
+// per step).  The value above a lane's first row comes from lane l-1 (its
+// last row, previous step) or, for lane 0, from the previous strip's last
+// row kept in `row`.  Stored values are negated when the cell was reached
+// diagonally (the reference's state encoding, MpDPHub.cpp:246-262).  Steps
+// run in groups of 16/R, one traceback word per lane and group.
+template <int R, bool gap0, bool usess>
+__device__ __forceinline__ void dp_pair(const float* t, float d02, float gcost, int lq, int lr,
+                                        const float* qx, const float* qy, const float* qz,
+                                        const float4* r4, const char* qs, const char* rs,
+                                        float* row, unsigned* bt, int lane) {
+    constexpr int ROWS = 32 * R, SPW = 16 / R;
+    const unsigned FULL = 0xffffffffu;
+    const int W = lr + 31;
+    const int ngrp = (W + SPW - 1) / SPW;
+    const int nstrips = (lq + ROWS - 1) / ROWS;
+    for (int s = 0; s < nstrips; s++) {
+        float tx[R], ty[R], tz[R], h[R];
+        char qss[R];
+        int nv = 0;  // valid rows of this lane (a prefix of its R rows)
+#pragma unroll
+        for (int r = 0; r < R; r++) {
+            int irow = s * ROWS + lane * R + r;
+            tx[r] = ty[r] = tz[r] = 0.f;
+            qss[r] = 0;
+            h[r] = 0.f;
+            if (irow < lq) {
+                xform(t, __ldg(qx + irow), __ldg(qy + irow), __ldg(qz + irow), tx[r], ty[r], tz[r]);
+                if (usess) qss[r] = qs[irow];
+                nv = r + 1;
+            }
+        }
+        float uplast = 0.f, rb = 0.f;
+        unsigned* bts = bt + (long long)s * ngrp * 32 + lane;
+        __syncwarp();
+        for (int g = 0; g < ngrp; g++) {
+            unsigned acc = 0u;
+#pragma unroll
+            for (int u = 0; u < SPW; u++) {
+                const int tt = g * SPW + u;   // steps past W find j >= lr on every lane
+                const int j = tt - lane;
+                if ((tt & 31) == 0) {
+                    int jj = tt + lane;
+                    rb = (s > 0 && jj < lr) ? row[jj] : 0.f;
+                }
+                float upv = __shfl_up_sync(FULL, h[R - 1], 1);
+                float up0 = __shfl_sync(FULL, rb, tt & 31);
+                if (lane == 0) upv = (j < lr) ? up0 : 0.f;
+                if (j >= 0 && j < lr && nv > 0) {
+                    float4 c4 = __ldg(r4 + j);
+                    char css = usess ? rs[j] : 0;
+                    float up = upv, dg = uplast;
+#pragma unroll
+                    for (int r = 0; r < R; r++) {
+                        if (r < nv) {
+                            float v = tmterm(d02, dist2(tx[r], ty[r], tz[r], c4.x, c4.y, c4.z));
+                            if (usess) v = __fadd_rn(v, __fmul_rn((float)(qss[r] == css), 0.5f));
+                            v = __fadd_rn(v, gap0 ? dg : fabsf(dg));
+                            int bk = BT_DIAG;
+                            float l = h[r];
+                            if (!gap0 && l < 0.f) l = __fsub_rn(gcost, l);
+                            if (v < l) { v = l; bk = BT_LEFT; }
+                            float uu = up;
+                            if (!gap0 && uu < 0.f) uu = __fsub_rn(gcost, uu);
+                            if (v < uu) { v = uu; bk = BT_UP; }
+                            float w = (gap0 || bk != BT_DIAG) ? v : -v;
+                            dg = h[r];   // (row r, j-1): the next row's diagonal
+                            up = w;      // (row r, j):   the next row's up
+                            h[r] = w;
+                            acc |= (unsigned)bk << (2 * R * u + 2 * r);
+                        }
+                    }
+                    if (lane == 31 && nv == R) row[j] = h[R - 1];
+                }
+                uplast = upv;
+            }
+            bts[g * 32] = acc;
+        }
+        __syncwarp();
+    }
+}
+
 template <int GAP0, int USESS>
 __global__ void __launch_bounds__(128) k_dp(Blk B, Bat T, int tfmsrc, float gcost, int dpscan,
                                             int skipmode) {
-    constexpr bool gap0 = GAP0 != 0, usess = USESS != 0;
-    const unsigned FULL = 0xffffffffu;
     const int lane = threadIdx.x & 31;
     const int i = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
     if (i >= T.np) return;
@@ -958,75 +1058,10 @@ __global__ void __launch_bounds__(128) k_dp(Blk B, Bat T, int tfmsrc, float gcos
     const char* rs = B.rs + B.roff[ri];
     float* row = T.row + T.off_row[i];
     unsigned* bt = T.bt + T.off_bt[i];
-    const int W = lr + 31;
-    const long long sw = bt_strip_words(lr);
-    const int nstrips = (lq + DP_ROWS - 1) / DP_ROWS;
-    for (int s = 0; s < nstrips; s++) {
-        float tx[DP_R], ty[DP_R], tz[DP_R], h[DP_R];
-        char qss[DP_R];
-        int nv = 0;  // valid rows of this lane (a prefix of its DP_R rows)
-#pragma unroll
-        for (int r = 0; r < DP_R; r++) {
-            int irow = s * DP_ROWS + lane * DP_R + r;
-            tx[r] = ty[r] = tz[r] = 0.f;
-            qss[r] = 0;
-            h[r] = 0.f;
-            if (irow < lq) {
-                xform(t, __ldg(qx + irow), __ldg(qy + irow), __ldg(qz + irow), tx[r], ty[r], tz[r]);
-                if (usess) qss[r] = qs[irow];
-                nv = r + 1;
-            }
-        }
-        float uplast = 0.f, rb = 0.f;
-        unsigned acc = 0u;
-        unsigned* bts = bt + s * sw + lane;
-        __syncwarp();
-        for (int tt = 0; tt < W; tt++) {
-            const int j = tt - lane;
-            if ((tt & 31) == 0) {
-                int jj = tt + lane;
-                rb = (s > 0 && jj < lr) ? row[jj] : 0.f;
-            }
-            float upv = __shfl_up_sync(FULL, h[DP_R - 1], 1);
-            float up0 = __shfl_sync(FULL, rb, tt & 31);
-            if (lane == 0) upv = (j < lr) ? up0 : 0.f;
-            unsigned bits = 0u;
-            if (j >= 0 && j < lr && nv > 0) {
-                float4 c4 = __ldg(r4 + j);
-                float cx = c4.x, cy = c4.y, cz = c4.z;
-                char css = usess ? rs[j] : 0;
-                float up = upv, dg = uplast;
-#pragma unroll
-                for (int r = 0; r < DP_R; r++) {
-                    if (r < nv) {
-                        float v = tmterm(d02, dist2(tx[r], ty[r], tz[r], cx, cy, cz));
-                        if (usess) v = __fadd_rn(v, __fmul_rn((float)(qss[r] == css), 0.5f));
-                        v = __fadd_rn(v, gap0 ? dg : fabsf(dg));
-                        int bk = BT_DIAG;
-                        float l = h[r];
-                        if (!gap0 && l < 0.f) l = __fsub_rn(gcost, l);
-                        if (v < l) { v = l; bk = BT_LEFT; }
-                        float u = up;
-                        if (!gap0 && u < 0.f) u = __fsub_rn(gcost, u);
-                        if (v < u) { v = u; bk = BT_UP; }
-                        float w = (gap0 || bk != BT_DIAG) ? v : -v;
-                        dg = h[r];   // (row r, j-1): the next row's diagonal
-                        up = w;      // (row r, j):   the next row's up
-                        h[r] = w;
-                        bits |= (unsigned)bk << (2 * r);
-                    }
-                }
-                if (lane == 31 && nv == DP_R) row[j] = h[DP_R - 1];
-            }
-            uplast = upv;
-            acc |= bits << (2 * DP_R * (tt % DP_SPW));
-            if (tt % DP_SPW == DP_SPW - 1 || tt == W - 1) {
-                bts[(tt / DP_SPW) * 32] = acc;
-                acc = 0u;
-            }
-        }
-        __syncwarp();
-    }
+    if (dp_r(lq) == 4)
+        dp_pair<4, GAP0 != 0, USESS != 0>(t, d02, gcost, lq, lr, qx, qy, qz, r4, qs, rs, row, bt, lane);
+    else
+        dp_pair<2, GAP0 != 0, USESS != 0>(t, d02, gcost, lq, lr, qx, qy, qz, r4, qs, rs, row, bt, lane);
 }
 
 void launch_dp(const Blk& B, const Bat& T, int tfmsrc, int gap0, float gcost, int usess,
@@ -1057,7 +1092,8 @@ __global__ void k_btck(Blk B, Bat T, int constrained) {
     const unsigned* bt = T.bt + T.off_bt[i];
     unsigned* aln = T.aln + T.off_aln[i];
     float* alc = T.alc + 6 * T.off_aln[i];
-    const long long sw = bt_strip_words(lr);
+    const int R = dp_r(lq), rows = 32 * R, spw = 16 / R;
+    const long long sw = bt_strip_words(lr, R);
     float t[12];
     float d82 = B.t_d82[ml];
     const float4* q4 = B.q4 + B.q4off[qi];
@@ -1068,9 +1104,9 @@ __global__ void k_btck(Blk B, Bat T, int constrained) {
     }
     int y = lq - 1, x = lr - 1, n = 0;
     while (x >= 0 && y >= 0) {
-        int yy = y % DP_ROWS, l = yy / DP_R, tt = x + l;
-        unsigned w = bt[(long long)(y / DP_ROWS) * sw + (tt / DP_SPW) * 32 + l];
-        int b = (int)((w >> (2 * DP_R * (tt % DP_SPW) + 2 * (yy % DP_R))) & 3u);
+        int yy = y % rows, l = yy / R, tt = x + l;
+        unsigned w = bt[(long long)(y / rows) * sw + (tt / spw) * 32 + l];
+        int b = (int)((w >> (2 * R * (tt % spw) + 2 * (yy % R))) & 3u);
         if (b == BT_UP) { y--; continue; }
         if (b == BT_LEFT) { x--; continue; }
         float4 cq = __ldg(q4 + y), cr = __ldg(r4 + x);

@@ -5,19 +5,21 @@
 
 namespace gtb {
 
-// DP traceback storage.  The DP sweeps strips of DP_ROWS query rows (DP_R
-// rows per lane of a warp) along anti-diagonals, lr + 31 steps per strip;
-// every lane packs the 2-bit directions of its DP_R rows for DP_SPW
-// consecutive steps into one 32-bit word, words of a strip stored
-// [step / DP_SPW][lane].
-constexpr int DP_R = 2;
-constexpr int DP_ROWS = 32 * DP_R;
-constexpr int DP_SPW = 16 / DP_R;
-__host__ __device__ inline long long bt_strip_words(int lr) {
-    return (long long)((lr + 31 + DP_SPW - 1) / DP_SPW) * 32;
+// DP traceback storage.  The DP sweeps strips of 32*R query rows (R rows
+// per lane of a warp; R = 4 for queries of at least DP_R4_MIN residues, 2
+// below) along anti-diagonals, lr + 31 steps per strip rounded up to a
+// multiple of 16/R; every lane packs the 2-bit directions of its R rows for
+// 16/R consecutive steps into one 32-bit word, words of a strip stored
+// [step / (16/R)][lane].
+constexpr int DP_R4_MIN = 384;
+__host__ __device__ inline int dp_r(int lq) { return lq >= DP_R4_MIN ? 4 : 2; }
+__host__ __device__ inline long long bt_strip_words(int lr, int R) {
+    const int spw = 16 / R;
+    return (long long)((lr + 31 + spw - 1) / spw) * 32;
 }
 __host__ __device__ inline long long bt_words(int lq, int lr) {
-    return (long long)((lq + DP_ROWS - 1) / DP_ROWS) * bt_strip_words(lr);
+    const int R = dp_r(lq);
+    return (long long)((lq + 32 * R - 1) / (32 * R)) * bt_strip_words(lr, R);
 }
 
 // Block of queries x references (device pointers, SoA).
