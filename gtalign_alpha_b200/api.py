@@ -45,7 +45,8 @@ class _COptions(ctypes.Structure):
                 ("convergence", ctypes.c_int), ("prescore", ctypes.c_float),
                 ("symmetric", ctypes.c_int), ("referenced", ctypes.c_int),
                 ("nodeletions", ctypes.c_int), ("nodetailedsearch", ctypes.c_int),
-                ("addsearchbyss", ctypes.c_int), ("twotmscore", ctypes.c_int)]
+                ("addsearchbyss", ctypes.c_int), ("twotmscore", ctypes.c_int),
+                ("polish_steps", ctypes.c_int)]
 
 
 class _CResults(ctypes.Structure):
@@ -71,6 +72,7 @@ class Options:
     nodetailedsearch: int = 1
     addsearchbyss: int = 0
     twotmscore: int = 0
+    polish_steps: int = 0      # adjoint polishing of the final transforms (this library only)
 
     @classmethod
     def speed(cls, level: int, **kw) -> "Options":
@@ -85,7 +87,8 @@ class Options:
     def _c(self) -> _COptions:
         return _COptions(self.refinement, self.depth, self.convergence, self.prescore,
                          self.symmetric, self.referenced, self.nodeletions,
-                         self.nodetailedsearch, self.addsearchbyss, self.twotmscore)
+                         self.nodetailedsearch, self.addsearchbyss, self.twotmscore,
+                         self.polish_steps)
 
 
 _lib = None

@@ -12,6 +12,8 @@
 #include <cuda_runtime.h>
 #include <cstdio>
 #include "gtb200.h"
+#include "gtb_device.cuh"
+#include "gtb_kernels.cuh"
 
 namespace {
 
@@ -33,17 +35,18 @@ struct Kahan {
 
 // TM-score and gradient for one pair; omega about the point `cen`
 // (cen = 0 gives the public origin-based derivative).
+template <int S>
 __device__ void tm_grad(const float* q, const float* r, int n, const float* T, float d0,
                         const float* cen, float* gq, float& tm, float* g6) {
     int lane = threadIdx.x & 31;
     float d02 = d0 * d0;
     Kahan s, gw[3], gt[3];
     for (int i = lane; i < n; i += 32) {
-        float qx = q[3 * i], qy = q[3 * i + 1], qz = q[3 * i + 2];
+        float qx = q[S * i], qy = q[S * i + 1], qz = q[S * i + 2];
         float px = T[0] * qx + T[1] * qy + T[2] * qz;
         float py = T[3] * qx + T[4] * qy + T[5] * qz;
         float pz = T[6] * qx + T[7] * qy + T[8] * qz;
-        float ex = px + T[9] - r[3 * i], ey = py + T[10] - r[3 * i + 1], ez = pz + T[11] - r[3 * i + 2];
+        float ex = px + T[9] - r[S * i], ey = py + T[10] - r[S * i + 1], ez = pz + T[11] - r[S * i + 2];
         float u = d02 + ex * ex + ey * ey + ez * ez;
         float iu = 1.f / u;
         s.add(d02 * iu);
@@ -79,39 +82,41 @@ __global__ void k_tm_adjoint(int npairs, const long long* off, const int* n, con
     float T[12];
     for (int f = 0; f < 12; f++) T[f] = tfm[p * 12 + f];
     float t, g6[6];
-    tm_grad(qxyz + 3 * o, rxyz + 3 * o, n[p], T, d0[p], zero, gq ? gq + 3 * o : nullptr, t, g6);
+    tm_grad<3>(qxyz + 3 * o, rxyz + 3 * o, n[p], T, d0[p], zero, gq ? gq + 3 * o : nullptr, t, g6);
     if (lane == 0) {
         if (tm) tm[p] = t;
         if (grad) for (int k = 0; k < 6; k++) grad[p * 6 + k] = g6[k];
     }
 }
 
+template <int S>
 __device__ float tm_only(const float* q, const float* r, int n, const float* T, float d0) {
     int lane = threadIdx.x & 31;
     float d02 = d0 * d0;
     Kahan s;
     for (int i = lane; i < n; i += 32) {
-        float qx = q[3 * i], qy = q[3 * i + 1], qz = q[3 * i + 2];
-        float ex = T[0] * qx + T[1] * qy + T[2] * qz + T[9] - r[3 * i];
-        float ey = T[3] * qx + T[4] * qy + T[5] * qz + T[10] - r[3 * i + 1];
-        float ez = T[6] * qx + T[7] * qy + T[8] * qz + T[11] - r[3 * i + 2];
+        float qx = q[S * i], qy = q[S * i + 1], qz = q[S * i + 2];
+        float ex = T[0] * qx + T[1] * qy + T[2] * qz + T[9] - r[S * i];
+        float ey = T[3] * qx + T[4] * qy + T[5] * qz + T[10] - r[S * i + 1];
+        float ez = T[6] * qx + T[7] * qy + T[8] * qz + T[11] - r[S * i + 2];
         s.add(d02 / (d02 + ex * ex + ey * ey + ez * ez));
     }
     return warp_sum(s.s + s.c);
 }
 
 // curvature scales for the step: h_t = sum 2 d0^2/u^2, h_w = sum 2 d0^2 |a|^2/u^2
+template <int S>
 __device__ void curvature(const float* q, const float* r, int n, const float* T, float d0,
                           const float* cen, float& ht, float& hw) {
     int lane = threadIdx.x & 31;
     float d02 = d0 * d0;
     float a1 = 0.f, a2 = 0.f;
     for (int i = lane; i < n; i += 32) {
-        float qx = q[3 * i], qy = q[3 * i + 1], qz = q[3 * i + 2];
+        float qx = q[S * i], qy = q[S * i + 1], qz = q[S * i + 2];
         float px = T[0] * qx + T[1] * qy + T[2] * qz + T[9];
         float py = T[3] * qx + T[4] * qy + T[5] * qz + T[10];
         float pz = T[6] * qx + T[7] * qy + T[8] * qz + T[11];
-        float ex = px - r[3 * i], ey = py - r[3 * i + 1], ez = pz - r[3 * i + 2];
+        float ex = px - r[S * i], ey = py - r[S * i + 1], ez = pz - r[S * i + 2];
         float u = d02 + ex * ex + ey * ey + ez * ez;
         float w = 2.f * d02 / (u * u);
         a1 += w;
@@ -153,41 +158,35 @@ __device__ void apply_step(const float* T, const float* w, const float* dt, cons
     for (int k = 0; k < 9; k++) Tn[k] = (float)Rn[k];
 }
 
-__global__ void k_polish(int npairs, const long long* off, const int* n, const float* qxyz,
-                         const float* rxyz, float* tfm, const float* d0v, int steps,
-                         float* tmb, float* tma) {
-    int p = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-    if (p >= npairs) return;
+// Projected-gradient ascent of TM (d0) over (R, t) for one pair, from T;
+// a step is kept only if it raises the score.  Returns the final score.
+template <int S>
+__device__ float polish_pair(const float* q, const float* r, int m, float d0, float* T, int steps,
+                             float* before) {
+    float Tn[12];
+    float cur = tm_only<S>(q, r, m, T, d0);
+    if (before) *before = cur;
     int lane = threadIdx.x & 31;
-    long long o = off[p];
-    const float* q = qxyz + 3 * o;
-    const float* r = rxyz + 3 * o;
-    int m = n[p];
-    float d0 = d0v[p];
-    float T[12], Tn[12];
-    for (int f = 0; f < 12; f++) T[f] = tfm[p * 12 + f];
-    float cur = tm_only(q, r, m, T, d0);
-    if (lane == 0 && tmb) tmb[p] = cur;
     for (int it = 0; it < steps && m > 0; it++) {
         // centroid of the transformed query
         float cx = 0.f, cy = 0.f, cz = 0.f;
         for (int i = lane; i < m; i += 32) {
-            float qx = q[3 * i], qy = q[3 * i + 1], qz = q[3 * i + 2];
+            float qx = q[S * i], qy = q[S * i + 1], qz = q[S * i + 2];
             cx += T[0] * qx + T[1] * qy + T[2] * qz + T[9];
             cy += T[3] * qx + T[4] * qy + T[5] * qz + T[10];
             cz += T[6] * qx + T[7] * qy + T[8] * qz + T[11];
         }
         float c[3] = {warp_sum(cx) / m, warp_sum(cy) / m, warp_sum(cz) / m};
         float tmv, g6[6], ht, hw;
-        tm_grad(q, r, m, T, d0, c, nullptr, tmv, g6);
-        curvature(q, r, m, T, d0, c, ht, hw);
+        tm_grad<S>(q, r, m, T, d0, c, nullptr, tmv, g6);
+        curvature<S>(q, r, m, T, d0, c, ht, hw);
         if (!(ht > 0.f) || !(hw > 0.f)) break;
         float w[3] = {g6[0] / hw, g6[1] / hw, g6[2] / hw};
         float dt[3] = {g6[3] / ht, g6[4] / ht, g6[5] / ht};
         bool acc = false;
         for (int bt = 0; bt < 10 && !acc; bt++) {
             apply_step(T, w, dt, c, Tn);
-            float nv = tm_only(q, r, m, Tn, d0);
+            float nv = tm_only<S>(q, r, m, Tn, d0);
             if (nv > cur) {
                 acc = true;
                 cur = nv;
@@ -198,13 +197,66 @@ __global__ void k_polish(int npairs, const long long* off, const int* n, const f
         }
         if (!acc) break;
     }
+    return cur;
+}
+
+__global__ void k_polish(int npairs, const long long* off, const int* n, const float* qxyz,
+                         const float* rxyz, float* tfm, const float* d0v, int steps,
+                         float* tmb, float* tma) {
+    int p = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    if (p >= npairs) return;
+    int lane = threadIdx.x & 31;
+    long long o = off[p];
+    float T[12], before;
+    for (int f = 0; f < 12; f++) T[f] = tfm[p * 12 + f];
+    float cur = polish_pair<3>(qxyz + 3 * o, rxyz + 3 * o, n[p], d0v[p], T, steps, &before);
     if (lane == 0) {
         for (int f = 0; f < 12; f++) tfm[p * 12 + f] = T[f];
+        if (tmb) tmb[p] = before;
         if (tma) tma[p] = cur;
     }
 }
 
+// Polishing inside the search, after the production scores: each pair's
+// final transform is polished against TM with the search's d0 (that of the
+// shorter structure) over its final alignment (the aligned coordinates the
+// traceback stored, 6 floats per aligned pair); when a step was kept, the
+// FP32 TM-scores by both lengths are recomputed for the new transform (the
+// FP64 recomputation and error record follow in the final kernel).
+__global__ void k_polish_final(gtb::Blk B, gtb::Bat T, int steps) {
+    int i = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    if (i >= T.np) return;
+    int lane = threadIdx.x & 31;
+    if (T.flags[i] & gtb::CONV_LOWTMSC) return;
+    int m = T.naln[i];
+    if (m < 3) return;
+    int qi = (int)((T.p0 + i) / B.nr), ri = (int)((T.p0 + i) % B.nr);
+    int lq = B.qlen[qi], lr = B.rlen[ri];
+    int ml = lq < lr ? lq : lr;
+    const float* q = T.alc + 6 * T.off_aln[i];
+    const float* r = q + 3;
+    float Tm[12], before;
+    for (int f = 0; f < 12; f++) Tm[f] = T.tfm_gr[i * 12 + f];
+    float cur = polish_pair<6>(q, r, m, B.t_d0fin[ml], Tm, steps, &before);
+    if (!(cur > before)) return;
+    float tq = tm_only<6>(q, r, m, Tm, B.t_d0fin[lq]);
+    float tr = tm_only<6>(q, r, m, Tm, B.t_d0fin[lr]);
+    if (lane == 0) {
+        for (int f = 0; f < 12; f++) T.tfm_gr[i * 12 + f] = Tm[f];
+        T.out[i * 16 + 9] = tq / (float)lq;
+        T.out[i * 16 + 10] = tr / (float)lr;
+    }
+}
+
 }  // namespace
+
+namespace gtb {
+void launch_polish_final(const Blk& B, const Bat& T, int steps, cudaStream_t st) {
+    if (steps <= 0 || T.np <= 0) return;
+    k_polish_final<<<(T.np + 3) / 4, 128, 0, st>>>(B, T, steps);
+    if (T.launches) (*T.launches)++;
+}
+}  // namespace gtb
 
 struct gtb_handle;
 extern "C" gtb_status gtb_tm_adjoint(gtb_handle* h, int npairs, const long long* off, const int* n,

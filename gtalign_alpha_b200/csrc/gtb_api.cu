@@ -130,6 +130,10 @@ static gtb_status check_options(gtb_handle* h) {
         snprintf(h->err, sizeof(h->err), "--refinement %d not implemented (0 or 1)", o.refinement);
         return GTB_ERR_UNSUPPORTED;
     }
+    if (o.polish_steps < 0 || o.polish_steps > 50) {
+        snprintf(h->err, sizeof(h->err), "polish_steps %d out of 0..50", o.polish_steps);
+        return GTB_ERR_ARG;
+    }
     if (o.depth < 0 || o.depth > 3 || o.convergence < 1 || o.convergence > 30 ||
         !(o.prescore >= 0.f && o.prescore < 1.f)) {
         snprintf(h->err, sizeof(h->err), "option out of range");
@@ -257,7 +261,7 @@ static gtb_status run_block(gtb_handle* h, const DevBlock& D, float scorethld,
         T.launches = &h->launches;
         CK(cudaMemcpyAsync(offs, off_bt, 4 * (size_t)(np + 1) * sizeof(long long), cudaMemcpyHostToDevice, st));
         launch_stages(B, T, o.refinement, o.depth, o.convergence, o.prescore, o.referenced,
-                      scorethld, st, h->sev[evset]);
+                      scorethld, st, h->sev[evset], o.polish_steps);
         CK(cudaGetLastError());
         if (h_alndata)
             CK(cudaMemcpyAsync(h_alndata + q0 * 16, T.out, (size_t)np * 16 * sizeof(float), cudaMemcpyDefault, st));

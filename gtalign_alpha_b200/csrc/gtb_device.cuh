@@ -192,7 +192,7 @@ __device__ __forceinline__ int qcp_rotation(const double (&S)[3][3], double (&R)
 // sums v: [0..8] sum q_i r_j, [9..11] sum q, [12..14] sum r, [15] n.
 // swap: solve with the reference rotated onto the query, then invert
 // (--symmetric for a shorter query, MpStageBase.h:1000-1023).
-__device__ __noinline__ void solve_sums(const float* v, int swap, float* tfm) {
+static __device__ __noinline__ void solve_sums(const float* v, int swap, float* tfm) {
     double dn = (double)v[15];
     double mq[3], mr[3], S[3][3];
 #pragma unroll

@@ -1349,7 +1349,7 @@ void make_tables(float* d0, float* d82, float* d0fin, int n) {
 // stage boundaries.
 void launch_stages(const Blk& B, const Bat& T, int refinement, int depth, int convergence,
                    float prescore, int referenced, float scorethld, cudaStream_t st,
-                   cudaEvent_t* ev) {
+                   cudaEvent_t* ev, int polish_steps) {
     auto mark = [&](int k) { if (ev) cudaEventRecord(ev[k], st); };
     // DPRefine: MpStage1.cpp:466-517
     // after the stage-1 --pre-score filter only a small share of pairs is left
@@ -1390,6 +1390,7 @@ void launch_stages(const Blk& B, const Bat& T, int refinement, int depth, int co
     launch_alnstr(B, T, st);
     launch_refine(RM_PROD1, B, T, st, few);
     launch_refine(RM_PROD2, B, T, st, few);
+    launch_polish_final(B, T, polish_steps, st);
     launch_final(B, T, referenced, st);
     mark(4);
 }

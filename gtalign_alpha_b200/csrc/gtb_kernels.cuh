@@ -82,9 +82,11 @@ void launch_post(const Blk& B, const Bat& T, int dpi, int maxit, int prescreen,
 void launch_lowscore(const Blk& B, const Bat& T, float thr, cudaStream_t st);
 void launch_alnstr(const Blk& B, const Bat& T, cudaStream_t st);
 void launch_final(const Blk& B, const Bat& T, int referenced, cudaStream_t st);
+// adjoint polishing of the final transforms (steps > 0), before launch_final
+void launch_polish_final(const Blk& B, const Bat& T, int steps, cudaStream_t st);
 void launch_stages(const Blk& B, const Bat& T, int refinement, int depth, int convergence,
                    float prescore, int referenced, float scorethld, cudaStream_t st,
-                   cudaEvent_t* ev);
+                   cudaEvent_t* ev, int polish_steps = 0);
 // Per-length constant tables (stagecnsts.cuh:48-175), n entries each.
 void make_tables(float* d0, float* d82, float* d0fin, int n);
 

@@ -105,7 +105,8 @@ extern "C" gtb_status gtb_process_block_noalloc(int device, const gtb_options* o
         return GTB_ERR_UNSUPPORTED;
     }
     if (!(scorethld >= 0.f && scorethld < 1.f) || opts->depth < 0 || opts->depth > 3 ||
-        opts->convergence < 1 || opts->convergence > 30 || !(opts->prescore >= 0.f && opts->prescore < 1.f)) {
+        opts->convergence < 1 || opts->convergence > 30 || !(opts->prescore >= 0.f && opts->prescore < 1.f) ||
+        opts->polish_steps < 0 || opts->polish_steps > 50) {
         setmsg(errbuf, errlen, "option out of range (%lld %lld)", 0, 0);
         return GTB_ERR_ARG;
     }
@@ -226,7 +227,7 @@ extern "C" gtb_status gtb_process_block_noalloc(int device, const gtb_options* o
         launch_secstr(q->d_ss, q->d_x, q->d_y, q->d_z, q->d_lens, q->d_offs, q->d_mol, q->n, st, &nl);
         launch_secstr(r->d_ss, r->d_x, r->d_y, r->d_z, r->d_lens, r->d_offs, r->d_mol, r->n, st, &nl);
         launch_stages(B, T, opts->refinement, opts->depth, opts->convergence, opts->prescore,
-                      opts->referenced, scorethld, st, nullptr);
+                      opts->referenced, scorethld, st, nullptr, opts->polish_steps);
         e = cudaGetLastError();
     }
     if (e == cudaSuccess)

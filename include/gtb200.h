@@ -72,6 +72,13 @@ typedef struct {
                                 search stage is not part of this library) */
     int   addsearchbyss;     /* --add-search-by-ss: must be 0 */
     int   twotmscore;        /* --2tm-score: must be 0 */
+    int   polish_steps;      /* no reference counterpart: 0 (the reference's
+                                results) or 1..50 projected-gradient steps on
+                                SO(3) x R^3 that polish each pair's final
+                                transform with the TM-score adjoint before the
+                                FP64 recomputation; a step is kept only if it
+                                raises the TM-score (d0 of the shorter
+                                structure) over the final alignment */
 } gtb_options;
 
 /* Result buffers (host memory), sizes for nq queries x nr references with

@@ -156,3 +156,25 @@ def test_autograd_function_matches_fp64():
     assert (gq - g64).abs().max() <= 1e-3 * g64.abs().max()
     gt, gt64 = tt.grad.cpu().double(), t64.grad
     assert (gt - gt64).abs().max() <= 1e-3 * gt64.abs().max()
+
+
+def test_polishing_in_the_search_never_lowers_the_score():
+    """polish_steps > 0 polishes each pair's final transform with the adjoint
+    before the FP64 recomputation: the score by the shorter structure's
+    length never goes down, the alignments stay, and homologs gain."""
+    from gtalign_alpha_b200 import synth
+    from gtalign_alpha_b200.api import GTalignB200, Options
+    wl = synth.config0(seed=23, n_refs=60, qlen=150, lmin=50, lmax=400)
+    q, r = synth.pack(wl.queries), synth.pack(wl.refs)
+    res = {}
+    for steps in (0, 10):
+        with GTalignB200(0, 0, Options(prescore=0.0, polish_steps=steps)) as g:
+            res[steps] = g.process_block(q, r, scorethld=0.0, alignments=False)
+    a, b = res[0].alndata[0], res[10].alndata[0]
+    lq = q.lens[0]
+    short = np.where(lq <= r.lens, a[:, 9], a[:, 10]), np.where(lq <= r.lens, b[:, 9], b[:, 10])
+    assert np.all(short[1] >= short[0] - 1e-6)
+    assert np.array_equal(a[:, 2:8], b[:, 2:8])          # same alignments
+    gain = short[1] - short[0]
+    assert (gain > 1e-5).sum() > 5
+    assert float(np.max(res[10].numerr[0][:, :2])) < 1e-5  # FP32 vs FP64 of the polished transform
