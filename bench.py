@@ -45,6 +45,10 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
+# k_findfrag DRAM read + write per pair (ncu, 2 queries x 40,000 references:
+# 101.39 MB + 6.31 MB for 13,333 pairs)
+FINDFRAG_DRAM_BYTES_PER_PAIR = (101.39e6 + 6.31e6) / 13333
+
 METRIC = "pairs/s on 1 B200 at |dTM|<=1e-4; batched+adjoint vs plain; HBM % of peak"
 UNIT = "pairs/s"
 
@@ -276,14 +280,23 @@ def run_ours(args):
     st_ms = stage_ms / args.steps
     # algorithmic bytes of the seed (scan) stage: every reference coordinate
     # read once per query block, query coordinates, and a 64-byte record per pair
-    algo_bytes = (12 * r.total + 12 * q.total) * args.steps / nchunk + 64 * done_pairs
-    algo_bytes /= args.steps
+    # per step (one query chunk): every reference residue once, the chunk's
+    # queries, a 64-byte record per pair; the step's seed launches (one per
+    # sub-batch) split these bytes, and stage_ms[0] sums their durations
+    algo_bytes = 12 * r.total + 12 * q.total / nchunk + 64 * done_pairs / args.steps
     seed_ms = float(st_ms[0])
     achieved = algo_bytes / (seed_ms / 1000.0) / 1e9 if seed_ms > 0 else 0.0
+    # DRAM bytes of one seed launch, scaled by pairs from an ncu capture of a
+    # smaller case of the same workload (profiles/top3_kernels_c1_2x40000.md)
+    step_pairs_avg = done_pairs / args.steps
+    nsub = max(1, min(6, int(step_pairs_avg) // 16384))
+    traffic = FINDFRAG_DRAM_BYTES_PER_PAIR * step_pairs_avg / nsub
+    algo_launch = algo_bytes / nsub
     roof = {"bound": "hbm", "kernel": "k_findfrag (stage-1 seed scan)",
             "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
             "frac": achieved / hbm_peak, "peak_source": peak_kind,
-            "traffic": None,
+            "traffic": traffic, "traffic_unit": "bytes per launch (scaled from ncu)",
+            "algorithmic_bytes_per_launch": algo_launch,
             "stage_ms": {"seed": float(st_ms[0]), "refine_init": float(st_ms[1]),
                          "dp_refine_loops": float(st_ms[2]), "final": float(st_ms[5]),
                          "total": float(st_ms[6])}}
