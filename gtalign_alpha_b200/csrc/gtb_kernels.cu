@@ -159,6 +159,27 @@ struct PairGeom {
             a = u.x; b = u.y; c = u.z; d = v.x; e = v.y; f = v.z;
         }
     }
+    // bring line `ln` (0..7) of the positions [k, k+32) into L1 ahead of use
+    __device__ __forceinline__ void prefetch(int k, int ln) const {
+        const char* p;
+        if (alc) {
+            int hi = n - 1 - k;                       // positions run backwards in memory
+            if (hi < 0) return;
+            int lo = hi - 31 < 0 ? 0 : hi - 31;
+            const char* base = (const char*)(alc + 3 * lo);
+            const char* end = (const char*)(alc + 3 * (hi + 1));
+            p = base + 128 * ln;
+            if (p >= end) return;
+        } else {
+            if (k >= n) return;
+            int k1 = k + 32 < n ? k + 32 : n;         // stay inside the pair's residues
+            const char* base = ln < 4 ? (const char*)(q4 + q0 + k) : (const char*)(r4 + r0 + k);
+            const char* end = ln < 4 ? (const char*)(q4 + q0 + k1) : (const char*)(r4 + r0 + k1);
+            p = base + 128 * (ln & 3);
+            if (p >= end) return;
+        }
+        asm volatile("prefetch.global.L1 [%0];" :: "l"(p));
+    }
 };
 
 // Every pass below walks its range in blocks of BLK positions (folded into
@@ -627,7 +648,7 @@ enum PassKind {
 template <bool M3, bool FR, bool SC>
 __device__ __forceinline__ float lane_pass_t(const PairGeom& G, int kind, int k0, int k1,
                                              const float* tfm, float d02, int chk, float d82,
-                                             float thr, int m3on, float* v, float& m3out) {
+                                             float thr, int m3on, float* v, float& m3out, int pl) {
     float ss = 0.f, sc = 0.f, sb = 0.f;
     float m1 = LARGEDST, m2 = LARGEDST, m3 = LARGEDST;
     const bool frag = FR && kind == PK_FRAG;
@@ -638,6 +659,7 @@ __device__ __forceinline__ float lane_pass_t(const PairGeom& G, int kind, int k0
     a.init();
     for (int b0 = frag ? (k0 & ~(BLK - 1)) : 0; b0 < n; b0 += BLK) {
         int b1 = b0 + BLK < n ? b0 + BLK : n;
+        if (pl < 8) G.prefetch(b0 + BLK, pl);    // the next block, one line per lane
 #pragma unroll 2
         for (int k = b0; k < b1; k++) {
             float qx, qy, qz, rx, ry, rz;
@@ -670,19 +692,19 @@ __device__ __forceinline__ float lane_pass_t(const PairGeom& G, int kind, int k0
 
 __device__ __forceinline__ float lane_pass(const PairGeom& G, int kind, int k0, int k1,
                                            const float* tfm, float d02, int chk, float d82,
-                                           float thr, int m3on, float* v, float& m3out) {
+                                           float thr, int m3on, float* v, float& m3out, int pl) {
     const unsigned FULL = 0xffffffffu;
     const bool sc = __any_sync(FULL, kind == PK_SCORE || kind == PK_GSCORE);
     const bool m3 = __any_sync(FULL, kind == PK_SCORE && m3on);
     const bool fr = __any_sync(FULL, kind == PK_FRAG);
     if (m3)
-        return fr ? lane_pass_t<true, true, true>(G, kind, k0, k1, tfm, d02, chk, d82, thr, m3on, v, m3out)
-                  : lane_pass_t<true, false, true>(G, kind, k0, k1, tfm, d02, chk, d82, thr, m3on, v, m3out);
+        return fr ? lane_pass_t<true, true, true>(G, kind, k0, k1, tfm, d02, chk, d82, thr, m3on, v, m3out, pl)
+                  : lane_pass_t<true, false, true>(G, kind, k0, k1, tfm, d02, chk, d82, thr, m3on, v, m3out, pl);
     if (sc)
-        return fr ? lane_pass_t<false, true, true>(G, kind, k0, k1, tfm, d02, chk, d82, thr, m3on, v, m3out)
-                  : lane_pass_t<false, false, true>(G, kind, k0, k1, tfm, d02, chk, d82, thr, m3on, v, m3out);
-    return fr ? lane_pass_t<false, true, false>(G, kind, k0, k1, tfm, d02, chk, d82, thr, m3on, v, m3out)
-              : lane_pass_t<false, false, false>(G, kind, k0, k1, tfm, d02, chk, d82, thr, m3on, v, m3out);
+        return fr ? lane_pass_t<false, true, true>(G, kind, k0, k1, tfm, d02, chk, d82, thr, m3on, v, m3out, pl)
+                  : lane_pass_t<false, false, true>(G, kind, k0, k1, tfm, d02, chk, d82, thr, m3on, v, m3out, pl);
+    return fr ? lane_pass_t<false, true, false>(G, kind, k0, k1, tfm, d02, chk, d82, thr, m3on, v, m3out, pl)
+              : lane_pass_t<false, false, false>(G, kind, k0, k1, tfm, d02, chk, d82, thr, m3on, v, m3out, pl);
 }
 
 // RF_LPP lanes per pair: 16 (two pairs per warp) where most pairs of a
@@ -700,7 +722,7 @@ __global__ void __launch_bounds__(RF_WARPS * 32) k_refine(Blk B, Bat T) {
     const unsigned FULL = 0xffffffffu;
     const int lane = threadIdx.x & 31;
     const int sub = lane / RF_LPP;
-    const unsigned smask = ((1u << RF_LPP) - 1u) << (sub * RF_LPP);
+    const unsigned smask = RF_LPP == 32 ? 0xffffffffu : ((1u << (RF_LPP & 31)) - 1u) << (sub * RF_LPP);
     const int slot = blockIdx.x * RF_PAIRS + (threadIdx.x >> 5) * RF_PPW + sub;
     const bool valid = slot < T.rhist[RL_NB];
     if (__ballot_sync(FULL, valid) == 0) return;
@@ -806,7 +828,8 @@ __global__ void __launch_bounds__(RF_WARPS * 32) k_refine(Blk B, Bat T) {
         }
         if (__ballot_sync(FULL, kind != PK_IDLE) == 0) break;
         float v[16], m3;
-        const float sc = lane_pass(G, kind, k0, k1, tfm, pd02, pchk, d82, thr, m3mode, v, m3);
+        const float sc = lane_pass(G, kind, k0, k1, tfm, pd02, pchk, d82, thr, m3mode, v, m3,
+                                   lane % RF_LPP);
         bool havev = false, done = false;
         if (kind == PK_FRAG) {
             if (v[15] < 1.0f) done = true;
