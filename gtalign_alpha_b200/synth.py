@@ -28,7 +28,7 @@ import ctypes
 import math
 import os
 from dataclasses import dataclass, field
-from typing import List, Optional, Sequence
+from typing import List, Optional, Sequence, Tuple
 
 import numpy as np
 
@@ -297,6 +297,65 @@ def config1(seed: int = 2, n_queries: int = 16, n_refs: int = 200_000,
             hom[ri] = qi
             k += 1
     return Workload(queries, refs, seed, f"config1 seed={seed}", hom)
+
+
+def _rot_small(rng: np.random.Generator, max_deg: float) -> np.ndarray:
+    """Rotation by a uniform angle in [0, max_deg] about a random axis."""
+    ax = rng.normal(size=3)
+    ax /= np.linalg.norm(ax)
+    th = math.radians(float(rng.uniform(0.0, max_deg)))
+    K = np.array([[0, -ax[2], ax[1]], [ax[2], 0, -ax[0]], [-ax[1], ax[0], 0]])
+    return np.eye(3) + math.sin(th) * K + (1 - math.cos(th)) * (K @ K)
+
+
+def assembly(rng: np.random.Generator, length: int, name: str) -> Tuple[Chain, List[int]]:
+    """A multi-domain chain of about ``length`` residues: 100-400-residue
+    domains, each placed by a random rigid transform 20-60 A from the
+    previous one.  Returns the chain and its domain lengths."""
+    dl: List[int] = []
+    while sum(dl) < length:
+        dl.append(int(min(rng.integers(100, 401), max(length - sum(dl), 1))))
+    doms = random_chains(rng, dl, name + "_d")
+    parts, centre = [], np.zeros(3)
+    for d in doms:
+        x = d.xyz.astype(np.float64)
+        x = (x - x.mean(axis=0)) @ _rot_random(rng).T
+        step = rng.normal(size=3)
+        step *= float(rng.uniform(20.0, 60.0)) / np.linalg.norm(step)
+        centre = centre + step
+        parts.append(x + centre)
+    xyz = np.concatenate(parts, axis=0)
+    seq = np.concatenate([d.seq for d in doms])
+    return Chain(_pdb_round_fast(xyz), seq, name), dl
+
+
+def assembly_partner(rng: np.random.Generator, ch: Chain, domains: Sequence[int],
+                     name: str, max_deg: float = 30.0, sigma: float = 1.5) -> Chain:
+    """The long-chain partner: every domain rigidly perturbed (rotation
+    about its centre up to ``max_deg``), then Gaussian noise ``sigma``."""
+    x = ch.xyz.astype(np.float64).copy()
+    o = 0
+    for L in domains:
+        c = x[o:o + L].mean(axis=0)
+        x[o:o + L] = (x[o:o + L] - c) @ _rot_small(rng, max_deg).T + c + rng.normal(0, 1.0, 3)
+        o += L
+    x += rng.normal(0.0, sigma, size=x.shape)
+    x = (x - x.mean(axis=0)) @ _rot_random(rng).T
+    return Chain(_pdb_round_fast(x), ch.seq.copy(), name)
+
+
+def config2(seed: int = 3, lengths: Sequence[int] = (5000, 8000, 12000, 16000, 20000,
+                                                     25000, 30000, 37860)) -> Workload:
+    """Long-chain pairs: for each length an assembly of 100-400-residue
+    domains and its partner (per-domain rotations <= 30 deg, sigma 1.5 A).
+    Query i pairs with reference i."""
+    rng = np.random.default_rng(seed)
+    qs, rs = [], []
+    for i, L in enumerate(lengths):
+        q, dl = assembly(rng, int(L), f"asm{i:02d}")
+        qs.append(q)
+        rs.append(assembly_partner(rng, q, dl, f"prt{i:02d}"))
+    return Workload(qs, rs, seed, f"config2 seed={seed}", list(range(len(lengths))))
 
 
 # -------------------------------------------------------------------------

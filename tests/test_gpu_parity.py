@@ -165,3 +165,17 @@ def test_status_codes():
         # the handle stays usable after errors
         res = g.process_block(q, r, scorethld=0.0)
         assert res.alndata.shape == (1, 2, 16)
+
+
+def test_long_chain_assemblies(oracle):
+    """Multi-domain assemblies and their per-domain-perturbed partners (the
+    long-chain configuration's construction at 1,200 and 2,000 residues):
+    large DP matrices, many strips and thousands of refinement variants."""
+    from gtalign_alpha_b200 import synth
+    wl = synth.config2(seed=3, lengths=(1200, 2000))
+    q, r = synth.pack(wl.queries), synth.pack(wl.refs)
+    d = dict(refinement=1, convergence=18, prescore=0.4, scorethld=0.5, symmetric=0,
+             referenced=0, nodeletions=0)
+    res, ora = run_both(oracle, q, r, d)
+    assert_same(res, ora, q.n, r.n)
+    assert res.alndata[0, 0, 9] > 0.5 and res.alndata[1, 1, 9] > 0.5
