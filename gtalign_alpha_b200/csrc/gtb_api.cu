@@ -167,7 +167,7 @@ static size_t pair_bytes(int lq, int lr, bool strings) {
     b += (size_t)lr * 4;                               // DP row buffer
     b += (size_t)std::min(lq, lr) * 28;                // aligned pairs + coordinates
     if (strings) b += (size_t)5 * (lq + lr + 1);       // alignment rows
-    b += 4 * 8 + 12 * 4 * 2 + 16 * 4 + 4 * 4 + 12 * 4 + 64 + 4;  // state, offsets, work list
+    b += 4 * 8 + 12 * 4 * 2 + 16 * 4 + 4 * 4 + 12 * 4 + 64 + 4 + 24;  // state, offsets, work lists
     return b;
 }
 
@@ -206,6 +206,7 @@ static gtb_status run_block(gtb_handle* h, const DevBlock& D, float scorethld,
     h->launches = 0;
     // host offsets of the sub-batches in flight (kept until their copies ran)
     std::vector<long long> offv[gtb_handle::NSUB];
+    std::vector<int> ffv[gtb_handle::NSUB], ffiv[gtb_handle::NSUB];
 
     // One sub-batch [q0, q0 + np): plan, carve one allocation, upload the
     // offsets, launch the stage sequence and the result copies on stream st.
@@ -217,6 +218,11 @@ static gtb_status run_block(gtb_handle* h, const DevBlock& D, float scorethld,
         long long* off_row = off_bt + (np + 1);
         long long* off_aln = off_bt + 2 * (np + 1);
         long long* off_str = off_bt + 3 * (np + 1);
+        // seed work items: pairs with more offsets than one CTA takes are split
+        std::vector<int>& ffn = ffv[j];
+        ffn.assign(np, 1);
+        long long nitems = 0;
+        bool split = false;
         for (int i = 0; i < np; i++) {
             long long p = q0 + i;
             int lq = D.hqlen[p / D.nr], lr = D.hrlen[p % D.nr];
@@ -224,6 +230,20 @@ static gtb_status run_block(gtb_handle* h, const DevBlock& D, float scorethld,
             off_row[i + 1] = off_row[i] + lr;
             off_aln[i + 1] = off_aln[i] + std::min(lq, lr);
             off_str[i + 1] = off_str[i] + (strings ? 5LL * (lq + lr + 1) : 0);
+            int n1, silo, sihi, prv;
+            gtb::seed_range(lq, lr, B.qmax, B.qmin, B.rmax, B.rmin, B.stepinit, n1, silo, sihi, prv);
+            int cnt = sihi - silo + 1;
+            int nch = cnt > gtb::FF_CHUNK ? (cnt + gtb::FF_CHUNK - 1) / gtb::FF_CHUNK : 1;
+            ffn[i] = nch;
+            nitems += nch;
+            split = split || nch > 1;
+        }
+        std::vector<int>& ffi = ffiv[j];
+        if (split) {
+            ffi.assign(2 * (size_t)nitems, 0);
+            long long t = 0;
+            for (int i = 0; i < np; i++)
+                for (int c = 0; c < ffn[i]; c++, t++) { ffi[t] = i; ffi[nitems + t] = c; }
         }
         size_t sz = 0;
         auto carve = [&](size_t bytes) { size_t o2 = sz; sz += align256(bytes); return o2; };
@@ -241,6 +261,9 @@ static gtb_status run_block(gtb_handle* h, const DevBlock& D, float scorethld,
         size_t o_alc = carve((size_t)off_aln[np] * 6 * sizeof(float));
         size_t o_rl = carve((size_t)np * sizeof(int));
         size_t o_rh = carve((size_t)4097 * sizeof(int));
+        size_t o_ffi = split ? carve((size_t)nitems * 2 * sizeof(int)) : 0;
+        size_t o_ffn = split ? carve((size_t)np * sizeof(int)) : 0;
+        size_t o_ffk = split ? carve((size_t)np * sizeof(unsigned long long)) : 0;
         char* base = nullptr;
         CK(cudaMallocAsync((void**)&base, sz, st));
         Bat T{};
@@ -259,7 +282,16 @@ static gtb_status run_block(gtb_handle* h, const DevBlock& D, float scorethld,
         T.alc = (float*)(base + o_alc);
         T.rlist = (int*)(base + o_rl); T.rhist = (int*)(base + o_rh);
         T.launches = &h->launches;
+        T.nff = np; T.ff_pair = nullptr; T.ff_chunk = nullptr; T.ff_nch = nullptr; T.ff_key = nullptr;
         CK(cudaMemcpyAsync(offs, off_bt, 4 * (size_t)(np + 1) * sizeof(long long), cudaMemcpyHostToDevice, st));
+        if (split) {
+            int* di = (int*)(base + o_ffi);
+            int* dn = (int*)(base + o_ffn);
+            T.nff = (int)nitems; T.ff_pair = di; T.ff_chunk = di + nitems; T.ff_nch = dn;
+            T.ff_key = (unsigned long long*)(base + o_ffk);
+            CK(cudaMemcpyAsync(di, ffi.data(), (size_t)nitems * 2 * sizeof(int), cudaMemcpyHostToDevice, st));
+            CK(cudaMemcpyAsync(dn, ffn.data(), (size_t)np * sizeof(int), cudaMemcpyHostToDevice, st));
+        }
         launch_stages(B, T, o.refinement, o.depth, o.convergence, o.prescore, o.referenced,
                       scorethld, st, h->sev[evset], o.polish_steps);
         CK(cudaGetLastError());

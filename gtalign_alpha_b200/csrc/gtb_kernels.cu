@@ -411,26 +411,29 @@ __device__ float findfrag_variant(const PairGeom& G, float d02, float d0s, int s
 }
 
 __global__ void __launch_bounds__(128) k_findfrag(Blk B, Bat T) {
-    int i = blockIdx.x;
+    const int item = blockIdx.x;
+    int i = item, c = 0, nch = 1;
+    if (T.ff_pair) {
+        if (item >= T.nff) return;
+        i = T.ff_pair[item];
+        c = T.ff_chunk[item];
+        nch = T.ff_nch[i];
+    }
     if (i >= T.np) return;
     int flags = T.flags[i];
     if (flags & CONV_LOWTMSC) return;
     int qi = pair_qi(B, T, i), ri = pair_ri(B, T, i);
     int lq = B.qlen[qi], lr = B.rlen[ri];
-    int minlenmin = B.qmin < B.rmin ? B.qmin : B.rmin;
-    int minalnmin = (minlenmin >> 1) > 5 ? (minlenmin >> 1) : 5;
-    int n1 = minalnmin - B.rmax;
-    int n2 = B.qmax - minalnmin;
-    int step = B.stepinit;
-    int nsteps = (n2 - n1) / step + 1;
-    int ml = lq < lr ? lq : lr;
-    int prv = (ml >> 1) > 5 ? (ml >> 1) : 5;
-    // per-pair admissible offsets: prv - lr <= ab <= lq - prv
-    int lo = prv - lr - n1;
-    int silo = lo <= 0 ? 0 : (lo + step - 1) / step;
-    int hi = lq - prv - n1;
-    int sihi = hi < 0 ? -1 : hi / step;
-    if (sihi > nsteps - 1) sihi = nsteps - 1;
+    const int step = B.stepinit;
+    int n1, silo, sihi, prv;
+    seed_range(lq, lr, B.qmax, B.qmin, B.rmax, B.rmin, step, n1, silo, sihi, prv);
+    const int ml = lq < lr ? lq : lr;
+    // this CTA's share of the offsets
+    int s0 = silo, s1 = sihi;
+    if (nch > 1) {
+        s0 = silo + c * FF_CHUNK;
+        s1 = s0 + FF_CHUNK - 1 < sihi ? s0 + FF_CHUNK - 1 : sihi;
+    }
     float d0 = B.t_d0[ml];
     float d02 = __fmul_rn(d0, d0);
     float d0s = d0s_of(d0);
@@ -440,7 +443,7 @@ __global__ void __launch_bounds__(128) k_findfrag(Blk B, Bat T) {
     G.alc = nullptr;
     float lbest = 0.f;
     int lsi = 0x7fffffff;
-    for (int si = silo + (int)threadIdx.x; si <= sihi; si += blockDim.x) {
+    for (int si = s0 + (int)threadIdx.x; si <= s1; si += blockDim.x) {
         int ab = n1 + si * step;
         int qpos = ab > 0 ? ab : 0;
         int rpos = -ab > 0 ? -ab : 0;
@@ -469,6 +472,15 @@ __global__ void __launch_bounds__(128) k_findfrag(Blk B, Bat T) {
     }
     if (threadIdx.x == 0) {
         float b = sb[0];
+        if (nch > 1) {
+            // larger score, then lower offset index, over the pair's CTAs
+            if (b > 0.f) {
+                unsigned long long key = ((unsigned long long)__float_as_uint(b) << 32) |
+                                         (unsigned long long)(0xffffffffu - (unsigned)ssi[0]);
+                atomicMax(T.ff_key + i, key);
+            }
+            return;
+        }
         T.best[i] = b;
         if (b > 0.f) {
             int ab = n1 + ssi[0] * step;
@@ -481,7 +493,37 @@ __global__ void __launch_bounds__(128) k_findfrag(Blk B, Bat T) {
     }
 }
 
+// seeds of the pairs split over several CTAs
+__global__ void k_findfrag_fin(Blk B, Bat T) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= T.np || T.ff_nch[i] <= 1) return;
+    if (T.flags[i] & CONV_LOWTMSC) return;
+    unsigned long long key = T.ff_key[i];
+    float b = __uint_as_float((unsigned)(key >> 32));
+    T.best[i] = b;
+    if (b > 0.f) {
+        int qi = pair_qi(B, T, i), ri = pair_ri(B, T, i);
+        int n1, silo, sihi, prv;
+        seed_range(B.qlen[qi], B.rlen[ri], B.qmax, B.qmin, B.rmax, B.rmin, B.stepinit, n1, silo,
+                   sihi, prv);
+        int si = (int)(0xffffffffu - (unsigned)(key & 0xffffffffu));
+        int ab = n1 + si * B.stepinit;
+        T.seedq[i] = ab > 0 ? ab : 0;
+        T.seedr[i] = -ab > 0 ? -ab : 0;
+    } else {
+        T.seedq[i] = 0;
+        T.seedr[i] = 0;
+    }
+}
+
 void launch_findfrag(const Blk& B, const Bat& T, cudaStream_t st) {
+    if (T.ff_pair) {
+        cudaMemsetAsync(T.ff_key, 0, (size_t)T.np * sizeof(unsigned long long), st);
+        k_findfrag<<<T.nff, 128, 0, st>>>(B, T);
+        k_findfrag_fin<<<(T.np + 255) / 256, 256, 0, st>>>(B, T);
+        if (T.launches) (*T.launches) += 2;
+        return;
+    }
     k_findfrag<<<T.np, 128, 0, st>>>(B, T);
     GTB_LAUNCHED(T);
 }

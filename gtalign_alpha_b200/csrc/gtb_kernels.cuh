@@ -52,6 +52,12 @@ struct Bat {
     float* alc;                      // their coordinates, 6 floats each (offset 6*off_aln)
     const long long *off_str; char* str;      // alignment rows per pair
     int *rlist, *rhist;              // refinement work list [np], buckets [4097]
+    // seed work items when some pair's offsets are split over several CTAs
+    // (null: one CTA per pair): item -> pair, item -> chunk, chunks per pair,
+    // per-pair packed (score, variant) maximum
+    int nff;
+    const int *ff_pair, *ff_chunk, *ff_nch;
+    unsigned long long* ff_key;
     long long* launches;             // host counter of kernel launches
 };
 
@@ -70,6 +76,25 @@ void launch_pack4_structs(float4* out, const float* x, const float* y, const flo
                           const int* off, const int* len, const int* coff, int n,
                           cudaStream_t st);
 void launch_init(const Blk& B, const Bat& T, cudaStream_t st);
+// Seed offsets per CTA (a pair with more is split over several CTAs).
+constexpr int FF_CHUNK = 512;
+// the seed's offset index range [silo, sihi] of a pair (MpStage1.cpp:299-318)
+__host__ __device__ inline void seed_range(int lq, int lr, int qmax, int qmin, int rmax, int rmin,
+                                           int step, int& n1, int& silo, int& sihi, int& prv) {
+    int minlenmin = qmin < rmin ? qmin : rmin;
+    int minalnmin = (minlenmin >> 1) > 5 ? (minlenmin >> 1) : 5;
+    n1 = minalnmin - rmax;
+    int n2 = qmax - minalnmin;
+    int nsteps = (n2 - n1) / step + 1;
+    int ml = lq < lr ? lq : lr;
+    prv = (ml >> 1) > 5 ? (ml >> 1) : 5;
+    // per-pair admissible offsets: prv - lr <= ab <= lq - prv
+    int lo = prv - lr - n1;
+    silo = lo <= 0 ? 0 : (lo + step - 1) / step;
+    int hi = lq - prv - n1;
+    sihi = hi < 0 ? -1 : hi / step;
+    if (sihi > nsteps - 1) sihi = nsteps - 1;
+}
 void launch_findfrag(const Blk& B, const Bat& T, cudaStream_t st);
 // few: most pairs of the batch are already filtered out (32 lanes per pair)
 void launch_refine(int mode, const Blk& B, const Bat& T, cudaStream_t st, bool few);

@@ -214,6 +214,7 @@ extern "C" gtb_status gtb_process_block_noalloc(int device, const gtb_options* o
     T.aln = (unsigned*)(base + o_aln); T.str = nullptr;
     T.alc = (float*)(base + o_alc);
     T.rlist = (int*)(base + o_rl); T.rhist = (int*)(base + o_rh);
+    T.nff = np; T.ff_pair = nullptr; T.ff_chunk = nullptr; T.ff_nch = nullptr; T.ff_key = nullptr;
     T.launches = nullptr;
 
     // the host offsets are copied from the static host array (no allocation)
