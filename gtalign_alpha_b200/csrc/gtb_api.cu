@@ -33,7 +33,8 @@ struct gtb_handle {
     // so the short, narrow launches at the end of one overlap the others
     static const int NSUB = 3;
     cudaStream_t sub[NSUB] = {};
-    cudaEvent_t sev[2 * NSUB][8] = {};  // stage events per sub-batch (two waves)
+    static const int NWAVE = 2;      // sub-batches per stream and batch
+    cudaEvent_t sev[NWAVE * NSUB][8] = {};  // stage events per sub-batch
 };
 
 static const int TBL = 65536;
@@ -77,7 +78,7 @@ extern "C" gtb_status gtb_create(int device, size_t mem_bytes, const gtb_options
     h->sub[0] = h->st;
     for (int j = 1; j < gtb_handle::NSUB; j++)
         CK(cudaStreamCreateWithFlags(&h->sub[j], cudaStreamNonBlocking));
-    for (int j = 0; j < 2 * gtb_handle::NSUB; j++)
+    for (int j = 0; j < gtb_handle::NWAVE * gtb_handle::NSUB; j++)
         for (int k = 0; k < 8; k++) CK(cudaEventCreate(&h->sev[j][k]));
     std::vector<float> a(TBL), b(TBL), c(TBL);
     make_tables(a.data(), b.data(), c.data(), TBL);
@@ -98,7 +99,7 @@ extern "C" void gtb_destroy(gtb_handle* h) {
     if (h->t_d82) cudaFree(h->t_d82);
     if (h->t_d0fin) cudaFree(h->t_d0fin);
     for (int k = 0; k < 8; k++) if (h->ev[k]) cudaEventDestroy(h->ev[k]);
-    for (int j = 0; j < 2 * gtb_handle::NSUB; j++)
+    for (int j = 0; j < gtb_handle::NWAVE * gtb_handle::NSUB; j++)
         for (int k = 0; k < 8; k++) if (h->sev[j][k]) cudaEventDestroy(h->sev[j][k]);
     for (int j = 1; j < gtb_handle::NSUB; j++)
         if (h->sub[j]) cudaStreamDestroy(h->sub[j]);
@@ -343,7 +344,8 @@ static gtb_status run_block(gtb_handle* h, const DevBlock& D, float scorethld,
         // over the streams: the narrow stage-2 launches of the first wave
         // overlap the wide stage-1 launches of the second
         long long nb = p1 - p0;
-        int nsub = (int)std::min<long long>(2 * gtb_handle::NSUB, std::max<long long>(1, nb / 16384));
+        int nsub = (int)std::min<long long>(gtb_handle::NWAVE * gtb_handle::NSUB,
+                                            std::max<long long>(1, nb / 16384));
         long long q0 = p0;
         for (int j = 0; j < nsub; j++) {
             long long q1 = p0 + nb * (j + 1) / nsub;
