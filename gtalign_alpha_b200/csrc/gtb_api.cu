@@ -35,6 +35,8 @@ struct gtb_handle {
     cudaStream_t sub[NSUB] = {};
     static const int NWAVE = 2;      // sub-batches per stream and batch
     cudaEvent_t sev[NWAVE * NSUB][8] = {};  // stage events per sub-batch
+    int dw_cap = 0;                  // CTAs the wavefront DP keeps resident
+    int* h_flag = nullptr;           // pinned: wavefront error flag per sub-batch
 };
 
 static const int TBL = 65536;
@@ -75,6 +77,9 @@ extern "C" gtb_status gtb_create(int device, size_t mem_bytes, const gtb_options
         cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
     }
     for (int k = 0; k < 8; k++) CK(cudaEventCreate(&h->ev[k]));
+    h->dw_cap = dp_wave_capacity();
+    CK(cudaHostAlloc((void**)&h->h_flag, gtb_handle::NWAVE * gtb_handle::NSUB * sizeof(int),
+                     cudaHostAllocDefault));
     h->sub[0] = h->st;
     for (int j = 1; j < gtb_handle::NSUB; j++)
         CK(cudaStreamCreateWithFlags(&h->sub[j], cudaStreamNonBlocking));
@@ -104,6 +109,7 @@ extern "C" void gtb_destroy(gtb_handle* h) {
     for (int j = 1; j < gtb_handle::NSUB; j++)
         if (h->sub[j]) cudaStreamDestroy(h->sub[j]);
     if (h->st) cudaStreamDestroy(h->st);
+    if (h->h_flag) cudaFreeHost(h->h_flag);
     delete h;
 }
 
@@ -207,7 +213,8 @@ static gtb_status run_block(gtb_handle* h, const DevBlock& D, float scorethld,
     h->launches = 0;
     // host offsets of the sub-batches in flight (kept until their copies ran)
     std::vector<long long> offv[gtb_handle::NSUB];
-    std::vector<int> ffv[gtb_handle::NSUB], ffiv[gtb_handle::NSUB];
+    std::vector<int> ffv[gtb_handle::NSUB], ffiv[gtb_handle::NSUB], dwvv[gtb_handle::NSUB];
+    std::vector<long long> dwsv[gtb_handle::NSUB];
 
     // One sub-batch [q0, q0 + np): plan, carve one allocation, upload the
     // offsets, launch the stage sequence and the result copies on stream st.
@@ -239,6 +246,48 @@ static gtb_status run_block(gtb_handle* h, const DevBlock& D, float scorethld,
             nitems += nch;
             split = split || nch > 1;
         }
+        // long pairs: DP as a wavefront over several CTAs
+        std::vector<int>& dwv = dwvv[j];
+        dwv.clear();
+        long long dnprog = 0;
+        int nl = 0, nitw = 0;
+        if (h->dw_cap > 0) {
+            std::vector<int> lp;
+            for (int i = 0; i < np; i++) {
+                long long p = q0 + i;
+                int lq = D.hqlen[p / D.nr], lr = D.hrlen[p % D.nr];
+                if (gtb::dp_wave(lq, lr) && (int)lp.size() < h->dw_cap) lp.push_back(i);
+            }
+            nl = (int)lp.size();
+            if (nl > 0) {
+                // layout: items (slot, c) | pair | G | mark bytes (np) ; soff separately
+                std::vector<int> G(nl), items;
+                std::vector<long long>& so = dwsv[j];
+                so.assign(nl, 0);
+                for (int k = 0; k < nl; k++) {
+                    long long p = q0 + lp[k];
+                    int lq = D.hqlen[p / D.nr];
+                    int ns = gtb::dp_strips(lq);
+                    G[k] = std::min(ns, std::max(1, h->dw_cap / nl));
+                    so[k] = dnprog;
+                    dnprog += ns;
+                    nitw += G[k];
+                }
+                dwv.assign(2 * (size_t)nitw + 2 * (size_t)nl + (np + 3) / 4, 0);
+                int t = 0;
+                for (int k = 0; k < nl; k++)
+                    for (int c = 0; c < G[k]; c++, t++) { dwv[t] = k; dwv[nitw + t] = c; }
+                for (int k = 0; k < nl; k++) { dwv[2 * nitw + k] = lp[k]; dwv[2 * nitw + nl + k] = G[k]; }
+                unsigned char* mk = (unsigned char*)(dwv.data() + 2 * nitw + 2 * nl);
+                for (int k = 0; k < nl; k++) mk[lp[k]] = 1;
+            }
+        }
+        // pairs that may reach RL_LONG refinement positions (n <= min(lq, lr))
+        int nlmax = 0;
+        for (int i = 0; i < np; i++) {
+            long long p = q0 + i;
+            if (std::min(D.hqlen[p / D.nr], D.hrlen[p % D.nr]) >= gtb::RL_LONG) nlmax++;
+        }
         std::vector<int>& ffi = ffiv[j];
         if (split) {
             ffi.assign(2 * (size_t)nitems, 0);
@@ -265,6 +314,12 @@ static gtb_status run_block(gtb_handle* h, const DevBlock& D, float scorethld,
         size_t o_ffi = split ? carve((size_t)nitems * 2 * sizeof(int)) : 0;
         size_t o_ffn = split ? carve((size_t)np * sizeof(int)) : 0;
         size_t o_ffk = split ? carve((size_t)np * sizeof(unsigned long long)) : 0;
+        size_t o_dw = nl ? carve(dwv.size() * sizeof(int)) : 0;
+        size_t o_dws = nl ? carve((size_t)nl * sizeof(long long)) : 0;
+        size_t o_dwp = nl ? carve((size_t)dnprog * sizeof(int)) : 0;
+        size_t o_dwe = nl ? carve(sizeof(int)) : 0;
+        size_t o_rll = nlmax ? carve((size_t)(2 * nlmax + 1) * sizeof(int)) : 0;
+        size_t o_rlc = nlmax ? carve((size_t)nlmax * gtb::RLW_WARPS * gtb::RLW_CAND * sizeof(float)) : 0;
         char* base = nullptr;
         CK(cudaMallocAsync((void**)&base, sz, st));
         Bat T{};
@@ -284,6 +339,28 @@ static gtb_status run_block(gtb_handle* h, const DevBlock& D, float scorethld,
         T.rlist = (int*)(base + o_rl); T.rhist = (int*)(base + o_rh);
         T.launches = &h->launches;
         T.nff = np; T.ff_pair = nullptr; T.ff_chunk = nullptr; T.ff_nch = nullptr; T.ff_key = nullptr;
+        T.rl_nlmax = nlmax; T.rl_long = T.rl_count = T.rl_next = nullptr; T.rl_cand = nullptr;
+        if (nlmax) {
+            int* rl = (int*)(base + o_rll);
+            T.rl_long = rl; T.rl_next = rl + nlmax; T.rl_count = rl + 2 * nlmax;
+            T.rl_cand = (float*)(base + o_rlc);
+        }
+        T.ndw = 0; T.dw_nprog = 0; T.dw_item = T.dw_pair = T.dw_G = nullptr; T.dw_soff = nullptr;
+        T.dw_mark = nullptr; T.dw_prog = nullptr; T.dw_err = nullptr;
+        h->h_flag[evset] = 0;
+        if (nl) {
+            int* dw = (int*)(base + o_dw);
+            T.ndw = nitw; T.dw_nprog = dnprog;
+            T.dw_item = dw; T.dw_pair = dw + 2 * nitw; T.dw_G = dw + 2 * nitw + nl;
+            T.dw_mark = (const unsigned char*)(dw + 2 * nitw + 2 * nl);
+            T.dw_soff = (const long long*)(base + o_dws);
+            T.dw_prog = (int*)(base + o_dwp);
+            T.dw_err = (int*)(base + o_dwe);
+            CK(cudaMemcpyAsync(dw, dwv.data(), dwv.size() * sizeof(int), cudaMemcpyHostToDevice, st));
+            CK(cudaMemcpyAsync(base + o_dws, dwsv[j].data(), (size_t)nl * sizeof(long long),
+                               cudaMemcpyHostToDevice, st));
+            CK(cudaMemsetAsync(T.dw_err, 0, sizeof(int), st));
+        }
         CK(cudaMemcpyAsync(offs, off_bt, 4 * (size_t)(np + 1) * sizeof(long long), cudaMemcpyHostToDevice, st));
         if (split) {
             int* di = (int*)(base + o_ffi);
@@ -304,6 +381,7 @@ static gtb_status run_block(gtb_handle* h, const DevBlock& D, float scorethld,
             CK(cudaMemcpyAsync(h_err + q0 * 4, T.err, (size_t)np * 4 * sizeof(float), cudaMemcpyDefault, st));
         if (strings)
             CK(cudaMemcpyAsync(hstr + (*hstroff)[q0], T.str, (size_t)off_str[np], cudaMemcpyDeviceToHost, st));
+        if (nl) CK(cudaMemcpyAsync(h->h_flag + evset, T.dw_err, sizeof(int), cudaMemcpyDeviceToHost, st));
         CK(cudaFreeAsync(base, st));
         return GTB_OK;
     };
@@ -360,6 +438,10 @@ static gtb_status run_block(gtb_handle* h, const DevBlock& D, float scorethld,
         for (int j = 0; j < nsub; j++) {
             gtb_status s = add_times(j);
             if (s != GTB_OK) return s;
+            if (h->h_flag[j]) {
+                snprintf(h->err, sizeof(h->err), "a wavefront DP wait exceeded its limit (sub-batch %d)", j);
+                return GTB_ERR_CUDA;
+            }
         }
         p0 = p1;
     }

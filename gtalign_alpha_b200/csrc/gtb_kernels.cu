@@ -554,6 +554,10 @@ __global__ void k_rlist_count(Blk B, Bat T, int mode) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= T.np) return;
     int n = refine_span(B, T, mode, i);
+    if (n >= RL_LONG && T.rl_long) {           // many warps for this pair
+        int slot = atomicAdd(T.rl_count, 1);
+        if (slot < T.rl_nlmax) { T.rl_long[slot] = i; return; }
+    }
     if (n > 0) {
         atomicAdd(&T.rhist[RL_NB - 1 - (n >> RL_SHIFT)], 1);
         return;
@@ -590,6 +594,7 @@ __global__ void k_rlist_fill(Blk B, Bat T, int mode) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= T.np) return;
     int n = refine_span(B, T, mode, i);
+    if (n >= RL_LONG && T.rl_long) return;      // listed by k_rlist_count
     if (n > 0) T.rlist[atomicAdd(&T.rhist[RL_NB - 1 - (n >> RL_SHIFT)], 1)] = i;
 }
 
@@ -749,12 +754,60 @@ __device__ __forceinline__ float lane_pass(const PairGeom& G, int kind, int k0, 
               : lane_pass_t<false, false, false>(G, kind, k0, k1, tfm, d02, chk, d82, thr, m3on, v, m3out, pl);
 }
 
+// The pair's result of a refinement launch (MpStage1.cpp:700-716 and the
+// final/production copies): winner score, transform and fragment, or the
+// "nothing scored" outputs.  tb: the winner's transform, stride tstr.
+template <int MODE>
+__device__ __forceinline__ void refine_commit(const Blk& B, const Bat& T, int i, int lq, int lr,
+                                              bool havewin, float wb, float lgbest, int wndx,
+                                              int wpos, const float* tb, int tstr) {
+    if (MODE == RM_PROD1 || MODE == RM_PROD2) {
+        if (!havewin) return;
+        float grand = T.grand[i];
+        bool write = (MODE == RM_PROD1) || (grand < wb);
+        if (write) {
+            T.grand[i] = wb;
+            float bs = wb, gb = lgbest;
+            if ((float)lr < (float)lq) { float t = bs; bs = gb; gb = t; }
+            T.out[i * 16 + 9] = __fdiv_rn(bs, (float)lq);
+            T.out[i * 16 + 10] = __fdiv_rn(gb, (float)lr);
+            T.out[i * 16 + 11] = B.t_d0fin[lq];
+            T.out[i * 16 + 12] = B.t_d0fin[lr];
+#pragma unroll
+            for (int f = 0; f < 12; f++) T.tfm_gr[i * 12 + f] = tb[f * tstr];
+            if (MODE == RM_PROD1) { T.sfndx[i] = wndx; T.sfpos[i] = wpos; }
+        }
+        return;
+    }
+    T.best[i] = havewin ? wb : 0.f;
+    if (havewin) {
+#pragma unroll
+        for (int f = 0; f < 12; f++) T.tfm_ib[i * 12 + f] = tb[f * tstr];
+        if (T.grand[i] < wb) {
+            T.grand[i] = wb;
+#pragma unroll
+            for (int f = 0; f < 12; f++) T.tfm_gr[i * 12 + f] = tb[f * tstr];
+        }
+    }
+    if (MODE == RM_FIN1) {
+        // the winner's fragment, or the previous one when no variant scored
+        int nd = havewin ? wndx : T.sfndx_cur[i];
+        int np_ = havewin ? wpos : T.sfpos_cur[i];
+        T.sfndx_cur[i] = nd; T.sfpos_cur[i] = np_;
+        T.sfndx[i] = nd; T.sfpos[i] = np_;
+    }
+}
+
 // RF_LPP lanes per pair: 16 (two pairs per warp) where most pairs of a
 // batch take part; 32 where few do (after the --pre-score filter), which
 // shortens the launches whose time is that of their slowest pair.
 constexpr int RF_WARPS = 4;
 
-template <int MODE, int RF_LPP>
+// LONG: the pairs with at least RL_LONG positions, RLW_CTAS CTAs each; every
+// warp of them takes the pair's variants from one counter in global memory
+// and leaves its best variant as a candidate; k_refine_long_fin picks the
+// pair's winner among them.
+template <int MODE, int RF_LPP, bool LONG>
 __global__ void __launch_bounds__(RF_WARPS * 32) k_refine(Blk B, Bat T) {
     constexpr int RF_PPW = 32 / RF_LPP;        // pairs per warp
     constexpr int RF_PAIRS = RF_PPW * RF_WARPS;  // pairs per CTA
@@ -765,10 +818,12 @@ __global__ void __launch_bounds__(RF_WARPS * 32) k_refine(Blk B, Bat T) {
     const int lane = threadIdx.x & 31;
     const int sub = lane / RF_LPP;
     const unsigned smask = RF_LPP == 32 ? 0xffffffffu : ((1u << (RF_LPP & 31)) - 1u) << (sub * RF_LPP);
-    const int slot = blockIdx.x * RF_PAIRS + (threadIdx.x >> 5) * RF_PPW + sub;
-    const bool valid = slot < T.rhist[RL_NB];
+    const int slot = LONG ? (int)(blockIdx.x / RLW_CTAS)
+                          : blockIdx.x * RF_PAIRS + (threadIdx.x >> 5) * RF_PPW + sub;
+    const int wlong = LONG ? (int)(blockIdx.x % RLW_CTAS) * RF_WARPS + (threadIdx.x >> 5) : 0;
+    const bool valid = LONG ? slot < *T.rl_count : slot < T.rhist[RL_NB];
     if (__ballot_sync(FULL, valid) == 0) return;
-    const int i = valid ? T.rlist[slot] : 0;
+    const int i = valid ? (LONG ? T.rl_long[slot] : T.rlist[slot]) : 0;
     const int str = RF_WARPS * 32;
     float* last = s_last + threadIdx.x;
     float* tbs = s_tb + threadIdx.x;
@@ -810,7 +865,7 @@ __global__ void __launch_bounds__(RF_WARPS * 32) k_refine(Blk B, Bat T) {
     if (gscore) { float g0 = B.t_d0fin[lq > lr ? lq : lr]; g02 = __fmul_rn(g0, g0); }
     VariantList V;
     variants_init(V, phase2, n, maxalnmax, phase2 ? T.sfndx[i] : 0, phase2 ? T.sfpos[i] : 0);
-    if (MODE == RM_PROD1 && (lane % RF_LPP) == 0 && V.total > 0) {
+    if (MODE == RM_PROD1 && (lane % RF_LPP) == 0 && V.total > 0 && wlong == 0) {
         // RMSD over the whole alignment (variant 0: fragment [0, n)) from
         // compensated FP32 sums, MpStageFin.cpp production phase 1
         int s0, nd0, ps0, fl0, kf0;
@@ -855,6 +910,11 @@ __global__ void __launch_bounds__(RF_WARPS * 32) k_refine(Blk B, Bat T) {
     for (;;) {
         const unsigned nm = __ballot_sync(FULL, need) & smask;
         if (nm) {
+            if (LONG) {                           // the pair's counter, shared by its warps
+                int base = 0;
+                if (lane == 0) base = atomicAdd(T.rl_next + slot, __popc(nm));
+                nextk = __shfl_sync(FULL, base, 0);
+            }
             int kv = nextk + __popc(nm & ((1u << lane) - 1u));
             nextk += __popc(nm);
             if (need) {
@@ -944,70 +1004,102 @@ __global__ void __launch_bounds__(RF_WARPS * 32) k_refine(Blk B, Bat T) {
     const bool havewin = wb > 0.f;
     const unsigned wmask = __ballot_sync(FULL, havewin && lsi == wsi) & smask;
     const int wl = wmask ? __ffs(wmask) - 1 : sub * RF_LPP;
-    const bool iamwin = havewin && lane == wl;
     const int wndx = __shfl_sync(FULL, lndx, wl);
     const int wpos = __shfl_sync(FULL, lpos, wl);
     if (!valid) return;
-    if (MODE == RM_PROD1 || MODE == RM_PROD2) {
-        if (iamwin) {
-            float grand = T.grand[i];
-            bool write = (MODE == RM_PROD1) || (grand < wb);
-            if (write) {
-                T.grand[i] = wb;
-                float bs = wb, gb = lgbest;
-                if ((float)lr < (float)lq) { float t = bs; bs = gb; gb = t; }
-                T.out[i * 16 + 9] = __fdiv_rn(bs, (float)lq);
-                T.out[i * 16 + 10] = __fdiv_rn(gb, (float)lr);
-                T.out[i * 16 + 11] = B.t_d0fin[lq];
-                T.out[i * 16 + 12] = B.t_d0fin[lr];
+    if (LONG) {
+        if (lane == wl) {
+            float* c = T.rl_cand + ((long long)slot * RLW_WARPS + wlong) * RLW_CAND;
+            c[0] = havewin ? wb : 0.f;
+            c[1] = __int_as_float(wsi);
+            c[2] = lgbest;
+            c[3] = __int_as_float(wndx);
+            c[4] = __int_as_float(wpos);
 #pragma unroll
-                for (int f = 0; f < 12; f++) T.tfm_gr[i * 12 + f] = tbest[f * str];
-                if (MODE == RM_PROD1) { T.sfndx[i] = wndx; T.sfpos[i] = wpos; }
-            }
+            for (int f = 0; f < 12; f++) c[5 + f] = tbest[f * str];
         }
         return;
     }
-    if (lane == wl) T.best[i] = havewin ? wb : 0.f;
-    if (iamwin) {
-#pragma unroll
-        for (int f = 0; f < 12; f++) T.tfm_ib[i * 12 + f] = tbest[f * str];
-        if (T.grand[i] < wb) {
-            T.grand[i] = wb;
-#pragma unroll
-            for (int f = 0; f < 12; f++) T.tfm_gr[i * 12 + f] = tbest[f * str];
-        }
+    if (lane == wl)
+        refine_commit<MODE>(B, T, i, lq, lr, havewin, wb, lgbest, wndx, wpos, tbest, str);
+}
+
+// the winner of each long pair among its warps' candidates
+template <int MODE>
+__global__ void k_refine_long_fin(Blk B, Bat T) {
+    const unsigned FULL = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    const int slot = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    if (slot >= *T.rl_count) return;
+    const int i = T.rl_long[slot];
+    const float* c0 = T.rl_cand + (long long)slot * RLW_WARPS * RLW_CAND;
+    float wb = 0.f;
+    int wsi = 0x7fffffff, wk = -1;
+    for (int k = lane; k < RLW_WARPS; k += 32) {
+        float b = c0[k * RLW_CAND];
+        int si = __float_as_int(c0[k * RLW_CAND + 1]);
+        if (b > 0.f && (wb < b || (wb == b && si < wsi))) { wb = b; wsi = si; wk = k; }
     }
-    if (MODE == RM_FIN1 && lane == wl) {
-        // the winner's fragment, or the previous one when no variant scored
-        int nd = havewin ? wndx : T.sfndx_cur[i];
-        int np_ = havewin ? wpos : T.sfpos_cur[i];
-        T.sfndx_cur[i] = nd; T.sfpos_cur[i] = np_;
-        T.sfndx[i] = nd; T.sfpos[i] = np_;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        float ob = __shfl_xor_sync(FULL, wb, o);
+        int os = __shfl_xor_sync(FULL, wsi, o);
+        int ok = __shfl_xor_sync(FULL, wk, o);
+        if (ob > wb || (ob == wb && os < wsi)) { wb = ob; wsi = os; wk = ok; }
+    }
+    if (lane != 0) return;
+    int qi = pair_qi(B, T, i), ri = pair_ri(B, T, i);
+    const bool havewin = wb > 0.f;
+    const float* c = c0 + (havewin ? wk : 0) * RLW_CAND;
+    refine_commit<MODE>(B, T, i, B.qlen[qi], B.rlen[ri], havewin, wb, c[2], __float_as_int(c[3]),
+                        __float_as_int(c[4]), c + 5, 1);
+}
+
+template <int LPP, bool LONG>
+static void launch_refine_k(int mode, const Blk& B, const Bat& T, cudaStream_t st) {
+    const int ng = LONG ? T.rl_nlmax * RLW_CTAS
+                        : (T.np + (32 / LPP) * RF_WARPS - 1) / ((32 / LPP) * RF_WARPS);
+    const int nt = RF_WARPS * 32;
+    switch (mode) {
+        case RM_INIT:  k_refine<RM_INIT, LPP, LONG><<<ng, nt, 0, st>>>(B, T); break;
+        case RM_DP:    k_refine<RM_DP, LPP, LONG><<<ng, nt, 0, st>>>(B, T); break;
+        case RM_FIN1:  k_refine<RM_FIN1, LPP, LONG><<<ng, nt, 0, st>>>(B, T); break;
+        case RM_FIN2:  k_refine<RM_FIN2, LPP, LONG><<<ng, nt, 0, st>>>(B, T); break;
+        case RM_PROD1: k_refine<RM_PROD1, LPP, LONG><<<ng, nt, 0, st>>>(B, T); break;
+        case RM_PROD2: k_refine<RM_PROD2, LPP, LONG><<<ng, nt, 0, st>>>(B, T); break;
     }
 }
 
-template <int LPP>
-static void launch_refine_k(int mode, const Blk& B, const Bat& T, cudaStream_t st) {
-    const int ng = (T.np + (32 / LPP) * RF_WARPS - 1) / ((32 / LPP) * RF_WARPS), nt = RF_WARPS * 32;
+static void launch_refine_long_fin(int mode, const Blk& B, const Bat& T, cudaStream_t st) {
+    const int ng = (T.rl_nlmax + 3) / 4;
     switch (mode) {
-        case RM_INIT:  k_refine<RM_INIT, LPP><<<ng, nt, 0, st>>>(B, T); break;
-        case RM_DP:    k_refine<RM_DP, LPP><<<ng, nt, 0, st>>>(B, T); break;
-        case RM_FIN1:  k_refine<RM_FIN1, LPP><<<ng, nt, 0, st>>>(B, T); break;
-        case RM_FIN2:  k_refine<RM_FIN2, LPP><<<ng, nt, 0, st>>>(B, T); break;
-        case RM_PROD1: k_refine<RM_PROD1, LPP><<<ng, nt, 0, st>>>(B, T); break;
-        case RM_PROD2: k_refine<RM_PROD2, LPP><<<ng, nt, 0, st>>>(B, T); break;
+        case RM_INIT:  k_refine_long_fin<RM_INIT><<<ng, 128, 0, st>>>(B, T); break;
+        case RM_DP:    k_refine_long_fin<RM_DP><<<ng, 128, 0, st>>>(B, T); break;
+        case RM_FIN1:  k_refine_long_fin<RM_FIN1><<<ng, 128, 0, st>>>(B, T); break;
+        case RM_FIN2:  k_refine_long_fin<RM_FIN2><<<ng, 128, 0, st>>>(B, T); break;
+        case RM_PROD1: k_refine_long_fin<RM_PROD1><<<ng, 128, 0, st>>>(B, T); break;
+        case RM_PROD2: k_refine_long_fin<RM_PROD2><<<ng, 128, 0, st>>>(B, T); break;
     }
 }
 
 void launch_refine(int mode, const Blk& B, const Bat& T, cudaStream_t st, bool few) {
     cudaMemsetAsync(T.rhist, 0, (RL_NB + 1) * sizeof(int), st);
+    if (T.rl_long) {
+        cudaMemsetAsync(T.rl_count, 0, sizeof(int), st);
+        cudaMemsetAsync(T.rl_next, 0, (size_t)T.rl_nlmax * sizeof(int), st);
+    }
     const int nb = (T.np + 255) / 256;
     k_rlist_count<<<nb, 256, 0, st>>>(B, T, mode);
     k_rlist_scan<<<1, 1024, 0, st>>>(T);
     k_rlist_fill<<<nb, 256, 0, st>>>(B, T, mode);
-    if (few) launch_refine_k<32>(mode, B, T, st);
-    else launch_refine_k<16>(mode, B, T, st);
+    if (few) launch_refine_k<32, false>(mode, B, T, st);
+    else launch_refine_k<16, false>(mode, B, T, st);
     if (T.launches) (*T.launches) += 4;
+    if (T.rl_long) {
+        launch_refine_k<32, true>(mode, B, T, st);
+        launch_refine_long_fin(mode, B, T, st);
+        if (T.launches) (*T.launches) += 2;
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -1019,17 +1111,24 @@ void launch_refine(int mode, const Blk& B, const Bat& T, cudaStream_t st, bool f
 // row kept in `row`.  Stored values are negated when the cell was reached
 // diagonally (the reference's state encoding, MpDPHub.cpp:246-262).  Steps
 // run in groups of 16/R, one traceback word per lane and group.
-template <int R, bool gap0, bool usess>
-__device__ __forceinline__ void dp_pair(const float* t, float d02, float gcost, int lq, int lr,
+// WAVE: the strips of one pair are shared by several CTAs (strip s by CTA
+// s mod s_step); a strip waits, with a bounded spin, until the previous one
+// has published the steps whose last-row values it is about to read
+// (`prog`: steps done per strip), and publishes its own progress after each
+// group of steps.  Returns false when a wait gave up (error flag set).
+template <int R, bool gap0, bool usess, bool WAVE>
+__device__ __forceinline__ bool dp_pair(const float* t, float d02, float gcost, int lq, int lr,
                                         const float* qx, const float* qy, const float* qz,
                                         const float4* r4, const char* qs, const char* rs,
-                                        float* row, unsigned* bt, int lane) {
+                                        float* row, unsigned* bt, int lane, int s_first = 0,
+                                        int s_step = 1, volatile int* prog = nullptr,
+                                        volatile int* err = nullptr) {
     constexpr int ROWS = 32 * R, SPW = 16 / R;
     const unsigned FULL = 0xffffffffu;
     const int W = lr + 31;
     const int ngrp = (W + SPW - 1) / SPW;
     const int nstrips = (lq + ROWS - 1) / ROWS;
-    for (int s = 0; s < nstrips; s++) {
+    for (int s = s_first; s < nstrips; s += s_step) {
         float tx[R], ty[R], tz[R], h[R];
         char qss[R];
         int nv = 0;  // valid rows of this lane (a prefix of its R rows)
@@ -1050,13 +1149,28 @@ __device__ __forceinline__ void dp_pair(const float* t, float d02, float gcost, 
         __syncwarp();
         for (int g = 0; g < ngrp; g++) {
             unsigned acc = 0u;
+            if (WAVE && s > 0 && ((g * SPW) & 31) == 0) {
+                // row[tt .. tt+31] of strip s-1: written up to its step tt+62
+                const int need = g * SPW + 64 < ngrp * SPW ? g * SPW + 64 : ngrp * SPW;
+                if (lane == 0) {
+                    long long it = 0;
+                    while (prog[s - 1] < need) {
+                        if (*err || ++it > (1LL << 24)) { *err = 1; break; }
+                        __nanosleep(64);
+                    }
+                }
+                __syncwarp();
+                __threadfence();
+                if (*err) return false;
+            }
 #pragma unroll
             for (int u = 0; u < SPW; u++) {
                 const int tt = g * SPW + u;   // steps past W find j >= lr on every lane
                 const int j = tt - lane;
                 if ((tt & 31) == 0) {
                     int jj = tt + lane;
-                    rb = (s > 0 && jj < lr) ? row[jj] : 0.f;
+                    if (WAVE) rb = (s > 0 && jj < lr) ? __ldcg(row + jj) : 0.f;
+                    else rb = (s > 0 && jj < lr) ? row[jj] : 0.f;
                 }
                 float upv = __shfl_up_sync(FULL, h[R - 1], 1);
                 float up0 = __shfl_sync(FULL, rb, tt & 31);
@@ -1090,9 +1204,14 @@ __device__ __forceinline__ void dp_pair(const float* t, float d02, float gcost, 
                 uplast = upv;
             }
             bts[g * 32] = acc;
+            if (WAVE && lane == 31) {
+                __threadfence();              // this group's row values before the count
+                prog[s] = (g + 1) * SPW;
+            }
         }
         __syncwarp();
     }
+    return true;
 }
 
 template <int GAP0, int USESS>
@@ -1104,6 +1223,7 @@ __global__ void __launch_bounds__(128) k_dp(Blk B, Bat T, int tfmsrc, float gcos
     int flags = T.flags[i];
     int skipmask = skipmode == 0 ? (CONV_LOWTMSC | CONV_SCOREDP) : CONV_LOWTMSC;
     if (flags & skipmask) return;
+    if (T.dw_mark && T.dw_mark[i]) return;       // done by the wavefront kernel
     int qi = pair_qi(B, T, i), ri = pair_ri(B, T, i);
     int lq = B.qlen[qi], lr = B.rlen[ri];
     int ml = lq < lr ? lq : lr;
@@ -1124,13 +1244,84 @@ __global__ void __launch_bounds__(128) k_dp(Blk B, Bat T, int tfmsrc, float gcos
     float* row = T.row + T.off_row[i];
     unsigned* bt = T.bt + T.off_bt[i];
     if (dp_r(lq) == 4)
-        dp_pair<4, GAP0 != 0, USESS != 0>(t, d02, gcost, lq, lr, qx, qy, qz, r4, qs, rs, row, bt, lane);
+        dp_pair<4, GAP0 != 0, USESS != 0, false>(t, d02, gcost, lq, lr, qx, qy, qz, r4, qs, rs, row, bt, lane);
     else
-        dp_pair<2, GAP0 != 0, USESS != 0>(t, d02, gcost, lq, lr, qx, qy, qz, r4, qs, rs, row, bt, lane);
+        dp_pair<2, GAP0 != 0, USESS != 0, false>(t, d02, gcost, lq, lr, qx, qy, qz, r4, qs, rs, row, bt, lane);
+}
+
+// One warp per CTA; the CTAs of a long pair take its strips round robin.
+// Launched cooperatively so that all CTAs are resident together.
+template <int GAP0, int USESS>
+__global__ void __launch_bounds__(32) k_dp_wave(Blk B, Bat T, int tfmsrc, float gcost, int dpscan,
+                                                int skipmode) {
+    const int lane = threadIdx.x & 31;
+    const int item = blockIdx.x;
+    if (item >= T.ndw) return;
+    const int slot = T.dw_item[item], c = T.dw_item[T.ndw + item];
+    const int i = T.dw_pair[slot], G = T.dw_G[slot];
+    int flags = T.flags[i];
+    int skipmask = skipmode == 0 ? (CONV_LOWTMSC | CONV_SCOREDP) : CONV_LOWTMSC;
+    if (flags & skipmask) return;                  // the same for every CTA of the pair
+    int qi = pair_qi(B, T, i), ri = pair_ri(B, T, i);
+    int lq = B.qlen[qi], lr = B.rlen[ri];
+    int ml = lq < lr ? lq : lr;
+    const float* tsrc = (tfmsrc == DP_TFM_GRAND ? T.tfm_gr : T.tfm_ib) + i * 12;
+    float t[12];
+#pragma unroll
+    for (int f = 0; f < 12; f++) t[f] = tsrc[f];
+    float d0 = B.t_d0[ml];
+    float d02;
+    if (dpscan) { float a = __fadd_rn(d0, 1.5f); d02 = __fmul_rn(a, a); }
+    else d02 = __fmul_rn(d0, d0);
+    const float* qx = B.qx + B.qoff[qi];
+    const float* qy = B.qy + B.qoff[qi];
+    const float* qz = B.qz + B.qoff[qi];
+    const float4* r4 = B.r4 + B.r4off[ri];
+    const char* qs = B.qs + B.qoff[qi];
+    const char* rs = B.rs + B.roff[ri];
+    float* row = T.row + T.off_row[i];
+    unsigned* bt = T.bt + T.off_bt[i];
+    volatile int* prog = T.dw_prog + T.dw_soff[slot];
+    if (dp_r(lq) == 4)
+        dp_pair<4, GAP0 != 0, USESS != 0, true>(t, d02, gcost, lq, lr, qx, qy, qz, r4, qs, rs, row,
+                                                bt, lane, c, G, prog, T.dw_err);
+    else
+        dp_pair<2, GAP0 != 0, USESS != 0, true>(t, d02, gcost, lq, lr, qx, qy, qz, r4, qs, rs, row,
+                                                bt, lane, c, G, prog, T.dw_err);
+}
+
+int dp_wave_capacity() {
+    int dev = 0, nsm = 0, m = 1 << 30, nb = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    const void* ks[4] = {(const void*)k_dp_wave<1, 0>, (const void*)k_dp_wave<0, 0>,
+                         (const void*)k_dp_wave<0, 1>, (const void*)k_dp_wave<1, 1>};
+    for (const void* k : ks) {
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k, 32, 0) != cudaSuccess) return 0;
+        m = nb < m ? nb : m;
+    }
+    return m * nsm;
+}
+
+template <int GAP0, int USESS>
+static void launch_dp_wave(const Blk& B, const Bat& T, int tfmsrc, float gcost, int dpscan,
+                           int skipmode, cudaStream_t st) {
+    Blk b = B;
+    Bat t = T;
+    void* args[] = {&b, &t, &tfmsrc, &gcost, &dpscan, &skipmode};
+    cudaLaunchCooperativeKernel((const void*)k_dp_wave<GAP0, USESS>, dim3(T.ndw), dim3(32), args, 0, st);
 }
 
 void launch_dp(const Blk& B, const Bat& T, int tfmsrc, int gap0, float gcost, int usess,
                int dpscan, int skipmode, cudaStream_t st) {
+    if (T.ndw > 0) {
+        cudaMemsetAsync(T.dw_prog, 0, (size_t)T.dw_nprog * sizeof(int), st);
+        if (gap0 && !usess) launch_dp_wave<1, 0>(B, T, tfmsrc, gcost, dpscan, skipmode, st);
+        else if (!gap0 && !usess) launch_dp_wave<0, 0>(B, T, tfmsrc, gcost, dpscan, skipmode, st);
+        else if (!gap0 && usess) launch_dp_wave<0, 1>(B, T, tfmsrc, gcost, dpscan, skipmode, st);
+        else launch_dp_wave<1, 1>(B, T, tfmsrc, gcost, dpscan, skipmode, st);
+        GTB_LAUNCHED(T);
+    }
     const int nb = (T.np + 3) / 4;
     if (gap0 && !usess) k_dp<1, 0><<<nb, 128, 0, st>>>(B, T, tfmsrc, gcost, dpscan, skipmode);
     else if (!gap0 && !usess) k_dp<0, 0><<<nb, 128, 0, st>>>(B, T, tfmsrc, gcost, dpscan, skipmode);

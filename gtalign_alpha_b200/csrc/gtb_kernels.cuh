@@ -11,12 +11,21 @@ namespace gtb {
 // multiple of 16/R; every lane packs the 2-bit directions of its R rows for
 // 16/R consecutive steps into one 32-bit word, words of a strip stored
 // [step / (16/R)][lane].
+// refinement: pairs with at least RL_LONG positions get RLW_CTAS CTAs
+constexpr int RL_LONG = 1536;
+constexpr int RLW_CTAS = 16;
+constexpr int RLW_WARPS = RLW_CTAS * 4;
+constexpr int RLW_CAND = 17;         // floats per warp candidate
+
 constexpr int DP_R4_MIN = 384;
 __host__ __device__ inline int dp_r(int lq) { return lq >= DP_R4_MIN ? 4 : 2; }
 __host__ __device__ inline long long bt_strip_words(int lr, int R) {
     const int spw = 16 / R;
     return (long long)((lr + 31 + spw - 1) / spw) * 32;
 }
+// pairs whose DP runs as a wavefront over several CTAs (one warp per strip)
+__host__ __device__ inline int dp_strips(int lq) { return (lq + 32 * dp_r(lq) - 1) / (32 * dp_r(lq)); }
+__host__ __device__ inline bool dp_wave(int lq, int lr) { return dp_strips(lq) >= 12 && lr >= 512; }
 __host__ __device__ inline long long bt_words(int lq, int lr) {
     const int R = dp_r(lq);
     return (long long)((lq + 32 * R - 1) / (32 * R)) * bt_strip_words(lr, R);
@@ -52,12 +61,26 @@ struct Bat {
     float* alc;                      // their coordinates, 6 floats each (offset 6*off_aln)
     const long long *off_str; char* str;      // alignment rows per pair
     int *rlist, *rhist;              // refinement work list [np], buckets [4097]
+    // long pairs of a refinement launch (null: none possible): list, count,
+    // per-pair variant counter, per-warp candidates; rl_nlmax = capacity
+    int rl_nlmax;
+    int *rl_long, *rl_count, *rl_next;
+    float* rl_cand;
     // seed work items when some pair's offsets are split over several CTAs
     // (null: one CTA per pair): item -> pair, item -> chunk, chunks per pair,
     // per-pair packed (score, variant) maximum
     int nff;
     const int *ff_pair, *ff_chunk, *ff_nch;
     unsigned long long* ff_key;
+    // long pairs whose DP strips run on several CTAs (null: none): CTA items
+    // [slot..., strip offset c...], per slot the pair, its CTA count and the
+    // offset of its per-strip progress counters; a per-pair mark; an error flag
+    int ndw;
+    long long dw_nprog;              // progress counters in dw_prog
+    const int *dw_item, *dw_pair, *dw_G;
+    const long long* dw_soff;
+    const unsigned char* dw_mark;
+    int *dw_prog, *dw_err;
     long long* launches;             // host counter of kernel launches
 };
 
@@ -102,6 +125,8 @@ void launch_refine(int mode, const Blk& B, const Bat& T, cudaStream_t st, bool f
 void launch_dp(const Blk& B, const Bat& T, int tfmsrc, int gap0, float gcost, int usess,
                int dpscan, int skipmode, cudaStream_t st);
 void launch_btck(const Blk& B, const Bat& T, int constrained, cudaStream_t st);
+// CTAs that the wavefront DP may keep resident at once on this device
+int dp_wave_capacity();
 void launch_post(const Blk& B, const Bat& T, int dpi, int maxit, int prescreen,
                  float prescore, cudaStream_t st);
 void launch_lowscore(const Blk& B, const Bat& T, float thr, cudaStream_t st);
