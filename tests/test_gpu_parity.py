@@ -179,3 +179,28 @@ def test_long_chain_assemblies(oracle):
     res, ora = run_both(oracle, q, r, d)
     assert_same(res, ora, q.n, r.n)
     assert res.alndata[0, 0, 9] > 0.5 and res.alndata[1, 1, 9] > 0.5
+
+
+def test_longest_chain_pair_properties():
+    """The longest pair of the long-chain configuration (37,860 residues,
+    an assembly against its per-domain perturbed partner), at full size,
+    checked through size-independent properties: the partner is found
+    (TM > 0.5 by both lengths), the reported TM-scores and RMSD agree with
+    their FP64 recomputation within the 1e-4 / 1e-3 tolerances, and the
+    alignment rows agree with the record and pair most residues."""
+    from gtalign_alpha_b200 import synth
+    from gtalign_alpha_b200.api import GTalignB200, Options
+    wl = synth.config2(seed=3, lengths=(37860,))
+    q, r = synth.pack(wl.queries), synth.pack(wl.refs)
+    with GTalignB200(0, 0, Options()) as g:
+        res = g.process_block(q, r, scorethld=0.5, alignments=True)
+    rec = res.alndata[0, 0]
+    assert rec[9] > 0.5 and rec[10] > 0.5
+    assert float(np.max(res.numerr[0, 0, :2])) <= 1e-4
+    assert float(res.numerr[0, 0, 2]) <= 1e-3
+    rows = res.alignment(0, 0)
+    qrow, trow = rows[0], rows[2]
+    assert len(qrow) == len(trow) == int(rec[4])
+    assert sum(c != '-' for c in qrow) <= 37860 and sum(c != '-' for c in trow) <= 37860
+    matched = sum(a != '-' and b != '-' for a, b in zip(qrow, trow))
+    assert matched > 0.8 * 37860
