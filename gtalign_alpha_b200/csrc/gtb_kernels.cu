@@ -590,6 +590,33 @@ __global__ void __launch_bounds__(1024) k_rlist_scan(Bat T) {
     if (t == 1023) T.rhist[RL_NB] = part[1023];
 }
 
+// DP work list: the pairs a DP launch works on (flags clear, not on the
+// wavefront path), largest matrices first; kept in the same buffers as the
+// refinement list (a DP launch is over before the next list is built).
+__device__ __forceinline__ int dlist_bucket(const Blk& B, const Bat& T, int i, int skipmode) {
+    int skipmask = skipmode == 0 ? (CONV_LOWTMSC | CONV_SCOREDP) : CONV_LOWTMSC;
+    if (T.flags[i] & skipmask) return -1;
+    if (T.dw_mark && T.dw_mark[i]) return -1;
+    int qi = pair_qi(B, T, i), ri = pair_ri(B, T, i);
+    long long cells = (long long)B.qlen[qi] * B.rlen[ri];
+    long long b = cells >> 8;
+    return RL_NB - 1 - (int)(b < RL_NB - 1 ? b : RL_NB - 1);
+}
+
+__global__ void k_dlist_count(Blk B, Bat T, int skipmode) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= T.np) return;
+    int b = dlist_bucket(B, T, i, skipmode);
+    if (b >= 0) atomicAdd(&T.rhist[b], 1);
+}
+
+__global__ void k_dlist_fill(Blk B, Bat T, int skipmode) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= T.np) return;
+    int b = dlist_bucket(B, T, i, skipmode);
+    if (b >= 0) T.rlist[atomicAdd(&T.rhist[b], 1)] = i;
+}
+
 __global__ void k_rlist_fill(Blk B, Bat T, int mode) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= T.np) return;
@@ -1218,12 +1245,9 @@ template <int GAP0, int USESS>
 __global__ void __launch_bounds__(128) k_dp(Blk B, Bat T, int tfmsrc, float gcost, int dpscan,
                                             int skipmode) {
     const int lane = threadIdx.x & 31;
-    const int i = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-    if (i >= T.np) return;
-    int flags = T.flags[i];
-    int skipmask = skipmode == 0 ? (CONV_LOWTMSC | CONV_SCOREDP) : CONV_LOWTMSC;
-    if (flags & skipmask) return;
-    if (T.dw_mark && T.dw_mark[i]) return;       // done by the wavefront kernel
+    const int slot = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    if (slot >= T.rhist[RL_NB]) return;            // the DP work list (k_dlist_*)
+    const int i = T.rlist[slot];
     int qi = pair_qi(B, T, i), ri = pair_ri(B, T, i);
     int lq = B.qlen[qi], lr = B.rlen[ri];
     int ml = lq < lr ? lq : lr;
@@ -1314,6 +1338,14 @@ static void launch_dp_wave(const Blk& B, const Bat& T, int tfmsrc, float gcost, 
 
 void launch_dp(const Blk& B, const Bat& T, int tfmsrc, int gap0, float gcost, int usess,
                int dpscan, int skipmode, cudaStream_t st) {
+    {
+        cudaMemsetAsync(T.rhist, 0, (RL_NB + 1) * sizeof(int), st);
+        const int nb = (T.np + 255) / 256;
+        k_dlist_count<<<nb, 256, 0, st>>>(B, T, skipmode);
+        k_rlist_scan<<<1, 1024, 0, st>>>(T);
+        k_dlist_fill<<<nb, 256, 0, st>>>(B, T, skipmode);
+        if (T.launches) (*T.launches) += 3;
+    }
     if (T.ndw > 0) {
         cudaMemsetAsync(T.dw_prog, 0, (size_t)T.dw_nprog * sizeof(int), st);
         if (gap0 && !usess) launch_dp_wave<1, 0>(B, T, tfmsrc, gcost, dpscan, skipmode, st);
