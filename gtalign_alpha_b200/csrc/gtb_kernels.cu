@@ -1,19 +1,26 @@
 // gtb_kernels.cu -- sm_100a kernels of the per-pair superposition search.
 //
 // Work decomposition (one launch covers every pair of a batch):
-//  * seed (stage 1, fragment search): one CTA per pair, one thread per
-//    diagonal offset; each thread runs the whole covariance -> rotation ->
-//    score -> threshold loop of its offset sequentially and keeps its best;
-//    the CTA reduces (max score, lowest offset index).
-//  * refinement (every fragment-based superposition refinement): one warp
-//    per pair, the lanes take the pair's admissible (fragment position,
-//    fragment length) variants in turn; the warp reduces (max score, lowest
-//    variant index) with shuffles.  The distance-threshold covariance pass
-//    of iteration k+1 is fused into the scoring pass of iteration k.
-//  * DP: one warp per pair; the warp sweeps strips of 32*R rows along
-//    anti-diagonals (R rows per lane, register-blocked), left/up/diagonal
-//    values move between lanes by shuffles, each lane packs the 2-bit
-//    directions of its cells into traceback words.
+//  * seed (stage 1, fragment search): one CTA per pair (a long pair's
+//    offsets are split over several CTAs, 512 each), one thread per diagonal
+//    offset; each thread runs the whole covariance -> rotation -> score ->
+//    threshold loop of its offset sequentially and keeps its best; the CTA
+//    reduces (max score, lowest offset index), across CTAs through a packed
+//    64-bit atomic maximum.
+//  * refinement (every fragment-based superposition refinement): pairs taken
+//    from a work list sorted by position count; 16 lanes per pair (32 after
+//    the --pre-score filter, 64 warps for pairs of 1,536+ positions) take the
+//    pair's admissible (fragment position, fragment length) variants from a
+//    pool and advance one pass over the positions at a time; the lanes
+//    reduce (max score, lowest variant index).  The distance-threshold
+//    covariance pass of iteration k+1 is fused into the scoring pass of
+//    iteration k.
+//  * DP: pairs from a work list (largest matrices first), one warp per pair;
+//    the warp sweeps strips of 32*R rows along anti-diagonals (R rows per
+//    lane, register-blocked), left/up/diagonal values move between lanes by
+//    shuffles, each lane packs the 2-bit directions of its cells into
+//    traceback words.  A long pair's strips run as a wavefront over several
+//    single-warp CTAs (cooperative launch, bounded waits on progress counters).
 //  * traceback, alignment rows, bookkeeping: one thread per pair.
 // All floating-point reductions are sequential per thread in forward position
 // order (blocks of BLK positions, Neumaier-compensated), so results do not
