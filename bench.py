@@ -46,8 +46,8 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 # k_findfrag DRAM read + write per pair (ncu, 2 queries x 40,000 references:
-# 101.39 MB + 6.31 MB for 13,333 pairs)
-FINDFRAG_DRAM_BYTES_PER_PAIR = (101.39e6 + 6.31e6) / 13333
+# 102.29 MB + 5.99 MB for 13,333 pairs)
+FINDFRAG_DRAM_BYTES_PER_PAIR = (102.29e6 + 5.99e6) / 13333
 
 METRIC = "pairs/s on 1 B200 at |dTM|<=1e-4; batched+adjoint vs plain; HBM % of peak"
 UNIT = "pairs/s"
@@ -287,7 +287,7 @@ def run_ours(args):
     seed_ms = float(st_ms[0])
     achieved = algo_bytes / (seed_ms / 1000.0) / 1e9 if seed_ms > 0 else 0.0
     # DRAM bytes of one seed launch, scaled by pairs from an ncu capture of a
-    # smaller case of the same workload (profiles/top3_kernels_c1_2x40000.md)
+    # smaller case of the same workload (profiles/top_kernels_c1_2x40000.md)
     step_pairs_avg = done_pairs / args.steps
     nsub = max(1, min(6, int(step_pairs_avg) // 16384))
     traffic = FINDFRAG_DRAM_BYTES_PER_PAIR * step_pairs_avg / nsub
