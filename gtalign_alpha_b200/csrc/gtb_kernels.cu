@@ -450,7 +450,12 @@ __global__ void __launch_bounds__(128) k_findfrag(Blk B, Bat T) {
     G.alc = nullptr;
     float lbest = 0.f;
     int lsi = 0x7fffffff;
-    for (int si = s0 + (int)threadIdx.x; si <= s1; si += blockDim.x) {
+    // offsets handed out one at a time (a thread's offsets still come in
+    // increasing order, so its strict-improvement rule keeps the lowest index)
+    __shared__ int s_next;
+    if (threadIdx.x == 0) s_next = s0 + (int)blockDim.x;
+    __syncthreads();
+    for (int si = s0 + (int)threadIdx.x; si <= s1; si = atomicAdd(&s_next, 1)) {
         int ab = n1 + si * step;
         int qpos = ab > 0 ? ab : 0;
         int rpos = -ab > 0 ? -ab : 0;
