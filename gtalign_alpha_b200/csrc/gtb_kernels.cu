@@ -25,6 +25,7 @@
 // All floating-point reductions are sequential per thread in forward position
 // order (blocks of BLK positions, Neumaier-compensated), so results do not
 // depend on the launch geometry.
+#include <type_traits>
 #include "gtb_device.cuh"
 #include "gtb_kernels.cuh"
 
@@ -1185,6 +1186,7 @@ __device__ __forceinline__ bool dp_pair(const float* t, float d02, float gcost, 
         }
         float uplast = 0.f, rb = 0.f;
         unsigned* bts = bt + (long long)s * ngrp * 32 + lane;
+        const bool full = (s + 1) * ROWS <= lq;    // every lane has R rows
         __syncwarp();
         for (int g = 0; g < ngrp; g++) {
             unsigned acc = 0u;
@@ -1202,46 +1204,53 @@ __device__ __forceinline__ bool dp_pair(const float* t, float d02, float gcost, 
                 __threadfence();
                 if (*err) return false;
             }
-#pragma unroll
-            for (int u = 0; u < SPW; u++) {
-                const int tt = g * SPW + u;   // steps past W find j >= lr on every lane
-                const int j = tt - lane;
-                if ((tt & 31) == 0) {
-                    int jj = tt + lane;
-                    if (WAVE) rb = (s > 0 && jj < lr) ? __ldcg(row + jj) : 0.f;
-                    else rb = (s > 0 && jj < lr) ? row[jj] : 0.f;
-                }
-                float upv = __shfl_up_sync(FULL, h[R - 1], 1);
-                float up0 = __shfl_sync(FULL, rb, tt & 31);
-                if (lane == 0) upv = (j < lr) ? up0 : 0.f;
-                if (j >= 0 && j < lr && nv > 0) {
-                    float4 c4 = __ldg(r4 + j);
-                    char css = usess ? rs[j] : 0;
-                    float up = upv, dg = uplast;
-#pragma unroll
-                    for (int r = 0; r < R; r++) {
-                        if (r < nv) {
-                            float v = tmterm(d02, dist2(tx[r], ty[r], tz[r], c4.x, c4.y, c4.z));
-                            if (usess) v = __fadd_rn(v, __fmul_rn((float)(qss[r] == css), 0.5f));
-                            v = __fadd_rn(v, gap0 ? dg : fabsf(dg));
-                            int bk = BT_DIAG;
-                            float l = h[r];
-                            if (!gap0 && l < 0.f) l = __fsub_rn(gcost, l);
-                            if (v < l) { v = l; bk = BT_LEFT; }
-                            float uu = up;
-                            if (!gap0 && uu < 0.f) uu = __fsub_rn(gcost, uu);
-                            if (v < uu) { v = uu; bk = BT_UP; }
-                            float w = (gap0 || bk != BT_DIAG) ? v : -v;
-                            dg = h[r];   // (row r, j-1): the next row's diagonal
-                            up = w;      // (row r, j):   the next row's up
-                            h[r] = w;
-                            acc |= (unsigned)bk << (2 * R * u + 2 * r);
-                        }
-                    }
-                    if (lane == 31 && nv == R) row[j] = h[R - 1];
-                }
-                uplast = upv;
+            if ((g * SPW & 31) == 0) {            // the previous strip's last row, 32 columns
+                int jj = g * SPW + lane;
+                if (WAVE) rb = (s > 0 && jj < lr) ? __ldcg(row + jj) : 0.f;
+                else rb = (s > 0 && jj < lr) ? row[jj] : 0.f;
             }
+            // SPW steps; CHK: some lane may be outside the matrix or have
+            // fewer than R rows (strip ramps, the last strip)
+            auto steps = [&](auto chk) {
+                constexpr bool CHK = decltype(chk)::value;
+#pragma unroll
+                for (int u = 0; u < SPW; u++) {
+                    const int tt = g * SPW + u;   // steps past W find j >= lr on every lane
+                    const int j = tt - lane;
+                    float upv = __shfl_up_sync(FULL, h[R - 1], 1);
+                    float up0 = __shfl_sync(FULL, rb, tt & 31);
+                    if (lane == 0) upv = (!CHK || j < lr) ? up0 : 0.f;
+                    if (!CHK || (j >= 0 && j < lr && nv > 0)) {
+                        float4 c4 = __ldg(r4 + j);
+                        char css = usess ? rs[j] : 0;
+                        float up = upv, dg = uplast;
+#pragma unroll
+                        for (int r = 0; r < R; r++) {
+                            if (!CHK || r < nv) {
+                                float v = tmterm(d02, dist2(tx[r], ty[r], tz[r], c4.x, c4.y, c4.z));
+                                if (usess) v = __fadd_rn(v, __fmul_rn((float)(qss[r] == css), 0.5f));
+                                v = __fadd_rn(v, gap0 ? dg : fabsf(dg));
+                                int bk = BT_DIAG;
+                                float l = h[r];
+                                if (!gap0 && l < 0.f) l = __fsub_rn(gcost, l);
+                                if (v < l) { v = l; bk = BT_LEFT; }
+                                float uu = up;
+                                if (!gap0 && uu < 0.f) uu = __fsub_rn(gcost, uu);
+                                if (v < uu) { v = uu; bk = BT_UP; }
+                                float w = (gap0 || bk != BT_DIAG) ? v : -v;
+                                dg = h[r];   // (row r, j-1): the next row's diagonal
+                                up = w;      // (row r, j):   the next row's up
+                                h[r] = w;
+                                acc |= (unsigned)bk << (2 * R * u + 2 * r);
+                            }
+                        }
+                        if (lane == 31 && (!CHK || nv == R)) row[j] = h[R - 1];
+                    }
+                    uplast = upv;
+                }
+            };
+            if (full && g * SPW >= 31 && (g + 1) * SPW <= lr) steps(std::false_type{});
+            else steps(std::true_type{});
             bts[g * 32] = acc;
             if (WAVE && lane == 31) {
                 __threadfence();              // this group's row values before the count
