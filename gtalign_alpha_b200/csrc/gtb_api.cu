@@ -78,6 +78,7 @@ extern "C" gtb_status gtb_create(int device, size_t mem_bytes, const gtb_options
     }
     for (int k = 0; k < 8; k++) CK(cudaEventCreate(&h->ev[k]));
     h->dw_cap = dp_wave_capacity();
+    configure_kernels();
     CK(cudaHostAlloc((void**)&h->h_flag, gtb_handle::NWAVE * gtb_handle::NSUB * sizeof(int),
                      cudaHostAllocDefault));
     h->sub[0] = h->st;

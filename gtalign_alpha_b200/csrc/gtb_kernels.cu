@@ -1110,6 +1110,23 @@ static void launch_refine_k(int mode, const Blk& B, const Bat& T, cudaStream_t s
     }
 }
 
+// The refinement kernels re-read each pair's positions on every pass: ask
+// for the smallest shared-memory carve-out that holds three CTAs (3 x 20 kB
+// of their static arrays), leaving the rest of the SM's 256 kB to L1.
+template <int LPP, bool LONG>
+static void carve_refine() {
+    const void* ks[6] = {(const void*)k_refine<RM_INIT, LPP, LONG>, (const void*)k_refine<RM_DP, LPP, LONG>,
+                         (const void*)k_refine<RM_FIN1, LPP, LONG>, (const void*)k_refine<RM_FIN2, LPP, LONG>,
+                         (const void*)k_refine<RM_PROD1, LPP, LONG>, (const void*)k_refine<RM_PROD2, LPP, LONG>};
+    for (const void* k : ks) cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, 27);
+}
+
+void configure_kernels() {
+    carve_refine<16, false>();
+    carve_refine<32, false>();
+    carve_refine<32, true>();
+}
+
 static void launch_refine_long_fin(int mode, const Blk& B, const Bat& T, cudaStream_t st) {
     const int ng = (T.rl_nlmax + 3) / 4;
     switch (mode) {

@@ -127,6 +127,8 @@ void launch_dp(const Blk& B, const Bat& T, int tfmsrc, int gap0, float gcost, in
 void launch_btck(const Blk& B, const Bat& T, int constrained, cudaStream_t st);
 // CTAs that the wavefront DP may keep resident at once on this device
 int dp_wave_capacity();
+// per-device kernel attributes (shared-memory carve-outs), once per device
+void configure_kernels();
 void launch_post(const Blk& B, const Bat& T, int dpi, int maxit, int prescreen,
                  float prescore, cudaStream_t st);
 void launch_lowscore(const Blk& B, const Bat& T, float thr, cudaStream_t st);

@@ -79,6 +79,7 @@ cudaError_t setup(int dev, cudaStream_t st) {
     if ((e = cudaGetSymbolAddress((void**)&D.d82, g_noalloc_d82)) != cudaSuccess) return e;
     if ((e = cudaGetSymbolAddress((void**)&D.d0fin, g_noalloc_d0fin)) != cudaSuccess) return e;
     make_tables(h_tbl[0], h_tbl[1], h_tbl[2], TBLN);
+    configure_kernels();
     if ((e = cudaMemcpyAsync(D.d0, h_tbl[0], sizeof(h_tbl[0]), cudaMemcpyHostToDevice, st)) != cudaSuccess) return e;
     if ((e = cudaMemcpyAsync(D.d82, h_tbl[1], sizeof(h_tbl[1]), cudaMemcpyHostToDevice, st)) != cudaSuccess) return e;
     if ((e = cudaMemcpyAsync(D.d0fin, h_tbl[2], sizeof(h_tbl[2]), cudaMemcpyHostToDevice, st)) != cudaSuccess) return e;
