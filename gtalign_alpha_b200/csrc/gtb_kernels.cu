@@ -26,6 +26,7 @@
 // order (blocks of BLK positions, Neumaier-compensated), so results do not
 // depend on the launch geometry.
 #include <type_traits>
+#include "gtb200.h"
 #include "gtb_device.cuh"
 #include "gtb_kernels.cuh"
 
@@ -1710,7 +1711,7 @@ void launch_stages(const Blk& B, const Bat& T, int refinement, int depth, int co
     launch_dp(B, T, DP_TFM_GRAND, 1, 0.0f, 0, 0, 1, st);
     launch_btck(B, T, 0, st);
     launch_refine(RM_FIN1, B, T, st, few);
-    if (!(depth == 3 || refinement == 0)) launch_refine(RM_FIN2, B, T, st, few);
+    if (!(depth == 3 || refinement == GTB_REFINEMENT_COARSE)) launch_refine(RM_FIN2, B, T, st, few);
     launch_dp(B, T, DP_TFM_GRAND, 1, 0.0f, 0, 0, 1, st);
     launch_btck(B, T, 1, st);
     launch_alnstr(B, T, st);

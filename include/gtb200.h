@@ -30,6 +30,15 @@ typedef enum {
     GTB_ERR_NOT_BUILT = 6     /* library built without device code */
 } gtb_status;
 
+/* --refinement codes of the gtalign command line (CLOptions.h:121-128) */
+enum {
+    GTB_REFINEMENT_LOG = 0,     /* production phase 2 by log search */
+    GTB_REFINEMENT_COARSE = 1,  /* no final phase 2 (the --speed 10..13 presets) */
+    GTB_REFINEMENT_ONE = 2,     /* one fragment length in phase 2 (default) */
+    GTB_REFINEMENT_FULL = 3,    /* every fragment length in production phase 2 */
+    GTB_REFINEMENT_FULLA = 4    /* every fragment length in both final phases 2 */
+};
+
 /* Field indices of the reference's SoA batch (PM2DVectorFields.h:220-239):
  * pmbeg[f]/pmend[f] delimit field f over all structures of a block. */
 enum {
@@ -61,7 +70,11 @@ enum { GTB_ERR_TMQ = 0, GTB_ERR_TMR = 1, GTB_ERR_RMSD = 2, GTB_NERR = 4 };
 /* Options the path reads (CuBatch.cu:353-366, custage_fin.cu:243-245,409),
  * with the values of the gtalign command line. */
 typedef struct {
-    int   refinement;        /* --refinement 0 (coarse) or 1 (one search) */
+    int   refinement;        /* --refinement, the command line's codes
+                                (CLOptions.h:121-128): 1 coarse, 2 one search
+                                (the command line's default); 0 log search,
+                                3 full search and 4 full search in both final
+                                phases are GTB_ERR_UNSUPPORTED */
     int   depth;             /* --depth 0..3 (3 = shallow: seed step 5) */
     int   convergence;       /* --convergence 1..30 */
     float prescore;          /* --pre-score [0,1) */

@@ -52,6 +52,12 @@
 #define RM_CONVEPS 1.e-5f
 #define SCORE_CONVEPS 1.e-6f
 #define FRAG_NSUB 6
+/* --refinement codes (CLOptions.h:121-128) */
+#define REF_LOG 0
+#define REF_COARSE 1
+#define REF_ONE 2
+#define REF_FULL 3
+#define REF_FULLA 4
 #define FRAG_STEP 40
 #define NMAXCONVIT 20
 #define FIN_MAXNPOS 128
@@ -558,19 +564,25 @@ static void refine_stage(pairctx* P, int dpmode, float d0, float d02, int chk,
     }
 }
 
-/* Final phase 2, MpStageFin.cpp:270-480 */
-static void final_phase2(pairctx* P) {
+/* Final phase 2: one fragment length (the phase-1 winner's, 0 promoted to 1)
+ * at nf positions around the phase-1 position (MpStageFin.cpp:270-480), or,
+ * with full = 1 (--refinement 4), every fragment length at each position,
+ * variant index = position factor * 6 + length index, no promotion
+ * (covariance_fin_dp_refn_complete.cu:464-630, custage_fin.cu:272-275,344). */
+static void final_phase2(pairctx* P, int full) {
     int maxalnmax = P->qmax < P->rmax ? P->qmax : P->rmax;
     int nf = 2 * maxalnmax < FIN_MAXNPOS ? 2 * maxalnmax : FIN_MAXNPOS;
     kspace s = {1, 0, 0, P->aq, P->ar};
     int n = P->naln;
     float wbest = 0.f, wtfm[12];
     int wsi = -1;
-    for (int si = 0; si < nf; si++) {
-        int sfragndx = P->sfndx;
+    int nsi = full ? nf * FRAG_NSUB : nf;
+    for (int si = 0; si < nsi; si++) {
+        int sfragfct = full ? si / FRAG_NSUB : si;
+        int sfragndx = full ? si % FRAG_NSUB : P->sfndx;
         int sfragpos = P->sfpos;
-        if (sfragndx == 0) sfragndx++;
-        sfragpos += (si - (nf >> 1));
+        if (!full && sfragndx == 0) sfragndx++;
+        sfragpos += (sfragfct - (nf >> 1));
         int fraglen = frag_length(n, sfragndx);
         if (fraglen < 1) continue;
         if (sfragpos < 0 || n + 1 <= sfragpos + fraglen) continue;
@@ -721,7 +733,46 @@ static double rmsd_from_sums(const double* v, double n) {
     return e > 0.0 ? sqrt(e) : 0.0;
 }
 
-static void production(pairctx* P) {
+/* Production phase 2 by log search (--refinement 0,
+ * covariance_production_dp_refn_complete.cu:752-915): from the phase-1
+ * position, steps of +-32, 16, ..., 1 positions; at each step the five
+ * fragment lengths 1..5 run in order, each carrying the best score so far
+ * (the grand best of phase 1 to begin with), and the position moves to the
+ * step's position when one of them raised it.  A fragment that reaches past
+ * the alignment's end by less than the step is shifted back to end there. */
+static void production_logsearch(pairctx* P, const kspace* s, int n) {
+    float bestorg = P->grand, best = bestorg, tb[12];
+    int posorg = P->sfpos;
+    for (int st = 32; st >= 1; st >>= 1)
+        for (int sgn = 1; sgn >= -1; sgn -= 2) {
+            int step = sgn * st;
+            int sfragpos = posorg + step;
+            int ext = step > 0 ? step : 0;
+            for (int sfragndx = 1; sfragndx < FRAG_NSUB; sfragndx++) {
+                int fraglen = frag_length(n, sfragndx);
+                if (fraglen < 1) continue;
+                if (sfragpos < 0 || n + ext <= sfragpos + fraglen) continue;
+                int delta = sfragpos + fraglen - n;
+                int kf = sfragpos - (delta > 0 ? delta : 0);
+                float bp = best;
+                refine_loop(P, s, n, kf, fraglen, P->d0fin, P->d0fin * P->d0fin, 0, P->d82,
+                            best, &best, tb);
+                if (bp < best) posorg = sfragpos;
+            }
+        }
+    if (best <= bestorg) return;
+    prodwin w;
+    w.best = best;
+    if (P->lq != P->lr) {
+        int gl = P->lq > P->lr ? P->lq : P->lr;
+        float g0 = c_d0fin(gl, gl);
+        w.gbest = score_pass(P, s, n, tb, g0 * g0, 0, P->d82, 0, NULL);
+    } else w.gbest = best;
+    memcpy(w.tfm, tb, sizeof(tb));
+    prod_write(P, &w);
+}
+
+static void production(pairctx* P, int refinement) {
     kspace s = {1, 0, 0, P->aq, P->ar};
     int n = P->naln;
     int nloc = nlocsteps_refine(P);
@@ -773,26 +824,35 @@ static void production(pairctx* P) {
         prod_write(P, &w);
         P->sfndx = w.ndx; P->sfpos = w.pos;
     }
-    /* phase 2 (one-search and coarse) */
-    int maxalnmax = P->qmax < P->rmax ? P->qmax : P->rmax;
-    int nf = 2 * maxalnmax < FIN_MAXNPOS ? 2 * maxalnmax : FIN_MAXNPOS;
-    prodwin w2; w2.best = 0.f; w2.si = -1;
-    for (int si = 0; si < nf && n > 0; si++) {
-        int sfragndx = P->sfndx, sfragpos = P->sfpos;
-        sfragpos += (si - (nf >> 1));
-        if (sfragndx == 0) sfragndx++;
-        int fraglen = frag_length(n, sfragndx);
-        if (fraglen < 1) continue;
-        if (sfragpos < 0 || n + 1 <= sfragpos + fraglen) continue;
-        float best, gbest, tb[12];
-        prod_variant(P, &s, n, sfragpos, fraglen, &best, &gbest, tb);
-        if (best > 0.f && w2.best < best) {
-            w2.best = best; w2.gbest = gbest; w2.si = si; memcpy(w2.tfm, tb, sizeof(tb));
+    /* phase 2 */
+    if (refinement == REF_LOG) production_logsearch(P, &s, n);
+    else {
+        /* one fragment length (coarse, one-search: MpStageFin.cpp:1310-1525)
+         * or every length (full, fullA: covariance_production_dp_refn_complete.cu:381-530,
+         * custage_fin.cu:475-481), nf positions around the phase-1 position */
+        int full = refinement >= REF_FULL;
+        int maxalnmax = P->qmax < P->rmax ? P->qmax : P->rmax;
+        int nf = 2 * maxalnmax < FIN_MAXNPOS ? 2 * maxalnmax : FIN_MAXNPOS;
+        int nsi = full ? nf * FRAG_NSUB : nf;
+        prodwin w2; w2.best = 0.f; w2.si = -1;
+        for (int si = 0; si < nsi && n > 0; si++) {
+            int sfragfct = full ? si / FRAG_NSUB : si;
+            int sfragndx = full ? si % FRAG_NSUB : P->sfndx, sfragpos = P->sfpos;
+            sfragpos += (sfragfct - (nf >> 1));
+            if (!full && sfragndx == 0) sfragndx++;
+            int fraglen = frag_length(n, sfragndx);
+            if (fraglen < 1) continue;
+            if (sfragpos < 0 || n + 1 <= sfragpos + fraglen) continue;
+            float best, gbest, tb[12];
+            prod_variant(P, &s, n, sfragpos, fraglen, &best, &gbest, tb);
+            if (best > 0.f && w2.best < best) {
+                w2.best = best; w2.gbest = gbest; w2.si = si; memcpy(w2.tfm, tb, sizeof(tb));
+            }
         }
-    }
-    if (w2.si >= 0 && P->grand < w2.best) {
-        P->grand = w2.best;
-        prod_write(P, &w2);
+        if (w2.si >= 0 && P->grand < w2.best) {
+            P->grand = w2.best;
+            prod_write(P, &w2);
+        }
     }
     /* FP64 recomputation of reported values */
     if (n > 0) {
@@ -931,12 +991,12 @@ static void run_pair(pairctx* P, char* alndst) {
     dp_run(P, P->tfm_gr, 1, 0.f, 0, P->d02);
     btck_matched(P);
     refine_stage(P, 2, P->d0, P->d02, 1, -1.0f, 1, 1);
-    if (!(o->depth == 3 || o->refinement == 1))
-        final_phase2(P);
+    if (!(o->depth == 3 || o->refinement == REF_COARSE))
+        final_phase2(P, o->refinement == REF_FULLA);
     dp_run(P, P->tfm_gr, 1, 0.f, 0, P->d02);
     btck_constrained(P);
     if (alndst) production_alignment(P, alndst);
-    production(P);
+    production(P, o->refinement);
     if (o->referenced) {
         float* t = P->tfm_gr;
         float R[9];

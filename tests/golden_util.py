@@ -30,13 +30,13 @@ def load(name):
 
 def cli_options(opts):
     """Translate the reference CLI options of a set into oracle/library options."""
-    d = dict(refinement=1, convergence=18, prescore=0.4, scorethld=0.5, depth=2,
+    d = dict(refinement=2, convergence=18, prescore=0.4, scorethld=0.5, depth=2,
              symmetric=0, referenced=0, nodeletions=0)
     i = 0
     while i < len(opts):
         o = opts[i]
         if o == "--speed=13":
-            d["refinement"], d["convergence"] = 0, 2
+            d["refinement"], d["convergence"] = 1, 2
         elif o.startswith("--pre-score="):
             d["prescore"] = float(o.split("=")[1])
         elif o == "-s":
