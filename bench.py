@@ -371,7 +371,7 @@ def run_reference_sample(wl, nq: int, nref: int, threads: int):
     import pyoracle
     q, r = synth.pack(sub.queries), synth.pack(sub.refs)
     t = time.time()
-    pyoracle.process_block(q, r, pyoracle.opts_from(refinement=2, convergence=18, prescore=0.4,
+    pyoracle.process_block(q, r, pyoracle.opts_from(refinement=1, convergence=18, prescore=0.4,
                                                     scorethld=0.5), nthreads=threads)
     return nq * nref, time.time() - t, "port"
 

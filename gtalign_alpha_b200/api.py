@@ -62,7 +62,7 @@ class Options:
     Defaults are the command line's defaults except ``nodetailedsearch``,
     which must be 1 (the spatial-index search stage is not in this library).
     """
-    refinement: int = 2        # 1 coarse, 2 one search (CLOptions.h:121-128)
+    refinement: int = 1
     depth: int = 2
     convergence: int = 18
     prescore: float = 0.4
@@ -77,11 +77,11 @@ class Options:
     @classmethod
     def speed(cls, level: int, **kw) -> "Options":
         """The --speed presets that keep the detailed search off
-        (gtalign.cpp:833-867): 13 = --no-detailed-search --refinement=1
-        (coarse) --convergence=2."""
+        (gtalign.cpp:833-867): 13 = --no-detailed-search --refinement=0
+        --convergence=2."""
         if level != 13:
             raise GTBError(4, "only --speed=13 runs without the detailed search")
-        o = cls(refinement=1, convergence=2, **kw)
+        o = cls(refinement=0, convergence=2, **kw)
         return o
 
     def _c(self) -> _COptions:

@@ -134,9 +134,8 @@ static gtb_status check_options(gtb_handle* h) {
         snprintf(h->err, sizeof(h->err), "--add-search-by-ss and --2tm-score are not implemented");
         return GTB_ERR_UNSUPPORTED;
     }
-    if (o.refinement != GTB_REFINEMENT_COARSE && o.refinement != GTB_REFINEMENT_ONE) {
-        snprintf(h->err, sizeof(h->err), "--refinement %d not implemented (1 coarse or 2 one search)",
-                 o.refinement);
+    if (o.refinement < 0 || o.refinement > 1) {
+        snprintf(h->err, sizeof(h->err), "--refinement %d not implemented (0 or 1)", o.refinement);
         return GTB_ERR_UNSUPPORTED;
     }
     if (o.polish_steps < 0 || o.polish_steps > 50) {

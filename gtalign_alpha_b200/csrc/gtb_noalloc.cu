@@ -100,7 +100,7 @@ extern "C" gtb_status gtb_process_block_noalloc(int device, const gtb_options* o
         return GTB_ERR_ARG;
     }
     if (!opts->nodetailedsearch || opts->addsearchbyss || opts->twotmscore ||
-        (opts->refinement != GTB_REFINEMENT_COARSE && opts->refinement != GTB_REFINEMENT_ONE)) {
+        opts->refinement < 0 || opts->refinement > 1) {
         setmsg(errbuf, errlen, "option combination not implemented (refinement %lld, detailed %lld)",
                opts->refinement, !opts->nodetailedsearch);
         return GTB_ERR_UNSUPPORTED;

@@ -30,13 +30,14 @@ typedef enum {
     GTB_ERR_NOT_BUILT = 6     /* library built without device code */
 } gtb_status;
 
-/* --refinement codes of the gtalign command line (CLOptions.h:121-128) */
+/* --refinement codes of the gtalign command line (gtalign.h:154-156); the
+ * reference stores code + 1 (gtalign.cpp:776-780, CLOptions.h:121-128) */
 enum {
-    GTB_REFINEMENT_LOG = 0,     /* production phase 2 by log search */
-    GTB_REFINEMENT_COARSE = 1,  /* no final phase 2 (the --speed 10..13 presets) */
-    GTB_REFINEMENT_ONE = 2,     /* one fragment length in phase 2 (default) */
-    GTB_REFINEMENT_FULL = 3,    /* every fragment length in production phase 2 */
-    GTB_REFINEMENT_FULLA = 4    /* every fragment length in both final phases 2 */
+    GTB_REFINEMENT_LOG = -1,    /* production phase 2 by log search */
+    GTB_REFINEMENT_COARSE = 0,  /* no final phase 2 (the --speed 10..13 presets) */
+    GTB_REFINEMENT_ONE = 1,     /* one fragment length in phase 2 (default) */
+    GTB_REFINEMENT_FULL = 2,    /* every fragment length in production phase 2 */
+    GTB_REFINEMENT_FULLA = 3    /* every fragment length in both final phases 2 */
 };
 
 /* Field indices of the reference's SoA batch (PM2DVectorFields.h:220-239):
@@ -70,11 +71,8 @@ enum { GTB_ERR_TMQ = 0, GTB_ERR_TMR = 1, GTB_ERR_RMSD = 2, GTB_NERR = 4 };
 /* Options the path reads (CuBatch.cu:353-366, custage_fin.cu:243-245,409),
  * with the values of the gtalign command line. */
 typedef struct {
-    int   refinement;        /* --refinement, the command line's codes
-                                (CLOptions.h:121-128): 1 coarse, 2 one search
-                                (the command line's default); 0 log search,
-                                3 full search and 4 full search in both final
-                                phases are GTB_ERR_UNSUPPORTED */
+    int   refinement;        /* --refinement (GTB_REFINEMENT_*): 0 coarse or 1 one
+                                search; -1, 2 and 3 are GTB_ERR_UNSUPPORTED */
     int   depth;             /* --depth 0..3 (3 = shallow: seed step 5) */
     int   convergence;       /* --convergence 1..30 */
     float prescore;          /* --pre-score [0,1) */

@@ -52,7 +52,7 @@
 #define RM_CONVEPS 1.e-5f
 #define SCORE_CONVEPS 1.e-6f
 #define FRAG_NSUB 6
-/* --refinement codes (CLOptions.h:121-128) */
+/* stored --refinement codes, command line code + 1 (CLOptions.h:121-128) */
 #define REF_LOG 0
 #define REF_COARSE 1
 #define REF_ONE 2

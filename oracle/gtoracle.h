@@ -33,8 +33,9 @@ enum { GTO_ERR_TMQ = 0, GTO_ERR_TMR, GTO_ERR_RMSD, GTO_NERR = 4 };
 
 typedef struct {
     int   stepinit;      /* 1 (default depth) or 5 (--depth=3 shallow) */
-    int   refinement;    /* --refinement: 0 log search, 1 coarse, 2 one search,
-                            3 full search, 4 full search in both final phases */
+    int   refinement;    /* the reference's stored code (command line code + 1):
+                            0 log search, 1 coarse, 2 one search, 3 full
+                            search, 4 full search in both final phases */
     int   depth;         /* 0..3 (3 = shallow) */
     int   convergence;   /* --convergence (max DP iterations in stage 2b) */
     float prescore;      /* --pre-score */

@@ -77,13 +77,14 @@ class OracleResult:
     rss: np.ndarray
 
 
-def opts_from(refinement: int = 1, convergence: int = 2, prescore: float = 0.0,
+def opts_from(refinement: int = 0, convergence: int = 2, prescore: float = 0.0,
               scorethld: float = 0.0, depth: int = 2, symmetric: int = 0,
               referenced: int = 0, nodeletions: int = 0) -> _Opts:
-    """Options in the gtalign command line's encoding: --refinement 0 log
-    search, 1 coarse, 2 one search (the CLI default), 3 full, 4 full in both
-    final phases; --depth 0..3 (3 = shallow)."""
-    return _Opts(5 if depth == 3 else 1, refinement, depth, convergence,
+    """Options in the gtalign command line's encoding: --refinement -1 log
+    search, 0 coarse, 1 one search (the default), 2 full, 3 full in both final
+    phases (the oracle, like the reference, stores code + 1); --depth 0..3
+    (3 = shallow)."""
+    return _Opts(5 if depth == 3 else 1, refinement + 1, depth, convergence,
                  prescore, scorethld, symmetric, referenced, nodeletions)
 
 

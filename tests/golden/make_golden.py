@@ -13,7 +13,7 @@ by a rigid rotation + translation (which leaves every score unchanged in
 exact arithmetic); the agreement between those two reference runs is the
 reference's own numerical reproducibility and is stored as `self_agreement`.
 
-    python tests/golden/make_golden.py        (needs oracle/_ref/gtalign)
+    python tests/golden/make_golden.py [set ...]   (needs oracle/_ref/gtalign)
 """
 from __future__ import annotations
 
@@ -45,15 +45,33 @@ SETS = {
     "c0_sym_ref_nodel": (lambda: synth.config0(seed=104, n_refs=40, qlen=100),
                          ["--speed=13", "--pre-score=0", "-s", "0", "--symmetric",
                           "--referenced", "--no-deletions"]),
+    # the final stage's phase-2 forms, one set per --refinement code, on
+    # homologs of the query only (one clear optimum per pair, so the level's
+    # small TM differences show); run with one compute thread: the
+    # reference's CPU build stalls intermittently in its full-search levels
+    # with several threads
+    "c0_level_m1": (lambda: synth.config0(seed=201, n_refs=40, qlen=180, homolog_frac=1.0),
+                    ["--no-detailed-search", "--refinement=-1", "--pre-score=0", "-s", "0"], 1),
+    "c0_level_0": (lambda: synth.config0(seed=201, n_refs=40, qlen=180, homolog_frac=1.0),
+                   ["--no-detailed-search", "--refinement=0", "--pre-score=0", "-s", "0"], 1),
+    "c0_level_1": (lambda: synth.config0(seed=201, n_refs=40, qlen=180, homolog_frac=1.0),
+                   ["--no-detailed-search", "--refinement=1", "--pre-score=0", "-s", "0"], 1),
+    "c0_level_2": (lambda: synth.config0(seed=201, n_refs=40, qlen=180, homolog_frac=1.0),
+                   ["--no-detailed-search", "--refinement=2", "--pre-score=0", "-s", "0"], 1),
+    "c0_level_3": (lambda: synth.config0(seed=201, n_refs=40, qlen=180, homolog_frac=1.0),
+                   ["--no-detailed-search", "--refinement=3", "--pre-score=0", "-s", "0"], 1),
+    "c0_shallow": (lambda: synth.config0(seed=108, n_refs=60, qlen=160),
+                   ["--no-detailed-search", "--depth=3", "--pre-score=0.3", "-s", "0.3",
+                    "--convergence=6"]),
 }
 
 
-def run(wl, opts):
+def run(wl, opts, threads=8):
     d = tempfile.mkdtemp(prefix="gtgold")
     try:
         synth.write_dirs(wl, d + "/q", d + "/r")
         subprocess.run([BIN, "--qrs=" + d + "/q", "--rfs=" + d + "/r", "-o", d + "/out",
-                        "--outfmt=1", "--cpu-threads=8", "--cpu-threads-reading=1"] + opts,
+                        "--outfmt=1", "--cpu-threads=%d" % threads, "--cpu-threads-reading=1"] + opts,
                        check=True, capture_output=True)
         res = {}
         for f in os.listdir(d + "/out"):
@@ -95,15 +113,18 @@ def agreement(a, b):
 def main():
     if not os.path.exists(BIN):
         sys.exit("build the reference first: make -f oracle/Makefile.ref")
-    for name, (mk, opts) in SETS.items():
+    names = sys.argv[1:] or list(SETS)
+    for name in names:
+        mk, opts = SETS[name][:2]
+        threads = SETS[name][2] if len(SETS[name]) > 2 else 8
         wl = mk()
-        res = run(wl, opts)
+        res = run(wl, opts, threads)
         wl2 = copy.deepcopy(wl)
         rng = np.random.default_rng(7)
         R = synth._rot_random(rng)
         q = wl2.queries[0]
         q.xyz = synth._pdb_round_fast(q.xyz.astype(np.float64) @ R.T + np.array([3.0, -5.0, 7.0]))
-        res2 = run(wl2, opts)
+        res2 = run(wl2, opts, threads)
         arrs = {}
         for tag, chains in (("q", wl.queries), ("r", wl.refs)):
             s = synth.pack(chains)

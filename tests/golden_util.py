@@ -7,7 +7,13 @@ import numpy as np
 from gtalign_alpha_b200.synth import SoA
 
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
-SETS = ["c0_speed13", "c0_default", "c0_filters", "c0_sym_ref_nodel"]
+# --refinement code -> the fixture set run at that code (homologs only)
+LEVEL_SETS = {-1: "c0_level_m1", 0: "c0_level_0", 1: "c0_level_1", 2: "c0_level_2",
+              3: "c0_level_3"}
+SETS = ["c0_speed13", "c0_default", "c0_filters", "c0_sym_ref_nodel", "c0_shallow"] + \
+    list(LEVEL_SETS.values())
+# the sets whose options the CUDA library implements
+LIBRARY_SETS = [s for s in SETS if s not in (LEVEL_SETS[-1], LEVEL_SETS[2], LEVEL_SETS[3])]
 
 
 def _soa(z, tag):
@@ -30,13 +36,19 @@ def load(name):
 
 def cli_options(opts):
     """Translate the reference CLI options of a set into oracle/library options."""
-    d = dict(refinement=2, convergence=18, prescore=0.4, scorethld=0.5, depth=2,
+    d = dict(refinement=1, convergence=18, prescore=0.4, scorethld=0.5, depth=2,
              symmetric=0, referenced=0, nodeletions=0)
     i = 0
     while i < len(opts):
         o = opts[i]
         if o == "--speed=13":
-            d["refinement"], d["convergence"] = 1, 2
+            d["refinement"], d["convergence"] = 0, 2
+        elif o.startswith("--refinement="):
+            d["refinement"] = int(o.split("=")[1])
+        elif o.startswith("--depth="):
+            d["depth"] = int(o.split("=")[1])
+        elif o.startswith("--convergence="):
+            d["convergence"] = int(o.split("=")[1])
         elif o.startswith("--pre-score="):
             d["prescore"] = float(o.split("=")[1])
         elif o == "-s":

@@ -37,7 +37,7 @@ def test_errors_without_device_are_status_codes(lib):
         pytest.skip("device present")
     from gtalign_alpha_b200.api import _COptions
     h = ctypes.c_void_p()
-    opts = _COptions(2, 2, 18, 0.4, 0, 0, 0, 1, 0, 0)
+    opts = _COptions(1, 2, 18, 0.4, 0, 0, 0, 1, 0, 0)
     lib.gtb_create.argtypes = [ctypes.c_int, ctypes.c_size_t, ctypes.POINTER(_COptions),
                                ctypes.POINTER(ctypes.c_void_p)]
     st = lib.gtb_create(0, 0, ctypes.byref(opts), ctypes.byref(h))

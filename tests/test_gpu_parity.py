@@ -47,7 +47,7 @@ def run_both(oracle, q, r, d, secstr=False):
     return res, ora
 
 
-@pytest.mark.parametrize("name", gu.SETS)
+@pytest.mark.parametrize("name", gu.LIBRARY_SETS)
 def test_golden_sets_bit_identical(oracle, name):
     q, r, qn, rn, meta = gu.load(name)
     d = gu.cli_options(meta["options"])
@@ -59,11 +59,11 @@ def test_golden_sets_bit_identical(oracle, name):
 
 
 OPTSETS = {
-    "speed13": dict(refinement=1, convergence=2, prescore=0.0, scorethld=0.0, symmetric=0, referenced=0, nodeletions=0),
-    "default": dict(refinement=2, convergence=18, prescore=0.0, scorethld=0.0, symmetric=0, referenced=0, nodeletions=0),
-    "filters": dict(refinement=2, convergence=18, prescore=0.4, scorethld=0.5, symmetric=0, referenced=0, nodeletions=0),
-    "shallow": dict(refinement=2, convergence=6, prescore=0.3, scorethld=0.3, symmetric=0, referenced=0, nodeletions=0, depth=3),
-    "sym": dict(refinement=2, convergence=4, prescore=0.0, scorethld=0.0, symmetric=1, referenced=1, nodeletions=1),
+    "speed13": dict(refinement=0, convergence=2, prescore=0.0, scorethld=0.0, symmetric=0, referenced=0, nodeletions=0),
+    "default": dict(refinement=1, convergence=18, prescore=0.0, scorethld=0.0, symmetric=0, referenced=0, nodeletions=0),
+    "filters": dict(refinement=1, convergence=18, prescore=0.4, scorethld=0.5, symmetric=0, referenced=0, nodeletions=0),
+    "shallow": dict(refinement=1, convergence=6, prescore=0.3, scorethld=0.3, symmetric=0, referenced=0, nodeletions=0, depth=3),
+    "sym": dict(refinement=1, convergence=4, prescore=0.0, scorethld=0.0, symmetric=1, referenced=1, nodeletions=1),
 }
 
 
@@ -174,7 +174,7 @@ def test_long_chain_assemblies(oracle):
     from gtalign_alpha_b200 import synth
     wl = synth.config2(seed=3, lengths=(1200, 2000))
     q, r = synth.pack(wl.queries), synth.pack(wl.refs)
-    d = dict(refinement=2, convergence=18, prescore=0.4, scorethld=0.5, symmetric=0,
+    d = dict(refinement=1, convergence=18, prescore=0.4, scorethld=0.5, symmetric=0,
              referenced=0, nodeletions=0)
     res, ora = run_both(oracle, q, r, d)
     assert_same(res, ora, q.n, r.n)

@@ -23,7 +23,7 @@ def _free_port():
 def _oracle_fn(q, r):
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import pyoracle
-    o = pyoracle.process_block(q, r, pyoracle.opts_from(refinement=1, convergence=2), nthreads=2)
+    o = pyoracle.process_block(q, r, pyoracle.opts_from(refinement=0, convergence=2), nthreads=2)
     return o.out, o.tfm
 
 

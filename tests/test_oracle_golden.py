@@ -46,7 +46,7 @@ def run_oracle(oracle, name):
     o = oracle.process_block(q, r, oracle.opts_from(
         refinement=d["refinement"], convergence=d["convergence"], prescore=d["prescore"],
         scorethld=d["scorethld"], symmetric=d["symmetric"], referenced=d["referenced"],
-        nodeletions=d["nodeletions"]))
+        nodeletions=d["nodeletions"], depth=d["depth"]))
     return q, r, qn, rn, meta, d, o
 
 
@@ -136,3 +136,30 @@ def test_oracle_homologs_overall(oracle):
             test_oracle_matches_reference(oracle, name)
     assert len(HOMOLOGS) >= 40
     assert np.mean(HOMOLOGS) >= 0.85, (np.mean(HOMOLOGS), len(HOMOLOGS))
+
+
+def test_refinement_levels_pinned(oracle):
+    """One homolog-only input, run by the reference at each --refinement code
+    (-1 log search, 0 coarse, 1 one search, 2 full, 3 full in both final
+    phases).  The oracle at the same code reproduces every pair (TM-scores
+    within 1e-4, identical alignment rows), and at any other code it
+    reproduces fewer: the five final-stage forms are told apart."""
+    n_match = {}
+    for lref, name in gu.LEVEL_SETS.items():
+        q, r, qn, rn, meta = gu.load(name)
+        for lo in gu.LEVEL_SETS:
+            o = oracle.process_block(q, r, oracle.opts_from(
+                refinement=lo, convergence=18, prescore=0.0, scorethld=0.0))
+            c = 0
+            for key, g in meta["results"].items():
+                a, b = key.split("|")
+                qi, ri = qn.index(a), rn.index(b)
+                out, rows = o.out[qi, ri], o.alns[qi][ri]
+                dd = max(abs(out[9] - g["tmq"]), abs(out[10] - g["tmr"]))
+                c += dd <= 1e-4 and rows[0] == g["query_aln"] and rows[2] == g["refrn_aln"]
+            n_match[lref, lo] = c
+        npairs = len(meta["results"])
+        assert n_match[lref, lref] >= 0.95 * npairs, (lref, n_match)
+        for lo in gu.LEVEL_SETS:
+            if lo != lref:
+                assert n_match[lref, lref] > n_match[lref, lo], (lref, lo, n_match)
