@@ -62,7 +62,7 @@ class Options:
     Defaults are the command line's defaults except ``nodetailedsearch``,
     which must be 1 (the spatial-index search stage is not in this library).
     """
-    refinement: int = 1
+    refinement: int = 1        # -1 log, 0 coarse, 1 one (default), 2 full, 3 full in both phases
     depth: int = 2
     convergence: int = 18
     prescore: float = 0.4

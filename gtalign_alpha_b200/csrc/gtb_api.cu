@@ -134,9 +134,9 @@ static gtb_status check_options(gtb_handle* h) {
         snprintf(h->err, sizeof(h->err), "--add-search-by-ss and --2tm-score are not implemented");
         return GTB_ERR_UNSUPPORTED;
     }
-    if (o.refinement < 0 || o.refinement > 1) {
-        snprintf(h->err, sizeof(h->err), "--refinement %d not implemented (0 or 1)", o.refinement);
-        return GTB_ERR_UNSUPPORTED;
+    if (o.refinement < GTB_REFINEMENT_LOG || o.refinement > GTB_REFINEMENT_FULLA) {
+        snprintf(h->err, sizeof(h->err), "--refinement %d out of -1..3", o.refinement);
+        return GTB_ERR_ARG;
     }
     if (o.polish_steps < 0 || o.polish_steps > 50) {
         snprintf(h->err, sizeof(h->err), "polish_steps %d out of 0..50", o.polish_steps);

@@ -640,35 +640,41 @@ __global__ void k_rlist_fill(Blk B, Bat T, int mode) {
 }
 
 // Variant list of one pair, enumerated compactly (admissible variants only).
-// Modes with 6 fragment lengths x step 40: variant si = fct*6 + ndx is
+// VK_STAGE (6 fragment lengths x step 40): variant si = fct*6 + ndx is
 // admissible when frag_length(n, ndx) >= 1 and 40*fct + fraglen < n + 40
-// (MpStage1.cpp:635-641); phase-2 modes: si in [0, nf) with 0 <= pos and
-// pos + fraglen <= n (MpStageFin.cpp:380-396).
+// (MpStage1.cpp:635-641).  VK_P2ONE (phase 2, one length: the phase-1
+// winner's, 0 promoted to 1): si in [0, nf), pos = pos1 - nf/2 + si, with
+// 0 <= pos and pos + fraglen <= n (MpStageFin.cpp:380-396).  VK_P2ALL (phase
+// 2, every length: --refinement 2 in production, 3 in both final phases):
+// si = fct*6 + ndx, pos = pos1 - nf/2 + fct, the same bounds
+// (covariance_production_dp_refn_complete.cu:381-530,
+// covariance_fin_dp_refn_complete.cu:464-630).  VK_LOG (one round of the
+// log search, covariance_production_dp_refn_complete.cu:836-880): lengths
+// 1..5 at pos = pos1 + step, si = ndx, admissible when 0 <= pos and
+// pos + fraglen < n + max(step, 0); a fragment reaching past the end is
+// shifted back to end at n.
+enum VariantKind { VK_STAGE = 0, VK_P2ONE = 1, VK_P2ALL = 2, VK_LOG = 3 };
+
 struct VariantList {
     int total;
-    int cnt[FRAG_NSUB], fl[FRAG_NSUB];
-    int lo, base, ndx2, fl2;  // phase 2
+    int cnt[FRAG_NSUB], fl[FRAG_NSUB], lo[FRAG_NSUB];
+    int base;                 // phase 2: position of si (or fct) = base + si; log: the round's position
 };
 
-__device__ __forceinline__ void variants_init(VariantList& V, bool phase2, int n, int maxalnmax,
-                                              int sfndx0, int sfpos0) {
+// the step of log-search round r: +32, -32, +16, -16, ..., +1, -1
+__device__ __forceinline__ int plog_step(int r) {
+    int st = 32 >> (r >> 1);
+    return (r & 1) ? -st : st;
+}
+
+__device__ __forceinline__ void variants_init(VariantList& V, int vk, int n, int maxalnmax,
+                                              int sfndx0, int sfpos0, int round) {
     V.total = 0;
-    V.lo = V.base = V.ndx2 = V.fl2 = 0;
+    V.base = 0;
 #pragma unroll
-    for (int d = 0; d < FRAG_NSUB; d++) { V.cnt[d] = 0; V.fl[d] = 0; }
+    for (int d = 0; d < FRAG_NSUB; d++) { V.cnt[d] = 0; V.fl[d] = 0; V.lo[d] = 0; }
     if (n <= 0) return;
-    if (phase2) {
-        int nf = 2 * maxalnmax < FIN_MAXNPOS ? 2 * maxalnmax : FIN_MAXNPOS;
-        V.ndx2 = sfndx0 == 0 ? 1 : sfndx0;
-        V.fl2 = frag_length(n, V.ndx2);
-        V.base = sfpos0 - (nf >> 1);            // pos = base + si
-        if (V.fl2 < 1) return;
-        int lo = -V.base > 0 ? -V.base : 0;     // pos >= 0
-        int hi = n - V.fl2 - V.base;            // pos + fl <= n
-        if (hi > nf - 1) hi = nf - 1;
-        V.lo = lo;
-        V.total = hi >= lo ? hi - lo + 1 : 0;
-    } else {
+    if (vk == VK_STAGE) {
         int NF = (int)ceilf((float)(maxalnmax + FRAG_STEP - MINFRAGLEN) / FRAG_STEP);
 #pragma unroll
         for (int d = 0; d < FRAG_NSUB; d++) {
@@ -683,30 +689,67 @@ __device__ __forceinline__ void variants_init(VariantList& V, bool phase2, int n
             V.cnt[d] = c;
             V.total += c;
         }
+        return;
+    }
+    if (vk == VK_LOG) {
+        int step = plog_step(round);
+        int pos = sfpos0 + step;
+        int ext = step > 0 ? step : 0;
+        V.base = pos;
+#pragma unroll
+        for (int d = 1; d < FRAG_NSUB; d++) {
+            int fl = frag_length(n, d);
+            int c = (fl >= 1 && pos >= 0 && pos + fl < n + ext) ? 1 : 0;
+            V.fl[d] = fl;
+            V.cnt[d] = c;
+            V.total += c;
+        }
+        return;
+    }
+    int nf = 2 * maxalnmax < FIN_MAXNPOS ? 2 * maxalnmax : FIN_MAXNPOS;
+    V.base = sfpos0 - (nf >> 1);                // pos = base + fct
+    const int lo = -V.base > 0 ? -V.base : 0;   // pos >= 0
+#pragma unroll
+    for (int d = 0; d < FRAG_NSUB; d++) {
+        bool use = vk == VK_P2ALL || d == (sfndx0 == 0 ? 1 : sfndx0);
+        int fl = use ? frag_length(n, d) : 0;
+        int c = 0;
+        if (fl >= 1) {
+            int hi = n - fl - V.base;           // pos + fl <= n
+            if (hi > nf - 1) hi = nf - 1;
+            c = hi >= lo ? hi - lo + 1 : 0;
+        }
+        V.fl[d] = fl;
+        V.lo[d] = lo;
+        V.cnt[d] = c;
+        V.total += c;
     }
 }
 
 // k-th admissible variant (0 <= k < total) -> (si, length index, position,
-// length, first position of the refined fragment)
-__device__ __forceinline__ void variants_get(const VariantList& V, bool phase2, int n, int k,
+// length, first position of the refined fragment); variants are grouped by
+// length index, so ties are broken by si, not by k
+__device__ __forceinline__ void variants_get(const VariantList& V, int vk, int n, int k,
                                              int& si, int& ndx, int& pos, int& fl, int& kf) {
-    if (phase2) {
-        si = V.lo + k;
-        ndx = V.ndx2;
-        pos = V.base + si;
-        fl = V.fl2;
-        kf = pos;
-        return;
-    }
-    int d = 0, fcl = V.fl[0], c = V.cnt[0];
+    // the group is selected inside the unrolled loop (no run-time array index)
+    int d = 0, c = V.cnt[0], fcl = V.fl[0], lol = V.lo[0];
 #pragma unroll
     for (int e = 1; e < FRAG_NSUB; e++) {
-        if (k >= c) { k -= c; d = e; c = V.cnt[e]; fcl = V.fl[e]; }
+        if (k >= c) { k -= c; d = e; c = V.cnt[e]; fcl = V.fl[e]; lol = V.lo[e]; }
     }
-    si = k * FRAG_NSUB + d;
     ndx = d;
     fl = fcl;
-    pos = k * FRAG_STEP;
+    if (vk == VK_STAGE) {
+        si = k * FRAG_NSUB + d;
+        pos = k * FRAG_STEP;
+    } else if (vk == VK_LOG) {
+        si = d;
+        pos = V.base;
+    } else {
+        int fct = lol + k;
+        si = vk == VK_P2ALL ? fct * FRAG_NSUB + d : fct;
+        pos = V.base + fct;
+    }
     int delta = pos + fl - n;
     kf = pos - (delta > 0 ? delta : 0);
 }
@@ -802,7 +845,7 @@ template <int MODE>
 __device__ __forceinline__ void refine_commit(const Blk& B, const Bat& T, int i, int lq, int lr,
                                               bool havewin, float wb, float lgbest, int wndx,
                                               int wpos, const float* tb, int tstr) {
-    if (MODE == RM_PROD1 || MODE == RM_PROD2) {
+    if (MODE == RM_PROD1 || MODE == RM_PROD2 || MODE == RM_PLOG) {
         if (!havewin) return;
         float grand = T.grand[i];
         bool write = (MODE == RM_PROD1) || (grand < wb);
@@ -817,6 +860,7 @@ __device__ __forceinline__ void refine_commit(const Blk& B, const Bat& T, int i,
 #pragma unroll
             for (int f = 0; f < 12; f++) T.tfm_gr[i * 12 + f] = tb[f * tstr];
             if (MODE == RM_PROD1) { T.sfndx[i] = wndx; T.sfpos[i] = wpos; }
+            if (MODE == RM_PLOG) T.sfpos[i] = wpos;   // the search moves to the round's position
         }
         return;
     }
@@ -888,13 +932,20 @@ __global__ void __launch_bounds__(RF_WARPS * 32) k_refine(Blk B, Bat T) {
     }
     if (!valid) G.n = 0;
     const int n = G.n;
-    const bool prod = (MODE == RM_PROD1 || MODE == RM_PROD2);
-    const bool phase2 = (MODE == RM_FIN2 || MODE == RM_PROD2);
+    const bool prod = (MODE == RM_PROD1 || MODE == RM_PROD2 || MODE == RM_PLOG);
+    const bool phase2 = (MODE == RM_FIN2 || MODE == RM_PROD2 || MODE == RM_PLOG);
+    const int vk = MODE == RM_PLOG ? VK_LOG
+                 : MODE == RM_FIN2 ? (B.refinement == GTB_REFINEMENT_FULLA ? VK_P2ALL : VK_P2ONE)
+                 : MODE == RM_PROD2 ? (B.refinement >= GTB_REFINEMENT_FULL ? VK_P2ALL : VK_P2ONE)
+                 : VK_STAGE;
     const float d0 = prod ? B.t_d0fin[ml] : B.t_d0[ml];
     const float d02 = __fmul_rn(d0, d0);
     const float d82 = B.t_d82[ml];
     const int chk = prod ? 0 : 1;
-    const float best_init = (MODE == RM_INIT || MODE == RM_DP) ? 0.f : -1.f;
+    // the log search carries the best score so far (phase 1's to begin with)
+    // into every variant; the other modes start each variant afresh
+    const float best_init = (MODE == RM_INIT || MODE == RM_DP) ? 0.f
+                          : MODE == RM_PLOG ? T.grand[i] : -1.f;
     const int maxalnmax = B.qmax < B.rmax ? B.qmax : B.rmax;
     const float d0s = d0s_of(d0);
     const float d0sm = __fsub_rn(d0s, 1.0f);
@@ -905,12 +956,12 @@ __global__ void __launch_bounds__(RF_WARPS * 32) k_refine(Blk B, Bat T) {
     float g02 = 0.f;
     if (gscore) { float g0 = B.t_d0fin[lq > lr ? lq : lr]; g02 = __fmul_rn(g0, g0); }
     VariantList V;
-    variants_init(V, phase2, n, maxalnmax, phase2 ? T.sfndx[i] : 0, phase2 ? T.sfpos[i] : 0);
+    variants_init(V, vk, n, maxalnmax, phase2 ? T.sfndx[i] : 0, phase2 ? T.sfpos[i] : 0, T.plog_round);
     if (MODE == RM_PROD1 && (lane % RF_LPP) == 0 && V.total > 0 && wlong == 0) {
         // RMSD over the whole alignment (variant 0: fragment [0, n)) from
         // compensated FP32 sums, MpStageFin.cpp production phase 1
         int s0, nd0, ps0, fl0, kf0;
-        variants_get(V, phase2, n, 0, s0, nd0, ps0, fl0, kf0);
+        variants_get(V, vk, n, 0, s0, nd0, ps0, fl0, kf0);
         CovAcc a;
         a.init();
         float sq[6], cq[6], bq[6];
@@ -963,7 +1014,7 @@ __global__ void __launch_bounds__(RF_WARPS * 32) k_refine(Blk B, Bat T) {
                 kind = PK_IDLE;
                 if (kv < V.total) {
                     int fl, kf;
-                    variants_get(V, phase2, n, kv, si, vndx, vpos, fl, kf);
+                    variants_get(V, vk, n, kv, si, vndx, vpos, fl, kf);
                     kind = PK_FRAG; k0 = kf; k1 = kf + fl;
                     best = best_init; cit = 0;
                 }
@@ -1015,7 +1066,7 @@ __global__ void __launch_bounds__(RF_WARPS * 32) k_refine(Blk B, Bat T) {
             }
         }
         if (done) {
-            if (kind != PK_GSCORE && gscore && best >= 0.f) {
+            if (kind != PK_GSCORE && gscore && best >= 0.f && (MODE != RM_PLOG || best > best_init)) {
                 // one more pass: the variant's best transform scored with the
                 // d0 of the longer structure
 #pragma unroll
@@ -1108,6 +1159,7 @@ static void launch_refine_k(int mode, const Blk& B, const Bat& T, cudaStream_t s
         case RM_FIN2:  k_refine<RM_FIN2, LPP, LONG><<<ng, nt, 0, st>>>(B, T); break;
         case RM_PROD1: k_refine<RM_PROD1, LPP, LONG><<<ng, nt, 0, st>>>(B, T); break;
         case RM_PROD2: k_refine<RM_PROD2, LPP, LONG><<<ng, nt, 0, st>>>(B, T); break;
+        case RM_PLOG:  k_refine<RM_PLOG, LPP, LONG><<<ng, nt, 0, st>>>(B, T); break;
     }
 }
 
@@ -1116,9 +1168,10 @@ static void launch_refine_k(int mode, const Blk& B, const Bat& T, cudaStream_t s
 // of their static arrays), leaving the rest of the SM's 256 kB to L1.
 template <int LPP, bool LONG>
 static void carve_refine() {
-    const void* ks[6] = {(const void*)k_refine<RM_INIT, LPP, LONG>, (const void*)k_refine<RM_DP, LPP, LONG>,
+    const void* ks[7] = {(const void*)k_refine<RM_INIT, LPP, LONG>, (const void*)k_refine<RM_DP, LPP, LONG>,
                          (const void*)k_refine<RM_FIN1, LPP, LONG>, (const void*)k_refine<RM_FIN2, LPP, LONG>,
-                         (const void*)k_refine<RM_PROD1, LPP, LONG>, (const void*)k_refine<RM_PROD2, LPP, LONG>};
+                         (const void*)k_refine<RM_PROD1, LPP, LONG>, (const void*)k_refine<RM_PROD2, LPP, LONG>,
+                         (const void*)k_refine<RM_PLOG, LPP, LONG>};
     for (const void* k : ks) cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, 27);
 }
 
@@ -1137,6 +1190,7 @@ static void launch_refine_long_fin(int mode, const Blk& B, const Bat& T, cudaStr
         case RM_FIN2:  k_refine_long_fin<RM_FIN2><<<ng, 128, 0, st>>>(B, T); break;
         case RM_PROD1: k_refine_long_fin<RM_PROD1><<<ng, 128, 0, st>>>(B, T); break;
         case RM_PROD2: k_refine_long_fin<RM_PROD2><<<ng, 128, 0, st>>>(B, T); break;
+        case RM_PLOG:  k_refine_long_fin<RM_PLOG><<<ng, 128, 0, st>>>(B, T); break;
     }
 }
 
@@ -1716,7 +1770,16 @@ void launch_stages(const Blk& B, const Bat& T, int refinement, int depth, int co
     launch_btck(B, T, 1, st);
     launch_alnstr(B, T, st);
     launch_refine(RM_PROD1, B, T, st, few);
-    launch_refine(RM_PROD2, B, T, st, few);
+    if (refinement == GTB_REFINEMENT_LOG) {
+        // MpStageFin.h:421-434: the log search, one launch per step
+        Bat TL = T;
+        for (int r = 0; r < PLOG_ROUNDS; r++) {
+            TL.plog_round = r;
+            launch_refine(RM_PLOG, B, TL, st, few);
+        }
+    } else {
+        launch_refine(RM_PROD2, B, T, st, few);
+    }
     launch_polish_final(B, T, polish_steps, st);
     launch_final(B, T, referenced, st);
     mark(4);

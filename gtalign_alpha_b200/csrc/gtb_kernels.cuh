@@ -65,6 +65,7 @@ struct Bat {
     // per-pair variant counter, per-warp candidates; rl_nlmax = capacity
     int rl_nlmax;
     int *rl_long, *rl_count, *rl_next;
+    int plog_round;                  // round of an RM_PLOG launch (0 .. PLOG_ROUNDS-1)
     float* rl_cand;
     // seed work items when some pair's offsets are split over several CTAs
     // (null: one CTA per pair): item -> pair, item -> chunk, chunks per pair,
@@ -84,7 +85,10 @@ struct Bat {
     long long* launches;             // host counter of kernel launches
 };
 
-enum RefineMode { RM_INIT = 0, RM_DP = 1, RM_FIN1 = 2, RM_FIN2 = 3, RM_PROD1 = 4, RM_PROD2 = 5 };
+// RM_PLOG: one round of the production phase-2 log search (--refinement -1)
+enum RefineMode { RM_INIT = 0, RM_DP = 1, RM_FIN1 = 2, RM_FIN2 = 3, RM_PROD1 = 4, RM_PROD2 = 5,
+                  RM_PLOG = 6 };
+constexpr int PLOG_ROUNDS = 12;   // steps +-32, +-16, ..., +-1
 enum DpTfm { DP_TFM_IBEST = 0, DP_TFM_GRAND = 1 };
 
 void launch_secstr(char* ss, const float* x, const float* y, const float* z,

@@ -99,13 +99,13 @@ extern "C" gtb_status gtb_process_block_noalloc(int device, const gtb_options* o
         setmsg(errbuf, errlen, "null argument or device out of range (%lld, %lld)", device, MAXDEV);
         return GTB_ERR_ARG;
     }
-    if (!opts->nodetailedsearch || opts->addsearchbyss || opts->twotmscore ||
-        opts->refinement < 0 || opts->refinement > 1) {
-        setmsg(errbuf, errlen, "option combination not implemented (refinement %lld, detailed %lld)",
-               opts->refinement, !opts->nodetailedsearch);
+    if (!opts->nodetailedsearch || opts->addsearchbyss || opts->twotmscore) {
+        setmsg(errbuf, errlen, "option combination not implemented (detailed search %lld, ss/2tm %lld)",
+               !opts->nodetailedsearch, opts->addsearchbyss * 2 + opts->twotmscore);
         return GTB_ERR_UNSUPPORTED;
     }
     if (!(scorethld >= 0.f && scorethld < 1.f) || opts->depth < 0 || opts->depth > 3 ||
+        opts->refinement < GTB_REFINEMENT_LOG || opts->refinement > GTB_REFINEMENT_FULLA ||
         opts->convergence < 1 || opts->convergence > 30 || !(opts->prescore >= 0.f && opts->prescore < 1.f) ||
         opts->polish_steps < 0 || opts->polish_steps > 50) {
         setmsg(errbuf, errlen, "option out of range (%lld %lld)", 0, 0);

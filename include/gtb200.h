@@ -71,8 +71,9 @@ enum { GTB_ERR_TMQ = 0, GTB_ERR_TMR = 1, GTB_ERR_RMSD = 2, GTB_NERR = 4 };
 /* Options the path reads (CuBatch.cu:353-366, custage_fin.cu:243-245,409),
  * with the values of the gtalign command line. */
 typedef struct {
-    int   refinement;        /* --refinement (GTB_REFINEMENT_*): 0 coarse or 1 one
-                                search; -1, 2 and 3 are GTB_ERR_UNSUPPORTED */
+    int   refinement;        /* --refinement (GTB_REFINEMENT_*): -1 log search,
+                                0 coarse, 1 one search (default), 2 full search,
+                                3 full search in both final phases */
     int   depth;             /* --depth 0..3 (3 = shallow: seed step 5) */
     int   convergence;       /* --convergence 1..30 */
     float prescore;          /* --pre-score [0,1) */

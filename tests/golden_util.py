@@ -12,8 +12,8 @@ LEVEL_SETS = {-1: "c0_level_m1", 0: "c0_level_0", 1: "c0_level_1", 2: "c0_level_
               3: "c0_level_3"}
 SETS = ["c0_speed13", "c0_default", "c0_filters", "c0_sym_ref_nodel", "c0_shallow"] + \
     list(LEVEL_SETS.values())
-# the sets whose options the CUDA library implements
-LIBRARY_SETS = [s for s in SETS if s not in (LEVEL_SETS[-1], LEVEL_SETS[2], LEVEL_SETS[3])]
+# the sets whose options the CUDA library implements (all of them)
+LIBRARY_SETS = list(SETS)
 
 
 def _soa(z, tag):

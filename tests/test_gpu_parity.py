@@ -64,6 +64,10 @@ OPTSETS = {
     "filters": dict(refinement=1, convergence=18, prescore=0.4, scorethld=0.5, symmetric=0, referenced=0, nodeletions=0),
     "shallow": dict(refinement=1, convergence=6, prescore=0.3, scorethld=0.3, symmetric=0, referenced=0, nodeletions=0, depth=3),
     "sym": dict(refinement=1, convergence=4, prescore=0.0, scorethld=0.0, symmetric=1, referenced=1, nodeletions=1),
+    # the other final-stage forms: log search, full search, full search in both phases
+    "log": dict(refinement=-1, convergence=6, prescore=0.2, scorethld=0.2, symmetric=0, referenced=0, nodeletions=0),
+    "full": dict(refinement=2, convergence=6, prescore=0.0, scorethld=0.0, symmetric=1, referenced=0, nodeletions=0),
+    "fulla": dict(refinement=3, convergence=4, prescore=0.0, scorethld=0.0, symmetric=0, referenced=1, nodeletions=0),
 }
 
 
@@ -147,10 +151,10 @@ def test_status_codes():
         with pytest.raises(GTBError) as e:
             g.process_block(q, r)
         assert e.value.status == 4
-    with GTalignB200(0, 0, Options(refinement=3)) as g:
+    with GTalignB200(0, 0, Options(refinement=4)) as g:
         with pytest.raises(GTBError) as e:
             g.process_block(q, r)
-        assert e.value.status == 4
+        assert e.value.status == 1
     with GTalignB200(0, 0, Options()) as g:
         with pytest.raises(GTBError) as e:
             g.process_block(q, r, scorethld=1.5)
@@ -167,15 +171,18 @@ def test_status_codes():
         assert res.alndata.shape == (1, 2, 16)
 
 
-def test_long_chain_assemblies(oracle):
+@pytest.mark.parametrize("refinement", [1, -1, 3])
+def test_long_chain_assemblies(oracle, refinement):
     """Multi-domain assemblies and their per-domain-perturbed partners (the
     long-chain configuration's construction at 1,200 and 2,000 residues):
-    large DP matrices, many strips and thousands of refinement variants."""
+    large DP matrices, many strips and thousands of refinement variants; the
+    2,000-residue pair takes the many-CTA refinement path in every final
+    form (one search, log search, full search in both phases)."""
     from gtalign_alpha_b200 import synth
     wl = synth.config2(seed=3, lengths=(1200, 2000))
     q, r = synth.pack(wl.queries), synth.pack(wl.refs)
-    d = dict(refinement=1, convergence=18, prescore=0.4, scorethld=0.5, symmetric=0,
-             referenced=0, nodeletions=0)
+    d = dict(refinement=refinement, convergence=18 if refinement == 1 else 4, prescore=0.4,
+             scorethld=0.5, symmetric=0, referenced=0, nodeletions=0)
     res, ora = run_both(oracle, q, r, d)
     assert_same(res, ora, q.n, r.n)
     assert res.alndata[0, 0, 9] > 0.5 and res.alndata[1, 1, 9] > 0.5
