@@ -1641,8 +1641,10 @@ __global__ void k_final(Blk B, Bat T, int referenced) {
     if (n > 0) {
         const float *qx = B.qx + B.qoff[qi], *qy = B.qy + B.qoff[qi], *qz = B.qz + B.qoff[qi];
         const float *rx = B.rx + B.roff[ri], *ry = B.ry + B.roff[ri], *rz = B.rz + B.roff[ri];
+        const char *qs = B.qs + B.qoff[qi], *rs = B.rs + B.roff[ri];
         double d0q = (double)B.t_d0fin[lq], d0r = (double)B.t_d0fin[lr];
         double d0q2 = __dmul_rn(d0q, d0q), d0r2 = __dmul_rn(d0r, d0r), tq = 0.0, tr = 0.0;
+        double t2q = 0.0, t2r = 0.0;   // --2tm-score sums
         double dv[21];
 #pragma unroll
         for (int f = 0; f < 21; f++) dv[f] = 0.0;
@@ -1659,8 +1661,15 @@ __global__ void k_final(Blk B, Bat T, int referenced) {
             double z = __dadd_rn(__dadd_rn(__dadd_rn(__dmul_rn(td[6], qq[0]), __dmul_rn(td[7], qq[1])), __dmul_rn(td[8], qq[2])), td[11]);
             double dx = __dsub_rn(x, rr[0]), dy = __dsub_rn(y, rr[1]), dz = __dsub_rn(z, rr[2]);
             double d = __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz));
-            tq = __dadd_rn(tq, __ddiv_rn(d0q2, __dadd_rn(d0q2, d)));
-            tr = __dadd_rn(tr, __ddiv_rn(d0r2, __dadd_rn(d0r2, d)));
+            const double sq = __ddiv_rn(d0q2, __dadd_rn(d0q2, d));
+            const double sr = __ddiv_rn(d0r2, __dadd_rn(d0r2, d));
+            tq = __dadd_rn(tq, sq);
+            tr = __dadd_rn(tr, sr);
+            if (B.twotm) {
+                // MpStageBase.h:825-856: a helix aligned to a non-helix residue is left out
+                const char a2 = qs[q], b2 = rs[r];
+                if (!((a2 == 'h' || b2 == 'h') && a2 != b2)) { t2q = __dadd_rn(t2q, sq); t2r = __dadd_rn(t2r, sr); }
+            }
 #pragma unroll
             for (int a = 0; a < 3; a++)
 #pragma unroll
@@ -1685,6 +1694,11 @@ __global__ void k_final(Blk B, Bat T, int referenced) {
             T.err[i * 4 + 1] = (float)fabs(__dsub_rn((double)out[10], tmr));
             out[9] = (float)tmq;
             out[10] = (float)tmr;
+        }
+        if (B.twotm) {
+            // secondary TM-scores (MpStageFin.cpp:1723-1818), FP64 like the primary ones
+            out[13] = (float)__ddiv_rn(t2q, (double)lq);
+            out[14] = (float)__ddiv_rn(t2r, (double)lr);
         }
     }
     if (referenced) {

@@ -45,6 +45,7 @@ struct Blk {
     int qmax, qmin, rmax, rmin;      // block-level length extremes
     const float *t_d0, *t_d82, *t_d0fin;  // per-length constants
     int stepinit, refinement, depth, symmetric, nodeletions;
+    int twotm;                       // --2tm-score: record fields 13 and 14
 };
 
 // Batch of consecutive pairs p0 .. p0+np-1 of a block (pair = qi*nr + ri).

@@ -83,7 +83,9 @@ typedef struct {
     int   nodetailedsearch;  /* --no-detailed-search: must be 1 (the spatial-index
                                 search stage is not part of this library) */
     int   addsearchbyss;     /* --add-search-by-ss: must be 0 */
-    int   twotmscore;        /* --2tm-score: must be 0 */
+    int   twotmscore;        /* --2tm-score: record fields GTB_OUT_2SCOREQ/R get
+                                the TM-scores without the aligned pairs of a
+                                helix and a non-helix residue */
     int   polish_steps;      /* no reference counterpart: 0 (the reference's
                                 results) or 1..50 projected-gradient steps on
                                 SO(3) x R^3 that polish each pair's final

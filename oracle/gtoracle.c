@@ -854,10 +854,13 @@ static void production(pairctx* P, int refinement) {
             prod_write(P, &w2);
         }
     }
-    /* FP64 recomputation of reported values */
+    /* FP64 recomputation of reported values; with --2tm-score also the
+     * secondary TM-scores: the same sums without the aligned pairs where one
+     * residue is in a helix and the other is not (MpStageFin.cpp:1723-1818,
+     * MpStageBase.h:825-856) */
     if (n > 0) {
         double d0q = c_d0fin(P->lq, P->lq), d0r = c_d0fin(P->lr, P->lr);
-        double d0q2 = d0q * d0q, d0r2 = d0r * d0r, tq = 0.0, tr = 0.0;
+        double d0q2 = d0q * d0q, d0r2 = d0r * d0r, tq = 0.0, tr = 0.0, t2q = 0.0, t2r = 0.0;
         double dv[21];
         memset(dv, 0, sizeof(dv));
         const float* t = P->tfm_gr;
@@ -869,8 +872,11 @@ static void production(pairctx* P, int refinement) {
             double y = t[3] * qx + t[4] * qy + t[5] * qz + t[10];
             double z = t[6] * qx + t[7] * qy + t[8] * qz + t[11];
             double d = (x - rx) * (x - rx) + (y - ry) * (y - ry) + (z - rz) * (z - rz);
-            tq += d0q2 / (d0q2 + d);
-            tr += d0r2 / (d0r2 + d);
+            double sq_ = d0q2 / (d0q2 + d), sr_ = d0r2 / (d0r2 + d);
+            tq += sq_;
+            tr += sr_;
+            char qs = P->qs[q], rs = P->rs[r];
+            if (!((qs == 'h' || rs == 'h') && qs != rs)) { t2q += sq_; t2r += sr_; }
             double qq[3] = {qx, qy, qz}, rr[3] = {rx, ry, rz};
             for (int i = 0; i < 3; i++)
                 for (int j = 0; j < 3; j++) dv[3 * i + j] += qq[i] * rr[j];
@@ -890,6 +896,10 @@ static void production(pairctx* P, int refinement) {
             P->err[GTO_ERR_TMR] = (float)fabs((double)P->out[GTO_SCORER] - tmr);
             P->out[GTO_SCOREQ] = (float)tmq;
             P->out[GTO_SCORER] = (float)tmr;
+        }
+        if (P->o->twotmscore) {
+            P->out[GTO_2SCOREQ] = (float)(t2q / P->lq);
+            P->out[GTO_2SCORER] = (float)(t2r / P->lr);
         }
     }
 }

@@ -43,6 +43,7 @@ typedef struct {
     int   symmetric;     /* --symmetric */
     int   referenced;    /* --referenced */
     int   nodeletions;   /* --no-deletions */
+    int   twotmscore;    /* --2tm-score */
 } gto_opts;
 
 /* Process a block of nq queries x nr references.

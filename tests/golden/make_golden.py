@@ -60,6 +60,8 @@ SETS = {
                    ["--no-detailed-search", "--refinement=2", "--pre-score=0", "-s", "0"], 1),
     "c0_level_3": (lambda: synth.config0(seed=201, n_refs=40, qlen=180, homolog_frac=1.0),
                    ["--no-detailed-search", "--refinement=3", "--pre-score=0", "-s", "0"], 1),
+    "c0_2tm": (lambda: synth.config0(seed=109, n_refs=50, qlen=150, homolog_frac=0.5),
+               ["--no-detailed-search", "--2tm-score", "--pre-score=0", "-s", "0"]),
     "c0_shallow": (lambda: synth.config0(seed=108, n_refs=60, qlen=160),
                    ["--no-detailed-search", "--depth=3", "--pre-score=0.3", "-s", "0.3",
                     "--convergence=6"]),
@@ -92,6 +94,9 @@ def run(wl, opts, threads=8):
                     "query_secstr": a["query_secstr"], "refrn_secstr": a["refrn_secstr"],
                     "rotation": h["rotation_matrix_rowmajor"], "translation": h["translation_vector"],
                 }
+                if "--2tm-score" in opts:
+                    res[qn + "|" + rn]["tm2q"] = float(a["2tmscore_query"])
+                    res[qn + "|" + rn]["tm2r"] = float(a["2tmscore_refn"])
         return res
     finally:
         shutil.rmtree(d, ignore_errors=True)

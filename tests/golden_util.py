@@ -10,7 +10,7 @@ GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 # --refinement code -> the fixture set run at that code (homologs only)
 LEVEL_SETS = {-1: "c0_level_m1", 0: "c0_level_0", 1: "c0_level_1", 2: "c0_level_2",
               3: "c0_level_3"}
-SETS = ["c0_speed13", "c0_default", "c0_filters", "c0_sym_ref_nodel", "c0_shallow"] + \
+SETS = ["c0_speed13", "c0_default", "c0_filters", "c0_sym_ref_nodel", "c0_shallow", "c0_2tm"] + \
     list(LEVEL_SETS.values())
 # the sets whose options the CUDA library implements (all of them)
 LIBRARY_SETS = list(SETS)
@@ -37,7 +37,7 @@ def load(name):
 def cli_options(opts):
     """Translate the reference CLI options of a set into oracle/library options."""
     d = dict(refinement=1, convergence=18, prescore=0.4, scorethld=0.5, depth=2,
-             symmetric=0, referenced=0, nodeletions=0)
+             symmetric=0, referenced=0, nodeletions=0, twotmscore=0)
     i = 0
     while i < len(opts):
         o = opts[i]
@@ -59,5 +59,7 @@ def cli_options(opts):
             d["referenced"] = 1
         elif o == "--no-deletions":
             d["nodeletions"] = 1
+        elif o == "--2tm-score":
+            d["twotmscore"] = 1
         i += 1
     return d

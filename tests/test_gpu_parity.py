@@ -17,14 +17,14 @@ def _lib_opts(d):
     from gtalign_alpha_b200.api import Options
     return Options(refinement=d["refinement"], depth=d.get("depth", 2), convergence=d["convergence"],
                    prescore=d["prescore"], symmetric=d["symmetric"], referenced=d["referenced"],
-                   nodeletions=d["nodeletions"])
+                   nodeletions=d["nodeletions"], twotmscore=d.get("twotmscore", 0))
 
 
 def _ora_opts(oracle, d):
     return oracle.opts_from(refinement=d["refinement"], convergence=d["convergence"],
                             prescore=d["prescore"], scorethld=d["scorethld"], depth=d.get("depth", 2),
                             symmetric=d["symmetric"], referenced=d["referenced"],
-                            nodeletions=d["nodeletions"])
+                            nodeletions=d["nodeletions"], twotmscore=d.get("twotmscore", 0))
 
 
 def assert_same(res, ora, nq, nr):
@@ -68,6 +68,8 @@ OPTSETS = {
     "log": dict(refinement=-1, convergence=6, prescore=0.2, scorethld=0.2, symmetric=0, referenced=0, nodeletions=0),
     "full": dict(refinement=2, convergence=6, prescore=0.0, scorethld=0.0, symmetric=1, referenced=0, nodeletions=0),
     "fulla": dict(refinement=3, convergence=4, prescore=0.0, scorethld=0.0, symmetric=0, referenced=1, nodeletions=0),
+    "twotm": dict(refinement=1, convergence=6, prescore=0.3, scorethld=0.3, symmetric=1, referenced=1, nodeletions=0,
+                  twotmscore=1),
 }
 
 

@@ -46,7 +46,7 @@ def run_oracle(oracle, name):
     o = oracle.process_block(q, r, oracle.opts_from(
         refinement=d["refinement"], convergence=d["convergence"], prescore=d["prescore"],
         scorethld=d["scorethld"], symmetric=d["symmetric"], referenced=d["referenced"],
-        nodeletions=d["nodeletions"], depth=d["depth"]))
+        nodeletions=d["nodeletions"], depth=d["depth"], twotmscore=d["twotmscore"]))
     return q, r, qn, rn, meta, d, o
 
 
@@ -163,3 +163,27 @@ def test_refinement_levels_pinned(oracle):
         for lo in gu.LEVEL_SETS:
             if lo != lref:
                 assert n_match[lref, lref] > n_match[lref, lo], (lref, lo, n_match)
+
+
+def test_oracle_2tm_scores(oracle):
+    """--2tm-score: the secondary TM-scores (helix aligned to non-helix left
+    out, printed to 5 significant digits) agree within 1e-4 wherever the
+    reference and the oracle report the same alignment and the same TM-scores
+    to the printed precision (the same superposition), on at least 90% of the
+    pairs whose TM-scores agree within 1e-4 (some of those end on a different
+    transform of nearly the same score, which moves the 2TM-score more)."""
+    q, r, qn, rn, meta, d, o = run_oracle(oracle, "c0_2tm")
+    same_sup, close = [], []
+    for key, g in meta["results"].items():
+        a, b = key.split("|")
+        qi, ri = qn.index(a), rn.index(b)
+        out, rows = o.out[qi, ri], o.alns[qi][ri]
+        dd = max(abs(out[9] - g["tmq"]), abs(out[10] - g["tmr"]))
+        e2 = max(abs(out[13] - g["tm2q"]), abs(out[14] - g["tm2r"]))
+        assert out[13] <= out[9] + 1e-6 and out[14] <= out[10] + 1e-6
+        if dd <= 1e-4:
+            close.append(e2 <= 1e-4)
+            if dd <= 1e-5 and rows[0] == g["query_aln"] and rows[2] == g["refrn_aln"]:
+                same_sup.append(e2)
+    assert len(same_sup) >= 20 and max(same_sup) <= 1e-4, (len(same_sup), max(same_sup))
+    assert np.mean(close) >= 0.9, np.mean(close)
