@@ -45,6 +45,7 @@
 #include <stdlib.h>
 #include <string.h>
 #include "gtoracle.h"
+#include "../gtalign_alpha_b200/csrc/gtb_gonnet.h"
 
 #define GTB_BLK 32
 #define LARGEDST 999999.9f
@@ -631,6 +632,52 @@ static void dp_run(pairctx* P, const float* tfm, int gap0, float gcost, int uses
     }
 }
 
+/* DP of the --add-search-by-ss stage (dpssw_btck.cu:280-330,
+ * MpDPHub.cpp:985-1210): no transform; a cell scores 1 for equal secondary
+ * structure plus 0.2 x the Gonnet score of the residue pair.  The gap cost
+ * is paid once, leaving a cell reached diagonally (gap extension free):
+ * such a cell stores its value plus DPSS_C (a large negative offset, so the
+ * stored value is rounded to a multiple of 1/8) and a reader takes the offset
+ * off again; the matrix border reads as a diagonal cell of value 0. */
+#define DPSS_C (-1048576.0f)
+#define DPSS_CMP (-524288.0f)
+static float g_gonnet[GTB_GONNET_NA * GTB_GONNET_NA];
+
+static float gonnet_score(unsigned char a, unsigned char b) {
+    if ('A' <= a && a <= 'Z' && 'A' <= b && b <= 'Z') return g_gonnet[(a - 'A') * GTB_GONNET_NA + (b - 'A')];
+    return 0.0f;
+}
+
+static void dp_ss_run(pairctx* P, float gcost) {
+    int lq = P->lq, lr = P->lr;
+    float* prev = P->h0;   /* row i-1 */
+    float* cur = P->h1;
+    for (int j = 0; j < lr; j++) prev[j] = DPSS_C;
+    for (int i = 0; i < lq; i++) {
+        char qs = P->qs[i];
+        unsigned char qa = P->qa[i];
+        float left = DPSS_C;
+        for (int j = 0; j < lr; j++) {
+            float v = fmaf(gonnet_score(qa, P->ra[j]), 0.2f, (float)(qs == P->rs[j]));
+            float dg = (i > 0 && j > 0) ? prev[j - 1] : DPSS_C;
+            if (dg < DPSS_CMP) dg = dg - DPSS_C;
+            v = v + dg;
+            int bk = BT_DIAG;
+            float l = left;
+            if (l < DPSS_CMP) l = (gcost + l) - DPSS_C;
+            if (v < l) { v = l; bk = BT_LEFT; }
+            float u = prev[j];
+            if (u < DPSS_CMP) u = (gcost + u) - DPSS_C;
+            if (v < u) { v = u; bk = BT_UP; }
+            float w = (bk == BT_DIAG) ? v + DPSS_C : v;
+            cur[j] = w;
+            left = w;
+            P->bt[(size_t)i * lr + j] = (unsigned char)bk;
+        }
+        float* t = prev; prev = cur; cur = t;
+    }
+}
+
 /* unconstrained traceback: MpDPHub.cpp:1515-1660 */
 static void btck_matched(pairctx* P) {
     int y = P->lq - 1, x = P->lr - 1, n = 0;
@@ -978,6 +1025,20 @@ static void run_pair(pairctx* P, char* alndst) {
     else P->best = 0.f;
     dprefine(P, 1, 1, 2);
 
+    /* --add-search-by-ss: MpStageSSRR.h:63-76, custage_ssrr.cu:43-140 --
+     * the alignment of the DP above, fragment refinement over it, then DP
+     * refinement with the gap cost and without, 2 iterations each */
+    if (o->addsearchbyss) {
+        if (!(P->flags & CONV_LOWTMSC)) {
+            dp_ss_run(P, -1.0f);
+            btck_matched(P);
+        } else P->naln = 0;
+        if (P->flags) P->best = 0.f;
+        else refine_stage(P, 1, P->d0, P->d02, 1, 0.f, 1, 0);
+        dprefine(P, 0, 0, 2);
+        dprefine(P, 1, 0, 2);
+    }
+
     /* stage 2, first call: MpStage2.h:63-83 with <false,true,DPSCAN> */
     for (int call = 0; call < 2; call++) {
         int gap0 = call == 1;
@@ -1029,6 +1090,7 @@ int gto_process_block(const gto_opts* o,
                       char* alns, const long long* aln_off,
                       char* qss, char* rss, int nthreads) {
     if (nq < 1 || nr < 1) return 1;
+    gtb_gonnet_scores(g_gonnet);
     long long* qoff = (long long*)malloc(sizeof(long long) * (nq + 1));
     long long* roff = (long long*)malloc(sizeof(long long) * (nr + 1));
     qoff[0] = roff[0] = 0;

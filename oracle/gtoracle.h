@@ -44,6 +44,7 @@ typedef struct {
     int   referenced;    /* --referenced */
     int   nodeletions;   /* --no-deletions */
     int   twotmscore;    /* --2tm-score */
+    int   addsearchbyss; /* --add-search-by-ss */
 } gto_opts;
 
 /* Process a block of nq queries x nr references.

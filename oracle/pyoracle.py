@@ -21,7 +21,9 @@ NERR = 4
 def build(force: bool = False) -> str:
     """Compile oracle/gtoracle.c into oracle/liboracle.so (gcc, OpenMP)."""
     src = os.path.join(HERE, "gtoracle.c")
-    if force or not os.path.exists(LIB) or os.path.getmtime(LIB) < os.path.getmtime(src):
+    deps = [src, os.path.join(HERE, "gtoracle.h"),
+            os.path.join(os.path.dirname(HERE), "gtalign_alpha_b200", "csrc", "gtb_gonnet.h")]
+    if force or not os.path.exists(LIB) or os.path.getmtime(LIB) < max(os.path.getmtime(d) for d in deps):
         subprocess.check_call([
             "gcc", "-O2", "-fPIC", "-shared", "-ffp-contract=off", "-fopenmp",
             "-o", LIB, src, "-lm"])
@@ -33,7 +35,8 @@ class _Opts(ctypes.Structure):
                 ("depth", ctypes.c_int), ("convergence", ctypes.c_int),
                 ("prescore", ctypes.c_float), ("scorethld", ctypes.c_float),
                 ("symmetric", ctypes.c_int), ("referenced", ctypes.c_int),
-                ("nodeletions", ctypes.c_int), ("twotmscore", ctypes.c_int)]
+                ("nodeletions", ctypes.c_int), ("twotmscore", ctypes.c_int),
+                ("addsearchbyss", ctypes.c_int)]
 
 
 _lib = None
@@ -79,13 +82,15 @@ class OracleResult:
 
 def opts_from(refinement: int = 0, convergence: int = 2, prescore: float = 0.0,
               scorethld: float = 0.0, depth: int = 2, symmetric: int = 0,
-              referenced: int = 0, nodeletions: int = 0, twotmscore: int = 0) -> _Opts:
+              referenced: int = 0, nodeletions: int = 0, twotmscore: int = 0,
+              addsearchbyss: int = 0) -> _Opts:
     """Options in the gtalign command line's encoding: --refinement -1 log
     search, 0 coarse, 1 one search (the default), 2 full, 3 full in both final
     phases (the oracle, like the reference, stores code + 1); --depth 0..3
-    (3 = shallow); --2tm-score."""
+    (3 = shallow); --2tm-score; --add-search-by-ss."""
     return _Opts(5 if depth == 3 else 1, refinement + 1, depth, convergence,
-                 prescore, scorethld, symmetric, referenced, nodeletions, twotmscore)
+                 prescore, scorethld, symmetric, referenced, nodeletions, twotmscore,
+                 addsearchbyss)
 
 
 def process_block(qsoa, rsoa, opts: _Opts, nthreads: int = 0) -> OracleResult:

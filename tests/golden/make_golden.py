@@ -62,6 +62,8 @@ SETS = {
                    ["--no-detailed-search", "--refinement=3", "--pre-score=0", "-s", "0"], 1),
     "c0_2tm": (lambda: synth.config0(seed=109, n_refs=50, qlen=150, homolog_frac=0.5),
                ["--no-detailed-search", "--2tm-score", "--pre-score=0", "-s", "0"]),
+    "c0_ssrr": (lambda: synth.config0(seed=110, n_refs=60, qlen=150, homolog_frac=0.5),
+                ["--no-detailed-search", "--add-search-by-ss", "--pre-score=0", "-s", "0"]),
     "c0_shallow": (lambda: synth.config0(seed=108, n_refs=60, qlen=160),
                    ["--no-detailed-search", "--depth=3", "--pre-score=0.3", "-s", "0.3",
                     "--convergence=6"]),

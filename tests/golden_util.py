@@ -10,10 +10,11 @@ GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 # --refinement code -> the fixture set run at that code (homologs only)
 LEVEL_SETS = {-1: "c0_level_m1", 0: "c0_level_0", 1: "c0_level_1", 2: "c0_level_2",
               3: "c0_level_3"}
-SETS = ["c0_speed13", "c0_default", "c0_filters", "c0_sym_ref_nodel", "c0_shallow", "c0_2tm"] + \
+SETS = ["c0_speed13", "c0_default", "c0_filters", "c0_sym_ref_nodel", "c0_shallow", "c0_2tm",
+        "c0_ssrr"] + \
     list(LEVEL_SETS.values())
-# the sets whose options the CUDA library implements (all of them)
-LIBRARY_SETS = list(SETS)
+# the sets whose options the CUDA library implements
+LIBRARY_SETS = [s for s in SETS if s != "c0_ssrr"]
 
 
 def _soa(z, tag):
@@ -37,7 +38,7 @@ def load(name):
 def cli_options(opts):
     """Translate the reference CLI options of a set into oracle/library options."""
     d = dict(refinement=1, convergence=18, prescore=0.4, scorethld=0.5, depth=2,
-             symmetric=0, referenced=0, nodeletions=0, twotmscore=0)
+             symmetric=0, referenced=0, nodeletions=0, twotmscore=0, addsearchbyss=0)
     i = 0
     while i < len(opts):
         o = opts[i]
@@ -61,5 +62,7 @@ def cli_options(opts):
             d["nodeletions"] = 1
         elif o == "--2tm-score":
             d["twotmscore"] = 1
+        elif o == "--add-search-by-ss":
+            d["addsearchbyss"] = 1
         i += 1
     return d

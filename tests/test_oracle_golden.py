@@ -46,7 +46,8 @@ def run_oracle(oracle, name):
     o = oracle.process_block(q, r, oracle.opts_from(
         refinement=d["refinement"], convergence=d["convergence"], prescore=d["prescore"],
         scorethld=d["scorethld"], symmetric=d["symmetric"], referenced=d["referenced"],
-        nodeletions=d["nodeletions"], depth=d["depth"], twotmscore=d["twotmscore"]))
+        nodeletions=d["nodeletions"], depth=d["depth"], twotmscore=d["twotmscore"],
+        addsearchbyss=d["addsearchbyss"]))
     return q, r, qn, rn, meta, d, o
 
 
@@ -187,3 +188,22 @@ def test_oracle_2tm_scores(oracle):
                 same_sup.append(e2)
     assert len(same_sup) >= 20 and max(same_sup) <= 1e-4, (len(same_sup), max(same_sup))
     assert np.mean(close) >= 0.9, np.mean(close)
+
+
+def test_oracle_search_by_ss_pinned(oracle):
+    """--add-search-by-ss: with the stage the oracle reproduces the
+    reference's run (TM-scores within 1e-4) at least as often as the
+    reference reproduces itself, and clearly more often than without it."""
+    q, r, qn, rn, meta = gu.load("c0_ssrr")
+    agree = {}
+    for ss in (0, 1):
+        o = oracle.process_block(q, r, oracle.opts_from(
+            refinement=1, convergence=18, prescore=0.0, scorethld=0.0, addsearchbyss=ss))
+        c = 0
+        for key, g in meta["results"].items():
+            a, b = key.split("|")
+            out = o.out[qn.index(a), rn.index(b)]
+            c += max(abs(out[9] - g["tmq"]), abs(out[10] - g["tmr"])) <= 1e-4
+        agree[ss] = c / len(meta["results"])
+    assert agree[1] >= meta["self_agreement"]["frac_tm_1e4"] - MARGIN, agree
+    assert agree[1] >= agree[0] + 0.1, agree
