@@ -130,10 +130,6 @@ static gtb_status check_options(gtb_handle* h) {
                  "the spatial-index detailed search is not implemented: set nodetailedsearch=1");
         return GTB_ERR_UNSUPPORTED;
     }
-    if (o.addsearchbyss) {
-        snprintf(h->err, sizeof(h->err), "--add-search-by-ss is not implemented");
-        return GTB_ERR_UNSUPPORTED;
-    }
     if (o.refinement < GTB_REFINEMENT_LOG || o.refinement > GTB_REFINEMENT_FULLA) {
         snprintf(h->err, sizeof(h->err), "--refinement %d out of -1..3", o.refinement);
         return GTB_ERR_ARG;
@@ -201,6 +197,7 @@ static gtb_status run_block(gtb_handle* h, const DevBlock& D, float scorethld,
     B.t_d0 = h->t_d0; B.t_d82 = h->t_d82; B.t_d0fin = h->t_d0fin;
     B.stepinit = (o.depth == 3) ? 5 : 1;
     B.refinement = o.refinement; B.depth = o.depth; B.twotm = o.twotmscore ? 1 : 0;
+    B.addss = o.addsearchbyss ? 1 : 0;
     B.symmetric = o.symmetric; B.nodeletions = o.nodeletions;
     const bool strings = hstr != nullptr;
 

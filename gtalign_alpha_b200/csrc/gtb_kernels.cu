@@ -29,8 +29,22 @@
 #include "gtb200.h"
 #include "gtb_device.cuh"
 #include "gtb_kernels.cuh"
+#include "gtb_gonnet.h"
 
 namespace gtb {
+
+// Residue exchange scores of the --add-search-by-ss DP (log2 Gonnet ratios
+// over the letters A..Z, built on the host by gtb_gonnet_scores); a global
+// array read through L1: the lanes of a warp look up different residues.
+__device__ float g_gonnet[GTB_GONNET_NA * GTB_GONNET_NA];
+constexpr float DPSS_C = -1048576.0f;     // offset of a diagonally reached cell
+constexpr float DPSS_CMP = -524288.0f;    // stored values below this carry it
+
+__device__ __forceinline__ float gonnet(unsigned char a, unsigned char b) {
+    return ('A' <= a && a <= 'Z' && 'A' <= b && b <= 'Z')
+               ? __ldg(g_gonnet + (a - 'A') * GTB_GONNET_NA + (b - 'A')) : 0.f;
+}
+
 
 #define GTB_LAUNCHED(T) do { if ((T).launches) (*(T).launches)++; } while (0)
 
@@ -1179,6 +1193,9 @@ void configure_kernels() {
     carve_refine<16, false>();
     carve_refine<32, false>();
     carve_refine<32, true>();
+    float gs[GTB_GONNET_NA * GTB_GONNET_NA];
+    gtb_gonnet_scores(gs);
+    cudaMemcpyToSymbol(g_gonnet, gs, sizeof(gs));
 }
 
 static void launch_refine_long_fin(int mode, const Blk& B, const Bat& T, cudaStream_t st) {
@@ -1228,13 +1245,22 @@ void launch_refine(int mode, const Blk& B, const Bat& T, cudaStream_t st, bool f
 // has published the steps whose last-row values it is about to read
 // (`prog`: steps done per strip), and publishes its own progress after each
 // group of steps.  Returns false when a wait gave up (error flag set).
-template <int R, bool gap0, bool usess, bool WAVE>
+// SC, the cell score: DP_SC_TFM (TM-score term under t), DP_SC_TFMSS (plus 0.5
+// for equal secondary structure), DP_SC_SSRR (the --add-search-by-ss DP,
+// dpssw_btck.cu:280-330: 1 for equal secondary structure + 0.2 x the Gonnet
+// score of the residues, no transform; a cell reached diagonally stores its
+// value + DPSS_C, a reader takes the offset off again, the gap cost is paid
+// once when leaving such a cell; the border reads as a diagonal cell of 0).
+template <int R, bool gap0, int SC, bool WAVE>
 __device__ __forceinline__ bool dp_pair(const float* t, float d02, float gcost, int lq, int lr,
                                         const float* qx, const float* qy, const float* qz,
                                         const float4* r4, const char* qs, const char* rs,
+                                        const unsigned char* qa, const unsigned char* ra,
                                         float* row, unsigned* bt, int lane, int s_first = 0,
                                         int s_step = 1, volatile int* prog = nullptr,
                                         volatile int* err = nullptr) {
+    constexpr bool usess = SC == DP_SC_TFMSS, ssrr = SC == DP_SC_SSRR;
+    constexpr float BND = ssrr ? DPSS_C : 0.f;   // the matrix border
     constexpr int ROWS = 32 * R, SPW = 16 / R;
     const unsigned FULL = 0xffffffffu;
     const int W = lr + 31;
@@ -1243,20 +1269,23 @@ __device__ __forceinline__ bool dp_pair(const float* t, float d02, float gcost, 
     for (int s = s_first; s < nstrips; s += s_step) {
         float tx[R], ty[R], tz[R], h[R];
         char qss[R];
+        unsigned char qaa[R];
         int nv = 0;  // valid rows of this lane (a prefix of its R rows)
 #pragma unroll
         for (int r = 0; r < R; r++) {
             int irow = s * ROWS + lane * R + r;
             tx[r] = ty[r] = tz[r] = 0.f;
             qss[r] = 0;
-            h[r] = 0.f;
+            qaa[r] = 0;
+            h[r] = BND;
             if (irow < lq) {
-                xform(t, __ldg(qx + irow), __ldg(qy + irow), __ldg(qz + irow), tx[r], ty[r], tz[r]);
-                if (usess) qss[r] = qs[irow];
+                if (!ssrr) xform(t, __ldg(qx + irow), __ldg(qy + irow), __ldg(qz + irow), tx[r], ty[r], tz[r]);
+                if (usess || ssrr) qss[r] = qs[irow];
+                if (ssrr) qaa[r] = qa[irow];
                 nv = r + 1;
             }
         }
-        float uplast = 0.f, rb = 0.f;
+        float uplast = BND, rb = BND;
         unsigned* bts = bt + (long long)s * ngrp * 32 + lane;
         const bool full = (s + 1) * ROWS <= lq;    // every lane has R rows
         __syncwarp();
@@ -1278,8 +1307,8 @@ __device__ __forceinline__ bool dp_pair(const float* t, float d02, float gcost, 
             }
             if ((g * SPW & 31) == 0) {            // the previous strip's last row, 32 columns
                 int jj = g * SPW + lane;
-                if (WAVE) rb = (s > 0 && jj < lr) ? __ldcg(row + jj) : 0.f;
-                else rb = (s > 0 && jj < lr) ? row[jj] : 0.f;
+                if (WAVE) rb = (s > 0 && jj < lr) ? __ldcg(row + jj) : BND;
+                else rb = (s > 0 && jj < lr) ? row[jj] : BND;
             }
             // SPW steps; CHK: some lane may be outside the matrix or have
             // fewer than R rows (strip ramps, the last strip)
@@ -1291,14 +1320,30 @@ __device__ __forceinline__ bool dp_pair(const float* t, float d02, float gcost, 
                     const int j = tt - lane;
                     float upv = __shfl_up_sync(FULL, h[R - 1], 1);
                     float up0 = __shfl_sync(FULL, rb, tt & 31);
-                    if (lane == 0) upv = (!CHK || j < lr) ? up0 : 0.f;
+                    if (lane == 0) upv = (!CHK || j < lr) ? up0 : BND;
                     if (!CHK || (j >= 0 && j < lr && nv > 0)) {
-                        float4 c4 = __ldg(r4 + j);
-                        char css = usess ? rs[j] : 0;
+                        float4 c4 = ssrr ? make_float4(0.f, 0.f, 0.f, 0.f) : __ldg(r4 + j);
+                        char css = (usess || ssrr) ? rs[j] : 0;
+                        unsigned char cra = ssrr ? ra[j] : 0;
                         float up = upv, dg = uplast;
 #pragma unroll
                         for (int r = 0; r < R; r++) {
-                            if (!CHK || r < nv) {
+                            if (ssrr && (!CHK || r < nv)) {
+                                float v = __fmaf_rn(gonnet(qaa[r], cra), 0.2f, (float)(qss[r] == css));
+                                v = __fadd_rn(v, dg < DPSS_CMP ? __fsub_rn(dg, DPSS_C) : dg);
+                                int bk = BT_DIAG;
+                                float l = h[r];
+                                if (l < DPSS_CMP) l = __fsub_rn(__fadd_rn(gcost, l), DPSS_C);
+                                if (v < l) { v = l; bk = BT_LEFT; }
+                                float uu = up;
+                                if (uu < DPSS_CMP) uu = __fsub_rn(__fadd_rn(gcost, uu), DPSS_C);
+                                if (v < uu) { v = uu; bk = BT_UP; }
+                                float w = bk == BT_DIAG ? __fadd_rn(v, DPSS_C) : v;
+                                dg = h[r];
+                                up = w;
+                                h[r] = w;
+                                acc |= (unsigned)bk << (2 * R * u + 2 * r);
+                            } else if (!ssrr && (!CHK || r < nv)) {
                                 float v = tmterm(d02, dist2(tx[r], ty[r], tz[r], c4.x, c4.y, c4.z));
                                 if (usess) v = __fadd_rn(v, __fmul_rn((float)(qss[r] == css), 0.5f));
                                 v = __fadd_rn(v, gap0 ? dg : fabsf(dg));
@@ -1334,7 +1379,7 @@ __device__ __forceinline__ bool dp_pair(const float* t, float d02, float gcost, 
     return true;
 }
 
-template <int GAP0, int USESS>
+template <int GAP0, int SC>
 __global__ void __launch_bounds__(128) k_dp(Blk B, Bat T, int tfmsrc, float gcost, int dpscan,
                                             int skipmode) {
     const int lane = threadIdx.x & 31;
@@ -1360,15 +1405,17 @@ __global__ void __launch_bounds__(128) k_dp(Blk B, Bat T, int tfmsrc, float gcos
     const char* rs = B.rs + B.roff[ri];
     float* row = T.row + T.off_row[i];
     unsigned* bt = T.bt + T.off_bt[i];
+    const unsigned char* qa = B.qa + B.qoff[qi];
+    const unsigned char* ra = B.ra + B.roff[ri];
     if (dp_r(lq) == 4)
-        dp_pair<4, GAP0 != 0, USESS != 0, false>(t, d02, gcost, lq, lr, qx, qy, qz, r4, qs, rs, row, bt, lane);
+        dp_pair<4, GAP0 != 0, SC, false>(t, d02, gcost, lq, lr, qx, qy, qz, r4, qs, rs, qa, ra, row, bt, lane);
     else
-        dp_pair<2, GAP0 != 0, USESS != 0, false>(t, d02, gcost, lq, lr, qx, qy, qz, r4, qs, rs, row, bt, lane);
+        dp_pair<2, GAP0 != 0, SC, false>(t, d02, gcost, lq, lr, qx, qy, qz, r4, qs, rs, qa, ra, row, bt, lane);
 }
 
 // One warp per CTA; the CTAs of a long pair take its strips round robin.
 // Launched cooperatively so that all CTAs are resident together.
-template <int GAP0, int USESS>
+template <int GAP0, int SC>
 __global__ void __launch_bounds__(32) k_dp_wave(Blk B, Bat T, int tfmsrc, float gcost, int dpscan,
                                                 int skipmode) {
     const int lane = threadIdx.x & 31;
@@ -1399,20 +1446,23 @@ __global__ void __launch_bounds__(32) k_dp_wave(Blk B, Bat T, int tfmsrc, float 
     float* row = T.row + T.off_row[i];
     unsigned* bt = T.bt + T.off_bt[i];
     volatile int* prog = T.dw_prog + T.dw_soff[slot];
+    const unsigned char* qa = B.qa + B.qoff[qi];
+    const unsigned char* ra = B.ra + B.roff[ri];
     if (dp_r(lq) == 4)
-        dp_pair<4, GAP0 != 0, USESS != 0, true>(t, d02, gcost, lq, lr, qx, qy, qz, r4, qs, rs, row,
-                                                bt, lane, c, G, prog, T.dw_err);
+        dp_pair<4, GAP0 != 0, SC, true>(t, d02, gcost, lq, lr, qx, qy, qz, r4, qs, rs, qa, ra, row,
+                                        bt, lane, c, G, prog, T.dw_err);
     else
-        dp_pair<2, GAP0 != 0, USESS != 0, true>(t, d02, gcost, lq, lr, qx, qy, qz, r4, qs, rs, row,
-                                                bt, lane, c, G, prog, T.dw_err);
+        dp_pair<2, GAP0 != 0, SC, true>(t, d02, gcost, lq, lr, qx, qy, qz, r4, qs, rs, qa, ra, row,
+                                        bt, lane, c, G, prog, T.dw_err);
 }
 
 int dp_wave_capacity() {
     int dev = 0, nsm = 0, m = 1 << 30, nb = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-    const void* ks[4] = {(const void*)k_dp_wave<1, 0>, (const void*)k_dp_wave<0, 0>,
-                         (const void*)k_dp_wave<0, 1>, (const void*)k_dp_wave<1, 1>};
+    const void* ks[5] = {(const void*)k_dp_wave<1, DP_SC_TFM>, (const void*)k_dp_wave<0, DP_SC_TFM>,
+                         (const void*)k_dp_wave<0, DP_SC_TFMSS>, (const void*)k_dp_wave<1, DP_SC_TFMSS>,
+                         (const void*)k_dp_wave<0, DP_SC_SSRR>};
     for (const void* k : ks) {
         if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k, 32, 0) != cudaSuccess) return 0;
         m = nb < m ? nb : m;
@@ -1420,13 +1470,13 @@ int dp_wave_capacity() {
     return m * nsm;
 }
 
-template <int GAP0, int USESS>
+template <int GAP0, int SC>
 static void launch_dp_wave(const Blk& B, const Bat& T, int tfmsrc, float gcost, int dpscan,
                            int skipmode, cudaStream_t st) {
     Blk b = B;
     Bat t = T;
     void* args[] = {&b, &t, &tfmsrc, &gcost, &dpscan, &skipmode};
-    cudaLaunchCooperativeKernel((const void*)k_dp_wave<GAP0, USESS>, dim3(T.ndw), dim3(32), args, 0, st);
+    cudaLaunchCooperativeKernel((const void*)k_dp_wave<GAP0, SC>, dim3(T.ndw), dim3(32), args, 0, st);
 }
 
 void launch_dp(const Blk& B, const Bat& T, int tfmsrc, int gap0, float gcost, int usess,
@@ -1441,17 +1491,19 @@ void launch_dp(const Blk& B, const Bat& T, int tfmsrc, int gap0, float gcost, in
     }
     if (T.ndw > 0) {
         cudaMemsetAsync(T.dw_prog, 0, (size_t)T.dw_nprog * sizeof(int), st);
-        if (gap0 && !usess) launch_dp_wave<1, 0>(B, T, tfmsrc, gcost, dpscan, skipmode, st);
-        else if (!gap0 && !usess) launch_dp_wave<0, 0>(B, T, tfmsrc, gcost, dpscan, skipmode, st);
-        else if (!gap0 && usess) launch_dp_wave<0, 1>(B, T, tfmsrc, gcost, dpscan, skipmode, st);
-        else launch_dp_wave<1, 1>(B, T, tfmsrc, gcost, dpscan, skipmode, st);
+        if (usess == DP_SC_SSRR) launch_dp_wave<0, DP_SC_SSRR>(B, T, tfmsrc, gcost, dpscan, skipmode, st);
+        else if (gap0 && !usess) launch_dp_wave<1, DP_SC_TFM>(B, T, tfmsrc, gcost, dpscan, skipmode, st);
+        else if (!gap0 && !usess) launch_dp_wave<0, DP_SC_TFM>(B, T, tfmsrc, gcost, dpscan, skipmode, st);
+        else if (!gap0 && usess) launch_dp_wave<0, DP_SC_TFMSS>(B, T, tfmsrc, gcost, dpscan, skipmode, st);
+        else launch_dp_wave<1, DP_SC_TFMSS>(B, T, tfmsrc, gcost, dpscan, skipmode, st);
         GTB_LAUNCHED(T);
     }
     const int nb = (T.np + 3) / 4;
-    if (gap0 && !usess) k_dp<1, 0><<<nb, 128, 0, st>>>(B, T, tfmsrc, gcost, dpscan, skipmode);
-    else if (!gap0 && !usess) k_dp<0, 0><<<nb, 128, 0, st>>>(B, T, tfmsrc, gcost, dpscan, skipmode);
-    else if (!gap0 && usess) k_dp<0, 1><<<nb, 128, 0, st>>>(B, T, tfmsrc, gcost, dpscan, skipmode);
-    else k_dp<1, 1><<<nb, 128, 0, st>>>(B, T, tfmsrc, gcost, dpscan, skipmode);
+    if (usess == DP_SC_SSRR) k_dp<0, DP_SC_SSRR><<<nb, 128, 0, st>>>(B, T, tfmsrc, gcost, dpscan, skipmode);
+    else if (gap0 && !usess) k_dp<1, DP_SC_TFM><<<nb, 128, 0, st>>>(B, T, tfmsrc, gcost, dpscan, skipmode);
+    else if (!gap0 && !usess) k_dp<0, DP_SC_TFM><<<nb, 128, 0, st>>>(B, T, tfmsrc, gcost, dpscan, skipmode);
+    else if (!gap0 && usess) k_dp<0, DP_SC_TFMSS><<<nb, 128, 0, st>>>(B, T, tfmsrc, gcost, dpscan, skipmode);
+    else k_dp<1, DP_SC_TFMSS><<<nb, 128, 0, st>>>(B, T, tfmsrc, gcost, dpscan, skipmode);
     GTB_LAUNCHED(T);
 }
 
@@ -1764,6 +1816,16 @@ void launch_stages(const Blk& B, const Bat& T, int refinement, int depth, int co
     launch_refine(RM_INIT, B, T, st, false);
     mark(2);
     dprefine(1, 1, 2, false);
+    if (B.addss) {
+        // --add-search-by-ss (custage_ssrr.cu:43-140, CuBatch.cu:583-600): the
+        // alignment of the SS and residue-scored DP, fragment refinement over it,
+        // DP refinement with the gap cost and without, 2 iterations each
+        launch_dp(B, T, DP_TFM_GRAND, 0, -1.0f, DP_SC_SSRR, 0, 1, st);
+        launch_btck(B, T, 0, st);
+        launch_refine(RM_DP, B, T, st, few);
+        dprefine(0, 0, 2, few);
+        dprefine(1, 0, 2, few);
+    }
     // two stage-2 passes: MpStage2.h:63-83, CuBatch.cu:627-650
     for (int call = 0; call < 2; call++) {
         int gap0 = call == 1;

@@ -46,6 +46,7 @@ struct Blk {
     const float *t_d0, *t_d82, *t_d0fin;  // per-length constants
     int stepinit, refinement, depth, symmetric, nodeletions;
     int twotm;                       // --2tm-score: record fields 13 and 14
+    int addss;                       // --add-search-by-ss
 };
 
 // Batch of consecutive pairs p0 .. p0+np-1 of a block (pair = qi*nr + ri).
@@ -86,6 +87,9 @@ struct Bat {
     long long* launches;             // host counter of kernel launches
 };
 
+// DP cell scores (launch_dp's usess): TM term under a transform, + SS, or the
+// --add-search-by-ss score (SS + Gonnet, no transform)
+enum DpScore { DP_SC_TFM = 0, DP_SC_TFMSS = 1, DP_SC_SSRR = 2 };
 // RM_PLOG: one round of the production phase-2 log search (--refinement -1)
 enum RefineMode { RM_INIT = 0, RM_DP = 1, RM_FIN1 = 2, RM_FIN2 = 3, RM_PROD1 = 4, RM_PROD2 = 5,
                   RM_PLOG = 6 };

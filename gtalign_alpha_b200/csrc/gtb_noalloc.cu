@@ -99,9 +99,9 @@ extern "C" gtb_status gtb_process_block_noalloc(int device, const gtb_options* o
         setmsg(errbuf, errlen, "null argument or device out of range (%lld, %lld)", device, MAXDEV);
         return GTB_ERR_ARG;
     }
-    if (!opts->nodetailedsearch || opts->addsearchbyss) {
-        setmsg(errbuf, errlen, "option combination not implemented (detailed search %lld, search by ss %lld)",
-               !opts->nodetailedsearch, opts->addsearchbyss);
+    if (!opts->nodetailedsearch) {
+        setmsg(errbuf, errlen, "the spatial-index detailed search is not implemented (%lld %lld)",
+               !opts->nodetailedsearch, 0);
         return GTB_ERR_UNSUPPORTED;
     }
     if (!(scorethld >= 0.f && scorethld < 1.f) || opts->depth < 0 || opts->depth > 3 ||
@@ -198,6 +198,7 @@ extern "C" gtb_status gtb_process_block_noalloc(int device, const gtb_options* o
     B.t_d0 = D.d0; B.t_d82 = D.d82; B.t_d0fin = D.d0fin;
     B.stepinit = (opts->depth == 3) ? 5 : 1;
     B.refinement = opts->refinement; B.depth = opts->depth; B.twotm = opts->twotmscore ? 1 : 0;
+    B.addss = opts->addsearchbyss ? 1 : 0;
     B.symmetric = opts->symmetric; B.nodeletions = opts->nodeletions;
 
     Bat T{};

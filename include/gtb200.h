@@ -82,7 +82,9 @@ typedef struct {
     int   nodeletions;       /* --no-deletions */
     int   nodetailedsearch;  /* --no-detailed-search: must be 1 (the spatial-index
                                 search stage is not part of this library) */
-    int   addsearchbyss;     /* --add-search-by-ss: must be 0 */
+    int   addsearchbyss;     /* --add-search-by-ss: after stage 1, an alignment
+                                by secondary structure and residue similarity,
+                                refined like stage 2's */
     int   twotmscore;        /* --2tm-score: record fields GTB_OUT_2SCOREQ/R get
                                 the TM-scores without the aligned pairs of a
                                 helix and a non-helix residue */

@@ -13,8 +13,8 @@ LEVEL_SETS = {-1: "c0_level_m1", 0: "c0_level_0", 1: "c0_level_1", 2: "c0_level_
 SETS = ["c0_speed13", "c0_default", "c0_filters", "c0_sym_ref_nodel", "c0_shallow", "c0_2tm",
         "c0_ssrr"] + \
     list(LEVEL_SETS.values())
-# the sets whose options the CUDA library implements
-LIBRARY_SETS = [s for s in SETS if s != "c0_ssrr"]
+# the sets whose options the CUDA library implements (all of them)
+LIBRARY_SETS = list(SETS)
 
 
 def _soa(z, tag):

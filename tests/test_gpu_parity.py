@@ -17,14 +17,16 @@ def _lib_opts(d):
     from gtalign_alpha_b200.api import Options
     return Options(refinement=d["refinement"], depth=d.get("depth", 2), convergence=d["convergence"],
                    prescore=d["prescore"], symmetric=d["symmetric"], referenced=d["referenced"],
-                   nodeletions=d["nodeletions"], twotmscore=d.get("twotmscore", 0))
+                   nodeletions=d["nodeletions"], twotmscore=d.get("twotmscore", 0),
+                   addsearchbyss=d.get("addsearchbyss", 0))
 
 
 def _ora_opts(oracle, d):
     return oracle.opts_from(refinement=d["refinement"], convergence=d["convergence"],
                             prescore=d["prescore"], scorethld=d["scorethld"], depth=d.get("depth", 2),
                             symmetric=d["symmetric"], referenced=d["referenced"],
-                            nodeletions=d["nodeletions"], twotmscore=d.get("twotmscore", 0))
+                            nodeletions=d["nodeletions"], twotmscore=d.get("twotmscore", 0),
+                            addsearchbyss=d.get("addsearchbyss", 0))
 
 
 def assert_same(res, ora, nq, nr):
@@ -70,6 +72,8 @@ OPTSETS = {
     "fulla": dict(refinement=3, convergence=4, prescore=0.0, scorethld=0.0, symmetric=0, referenced=1, nodeletions=0),
     "twotm": dict(refinement=1, convergence=6, prescore=0.3, scorethld=0.3, symmetric=1, referenced=1, nodeletions=0,
                   twotmscore=1),
+    "ssrr": dict(refinement=1, convergence=6, prescore=0.3, scorethld=0.3, symmetric=0, referenced=0, nodeletions=0,
+                 addsearchbyss=1),
 }
 
 
@@ -173,18 +177,19 @@ def test_status_codes():
         assert res.alndata.shape == (1, 2, 16)
 
 
-@pytest.mark.parametrize("refinement", [1, -1, 3])
-def test_long_chain_assemblies(oracle, refinement):
+@pytest.mark.parametrize("refinement,addss", [(1, 0), (-1, 0), (3, 0), (1, 1)])
+def test_long_chain_assemblies(oracle, refinement, addss):
     """Multi-domain assemblies and their per-domain-perturbed partners (the
     long-chain configuration's construction at 1,200 and 2,000 residues):
     large DP matrices, many strips and thousands of refinement variants; the
     2,000-residue pair takes the many-CTA refinement path in every final
-    form (one search, log search, full search in both phases)."""
+    form (one search, log search, full search in both phases); with
+    --add-search-by-ss its DP runs there as a wavefront too."""
     from gtalign_alpha_b200 import synth
     wl = synth.config2(seed=3, lengths=(1200, 2000))
     q, r = synth.pack(wl.queries), synth.pack(wl.refs)
     d = dict(refinement=refinement, convergence=18 if refinement == 1 else 4, prescore=0.4,
-             scorethld=0.5, symmetric=0, referenced=0, nodeletions=0)
+             scorethld=0.5, symmetric=0, referenced=0, nodeletions=0, addsearchbyss=addss)
     res, ora = run_both(oracle, q, r, d)
     assert_same(res, ora, q.n, r.n)
     assert res.alndata[0, 0, 9] > 0.5 and res.alndata[1, 1, 9] > 0.5
