@@ -46,7 +46,7 @@ class _COptions(ctypes.Structure):
                 ("symmetric", ctypes.c_int), ("referenced", ctypes.c_int),
                 ("nodeletions", ctypes.c_int), ("nodetailedsearch", ctypes.c_int),
                 ("addsearchbyss", ctypes.c_int), ("twotmscore", ctypes.c_int),
-                ("polish_steps", ctypes.c_int)]
+                ("polish_steps", ctypes.c_int), ("presimilarity", ctypes.c_float)]
 
 
 class _CResults(ctypes.Structure):
@@ -73,6 +73,7 @@ class Options:
     addsearchbyss: int = 0
     twotmscore: int = 0
     polish_steps: int = 0      # adjoint polishing of the final transforms (this library only)
+    presimilarity: float = 0.0  # --pre-similarity (0: off)
 
     @classmethod
     def speed(cls, level: int, **kw) -> "Options":
@@ -88,7 +89,7 @@ class Options:
         return _COptions(self.refinement, self.depth, self.convergence, self.prescore,
                          self.symmetric, self.referenced, self.nodeletions,
                          self.nodetailedsearch, self.addsearchbyss, self.twotmscore,
-                         self.polish_steps)
+                         self.polish_steps, self.presimilarity)
 
 
 _lib = None

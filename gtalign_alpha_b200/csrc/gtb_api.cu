@@ -134,6 +134,10 @@ static gtb_status check_options(gtb_handle* h) {
         snprintf(h->err, sizeof(h->err), "--refinement %d out of -1..3", o.refinement);
         return GTB_ERR_ARG;
     }
+    if (!(o.presimilarity >= 0.f && o.presimilarity < 1e6f)) {
+        snprintf(h->err, sizeof(h->err), "--pre-similarity out of range");
+        return GTB_ERR_ARG;
+    }
     if (o.polish_steps < 0 || o.polish_steps > 50) {
         snprintf(h->err, sizeof(h->err), "polish_steps %d out of 0..50", o.polish_steps);
         return GTB_ERR_ARG;
@@ -198,6 +202,9 @@ static gtb_status run_block(gtb_handle* h, const DevBlock& D, float scorethld,
     B.stepinit = (o.depth == 3) ? 5 : 1;
     B.refinement = o.refinement; B.depth = o.depth; B.twotm = o.twotmscore ? 1 : 0;
     B.addss = o.addsearchbyss ? 1 : 0;
+    // the screen runs when the block's longest structures exceed the edge
+    // (CuBatch.cu:459-462)
+    B.presim = (0.f < o.presimilarity && PRESIM_EDGE < B.qmax && PRESIM_EDGE < B.rmax) ? o.presimilarity : 0.f;
     B.symmetric = o.symmetric; B.nodeletions = o.nodeletions;
     const bool strings = hstr != nullptr;
 

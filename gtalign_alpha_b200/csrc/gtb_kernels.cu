@@ -141,7 +141,9 @@ __global__ void k_init(Blk B, Bat T) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= T.np) return;
     int qi = pair_qi(B, T, i), ri = pair_ri(B, T, i);
-    T.flags[i] = (B.qmol[qi] != B.rmol[ri]) ? CONV_LOWTMSC : 0;
+    // with the --pre-similarity screen every pair starts filtered, with no
+    // molecule-type check (custage1.cu:74-82); k_presim releases the ones that pass
+    T.flags[i] = (B.presim > 0.f || B.qmol[qi] != B.rmol[ri]) ? CONV_LOWTMSC : 0;
     T.grand[i] = 0.f; T.best[i] = 0.f; T.best0[i] = 0.f; T.rmsd32[i] = -1.f;
     T.seedq[i] = 0; T.seedr[i] = 0; T.naln[i] = 0;
     T.sfndx[i] = T.sfpos[i] = T.sfndx_cur[i] = T.sfpos_cur[i] = 0;
@@ -159,6 +161,56 @@ __global__ void k_init(Blk B, Bat T) {
 
 void launch_init(const Blk& B, const Bat& T, cudaStream_t st) {
     k_init<<<(T.np + 127) / 128, 128, 0, st>>>(B, T);
+    GTB_LAUNCHED(T);
+}
+
+// --pre-similarity (MpStage1.cpp:175-248, PMBatchStrData.inl:37-95; the
+// reference's GPU form similarity.cu): a pair passes when some diagonal,
+// every 2nd one at least PRESIM_EDGE residues from either end, has an
+// ungapped run whose Gonnet scores sum to the threshold or more.  Diagonals
+// are numbered over the block's longest query and reference: diagonal di
+// starts at query position 2*di or, past the query's last admissible start,
+// at reference position ((2*di - (lq - 20)) rounded down to even) + 2.  A
+// warp per pair, its lanes on 32 diagonals at a time, each summing its run
+// in position order (prefix sum minus the smallest prefix so far).
+__global__ void __launch_bounds__(128) k_presim(Blk B, Bat T) {
+    const unsigned FULL = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    const int i = blockIdx.x * 4 + (threadIdx.x >> 5);
+    if (i >= T.np) return;                        // the same for the whole warp
+    int qi = pair_qi(B, T, i), ri = pair_ri(B, T, i);
+    const int ql = B.qlen[qi], rl = B.rlen[ri];
+    const unsigned char* qa = B.qa + B.qoff[qi];
+    const unsigned char* ra = B.ra + B.roff[ri];
+    const int ndiag = (B.qmax + B.rmax - 2 * PRESIM_EDGE) >> 1;
+    bool pass = false;
+    for (int d0 = 0; d0 < ndiag; d0 += 32) {
+        const int di = d0 + lane;
+        if (di < ndiag && !pass) {
+            int qp = di * 2, rp = 0;
+            if (ql - PRESIM_EDGE <= qp) { rp = ((qp - (ql - PRESIM_EDGE)) & ~1) + 2; qp = 0; }
+            if (!(ql - PRESIM_EDGE <= qp || rl - PRESIM_EDGE <= rp)) {
+                const int n1 = ql - qp < rl ? ql - qp : rl, n2 = rl - rp < ql ? rl - rp : ql;
+                const int n = n1 < n2 ? n1 : n2;
+                float s = 0.f, mn = 0.f, best = 0.f;
+                for (int k = 0; k < n; k++) {
+                    s = __fadd_rn(s, gonnet(qa[qp + k], ra[rp + k]));
+                    mn = s < mn ? s : mn;
+                    const float loc = __fsub_rn(s, mn);
+                    best = loc > best ? loc : best;
+                }
+                pass = B.presim <= best;
+            }
+        }
+        if (__any_sync(FULL, pass)) {
+            if (lane == 0) T.flags[i] = 0;
+            return;
+        }
+    }
+}
+
+void launch_presim(const Blk& B, const Bat& T, cudaStream_t st) {
+    k_presim<<<(T.np + 3) / 4, 128, 0, st>>>(B, T);
     GTB_LAUNCHED(T);
 }
 
@@ -1811,6 +1863,7 @@ void launch_stages(const Blk& B, const Bat& T, int refinement, int depth, int co
     };
     mark(0);
     launch_init(B, T, st);
+    if (B.presim > 0.f) launch_presim(B, T, st);
     launch_findfrag(B, T, st);
     mark(1);
     launch_refine(RM_INIT, B, T, st, false);

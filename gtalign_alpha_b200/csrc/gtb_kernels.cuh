@@ -47,6 +47,7 @@ struct Blk {
     int stepinit, refinement, depth, symmetric, nodeletions;
     int twotm;                       // --2tm-score: record fields 13 and 14
     int addss;                       // --add-search-by-ss
+    float presim;                    // --pre-similarity threshold when the screen runs, else 0
 };
 
 // Batch of consecutive pairs p0 .. p0+np-1 of a block (pair = qi*nr + ri).
@@ -108,6 +109,9 @@ void launch_pack4_structs(float4* out, const float* x, const float* y, const flo
                           const int* off, const int* len, const int* coff, int n,
                           cudaStream_t st);
 void launch_init(const Blk& B, const Bat& T, cudaStream_t st);
+// the --pre-similarity screen (B.presim > 0): 20 positions kept from the ends
+constexpr int PRESIM_EDGE = 20;
+void launch_presim(const Blk& B, const Bat& T, cudaStream_t st);
 // Seed offsets per CTA (a pair with more is split over several CTAs).
 constexpr int FF_CHUNK = 512;
 // the seed's offset index range [silo, sihi] of a pair (MpStage1.cpp:299-318)

@@ -107,7 +107,8 @@ extern "C" gtb_status gtb_process_block_noalloc(int device, const gtb_options* o
     if (!(scorethld >= 0.f && scorethld < 1.f) || opts->depth < 0 || opts->depth > 3 ||
         opts->refinement < GTB_REFINEMENT_LOG || opts->refinement > GTB_REFINEMENT_FULLA ||
         opts->convergence < 1 || opts->convergence > 30 || !(opts->prescore >= 0.f && opts->prescore < 1.f) ||
-        opts->polish_steps < 0 || opts->polish_steps > 50) {
+        opts->polish_steps < 0 || opts->polish_steps > 50 ||
+        !(opts->presimilarity >= 0.f && opts->presimilarity < 1e6f)) {
         setmsg(errbuf, errlen, "option out of range (%lld %lld)", 0, 0);
         return GTB_ERR_ARG;
     }
@@ -199,6 +200,7 @@ extern "C" gtb_status gtb_process_block_noalloc(int device, const gtb_options* o
     B.stepinit = (opts->depth == 3) ? 5 : 1;
     B.refinement = opts->refinement; B.depth = opts->depth; B.twotm = opts->twotmscore ? 1 : 0;
     B.addss = opts->addsearchbyss ? 1 : 0;
+    B.presim = (0.f < opts->presimilarity && PRESIM_EDGE < qmax && PRESIM_EDGE < rmax) ? opts->presimilarity : 0.f;
     B.symmetric = opts->symmetric; B.nodeletions = opts->nodeletions;
 
     Bat T{};

@@ -95,6 +95,10 @@ typedef struct {
                                 FP64 recomputation; a step is kept only if it
                                 raises the TM-score (d0 of the shorter
                                 structure) over the final alignment */
+    float presimilarity;     /* --pre-similarity: 0 (off) or the score an
+                                ungapped run of Gonnet residue scores on some
+                                diagonal of a pair must reach for the pair to
+                                be compared at all */
 } gtb_options;
 
 /* Result buffers (host memory), sizes for nq queries x nr references with

@@ -678,6 +678,39 @@ static void dp_ss_run(pairctx* P, float gcost) {
     }
 }
 
+/* --pre-similarity (MpStage1.cpp:175-248, PMBatchStrData.inl:37-95): the pair
+ * passes when some diagonal, every 2nd one at least 20 residues from either
+ * end, has an ungapped run of residue pairs whose Gonnet scores sum to the
+ * threshold or more.  The diagonals are numbered over the block's longest
+ * query and reference; diagonal di starts at query position 2*di, or, past
+ * the query's last admissible start, at reference position
+ * ((2*di - (lq - 20)) rounded down to even) + 2. */
+#define PRESIM_EDGE 20
+#define PRESIM_STEP 2
+static int presim_pass(const pairctx* P, float thr) {
+    int ql = P->lq, rl = P->lr;
+    int ndiag = (P->qmax + P->rmax - 2 * PRESIM_EDGE) >> 1;
+    for (int di = 0; di < ndiag; di++) {
+        int qp = di * PRESIM_STEP, rp = 0;
+        if (ql - PRESIM_EDGE <= qp) {
+            rp = ((qp - (ql - PRESIM_EDGE)) & ~1) + PRESIM_STEP;
+            qp = 0;
+        }
+        if (ql - PRESIM_EDGE <= qp || rl - PRESIM_EDGE <= rp) continue;
+        int n1 = ql - qp < rl ? ql - qp : rl, n2 = rl - rp < ql ? rl - rp : ql;
+        int n = n1 < n2 ? n1 : n2;
+        float s = 0.f, mn = 0.f, best = 0.f;
+        for (int k = 0; k < n; k++) {
+            s = s + gonnet_score(P->qa[qp + k], P->ra[rp + k]);
+            mn = s < mn ? s : mn;
+            float loc = s - mn;
+            best = loc > best ? loc : best;
+        }
+        if (thr <= best) return 1;
+    }
+    return 0;
+}
+
 /* unconstrained traceback: MpDPHub.cpp:1515-1660 */
 static void btck_matched(pairctx* P) {
     int y = P->lq - 1, x = P->lr - 1, n = 0;
@@ -1002,7 +1035,12 @@ static void production_alignment(pairctx* P, char* dst) {
 static void run_pair(pairctx* P, char* alndst) {
     const gto_opts* o = P->o;
     /* preinit: MpStage1.cpp:28-167 */
-    P->flags = (P->qmol != P->rmol) ? CONV_LOWTMSC : 0;
+    /* with --pre-similarity active every pair starts filtered, with no
+     * molecule-type check, and the ones that pass are released
+     * (custage1.cu:74-82, MpStage1.cpp:123-128) */
+    int presim = 0.0f < o->presimilarity && PRESIM_EDGE < P->qmax && PRESIM_EDGE < P->rmax;
+    P->flags = (presim || P->qmol != P->rmol) ? CONV_LOWTMSC : 0;
+    if (presim && presim_pass(P, o->presimilarity)) P->flags = 0;
     P->grand = P->best = P->best0 = 0.f;
     P->seedq = P->seedr = 0;
     P->naln = 0;

@@ -45,6 +45,7 @@ typedef struct {
     int   nodeletions;   /* --no-deletions */
     int   twotmscore;    /* --2tm-score */
     int   addsearchbyss; /* --add-search-by-ss */
+    float presimilarity; /* --pre-similarity (0: off) */
 } gto_opts;
 
 /* Process a block of nq queries x nr references.

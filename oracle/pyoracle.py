@@ -36,7 +36,7 @@ class _Opts(ctypes.Structure):
                 ("prescore", ctypes.c_float), ("scorethld", ctypes.c_float),
                 ("symmetric", ctypes.c_int), ("referenced", ctypes.c_int),
                 ("nodeletions", ctypes.c_int), ("twotmscore", ctypes.c_int),
-                ("addsearchbyss", ctypes.c_int)]
+                ("addsearchbyss", ctypes.c_int), ("presimilarity", ctypes.c_float)]
 
 
 _lib = None
@@ -83,14 +83,14 @@ class OracleResult:
 def opts_from(refinement: int = 0, convergence: int = 2, prescore: float = 0.0,
               scorethld: float = 0.0, depth: int = 2, symmetric: int = 0,
               referenced: int = 0, nodeletions: int = 0, twotmscore: int = 0,
-              addsearchbyss: int = 0) -> _Opts:
+              addsearchbyss: int = 0, presimilarity: float = 0.0) -> _Opts:
     """Options in the gtalign command line's encoding: --refinement -1 log
     search, 0 coarse, 1 one search (the default), 2 full, 3 full in both final
     phases (the oracle, like the reference, stores code + 1); --depth 0..3
-    (3 = shallow); --2tm-score; --add-search-by-ss."""
+    (3 = shallow); --2tm-score; --add-search-by-ss; --pre-similarity."""
     return _Opts(5 if depth == 3 else 1, refinement + 1, depth, convergence,
                  prescore, scorethld, symmetric, referenced, nodeletions, twotmscore,
-                 addsearchbyss)
+                 addsearchbyss, presimilarity)
 
 
 def process_block(qsoa, rsoa, opts: _Opts, nthreads: int = 0) -> OracleResult:

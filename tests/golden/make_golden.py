@@ -64,6 +64,8 @@ SETS = {
                ["--no-detailed-search", "--2tm-score", "--pre-score=0", "-s", "0"]),
     "c0_ssrr": (lambda: synth.config0(seed=110, n_refs=60, qlen=150, homolog_frac=0.5),
                 ["--no-detailed-search", "--add-search-by-ss", "--pre-score=0", "-s", "0"]),
+    "c0_presim": (lambda: synth.config0(seed=111, n_refs=80, qlen=150, homolog_frac=0.3),
+                  ["--no-detailed-search", "--pre-similarity=15", "--pre-score=0", "-s", "0"]),
     "c0_shallow": (lambda: synth.config0(seed=108, n_refs=60, qlen=160),
                    ["--no-detailed-search", "--depth=3", "--pre-score=0.3", "-s", "0.3",
                     "--convergence=6"]),

@@ -11,7 +11,7 @@ GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 LEVEL_SETS = {-1: "c0_level_m1", 0: "c0_level_0", 1: "c0_level_1", 2: "c0_level_2",
               3: "c0_level_3"}
 SETS = ["c0_speed13", "c0_default", "c0_filters", "c0_sym_ref_nodel", "c0_shallow", "c0_2tm",
-        "c0_ssrr"] + \
+        "c0_ssrr", "c0_presim"] + \
     list(LEVEL_SETS.values())
 # the sets whose options the CUDA library implements (all of them)
 LIBRARY_SETS = list(SETS)
@@ -38,7 +38,8 @@ def load(name):
 def cli_options(opts):
     """Translate the reference CLI options of a set into oracle/library options."""
     d = dict(refinement=1, convergence=18, prescore=0.4, scorethld=0.5, depth=2,
-             symmetric=0, referenced=0, nodeletions=0, twotmscore=0, addsearchbyss=0)
+             symmetric=0, referenced=0, nodeletions=0, twotmscore=0, addsearchbyss=0,
+             presimilarity=0.0)
     i = 0
     while i < len(opts):
         o = opts[i]
@@ -64,5 +65,7 @@ def cli_options(opts):
             d["twotmscore"] = 1
         elif o == "--add-search-by-ss":
             d["addsearchbyss"] = 1
+        elif o.startswith("--pre-similarity="):
+            d["presimilarity"] = float(o.split("=")[1])
         i += 1
     return d

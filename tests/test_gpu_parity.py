@@ -18,7 +18,7 @@ def _lib_opts(d):
     return Options(refinement=d["refinement"], depth=d.get("depth", 2), convergence=d["convergence"],
                    prescore=d["prescore"], symmetric=d["symmetric"], referenced=d["referenced"],
                    nodeletions=d["nodeletions"], twotmscore=d.get("twotmscore", 0),
-                   addsearchbyss=d.get("addsearchbyss", 0))
+                   addsearchbyss=d.get("addsearchbyss", 0), presimilarity=d.get("presimilarity", 0.0))
 
 
 def _ora_opts(oracle, d):
@@ -26,7 +26,8 @@ def _ora_opts(oracle, d):
                             prescore=d["prescore"], scorethld=d["scorethld"], depth=d.get("depth", 2),
                             symmetric=d["symmetric"], referenced=d["referenced"],
                             nodeletions=d["nodeletions"], twotmscore=d.get("twotmscore", 0),
-                            addsearchbyss=d.get("addsearchbyss", 0))
+                            addsearchbyss=d.get("addsearchbyss", 0),
+                            presimilarity=d.get("presimilarity", 0.0))
 
 
 def assert_same(res, ora, nq, nr):
@@ -74,6 +75,8 @@ OPTSETS = {
                   twotmscore=1),
     "ssrr": dict(refinement=1, convergence=6, prescore=0.3, scorethld=0.3, symmetric=0, referenced=0, nodeletions=0,
                  addsearchbyss=1),
+    "presim": dict(refinement=1, convergence=6, prescore=0.0, scorethld=0.0, symmetric=0, referenced=0, nodeletions=0,
+                   presimilarity=12.0),
 }
 
 

@@ -47,7 +47,7 @@ def run_oracle(oracle, name):
         refinement=d["refinement"], convergence=d["convergence"], prescore=d["prescore"],
         scorethld=d["scorethld"], symmetric=d["symmetric"], referenced=d["referenced"],
         nodeletions=d["nodeletions"], depth=d["depth"], twotmscore=d["twotmscore"],
-        addsearchbyss=d["addsearchbyss"]))
+        addsearchbyss=d["addsearchbyss"], presimilarity=d["presimilarity"]))
     return q, r, qn, rn, meta, d, o
 
 
@@ -207,3 +207,22 @@ def test_oracle_search_by_ss_pinned(oracle):
         agree[ss] = c / len(meta["results"])
     assert agree[1] >= meta["self_agreement"]["frac_tm_1e4"] - MARGIN, agree
     assert agree[1] >= agree[0] + 0.1, agree
+
+
+def test_oracle_presimilarity_pinned(oracle):
+    """--pre-similarity: the pairs that pass the ungapped sequence-similarity
+    screen are exactly the ones the reference reports (it reports every pair
+    that proceeds with -s 0 and --pre-score 0); without the screen every pair
+    proceeds."""
+    q, r, qn, rn, meta = gu.load("c0_presim")
+    d = gu.cli_options(meta["options"])
+    theirs = set(meta["results"])
+    for thr, expect in ((d["presimilarity"], theirs), (0.0, None)):
+        o = oracle.process_block(q, r, oracle.opts_from(
+            refinement=1, convergence=18, prescore=0.0, scorethld=0.0, presimilarity=thr))
+        ours = {qn[qi] + "|" + rn[ri] for qi in range(q.n) for ri in range(r.n)
+                if o.out[qi, ri, 4] >= 1}
+        if expect is not None:
+            assert ours == expect, (sorted(ours ^ expect))
+        else:
+            assert len(ours) == q.n * r.n > len(theirs)
