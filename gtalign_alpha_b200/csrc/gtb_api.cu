@@ -502,6 +502,25 @@ static gtb_status parse_soa(gtb_handle* h, char* const* beg, char* const* end, H
     return GTB_OK;
 }
 
+// Pairs of two nucleic-acid structures need the reference's base-pairing
+// secondary structure (sskna.cu, MpSecStr.cpp:140-200) and the nucleic-acid
+// final d0 (GetD0finNA, stagecnsts.cuh:95-106), which this library does not
+// have: blocks that would compare such a pair are refused rather than scored
+// with the protein rules.  Protein/nucleic-acid pairs are skipped, as in the
+// reference, except under --pre-similarity, which compares them too
+// (custage1.cu:74-82), so there any nucleic-acid structure is refused.
+static gtb_status check_na_pairs(gtb_handle* h, const std::vector<int>& qmol,
+                                 const std::vector<int>& rmol) {
+    const bool qna = std::find(qmol.begin(), qmol.end(), 1) != qmol.end();
+    const bool rna = std::find(rmol.begin(), rmol.end(), 1) != rmol.end();
+    if ((qna && rna) || (0.f < h->opts.presimilarity && (qna || rna))) {
+        snprintf(h->err, sizeof(h->err),
+                 "nucleic-acid structure pairs are not supported (protein rules would be applied)");
+        return GTB_ERR_UNSUPPORTED;
+    }
+    return GTB_OK;
+}
+
 extern "C" size_t gtb_alns_size(char* const* qb, char* const* qe, char* const* rb, char* const* re) {
     if (!qb || !qe || !rb || !re) return 0;
     long long nq = (qe[GTB_FLD_LEN] - qb[GTB_FLD_LEN]) / (long)sizeof(int);
@@ -607,6 +626,7 @@ extern "C" gtb_status gtb_process_resident(gtb_handle* h, float scorethld, const
     if (!(scorethld >= 0.f && scorethld < 1.f)) { snprintf(h->err, sizeof(h->err), "scorethld out of [0,1)"); return GTB_ERR_ARG; }
     gtb_status s = check_options(h);
     if (s != GTB_OK) return s;
+    if ((s = check_na_pairs(h, queries->mol, refs->mol)) != GTB_OK) return s;
     CK(cudaSetDevice(h->dev));
     DevBlock D = make_devblock(queries, refs);
     return run_block(h, D, scorethld, d_alndata, d_tfm, d_numerr, nullptr, nullptr);
@@ -625,6 +645,7 @@ extern "C" gtb_status gtb_process_block(gtb_handle* h, float scorethld,
     HostSoA Q, R;
     if ((s = parse_soa(h, querypmbeg, querypmend, Q, "queries")) != GTB_OK) return s;
     if ((s = parse_soa(h, bdbCpmbeg, bdbCpmend, R, "references")) != GTB_OK) return s;
+    if ((s = check_na_pairs(h, Q.mol, R.mol)) != GTB_OK) return s;
     CK(cudaSetDevice(h->dev));
     cudaStream_t st = h->st;
     gtb_block* qb = new gtb_block();

@@ -164,6 +164,18 @@ def test_status_codes():
         with pytest.raises(GTBError) as e:
             g.process_block(q, r)
         assert e.value.status == 1
+    # a pair of two nucleic-acid structures is refused (the library has no
+    # nucleic-acid secondary structure or final d0); a protein query against
+    # a nucleic-acid reference is accepted and the pair skipped
+    qn, rn = synth.pack(wl.queries), synth.pack(wl.refs)
+    qn.mol[0] = 1
+    rn.mol[1] = 1
+    with GTalignB200(0, 0, Options()) as g:
+        with pytest.raises(GTBError) as e:
+            g.process_block(qn, rn)
+        assert e.value.status == 4
+        qn.mol[0] = 0
+        g.process_block(qn, rn)
     with GTalignB200(0, 0, Options()) as g:
         with pytest.raises(GTBError) as e:
             g.process_block(q, r, scorethld=1.5)
