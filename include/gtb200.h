@@ -203,7 +203,10 @@ gtb_status gtb_polish(gtb_handle* h, int npairs, const long long* off,
  * a one-time set-up there (device addresses of the static arrays, constant
  * tables): make it before any stream capture.  All calls share the scratch
  * array, so calls that overlap on the GPU race; issue them one after another.
- * Results are those of gtb_process_block (records and transforms only). */
+ * Results are those of gtb_process_block (records and transforms only).
+ * The molecule types are device data here, so the nucleic-acid refusal of
+ * gtb_process_block is not made: the caller must not pass blocks that pair
+ * two nucleic-acid structures (they would be scored with protein rules). */
 #define GTB_NOALLOC_SCRATCH_BYTES ((size_t)16 << 20)
 #define GTB_NOALLOC_MAX_PAIRS 4096
 
