@@ -70,3 +70,25 @@ def test_pack_fields_layout():
         assert pk.end[f] - pk.beg[f] == a.nbytes
     ins = pk.arrays[6]
     assert ins[s.offs[2]] > 0 and (ins[s.offs[[0, 1, 3, 4]]] <= 0).all()
+
+
+def test_python_structs_match_the_c_header(tmp_path):
+    """The ctypes mirrors of gtb_options and gtb_results have the C header's
+    field offsets and sizes (compiled with the host C compiler)."""
+    import subprocess
+    from gtalign_alpha_b200.api import _COptions, _CResults
+    src = tmp_path / "layout.c"
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "gtb200.h"', "int main(void) {"]
+    for cname, py in (("gtb_options", _COptions), ("gtb_results", _CResults)):
+        lines.append('printf("%s size %%zu\\n", sizeof(%s));' % (cname, cname))
+        for fname, _ in py._fields_:
+            lines.append('printf("%s.%s %%zu\\n", offsetof(%s, %s));' % (cname, fname, cname, fname))
+    lines.append("return 0; }")
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "layout"
+    subprocess.check_call(["gcc", "-I", os.path.join(ROOT, "include"), "-o", str(exe), str(src)])
+    got = dict(l.rsplit(" ", 1) for l in subprocess.check_output([str(exe)]).decode().splitlines())
+    for cname, py in (("gtb_options", _COptions), ("gtb_results", _CResults)):
+        assert int(got[cname + " size"]) == ctypes.sizeof(py), cname
+        for fname, _ in py._fields_:
+            assert int(got["%s.%s" % (cname, fname)]) == getattr(py, fname).offset, (cname, fname)
