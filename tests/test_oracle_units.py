@@ -1,5 +1,7 @@
 """Building blocks of the oracle: the FP64 rotation solve, secondary
 structure, constants."""
+import os
+
 import numpy as np
 
 
@@ -82,3 +84,33 @@ def test_constants_follow_reference_formulas(oracle):
     assert abs(v[3].value - (1.24 * np.cbrt(135) - 1.8)) < 1e-5
     L.gto_constants(10, 300, *[ctypes.byref(x) for x in v])
     assert abs(v[0].value - (0.168 + 0.8)) < 1e-6 and abs(v[3].value - 0.5) < 1e-7
+
+
+def test_gonnet_scores_table():
+    """gtb_gonnet.h: log2 of the Gonnet (1992) frequency ratios, 10^(G/10)
+    rounded to 6 decimals: symmetric, the published diagonal (A 2.4, W 14.2,
+    C 11.5), 0 for letters outside the 20 amino acids, 26 x 26 over A..Z."""
+    import ctypes
+    import math
+    import subprocess
+    import tempfile
+    import numpy as np
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    d = tempfile.mkdtemp()
+    src = os.path.join(d, "g.c")
+    with open(src, "w") as f:
+        f.write('#include "gtb_gonnet.h"\nvoid dump(float* o) { gtb_gonnet_scores(o); }\n')
+    so = os.path.join(d, "g.so")
+    subprocess.check_call(["gcc", "-O2", "-shared", "-fPIC", "-I",
+                           os.path.join(root, "gtalign_alpha_b200", "csrc"), "-o", so, src, "-lm"])
+    out = np.zeros(26 * 26, np.float32)
+    ctypes.CDLL(so).dump(out.ctypes.data_as(ctypes.POINTER(ctypes.c_float)))
+    s = out.reshape(26, 26)
+    assert np.array_equal(s, s.T)
+    ix = lambda c: ord(c) - 65
+    for c, g in (("A", 24), ("W", 142), ("C", 115), ("G", 66)):
+        ratio = np.float32(round(10 ** (g / 100.0) * 1e6) / 1e6)
+        assert abs(float(s[ix(c), ix(c)]) - math.log2(float(ratio))) < 1e-6
+    for c in "BJOUXZ":
+        assert (s[ix(c)] == 0).all()
+    assert s[ix("W"), ix("W")] == s.max() and s[ix("W"), ix("D")] < 0
