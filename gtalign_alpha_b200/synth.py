@@ -51,6 +51,7 @@ class Chain:
     xyz: np.ndarray            # (L, 3) float32
     seq: np.ndarray            # (L,) uint8 residue letters
     name: str = "chain"
+    na: bool = False           # nucleic acid: C3' atoms, bases A/C/G/U
 
     @property
     def length(self) -> int:
@@ -224,11 +225,60 @@ def homolog(rng: np.random.Generator, tmpl: Chain, sigma: float,
     return Chain(_pdb_round_fast(P), aas.astype(np.uint8), name)
 
 
+NA_COMPLEMENT = {"A": "U", "U": "A", "G": "C", "C": "G"}
+
+
+def na_hairpins(rng: np.random.Generator, n_hairpins: int, stem: int, loop: int,
+                name: str, noise: float = 0.3, rise: float = 5.9) -> Chain:
+    """A nucleic-acid chain of C3' atoms: hairpins in a row, each an
+    antiparallel stem of ``stem`` complementary base pairs whose C3' atoms
+    are 13.75 A apart (the middle of the 12.5-15 A pairing window of the
+    reference's base-pair assignment), ``rise`` A between stem neighbours,
+    closed by a ``loop``-residue arc; hairpins 30 A apart, joined by 2
+    residues."""
+    pts, seq = [], []
+    for h in range(n_hairpins):
+        x0 = 30.0 * h
+        s1 = [rng.choice(list("ACGU")) for _ in range(stem)]
+        if h > 0:   # linker from the previous hairpin's last residue
+            for t in (1, 2):
+                pts.append((x0 - 16.25 + 5.4 * t, 0.0, -3.0))
+                seq.append(rng.choice(list("ACGU")))
+        for k in range(stem):
+            pts.append((x0, 0.0, rise * k))
+            seq.append(s1[k])
+        top = rise * (stem - 1)
+        for t in range(loop):
+            a = np.pi * (t + 1) / (loop + 1)
+            pts.append((x0 + 6.875 - 6.875 * np.cos(a), 2.0 * np.sin(a), top + 6.0 * np.sin(a)))
+            seq.append(rng.choice(list("ACGU")))
+        for k in range(stem - 1, -1, -1):
+            pts.append((x0 + 13.75, 0.0, rise * k))
+            seq.append(NA_COMPLEMENT[s1[k]])
+    xyz = np.array(pts, dtype=np.float64) + rng.normal(0.0, noise, size=(len(pts), 3))
+    xyz = xyz @ _rot_random(rng).T
+    return Chain(_pdb_round_fast(xyz).astype(np.float32),
+                 np.frombuffer("".join(seq).encode(), dtype=np.uint8).copy(), name, na=True)
+
+
+def na_moved_copy(rng: np.random.Generator, tmpl: Chain, sigma: float, name: str) -> Chain:
+    """A rigidly moved copy of a nucleic-acid chain with Gaussian noise."""
+    xyz = tmpl.xyz.astype(np.float64) @ _rot_random(rng).T + rng.uniform(-20, 20, size=3)
+    xyz = xyz + rng.normal(0.0, sigma, size=xyz.shape)
+    return Chain(_pdb_round_fast(xyz).astype(np.float32), tmpl.seq.copy(), name, na=True)
+
+
 def write_pdb(ch: Chain, path: str) -> None:
-    """Write a C-alpha-only PDB file the reference reader accepts."""
+    """Write a PDB file the reference reader accepts: C-alpha atoms of a
+    protein, or C3' atoms of a nucleic acid (residue names "  A" etc., which
+    the reader takes for nucleotides)."""
     lines = []
     for i in range(ch.length):
         x, y, z = (float(v) for v in ch.xyz[i])
+        if ch.na:
+            lines.append("ATOM  %5d  C3'   %s A%4d    %8.3f%8.3f%8.3f  1.00  0.00           C\n"
+                         % (i + 1, chr(int(ch.seq[i])), i + 1, x, y, z))
+            continue
         res = AA3[chr(int(ch.seq[i]))]
         lines.append("ATOM  %5d  CA  %3s A%4d    %8.3f%8.3f%8.3f  1.00  0.00           C\n"
                      % (i + 1, res, i + 1, x, y, z))
@@ -393,7 +443,7 @@ def pack(chains: Sequence[Chain]) -> SoA:
                np.ascontiguousarray(xyz[:, 1], dtype=np.float32),
                np.ascontiguousarray(xyz[:, 2], dtype=np.float32),
                np.ascontiguousarray(rsd, dtype=np.uint8),
-               np.zeros(len(lens), dtype=np.int32))
+               np.array([1 if c.na else 0 for c in chains], dtype=np.int32))
 
 
 def write_dirs(wl: Workload, qdir: str, rdir: str) -> None:

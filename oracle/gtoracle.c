@@ -89,6 +89,19 @@ static float c_d0fin(int lq, int lr) {
     if (d0 < 0.5f) d0 = 0.5f;
     return d0;
 }
+/* GetD0finNA, stagecnsts.cuh:93-106: the final d0 of a nucleic-acid pair */
+static float c_d0fin_na(int lq, int lr) {
+    float l = (float)(lq < lr ? lq : lr);
+    float d0 = 0.3f;
+    if (30.f <= l) d0 = 0.6f * sqrtf(l - 0.5f) - 2.5f;
+    else if (23.f < l) d0 = 0.7f;
+    else if (19.f < l) d0 = 0.6f;
+    else if (15.f < l) d0 = 0.5f;
+    else if (11.f < l) d0 = 0.4f;
+    return d0 > 0.3f ? d0 : 0.3f;
+}
+/* GetD0fin(l1, l2, type), stagecnsts.cuh:108-114: type of the reference structure */
+static float c_d0fin_t(int lq, int lr, int na) { return na ? c_d0fin_na(lq, lr) : c_d0fin(lq, lr); }
 static float c_d0s(float d0) {
     float d = d0;
     d = d < 8.f ? d : 8.f;
@@ -293,6 +306,38 @@ static float ss_dst(const float* x, const float* y, const float* z, int i, int j
     float c = dz * dz;
     return sqrtf((a + b) + c);
 }
+/* Secondary structure of a nucleic-acid chain (MpSecStr.cpp:140-200 and
+ * 265-360, MpSecStr.h:163-200): every residue gets '.'; residue y's
+ * partner is the residue x, more than 2 positions away and of a
+ * complementary base (A-T/U, G-C, G-U), whose C3' distance deviates least
+ * from 13.75 A (at most 1.25 A); y and x pair, '(' then ')', when each is
+ * the other's partner. */
+void gto_secstr_na(int len, const float* x, const float* y, const float* z,
+                   const unsigned char* rsd, char* ss) {
+    int* partner = (int*)malloc(sizeof(int) * (len > 0 ? len : 1));
+    for (int p = 0; p < len; p++) { ss[p] = '.'; partner[p] = -1; }
+    for (int yi = 0; yi < len; yi++) {
+        char a = (char)rsd[yi];
+        float best = 9999.9f;
+        int col = -1;
+        for (int xi = 0; xi < len; xi++) {
+            char b = (char)rsd[xi];
+            int cond = ((a == 'T' || a == 'U') && b == 'A') || (a == 'A' && (b == 'T' || b == 'U')) ||
+                       (a == 'G' && (b == 'C' || b == 'U')) || ((a == 'C' || a == 'U') && b == 'G');
+            if (!cond || abs(xi - yi) <= 2) continue;
+            float dev = fabsf(ss_dst(x, y, z, yi, xi) - 13.75f);
+            if (1.25f < dev) dev = 9999.9f;
+            if (dev < best) { best = dev; col = xi; }
+        }
+        if (best < 1.5f) partner[yi] = col;
+    }
+    for (int p = 0; p < len; p++) {
+        int q = partner[p];
+        if (0 <= q && q < len && p < q && partner[q] == p) { ss[p] = '('; ss[q] = ')'; }
+    }
+    free(partner);
+}
+
 void gto_secstr(int len, const float* x, const float* y, const float* z, char* ss) {
     for (int p = 0; p < len; p++) ss[p] = ' ';
     for (int p = 2; p + 2 < len; p++) {
@@ -785,7 +830,7 @@ static void prod_variant(const pairctx* P, const kspace* s, int n, int kf, int f
     if (*best < 0.f) { *gbest = *best; return; }   /* nothing computed */
     if (P->lq != P->lr) {
         int gl = P->lq > P->lr ? P->lq : P->lr;
-        float g0 = c_d0fin(gl, gl);
+        float g0 = c_d0fin_t(gl, gl, P->rmol);
         *gbest = score_pass(P, s, n, tb, g0 * g0, 0, P->d82, 0, NULL);
     } else *gbest = *best;
 }
@@ -795,8 +840,8 @@ static void prod_write(pairctx* P, const prodwin* w) {
     if ((float)P->lr < (float)P->lq) { float t = bs; bs = gb; gb = t; }
     P->out[GTO_SCOREQ] = bs / (float)P->lq;
     P->out[GTO_SCORER] = gb / (float)P->lr;
-    P->out[GTO_D0Q] = c_d0fin(P->lq, P->lq);
-    P->out[GTO_D0R] = c_d0fin(P->lr, P->lr);
+    P->out[GTO_D0Q] = c_d0fin_t(P->lq, P->lq, P->rmol);
+    P->out[GTO_D0R] = c_d0fin_t(P->lr, P->lr, P->rmol);
     memcpy(P->tfm_gr, w->tfm, sizeof(w->tfm));
 }
 
@@ -845,7 +890,7 @@ static void production_logsearch(pairctx* P, const kspace* s, int n) {
     w.best = best;
     if (P->lq != P->lr) {
         int gl = P->lq > P->lr ? P->lq : P->lr;
-        float g0 = c_d0fin(gl, gl);
+        float g0 = c_d0fin_t(gl, gl, P->rmol);
         w.gbest = score_pass(P, s, n, tb, g0 * g0, 0, P->d82, 0, NULL);
     } else w.gbest = best;
     memcpy(w.tfm, tb, sizeof(tb));
@@ -939,7 +984,7 @@ static void production(pairctx* P, int refinement) {
      * residue is in a helix and the other is not (MpStageFin.cpp:1723-1818,
      * MpStageBase.h:825-856) */
     if (n > 0) {
-        double d0q = c_d0fin(P->lq, P->lq), d0r = c_d0fin(P->lr, P->lr);
+        double d0q = c_d0fin_t(P->lq, P->lq, P->rmol), d0r = c_d0fin_t(P->lr, P->lr, P->rmol);
         double d0q2 = d0q * d0q, d0r2 = d0r * d0r, tq = 0.0, tr = 0.0, t2q = 0.0, t2r = 0.0;
         double dv[21];
         memset(dv, 0, sizeof(dv));
@@ -1051,6 +1096,7 @@ static void run_pair(pairctx* P, char* alndst) {
     memset(P->err, 0, sizeof(P->err));
     P->out[GTO_RMSD] = 9999.9f;
     gto_constants(P->lq, P->lr, &P->d0, &P->d02, &P->d82, &P->d0fin, NULL);
+    if (P->rmol) P->d0fin = c_d0fin_na(P->lq, P->lr);
     P->d0s = c_d0s(P->d0);
     float d02dpscan = (P->d0 + 1.5f) * (P->d0 + 1.5f);
     if (alndst) alndst[0] = alndst[P->lq + P->lr + 1] = alndst[2 * (P->lq + P->lr + 1)] =
@@ -1143,16 +1189,16 @@ int gto_process_block(const gto_opts* o,
         if (rlen[i] > rmax) rmax = rlen[i];
         if (rlen[i] < rmin) rmin = rlen[i];
     }
-    /* secondary structure (protein only) */
+    /* secondary structure: protein, or nucleic-acid base pairs */
     for (int i = 0; i < nq; i++) {
         long long b = qoff[i];
         if (!qmol || qmol[i] == 0) gto_secstr(qlen[i], qx + b, qy + b, qz + b, qss + b);
-        else memset(qss + b, ' ', qlen[i]);
+        else gto_secstr_na(qlen[i], qx + b, qy + b, qz + b, qrsd + b, qss + b);
     }
     for (int i = 0; i < nr; i++) {
         long long b = roff[i];
         if (!rmol || rmol[i] == 0) gto_secstr(rlen[i], rx + b, ry + b, rz + b, rss + b);
-        else memset(rss + b, ' ', rlen[i]);
+        else gto_secstr_na(rlen[i], rx + b, ry + b, rz + b, rrsd + b, rss + b);
     }
     long long npairs = (long long)nq * nr;
     (void)nthreads;

@@ -68,6 +68,8 @@ int gto_process_block(const gto_opts* o,
 
 /* single building blocks (exposed for unit tests) */
 void gto_secstr(int len, const float* x, const float* y, const float* z, char* ss);
+void gto_secstr_na(int len, const float* x, const float* y, const float* z,
+                   const unsigned char* rsd, char* ss);
 int  gto_solve(const float* sums15, int n, float* tfm12);
 void gto_constants(int lq, int lr, float* d0, float* d02, float* d82,
                    float* d0fin, float* d02dpscan);

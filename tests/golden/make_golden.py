@@ -34,6 +34,23 @@ from gtalign_alpha_b200 import synth  # noqa: E402
 
 BIN = os.path.join(ROOT, "oracle", "_ref", "gtalign")
 
+def na_set(seed):
+    """Nucleic acids: a query of 3 hairpins, moved noisy copies of it,
+    unrelated hairpin chains, and a few proteins (skipped against it).  The
+    stems rise 7.5 A per pair, so that a stem residue's only C3' within the
+    12.5-15 A pairing window is its partner's (the diagonal neighbours sit
+    at 15.7 A): the reference's CPU build picks a partner among several
+    candidates with a vectorised reduction whose winner is not always the
+    closest one, unlike its GPU form."""
+    rng = np.random.default_rng(seed)
+    q = synth.na_hairpins(rng, 3, 10, 6, "qry000000", rise=7.5)
+    refs = [synth.na_moved_copy(rng, q, float(rng.uniform(0.3, 1.5)), "hom%06d" % k) for k in range(10)]
+    refs += [synth.na_hairpins(rng, int(rng.integers(1, 5)), int(rng.integers(5, 13)),
+                               int(rng.integers(4, 9)), "ref%06d" % k, rise=7.5) for k in range(14)]
+    refs += synth.random_chains(rng, list(rng.integers(60, 200, size=4)), "prt")
+    return synth.Workload([q], refs, seed, "nucleic acids")
+
+
 SETS = {
     # name: (workload builder, reference CLI options)
     "c0_speed13": (lambda: synth.config0(seed=101, n_refs=80, qlen=150),
@@ -66,6 +83,7 @@ SETS = {
                 ["--no-detailed-search", "--add-search-by-ss", "--pre-score=0", "-s", "0"]),
     "c0_presim": (lambda: synth.config0(seed=111, n_refs=80, qlen=150, homolog_frac=0.3),
                   ["--no-detailed-search", "--pre-similarity=15", "--pre-score=0", "-s", "0"]),
+    "c0_na": (lambda: na_set(112), ["--no-detailed-search", "--pre-score=0", "-s", "0"]),
     "c0_shallow": (lambda: synth.config0(seed=108, n_refs=60, qlen=160),
                    ["--no-detailed-search", "--depth=3", "--pre-score=0.3", "-s", "0.3",
                     "--convergence=6"]),
@@ -140,6 +158,7 @@ def main():
             arrs[tag + "_lens"] = s.lens
             arrs[tag + "_xyz"] = np.stack([s.x, s.y, s.z], axis=1)
             arrs[tag + "_rsd"] = s.rsd
+            arrs[tag + "_mol"] = s.mol
             arrs[tag + "_names"] = np.array([c.name for c in chains])
         np.savez_compressed(os.path.join(HERE, name + ".npz"), **arrs)
         with open(os.path.join(HERE, name + ".json"), "w") as f:

@@ -11,10 +11,10 @@ GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 LEVEL_SETS = {-1: "c0_level_m1", 0: "c0_level_0", 1: "c0_level_1", 2: "c0_level_2",
               3: "c0_level_3"}
 SETS = ["c0_speed13", "c0_default", "c0_filters", "c0_sym_ref_nodel", "c0_shallow", "c0_2tm",
-        "c0_ssrr", "c0_presim"] + \
+        "c0_ssrr", "c0_presim", "c0_na"] + \
     list(LEVEL_SETS.values())
-# the sets whose options the CUDA library implements (all of them)
-LIBRARY_SETS = list(SETS)
+# the sets the CUDA library takes (it refuses nucleic-acid pairs)
+LIBRARY_SETS = [s for s in SETS if s != "c0_na"]
 
 
 def _soa(z, tag):
@@ -23,9 +23,9 @@ def _soa(z, tag):
     if len(lens) > 1:
         offs[1:] = np.cumsum(lens[:-1])
     xyz = z[tag + "_xyz"].astype(np.float32)
+    mol = z[tag + "_mol"].astype(np.int32) if tag + "_mol" in z else np.zeros(len(lens), np.int32)
     return SoA(lens, offs, np.ascontiguousarray(xyz[:, 0]), np.ascontiguousarray(xyz[:, 1]),
-               np.ascontiguousarray(xyz[:, 2]), z[tag + "_rsd"].astype(np.uint8),
-               np.zeros(len(lens), np.int32))
+               np.ascontiguousarray(xyz[:, 2]), z[tag + "_rsd"].astype(np.uint8), mol)
 
 
 def load(name):
