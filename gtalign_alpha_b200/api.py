@@ -285,3 +285,56 @@ class GTalignB200:
                            err.reshape(nq, nr, NERR) if err is not None else None,
                            alns, qb.arrays[0].copy(), rb.arrays[0].copy(), rb.arrays[1].copy(),
                            qss, rss, int(self.lib.gtb_last_launch_count(self._h)), tms)
+
+
+class _CClusterOptions(ctypes.Structure):
+    _fields_ = [("linkage", ctypes.c_int), ("measure", ctypes.c_int),
+                ("threshold", ctypes.c_float), ("coverage", ctypes.c_float),
+                ("onesided", ctypes.c_int)]
+
+
+@dataclass
+class Clusters:
+    """Clusters of n structures: each a list of structure indices with the
+    representative first, listed as the reference's cluster file lists them
+    (largest first, then by the representative's id); and the pointer
+    representation (pi, lambda) of the linkage."""
+    clusters: list
+    pi: np.ndarray
+    lam: np.ndarray
+
+
+def cluster(alndata: np.ndarray, lens: np.ndarray, ids: Optional[list] = None,
+            linkage: int = 0, measure: int = 0, threshold: float = 0.5,
+            coverage: float = 0.7, onesided: bool = False) -> Clusters:
+    """Cluster n structures from the (n, n, GTB_NOUT) records of their
+    all-against-all block with gtb_cluster (the --cls options: linkage 0
+    complete / 1 single, measure = --sort, threshold, coverage, one-sided).
+    ``ids`` (default: the indices as strings) order clusters of equal size."""
+    L = load_library()
+    rec = np.ascontiguousarray(alndata, dtype=np.float32)
+    n = int(rec.shape[0])
+    if rec.shape != (n, n, NOUT):
+        raise GTBError(1, "records must have shape (n, n, %d)" % NOUT)
+    lens = np.ascontiguousarray(lens, dtype=np.int32)
+    ids = [str(i) for i in range(n)] if ids is None else list(ids)
+    o = _CClusterOptions(linkage, measure, threshold, coverage, 1 if onesided else 0)
+    pi = np.zeros(n, np.int32)
+    lam = np.zeros(n, np.float32)
+    member = np.zeros(n, np.int32)
+    offset = np.zeros(n + 1, np.int32)
+    rep = np.zeros(n, np.int32)
+    ncl = ctypes.c_int(0)
+    ip = ctypes.POINTER(ctypes.c_int)
+    fp = ctypes.POINTER(ctypes.c_float)
+    L.gtb_cluster.argtypes = [ctypes.c_int, fp, ip, ctypes.POINTER(_CClusterOptions),
+                              ip, fp, ip, ip, ip, ip]
+    L.gtb_cluster.restype = ctypes.c_int
+    st = L.gtb_cluster(n, rec.ctypes.data_as(fp), lens.ctypes.data_as(ip), ctypes.byref(o),
+                       pi.ctypes.data_as(ip), lam.ctypes.data_as(fp), member.ctypes.data_as(ip),
+                       offset.ctypes.data_as(ip), rep.ctypes.data_as(ip), ctypes.byref(ncl))
+    if st != 0:
+        raise GTBError(st, "gtb_cluster: invalid arguments")
+    cl = [list(member[offset[c]:offset[c + 1]]) for c in range(ncl.value)]
+    cl.sort(key=lambda c: (-len(c), ids[c[0]]))
+    return Clusters(cl, pi, lam)

@@ -9,8 +9,8 @@ PKG = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(PKG)
 CSRC = os.path.join(PKG, "csrc")
 LIB = os.path.join(PKG, "libgtb200.so")
-SOURCES = ["gtb_kernels.cu", "gtb_api.cu", "gtb_adjoint.cu", "gtb_noalloc.cu"]
-HEADERS = ["gtb_device.cuh", "gtb_kernels.cuh"]
+SOURCES = ["gtb_kernels.cu", "gtb_api.cu", "gtb_adjoint.cu", "gtb_noalloc.cu", "gtb_cluster.cu"]
+HEADERS = ["gtb_device.cuh", "gtb_kernels.cuh", "gtb_gonnet.h"]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",

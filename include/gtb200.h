@@ -241,6 +241,42 @@ gtb_status gtb_last_timings(const gtb_handle* h, float* ms7);
 
 void gtb_destroy(gtb_handle* h);
 
+/* Clustering of n structures from the records of their all-against-all
+ * block (queries = references = the n structures, record (q, i) at
+ * (q*n + i)*GTB_NOUT), as the reference's clustering writer does it
+ * (TdClustWriter.h:225-488, TdClustWriter.cpp:271-414; the --cls options).
+ * The distance of structure q to an earlier structure i comes from record
+ * (q, i): 1 - TM-score by the --sort measure (or the RMSD), or the largest
+ * distance when the aligned residues cover less than `coverage` of either
+ * length (of both with `onesided`) or the pair was not aligned.  The
+ * pointer representation of single or complete linkage is built over the
+ * structures in their order; clusters are cut at the threshold.  Host code:
+ * needs no device. */
+enum { GTB_LINKAGE_COMPLETE = 0, GTB_LINKAGE_SINGLE = 1 };
+/* --sort codes that define the distance (CLOptions.h:64-70) */
+enum {
+    GTB_SORT_TMGREATER = 0, GTB_SORT_TMREF = 1, GTB_SORT_TMQUERY = 2,
+    GTB_SORT_TMHARMONIC = 3, GTB_SORT_RMSD = 4
+};
+typedef struct {
+    int   linkage;     /* --cls-algorithm: 0 complete (default), 1 single */
+    int   measure;     /* --sort: GTB_SORT_* (default 0) */
+    float threshold;   /* --cls-threshold: TM-score (or RMSD) to join (default 0.5) */
+    float coverage;    /* --cls-coverage (0,1] (default 0.7) */
+    int   onesided;    /* --cls-one-sided-coverage */
+} gtb_cluster_options;
+
+/* Out: pi/lambda (n each, may be NULL): the pointer representation; the
+ * clusters: *ncl of them, cluster c's structures at member[offset[c] ..
+ * offset[c+1]) (n entries in all; the representative, the member of the
+ * smallest lambda, first, then the others in the writer's order), rep[c]
+ * its representative (rep and offset sized n and n+1).  The reference's
+ * file lists clusters by size, largest first, then by the representative's
+ * id. */
+gtb_status gtb_cluster(int n, const float* alndata, const int* lens,
+                       const gtb_cluster_options* opts, int* pi, float* lambda,
+                       int* member, int* offset, int* rep, int* ncl);
+
 #ifdef __cplusplus
 }
 #endif
