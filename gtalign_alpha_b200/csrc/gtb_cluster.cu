@@ -99,26 +99,54 @@ void clink(int n, std::vector<float>& mu, std::vector<int>& pi, std::vector<floa
 
 }  // namespace
 
-extern "C" gtb_status gtb_cluster(int n, const float* alndata, const int* lens,
-                                  const gtb_cluster_options* opts, int* pi_out, float* lambda_out,
-                                  int* member, int* offset, int* rep, int* ncl) {
-    if (n < 1 || !alndata || !lens || !opts || !member || !offset || !rep || !ncl) return GTB_ERR_ARG;
-    const gtb_cluster_options& o = *opts;
-    if ((o.linkage != GTB_LINKAGE_COMPLETE && o.linkage != GTB_LINKAGE_SINGLE) ||
-        o.measure < GTB_SORT_TMGREATER || o.measure > GTB_SORT_RMSD ||
-        !(o.coverage > 0.0f && o.coverage <= 1.0f) || !(o.threshold >= 0.0f && o.threshold < 100.0f))
-        return GTB_ERR_ARG;
+struct gtb_clusterer {
+    int n = 0, next = 0;
+    gtb_cluster_options o{};
+    std::vector<int> lens, pi;
+    std::vector<float> lambda, mu;
+};
 
-    // pointer representation, one structure at a time
-    std::vector<int> pi(n);
-    std::vector<float> lambda(n), mu(n);
-    for (int q = 0; q < n; q++) {
-        for (int i = 0; i < q; i++)
-            mu[i] = pair_distance(alndata + ((long long)q * n + i) * GTB_NOUT, lens[q], lens[i], o);
-        if (o.linkage == GTB_LINKAGE_SINGLE) slink(q, mu, pi, lambda);
-        else clink(q, mu, pi, lambda);
-    }
+static bool valid(const gtb_cluster_options& o) {
+    return (o.linkage == GTB_LINKAGE_COMPLETE || o.linkage == GTB_LINKAGE_SINGLE) &&
+           o.measure >= GTB_SORT_TMGREATER && o.measure <= GTB_SORT_RMSD &&
+           (o.coverage > 0.0f && o.coverage <= 1.0f) && (o.threshold >= 0.0f && o.threshold < 100.0f);
+}
 
+extern "C" gtb_status gtb_cluster_create(int n, const int* lens, const gtb_cluster_options* opts,
+                                         gtb_clusterer** out) {
+    if (!out) return GTB_ERR_ARG;
+    *out = nullptr;
+    if (n < 1 || !lens || !opts || !valid(*opts)) return GTB_ERR_ARG;
+    gtb_clusterer* c = new gtb_clusterer();
+    c->n = n;
+    c->o = *opts;
+    c->lens.assign(lens, lens + n);
+    c->pi.assign(n, 0);
+    c->lambda.assign(n, 0.0f);
+    c->mu.assign(n, 0.0f);
+    *out = c;
+    return GTB_OK;
+}
+
+// structure q's records against the structures before it, in order (the
+// reference runs the linkage as each query's results arrive,
+// TdClustWriter.cpp:229-249)
+extern "C" gtb_status gtb_cluster_add(gtb_clusterer* c, int q, const float* rec) {
+    if (!c || q != c->next || q >= c->n || (q > 0 && !rec)) return GTB_ERR_ARG;
+    for (int i = 0; i < q; i++) c->mu[i] = pair_distance(rec + (long long)i * GTB_NOUT, c->lens[q], c->lens[i], c->o);
+    if (c->o.linkage == GTB_LINKAGE_SINGLE) slink(q, c->mu, c->pi, c->lambda);
+    else clink(q, c->mu, c->pi, c->lambda);
+    c->next++;
+    return GTB_OK;
+}
+
+extern "C" gtb_status gtb_cluster_finish(gtb_clusterer* cl, int* pi_out, float* lambda_out, int* member,
+                                         int* offset, int* rep, int* ncl) {
+    if (!cl || cl->next != cl->n || !member || !offset || !rep || !ncl) return GTB_ERR_ARG;
+    const int n = cl->n;
+    const gtb_cluster_options& o = cl->o;
+    const std::vector<int>& pi = cl->pi;
+    const std::vector<float>& lambda = cl->lambda;
     // clusters at the threshold (TdClustWriter.cpp:271-346): subclusters
     // ("layers") of structures, and clusters of subclusters
     const float thr = o.measure == GTB_SORT_RMSD ? o.threshold : std::max(0.0f, 1.0f - o.threshold);
@@ -184,4 +212,19 @@ extern "C" gtb_status gtb_cluster(int n, const float* alndata, const int* lens,
     if (pi_out) std::memcpy(pi_out, pi.data(), sizeof(int) * n);
     if (lambda_out) std::memcpy(lambda_out, lambda.data(), sizeof(float) * n);
     return GTB_OK;
+}
+
+extern "C" void gtb_cluster_destroy(gtb_clusterer* c) { delete c; }
+
+extern "C" gtb_status gtb_cluster(int n, const float* alndata, const int* lens,
+                                  const gtb_cluster_options* opts, int* pi_out, float* lambda_out,
+                                  int* member, int* offset, int* rep, int* ncl) {
+    if (n < 1 || !alndata) return GTB_ERR_ARG;
+    gtb_clusterer* c = nullptr;
+    gtb_status s = gtb_cluster_create(n, lens, opts, &c);
+    for (int q = 0; s == GTB_OK && q < n; q++)
+        s = gtb_cluster_add(c, q, alndata + (long long)q * n * GTB_NOUT);
+    if (s == GTB_OK) s = gtb_cluster_finish(c, pi_out, lambda_out, member, offset, rep, ncl);
+    gtb_cluster_destroy(c);
+    return s;
 }

@@ -277,6 +277,19 @@ gtb_status gtb_cluster(int n, const float* alndata, const int* lens,
                        const gtb_cluster_options* opts, int* pi, float* lambda,
                        int* member, int* offset, int* rep, int* ncl);
 
+/* The same, one structure at a time (O(n) memory, as the reference runs it
+ * while query blocks finish): create with the n lengths; add structure q =
+ * 0, 1, ..., n-1 in order with rec = its records against structures 0..q-1
+ * (rec[i*GTB_NOUT], i < q; a query's row of its all-against-all block);
+ * finish once all n are added (outputs as gtb_cluster); destroy. */
+typedef struct gtb_clusterer gtb_clusterer;
+gtb_status gtb_cluster_create(int n, const int* lens, const gtb_cluster_options* opts,
+                              gtb_clusterer** out);
+gtb_status gtb_cluster_add(gtb_clusterer* c, int q, const float* rec);
+gtb_status gtb_cluster_finish(gtb_clusterer* c, int* pi, float* lambda, int* member,
+                              int* offset, int* rep, int* ncl);
+void gtb_cluster_destroy(gtb_clusterer* c);
+
 #ifdef __cplusplus
 }
 #endif

@@ -169,3 +169,42 @@ def test_invalid_options():
         with pytest.raises(GTBError) as e:
             cluster(rec, lens, **kw)
         assert e.value.status == 1
+
+
+def test_streaming_equals_all_at_once():
+    """gtb_cluster_create/add/finish, one structure's records at a time
+    (only the entries before it), give the all-at-once result; rows must
+    come in order."""
+    import ctypes
+    from gtalign_alpha_b200.api import _CClusterOptions, load_library
+    L = load_library()
+    tm = planted(8, n=30)
+    rec, lens = records(tm)
+    for linkage in (0, 1):
+        ref = cluster(rec, lens, linkage=linkage)
+        o = _CClusterOptions(linkage, 0, 0.5, 0.7, 0)
+        vp, ip, fp = ctypes.c_void_p, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_float)
+        L.gtb_cluster_create.argtypes = [ctypes.c_int, ip, ctypes.POINTER(_CClusterOptions),
+                                         ctypes.POINTER(vp)]
+        L.gtb_cluster_add.argtypes = [vp, ctypes.c_int, fp]
+        L.gtb_cluster_finish.argtypes = [vp, ip, fp, ip, ip, ip, ip]
+        L.gtb_cluster_destroy.argtypes = [vp]
+        h = vp()
+        assert L.gtb_cluster_create(30, lens.ctypes.data_as(ip), ctypes.byref(o), ctypes.byref(h)) == 0
+        assert L.gtb_cluster_add(h, 1, None) == 1           # out of order
+        for q in range(30):
+            row = np.ascontiguousarray(rec[q, :q]) if q else np.zeros((1, NOUT), np.float32)
+            assert L.gtb_cluster_add(h, q, row.ctypes.data_as(fp)) == 0
+        pi = np.zeros(30, np.int32)
+        lam = np.zeros(30, np.float32)
+        member = np.zeros(30, np.int32)
+        offset = np.zeros(31, np.int32)
+        rep = np.zeros(30, np.int32)
+        ncl = ctypes.c_int()
+        assert L.gtb_cluster_finish(h, pi.ctypes.data_as(ip), lam.ctypes.data_as(fp),
+                                    member.ctypes.data_as(ip), offset.ctypes.data_as(ip),
+                                    rep.ctypes.data_as(ip), ctypes.byref(ncl)) == 0
+        L.gtb_cluster_destroy(h)
+        assert np.array_equal(pi, ref.pi) and np.array_equal(lam, ref.lam)
+        got = sorted((sorted(member[offset[c]:offset[c + 1]]) for c in range(ncl.value)))
+        assert got == sorted(sorted(x) for x in ref.clusters)
