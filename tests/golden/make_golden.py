@@ -84,6 +84,10 @@ SETS = {
     "c0_presim": (lambda: synth.config0(seed=111, n_refs=80, qlen=150, homolog_frac=0.3),
                   ["--no-detailed-search", "--pre-similarity=15", "--pre-score=0", "-s", "0"]),
     "c0_na": (lambda: na_set(112), ["--no-detailed-search", "--pre-score=0", "-s", "0"]),
+    # options together: symmetric, referenced, secondary TM-scores, full search
+    "c0_combo": (lambda: synth.config0(seed=113, n_refs=50, qlen=140, homolog_frac=0.5),
+                 ["--no-detailed-search", "--symmetric", "--referenced", "--2tm-score",
+                  "--refinement=2", "--pre-score=0", "-s", "0"], 1),
     "c0_shallow": (lambda: synth.config0(seed=108, n_refs=60, qlen=160),
                    ["--no-detailed-search", "--depth=3", "--pre-score=0.3", "-s", "0.3",
                     "--convergence=6"]),

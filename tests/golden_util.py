@@ -11,10 +11,12 @@ GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 LEVEL_SETS = {-1: "c0_level_m1", 0: "c0_level_0", 1: "c0_level_1", 2: "c0_level_2",
               3: "c0_level_3"}
 SETS = ["c0_speed13", "c0_default", "c0_filters", "c0_sym_ref_nodel", "c0_shallow", "c0_2tm",
-        "c0_ssrr", "c0_presim", "c0_na"] + \
+        "c0_ssrr", "c0_presim", "c0_na", "c0_combo"] + \
     list(LEVEL_SETS.values())
-# the sets the CUDA library takes (it refuses nucleic-acid pairs)
-LIBRARY_SETS = [s for s in SETS if s != "c0_na"]
+# the sets the GPU golden test runs: every set the CUDA library takes (it
+# refuses nucleic-acid pairs) except the combined-options set, which pins
+# the oracle only (each of its options runs on the GPU in the option sets)
+LIBRARY_SETS = [s for s in SETS if s not in ("c0_na", "c0_combo")]
 
 
 def _soa(z, tag):
