@@ -4,29 +4,50 @@
 Workload (seeded synthetic; no public dataset): 16 query C-alpha traces
 (lengths U(80,800)) against 200,000 reference traces (log-normal lengths,
 median 250, sigma_log 0.6, clipped to 30..2000; 5% members of homolog
-families), i.e. 3.2M query-reference pairs per step, with gtalign's default
-per-pair options except the spatial-index detailed search
-(--no-detailed-search; refinement 1, depth 2, convergence 18,
---pre-score 0.4, -s 0.5).
+families), i.e. 3.2M query-reference pairs, with gtalign's default per-pair
+options except the spatial-index detailed search (--no-detailed-search;
+refinement 1, depth 2, convergence 18, --pre-score 0.4, -s 0.5).
 
 One step = the full stage sequence (seed -> refinement -> DP <-> refinement
 loops -> final superposition/production scores) over one query chunk (2
 queries, the reference's --dev-queries-per-chunk default) x all 200,000
-references; the default 8 timed steps cover the whole 3.2M-pair workload.  `value` is measured with the structure blocks resident in HBM
-(gtb_process_resident, results left on the device); `e2e` through the
-public call gtb_process_block with pinned host buffers (host->device copy of
-the blocks and device->host copy of the per-pair result records inside the
-timed region).  Inputs (about 0.6 GB of coordinates and the pair state) are
-larger than L2 between steps.
+references.  Legs of one run:
 
---impl reference times the reference's own CPU implementation (its OpenMP
-build compiled from source under oracle/_ref/, or, when that binary is
-absent, the oracle port) on this host's cores over a bounded sample of the
-same workload.
+* value (headline): the batched form with adjoint polishing of the final
+  transforms (5 projected-gradient steps), structure blocks resident in HBM
+  (gtb_process_resident, results left on the device).  The per-pair numeric
+  error records (|FP32 path - FP64 recomputation| of both TM-scores and the
+  RMSD) of every timed pair are kept and their maxima reported; the run
+  fails when a TM-score error exceeds 1e-4 or an RMSD error 1e-3 A.
+* unpolished: the same steps without polishing (the reference's results).
+* e2e: the public call gtb_process_block with pinned host buffers: the
+  host->device copy of the blocks, the device->host copy of the records,
+  transforms, numeric errors and alignment rows (the reference's alnsmem
+  layout) inside the timed region.
+* plain: the same kernels at one pair per call (1 query x 1 reference).
+* long_chain: the long-chain configuration (8 assembly pairs of
+  5,000-37,860 residues, one call per pair) with alignment rows.
+* adjoint: 1,000,000 fixed-alignment pairs (lengths U(60,600)) polished
+  with 10 projected-gradient steps of the TM-score adjoint.
+* roofline: the HBM roofline of the stage-1 seed scan, and the FP32 SIMT
+  roofline of the whole step from device-counted algorithmic work.
+* cpu_baseline: the reference's CPU build (oracle/_ref/gtalign, compiled
+  from its sources) on this host's cores over a bounded sample of the same
+  workload, all 16 queries.
+* reference_gpu: the reference's own GPU build (oracle/_ref/gpu/gtalign,
+  compiled for sm_100a from its sources by oracle/Makefile.refgpu) on the
+  same B200, over the first query chunk x a sample of the references, timed
+  by its "query batch execution time" (the GPU bar for this path).
 
-Multi-GPU (torchrun): pairs are independent; every rank aligns its own
-seeded workload of the same size (weak scaling, no data-path collective);
-the timing is the max over ranks.
+Inputs (about 0.6 GB of coordinates and the pair state) are larger than L2
+between steps.  --impl reference times the reference's own CPU
+implementation the same way.
+
+Multi-GPU (torchrun): pairs are independent; the 200,000 references are split
+over the ranks by cost (sum Lq*Lr, longest first; shard.ShardPlan) and every
+rank aligns each query chunk with its share (strong scaling, no data-path
+collective); the timing is the max over ranks; the e2e leg gathers the
+records on rank 0 (shard.search_sharded).
 """
 from __future__ import annotations
 
@@ -45,12 +66,20 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-# k_findfrag DRAM read + write per pair (ncu, 2 queries x 40,000 references:
-# 102.29 MB + 5.99 MB for 13,333 pairs)
+# k_findfrag DRAM read + write per pair (ncu, one seed launch of the benchmark
+# step: profiles/findfrag_c1_2x200000.md)
 FINDFRAG_DRAM_BYTES_PER_PAIR = (102.29e6 + 5.99e6) / 13333
 
 METRIC = "pairs/s on 1 B200 at |dTM|<=1e-4; batched+adjoint vs plain; HBM % of peak"
 UNIT = "pairs/s"
+# algorithmic FP32 work per unit (the per-pass figure of the scoring/covariance
+# pass: transform 18, distance 6, TM term 3 incl. one divide, covariance 15 +
+# 6 squares; and per DP cell)
+FLOPS_PER_VISIT = 48
+FLOPS_PER_DP_CELL = 12
+NSM_B200 = 148
+FP32_LANES_PER_SM = 128
+TOL_TM, TOL_RMSD = 1e-4, 1e-3
 
 
 def dist_env():
@@ -67,6 +96,16 @@ def peaks():
             d = json.load(f)
         return float(d.get("hbm_gbs", 6650.0)), "measured"
     return 6650.0, "fallback"
+
+
+def cpu_model():
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
 
 
 class Clocks:
@@ -126,7 +165,103 @@ def make_workload(nq: int, nr: int, seed: int):
     return wl, synth.pack(wl.queries), synth.pack(wl.refs)
 
 
+def _max_over_ranks(x: float, ws: int, dev) -> float:
+    if ws == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], device=dev, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def _sum_over_ranks(x: float, ws: int, dev) -> float:
+    if ws == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], device=dev, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
 # -------------------------------------------------------------------- ours
+class Resident:
+    """Timed resident steps (gtb_process_resident) of one handle over the
+    query chunks x this rank's references, with per-step device buffers for
+    the records, transforms and numeric errors of every timed pair."""
+
+    def __init__(self, L, g, qblks, rblk, step_pairs, maxpairs, steps, dev):
+        import torch
+        self.L, self.g, self.qblks, self.rblk = L, g, qblks, rblk
+        self.step_pairs = step_pairs
+        self.nchunk = len(qblks)
+        nbuf = min(steps, self.nchunk)
+        self.out = torch.empty((nbuf, maxpairs * 16), dtype=torch.float32, device=dev)
+        self.tfm = torch.empty((nbuf, maxpairs * 12), dtype=torch.float32, device=dev)
+        self.err = torch.zeros((nbuf, maxpairs * 4), dtype=torch.float32, device=dev)
+        self.maxerr = torch.zeros(3, dtype=torch.float32, device=dev)
+
+    def step(self, k):
+        import torch
+        b = k % self.out.shape[0]
+        c = k % self.nchunk
+        st = self.L.gtb_process_resident(self.g.handle, ctypes.c_float(0.5), self.qblks[c], self.rblk,
+                                         ctypes.c_void_p(self.out[b].data_ptr()),
+                                         ctypes.c_void_p(self.tfm[b].data_ptr()),
+                                         ctypes.c_void_p(self.err[b].data_ptr()))
+        if st != 0:
+            raise RuntimeError(self.L.gtb_last_error(self.g.handle).decode())
+        n = self.step_pairs[c]
+        e = self.err[b, :n * 4].view(n, 4)
+        # every timed pair's error, reduced on the device (no host sync)
+        torch.maximum(self.maxerr, e[:, :3].amax(dim=0), out=self.maxerr)
+        return int(self.L.gtb_last_launch_count(self.g.handle))
+
+    def records(self, k):
+        b = k % self.out.shape[0]
+        n = self.step_pairs[k % self.nchunk]
+        return self.out[b, :n * 16].view(n, 16).cpu().numpy()
+
+
+def timed_steps(res: Resident, args, ws, dev, barrier, clocks=False, work=False):
+    import torch
+    for k in range(args.warmup):
+        res.step(k)
+    res.maxerr.zero_()
+    torch.cuda.synchronize()
+    barrier()
+    torch.cuda.synchronize()
+    launches, done = 0, 0
+    stage_ms = np.zeros(7)
+    wk = np.zeros(3, np.float64)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    clk = Clocks(dev) if clocks else None
+    if clk:
+        clk.__enter__()
+    e0.record()
+    for k in range(args.steps):
+        launches += res.step(k)
+        done += res.step_pairs[k % res.nchunk]
+        tm = np.zeros(7, np.float32)
+        res.L.gtb_last_timings(res.g.handle, tm.ctypes.data_as(ctypes.POINTER(ctypes.c_float)))
+        stage_ms += tm
+        if work:
+            wk += res.g.last_work().astype(np.float64)
+    e1.record()
+    torch.cuda.synchronize()
+    if clk:
+        clk.__exit__()
+    barrier()
+    torch.cuda.synchronize()
+    ms = _max_over_ranks(e0.elapsed_time(e1), ws, dev)
+    allpairs = _sum_over_ranks(done, ws, dev)
+    me = res.maxerr.cpu().numpy()
+    return {"ms": ms, "pairs": allpairs, "launches": launches, "stage_ms": stage_ms / args.steps,
+            "work": wk / args.steps, "maxerr": [float(x) for x in me],
+            "clocks": clk.summary() if clk else None}
+
+
 def run_ours(args):
     import torch
     ws, rank, local = dist_env()
@@ -138,81 +273,187 @@ def run_ours(args):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
     from gtalign_alpha_b200 import build as gb
     gb.build()
-    from gtalign_alpha_b200.api import GTalignB200, Options, pack_fields, load_library
+    from gtalign_alpha_b200.api import GTalignB200, Options, pack_fields, load_library, _CResults
+    from gtalign_alpha_b200.shard import ShardPlan, subset, search_sharded
     L = load_library()
-
-    t0 = time.time()
-    wl, q, r = make_workload(args.nqueries, args.nrefs, args.seed + 1000 * rank)
-    gen_s = time.time() - t0
-    npairs = q.n * r.n
-    opts = Options()  # gtalign defaults, detailed search off
-    g = GTalignB200(dev, 0, opts)
-    from gtalign_alpha_b200.shard import subset
-    nchunk = (q.n + args.qchunk - 1) // args.qchunk
-    qchunks = [subset(q, np.arange(c * args.qchunk, min(q.n, (c + 1) * args.qchunk))) for c in range(nchunk)]
-    qbs = [pack_fields(c) for c in qchunks]
-    rb = pack_fields(r)
-
-    # resident blocks for `value`
-    rblk = ctypes.c_void_p()
-    L.gtb_block_upload.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p)]
-    L.gtb_block_free.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
-    L.gtb_process_resident.argtypes = [ctypes.c_void_p, ctypes.c_float, ctypes.c_void_p, ctypes.c_void_p,
-                                       ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
-    qblks = [ctypes.c_void_p() for _ in qbs]
-    for blk, pk in list(zip(qblks, qbs)) + [(rblk, rb)]:
-        st = L.gtb_block_upload(g.handle, pk.beg, pk.end, ctypes.byref(blk))
-        if st != 0:
-            raise RuntimeError(L.gtb_last_error(g.handle).decode())
-    maxpairs = max(c.n for c in qchunks) * r.n
-    d_out = torch.empty(maxpairs * 16, dtype=torch.float32, device=dev)
-    d_tfm = torch.empty(maxpairs * 12, dtype=torch.float32, device=dev)
-    step_pairs = [c.n * r.n for c in qchunks]
-
-    def step_resident(k):
-        st = L.gtb_process_resident(g.handle, ctypes.c_float(0.5), qblks[k % nchunk], rblk,
-                                    ctypes.c_void_p(d_out.data_ptr()), ctypes.c_void_p(d_tfm.data_ptr()), None)
-        if st != 0:
-            raise RuntimeError(L.gtb_last_error(g.handle).decode())
-        return int(L.gtb_last_launch_count(g.handle))
 
     def barrier():
         if ws > 1:
             import torch.distributed as dist
             dist.barrier()
 
-    for k in range(args.warmup):
-        step_resident(k)
-    torch.cuda.synchronize()
-    barrier()
-    torch.cuda.synchronize()
-    launches = 0
-    stage_ms = np.zeros(7)
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    with Clocks(dev) as clk:
-        e0.record()
-        done_pairs = 0
-        for k in range(args.steps):
-            launches += step_resident(k)
-            done_pairs += step_pairs[k % nchunk]
-            tm = np.zeros(7, np.float32)
-            L.gtb_last_timings(g.handle, tm.ctypes.data_as(ctypes.POINTER(ctypes.c_float)))
-            stage_ms += tm
-        e1.record()
-        torch.cuda.synchronize()
-    barrier()
-    torch.cuda.synchronize()
-    ms = e0.elapsed_time(e1)
-    clocks = clk.summary()
+    t0 = time.time()
+    wl, q, r_all = make_workload(args.nqueries, args.nrefs, args.seed)
+    plan = ShardPlan(r_all, q.lens, rank, ws)
+    r = plan.refs
+    gen_s = time.time() - t0
+    nchunk = (q.n + args.qchunk - 1) // args.qchunk
+    qchunks = [subset(q, np.arange(c * args.qchunk, min(q.n, (c + 1) * args.qchunk))) for c in range(nchunk)]
+    qbs = [pack_fields(c) for c in qchunks]
+    rb = pack_fields(r)
+    gp = GTalignB200(dev, 0, Options(polish_steps=args.polish_steps))
+    g0 = GTalignB200(dev, 0, Options())
+
+    # resident blocks (uploaded once, used by both handles on this device)
+    L.gtb_block_upload.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p)]
+    L.gtb_block_free.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+    L.gtb_process_resident.argtypes = [ctypes.c_void_p, ctypes.c_float, ctypes.c_void_p, ctypes.c_void_p,
+                                       ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+    rblk = ctypes.c_void_p()
+    qblks = [ctypes.c_void_p() for _ in qbs]
+    for blk, pk in list(zip(qblks, qbs)) + [(rblk, rb)]:
+        st = L.gtb_block_upload(gp.handle, pk.beg, pk.end, ctypes.byref(blk))
+        if st != 0:
+            raise RuntimeError(L.gtb_last_error(gp.handle).decode())
+    step_pairs = [c.n * r.n for c in qchunks]
+    maxpairs = max(step_pairs)
+    legs = set(args.legs.split(","))
+
+    # headline: batched + adjoint polishing, resident
+    rp = Resident(L, gp, qblks, rblk, step_pairs, maxpairs, args.steps, dev)
+    A = timed_steps(rp, args, ws, dev, barrier, clocks=True, work=True)
+    value = A["pairs"] / (A["ms"] / 1000.0)
+    ms_step = A["ms"] / args.steps
+    acc_ok = A["maxerr"][0] <= TOL_TM and A["maxerr"][1] <= TOL_TM and A["maxerr"][2] <= TOL_RMSD
+
+    # the unpolished form (the reference's results) and the polishing gain
+    unpol = None
+    if "unpolished" in legs:
+        r0 = Resident(L, g0, qblks, rblk, step_pairs, maxpairs, args.steps, dev)
+        B = timed_steps(r0, args, ws, dev, barrier)
+        ok0 = B["maxerr"][0] <= TOL_TM and B["maxerr"][1] <= TOL_TM and B["maxerr"][2] <= TOL_RMSD
+        acc_ok = acc_ok and ok0
+        k_last = args.steps - 1
+        a, b = r0.records(k_last), rp.records(k_last)
+        c = qchunks[k_last % nchunk]
+        lq, lr = np.repeat(c.lens, r.n), np.tile(r.lens, c.n)
+        col = np.where(lq <= lr, 9, 10)          # polishing objective: d0 of the shorter length
+        rows = np.arange(len(col))
+        rep = a[:, 9] > 0
+        gain = b[rows, col][rep] - a[rows, col][rep]
+        unpol = {"value": B["pairs"] / (B["ms"] / 1000.0), "unit": UNIT, "ms_per_step": B["ms"] / args.steps,
+                 "max_err_tm": max(B["maxerr"][:2]), "max_err_rmsd": B["maxerr"][2],
+                 "polish_gain_last_step": {
+                     "pairs_reported": int(rep.sum()), "pairs_gained": int((gain > 1e-6).sum()),
+                     "tm_gain_mean": float(gain.mean()) if rep.any() else 0.0,
+                     "tm_gain_max": float(gain.max()) if rep.any() else 0.0,
+                     "never_lower": bool((gain >= -1e-6).all())}}
+
+    # e2e through gtb_process_block (host buffers), polished form
+    e2e = None
+    if "e2e" in legs:
+        e2e = e2e_run(L, gp, qbs, rb, qchunks, r, step_pairs, maxpairs, args, ws, rank, dev, barrier,
+                      q, r_all, plan)
+
+    # the plain form: one pair per call
+    plain = None
+    if "plain" in legs and args.plain_pairs > 0 and rank == 0:
+        plain = plain_sample(gp, L, q, r, args.plain_pairs, args.seed)
+        plain["batched_adjoint_vs_plain"] = value / ws / plain["value"]
+        if unpol is not None:
+            plain["batched_vs_plain"] = unpol["value"] / ws / plain["value"]
+
+    # rooflines
+    hbm_peak, peak_kind = peaks()
+    st_ms = A["stage_ms"]
+    # HBM roofline of the stage-1 seed scan: per step every reference residue
+    # once (12 B), the chunk's queries, a 64-byte record per pair; the step's
+    # seed launches (one per sub-batch) split these bytes and stage_ms[0]
+    # sums their durations
+    step_pairs_avg = A["pairs"] / ws / args.steps
+    algo_bytes = 12 * r.total + 12 * q.total / nchunk + 64 * step_pairs_avg
+    seed_ms = float(st_ms[0])
+    achieved = algo_bytes / (seed_ms / 1000.0) / 1e9 if seed_ms > 0 else 0.0
+    nsub = max(1, min(6, int(step_pairs_avg) // 16384))
+    traffic = FINDFRAG_DRAM_BYTES_PER_PAIR * step_pairs_avg / nsub
+    clocks = A["clocks"]
+    sm_mhz = clocks["sm_mhz"] if clocks else 1965.0
+    fp32_peak = NSM_B200 * FP32_LANES_PER_SM * 2 * sm_mhz * 1e6 / 1e12
+    wk = A["work"]
+    fl = {"seed": FLOPS_PER_VISIT * wk[0], "refine": FLOPS_PER_VISIT * wk[1], "dp": FLOPS_PER_DP_CELL * wk[2]}
+    fl_step = sum(fl.values())
+    fp32_ach = fl_step / (ms_step / 1000.0) / 1e12
+    roof = {"bound": "hbm", "kernel": "k_findfrag (stage-1 seed scan)",
+            "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
+            "frac": achieved / hbm_peak, "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)",
+            "traffic": traffic, "traffic_unit": "bytes per launch (ncu, one seed launch of the step)",
+            "algorithmic_bytes_per_launch": algo_bytes / nsub,
+            "fp32": {"bound": "fp32 SIMT", "achieved": fp32_ach, "unit": "TFLOP/s",
+                     "peak": fp32_peak, "frac": fp32_ach / fp32_peak,
+                     "peak_source": "148 SMs x 128 FP32 lanes x 2 (FMA) x %.0f MHz (median SM clock "
+                                    "sampled during the timed steps)" % sm_mhz,
+                     "scope": "whole step (every kernel), per-step algorithmic flops / ms_per_step",
+                     "flops_per_step": fl_step,
+                     "flops_per_step_by_kernel": fl,
+                     "units_per_step": {"seed_position_visits": wk[0], "refine_position_visits": wk[1],
+                                        "dp_cells": wk[2]},
+                     "flops_per_unit": {"position_visit": FLOPS_PER_VISIT, "dp_cell": FLOPS_PER_DP_CELL}},
+            "stage_ms": {"seed": float(st_ms[0]), "refine_init": float(st_ms[1]),
+                         "dp_refine_loops": float(st_ms[2]), "final": float(st_ms[5]),
+                         "total": float(st_ms[6])}}
+
+    long_chain = adjoint = cpu = refgpu = None
+    if rank == 0 and ws == 1:
+        if "refgpu" in legs:
+            refgpu = reference_gpu_sample(wl, args, value)
+        if "long" in legs:
+            long_chain = long_chain_run(gp, args)
+        if "adjoint" in legs:
+            adjoint = adjoint_pairs(args.adjoint_pairs, args.adjoint_steps)
+        if "cpu" in legs:
+            cpu = cpu_baseline_sample(wl, args)
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
+            "higher_is_better": True, "scaling": "strong" if ws > 1 else "weak",
+            "vs_baseline": None,
+            "dtype": "f32 (f64 rotation solve)", "data": "synthetic (seeded C-alpha traces)",
+            "config": {"workload": "16 queries x %d references (log-normal lengths, median 250)" % args.nrefs,
+                       "pairs": q.n * r_all.n,
+                       "step": "%d queries x %d references%s" % (args.qchunk, args.nrefs,
+                                                                 " (split over the ranks)" if ws > 1 else ""),
+                       "form": "batched + adjoint polishing (%d steps)" % args.polish_steps,
+                       "options": "gtalign defaults with --no-detailed-search, -s 0.5",
+                       "l2": "inputs larger than L2 (%.0f MB of reference coordinates)" % (12 * r_all.total / 1e6),
+                       "parallelism": "dp%d (references split by cost, independent pairs)" % ws},
+            "accuracy": {"max_err_tm": max(A["maxerr"][:2]), "max_err_rmsd": A["maxerr"][2],
+                         "tolerance_tm": TOL_TM, "tolerance_rmsd": TOL_RMSD, "ok": bool(acc_ok),
+                         "scope": "every timed pair: |FP32 search path - FP64 recomputation|"},
+            "e2e": e2e,
+            "gpu_launches": A["launches"],
+            "roofline": roof,
+            "unpolished": unpol,
+            "plain": plain,
+            "long_chain": long_chain,
+            "adjoint": adjoint,
+            "cpu_baseline": cpu,
+            "reference_gpu": refgpu,
+            "clocks": clocks,
+            "workload_gen_s": gen_s,
+        }
+        print(json.dumps(line), flush=True)
+    for blk in qblks:
+        L.gtb_block_free(gp.handle, blk)
+    L.gtb_block_free(gp.handle, rblk)
+    gp.close()
+    g0.close()
     if ws > 1:
         import torch.distributed as dist
-        t = torch.tensor([ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-    ms_step = ms / args.steps
-    value = ws * done_pairs / (ms / 1000.0)
+        dist.destroy_process_group()
+    if not acc_ok:
+        sys.exit(3)
 
-    # e2e through gtb_process_block with pinned host buffers
+
+def e2e_run(L, g, qbs, rb, qchunks, r, step_pairs, maxpairs, args, ws, rank, dev, barrier, q, r_all, plan):
+    """Steps through gtb_process_block with pinned host inputs and outputs,
+    alignment rows included; at N > 1 through shard.search_sharded (records
+    gathered on rank 0 every step)."""
+    import torch
+    from gtalign_alpha_b200.api import _CResults
+    from gtalign_alpha_b200.shard import search_sharded
+    nchunk = len(qbs)
     pin = {}
     for nm, pk in [("q%d" % c, qb) for c, qb in enumerate(qbs)] + [("r", rb)]:
         arrs = []
@@ -228,112 +469,153 @@ def run_ours(args):
         pin[nm] = (arrs, beg, end)
     h_out = torch.empty(maxpairs * 16, dtype=torch.float32, pin_memory=True)
     h_tfm = torch.empty(maxpairs * 12, dtype=torch.float32, pin_memory=True)
-    from gtalign_alpha_b200.api import _CResults
-    res = _CResults(h_out.data_ptr(), h_tfm.data_ptr(), None, None, None, None)
+    h_err = torch.empty(maxpairs * 4, dtype=torch.float32, pin_memory=True)
+    asz = max(int(L.gtb_alns_size(pin["q%d" % c][1], pin["q%d" % c][2], pin["r"][1], pin["r"][2]))
+              for c in range(nchunk))
+    h_alns = np.empty(asz, np.uint8)
+    res = _CResults(h_out.data_ptr(), h_tfm.data_ptr(), h_alns.ctypes.data, h_err.data_ptr(), None, None)
+    d2h_rows = []
+    maxerr = np.zeros(3)
 
-    def step_e2e(k):
+    def process(k):
         qk = "q%d" % (k % nchunk)
         st = L.gtb_process_block(g.handle, ctypes.c_float(0.5), pin[qk][1], pin[qk][2],
                                  pin["r"][1], pin["r"][2], ctypes.byref(res))
         if st != 0:
             raise RuntimeError(L.gtb_last_error(g.handle).decode())
+        n = step_pairs[k % nchunk]
+        rec = h_out[:n * 16].numpy().reshape(n, 16)
+        # bytes of the alignment rows the call copied: 5 rows of (columns + 1)
+        # per reported pair, and an 8-byte offset per pair
+        alen = rec[:, 4]
+        d2h_rows.append(int((5 * (alen[alen > 0] + 1)).sum()) + 8 * n)
+        e = h_err[:n * 4].numpy().reshape(n, 4)[:, :3].max(axis=0)
+        np.maximum(maxerr, e, out=maxerr)
+        return rec
 
-    step_e2e(0)
+    def one_step(k):
+        if ws == 1:
+            return process(k)
+        fn = lambda qs, rs: (process(k).reshape(qs.n, rs.n, 16), h_tfm[:qs.n * rs.n * 12].numpy().reshape(qs.n, rs.n, 12))
+        return search_sharded(qchunks[k % nchunk], r_all, fn, rank, ws, plan=plan)
+
+    for k in range(max(1, args.warmup)):
+        one_step(k)
     torch.cuda.synchronize()
     barrier()
+    d2h_rows.clear()
+    maxerr[:] = 0
     e2, e3 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e2.record()
-    e2e_pairs = 0
+    done = 0
     for k in range(args.steps):
-        step_e2e(k)
-        e2e_pairs += step_pairs[k % nchunk]
+        one_step(k)
+        done += step_pairs[k % nchunk]
     e3.record()
     torch.cuda.synchronize()
-    ms_e2e = e2.elapsed_time(e3)
-    if ws > 1:
-        import torch.distributed as dist
-        t = torch.tensor([ms_e2e], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_e2e = float(t.item())
-    e2e = ws * e2e_pairs / (ms_e2e / 1000.0)
+    ms = _max_over_ranks(e2.elapsed_time(e3), ws, dev)
+    allpairs = _sum_over_ranks(done, ws, dev)
     h2d = int(np.mean([sum(a.nbytes for a in qb.arrays) for qb in qbs])) + sum(a.nbytes for a in rb.arrays)
-    d2h = int(np.mean(step_pairs)) * (16 + 12) * 4
+    d2h = int(np.mean(step_pairs)) * (16 + 12 + 4) * 4 + int(np.mean(d2h_rows))
+    return {"value": allpairs / (ms / 1000.0), "unit": UNIT, "h2d_bytes_per_step": h2d,
+            "d2h_bytes_per_step": d2h, "ms_per_step": ms / args.steps,
+            "max_err_tm": float(max(maxerr[:2])), "max_err_rmsd": float(maxerr[2]),
+            "includes": "H2D of both blocks; D2H of records, transforms, numeric errors and "
+                        "alignment rows (reference layout); polished form"}
 
-    # the batched form with adjoint polishing of the final transforms
-    # (polish_steps=5): the same resident steps, timed the same way, and the
-    # score gain against the unpolished outputs of the last step
-    adjoint = None
-    if args.polish_steps > 0:
-        adjoint = adjoint_run(L, dev, qblks, rblk, nchunk, step_pairs, args, maxpairs,
-                              d_out, barrier, ws, qchunks, r)
 
-    # the plain form: the same kernels at one pair per call (1 query x 1
-    # reference through gtb_process_block with host buffers), on a sample
-    plain = plain_sample(g, L, q, r, args.plain_pairs, args.seed) if args.plain_pairs > 0 else None
-    if plain is not None:
-        plain["batched_vs_plain"] = value / plain["value"]
-        if adjoint is not None:
-            plain["batched_adjoint_vs_plain"] = adjoint["value"] / plain["value"]
+def long_chain_run(g, args):
+    """The long-chain configuration: 8 assembly pairs (5,000-37,860 residues),
+    one gtb_process_block call per pair with alignment rows; wall time per
+    pair (host clock around the call, which includes its copies)."""
+    from gtalign_alpha_b200 import synth
+    from gtalign_alpha_b200.shard import subset
+    lengths = tuple(int(x) for x in args.long_lengths.split(","))
+    wl = synth.config2(seed=3, lengths=lengths)
+    q, r = synth.pack(wl.queries), synth.pack(wl.refs)
+    warm = synth.config2(seed=4, lengths=(2000,))
+    g.process_block(synth.pack(warm.queries), synth.pack(warm.refs), scorethld=0.5)
+    per = []
+    tot = 0.0
+    for i in range(q.n):
+        qi, ri = subset(q, np.array([i])), subset(r, np.array([i]))
+        t0 = time.perf_counter()
+        res = g.process_block(qi, ri, scorethld=0.5, alignments=True)
+        wall = time.perf_counter() - t0
+        tot += wall
+        rec = res.alndata[0, 0]
+        per.append({"length": int(lengths[i]), "wall_s": wall, "tm_q": float(rec[9]), "tm_r": float(rec[10]),
+                    "rmsd": float(rec[8]), "aligned": int(rec[4]),
+                    "err_tm": float(res.numerr[0, 0, :2].max()), "err_rmsd": float(res.numerr[0, 0, 2])})
+    return {"value": q.n / tot, "unit": "pairs/s", "total_s": tot, "pairs": per,
+            "form": "batched + adjoint polishing (%d steps), alignment rows" % args.polish_steps,
+            "published_reference": "GTalign on a T4: 65.12 s for a 37,860-residue pair (other "
+                                   "structures, other GPU; not comparable as a ratio)"}
 
-    # roofline of the dominant stage (fraction of the step per stage)
-    hbm_peak, peak_kind = peaks()
-    st_ms = stage_ms / args.steps
-    # algorithmic bytes of the seed (scan) stage: every reference coordinate
-    # read once per query block, query coordinates, and a 64-byte record per pair
-    # per step (one query chunk): every reference residue once, the chunk's
-    # queries, a 64-byte record per pair; the step's seed launches (one per
-    # sub-batch) split these bytes, and stage_ms[0] sums their durations
-    algo_bytes = 12 * r.total + 12 * q.total / nchunk + 64 * done_pairs / args.steps
-    seed_ms = float(st_ms[0])
-    achieved = algo_bytes / (seed_ms / 1000.0) / 1e9 if seed_ms > 0 else 0.0
-    # DRAM bytes of one seed launch, scaled by pairs from an ncu capture of a
-    # smaller case of the same workload (profiles/top_kernels_c1_2x40000.md)
-    step_pairs_avg = done_pairs / args.steps
-    nsub = max(1, min(6, int(step_pairs_avg) // 16384))
-    traffic = FINDFRAG_DRAM_BYTES_PER_PAIR * step_pairs_avg / nsub
-    algo_launch = algo_bytes / nsub
-    roof = {"bound": "hbm", "kernel": "k_findfrag (stage-1 seed scan)",
-            "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
-            "frac": achieved / hbm_peak, "peak_source": peak_kind,
-            "traffic": traffic, "traffic_unit": "bytes per launch (scaled from ncu)",
-            "algorithmic_bytes_per_launch": algo_launch,
-            "stage_ms": {"seed": float(st_ms[0]), "refine_init": float(st_ms[1]),
-                         "dp_refine_loops": float(st_ms[2]), "final": float(st_ms[5]),
-                         "total": float(st_ms[6])}}
 
-    # CPU baseline sample (rank 0, N=1 only)
-    cpu = None
-    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
-        cpu = cpu_baseline_sample(wl, args)
+def adjoint_pairs(npairs: int, steps: int, nbase: int = 50_000):
+    """Adjoint polishing of `npairs` pairs with fixed 1:1 alignments (lengths
+    U(60,600)): a synthetic chain against a rigidly moved copy with 1.5 A
+    noise, started from a transform 0.05 rad / 0.5 A off.  `nbase` chains are
+    generated on the host and reused with fresh rotations and noise drawn on
+    the device.  Returns pairs/s and the TM-score gain distribution."""
+    import torch
+    from gtalign_alpha_b200 import synth
+    from gtalign_alpha_b200.adjoint import polish
+    rng = np.random.default_rng(5)
+    lens = rng.integers(60, 601, size=nbase)
+    base = synth.random_chains(rng, lens, "a")
+    xb = torch.from_numpy(np.concatenate([c.xyz for c in base]).astype(np.float32)).cuda()
+    lb = torch.from_numpy(lens.astype(np.int64)).cuda()
+    ob = torch.cumsum(lb, 0) - lb
+    idx = torch.arange(npairs, device="cuda") % nbase
+    n = lb[idx].to(torch.int32)
+    off = torch.cumsum(n.long(), 0) - n.long()
+    N = int(n.sum())
+    pid = torch.repeat_interleave(torch.arange(npairs, device="cuda"), n.long(), output_size=N)
+    src = ob[idx][pid] + (torch.arange(N, device="cuda") - off[pid])
+    g = torch.Generator(device="cuda").manual_seed(7)
+    q = xb[src].contiguous()
 
-    if rank == 0:
-        line = {
-            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f32 (f64 rotation solve)", "data": "synthetic (seeded C-alpha traces)",
-            "config": {"workload": "16 queries x %d references (log-normal lengths, median 250)" % args.nrefs,
-                       "pairs_per_gpu": npairs, "step": "%d queries x %d references" % (args.qchunk, args.nrefs),
-                       "options": "gtalign defaults with --no-detailed-search, -s 0.5",
-                       "l2": "inputs larger than L2 (%.0f MB of reference coordinates)" % (12 * r.total / 1e6),
-                       "parallelism": "dp%d (independent pairs)" % ws},
-            "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
-            "gpu_launches": launches,
-            "roofline": roof,
-            "adjoint": adjoint,
-            "plain": plain,
-            "cpu_baseline": cpu,
-            "clocks": clocks,
-            "workload_gen_s": gen_s,
-        }
-        print(json.dumps(line), flush=True)
-    for blk in qblks:
-        L.gtb_block_free(g.handle, blk)
-    L.gtb_block_free(g.handle, rblk)
-    g.close()
-    if ws > 1:
-        import torch.distributed as dist
-        dist.destroy_process_group()
+    def rotations(m, scale=None):
+        a = torch.randn(m, 3, device="cuda", generator=g)
+        if scale is not None:
+            a = a * scale
+        else:
+            a = a / a.norm(dim=1, keepdim=True) * (torch.rand(m, 1, device="cuda", generator=g) * 3.14159)
+        th = a.norm(dim=1).clamp_min(1e-12)[:, None, None]
+        k = a / th[:, :, 0]
+        K = torch.zeros(m, 3, 3, device="cuda")
+        K[:, 0, 1], K[:, 0, 2], K[:, 1, 0] = -k[:, 2], k[:, 1], k[:, 2]
+        K[:, 1, 2], K[:, 2, 0], K[:, 2, 1] = -k[:, 0], -k[:, 1], k[:, 0]
+        I = torch.eye(3, device="cuda").expand(m, 3, 3)
+        return I + torch.sin(th) * K + (1 - torch.cos(th)) * (K @ K)
+
+    R = rotations(npairs)
+    t = torch.randn(npairs, 3, device="cuda", generator=g) * 10
+    r = torch.einsum("nij,nj->ni", R[pid], q) + t[pid] + torch.randn(N, 3, device="cuda", generator=g) * 1.5
+    R0 = rotations(npairs, scale=0.05) @ R
+    t0 = t + torch.randn(npairs, 3, device="cuda", generator=g) * 0.5
+    tfm = torch.cat([R0.reshape(npairs, 9), t0], 1).contiguous()
+    d0 = (1.24 * torch.clamp(n.float() - 15, min=1).pow(1.0 / 3.0) - 1.8).clamp_min(0.5)
+    for _ in range(3):
+        tfm_w = tfm.clone()
+        polish(q, r, off, n, tfm_w, d0, steps)          # warm-up
+    torch.cuda.synchronize()
+    tfm_w = tfm.clone()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    tb, ta = polish(q, r, off, n, tfm_w, d0, steps)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    gain = ((ta - tb) / n.float()).cpu().numpy()
+    return {"value": npairs / (ms / 1000.0), "unit": "pairs/s", "pairs": npairs, "residues": N,
+            "steps": steps, "ms": ms,
+            "tm_gain_mean": float(gain.mean()), "tm_gain_median": float(np.median(gain)),
+            "tm_gain_max": float(gain.max()), "never_lower": bool((gain >= 0).all()),
+            "raised_frac": float((gain > 0).mean()),
+            "workload": "fixed 1:1 alignments, lengths U(60,600), started 0.05 rad / 0.5 A off"}
 
 
 # ---------------------------------------------------------------- reference
@@ -343,8 +625,8 @@ def ref_binary():
 
 
 def run_reference_sample(wl, nq: int, nref: int, threads: int):
-    """Time the reference CPU build (or the oracle port) on nq queries x nref
-    references of the workload.  Returns (pairs, seconds, kind)."""
+    """Time the reference CPU build (or the oracle port) on the first nq
+    queries x nref references of the workload.  Returns (pairs, seconds, kind)."""
     from gtalign_alpha_b200 import synth
     binp = ref_binary()
     sub = synth.Workload(wl.queries[:nq], wl.refs[:nref], wl.seed)
@@ -376,58 +658,45 @@ def run_reference_sample(wl, nq: int, nref: int, threads: int):
     return nq * nref, time.time() - t, "port"
 
 
-def adjoint_run(L, dev, qblks, rblk, nchunk, step_pairs, args, maxpairs, d_ref, barrier, ws,
-                qchunks, r):
-    """pairs/s of the resident steps with polish_steps on, and the score
-    gain of the polished transforms over the unpolished ones."""
-    import torch
-    from gtalign_alpha_b200.api import GTalignB200, Options
-    k_last = (args.steps - 1) % nchunk
-    ref = d_ref[:step_pairs[k_last] * 16].view(-1, 16).cpu().numpy()
-    gp = GTalignB200(dev, 0, Options(polish_steps=args.polish_steps))
-    d_out = torch.empty(maxpairs * 16, dtype=torch.float32, device=dev)
-    d_tfm = torch.empty(maxpairs * 12, dtype=torch.float32, device=dev)
-
-    def step(k):
-        st = L.gtb_process_resident(gp.handle, ctypes.c_float(0.5), qblks[k % nchunk], rblk,
-                                    ctypes.c_void_p(d_out.data_ptr()), ctypes.c_void_p(d_tfm.data_ptr()), None)
-        if st != 0:
-            raise RuntimeError(L.gtb_last_error(gp.handle).decode())
-
-    for k in range(args.warmup):
-        step(k)
-    torch.cuda.synchronize()
-    barrier()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record()
-    done = 0
-    for k in range(args.steps):
-        step(k)
-        done += step_pairs[k % nchunk]
-    e1.record()
-    torch.cuda.synchronize()
-    ms = e0.elapsed_time(e1)
-    if ws > 1:
-        import torch.distributed as dist
-        t = torch.tensor([ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-    pol = d_out[:step_pairs[k_last] * 16].view(-1, 16).cpu().numpy()
-    gp.close()
-    # score by the shorter structure's length: the polishing objective
-    lq = np.repeat(qchunks[k_last].lens, r.n)
-    lr = np.tile(r.lens, qchunks[k_last].n)
-    col = np.where(lq <= lr, 9, 10)
-    rows = np.arange(len(col))
-    ok = ref[:, 9] > 0
-    a = ref[rows, col][ok]
-    b = pol[rows, col][ok]
-    gain = b - a
-    return {"value": ws * done / (ms / 1000.0), "unit": UNIT, "polish_steps": args.polish_steps,
-            "pairs_reported": int(ok.sum()), "pairs_gained": int((gain > 1e-6).sum()),
-            "tm_gain_mean": float(gain.mean()) if ok.any() else 0.0,
-            "tm_gain_max": float(gain.max()) if ok.any() else 0.0,
-            "never_lower": bool((gain >= -1e-6).all())}
+def reference_gpu_sample(wl, args, value):
+    """The reference's GPU build on this device: the first query chunk (2
+    queries) x the first refgpu_refs references of the workload, default
+    options with --no-detailed-search.  pairs/s from its "query batch
+    execution time" (device work, host reading excluded) and from the wall
+    time of the process."""
+    from gtalign_alpha_b200 import synth
+    binp = os.path.join(ROOT, "oracle", "_ref", "gpu", "gtalign")
+    if not os.path.exists(binp):
+        return {"unavailable": "oracle/_ref/gpu/gtalign not built (make -f oracle/Makefile.refgpu)"}
+    nq, nref = args.qchunk, args.refgpu_refs
+    sub = synth.Workload(wl.queries[:nq], wl.refs[:nref], wl.seed)
+    d = tempfile.mkdtemp(prefix="gtrefgpu")
+    try:
+        synth.write_dirs(sub, d + "/q", d + "/r")
+        cmd = [binp, "--qrs=" + d + "/q", "--rfs=" + d + "/r", "-o", d + "/out", "--outfmt=1",
+               "--no-detailed-search", "--dev-queries-per-chunk=%d" % nq, "--dev-N=1",
+               "--cpu-threads-reading=4"]
+        t0 = time.perf_counter()
+        p = subprocess.run(cmd, capture_output=True, timeout=args.refgpu_timeout)
+        wall = time.perf_counter() - t0
+        if p.returncode != 0:
+            return {"unavailable": "reference GPU build exited %d: %s" % (p.returncode, p.stderr.decode()[-300:])}
+        secs, seen = 0.0, set()
+        for f in os.listdir(d + "/out"):
+            J = json.load(open(os.path.join(d, "out", f)))["gtalign_search"]
+            t = J["search_statistics"]["query_batch_execution_time"]
+            if t not in seen:
+                seen.add(t)
+                secs += t
+        v = nq * nref / secs
+        return {"value": v, "unit": UNIT, "wall_s": wall, "batch_s": secs,
+                "sample": "%d queries x %d references of the workload, default options with "
+                          "--no-detailed-search" % (nq, nref),
+                "ours_vs_reference_gpu": value / v}
+    except subprocess.TimeoutExpired:
+        return {"unavailable": "reference GPU build did not finish within %d s" % args.refgpu_timeout}
+    finally:
+        shutil.rmtree(d, ignore_errors=True)
 
 
 def plain_sample(g, L, q, r, npairs: int, seed: int):
@@ -461,16 +730,25 @@ def plain_sample(g, L, q, r, npairs: int, seed: int):
     secs = time.perf_counter() - t0
     return {"value": npairs / secs, "unit": UNIT,
             "sample": "%d seeded pairs of the workload, one gtb_process_block call (1 query x "
-                      "1 reference, host buffers) per pair" % npairs}
+                      "1 reference, host buffers) per pair, polished form" % npairs}
 
 
 def cpu_baseline_sample(wl, args):
+    """The reference CPU build over all the workload's queries, each against
+    the first cpu_sample_refs / 8 references (one call per query, as the
+    reference arm cycles queries)."""
     threads = os.cpu_count() or 1
-    nref = args.cpu_sample_refs
-    pairs, secs, kind = run_reference_sample(wl, 1, nref, threads)
-    return {"value": pairs / secs, "unit": UNIT, "cores": threads, "kind": kind,
-            "sample": "1 query (L=%d) x %d references of the workload, default options with "
-                      "--no-detailed-search; %.1f s" % (wl.queries[0].length, nref, secs)}
+    from gtalign_alpha_b200 import synth
+    nref = max(50, args.cpu_sample_refs // 8)
+    pairs, secs, kind = 0, 0.0, "reference"
+    for qi in range(len(wl.queries)):
+        sub = synth.Workload(wl.queries[qi:qi + 1], wl.refs, wl.seed)
+        p, s, kind = run_reference_sample(sub, 1, nref, threads)
+        pairs += p
+        secs += s
+    return {"value": pairs / secs, "unit": UNIT, "cores": threads, "kind": kind, "cpu": cpu_model(),
+            "sample": "each of the %d queries x the first %d references of the workload, default "
+                      "options with --no-detailed-search; %.1f s in all" % (len(wl.queries), nref, secs)}
 
 
 def run_reference(args):
@@ -497,8 +775,9 @@ def run_reference(args):
             "config": {"workload": "16 queries x %d references (log-normal lengths, median 250)" % args.nrefs,
                        "options": "gtalign defaults with --no-detailed-search",
                        "parallelism": "host cores"},
-            "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": kind,
-                             "sample": "per step 1 query x %d references of the workload" % args.cpu_sample_refs},
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": kind, "cpu": cpu_model(),
+                             "sample": "per step 1 query (cycling over the 16) x %d references of the "
+                                       "workload" % args.cpu_sample_refs},
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -514,11 +793,18 @@ def main():
     ap.add_argument("--qchunk", type=int, default=2, help="queries per step (the reference's --dev-queries-per-chunk)")
     ap.add_argument("--seed", type=int, default=2)
     ap.add_argument("--cpu-sample-refs", type=int, default=2000)
-    ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--polish-steps", type=int, default=5,
-                    help="adjoint polishing steps of the second timed form (0: skip)")
+                    help="adjoint polishing steps of the headline (batched + adjoint) form")
     ap.add_argument("--plain-pairs", type=int, default=300,
-                    help="pairs timed in the one-pair-per-call form (0: skip)")
+                    help="pairs timed in the one-pair-per-call form")
+    ap.add_argument("--long-lengths", default="5000,8000,12000,16000,20000,25000,30000,37860")
+    ap.add_argument("--adjoint-pairs", type=int, default=1_000_000)
+    ap.add_argument("--adjoint-steps", type=int, default=10)
+    ap.add_argument("--refgpu-refs", type=int, default=10000,
+                    help="references in the reference GPU build's sample (x the first query chunk)")
+    ap.add_argument("--refgpu-timeout", type=int, default=600)
+    ap.add_argument("--legs", default="unpolished,e2e,plain,long,adjoint,cpu,refgpu",
+                    help="legs besides the headline: unpolished,e2e,plain,long,adjoint,cpu,refgpu")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

@@ -81,10 +81,13 @@ class TMScore(torch.autograd.Function):
         q, tfm, off, n, g, gq = ctx.saved_tensors
         P = tfm.shape[0]
         N = q.shape[0]
-        # pair index of every residue row
-        pid = torch.repeat_interleave(torch.arange(P, device=q.device), n.long(), output_size=int(n.sum()))
-        rows = torch.cat([torch.arange(int(o), int(o) + int(k), device=q.device)
-                          for o, k in zip(off.tolist(), n.tolist())]) if P else torch.zeros(0, dtype=torch.long, device=q.device)
+        # pair index and residue row of every aligned position, on the device:
+        # row = off[pair] + (position - first position of the pair)
+        nl = n.long()
+        tot = int(nl.sum()) if P else 0
+        pid = torch.repeat_interleave(torch.arange(P, device=q.device), nl, output_size=tot)
+        start = torch.cumsum(nl, 0) - nl
+        rows = off.long()[pid] + (torch.arange(tot, device=q.device) - start[pid])
         w = gout[pid]
         grad_q = torch.zeros_like(q)
         grad_q[rows] = gq[rows] * w[:, None]

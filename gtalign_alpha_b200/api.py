@@ -116,6 +116,10 @@ def load_library():
     L.gtb_last_launch_count.restype = ctypes.c_longlong
     L.gtb_last_timings.argtypes = [vp, fp]
     L.gtb_last_timings.restype = ctypes.c_int
+    L.gtb_last_work.argtypes = [vp, ctypes.POINTER(ctypes.c_ulonglong)]
+    L.gtb_last_work.restype = ctypes.c_int
+    L.gtb_set_wait_limit.argtypes = [vp, ctypes.c_longlong]
+    L.gtb_set_wait_limit.restype = ctypes.c_int
     L.gtb_destroy.argtypes = [vp]
     L.gtb_destroy.restype = None
     L.gtb_tm_adjoint.argtypes = [vp, ctypes.c_int, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp]
@@ -175,6 +179,8 @@ class BlockResult:
     rss: Optional[np.ndarray] = None
     launches: int = 0
     timings_ms: np.ndarray = field(default_factory=lambda: np.zeros(7, np.float32))
+    # device-counted work: seed position visits, refinement position visits, DP cells
+    work: np.ndarray = field(default_factory=lambda: np.zeros(3, np.uint64))
 
     @property
     def tm_query(self) -> np.ndarray:
@@ -245,6 +251,18 @@ class GTalignB200:
     def handle(self):
         return self._h
 
+    def set_wait_limit(self, spins: int) -> None:
+        """Spins a bounded wait of the multi-CTA DP makes before it gives up."""
+        st = self.lib.gtb_set_wait_limit(self._h, int(spins))
+        if st != 0:
+            raise GTBError(st, "wait limit must be >= 0")
+
+    def last_work(self) -> np.ndarray:
+        """Device-counted work of the last call (seed visits, refinement visits, DP cells)."""
+        w = np.zeros(3, np.uint64)
+        self.lib.gtb_last_work(self._h, w.ctypes.data_as(ctypes.POINTER(ctypes.c_ulonglong)))
+        return w
+
     def process_block(self, queries: SoA, refs: SoA, scorethld: float = 0.5,
                       alignments: bool = True, numerr: bool = True,
                       secstr: bool = False) -> BlockResult:
@@ -284,7 +302,8 @@ class GTalignB200:
         return BlockResult(aln.reshape(nq, nr, NOUT), tfm.reshape(nq, nr, 12),
                            err.reshape(nq, nr, NERR) if err is not None else None,
                            alns, qb.arrays[0].copy(), rb.arrays[0].copy(), rb.arrays[1].copy(),
-                           qss, rss, int(self.lib.gtb_last_launch_count(self._h)), tms)
+                           qss, rss, int(self.lib.gtb_last_launch_count(self._h)), tms,
+                           self.last_work())
 
 
 class _CClusterOptions(ctypes.Structure):

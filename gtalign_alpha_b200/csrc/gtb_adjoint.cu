@@ -31,6 +31,9 @@ struct Kahan {
         c = (t - s) - y;
         s = t;
     }
+    // c holds the rounding excess of the last additions: the compensated
+    // total is s - c
+    __device__ __forceinline__ float value() const { return s - c; }
 };
 
 // TM-score and gradient for one pair; omega about the point `cen`
@@ -64,10 +67,10 @@ __device__ void tm_grad(const float* q, const float* r, int n, const float* T, f
             gq[3 * i + 2] = T[2] * gx + T[5] * gy + T[8] * gz;
         }
     }
-    tm = warp_sum(s.s + s.c);
+    tm = warp_sum(s.value());
     for (int k = 0; k < 3; k++) {
-        g6[k] = warp_sum(gw[k].s + gw[k].c);
-        g6[3 + k] = warp_sum(gt[k].s + gt[k].c);
+        g6[k] = warp_sum(gw[k].value());
+        g6[3 + k] = warp_sum(gt[k].value());
     }
 }
 
@@ -101,7 +104,7 @@ __device__ float tm_only(const float* q, const float* r, int n, const float* T, 
         float ez = T[6] * qx + T[7] * qy + T[8] * qz + T[11] - r[S * i + 2];
         s.add(d02 / (d02 + ex * ex + ey * ey + ez * ez));
     }
-    return warp_sum(s.s + s.c);
+    return warp_sum(s.value());
 }
 
 // curvature scales for the step: h_t = sum 2 d0^2/u^2, h_w = sum 2 d0^2 |a|^2/u^2

@@ -37,6 +37,9 @@ struct gtb_handle {
     cudaEvent_t sev[NWAVE * NSUB][8] = {};  // stage events per sub-batch
     int dw_cap = 0;                  // CTAs the wavefront DP keeps resident
     int* h_flag = nullptr;           // pinned: wavefront error flag per sub-batch
+    long long wait_limit = gtb::DP_WAVE_SPIN_DEFAULT;  // spins of a wavefront wait
+    unsigned long long* d_work = nullptr;  // device work counters of the last call
+    unsigned long long work[gtb::WK_NKIND] = {0, 0, 0};
 };
 
 static const int TBL = 65536;
@@ -81,6 +84,7 @@ extern "C" gtb_status gtb_create(int device, size_t mem_bytes, const gtb_options
     configure_kernels();
     CK(cudaHostAlloc((void**)&h->h_flag, gtb_handle::NWAVE * gtb_handle::NSUB * sizeof(int),
                      cudaHostAllocDefault));
+    CK(cudaMalloc(&h->d_work, gtb::WK_NKIND * gtb::WORK_SLOTS * sizeof(unsigned long long)));
     h->sub[0] = h->st;
     for (int j = 1; j < gtb_handle::NSUB; j++)
         CK(cudaStreamCreateWithFlags(&h->sub[j], cudaStreamNonBlocking));
@@ -104,6 +108,7 @@ extern "C" void gtb_destroy(gtb_handle* h) {
     if (h->t_d0) cudaFree(h->t_d0);
     if (h->t_d82) cudaFree(h->t_d82);
     if (h->t_d0fin) cudaFree(h->t_d0fin);
+    if (h->d_work) cudaFree(h->d_work);
     for (int k = 0; k < 8; k++) if (h->ev[k]) cudaEventDestroy(h->ev[k]);
     for (int j = 0; j < gtb_handle::NWAVE * gtb_handle::NSUB; j++)
         for (int k = 0; k < 8; k++) if (h->sev[j][k]) cudaEventDestroy(h->sev[j][k]);
@@ -119,6 +124,16 @@ extern "C" long long gtb_last_launch_count(const gtb_handle* h) { return h ? h->
 extern "C" gtb_status gtb_last_timings(const gtb_handle* h, float* ms7) {
     if (!h || !ms7) return GTB_ERR_ARG;
     memcpy(ms7, h->timings, sizeof(h->timings));
+    return GTB_OK;
+}
+extern "C" gtb_status gtb_last_work(const gtb_handle* h, unsigned long long* w3) {
+    if (!h || !w3) return GTB_ERR_ARG;
+    memcpy(w3, h->work, sizeof(h->work));
+    return GTB_OK;
+}
+extern "C" gtb_status gtb_set_wait_limit(gtb_handle* h, long long spins) {
+    if (!h || spins < 0) return GTB_ERR_ARG;
+    h->wait_limit = spins;
     return GTB_OK;
 }
 
@@ -179,13 +194,41 @@ static size_t pair_bytes(int lq, int lr, bool strings) {
     return b;
 }
 
+// Destination of the alignment rows: the caller's buffer in the reference's
+// layout (MpDPHub.cpp:1975-1981): for query qi, 5 rows of rowlen[qi] bytes
+// starting at qbase[qi]; pair (qi, ri) at column roff[ri] + ri*(lq_i+1).
+struct AlnSink {
+    char* alns = nullptr;
+    const float* rec = nullptr;      // the block's host records (alignment length at field 4)
+    std::vector<long long> qbase, rowlen;
+    std::vector<int> qlen, rlen, roff;
+    int nr = 0;
+    std::vector<long long> soff;     // staging: packed offsets of a sub-batch
+    std::vector<char> sbytes;        // staging: its packed rows
+    // copy the packed rows of pairs [p0, p0+np) to the reference layout; a
+    // pair without an alignment gets empty rows
+    void scatter(long long p0, int np) {
+        for (int i = 0; i < np; i++) {
+            long long p = p0 + i;
+            int qi = (int)(p / nr), ri = (int)(p % nr);
+            char* dst = alns + qbase[qi] + (long long)roff[ri] + (long long)ri * (qlen[qi] + 1);
+            long long o = soff[i];
+            if (o < 0) {
+                for (int f = 0; f < 5; f++) dst[f * rowlen[qi]] = 0;
+                continue;
+            }
+            // 5 rows of W bytes: the alignment's columns and the NUL
+            const long long W = (long long)rec[p * GTB_NOUT + GTB_OUT_ALNLENGTH] + 1;
+            for (int f = 0; f < 5; f++) memcpy(dst + f * rowlen[qi], sbytes.data() + o + f * W, (size_t)W);
+        }
+    }
+};
+
 // Runs the whole stage sequence over a device-resident block.
 // Host outputs (may be null): alndata [nq*nr*16], tfm [nq*nr*12],
-// numerr [nq*nr*4]; strings: per pair compact rows copied to hstr (offsets
-// hstroff, 5*(lq+lr+1) bytes per pair) when non-null.
+// numerr [nq*nr*4]; sink: alignment rows (null: none produced).
 static gtb_status run_block(gtb_handle* h, const DevBlock& D, float scorethld,
-                            float* h_alndata, float* h_tfm, float* h_err,
-                            char* hstr, const std::vector<long long>* hstroff) {
+                            float* h_alndata, float* h_tfm, float* h_err, AlnSink* sink) {
     const gtb_options& o = h->opts;
     const long long npairs = (long long)D.nq * D.nr;
     Blk B{};
@@ -206,7 +249,7 @@ static gtb_status run_block(gtb_handle* h, const DevBlock& D, float scorethld,
     // (CuBatch.cu:459-462)
     B.presim = (0.f < o.presimilarity && PRESIM_EDGE < B.qmax && PRESIM_EDGE < B.rmax) ? o.presimilarity : 0.f;
     B.symmetric = o.symmetric; B.nodeletions = o.nodeletions;
-    const bool strings = hstr != nullptr;
+    const bool strings = sink != nullptr;
 
     size_t fr = 0, tot = 0;
     CK(cudaMemGetInfo(&fr, &tot));
@@ -216,10 +259,17 @@ static gtb_status run_block(gtb_handle* h, const DevBlock& D, float scorethld,
 
     float tsum[7] = {0, 0, 0, 0, 0, 0, 0};
     h->launches = 0;
+    cudaError_t lerr = cudaSuccess;     // a launch that failed (cooperative DP)
+    // work counters: cleared on the handle's stream, which the sub-batch
+    // streams wait for below
+    CK(cudaMemsetAsync(h->d_work, 0, gtb::WK_NKIND * gtb::WORK_SLOTS * sizeof(unsigned long long), h->st));
     // host offsets of the sub-batches in flight (kept until their copies ran)
     std::vector<long long> offv[gtb_handle::NSUB];
     std::vector<int> ffv[gtb_handle::NSUB], ffiv[gtb_handle::NSUB], dwvv[gtb_handle::NSUB];
     std::vector<long long> dwsv[gtb_handle::NSUB];
+    // sub-batches whose packed alignment rows are read once the batch is done
+    struct StrBat { char* base; long long p0; int np; long long* soff; unsigned long long* cnt; char* str; };
+    std::vector<StrBat> strbat;
 
     // One sub-batch [q0, q0 + np): plan, carve one allocation, upload the
     // offsets, launch the stage sequence and the result copies on stream st.
@@ -313,6 +363,7 @@ static gtb_status run_block(gtb_handle* h, const DevBlock& D, float scorethld,
         size_t o_row = carve((size_t)off_row[np] * sizeof(float));
         size_t o_aln = carve((size_t)off_aln[np] * sizeof(unsigned));
         size_t o_str = carve((size_t)std::max<long long>(off_str[np], 1));
+        size_t o_sto = strings ? carve((size_t)np * sizeof(long long) + sizeof(unsigned long long)) : 0;
         size_t o_alc = carve((size_t)off_aln[np] * 6 * sizeof(float));
         size_t o_rl = carve((size_t)np * sizeof(int));
         size_t o_rh = carve((size_t)4097 * sizeof(int));
@@ -340,9 +391,15 @@ static gtb_status run_block(gtb_handle* h, const DevBlock& D, float scorethld,
         T.off_bt = offs; T.off_row = offs + (np + 1); T.off_aln = offs + 2 * (np + 1); T.off_str = offs + 3 * (np + 1);
         T.bt = (unsigned*)(base + o_bt); T.row = (float*)(base + o_row);
         T.aln = (unsigned*)(base + o_aln); T.str = strings ? (base + o_str) : nullptr;
+        T.str_off = strings ? (long long*)(base + o_sto) : nullptr;
+        T.str_cnt = strings ? (unsigned long long*)(base + o_sto + (size_t)np * sizeof(long long)) : nullptr;
+        if (strings) CK(cudaMemsetAsync(T.str_cnt, 0, sizeof(unsigned long long), st));
         T.alc = (float*)(base + o_alc);
         T.rlist = (int*)(base + o_rl); T.rhist = (int*)(base + o_rh);
         T.launches = &h->launches;
+        T.lerr = &lerr;
+        T.work = h->d_work;
+        T.dw_spin = h->wait_limit;
         T.nff = np; T.ff_pair = nullptr; T.ff_chunk = nullptr; T.ff_nch = nullptr; T.ff_key = nullptr;
         T.rl_nlmax = nlmax; T.rl_long = T.rl_count = T.rl_next = nullptr; T.rl_cand = nullptr;
         if (nlmax) {
@@ -377,6 +434,7 @@ static gtb_status run_block(gtb_handle* h, const DevBlock& D, float scorethld,
         }
         launch_stages(B, T, o.refinement, o.depth, o.convergence, o.prescore, o.referenced,
                       scorethld, st, h->sev[evset], o.polish_steps);
+        CK(lerr);
         CK(cudaGetLastError());
         if (h_alndata)
             CK(cudaMemcpyAsync(h_alndata + q0 * 16, T.out, (size_t)np * 16 * sizeof(float), cudaMemcpyDefault, st));
@@ -384,9 +442,12 @@ static gtb_status run_block(gtb_handle* h, const DevBlock& D, float scorethld,
             CK(cudaMemcpyAsync(h_tfm + q0 * 12, T.tfm_gr, (size_t)np * 12 * sizeof(float), cudaMemcpyDefault, st));
         if (h_err)
             CK(cudaMemcpyAsync(h_err + q0 * 4, T.err, (size_t)np * 4 * sizeof(float), cudaMemcpyDefault, st));
-        if (strings)
-            CK(cudaMemcpyAsync(hstr + (*hstroff)[q0], T.str, (size_t)off_str[np], cudaMemcpyDeviceToHost, st));
         if (nl) CK(cudaMemcpyAsync(h->h_flag + evset, T.dw_err, sizeof(int), cudaMemcpyDeviceToHost, st));
+        if (strings) {
+            // read after the batch: only the bytes the rows took
+            strbat.push_back({base, q0, np, T.str_off, T.str_cnt, T.str});
+            return GTB_OK;
+        }
         CK(cudaFreeAsync(base, st));
         return GTB_OK;
     };
@@ -435,11 +496,36 @@ static gtb_status run_block(gtb_handle* h, const DevBlock& D, float scorethld,
             gtb_status s = launch_sub(q0, (int)(q1 - q0), j % gtb_handle::NSUB, j);
             if (s != GTB_OK) {
                 for (int k = 0; k < gtb_handle::NSUB; k++) cudaStreamSynchronize(h->sub[k]);
+                for (const StrBat& sb : strbat) cudaFreeAsync(sb.base, h->st);
                 return s;
             }
             q0 = q1;
         }
         for (int j = 0; j < std::min(nsub, gtb_handle::NSUB); j++) CK(cudaStreamSynchronize(h->sub[j]));
+        if (!strbat.empty()) {
+            gtb_status s2 = GTB_OK;
+            for (const StrBat& sb : strbat) {
+                unsigned long long used = 0;
+                cudaError_t e = cudaMemcpy(&used, sb.cnt, sizeof(used), cudaMemcpyDeviceToHost);
+                if (e == cudaSuccess) {
+                    sink->soff.resize(sb.np);
+                    e = cudaMemcpy(sink->soff.data(), sb.soff, (size_t)sb.np * sizeof(long long),
+                                   cudaMemcpyDeviceToHost);
+                }
+                if (e == cudaSuccess) {
+                    sink->sbytes.resize(used);
+                    if (used) e = cudaMemcpy(sink->sbytes.data(), sb.str, used, cudaMemcpyDeviceToHost);
+                }
+                if (e != cudaSuccess && s2 == GTB_OK) {
+                    snprintf(h->err, sizeof(h->err), "alignment rows: %s", cudaGetErrorString(e));
+                    s2 = GTB_ERR_CUDA;
+                }
+                if (s2 == GTB_OK) sink->scatter(sb.p0, sb.np);
+                cudaFreeAsync(sb.base, h->st);
+            }
+            strbat.clear();
+            if (s2 != GTB_OK) return s2;
+        }
         for (int j = 0; j < nsub; j++) {
             gtb_status s = add_times(j);
             if (s != GTB_OK) return s;
@@ -451,6 +537,15 @@ static gtb_status run_block(gtb_handle* h, const DevBlock& D, float scorethld,
         p0 = p1;
     }
     memcpy(h->timings, tsum, sizeof(tsum));
+    {
+        unsigned long long wk[gtb::WK_NKIND * gtb::WORK_SLOTS];
+        CK(cudaMemcpy(wk, h->d_work, sizeof(wk), cudaMemcpyDeviceToHost));
+        for (int k = 0; k < gtb::WK_NKIND; k++) {
+            unsigned long long t = 0;
+            for (int j = 0; j < gtb::WORK_SLOTS; j++) t += wk[k * gtb::WORK_SLOTS + j];
+            h->work[k] = t;
+        }
+    }
     return GTB_OK;
 }
 
@@ -629,7 +724,7 @@ extern "C" gtb_status gtb_process_resident(gtb_handle* h, float scorethld, const
     if ((s = check_na_pairs(h, queries->mol, refs->mol)) != GTB_OK) return s;
     CK(cudaSetDevice(h->dev));
     DevBlock D = make_devblock(queries, refs);
-    return run_block(h, D, scorethld, d_alndata, d_tfm, d_numerr, nullptr, nullptr);
+    return run_block(h, D, scorethld, d_alndata, d_tfm, d_numerr, nullptr);
 }
 
 extern "C" gtb_status gtb_process_block(gtb_handle* h, float scorethld,
@@ -655,19 +750,25 @@ extern "C" gtb_status gtb_process_block(gtb_handle* h, float scorethld,
     if (s != GTB_OK) { cudaStreamSynchronize(st); free_block(qb); free_block(rb); return s; }
     DevBlock D = make_devblock(qb, rb);
 
-    // compact per-pair alignment rows, scattered to the reference layout after
-    std::vector<long long> stroff;
-    std::vector<char> hstr;
+    // alignment rows go straight from the packed device rows to the caller's
+    // buffer in the reference layout
+    AlnSink sink;
     if (out->alns) {
-        long long np = (long long)Q.n * R.n;
-        stroff.resize(np + 1);
-        stroff[0] = 0;
-        for (long long p = 0; p < np; p++)
-            stroff[p + 1] = stroff[p] + 5LL * (Q.len[p / R.n] + R.len[p % R.n] + 1);
-        hstr.assign((size_t)stroff[np], 0);
+        sink.alns = out->alns;
+        sink.rec = out->alndata;
+        sink.nr = R.n;
+        sink.qlen.assign(Q.len, Q.len + Q.n);
+        sink.rlen.assign(R.len, R.len + R.n);
+        sink.roff = R.off;
+        long long base = 0;
+        for (int qi = 0; qi < Q.n; qi++) {
+            long long rowlen = R.npos + (long long)R.n * (Q.len[qi] + 1);
+            sink.qbase.push_back(base);
+            sink.rowlen.push_back(rowlen);
+            base += 5 * rowlen;
+        }
     }
-    s = run_block(h, D, scorethld, out->alndata, out->tfm, out->numerr,
-                  out->alns ? hstr.data() : nullptr, out->alns ? &stroff : nullptr);
+    s = run_block(h, D, scorethld, out->alndata, out->tfm, out->numerr, out->alns ? &sink : nullptr);
     h->launches += 2;  // secondary-structure launches of the two uploads
     if (s == GTB_OK) {
         cudaError_t e1 = cudaSuccess;
@@ -682,30 +783,5 @@ extern "C" gtb_status gtb_process_block(gtb_handle* h, float scorethld,
     cudaStreamSynchronize(st);
     free_block(qb);
     free_block(rb);
-    if (s != GTB_OK) return s;
-
-    if (out->alns) {
-        // reference layout (MpDPHub.cpp:1975-1981)
-        long long Nr = R.npos;
-        long long base = 0;
-        for (int qi = 0; qi < Q.n; qi++) {
-            int lq = Q.len[qi];
-            long long rowlen = Nr + (long long)R.n * (lq + 1);
-            char* blk = out->alns + base;
-            for (int f = 0; f < 5; f++) memset(blk + f * rowlen, 0, (size_t)rowlen);
-            for (int ri = 0; ri < R.n; ri++) {
-                long long p = (long long)qi * R.n + ri;
-                int W = lq + R.len[ri] + 1;
-                const char* src = hstr.data() + stroff[p];
-                long long col = (long long)R.off[ri] + (long long)ri * (lq + 1);
-                for (int f = 0; f < 5; f++) {
-                    int n = 0;
-                    while (n < W && src[f * W + n]) n++;
-                    memcpy(blk + f * rowlen + col, src + f * W, (size_t)n);
-                }
-            }
-            base += 5 * rowlen;
-        }
-    }
-    return GTB_OK;
+    return s;
 }

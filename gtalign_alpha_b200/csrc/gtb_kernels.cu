@@ -48,6 +48,13 @@ __device__ __forceinline__ float gonnet(unsigned char a, unsigned char b) {
 
 #define GTB_LAUNCHED(T) do { if ((T).launches) (*(T).launches)++; } while (0)
 
+// algorithmic work counters (Bat::work): one atomic per caller, spread over
+// WORK_SLOTS addresses by CTA
+__device__ __forceinline__ void work_add(const Bat& T, int kind, unsigned long long v) {
+    if (T.work && v)
+        atomicAdd(T.work + kind * WORK_SLOTS + (blockIdx.x & (WORK_SLOTS - 1)), v);
+}
+
 __device__ __forceinline__ int pair_qi(const Blk& B, const Bat& T, int i) {
     return (int)((T.p0 + i) / B.nr);
 }
@@ -454,12 +461,16 @@ __device__ void seed_cov_list(const PairGeom& G, const float* kd, const int* kk,
     a.final(v);
 }
 
-__device__ float findfrag_variant(const PairGeom& G, float d02, float d0s, int swap) {
+// vis: position visits of the passes made (the algorithmic work count)
+__device__ float findfrag_variant(const PairGeom& G, float d02, float d0s, int swap,
+                                  unsigned long long& vis) {
     float v[16], tfm[12], m3, best = 0.f;
     float d02s0 = __fmul_rn(d0s, d0s);
     cov_range(G, 0, G.n, v);
+    vis += G.n;
     for (int it = 0; it < 3; it++) {
         solve_sums(v, swap, tfm);
+        vis += G.n;
         if (it == 2) {
             float sc = score_pass(G, tfm, d02, 0, 0.f, 0, m3);
             if (best < sc) best = sc;
@@ -477,7 +488,7 @@ __device__ float findfrag_variant(const PairGeom& G, float d02, float d0s, int s
         else dst32 = __fadd_rn(d02s, __fmul_rn(ceilf(__fmul_rn(__fsub_rn(m3, d02s), 2.0f)), 0.5f));
         if (dst32 != d02s) {
             if (dst32 < kd[SEED_K - 1]) seed_cov_list(G, kd, kk, dst32, v);
-            else cov_ext(G, tfm, dst32, v);
+            else { cov_ext(G, tfm, dst32, v); vis += G.n; }
         }
         if (v[15] < 1.0f) break;
         if ((int)v[15] == G.n) break;
@@ -518,6 +529,7 @@ __global__ void __launch_bounds__(128) k_findfrag(Blk B, Bat T) {
     G.alc = nullptr;
     float lbest = 0.f;
     int lsi = 0x7fffffff;
+    unsigned long long vis = 0;
     // offsets handed out one at a time (a thread's offsets still come in
     // increasing order, so its strict-improvement rule keeps the lowest index)
     __shared__ int s_next;
@@ -531,14 +543,17 @@ __global__ void __launch_bounds__(128) k_findfrag(Blk B, Bat T) {
         if (lq - qpos < prv || lr - rpos < prv) continue;
         G.q0 = qpos; G.r0 = rpos;
         G.n = (lq - qpos) < (lr - rpos) ? (lq - qpos) : (lr - rpos);
-        float b = findfrag_variant(G, d02, d0s, swap);
+        float b = findfrag_variant(G, d02, d0s, swap, vis);
         if (b > 0.f && lbest < b) { lbest = b; lsi = si; }
     }
     __shared__ float sb[128];
     __shared__ int ssi[128];
+    __shared__ unsigned long long s_vis;
+    if (threadIdx.x == 0) s_vis = 0;
     sb[threadIdx.x] = lbest;
     ssi[threadIdx.x] = lsi;
     __syncthreads();
+    if (T.work) atomicAdd(&s_vis, vis);
     for (int s = blockDim.x >> 1; s > 0; s >>= 1) {
         if ((int)threadIdx.x < s) {
             float o = sb[threadIdx.x + s];
@@ -551,6 +566,7 @@ __global__ void __launch_bounds__(128) k_findfrag(Blk B, Bat T) {
         __syncthreads();
     }
     if (threadIdx.x == 0) {
+        work_add(T, WK_SEED, s_vis);
         float b = sb[0];
         if (nch > 1) {
             // larger score, then lower offset index, over the pair's CTAs
@@ -1065,6 +1081,7 @@ __global__ void __launch_bounds__(RF_WARPS * 32) k_refine(Blk B, Bat T) {
     for (int f = 0; f < 12; f++) tfm[f] = 0.f;
     bool need = true;
     int nextk = 0;                                // the pair's next variant to hand out
+    unsigned long long vis = 0;                   // position visits of this lane's passes
     for (;;) {
         const unsigned nm = __ballot_sync(FULL, need) & smask;
         if (nm) {
@@ -1090,6 +1107,7 @@ __global__ void __launch_bounds__(RF_WARPS * 32) k_refine(Blk B, Bat T) {
         float v[16], m3;
         const float sc = lane_pass(G, kind, k0, k1, tfm, pd02, pchk, d82, thr, m3mode, v, m3,
                                    lane % RF_LPP);
+        vis += kind == PK_IDLE ? 0u : (kind == PK_FRAG ? (unsigned)(k1 - k0) : (unsigned)n);
         bool havev = false, done = false;
         if (kind == PK_FRAG) {
             if (v[15] < 1.0f) done = true;
@@ -1149,6 +1167,11 @@ __global__ void __launch_bounds__(RF_WARPS * 32) k_refine(Blk B, Bat T) {
                 kind = PK_IDLE;
             }
         }
+    }
+    if (T.work) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) vis += __shfl_xor_sync(FULL, vis, o);
+        if (lane == 0) work_add(T, WK_REFINE, vis);
     }
     // arg-max over the pair's lanes: larger score, then lower variant index
     float wb = lbest;
@@ -1310,7 +1333,8 @@ __device__ __forceinline__ bool dp_pair(const float* t, float d02, float gcost, 
                                         const unsigned char* qa, const unsigned char* ra,
                                         float* row, unsigned* bt, int lane, int s_first = 0,
                                         int s_step = 1, volatile int* prog = nullptr,
-                                        volatile int* err = nullptr) {
+                                        volatile int* err = nullptr,
+                                        long long spin = DP_WAVE_SPIN_DEFAULT) {
     constexpr bool usess = SC == DP_SC_TFMSS, ssrr = SC == DP_SC_SSRR;
     constexpr float BND = ssrr ? DPSS_C : 0.f;   // the matrix border
     constexpr int ROWS = 32 * R, SPW = 16 / R;
@@ -1349,7 +1373,7 @@ __device__ __forceinline__ bool dp_pair(const float* t, float d02, float gcost, 
                 if (lane == 0) {
                     long long it = 0;
                     while (prog[s - 1] < need) {
-                        if (*err || ++it > (1LL << 24)) { *err = 1; break; }
+                        if (*err || ++it > spin) { *err = 1; break; }
                         __nanosleep(64);
                     }
                 }
@@ -1459,6 +1483,7 @@ __global__ void __launch_bounds__(128) k_dp(Blk B, Bat T, int tfmsrc, float gcos
     unsigned* bt = T.bt + T.off_bt[i];
     const unsigned char* qa = B.qa + B.qoff[qi];
     const unsigned char* ra = B.ra + B.roff[ri];
+    if (lane == 0) work_add(T, WK_DPCELL, (unsigned long long)lq * (unsigned long long)lr);
     if (dp_r(lq) == 4)
         dp_pair<4, GAP0 != 0, SC, false>(t, d02, gcost, lq, lr, qx, qy, qz, r4, qs, rs, qa, ra, row, bt, lane);
     else
@@ -1500,12 +1525,13 @@ __global__ void __launch_bounds__(32) k_dp_wave(Blk B, Bat T, int tfmsrc, float 
     volatile int* prog = T.dw_prog + T.dw_soff[slot];
     const unsigned char* qa = B.qa + B.qoff[qi];
     const unsigned char* ra = B.ra + B.roff[ri];
+    if (lane == 0 && c == 0) work_add(T, WK_DPCELL, (unsigned long long)lq * (unsigned long long)lr);
     if (dp_r(lq) == 4)
         dp_pair<4, GAP0 != 0, SC, true>(t, d02, gcost, lq, lr, qx, qy, qz, r4, qs, rs, qa, ra, row,
-                                        bt, lane, c, G, prog, T.dw_err);
+                                        bt, lane, c, G, prog, T.dw_err, T.dw_spin);
     else
         dp_pair<2, GAP0 != 0, SC, true>(t, d02, gcost, lq, lr, qx, qy, qz, r4, qs, rs, qa, ra, row,
-                                        bt, lane, c, G, prog, T.dw_err);
+                                        bt, lane, c, G, prog, T.dw_err, T.dw_spin);
 }
 
 int dp_wave_capacity() {
@@ -1528,7 +1554,9 @@ static void launch_dp_wave(const Blk& B, const Bat& T, int tfmsrc, float gcost, 
     Blk b = B;
     Bat t = T;
     void* args[] = {&b, &t, &tfmsrc, &gcost, &dpscan, &skipmode};
-    cudaLaunchCooperativeKernel((const void*)k_dp_wave<GAP0, SC>, dim3(T.ndw), dim3(32), args, 0, st);
+    cudaError_t e = cudaLaunchCooperativeKernel((const void*)k_dp_wave<GAP0, SC>, dim3(T.ndw),
+                                                dim3(32), args, 0, st);
+    if (e != cudaSuccess && T.lerr && *T.lerr == cudaSuccess) *T.lerr = e;
 }
 
 void launch_dp(const Blk& B, const Bat& T, int tfmsrc, int gap0, float gcost, int usess,
@@ -1658,21 +1686,19 @@ void launch_lowscore(const Blk& B, const Bat& T, float thr, cudaStream_t st) {
 }
 
 // ---------------------------------------------------------------------------
-// alignment rows: MpDPHub.cpp:1919-2125
+// alignment rows: MpDPHub.cpp:1919-2125.  The rows of a pair with an
+// alignment are packed at an offset it reserves (atomically) once its column
+// count is known; that count follows from the first and last aligned pairs:
+// every aligned pair is one column, every skipped query residue between them
+// one, and every skipped reference residue one unless --no-deletions.
 __global__ void k_alnstr(Blk B, Bat T) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= T.np) return;
-    int qi = pair_qi(B, T, i), ri = pair_ri(B, T, i);
-    int lq = B.qlen[qi], lr = B.rlen[ri];
     if (T.flags[i] & CONV_LOWTMSC) {
-        // no alignment: five empty rows (the batch memory is reused between calls)
-        if (T.str) {
-            char* d = T.str + T.off_str[i];
-            int W = lq + lr + 1;
-            d[0] = 0; d[W] = 0; d[2 * W] = 0; d[3 * W] = 0; d[4 * W] = 0;
-        }
+        if (T.str) T.str_off[i] = -1;      // no alignment
         return;
     }
+    int qi = pair_qi(B, T, i), ri = pair_ri(B, T, i);
     const unsigned* aln = T.aln + T.off_aln[i];
     int n = T.naln[i];
     float t[12];
@@ -1684,8 +1710,21 @@ __global__ void k_alnstr(Blk B, Bat T) {
     const unsigned char* ra = B.ra + B.roff[ri];
     const char* qs = B.qs + B.qoff[qi];
     const char* rs = B.rs + B.roff[ri];
-    int W = lq + lr + 1;
-    char* dst = T.str ? T.str + T.off_str[i] : nullptr;
+    char* dst = nullptr;
+    int W = 1;
+    if (T.str) {
+        int ncol = 0;
+        if (n > 0) {
+            const unsigned wf = aln[n - 1], wl = aln[0];   // first and last aligned pairs
+            const int qf = (int)(wf >> 16), rf = (int)(wf & 0xffffu);
+            const int ql = (int)(wl >> 16), rl = (int)(wl & 0xffffu);
+            ncol = n + (ql - qf + 1 - n) + (B.nodeletions ? 0 : (rl - rf + 1 - n));
+        }
+        W = ncol + 1;
+        const unsigned long long o = atomicAdd(T.str_cnt, 5ull * (unsigned long long)W);
+        T.str_off[i] = (long long)o;
+        dst = T.str + o;
+    }
     int col = 0, psts = 0, idts = 0, gaps = 0;
     unsigned bc = 0, ec = 0;
     for (int k = 0; k < n; k++) {

@@ -62,7 +62,12 @@ struct Bat {
     const long long *off_row; float* row;     // DP row buffer per pair
     const long long *off_aln; unsigned* aln;  // aligned pairs, reverse order
     float* alc;                      // their coordinates, 6 floats each (offset 6*off_aln)
-    const long long *off_str; char* str;      // alignment rows per pair
+    const long long *off_str; char* str;      // alignment rows (null: not produced)
+    // rows of the pairs with an alignment, packed back to back in str: pair i
+    // at str + str_off[i] (-1: none), 5 rows of (columns + 1) bytes each, the
+    // last byte of a row its NUL; str_cnt: bytes used
+    long long* str_off;
+    unsigned long long* str_cnt;
     int *rlist, *rhist;              // refinement work list [np], buckets [4097]
     // long pairs of a refinement launch (null: none possible): list, count,
     // per-pair variant counter, per-warp candidates; rl_nlmax = capacity
@@ -85,8 +90,18 @@ struct Bat {
     const long long* dw_soff;
     const unsigned char* dw_mark;
     int *dw_prog, *dw_err;
+    long long dw_spin;               // spins a wavefront wait makes before it gives up
     long long* launches;             // host counter of kernel launches
+    cudaError_t* lerr;               // host: first failed launch (null: not recorded)
+    // device work counters (null: not counted), WORK_SLOTS slots per kind,
+    // summed on the host: position visits of the seed passes, position
+    // visits of the refinement passes, DP cells
+    unsigned long long* work;
 };
+
+enum WorkKind { WK_SEED = 0, WK_REFINE = 1, WK_DPCELL = 2, WK_NKIND = 3 };
+constexpr int WORK_SLOTS = 64;       // spread over addresses: fewer atomic collisions
+constexpr long long DP_WAVE_SPIN_DEFAULT = 1LL << 24;
 
 // DP cell scores (launch_dp's usess): TM term under a transform, + SS, or the
 // --add-search-by-ss score (SS + Gonnet, no transform)

@@ -21,11 +21,18 @@
 //    tables, with that device current); make that first call before any
 //    stream capture;
 //  * every call uses the same scratch array and leaves its contents behind.
-//    Nothing in it has to start at zero: the pair state is initialised by
-//    the first kernel of each call and every other region is written before
-//    it is read.  Calls that overlap on the GPU (on different streams, or
-//    from different host threads at once) race on the scratch array and must
-//    not be issued; calls in order on one stream are fine;
+//    Only the two molecule-type flags must start at zero, and each call
+//    clears them first; the pair state is initialised by the first kernel of
+//    each call and every other region is written before it is read.  Calls
+//    that overlap on the GPU of one device (on different streams, or from
+//    different host threads at once) race on that device's scratch array and
+//    must not be issued; calls in order on one stream are fine, and so are
+//    calls from different host threads on different devices (the host-side
+//    plan is per thread);
+//  * a block that would pair two nucleic-acid structures is refused with
+//    GTB_ERR_UNSUPPORTED, like gtb_process_block refuses it: the molecule
+//    types are read back from the device before any search work;
+//  * the caller's current device is restored before the call returns;
 //  * nothing here calls cudaMalloc, cudaFree or any allocating routine.
 #include <cstdio>
 #include <cstring>
@@ -56,12 +63,36 @@ struct DevState {
 static DevState g_dev[MAXDEV];
 static std::mutex g_setup_mutex;
 static float h_tbl[3][TBLN];
-// host copies of the per-pair offsets (4 arrays of up to MAX_PAIRS+1 entries)
-static long long h_offs[4 * (GTB_NOALLOC_MAX_PAIRS + 1)];
-// host copies of the back-to-back residue offsets of the (x, y, z, 0) copies
-static int h_coff[2 * (GTB_NOALLOC_MAX_PAIRS + 1)];
+// Host copies of the per-pair offsets (4 arrays of up to MAX_PAIRS+1 entries)
+// and of the back-to-back residue offsets of the (x, y, z, 0) copies.  One set
+// per host thread, so that threads calling on different devices at once do
+// not overwrite each other's plan before it is copied to the device.
+static thread_local long long h_offs[4 * (GTB_NOALLOC_MAX_PAIRS + 1)];
+static thread_local int h_coff[2 * (GTB_NOALLOC_MAX_PAIRS + 1)];
+// Flag read back after the molecule-type check (per host thread, as above).
+static thread_local int h_naflag[2];
+
+// Sets flag[0] when some query is a nucleic acid and flag[1] when some
+// reference is; a pair of two nucleic acids is refused by the caller.
+__global__ void k_na_check(const int* qmol, int nq, const int* rmol, int nr, int* flag) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < nq) { if (qmol[i] == 1) atomicOr(flag, 1); }
+    else if (i < nq + nr) { if (rmol[i - nq] == 1) atomicOr(flag + 1, 1); }
+}
+
+// Restores the caller's current device when the call returns.
+struct DeviceGuard {
+    int prev = -1;
+    DeviceGuard() { if (cudaGetDevice(&prev) != cudaSuccess) prev = -1; }
+    ~DeviceGuard() { if (prev >= 0) cudaSetDevice(prev); }
+};
 
 size_t al256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+// the --pre-similarity screen runs for this block (as in launch setup below)
+bool B_presim_on(const gtb_options* o, int qmax, int rmax) {
+    return 0.f < o->presimilarity && PRESIM_EDGE < qmax && PRESIM_EDGE < rmax;
+}
 
 void setmsg(char* buf, size_t len, const char* fmt, long long a, long long b) {
     if (buf && len) snprintf(buf, len, fmt, a, b);
@@ -170,6 +201,7 @@ extern "C" gtb_status gtb_process_block_noalloc(int device, const gtb_options* o
     size_t o_co = carve((size_t)(q->n + r->n) * sizeof(int));
     size_t o_rl = carve((size_t)np * sizeof(int));
     size_t o_rh = carve((size_t)4097 * sizeof(int));
+    size_t o_na = carve(2 * sizeof(int));
     if (sz > SCRATCH_BYTES) {
         setmsg(errbuf, errlen, "block needs %lld bytes of working memory; the static scratch holds %lld",
                (long long)sz, (long long)SCRATCH_BYTES);
@@ -177,6 +209,7 @@ extern "C" gtb_status gtb_process_block_noalloc(int device, const gtb_options* o
     }
 
     cudaStream_t st = (cudaStream_t)stream;
+    DeviceGuard keep_device;
     cudaError_t e = cudaSetDevice(device);
     if (e == cudaSuccess) e = setup(device, st);
     if (e != cudaSuccess) {
@@ -185,6 +218,30 @@ extern "C" gtb_status gtb_process_block_noalloc(int device, const gtb_options* o
     }
     const DevState& D = g_dev[device];
     unsigned char* base = D.scratch;
+
+    // The molecule types are device data: look at them before any work, and
+    // refuse a block that would pair two nucleic-acid structures (the search
+    // here scores with protein rules only), as gtb_process_block does.
+    {
+        int* naf = (int*)(base + o_na);
+        e = cudaMemsetAsync(naf, 0, 2 * sizeof(int), st);
+        if (e == cudaSuccess) {
+            int nt = q->n + r->n;
+            k_na_check<<<(nt + 255) / 256, 256, 0, st>>>(q->d_mol, q->n, r->d_mol, r->n, naf);
+            e = cudaGetLastError();
+        }
+        if (e == cudaSuccess) e = cudaMemcpyAsync(h_naflag, naf, sizeof(h_naflag), cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        if (e != cudaSuccess) {
+            if (errbuf && errlen) snprintf(errbuf, errlen, "molecule-type check: %s", cudaGetErrorString(e));
+            return GTB_ERR_CUDA;
+        }
+        if ((h_naflag[0] && h_naflag[1]) || (B_presim_on(opts, qmax, rmax) && (h_naflag[0] || h_naflag[1]))) {
+            setmsg(errbuf, errlen, "nucleic-acid structure pairs are not supported (%lld, %lld)",
+                   h_naflag[0], h_naflag[1]);
+            return GTB_ERR_UNSUPPORTED;
+        }
+    }
 
     Blk B{};
     B.nq = q->n; B.nr = r->n;
@@ -200,7 +257,7 @@ extern "C" gtb_status gtb_process_block_noalloc(int device, const gtb_options* o
     B.stepinit = (opts->depth == 3) ? 5 : 1;
     B.refinement = opts->refinement; B.depth = opts->depth; B.twotm = opts->twotmscore ? 1 : 0;
     B.addss = opts->addsearchbyss ? 1 : 0;
-    B.presim = (0.f < opts->presimilarity && PRESIM_EDGE < qmax && PRESIM_EDGE < rmax) ? opts->presimilarity : 0.f;
+    B.presim = B_presim_on(opts, qmax, rmax) ? opts->presimilarity : 0.f;
     B.symmetric = opts->symmetric; B.nodeletions = opts->nodeletions;
 
     Bat T{};

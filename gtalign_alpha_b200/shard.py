@@ -54,19 +54,33 @@ def subset(s: SoA, idx: np.ndarray) -> SoA:
 ProcessFn = Callable[[SoA, SoA], Tuple[np.ndarray, np.ndarray]]
 
 
+class ShardPlan:
+    """This rank's share of a reference block, made once and reused for every
+    query block (the reference streams each reference chunk to every device
+    for every query block; here a rank keeps its share)."""
+
+    def __init__(self, refs: SoA, qlens: Sequence[int], rank: int, world: int):
+        self.rank, self.world, self.nref = rank, world, refs.n
+        self.shards = lpt_shards(refs.lens, qlens, world)
+        self.mine = self.shards[rank]
+        self.refs = refs if world == 1 else subset(refs, self.mine)
+
+
 def search_sharded(queries: SoA, refs: SoA, process: ProcessFn, rank: int, world: int,
-                   group=None):
+                   group=None, plan: "ShardPlan" = None):
     """Align all queries with this rank's reference shard and gather the
     (nq, nr, 16) result records and (nq, nr, 12) transforms on rank 0.
 
     `process(queries, refs_shard)` returns (alndata, tfm) for the shard.
     Returns the full arrays on rank 0 and None elsewhere.  Uses
-    torch.distributed (gloo or nccl) when world > 1.
+    torch.distributed (gloo or nccl) when world > 1.  `plan` (a ShardPlan
+    of `refs`) saves re-splitting the references on every call.
     """
-    shards = lpt_shards(refs.lens, queries.lens, world)
-    mine = shards[rank]
+    if plan is None:
+        plan = ShardPlan(refs, queries.lens, rank, world)
+    mine = plan.mine
     if len(mine):
-        aln, tfm = process(queries, subset(refs, mine))
+        aln, tfm = process(queries, plan.refs)
     else:
         aln = np.zeros((queries.n, 0, 16), np.float32)
         tfm = np.zeros((queries.n, 0, 12), np.float32)

@@ -201,12 +201,14 @@ gtb_status gtb_polish(gtb_handle* h, int npairs, const long long* off,
  * array, or with more than GTB_NOALLOC_MAX_PAIRS pairs, are rejected with
  * GTB_ERR_NOMEM and a message in errbuf.  The first call on a device performs
  * a one-time set-up there (device addresses of the static arrays, constant
- * tables): make it before any stream capture.  All calls share the scratch
- * array, so calls that overlap on the GPU race; issue them one after another.
- * Results are those of gtb_process_block (records and transforms only).
- * The molecule types are device data here, so the nucleic-acid refusal of
- * gtb_process_block is not made: the caller must not pass blocks that pair
- * two nucleic-acid structures (they would be scored with protein rules). */
+ * tables): make it before any stream capture.  All calls on one device share
+ * that device's scratch array, so calls that overlap on the same GPU race;
+ * issue them one after another.  Host threads calling on different devices
+ * at once do not conflict.  The caller's current device is restored before
+ * the call returns.  Results are those of gtb_process_block (records and
+ * transforms only).  Blocks that would pair two nucleic-acid structures are
+ * refused with GTB_ERR_UNSUPPORTED, as by gtb_process_block (the molecule
+ * types are read back from the device before any search work). */
 #define GTB_NOALLOC_SCRATCH_BYTES ((size_t)16 << 20)
 #define GTB_NOALLOC_MAX_PAIRS 4096
 
@@ -238,6 +240,20 @@ long long gtb_last_launch_count(const gtb_handle* h);
  * unused (0), [5] final + production stages, [6] total.  A batch runs as up
  * to three concurrent sub-batches; the times are summed over them. */
 gtb_status gtb_last_timings(const gtb_handle* h, float* ms7);
+
+/* Algorithmic work of the last gtb_process_block / gtb_process_resident
+ * call, counted on the device (no reference counterpart; the measurement
+ * behind a FP32 roofline): w3[0] position visits of the seed passes (one
+ * visit = one aligned residue pair transformed, scored or added to a
+ * covariance in one pass), w3[1] position visits of the refinement passes,
+ * w3[2] DP matrix cells. */
+gtb_status gtb_last_work(const gtb_handle* h, unsigned long long* w3);
+
+/* Spins a bounded wait of the multi-CTA DP makes before it gives up (no
+ * reference counterpart; default 2^24).  A wait that gives up ends the call
+ * with GTB_ERR_CUDA and a message; the handle stays usable.  Small values
+ * make the waits give up early, which is how the failure path is tested. */
+gtb_status gtb_set_wait_limit(gtb_handle* h, long long spins);
 
 void gtb_destroy(gtb_handle* h);
 

@@ -14,6 +14,15 @@ exact arithmetic); the agreement between those two reference runs is the
 reference's own numerical reproducibility and is stored as `self_agreement`.
 
     python tests/golden/make_golden.py [set ...]   (needs oracle/_ref/gtalign)
+
+The same sets run by the reference's GPU build (oracle/_ref/gpu/gtalign,
+compiled by oracle/Makefile.refgpu; on a machine with a GPU):
+
+    python tests/golden/make_golden.py --gpu --outdir DIR [set ...]
+
+writes DIR/<set>_refgpu.json (its results and self-agreement; the inputs are
+those of <set>.npz) and, for every pair both builds report, the agreement
+between the reference's GPU and CPU builds.
 """
 from __future__ import annotations
 
@@ -33,6 +42,7 @@ sys.path.insert(0, ROOT)
 from gtalign_alpha_b200 import synth  # noqa: E402
 
 BIN = os.path.join(ROOT, "oracle", "_ref", "gtalign")
+BIN_GPU = os.path.join(ROOT, "oracle", "_ref", "gpu", "gtalign")
 
 def na_set(seed):
     """Nucleic acids: a query of 3 hairpins, moved noisy copies of it,
@@ -91,14 +101,20 @@ SETS = {
     "c0_shallow": (lambda: synth.config0(seed=108, n_refs=60, qlen=160),
                    ["--no-detailed-search", "--depth=3", "--pre-score=0.3", "-s", "0.3",
                     "--convergence=6"]),
+    # the small configuration at its full size: one 150-residue query against
+    # 1,000 targets (lengths U(50,500), 20% homologs), default options (the
+    # default --pre-score 0.4 and -s 0.5) without the detailed search, and
+    # the --speed=13 preset
+    "c0_full": (lambda: synth.config0(seed=1, n_refs=1000, qlen=150), ["--no-detailed-search"]),
+    "c0_full_s13": (lambda: synth.config0(seed=1, n_refs=1000, qlen=150), ["--speed=13"]),
 }
 
 
-def run(wl, opts, threads=8):
+def run(wl, opts, threads=8, binary=BIN):
     d = tempfile.mkdtemp(prefix="gtgold")
     try:
         synth.write_dirs(wl, d + "/q", d + "/r")
-        subprocess.run([BIN, "--qrs=" + d + "/q", "--rfs=" + d + "/r", "-o", d + "/out",
+        subprocess.run([binary, "--qrs=" + d + "/q", "--rfs=" + d + "/r", "-o", d + "/out",
                         "--outfmt=1", "--cpu-threads=%d" % threads, "--cpu-threads-reading=1"] + opts,
                        check=True, capture_output=True)
         res = {}
@@ -142,20 +158,39 @@ def agreement(a, b):
 
 
 def main():
-    if not os.path.exists(BIN):
-        sys.exit("build the reference first: make -f oracle/Makefile.ref")
-    names = sys.argv[1:] or list(SETS)
+    import argparse
+    ap = argparse.ArgumentParser()
+    ap.add_argument("sets", nargs="*")
+    ap.add_argument("--gpu", action="store_true", help="run the reference's GPU build")
+    ap.add_argument("--outdir", default=HERE)
+    a = ap.parse_args()
+    binary = BIN_GPU if a.gpu else BIN
+    if not os.path.exists(binary):
+        sys.exit("build the reference first: make -f oracle/Makefile.ref%s" % ("gpu" if a.gpu else ""))
+    names = a.sets or list(SETS)
     for name in names:
         mk, opts = SETS[name][:2]
         threads = SETS[name][2] if len(SETS[name]) > 2 else 8
         wl = mk()
-        res = run(wl, opts, threads)
+        res = run(wl, opts, threads, binary)
         wl2 = copy.deepcopy(wl)
         rng = np.random.default_rng(7)
         R = synth._rot_random(rng)
         q = wl2.queries[0]
         q.xyz = synth._pdb_round_fast(q.xyz.astype(np.float64) @ R.T + np.array([3.0, -5.0, 7.0]))
-        res2 = run(wl2, opts, threads)
+        res2 = run(wl2, opts, threads, binary)
+        if a.gpu:
+            out = {"options": opts, "seed_desc": wl.desc, "results": res,
+                   "self_agreement": agreement(res, res2), "binary": "reference GPU build (sm_100a)"}
+            cpu = os.path.join(HERE, name + ".json")
+            if os.path.exists(cpu):
+                out["agreement_with_cpu_build"] = agreement(res, json.load(open(cpu))["results"])
+            os.makedirs(a.outdir, exist_ok=True)
+            with open(os.path.join(a.outdir, name + "_refgpu.json"), "w") as f:
+                json.dump(out, f, indent=0, sort_keys=True)
+            print(name, len(res), "pairs; GPU build self-agreement:", out["self_agreement"],
+                  "vs CPU build:", out.get("agreement_with_cpu_build"))
+            continue
         arrs = {}
         for tag, chains in (("q", wl.queries), ("r", wl.refs)):
             s = synth.pack(chains)
@@ -164,8 +199,10 @@ def main():
             arrs[tag + "_rsd"] = s.rsd
             arrs[tag + "_mol"] = s.mol
             arrs[tag + "_names"] = np.array([c.name for c in chains])
-        np.savez_compressed(os.path.join(HERE, name + ".npz"), **arrs)
-        with open(os.path.join(HERE, name + ".json"), "w") as f:
+        # sets on another set's inputs (the same builder) keep one input file
+        if name not in ("c0_full_s13",):
+            np.savez_compressed(os.path.join(a.outdir, name + ".npz"), **arrs)
+        with open(os.path.join(a.outdir, name + ".json"), "w") as f:
             json.dump({"options": opts, "seed_desc": wl.desc, "results": res,
                        "self_agreement": agreement(res, res2)}, f, indent=0, sort_keys=True)
         print(name, len(res), "pairs; reference self-agreement:", agreement(res, res2))

@@ -12,11 +12,16 @@ LEVEL_SETS = {-1: "c0_level_m1", 0: "c0_level_0", 1: "c0_level_1", 2: "c0_level_
               3: "c0_level_3"}
 SETS = ["c0_speed13", "c0_default", "c0_filters", "c0_sym_ref_nodel", "c0_shallow", "c0_2tm",
         "c0_ssrr", "c0_presim", "c0_na", "c0_combo"] + \
-    list(LEVEL_SETS.values())
+    list(LEVEL_SETS.values()) + ["c0_full", "c0_full_s13"]
 # the sets the GPU golden test runs: every set the CUDA library takes (it
 # refuses nucleic-acid pairs) except the combined-options set, which pins
 # the oracle only (each of its options runs on the GPU in the option sets)
-LIBRARY_SETS = [s for s in SETS if s not in ("c0_na", "c0_combo")]
+LIBRARY_SETS = [s for s in SETS if s not in ("c0_na", "c0_combo", "c0_full", "c0_full_s13")]
+# the small configuration at full size (1 x 1,000 pairs): default options
+# without the detailed search, and --speed=13, on the same inputs
+FULL_SETS = ["c0_full", "c0_full_s13"]
+# sets whose inputs are another set's
+INPUTS = {"c0_full_s13": "c0_full"}
 
 
 def _soa(z, tag):
@@ -31,7 +36,7 @@ def _soa(z, tag):
 
 
 def load(name):
-    z = np.load(os.path.join(GOLDEN, name + ".npz"))
+    z = np.load(os.path.join(GOLDEN, INPUTS.get(name, name) + ".npz"))
     with open(os.path.join(GOLDEN, name + ".json")) as f:
         meta = json.load(f)
     return (_soa(z, "q"), _soa(z, "r"), list(z["q_names"]), list(z["r_names"]), meta)

@@ -61,6 +61,37 @@ def test_golden_sets_bit_identical(oracle, name):
     assert res.launches > 20
 
 
+@pytest.mark.parametrize("name", gu.FULL_SETS)
+def test_small_configuration_full_size(oracle, name):
+    """The small configuration at its full size: one 150-residue query
+    against 1,000 targets (lengths U(50,500), 20% homologs), default options
+    without the detailed search (--pre-score 0.4, -s 0.5) and --speed=13:
+    records, transforms, numeric errors and alignment rows bit for bit."""
+    q, r, qn, rn, meta = gu.load(name)
+    d = gu.cli_options(meta["options"])
+    res, ora = run_both(oracle, q, r, d)
+    assert_same(res, ora, q.n, r.n)
+    assert (res.alndata[0, :, 9] > 0).sum() > 150         # the reported pairs
+    assert float(res.numerr[..., :2].max()) <= 1e-4 and float(res.numerr[..., 2].max()) <= 1e-3
+
+
+def test_benchmark_workload_sample(oracle):
+    """A seeded sample of the benchmark workload (2 queries of the 16 x 3,000
+    references of its generator: log-normal lengths up to 2,000, homolog
+    families), with the benchmark's options (defaults without the detailed
+    search, -s 0.5), GPU against the oracle bit for bit."""
+    from gtalign_alpha_b200 import synth
+    from gtalign_alpha_b200.shard import subset
+    wl = synth.config1(seed=2, n_queries=16, n_refs=3000)
+    q, r = synth.pack(wl.queries), synth.pack(wl.refs)
+    q = subset(q, np.array([0, 1]))
+    d = dict(refinement=1, convergence=18, prescore=0.4, scorethld=0.5, symmetric=0, referenced=0,
+             nodeletions=0)
+    res, ora = run_both(oracle, q, r, d)
+    assert_same(res, ora, q.n, r.n)
+    assert (res.alndata[..., 9] > 0).sum() > 20
+
+
 OPTSETS = {
     "speed13": dict(refinement=0, convergence=2, prescore=0.0, scorethld=0.0, symmetric=0, referenced=0, nodeletions=0),
     "default": dict(refinement=1, convergence=18, prescore=0.0, scorethld=0.0, symmetric=0, referenced=0, nodeletions=0),

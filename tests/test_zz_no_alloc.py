@@ -115,3 +115,62 @@ def test_noalloc_rejects_blocks_beyond_its_scratch():
     assert st == 3
     assert b"static scratch" in msg.value
     assert float(out.abs().sum().item()) == 0.0
+
+
+def _call(L, opts, q, r, thr=0.5):
+    import torch
+    keep = []
+    dq, tq = _dev_block(q, keep)
+    dr, tr = _dev_block(r, keep)
+    np_ = q.n * r.n
+    out = torch.full((np_ * 16,), -1.0, dtype=torch.float32, device="cuda")
+    tfm = torch.full((np_ * 12,), -1.0, dtype=torch.float32, device="cuda")
+    err = torch.zeros(np_ * 4, dtype=torch.float32, device="cuda")
+    msg = ctypes.create_string_buffer(256)
+    copt = opts._c()
+    st = L.gtb_process_block_noalloc(0, ctypes.byref(copt), ctypes.c_float(thr), ctypes.byref(dq),
+                                     ctypes.byref(dr), out.data_ptr(), tfm.data_ptr(), err.data_ptr(),
+                                     torch.cuda.current_stream().cuda_stream, msg, 256)
+    torch.cuda.synchronize()
+    return st, msg.value, out.cpu().numpy(), tfm.cpu().numpy(), err.cpu().numpy()
+
+
+def test_noalloc_long_pair_matches_allocating_entry_point():
+    """A 2,000 x 2,000-residue assembly pair: gtb_process_block runs its DP
+    as a multi-CTA wavefront and its refinement over many CTAs; the
+    allocation-free call runs both on single warps.  The results must be the
+    same bits, on two calls in a row."""
+    from gtalign_alpha_b200 import synth
+    from gtalign_alpha_b200.api import GTalignB200, Options
+    L = _lib()
+    wl = synth.config2(seed=3, lengths=(2000,))
+    q, r = synth.pack(wl.queries), synth.pack(wl.refs)
+    opts = Options(prescore=0.4, convergence=4)
+    with GTalignB200(0, 0, opts) as g:
+        ref = g.process_block(q, r, scorethld=0.5, alignments=False)
+    assert ref.alndata[0, 0, 9] > 0.5
+    for _ in range(2):
+        st, msg, out, tfm, err = _call(L, opts, q, r)
+        assert st == 0, msg
+        assert np.array_equal(out.view(np.uint32), ref.alndata.ravel().view(np.uint32))
+        assert np.array_equal(tfm.view(np.uint32), ref.tfm.ravel().view(np.uint32))
+        assert np.array_equal(err.view(np.uint32), ref.numerr.ravel().view(np.uint32))
+
+
+def test_noalloc_refuses_nucleic_acid_pairs():
+    """A block pairing two nucleic-acid structures is refused before any work
+    (the output buffers keep their contents), as gtb_process_block refuses it;
+    a protein query against the same nucleic-acid reference is accepted."""
+    from gtalign_alpha_b200 import synth
+    from gtalign_alpha_b200.api import Options
+    L = _lib()
+    rng = np.random.default_rng(9)
+    na = synth.na_hairpins(rng, 2, 8, 5, "na0")
+    na2 = synth.na_moved_copy(rng, na, 0.5, "na1")
+    prot = synth.random_chains(rng, [60], "p")
+    st, msg, out, _, _ = _call(L, Options(), synth.pack([na]), synth.pack([na2]))
+    assert st == 4, msg
+    assert b"nucleic" in msg
+    assert np.all(out == -1.0)
+    st, msg, out, _, _ = _call(L, Options(), synth.pack(prot), synth.pack([na2]))
+    assert st == 0, msg
