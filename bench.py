@@ -82,6 +82,14 @@ FP32_LANES_PER_SM = 128
 TOL_TM, TOL_RMSD = 1e-4, 1e-3
 
 
+_T0 = time.time()
+
+
+def progress(msg: str) -> None:
+    """A timestamped line on stderr (the JSON line stays alone on stdout)."""
+    print("[bench %7.1fs] %s" % (time.time() - _T0, msg), file=sys.stderr, flush=True)
+
+
 def dist_env():
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -283,6 +291,7 @@ def run_ours(args):
             dist.barrier()
 
     t0 = time.time()
+    progress("generating the workload")
     wl, q, r_all = make_workload(args.nqueries, args.nrefs, args.seed)
     plan = ShardPlan(r_all, q.lens, rank, ws)
     r = plan.refs
@@ -310,6 +319,7 @@ def run_ours(args):
     legs = set(args.legs.split(","))
 
     # headline: batched + adjoint polishing, resident
+    progress("headline (batched + adjoint, resident)")
     rp = Resident(L, gp, qblks, rblk, step_pairs, maxpairs, args.steps, dev)
     A = timed_steps(rp, args, ws, dev, barrier, clocks=True, work=True)
     value = A["pairs"] / (A["ms"] / 1000.0)
@@ -319,6 +329,7 @@ def run_ours(args):
     # the unpolished form (the reference's results) and the polishing gain
     unpol = None
     if "unpolished" in legs:
+        progress("unpolished")
         r0 = Resident(L, g0, qblks, rblk, step_pairs, maxpairs, args.steps, dev)
         B = timed_steps(r0, args, ws, dev, barrier)
         ok0 = B["maxerr"][0] <= TOL_TM and B["maxerr"][1] <= TOL_TM and B["maxerr"][2] <= TOL_RMSD
@@ -342,12 +353,14 @@ def run_ours(args):
     # e2e through gtb_process_block (host buffers), polished form
     e2e = None
     if "e2e" in legs:
+        progress("e2e")
         e2e = e2e_run(L, gp, qbs, rb, qchunks, r, step_pairs, maxpairs, args, ws, rank, dev, barrier,
                       q, r_all, plan)
 
     # the plain form: one pair per call
     plain = None
     if "plain" in legs and args.plain_pairs > 0 and rank == 0:
+        progress("plain")
         plain = plain_sample(gp, L, q, r, args.plain_pairs, args.seed)
         plain["batched_adjoint_vs_plain"] = value / ws / plain["value"]
         if unpol is not None:
@@ -395,13 +408,18 @@ def run_ours(args):
     long_chain = adjoint = cpu = refgpu = None
     if rank == 0 and ws == 1:
         if "refgpu" in legs:
+            progress("reference GPU build")
             refgpu = reference_gpu_sample(wl, args, value)
         if "long" in legs:
+            progress("long chains")
             long_chain = long_chain_run(gp, args)
         if "adjoint" in legs:
+            progress("adjoint polishing")
             adjoint = adjoint_pairs(args.adjoint_pairs, args.adjoint_steps)
         if "cpu" in legs:
+            progress("reference CPU build sample")
             cpu = cpu_baseline_sample(wl, args)
+        progress("done")
 
     if rank == 0:
         line = {

@@ -46,7 +46,9 @@ class _COptions(ctypes.Structure):
                 ("symmetric", ctypes.c_int), ("referenced", ctypes.c_int),
                 ("nodeletions", ctypes.c_int), ("nodetailedsearch", ctypes.c_int),
                 ("addsearchbyss", ctypes.c_int), ("twotmscore", ctypes.c_int),
-                ("polish_steps", ctypes.c_int), ("presimilarity", ctypes.c_float)]
+                ("polish_steps", ctypes.c_int), ("presimilarity", ctypes.c_float),
+                ("trigger", ctypes.c_int), ("nbranches", ctypes.c_int),
+                ("gapcost", ctypes.c_int), ("seedrule", ctypes.c_int), ("window", ctypes.c_int)]
 
 
 class _CResults(ctypes.Structure):
@@ -60,7 +62,8 @@ class Options:
     """Per-pair computation options, with the gtalign command line's codes.
 
     Defaults are the command line's defaults except ``nodetailedsearch``,
-    which must be 1 (the spatial-index search stage is not in this library).
+    which is 1 here (the spatial-index detailed search off); the command
+    line's default, --speed 9, is ``Options.speed(9)``.
     """
     refinement: int = 1        # -1 log, 0 coarse, 1 one (default), 2 full, 3 full in both phases
     depth: int = 2
@@ -74,22 +77,35 @@ class Options:
     twotmscore: int = 0
     polish_steps: int = 0      # adjoint polishing of the final transforms (this library only)
     presimilarity: float = 0.0  # --pre-similarity (0: off)
+    trigger: int = 50          # detailed search: --trigger (percent)
+    nbranches: int = 5         # --nbranches
+    gapcost: int = 1           # --gapcost code: -0.8, -1.2, -3.0
+    seedrule: int = 1          # --seedrule code: fragments, 64-, 128-residue frames
+    window: int = 256          # --window
 
     @classmethod
     def speed(cls, level: int, **kw) -> "Options":
-        """The --speed presets that keep the detailed search off
-        (gtalign.cpp:833-867): 13 = --no-detailed-search --refinement=0
-        --convergence=2."""
-        if level != 13:
-            raise GTBError(4, "only --speed=13 runs without the detailed search")
-        o = cls(refinement=0, convergence=2, **kw)
-        return o
+        """The --speed presets (gtalign.cpp:833-867, gtalign.h:189-208):
+        13 = --no-detailed-search --refinement=0 --convergence=2; 10..12 =
+        --depth=3 with --trigger 0/20/50, --refinement=0 --convergence=2; 7..9
+        = --depth=2 with --trigger 0/20/50 (9 is the command line's default).
+        The presets at --depth 0 and 1 (0..6) are not available."""
+        if level == 13:
+            return cls(refinement=0, convergence=2, **kw)
+        trig = {0: 0, 1: 20, 2: 50}
+        if 10 <= level <= 12:
+            return cls(nodetailedsearch=0, depth=3, trigger=trig[level - 10], refinement=0,
+                       convergence=2, **kw)
+        if 7 <= level <= 9:
+            return cls(nodetailedsearch=0, depth=2, trigger=trig[level - 7], **kw)
+        raise GTBError(4, "--speed %d (detailed search at --depth 0 or 1) is not available" % level)
 
     def _c(self) -> _COptions:
         return _COptions(self.refinement, self.depth, self.convergence, self.prescore,
                          self.symmetric, self.referenced, self.nodeletions,
                          self.nodetailedsearch, self.addsearchbyss, self.twotmscore,
-                         self.polish_steps, self.presimilarity)
+                         self.polish_steps, self.presimilarity, self.trigger, self.nbranches,
+                         self.gapcost, self.seedrule, self.window)
 
 
 _lib = None
@@ -116,6 +132,11 @@ def load_library():
     L.gtb_last_launch_count.restype = ctypes.c_longlong
     L.gtb_last_timings.argtypes = [vp, fp]
     L.gtb_last_timings.restype = ctypes.c_int
+    L.gtb_process_block_ndx.argtypes = [vp, ctypes.c_float, vp, vp, vp, vp, vp, vp,
+                                        ctypes.POINTER(_CResults)]
+    L.gtb_process_block_ndx.restype = ctypes.c_int
+    L.gtb_build_index.argtypes = [vp, vp, vp]
+    L.gtb_build_index.restype = ctypes.c_int
     L.gtb_last_work.argtypes = [vp, ctypes.POINTER(ctypes.c_ulonglong)]
     L.gtb_last_work.restype = ctypes.c_int
     L.gtb_set_wait_limit.argtypes = [vp, ctypes.c_longlong]
@@ -164,6 +185,20 @@ def pack_fields(s: SoA) -> PackedBlock:
         beg[f] = a.ctypes.data
         end[f] = a.ctypes.data + a.nbytes
     return PackedBlock(arrays, beg, end, n, N)
+
+
+def build_index(s: SoA) -> Tuple[np.ndarray, ...]:
+    """The block's index trees as the reference's reader makes them
+    (gtb_build_index): node x, y, z (float32), left and right child and
+    residue (int32), one entry per residue."""
+    L = load_library()
+    pk = pack_fields(s)
+    arrs = [np.zeros(s.total, np.float32) for _ in range(3)] + [np.zeros(s.total, np.int32) for _ in range(3)]
+    ndx = (ctypes.c_void_p * 6)(*[a.ctypes.data for a in arrs])
+    st = L.gtb_build_index(pk.beg, pk.end, ndx)
+    if st != 0:
+        raise GTBError(st, "gtb_build_index failed")
+    return tuple(arrs)
 
 
 @dataclass
@@ -265,13 +300,17 @@ class GTalignB200:
 
     def process_block(self, queries: SoA, refs: SoA, scorethld: float = 0.5,
                       alignments: bool = True, numerr: bool = True,
-                      secstr: bool = False) -> BlockResult:
+                      secstr: bool = False, qndx=None, rndx=None) -> BlockResult:
+        """qndx/rndx (build_index): the blocks' index trees as a reader made
+        them; without them the library builds the same when it needs them."""
         qb, rb = pack_fields(queries), pack_fields(refs)
-        return self.process_packed(qb, rb, scorethld, alignments, numerr, secstr)
+        return self.process_packed(qb, rb, scorethld, alignments, numerr, secstr, qndx=qndx,
+                                   rndx=rndx)
 
     def process_packed(self, qb: PackedBlock, rb: PackedBlock, scorethld: float = 0.5,
                        alignments: bool = True, numerr: bool = True,
-                       secstr: bool = False, out: Optional[dict] = None) -> BlockResult:
+                       secstr: bool = False, out: Optional[dict] = None,
+                       qndx=None, rndx=None) -> BlockResult:
         nq, nr = qb.n, rb.n
         if out is None:
             out = {}
@@ -293,8 +332,14 @@ class GTalignB200:
                         err.ctypes.data if err is not None else None,
                         qss.ctypes.data if qss is not None else None,
                         rss.ctypes.data if rss is not None else None)
-        st = self.lib.gtb_process_block(self._h, float(scorethld), qb.beg, qb.end, rb.beg, rb.end,
-                                        ctypes.byref(res))
+        if qndx is not None and rndx is not None:
+            qn = (ctypes.c_void_p * 6)(*[a.ctypes.data for a in qndx])
+            rn = (ctypes.c_void_p * 6)(*[a.ctypes.data for a in rndx])
+            st = self.lib.gtb_process_block_ndx(self._h, float(scorethld), qb.beg, qb.end, qn,
+                                                rb.beg, rb.end, rn, ctypes.byref(res))
+        else:
+            st = self.lib.gtb_process_block(self._h, float(scorethld), qb.beg, qb.end, rb.beg,
+                                            rb.end, ctypes.byref(res))
         if st != 0:
             raise GTBError(st, self.lib.gtb_last_error(self._h).decode())
         tms = np.zeros(7, np.float32)

@@ -9,7 +9,8 @@ PKG = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(PKG)
 CSRC = os.path.join(PKG, "csrc")
 LIB = os.path.join(PKG, "libgtb200.so")
-SOURCES = ["gtb_kernels.cu", "gtb_api.cu", "gtb_adjoint.cu", "gtb_noalloc.cu", "gtb_cluster.cu"]
+SOURCES = ["gtb_kernels.cu", "gtb_api.cu", "gtb_adjoint.cu", "gtb_noalloc.cu", "gtb_cluster.cu",
+           "gtb_index.cpp", "gtb_frg3.cu"]
 HEADERS = ["gtb_device.cuh", "gtb_kernels.cuh", "gtb_gonnet.h"]
 
 NVCC_FLAGS = [
@@ -44,7 +45,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
     os.makedirs(objdir, exist_ok=True)
     objs = []
     for s in SOURCES:
-        obj = os.path.join(objdir, s.replace(".cu", ".o"))
+        obj = os.path.join(objdir, os.path.splitext(s)[0] + ".o")
         cmd = [nvcc()] + NVCC_FLAGS + ["-I", os.path.join(ROOT, "include"), "-c",
                                        os.path.join(CSRC, s), "-o", obj]
         if verbose:

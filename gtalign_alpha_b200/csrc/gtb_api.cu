@@ -141,9 +141,19 @@ extern "C" gtb_status gtb_set_wait_limit(gtb_handle* h, long long spins) {
 static gtb_status check_options(gtb_handle* h) {
     const gtb_options& o = h->opts;
     if (!o.nodetailedsearch) {
-        snprintf(h->err, sizeof(h->err),
-                 "the spatial-index detailed search is not implemented: set nodetailedsearch=1");
-        return GTB_ERR_UNSUPPORTED;
+        if (o.trigger < 0 || o.trigger > 100 || o.nbranches < 1 || o.nbranches > F3_NBMAX ||
+            o.gapcost < 0 || o.gapcost > 2 || o.seedrule < 0 || o.seedrule > 2 ||
+            o.window < 256 || o.window > 512) {
+            snprintf(h->err, sizeof(h->err), "detailed-search option out of range");
+            return GTB_ERR_ARG;
+        }
+        if (o.depth < 2) {
+            // --depth deep/high add the secondary configuration sections
+            // (MpStageFrg3.cpp:196-215, 249-266), not built here
+            snprintf(h->err, sizeof(h->err),
+                     "the detailed search at --depth 0 or 1 is not implemented (use 2 or 3)");
+            return GTB_ERR_UNSUPPORTED;
+        }
     }
     if (o.refinement < GTB_REFINEMENT_LOG || o.refinement > GTB_REFINEMENT_FULLA) {
         snprintf(h->err, sizeof(h->err), "--refinement %d out of -1..3", o.refinement);
@@ -173,6 +183,9 @@ struct DevBlock {
     const float4 *q4, *r4;
     const unsigned char *qa, *ra;
     char *qs, *rs;
+    // index trees (null: none)
+    const float *qnx = nullptr, *qny = nullptr, *qnz = nullptr, *rnx = nullptr, *rny = nullptr, *rnz = nullptr;
+    const int *qnl = nullptr, *qnr = nullptr, *qno = nullptr, *rnl = nullptr, *rnr = nullptr, *rno = nullptr;
     std::vector<int> hqlen, hrlen;
 };
 
@@ -184,9 +197,11 @@ struct BatchBufs {
 
 static size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 
-// Bytes of device scratch one pair needs.
-static size_t pair_bytes(int lq, int lr, bool strings) {
+// Bytes of device scratch one pair needs (f3: the detailed search's local
+// score matrix, slots and branches).
+static size_t pair_bytes(int lq, int lr, bool strings, bool f3 = false) {
     size_t b = (size_t)gtb::bt_words(lq, lr) * 4;     // traceback words
+    if (f3) b += (size_t)lq * lr + (size_t)F3_NTOP * 14 * 4 + (size_t)F3_NBMAX * 13 * 4 + 13 * 4 + 8;
     b += (size_t)lr * 4;                               // DP row buffer
     b += (size_t)std::min(lq, lr) * 28;                // aligned pairs + coordinates
     if (strings) b += (size_t)5 * (lq + lr + 1);       // alignment rows
@@ -249,6 +264,19 @@ static gtb_status run_block(gtb_handle* h, const DevBlock& D, float scorethld,
     // (CuBatch.cu:459-462)
     B.presim = (0.f < o.presimilarity && PRESIM_EDGE < B.qmax && PRESIM_EDGE < B.rmax) ? o.presimilarity : 0.f;
     B.symmetric = o.symmetric; B.nodeletions = o.nodeletions;
+    B.f3 = o.nodetailedsearch ? 0 : 1;
+    if (B.f3) {
+        if (!D.qnx || !D.rnx) {
+            snprintf(h->err, sizeof(h->err), "the detailed search needs the blocks' index trees");
+            return GTB_ERR_ARG;
+        }
+        B.qnx = D.qnx; B.qny = D.qny; B.qnz = D.qnz; B.qnl = D.qnl; B.qnr = D.qnr; B.qno = D.qno;
+        B.rnx = D.rnx; B.rny = D.rny; B.rnz = D.rnz; B.rnl = D.rnl; B.rnr = D.rnr; B.rno = D.rno;
+        B.f3trigger = o.trigger; B.f3nbranches = o.nbranches;
+        B.f3gapcost = o.gapcost == 0 ? -0.8f : (o.gapcost == 1 ? -1.2f : -3.0f);
+        B.f3seedrule = o.seedrule == 0 ? 0 : (o.seedrule == 1 ? 64 : 128);
+        B.f3window = o.window;
+    }
     const bool strings = sink != nullptr;
 
     size_t fr = 0, tot = 0;
@@ -276,11 +304,12 @@ static gtb_status run_block(gtb_handle* h, const DevBlock& D, float scorethld,
     auto launch_sub = [&](long long q0, int np, int j, int evset) -> gtb_status {
         cudaStream_t st = h->sub[j];
         std::vector<long long>& ov = offv[j];
-        ov.assign(4 * (size_t)(np + 1), 0);
+        ov.assign((B.f3 ? 5 : 4) * (size_t)(np + 1), 0);
         long long* off_bt = ov.data();
         long long* off_row = off_bt + (np + 1);
         long long* off_aln = off_bt + 2 * (np + 1);
         long long* off_str = off_bt + 3 * (np + 1);
+        long long* off_lsm = B.f3 ? off_bt + 4 * (np + 1) : nullptr;
         // seed work items: pairs with more offsets than one CTA takes are split
         std::vector<int>& ffn = ffv[j];
         ffn.assign(np, 1);
@@ -293,6 +322,7 @@ static gtb_status run_block(gtb_handle* h, const DevBlock& D, float scorethld,
             off_row[i + 1] = off_row[i] + lr;
             off_aln[i + 1] = off_aln[i] + std::min(lq, lr);
             off_str[i + 1] = off_str[i] + (strings ? 5LL * (lq + lr + 1) : 0);
+            if (off_lsm) off_lsm[i + 1] = off_lsm[i] + (long long)lq * lr;
             int n1, silo, sihi, prv;
             gtb::seed_range(lq, lr, B.qmax, B.qmin, B.rmax, B.rmin, B.stepinit, n1, silo, sihi, prv);
             int cnt = sihi - silo + 1;
@@ -358,7 +388,7 @@ static gtb_status run_block(gtb_handle* h, const DevBlock& D, float scorethld,
         size_t o_tgr = carve((size_t)np * 12 * sizeof(float));
         size_t o_out = carve((size_t)np * 16 * sizeof(float));
         size_t o_err = carve((size_t)np * 4 * sizeof(float));
-        size_t o_offs = carve((size_t)(np + 1) * 4 * sizeof(long long));
+        size_t o_offs = carve((size_t)(np + 1) * (B.f3 ? 5 : 4) * sizeof(long long));
         size_t o_bt = carve((size_t)off_bt[np] * sizeof(unsigned));
         size_t o_row = carve((size_t)off_row[np] * sizeof(float));
         size_t o_aln = carve((size_t)off_aln[np] * sizeof(unsigned));
@@ -376,6 +406,14 @@ static gtb_status run_block(gtb_handle* h, const DevBlock& D, float scorethld,
         size_t o_dwe = nl ? carve(sizeof(int)) : 0;
         size_t o_rll = nlmax ? carve((size_t)(2 * nlmax + 1) * sizeof(int)) : 0;
         size_t o_rlc = nlmax ? carve((size_t)nlmax * gtb::RLW_WARPS * gtb::RLW_CAND * sizeof(float)) : 0;
+        // detailed search: local score matrices, slots, DP scores, branches
+        size_t o_lsm = B.f3 ? carve((size_t)std::max<long long>(off_lsm[np], 1)) : 0;
+        size_t o_f3s = B.f3 ? carve((size_t)np * F3_NTOP * 13 * sizeof(float)) : 0;
+        size_t o_f3d = B.f3 ? carve((size_t)np * F3_NTOP * sizeof(float)) : 0;
+        size_t o_f3a = B.f3 ? carve((size_t)np * F3_NBMAX * 12 * sizeof(float)) : 0;
+        size_t o_f3o = B.f3 ? carve((size_t)np * F3_NBMAX) : 0;
+        size_t o_f32 = B.f3 ? carve((size_t)np * 13 * sizeof(float)) : 0;
+        size_t o_f3v = B.f3 ? carve((size_t)np * sizeof(unsigned)) : 0;
         char* base = nullptr;
         CK(cudaMallocAsync((void**)&base, sz, st));
         Bat T{};
@@ -398,6 +436,19 @@ static gtb_status run_block(gtb_handle* h, const DevBlock& D, float scorethld,
         T.rlist = (int*)(base + o_rl); T.rhist = (int*)(base + o_rh);
         T.launches = &h->launches;
         T.lerr = &lerr;
+        T.alt_rci = -1;
+        T.vskip = nullptr;
+        if (B.f3) {
+            T.off_lsm = offs + 4 * (np + 1);
+            T.lsm = (unsigned char*)(base + o_lsm);
+            T.f3slot = (float*)(base + o_f3s);
+            T.f3dps = (float*)(base + o_f3d);
+            T.f3alt = (float*)(base + o_f3a);
+            T.f3ok = (unsigned char*)(base + o_f3o);
+            T.tfm_2nd = (float*)(base + o_f32);
+            T.best2 = T.tfm_2nd + (size_t)np * 12;
+            T.vskip_mask = (unsigned*)(base + o_f3v);
+        }
         T.work = h->d_work;
         T.dw_spin = h->wait_limit;
         T.nff = np; T.ff_pair = nullptr; T.ff_chunk = nullptr; T.ff_nch = nullptr; T.ff_key = nullptr;
@@ -423,7 +474,8 @@ static gtb_status run_block(gtb_handle* h, const DevBlock& D, float scorethld,
                                cudaMemcpyHostToDevice, st));
             CK(cudaMemsetAsync(T.dw_err, 0, sizeof(int), st));
         }
-        CK(cudaMemcpyAsync(offs, off_bt, 4 * (size_t)(np + 1) * sizeof(long long), cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(offs, off_bt, (B.f3 ? 5 : 4) * (size_t)(np + 1) * sizeof(long long),
+                           cudaMemcpyHostToDevice, st));
         if (split) {
             int* di = (int*)(base + o_ffi);
             int* dn = (int*)(base + o_ffn);
@@ -475,7 +527,7 @@ static gtb_status run_block(gtb_handle* h, const DevBlock& D, float scorethld,
         long long p1 = p0;
         while (p1 < npairs && p1 - p0 < maxbatch) {
             int lq = D.hqlen[p1 / D.nr], lr = D.hrlen[p1 % D.nr];
-            size_t b = pair_bytes(lq, lr, strings);
+            size_t b = pair_bytes(lq, lr, strings, B.f3 != 0);
             if (used + b > budget && p1 > p0) break;
             used += b;
             p1++;
@@ -638,10 +690,57 @@ struct gtb_block {
     cudaStream_t st = nullptr;       // stream of the allocation and of the free
     unsigned char* rsd = nullptr;
     char* ss = nullptr;
+    // index trees (null: none): node x, y, z; left, right, residue
+    float *nx = nullptr, *ny = nullptr, *nz = nullptr;
+    int *nl = nullptr, *nr = nullptr, *no = nullptr;
 };
 
-static gtb_status upload_block(gtb_handle* h, const HostSoA& S, gtb_block* b) {
+// the detailed search needs the blocks' index trees
+static bool needs_index(const gtb_handle* h) { return h->opts.nodetailedsearch == 0; }
+
+// ndxbeg: the block's index fields (host), or null: built here when the
+// detailed search needs them
+static gtb_status upload_block(gtb_handle* h, const HostSoA& S, gtb_block* b,
+                               char* const* ndxbeg = nullptr) {
     cudaStream_t st = h->st;
+    const bool ndx = needs_index(h);
+    std::vector<float> hf;
+    std::vector<int> hi;
+    const void* src[GTB_NNDXFIELDS] = {};
+    if (ndx) {
+        if (ndxbeg) {
+            for (int f = 0; f < GTB_NNDXFIELDS; f++) {
+                if (!ndxbeg[f]) { snprintf(h->err, sizeof(h->err), "null index field %d", f); return GTB_ERR_ARG; }
+                src[f] = ndxbeg[f];
+            }
+            // a caller's trees are walked on the device: every child must be a
+            // node of the same structure (or -1) and every residue its own
+            const int* nl = (const int*)ndxbeg[GTB_NDX_LEFT];
+            const int* nr = (const int*)ndxbeg[GTB_NDX_RIGHT];
+            const int* no = (const int*)ndxbeg[GTB_NDX_ORGNDX];
+            for (int si = 0; si < S.n; si++) {
+                const long long a = S.off[si];
+                const int L = S.len[si];
+                for (int k = 0; k < L; k++) {
+                    if (nl[a + k] < -1 || nl[a + k] >= L || nr[a + k] < -1 || nr[a + k] >= L ||
+                        no[a + k] < 0 || no[a + k] >= L) {
+                        snprintf(h->err, sizeof(h->err), "index tree of structure %d: node %d out of range", si, k);
+                        return GTB_ERR_ARG;
+                    }
+                }
+            }
+        } else {
+            hf.resize((size_t)3 * S.npos);
+            hi.resize((size_t)3 * S.npos);
+            if (!gtb::build_index_host(S.n, S.len, S.dist, S.x, S.y, S.z, S.npos, hf.data(),
+                                       hf.data() + S.npos, hf.data() + 2 * S.npos, hi.data(),
+                                       hi.data() + S.npos, hi.data() + 2 * S.npos)) {
+                snprintf(h->err, sizeof(h->err), "inconsistent block for the index");
+                return GTB_ERR_ARG;
+            }
+            for (int f = 0; f < 3; f++) { src[f] = hf.data() + f * S.npos; src[3 + f] = hi.data() + f * S.npos; }
+        }
+    }
     b->n = S.n; b->npos = S.npos;
     b->len.assign(S.len, S.len + S.n);
     b->off = S.off; b->mol = S.mol;
@@ -651,6 +750,7 @@ static gtb_status upload_block(gtb_handle* h, const HostSoA& S, gtb_block* b) {
     size_t ox = carve(S.npos * 4), oy = carve(S.npos * 4), oz = carve(S.npos * 4);
     size_t oa = carve(S.npos), os = carve(S.npos);
     size_t o4 = carve(S.npos * 16);
+    size_t on = ndx ? carve((size_t)S.npos * 4 * GTB_NNDXFIELDS) : 0;
     // from the device's memory pool (kept between calls), in stream order
     CK(cudaMallocAsync((void**)&b->dbase, sz, st));
     b->st = st;
@@ -659,6 +759,15 @@ static gtb_status upload_block(gtb_handle* h, const HostSoA& S, gtb_block* b) {
     b->x = (float*)(d + ox); b->y = (float*)(d + oy); b->z = (float*)(d + oz);
     b->rsd = (unsigned char*)(d + oa); b->ss = d + os;
     b->c4 = (float4*)(d + o4);
+    if (ndx) {
+        float* nf = (float*)(d + on);
+        int* ni = (int*)(nf + 3 * S.npos);
+        b->nx = nf; b->ny = nf + S.npos; b->nz = nf + 2 * S.npos;
+        b->nl = ni; b->nr = ni + S.npos; b->no = ni + 2 * S.npos;
+        void* dst[GTB_NNDXFIELDS] = {b->nx, b->ny, b->nz, b->nl, b->nr, b->no};
+        for (int f = 0; f < GTB_NNDXFIELDS; f++)
+            CK(cudaMemcpyAsync(dst[f], src[f], (size_t)S.npos * 4, cudaMemcpyHostToDevice, st));
+    }
     CK(cudaMemcpyAsync(b->dlen, S.len, S.n * 4, cudaMemcpyHostToDevice, st));
     CK(cudaMemcpyAsync(b->doff, S.off.data(), S.n * 4, cudaMemcpyHostToDevice, st));
     CK(cudaMemcpyAsync(b->dmol, S.mol.data(), S.n * 4, cudaMemcpyHostToDevice, st));
@@ -681,6 +790,11 @@ static void free_block(gtb_block* b) {
 
 extern "C" gtb_status gtb_block_upload(gtb_handle* h, char* const* pmbeg, char* const* pmend,
                                        gtb_block** out) {
+    return gtb_block_upload_ndx(h, pmbeg, pmend, nullptr, out);
+}
+
+extern "C" gtb_status gtb_block_upload_ndx(gtb_handle* h, char* const* pmbeg, char* const* pmend,
+                                           char* const* ndxbeg, gtb_block** out) {
     if (!h || !out) return GTB_ERR_ARG;
     *out = nullptr;
     h->err[0] = 0;
@@ -689,8 +803,8 @@ extern "C" gtb_status gtb_block_upload(gtb_handle* h, char* const* pmbeg, char* 
     if (s != GTB_OK) return s;
     CK(cudaSetDevice(h->dev));
     gtb_block* b = new gtb_block();
-    s = upload_block(h, S, b);
-    if (s != GTB_OK) { free_block(b); return s; }
+    s = upload_block(h, S, b, ndxbeg);
+    if (s != GTB_OK) { cudaStreamSynchronize(h->st); free_block(b); return s; }
     CK(cudaStreamSynchronize(h->st));
     *out = b;
     return GTB_OK;
@@ -709,6 +823,8 @@ static DevBlock make_devblock(const gtb_block* Q, const gtb_block* R) {
     D.qx = Q->x; D.qy = Q->y; D.qz = Q->z; D.rx = R->x; D.ry = R->y; D.rz = R->z;
     D.q4 = Q->c4; D.r4 = R->c4;
     D.qa = Q->rsd; D.ra = R->rsd; D.qs = Q->ss; D.rs = R->ss;
+    D.qnx = Q->nx; D.qny = Q->ny; D.qnz = Q->nz; D.qnl = Q->nl; D.qnr = Q->nr; D.qno = Q->no;
+    D.rnx = R->nx; D.rny = R->ny; D.rnz = R->nz; D.rnl = R->nl; D.rnr = R->nr; D.rno = R->no;
     D.hqlen = Q->len; D.hrlen = R->len;
     return D;
 }
@@ -731,6 +847,15 @@ extern "C" gtb_status gtb_process_block(gtb_handle* h, float scorethld,
                                         char* const* querypmbeg, char* const* querypmend,
                                         char* const* bdbCpmbeg, char* const* bdbCpmend,
                                         gtb_results* out) {
+    return gtb_process_block_ndx(h, scorethld, querypmbeg, querypmend, nullptr, bdbCpmbeg,
+                                 bdbCpmend, nullptr, out);
+}
+
+extern "C" gtb_status gtb_process_block_ndx(gtb_handle* h, float scorethld,
+                                            char* const* querypmbeg, char* const* querypmend,
+                                            char* const* queryndxpmbeg,
+                                            char* const* bdbCpmbeg, char* const* bdbCpmend,
+                                            char* const* bdbCndxpmbeg, gtb_results* out) {
     if (!h) return GTB_ERR_ARG;
     h->err[0] = 0;
     if (!out || !out->alndata || !out->tfm) { snprintf(h->err, sizeof(h->err), "null result buffers"); return GTB_ERR_ARG; }
@@ -745,8 +870,8 @@ extern "C" gtb_status gtb_process_block(gtb_handle* h, float scorethld,
     cudaStream_t st = h->st;
     gtb_block* qb = new gtb_block();
     gtb_block* rb = new gtb_block();
-    s = upload_block(h, Q, qb);
-    if (s == GTB_OK) s = upload_block(h, R, rb);
+    s = upload_block(h, Q, qb, queryndxpmbeg);
+    if (s == GTB_OK) s = upload_block(h, R, rb, bdbCndxpmbeg);
     if (s != GTB_OK) { cudaStreamSynchronize(st); free_block(qb); free_block(rb); return s; }
     DevBlock D = make_devblock(qb, rb);
 

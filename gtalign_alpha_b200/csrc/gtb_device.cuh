@@ -190,8 +190,10 @@ __device__ __forceinline__ int qcp_rotation(const double (&S)[3][3], double (&R)
 }
 
 // sums v: [0..8] sum q_i r_j, [9..11] sum q, [12..14] sum r, [15] n.
-// swap: solve with the reference rotated onto the query, then invert
-// (--symmetric for a shorter query, MpStageBase.h:1000-1023).
+// swap 1: solve with the reference rotated onto the query, then invert
+// (--symmetric for a shorter query, MpStageBase.h:1000-1023); swap 2: the
+// reference rotated onto the query, not inverted (the detailed search's
+// orientation towards the longer structure, MpStageBase.h:1086-1101).
 static __device__ __noinline__ void solve_sums(const float* v, int swap, float* tfm) {
     double dn = (double)v[15];
     double mq[3], mr[3], S[3][3];
@@ -223,6 +225,14 @@ static __device__ __noinline__ void solve_sums(const float* v, int swap, float* 
                                                  __dmul_rn(R[3 * i + 2], mq[2])));
             tfm[9 + i] = (float)t;
         }
+#pragma unroll
+        for (int k = 0; k < 9; k++) tfm[k] = (float)R[k];
+    } else if (swap == 2) {
+#pragma unroll
+        for (int i = 0; i < 3; i++)
+            tfm[9 + i] = (float)__dsub_rn(mq[i], __dadd_rn(__dadd_rn(__dmul_rn(R[3 * i], mr[0]),
+                                                                     __dmul_rn(R[3 * i + 1], mr[1])),
+                                                           __dmul_rn(R[3 * i + 2], mr[2])));
 #pragma unroll
         for (int k = 0; k < 9; k++) tfm[k] = (float)R[k];
     } else {

@@ -55,6 +55,18 @@ __device__ __forceinline__ void work_add(const Bat& T, int kind, unsigned long l
         atomicAdd(T.work + kind * WORK_SLOTS + (blockIdx.x & (WORK_SLOTS - 1)), v);
 }
 
+// the transform a DP of pair i uses (DpTfm)
+__device__ __forceinline__ const float* dp_tfm(const Bat& T, int i, int tfmsrc) {
+    if (tfmsrc == DP_TFM_GRAND) return T.tfm_gr + i * 12;
+    if (tfmsrc == DP_TFM_ALT) return T.f3alt + ((long long)i * F3_NBMAX + T.alt_rci) * 12;
+    if (tfmsrc == DP_TFM_2ND) return T.tfm_2nd + i * 12;
+    return T.tfm_ib + i * 12;
+}
+// the detailed search's branch T.alt_rci of pair i is empty
+__device__ __forceinline__ bool alt_empty(const Bat& T, int i) {
+    return T.f3ok && T.alt_rci >= 0 && !T.f3ok[(long long)i * F3_NBMAX + T.alt_rci];
+}
+
 __device__ __forceinline__ int pair_qi(const Blk& B, const Bat& T, int i) {
     return (int)((T.p0 + i) / B.nr);
 }
@@ -693,6 +705,7 @@ __device__ __forceinline__ int dlist_bucket(const Blk& B, const Bat& T, int i, i
     int skipmask = skipmode == 0 ? (CONV_LOWTMSC | CONV_SCOREDP) : CONV_LOWTMSC;
     if (T.flags[i] & skipmask) return -1;
     if (T.dw_mark && T.dw_mark[i]) return -1;
+    if (alt_empty(T, i)) return -1;
     int qi = pair_qi(B, T, i), ri = pair_ri(B, T, i);
     long long cells = (long long)B.qlen[qi] * B.rlen[ri];
     long long b = cells >> 8;
@@ -710,6 +723,26 @@ __global__ void k_dlist_fill(Blk B, Bat T, int skipmode) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= T.np) return;
     int b = dlist_bucket(B, T, i, skipmode);
+    if (b >= 0) T.rlist[atomicAdd(&T.rhist[b], 1)] = i;
+}
+
+// pair list without any flag of skipmask (every size, wavefront pairs too)
+__device__ __forceinline__ int plist_bucket(const Blk& B, const Bat& T, int i, int skipmask) {
+    if (T.flags[i] & skipmask) return -1;
+    int qi = pair_qi(B, T, i), ri = pair_ri(B, T, i);
+    long long b = ((long long)B.qlen[qi] * B.rlen[ri]) >> 8;
+    return RL_NB - 1 - (int)(b < RL_NB - 1 ? b : RL_NB - 1);
+}
+__global__ void k_plist_count(Blk B, Bat T, int skipmask) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= T.np) return;
+    int b = plist_bucket(B, T, i, skipmask);
+    if (b >= 0) atomicAdd(&T.rhist[b], 1);
+}
+__global__ void k_plist_fill(Blk B, Bat T, int skipmask) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= T.np) return;
+    int b = plist_bucket(B, T, i, skipmask);
     if (b >= 0) T.rlist[atomicAdd(&T.rhist[b], 1)] = i;
 }
 
@@ -1098,12 +1131,20 @@ __global__ void __launch_bounds__(RF_WARPS * 32) k_refine(Blk B, Bat T) {
                 if (kv < V.total) {
                     int fl, kf;
                     variants_get(V, vk, n, kv, si, vndx, vpos, fl, kf);
-                    kind = PK_FRAG; k0 = kf; k1 = kf + fl;
-                    best = best_init; cit = 0;
+                    if (MODE == RM_DP && T.vskip && si < 32 && ((T.vskip[i] >> si) & 1u)) {
+                        need = true;       // a variant the detailed search's slots rule out
+                    } else {
+                        kind = PK_FRAG; k0 = kf; k1 = kf + fl;
+                        best = best_init; cit = 0;
+                    }
                 }
             }
         }
-        if (__ballot_sync(FULL, kind != PK_IDLE) == 0) break;
+        if (__ballot_sync(FULL, kind != PK_IDLE) == 0) {
+            // lanes that passed over a skipped variant take the next one
+            if (MODE == RM_DP && T.vskip && __any_sync(FULL, need && nextk < V.total)) continue;
+            break;
+        }
         float v[16], m3;
         const float sc = lane_pass(G, kind, k0, k1, tfm, pd02, pchk, d82, thr, m3mode, v, m3,
                                    lane % RF_LPP);
@@ -1326,7 +1367,8 @@ void launch_refine(int mode, const Blk& B, const Bat& T, cudaStream_t st, bool f
 // score of the residues, no transform; a cell reached diagonally stores its
 // value + DPSS_C, a reader takes the offset off again, the gap cost is paid
 // once when leaving such a cell; the border reads as a diagonal cell of 0).
-template <int R, bool gap0, int SC, bool WAVE>
+// SCOREONLY: no traceback words; the last cell's value goes to *fin.
+template <int R, bool gap0, int SC, bool WAVE, bool SCOREONLY = false>
 __device__ __forceinline__ bool dp_pair(const float* t, float d02, float gcost, int lq, int lr,
                                         const float* qx, const float* qy, const float* qz,
                                         const float4* r4, const char* qs, const char* rs,
@@ -1334,7 +1376,7 @@ __device__ __forceinline__ bool dp_pair(const float* t, float d02, float gcost, 
                                         float* row, unsigned* bt, int lane, int s_first = 0,
                                         int s_step = 1, volatile int* prog = nullptr,
                                         volatile int* err = nullptr,
-                                        long long spin = DP_WAVE_SPIN_DEFAULT) {
+                                        long long spin = DP_WAVE_SPIN_DEFAULT, float* fin = nullptr) {
     constexpr bool usess = SC == DP_SC_TFMSS, ssrr = SC == DP_SC_SSRR;
     constexpr float BND = ssrr ? DPSS_C : 0.f;   // the matrix border
     constexpr int ROWS = 32 * R, SPW = 16 / R;
@@ -1362,8 +1404,9 @@ __device__ __forceinline__ bool dp_pair(const float* t, float d02, float gcost, 
             }
         }
         float uplast = BND, rb = BND;
-        unsigned* bts = bt + (long long)s * ngrp * 32 + lane;
+        unsigned* bts = SCOREONLY ? nullptr : bt + (long long)s * ngrp * 32 + lane;
         const bool full = (s + 1) * ROWS <= lq;    // every lane has R rows
+        const int lastr = (lq - 1) - s * ROWS - lane * R;   // the last row among this lane's (if 0..R-1)
         __syncwarp();
         for (int g = 0; g < ngrp; g++) {
             unsigned acc = 0u;
@@ -1434,7 +1477,8 @@ __device__ __forceinline__ bool dp_pair(const float* t, float d02, float gcost, 
                                 dg = h[r];   // (row r, j-1): the next row's diagonal
                                 up = w;      // (row r, j):   the next row's up
                                 h[r] = w;
-                                acc |= (unsigned)bk << (2 * R * u + 2 * r);
+                                if (SCOREONLY) { if (r == lastr && j == lr - 1) *fin = w; }
+                                else acc |= (unsigned)bk << (2 * R * u + 2 * r);
                             }
                         }
                         if (lane == 31 && (!CHK || nv == R)) row[j] = h[R - 1];
@@ -1444,7 +1488,7 @@ __device__ __forceinline__ bool dp_pair(const float* t, float d02, float gcost, 
             };
             if (full && g * SPW >= 31 && (g + 1) * SPW <= lr) steps(std::false_type{});
             else steps(std::true_type{});
-            bts[g * 32] = acc;
+            if (!SCOREONLY) bts[g * 32] = acc;
             if (WAVE && lane == 31) {
                 __threadfence();              // this group's row values before the count
                 prog[s] = (g + 1) * SPW;
@@ -1465,7 +1509,7 @@ __global__ void __launch_bounds__(128) k_dp(Blk B, Bat T, int tfmsrc, float gcos
     int qi = pair_qi(B, T, i), ri = pair_ri(B, T, i);
     int lq = B.qlen[qi], lr = B.rlen[ri];
     int ml = lq < lr ? lq : lr;
-    const float* tsrc = (tfmsrc == DP_TFM_GRAND ? T.tfm_gr : T.tfm_ib) + i * 12;
+    const float* tsrc = dp_tfm(T, i, tfmsrc);
     float t[12];
 #pragma unroll
     for (int f = 0; f < 12; f++) t[f] = tsrc[f];
@@ -1503,10 +1547,11 @@ __global__ void __launch_bounds__(32) k_dp_wave(Blk B, Bat T, int tfmsrc, float 
     int flags = T.flags[i];
     int skipmask = skipmode == 0 ? (CONV_LOWTMSC | CONV_SCOREDP) : CONV_LOWTMSC;
     if (flags & skipmask) return;                  // the same for every CTA of the pair
+    if (alt_empty(T, i)) return;
     int qi = pair_qi(B, T, i), ri = pair_ri(B, T, i);
     int lq = B.qlen[qi], lr = B.rlen[ri];
     int ml = lq < lr ? lq : lr;
-    const float* tsrc = (tfmsrc == DP_TFM_GRAND ? T.tfm_gr : T.tfm_ib) + i * 12;
+    const float* tsrc = dp_tfm(T, i, tfmsrc);
     float t[12];
 #pragma unroll
     for (int f = 0; f < 12; f++) t[f] = tsrc[f];
@@ -1587,6 +1632,63 @@ void launch_dp(const Blk& B, const Bat& T, int tfmsrc, int gap0, float gcost, in
     GTB_LAUNCHED(T);
 }
 
+void launch_pair_list(const Blk& B, const Bat& T, int skipmask, cudaStream_t st) {
+    cudaMemsetAsync(T.rhist, 0, (RL_NB + 1) * sizeof(int), st);
+    const int nb = (T.np + 255) / 256;
+    k_plist_count<<<nb, 256, 0, st>>>(B, T, skipmask);
+    k_rlist_scan<<<1, 1024, 0, st>>>(T);
+    k_plist_fill<<<nb, 256, 0, st>>>(B, T, skipmask);
+    if (T.launches) (*T.launches) += 3;
+}
+
+// Detailed search: the DP scores of a pair's fragment slots
+// (ExecDPScore128xKernel, MpDPHub.cpp:389-645): for every slot with a
+// positive score, the last cell of the gap-0 DP under the slot's transform
+// (search d0), no traceback; 0 for the others.  A warp per listed pair, its
+// slots one after another (they share the pair's row buffer).
+__global__ void __launch_bounds__(128) k_f3_dpscore(Blk B, Bat T) {
+    const int lane = threadIdx.x & 31;
+    const int slot = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    if (slot >= T.rhist[RL_NB]) return;
+    const int i = T.rlist[slot];
+    int qi = pair_qi(B, T, i), ri = pair_ri(B, T, i);
+    int lq = B.qlen[qi], lr = B.rlen[ri];
+    int ml = lq < lr ? lq : lr;
+    const float d0 = B.t_d0[ml];
+    const float d02 = __fmul_rn(d0, d0);
+    const float* qx = B.qx + B.qoff[qi];
+    const float* qy = B.qy + B.qoff[qi];
+    const float* qz = B.qz + B.qoff[qi];
+    const float4* r4 = B.r4 + B.r4off[ri];
+    float* row = T.row + T.off_row[i];
+    for (int k = 0; k < F3_NTOP; k++) {
+        const float* sl = T.f3slot + ((long long)i * F3_NTOP + k) * 13;
+        float* fin = T.f3dps + (long long)i * F3_NTOP + k;
+        if (!(0.f < sl[0])) {
+            if (lane == 0) *fin = 0.f;
+            continue;
+        }
+        float t[12];
+#pragma unroll
+        for (int f = 0; f < 12; f++) t[f] = sl[1 + f];
+        if (lane == 0) work_add(T, WK_DPCELL, (unsigned long long)lq * (unsigned long long)lr);
+        if (dp_r(lq) == 4)
+            dp_pair<4, true, DP_SC_TFM, false, true>(t, d02, 0.f, lq, lr, qx, qy, qz, r4, nullptr,
+                                                     nullptr, nullptr, nullptr, row, nullptr, lane,
+                                                     0, 1, nullptr, nullptr, DP_WAVE_SPIN_DEFAULT, fin);
+        else
+            dp_pair<2, true, DP_SC_TFM, false, true>(t, d02, 0.f, lq, lr, qx, qy, qz, r4, nullptr,
+                                                     nullptr, nullptr, nullptr, row, nullptr, lane,
+                                                     0, 1, nullptr, nullptr, DP_WAVE_SPIN_DEFAULT, fin);
+        __syncwarp();
+    }
+}
+
+void launch_f3_dpscore(const Blk& B, const Bat& T, cudaStream_t st) {
+    k_f3_dpscore<<<(T.np + 3) / 4, 128, 0, st>>>(B, T);
+    GTB_LAUNCHED(T);
+}
+
 // ---------------------------------------------------------------------------
 // traceback: MpDPHub.cpp:1515-1660 (plain) and 1699-1905 (constrained)
 __global__ void k_btck(Blk B, Bat T, int constrained) {
@@ -1595,7 +1697,7 @@ __global__ void k_btck(Blk B, Bat T, int constrained) {
     int flags = T.flags[i];
     if (constrained) {
         if (flags & CONV_LOWTMSC) return;
-    } else if (flags & (CONV_LOWTMSC | CONV_SCOREDP)) {
+    } else if ((flags & (CONV_LOWTMSC | CONV_SCOREDP)) || alt_empty(T, i)) {
         T.naln[i] = 0;
         return;
     }
@@ -1881,6 +1983,20 @@ void make_tables(float* d0, float* d82, float* d0fin, int n) {
     }
 }
 
+// DPRefine (MpStage1.cpp:466-517): maxit rounds of DP, traceback, fragment
+// refinement over the alignment and the convergence bookkeeping; the first
+// DP uses the transform tfm1 (DP_TFM_IBEST, or DP_TFM_2ND after the detailed
+// search, WRKMEMTM1)
+void launch_dprefine(const Blk& B, const Bat& T, int gap0, int prescreen, int maxit,
+                     float prescore, bool few, int tfm1, cudaStream_t st) {
+    for (int dpi = 0; dpi < maxit; dpi++) {
+        launch_dp(B, T, dpi == 0 ? tfm1 : DP_TFM_IBEST, gap0, gap0 ? 0.0f : -0.6f, 0, 0, 0, st);
+        launch_btck(B, T, 0, st);
+        launch_refine(RM_DP, B, T, st, few);
+        launch_post(B, T, dpi, maxit, prescreen, prescore, st);
+    }
+}
+
 // ---------------------------------------------------------------------------
 // The stage sequence of one batch: CuBatch::ProcessBlock (CuBatch.cu:537-700)
 // with the detailed search off.  ev (may be null): 5 events recorded at the
@@ -1893,12 +2009,7 @@ void launch_stages(const Blk& B, const Bat& T, int refinement, int depth, int co
     // after the stage-1 --pre-score filter only a small share of pairs is left
     const bool few = 0.0f < prescore;
     auto dprefine = [&](int gap0, int prescreen, int maxit, bool fewp) {
-        for (int dpi = 0; dpi < maxit; dpi++) {
-            launch_dp(B, T, DP_TFM_IBEST, gap0, gap0 ? 0.0f : -0.6f, 0, 0, 0, st);
-            launch_btck(B, T, 0, st);
-            launch_refine(RM_DP, B, T, st, fewp);
-            launch_post(B, T, dpi, maxit, prescreen, prescore, st);
-        }
+        launch_dprefine(B, T, gap0, prescreen, maxit, prescore, fewp, DP_TFM_IBEST, st);
     };
     mark(0);
     launch_init(B, T, st);
@@ -1918,6 +2029,8 @@ void launch_stages(const Blk& B, const Bat& T, int refinement, int depth, int co
         dprefine(0, 0, 2, few);
         dprefine(1, 0, 2, few);
     }
+    // the spatial-index detailed search (CuBatch.cu:612-623)
+    if (B.f3) launch_frg3(B, T, st);
     // two stage-2 passes: MpStage2.h:63-83, CuBatch.cu:627-650
     for (int call = 0; call < 2; call++) {
         int gap0 = call == 1;

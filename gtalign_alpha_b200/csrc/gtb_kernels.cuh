@@ -13,6 +13,7 @@ namespace gtb {
 // [step / (16/R)][lane].
 // refinement: pairs with at least RL_LONG positions get RLW_CTAS CTAs
 constexpr int RL_LONG = 1536;
+constexpr int RL_NBUCKET = 65536 >> 4;   // work-list buckets; rhist[RL_NBUCKET] = list length
 constexpr int RLW_CTAS = 16;
 constexpr int RLW_WARPS = RLW_CTAS * 4;
 constexpr int RLW_CAND = 17;         // floats per warp candidate
@@ -48,7 +49,19 @@ struct Blk {
     int twotm;                       // --2tm-score: record fields 13 and 14
     int addss;                       // --add-search-by-ss
     float presim;                    // --pre-similarity threshold when the screen runs, else 0
+    // the spatial-index detailed search (f3 = 1: on): the structures' index
+    // trees (node x, y, z; left, right child; residue), at the residue offsets
+    // of the coordinates, and its options
+    int f3;
+    const float *qnx, *qny, *qnz, *rnx, *rny, *rnz;
+    const int *qnl, *qnr, *qno, *rnl, *rnr, *rno;
+    int f3trigger, f3nbranches, f3seedrule, f3window;
+    float f3gapcost;
 };
+
+// detailed search: fragment slots, branches per pair at most
+constexpr int F3_NTOP = 32;
+constexpr int F3_NBMAX = 16;
 
 // Batch of consecutive pairs p0 .. p0+np-1 of a block (pair = qi*nr + ri).
 struct Bat {
@@ -97,6 +110,19 @@ struct Bat {
     // summed on the host: position visits of the seed passes, position
     // visits of the refinement passes, DP cells
     unsigned long long* work;
+    // detailed search (null when off): per pair the local score matrix
+    // (lq x lr bytes, row major, at off_lsm[i]); the 32 fragment slots'
+    // score and transform ([np][32][13]); their DP scores ([np][32]); the
+    // branches' transforms and validity ([np][F3_NBMAX][12], [np][F3_NBMAX]);
+    // the best branch's transform and score; the refinement variants (1..31)
+    // the next DP refinement skips
+    const long long* off_lsm;
+    unsigned char* lsm;
+    float *f3slot, *f3dps, *f3alt, *tfm_2nd, *best2;
+    unsigned char* f3ok;
+    unsigned* vskip_mask;
+    int alt_rci;                     // DP/traceback of branch alt_rci (-1: none)
+    const unsigned* vskip;           // refinement variant skips in force (null: none)
 };
 
 enum WorkKind { WK_SEED = 0, WK_REFINE = 1, WK_DPCELL = 2, WK_NKIND = 3 };
@@ -110,7 +136,9 @@ enum DpScore { DP_SC_TFM = 0, DP_SC_TFMSS = 1, DP_SC_SSRR = 2 };
 enum RefineMode { RM_INIT = 0, RM_DP = 1, RM_FIN1 = 2, RM_FIN2 = 3, RM_PROD1 = 4, RM_PROD2 = 5,
                   RM_PLOG = 6 };
 constexpr int PLOG_ROUNDS = 12;   // steps +-32, +-16, ..., +-1
-enum DpTfm { DP_TFM_IBEST = 0, DP_TFM_GRAND = 1 };
+// the transform a DP uses: iteration best, grand best, the detailed search's
+// branch T.alt_rci, or its best branch's result
+enum DpTfm { DP_TFM_IBEST = 0, DP_TFM_GRAND = 1, DP_TFM_ALT = 2, DP_TFM_2ND = 3 };
 
 void launch_secstr(char* ss, const float* x, const float* y, const float* z,
                    const int* len, const int* off, const int* mol, int nstr,
@@ -164,9 +192,23 @@ void launch_alnstr(const Blk& B, const Bat& T, cudaStream_t st);
 void launch_final(const Blk& B, const Bat& T, int referenced, cudaStream_t st);
 // adjoint polishing of the final transforms (steps > 0), before launch_final
 void launch_polish_final(const Blk& B, const Bat& T, int steps, cudaStream_t st);
+// detailed search (gtb_frg3.cu): the stage between stage 1 and stage 2
+void launch_frg3(const Blk& B, const Bat& T, cudaStream_t st);
+// work list of the pairs without any flag in skipmask, largest matrices
+// first, in T.rlist / T.rhist[RL_NB]
+void launch_pair_list(const Blk& B, const Bat& T, int skipmask, cudaStream_t st);
+// DP scores (last cell of a gap-0 DP, no traceback) of every pair's 32
+// fragment slots with a positive score, over the pair list
+void launch_f3_dpscore(const Blk& B, const Bat& T, cudaStream_t st);
+void launch_dprefine(const Blk& B, const Bat& T, int gap0, int prescreen, int maxit,
+                     float prescore, bool few, int tfm1, cudaStream_t st);
 void launch_stages(const Blk& B, const Bat& T, int refinement, int depth, int convergence,
                    float prescore, int referenced, float scorethld, cudaStream_t st,
                    cudaEvent_t* ev, int polish_steps = 0);
+// the reader's index trees of n structures (host, gtb_index.cpp)
+bool build_index_host(long long n, const int* len, const unsigned* dist, const float* X,
+                      const float* Y, const float* Z, long long npos, float* ox, float* oy,
+                      float* oz, int* ol, int* orr, int* oo);
 // Per-length constant tables (stagecnsts.cuh:48-175), n entries each.
 void make_tables(float* d0, float* d82, float* d0fin, int n);
 

@@ -277,6 +277,7 @@ extern "C" gtb_status gtb_process_block_noalloc(int device, const gtb_options* o
     T.rlist = (int*)(base + o_rl); T.rhist = (int*)(base + o_rh);
     T.nff = np; T.ff_pair = nullptr; T.ff_chunk = nullptr; T.ff_nch = nullptr; T.ff_key = nullptr;
     T.launches = nullptr;
+    T.alt_rci = -1;
 
     // the host offsets are copied from the static host array (no allocation)
     e = cudaMemcpyAsync(offs, h_offs, (size_t)(np + 1) * 4 * sizeof(long long), cudaMemcpyHostToDevice, st);

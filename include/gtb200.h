@@ -57,6 +57,18 @@ enum {
     GTB_NFIELDS = 10
 };
 
+/* Index fields of a block (PM2DVectorFields.h:260-281): per structure a 3-d
+ * tree over its residues in the structure's own position range; node n holds
+ * coordinates x, y, z (float), its left and right child nodes (int32, -1 for
+ * none) and the residue it stands for (int32).  The reader makes them
+ * (PMBatchStrDataIndex::MakeIndex, PMBatchStrDataIndex.cpp); the
+ * spatial-index detailed search reads them. */
+enum {
+    GTB_NDX_X = 0, GTB_NDX_Y = 1, GTB_NDX_Z = 2,
+    GTB_NDX_LEFT = 3, GTB_NDX_RIGHT = 4, GTB_NDX_ORGNDX = 5,
+    GTB_NNDXFIELDS = 6
+};
+
 /* Per-pair output record (gproc.h:148-168, TDP2OutputAlnData) */
 enum {
     GTB_OUT_ORGSTRNO = 0, GTB_OUT_STRNEWDST = 1, GTB_OUT_BEGCOORDS = 2,
@@ -80,8 +92,10 @@ typedef struct {
     int   symmetric;         /* --symmetric */
     int   referenced;        /* --referenced */
     int   nodeletions;       /* --no-deletions */
-    int   nodetailedsearch;  /* --no-detailed-search: must be 1 (the spatial-index
-                                search stage is not part of this library) */
+    int   nodetailedsearch;  /* --no-detailed-search: 0 runs the spatial-index
+                                detailed search (MpStageFrg3) between stage 1
+                                and stage 2, as the reference does at --speed
+                                <= 12; its options are the last five below */
     int   addsearchbyss;     /* --add-search-by-ss: after stage 1, an alignment
                                 by secondary structure and residue similarity,
                                 refined like stage 2's */
@@ -99,6 +113,14 @@ typedef struct {
                                 ungapped run of Gonnet residue scores on some
                                 diagonal of a pair must reach for the pair to
                                 be compared at all */
+    /* the detailed search (read when nodetailedsearch is 0), the command
+     * line's codes (CLOptions.h:122-160, gtalign.h:157-186) */
+    int   trigger;           /* --trigger 0..100 (default 50) */
+    int   nbranches;         /* --nbranches 1..16 (default 5) */
+    int   gapcost;           /* --gapcost 0..2 (-0.8, -1.2, -3.0; default 1) */
+    int   seedrule;          /* --seedrule 0..2 (fragments, 64- or 128-residue
+                                local alignment frames; default 1) */
+    int   window;            /* --window 256..512 (default 256) */
 } gtb_options;
 
 /* Result buffers (host memory), sizes for nq queries x nr references with
@@ -143,6 +165,17 @@ gtb_status gtb_process_block(gtb_handle* h, float scorethld,
                              char* const* bdbCpmbeg, char* const* bdbCpmend,
                              gtb_results* out);
 
+/* The same with the blocks' index fields as the reader made them
+ * (queryndxpmbeg / bdbCndxpmbeg: GTB_NNDXFIELDS host pointers each, the
+ * index data CuBatch transfers beside the SoA fields, CuBatch.cuh:54-72).
+ * gtb_process_block builds them itself (gtb_build_index) when the detailed
+ * search is on; a reader that has them saves that work. */
+gtb_status gtb_process_block_ndx(gtb_handle* h, float scorethld,
+                                 char* const* querypmbeg, char* const* querypmend,
+                                 char* const* queryndxpmbeg,
+                                 char* const* bdbCpmbeg, char* const* bdbCpmend,
+                                 char* const* bdbCndxpmbeg, gtb_results* out);
+
 /* Device-resident blocks: the reference uploads a reference chunk once and
  * reuses it for every query block (TdCommutator.cpp:265-285,
  * CuDeviceMemory::TransferCPMDataToDevice); gtb_block_upload is that step.
@@ -152,11 +185,22 @@ gtb_status gtb_process_block(gtb_handle* h, float scorethld,
 typedef struct gtb_block gtb_block;
 gtb_status gtb_block_upload(gtb_handle* h, char* const* pmbeg, char* const* pmend,
                             gtb_block** out);
+/* The same with the block's index fields (GTB_NNDXFIELDS host pointers; NULL:
+ * built here when the handle's detailed search is on). */
+gtb_status gtb_block_upload_ndx(gtb_handle* h, char* const* pmbeg, char* const* pmend,
+                                char* const* ndxbeg, gtb_block** out);
 /* Free a block with the handle that uploaded it, before gtb_destroy. */
 void gtb_block_free(gtb_handle* h, gtb_block* b);
 gtb_status gtb_process_resident(gtb_handle* h, float scorethld, const gtb_block* queries,
                                 const gtb_block* refs, float* d_alndata, float* d_tfm,
                                 float* d_numerr);
+
+/* Build the index fields of a block (replaces PMBatchStrDataIndex::MakeIndex,
+ * src/libgenp/gdats/PMBatchStrDataIndex.cpp:48-110, for callers that do not
+ * run the reference's reader): ndxbeg[GTB_NNDXFIELDS] are host arrays of as
+ * many entries as the block has residues (x, y, z float; left, right, residue
+ * int32).  The tree is the reader's, node for node.  Host code. */
+gtb_status gtb_build_index(char* const* pmbeg, char* const* pmend, char* const* ndxbeg);
 
 /* Total bytes of the alns buffer for a block (GetSizeOfDP2Alns,
  * CuMemoryBase.h:150-158). */

@@ -258,7 +258,11 @@ static int qcp_rotation(const double S[3][3], double R[9], double* lamout) {
 }
 
 /* sums: [0..8] sum q_i r_j, [9..11] sum q, [12..14] sum r; n.
- * tfm rotates/translates the query onto the reference (row-major R, t). */
+ * swap 0: tfm rotates/translates the query onto the reference (row-major R,
+ * t); 1: solved with the reference moving onto the query, then inverted
+ * (--symmetric); 2: the reference moving onto the query, not inverted (the
+ * detailed search's orientation towards the longer structure,
+ * MpStageBase.h:1086-1101). */
 static int solve_sums(const float* v, int n, int swap, float* tfm) {
     double dn = (double)n;
     double mq[3], mr[3], S[3][3];
@@ -284,6 +288,11 @@ static int solve_sums(const float* v, int n, int swap, float* tfm) {
         if (!ok) { memset(R, 0, sizeof(R)); R[0] = R[4] = R[8] = 1.0; }
         double t[3];
         for (int i = 0; i < 3; i++) t[i] = mq[i] - (R[3*i] * mr[0] + R[3*i+1] * mr[1] + R[3*i+2] * mr[2]);
+        if (swap == 2) {
+            for (int k = 0; k < 9; k++) tfm[k] = (float)R[k];
+            for (int i = 0; i < 3; i++) tfm[9 + i] = (float)t[i];
+            return ok;
+        }
         /* inverse: R^T, -R^T t */
         for (int i = 0; i < 3; i++)
             for (int j = 0; j < 3; j++) tfm[3 * i + j] = (float)R[3 * j + i];
@@ -390,6 +399,13 @@ typedef struct {
     float out[GTO_NOUT];
     float err[GTO_NERR];
     float d0, d02, d82, d0fin, d0s;
+    /* detailed search: the structures' index trees, the best transform among
+     * its refined branches, and the refinement variants (1..31) the first DP
+     * refinement after it skips (the fragment slots its sorting left empty) */
+    const float *qnx, *qny, *qnz, *rnx, *rny, *rnz;
+    const int *qnl, *qnr, *qno, *rnl, *rnr, *rno;
+    float tfm_2nd[12];
+    unsigned vskip;
 } pairctx;
 
 static void tfm_identity(float* t) { memset(t, 0, 12 * sizeof(float)); t[0] = t[4] = t[8] = 1.f; }
@@ -584,6 +600,7 @@ static void refine_stage(pairctx* P, int dpmode, float d0, float d02, int chk,
     float wbest = 0.f, wtfm[12];
     int wsi = -1, wndx = 0, wpos = 0;
     for (int si = 0; si < nloc && nrange > 0; si++) {
+        if (dpmode == 1 && si < 32 && ((P->vskip >> si) & 1u)) continue;
         int sfragfct = si / FRAG_NSUB, sfragndx = si % FRAG_NSUB;
         int fraglen = frag_length(nrange, sfragndx);
         if (fraglen < 1) continue;
@@ -798,11 +815,13 @@ static int dp_skip_plain(const pairctx* P) {
     return (P->flags & CONV_LOWTMSC) || (P->flags & CONV_SCOREDP);
 }
 
-static void dprefine(pairctx* P, int gap0, int prescreen, int maxit) {
+/* tfm1 (may be NULL): the transform of the first DP instead of the
+ * iteration-best one (WRKMEMTM1, MpStage1.cpp:489-493) */
+static void dprefine_t(pairctx* P, int gap0, int prescreen, int maxit, const float* tfm1) {
     float gcost = gap0 ? 0.0f : -0.6f;
     for (int dpi = 0; dpi < maxit; dpi++) {
         if (!dp_skip_plain(P)) {
-            dp_run(P, P->tfm_ib, gap0, gcost, 0, P->d02);
+            dp_run(P, (tfm1 && dpi == 0) ? tfm1 : P->tfm_ib, gap0, gcost, 0, P->d02);
             btck_matched(P);
         } else P->naln = 0;
         if (P->flags) P->best = 0.f;   /* variants skipped: slot bests were reset */
@@ -817,7 +836,446 @@ static void dprefine(pairctx* P, int gap0, int prescreen, int maxit) {
             if (P->grand < P->o->prescore * (float)ml) P->flags |= CONV_LOWTMSC;
         }
     }
+    /* InitScoresKernel<INITOPT_CONVFLAG_SCOREDP> over every slot
+     * (MpStage1.cpp:510): the pair's flag and the fragment slots' flags */
     P->flags &= ~CONV_SCOREDP;
+    P->vskip = 0u;
+}
+
+static void dprefine(pairctx* P, int gap0, int prescreen, int maxit) {
+    dprefine_t(P, gap0, prescreen, maxit, NULL);
+}
+
+/* ------------------------------------------------------------------------ */
+/* Spatial-index detailed search: MpStageFrg3::Run (MpStageFrg3.h:80-115,     */
+/* MpStageFrg3.cpp:35-469), one pair as if alone in its chunk and processed  */
+/* by one thread (the reference's fragment slot of a scored configuration is */
+/* its thread's running count of them; its memory alignment of the local    */
+/* score matrix follows the chunk layout).                                   */
+#define FRG3_NTOP 32            /* CUS1_TBSP_DPSCORE_TOP_N */
+#define FRG3_MAXVISIT 64        /* CUSF_TBSP_INDEX_SCORE_MAXDEPTH */
+#define FRG3_HASH 512           /* CUSF_TBSP_INDEX_SCORE_POSLIMIT2 */
+#define FRG3_SIMROWS 96         /* MPSF_TBSP_LOCAL_SIMILARITY_YDIM x 3 */
+#define FRG3_SIMCOLS 128        /* MPSF_TBSP_LOCAL_SIMILARITY_XDIM */
+#define FRG3_MAXSTACK 17
+#define FRG3_SSDST2 64.0f       /* SS-matched neighbour farther than 8 A: none */
+
+/* local alignment by secondary structure (ExecDPSSLocal128xKernel,
+ * MpDPHub.cpp:1256-1480): a cell scores +1 for equal, -1 for different SS,
+ * floored at 0 (STOP); gaps cost gcost; the byte kept per cell is the
+ * truncated score rounded down to a multiple of 4 (mod 256) with the
+ * direction in its two low bits */
+static void frg3_localdp(pairctx* P, float gcost, unsigned char* m) {
+    int lq = P->lq, lr = P->lr;
+    float* prev = P->h0;
+    float* cur = P->h1;
+    for (int j = 0; j < lr; j++) prev[j] = 0.f;
+    for (int i = 0; i < lq; i++) {
+        char qs = P->qs[i];
+        float left = 0.f;
+        for (int j = 0; j < lr; j++) {
+            float v = (float)((qs == P->rs[j]) * 2) - 1.0f;
+            v = v + ((j > 0) ? prev[j - 1] : 0.f);
+            int bk = BT_DIAG;
+            if (v < 0.f) { v = 0.f; bk = BT_STOP; }
+            float l = left + gcost;
+            if (v < l) { v = l; bk = BT_LEFT; }
+            float u = prev[j] + gcost;
+            if (v < u) { v = u; bk = BT_UP; }
+            cur[j] = v;
+            left = v;
+            m[(size_t)i * lr + j] = (unsigned char)((((unsigned)v) & 0xfcu) | (unsigned)bk);
+        }
+        float* t = prev; prev = cur; cur = t;
+    }
+}
+
+/* fragment lengths (GetNAlnPoss_frg, covariancebase.h:93-110) */
+static int frg3_fraglen(int lq, int lr, int fi, int seedrule) {
+    int minlen = lq < lr ? lq : lr;
+    int half = minlen >> 1;
+    if (seedrule) return seedrule < half ? seedrule : half;
+    if (fi == 0) {
+        int leno3 = (int)((float)minlen * (1.0f / 3.0f));
+        if (leno3 < 1) leno3 = 1;
+        return leno3 < 20 ? leno3 : 20;
+    }
+    return half < 100 ? half : 100;
+}
+
+/* position step of the configurations (GetFragStepSize_frg_*,
+ * covariancebase.h:22-84) */
+static int frg3_step(int depth, int len) {
+    int leno3 = (int)((float)len * (1.0f / 3.0f));
+    if (leno3 < 1) leno3 = 1;
+    int small = leno3 < 15 ? leno3 : 15;
+    if (depth == 0) return len > 150 ? 15 : small;
+    if (depth == 1) return len > 150 ? 23 : small;
+    int med = len > 250 ? 45 : len > 200 ? 35 : len > 150 ? 25 : small;
+    return depth == 2 ? med : 2 * med;
+}
+
+/* The local similarity test of a configuration (CalcLocalSimilarity2_frg2,
+ * MpStageFrg3.h:327-415): the largest score byte over 96 rows from qrypos and
+ * up to 128 columns from rfnpos (rounded up to a multiple of 4, as the
+ * 4-byte reads of a structure starting on such a boundary) must reach the
+ * fragment length x the trigger fraction. */
+static int frg3_similar(const pairctx* P, const unsigned char* m, int qrypos, int rfnpos,
+                        int fl, float thr) {
+    if (P->lq < qrypos + fl) fl = P->lq - qrypos;
+    if (P->lr < rfnpos + fl) fl = P->lr - rfnpos;
+    int pidelta = (P->lr - 3 - rfnpos) & ~3;
+    if (pidelta > FRG3_SIMCOLS) pidelta = FRG3_SIMCOLS;
+    int pibeg = (rfnpos + 3) & ~3;
+    unsigned maxg = 0;
+    for (int ii = 0; qrypos + ii < P->lq && ii < FRG3_SIMROWS; ii++) {
+        const unsigned char* row = m + (size_t)(qrypos + ii) * P->lr;
+        for (int pi = pibeg; pi < pibeg + pidelta; pi++) {
+            unsigned v = row[pi] & 0xfcu;
+            if (v > maxg) maxg = v;
+        }
+    }
+    return !((float)maxg < (float)fl * thr);
+}
+
+/* Sum over 32 values in the order of a warp's xor-shuffle reduction
+ * (offsets 16, 8, 4, 2, 1); every lane ends with this value. */
+static float tree32(const float* t) {
+    float a[32];
+    memcpy(a, t, sizeof(a));
+    for (int off = 16; off > 0; off >>= 1) {
+        float b[32];
+        for (int k = 0; k < 32; k++) b[k] = a[k] + a[k ^ off];
+        memcpy(a, b, sizeof(a));
+    }
+    return a[0];
+}
+
+/* Covariance sums over position slots 0..n-1 (pairs (pq[k], pr[k]); a
+ * negative index: no pair): slots in blocks of 32, each block summed by
+ * tree32 per field and folded into Neumaier totals in block order. */
+static void frg3_cov(const pairctx* P, const int* pq, const int* pr, int n, float* v) {
+    float s[15], c[15], b[15];
+    for (int f = 0; f < 15; f++) s[f] = c[f] = 0.f;
+    int cnt = 0;
+    for (int b0 = 0; b0 < n; b0 += 32) {
+        float t[15][32];
+        for (int k = 0; k < 32; k++) {
+            int i = b0 + k;
+            int ok = i < n && pq[i] >= 0 && pr[i] >= 0;
+            float qx = ok ? P->qx[pq[i]] : 0.f, qy = ok ? P->qy[pq[i]] : 0.f, qz = ok ? P->qz[pq[i]] : 0.f;
+            float rx = ok ? P->rx[pr[i]] : 0.f, ry = ok ? P->ry[pr[i]] : 0.f, rz = ok ? P->rz[pr[i]] : 0.f;
+            t[0][k] = qx * rx; t[1][k] = qx * ry; t[2][k] = qx * rz;
+            t[3][k] = qy * rx; t[4][k] = qy * ry; t[5][k] = qy * rz;
+            t[6][k] = qz * rx; t[7][k] = qz * ry; t[8][k] = qz * rz;
+            t[9][k] = qx; t[10][k] = qy; t[11][k] = qz;
+            t[12][k] = rx; t[13][k] = ry; t[14][k] = rz;
+            cnt += ok;
+        }
+        for (int f = 0; f < 15; f++) { b[f] = tree32(t[f]); nfold(&s[f], &c[f], &b[f]); }
+    }
+    for (int f = 0; f < 15; f++) v[f] = s[f] + c[f];
+    v[15] = (float)cnt;
+}
+
+/* Seed positions from the local alignment (CalcCCMatricesLocallyAligned_
+ * Complete, MpStage1.h:395-470): of 4 evenly spaced cells, the first with
+ * the largest score byte; the local alignment traced back from it within the
+ * rectangle from (qrypos, rfnpos).  Returns the aligned pairs in increasing
+ * order, or 0 when too few. */
+static int frg3_seed_local(const pairctx* P, const unsigned char* m, int trig, int fraglen,
+                           int qrypos, int rfnpos, int* pq, int* pr) {
+    int lq = P->lq, lr = P->lr;
+    if (lq < qrypos + fraglen && lr < rfnpos + fraglen)
+        fraglen = (lq - qrypos) > (lr - rfnpos) ? (lq - qrypos) : (lr - rfnpos);
+    fraglen >>= 2;
+    int y = qrypos, x = rfnpos;
+    float vr = 0.f;
+    for (int f = 0; f < 4; f++) {
+        int yt = qrypos + (f + 1) * fraglen, xt = rfnpos + (f + 1) * fraglen;
+        if (yt > lq - 1) yt = lq - 1;
+        if (xt > lr - 1) xt = lr - 1;
+        float vrt = (float)(m[(size_t)yt * lr + xt] & 0xfcu);
+        if (vr < vrt) { vr = vrt; y = yt; x = xt; }
+    }
+    int n = 0;
+    while (y >= qrypos && x >= rfnpos) {
+        int b = m[(size_t)y * lr + x] & 3;
+        if (b == BT_STOP) break;
+        if (b == BT_UP) { y--; continue; }
+        if (b == BT_LEFT) { x--; continue; }
+        pq[n] = y; pr[n] = x; n++;
+        x--; y--;
+    }
+    int minf = fraglen < 16 ? fraglen : 16;
+    if (n < 1 || (trig && n < minf)) return 0;
+    for (int i = 0, j = n - 1; i < j; i++, j--) {
+        int t = pq[i]; pq[i] = pq[j]; pq[j] = t;
+        t = pr[i]; pr[i] = pr[j]; pr[j] = t;
+    }
+    return n;
+}
+
+/* Nearest neighbour of (px, py, pz) in a structure's 3-d tree (NNByIndex*,
+ * MpStageFrg3.h:1270-1440): depth-first with a bounded stack, at most 64
+ * nodes visited; with ss, only residues of that secondary structure count
+ * and one farther than 8 A is none.  Returns the residue index or -1. */
+static int frg3_nn(const float* nx, const float* ny, const float* nz, const int* nl,
+                   const int* nr, const int* no, const char* sss, int len, int ssfilt, char ss,
+                   float px, float py, float pz, int stacksize) {
+    int stk_node[FRG3_MAXSTACK], stk_dim[FRG3_MAXSTACK];
+    float stk_diff[FRG3_MAXSTACK];
+    int sp = 0, nvisited = 0, best = -1, root = len >> 1, dim = 0;
+    float bestd = 9.9e6f;
+    while (0 < sp || 0 <= root) {
+        if (0 <= root) {
+            nvisited++;
+            if (FRG3_MAXVISIT <= nvisited) break;
+            int org = no[root];
+            float x = nx[root], y = ny[root], z = nz[root];
+            float dx = x - px, dy = y - py, dz = z - pz;
+            float d2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+            if ((best < 0 || d2 < bestd) && (!ssfilt || sss[org] == ss)) {
+                bestd = d2;
+                best = ssfilt ? org : root;
+            }
+            if (bestd == 0.0f) break;
+            float diffc = dim == 0 ? dx : (dim == 1 ? dy : dz);
+            if (2 < ++dim) dim = 0;
+            if (sp < stacksize) { stk_node[sp] = root; stk_dim[sp] = dim; stk_diff[sp] = diffc; sp++; }
+            root = (0.0f < diffc) ? nl[root] : nr[root];
+        } else {
+            int cond = 0;
+            float diffc = 0.f;
+            while (0 < sp && !cond) {
+                sp--;
+                root = stk_node[sp]; dim = stk_dim[sp]; diffc = stk_diff[sp];
+                cond = diffc * diffc < bestd;
+            }
+            if (!cond) break;
+            root = (0.0f < diffc) ? nr[root] : nl[root];
+        }
+    }
+    if (ssfilt) return FRG3_SSDST2 < bestd ? -1 : best;
+    return 0 <= best ? no[best] : -1;
+}
+
+/* Neighbours over the window of the shorter structure
+ * (ProduceAlignmentUsingIndex2Reference/Query, MpStageFrg3.h:500-680): the
+ * window of up to `window` positions about the configuration's position of
+ * the shorter structure is moved by tfm (which maps the shorter onto the
+ * longer structure) and each position paired with its nearest residue of the
+ * longer one; a neighbour at residue 0 or none leaves the slot empty.
+ * Fills pq/pr per window slot (-1: empty); returns the window length. */
+static int frg3_window(const pairctx* P, const float* tfm, int ssfilt, int window, int qrypos,
+                       int rfnpos, int stacksize, int* pq, int* pr) {
+    int lq = P->lq, lr = P->lr;
+    if (lq < lr) {
+        int fl = lr < window ? lr : window;
+        int qp = qrypos - (fl >> 1); if (qp < 0) qp = 0;
+        int ql = qp + fl < lq ? qp + fl : lq;
+        qp = ql - fl; if (qp < 0) qp = 0;
+        for (int pi = 0; pi < ql - qp; pi++) {
+            int q = qp + pi;
+            float x, y, z;
+            xform(tfm, P->qx[q], P->qy[q], P->qz[q], &x, &y, &z);
+            int r = frg3_nn(P->rnx, P->rny, P->rnz, P->rnl, P->rnr, P->rno, P->rs, lr, ssfilt,
+                            P->qs[q], x, y, z, stacksize);
+            pq[pi] = q;
+            pr[pi] = r > 0 ? r : -1;
+        }
+        return ql - qp;
+    }
+    int fl = lq < window ? lq : window;
+    int rp = rfnpos - (fl >> 1); if (rp < 0) rp = 0;
+    int rl = rp + fl < lr ? rp + fl : lr;
+    rp = rl - fl; if (rp < 0) rp = 0;
+    for (int pi = 0; pi < rl - rp; pi++) {
+        int r = rp + pi;
+        float x, y, z;
+        xform(tfm, P->rx[r], P->ry[r], P->rz[r], &x, &y, &z);
+        int q = frg3_nn(P->qnx, P->qny, P->qnz, P->qnl, P->qnr, P->qno, P->qs, lq, ssfilt,
+                        P->rs[r], x, y, z, stacksize);
+        pq[pi] = q > 0 ? q : -1;
+        pr[pi] = r;
+    }
+    return rl - rp;
+}
+
+/* Order-dependent score of the window's neighbour pairs
+ * (CalcScoresUnrl_SWFTscanProgressive_Complete, MpStageFrg3.h:760-850): over
+ * the first `cnt` window slots (cnt = the number of non-empty ones), each
+ * pair extends the best chain of earlier-partnered pairs kept in a 512-entry
+ * table hashed by partner index. */
+static float frg3_progressive(const pairctx* P, const float* tfm, const int* pq, const int* pr,
+                              int cnt, int partner_is_r) {
+    float omax[FRG3_HASH], ondx[FRG3_HASH];
+    for (int i = 0; i < FRG3_HASH; i++) { omax[i] = 0.f; ondx[i] = -1.f; }
+    for (int pi = 0; pi < cnt; pi++) {
+        if (pq[pi] < 0 || pr[pi] < 0) continue;
+        float d = dist2_tf(tfm, P->qx[pq[pi]], P->qy[pq[pi]], P->qz[pq[pi]],
+                           P->rx[pr[pi]], P->ry[pr[pi]], P->rz[pr[pi]]);
+        float sco = P->d02 / (P->d02 + d);
+        float qnx = (float)(partner_is_r ? pr[pi] : pq[pi]);
+        if (sco <= 0.f) continue;
+        float max1 = 0.f;
+        for (int ni = 0; ni < FRG3_HASH; ni++)
+            if (ondx[ni] < qnx && max1 < omax[ni]) max1 = omax[ni];
+        int c = (int)qnx & (FRG3_HASH - 1);
+        float st = ondx[c], ss = omax[c], nsc = max1 + sco;
+        int half2nd = pi > (cnt >> 1);
+        if (st < 0.f || (st == qnx && ss < nsc) || ((half2nd && st < qnx) || (!half2nd && qnx < st))) {
+            ondx[c] = qnx;
+            omax[c] = nsc;
+        }
+    }
+    float mx = 0.f;
+    for (int i = 0; i < FRG3_HASH; i++) if (mx < omax[i]) mx = omax[i];
+    return mx;
+}
+
+/* GAP0 DP score without traceback (ExecDPScore128xKernel,
+ * MpDPHub.cpp:389-645): the value of the last cell */
+static float frg3_dpscore(pairctx* P, const float* tfm) {
+    int lq = P->lq, lr = P->lr;
+    float* prev = P->h0;
+    float* cur = P->h1;
+    for (int j = 0; j < lr; j++) prev[j] = 0.f;
+    for (int i = 0; i < lq; i++) {
+        float tx, ty, tz;
+        xform(tfm, P->qx[i], P->qy[i], P->qz[i], &tx, &ty, &tz);
+        float left = 0.f;
+        for (int j = 0; j < lr; j++) {
+            float dx = tx - P->rx[j], dy = ty - P->ry[j], dz = tz - P->rz[j];
+            float d = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+            float v = P->d02 / (P->d02 + d);
+            v += (j > 0) ? prev[j - 1] : 0.f;
+            if (v < left) v = left;
+            if (v < prev[j]) v = prev[j];
+            cur[j] = v;
+            left = v;
+        }
+        float* t = prev; prev = cur; cur = t;
+    }
+    return prev[lr - 1];
+}
+
+static int frg3_stacksize(int lq, int lr) {
+    int L = lq > lr ? lq : lr, b = 0;
+    while ((1 << b) < L) b++;          /* ceil(log2 L) */
+    b += 1;
+    return b < FRG3_MAXSTACK ? b : FRG3_MAXSTACK;
+}
+
+/* the stage for one pair (runs when the pair is not filtered out) */
+static void frg3_stage(pairctx* P) {
+    const gto_opts* o = P->o;
+    int lq = P->lq, lr = P->lr;
+    float thr = (float)o->trigger / 100.0f;
+    int seedrule = o->seedrule;
+    int mx = lq > lr ? lq : lr;
+    int* pq = (int*)malloc(sizeof(int) * (size_t)(mx + o->window + 8));
+    int* pr = (int*)malloc(sizeof(int) * (size_t)(mx + o->window + 8));
+    unsigned char* m = P->bt;          /* the local score matrix; DP scores below keep it */
+    if (0.0f < thr || seedrule) frg3_localdp(P, o->gapcost, m);
+
+    float sbest[FRG3_NTOP], stfm[FRG3_NTOP][12];
+    for (int k = 0; k < FRG3_NTOP; k++) sbest[k] = 0.f;
+    int nscored = 0;
+    int qstep = frg3_step(o->depth, lq), rstep = frg3_step(o->depth, lr);
+    int minn = o->depth == 3 ? 5 : 10;
+    int nsy = lq / qstep + 1; if (nsy < minn) nsy = minn;
+    int nsx = lr / rstep + 1; if (nsx < minn) nsx = minn;
+    int stacksize = frg3_stacksize(lq, lr);
+    int f0 = frg3_fraglen(lq, lr, 0, 0), f1 = frg3_fraglen(lq, lr, 1, 0);
+    int nfr = seedrule ? 1 : 2;
+    for (int ys = 0; ys < nsy; ys++)
+    for (int xs = 0; xs < nsx; xs++) {
+        int qrypos = ys * qstep, rfnpos = xs * rstep;
+        /* CalcLocalSimilarity2_frg2: flags of the two fragment lengths */
+        if (lq < qrypos + f0 || lr < rfnpos + f0 || f0 < 1) continue;
+        int conv1 = (lq < qrypos + f1 || lr < rfnpos + f1 || f1 < 1);
+        if (0.0f < thr && !frg3_similar(P, m, qrypos, rfnpos, f1, thr)) continue;
+        for (int fi = 0; fi < nfr; fi++) {
+            if (fi == 1 && conv1) continue;
+            int fraglen = fi == 0 ? f0 : f1;
+            if (lq < qrypos + fraglen || lr < rfnpos + fraglen) continue;
+            float v[16], tfm[12];
+            int n;
+            if (seedrule) {
+                n = frg3_seed_local(P, m, o->trigger > 0, frg3_fraglen(lq, lr, fi, seedrule),
+                                    qrypos, rfnpos, pq, pr);
+            } else {
+                for (int k = 0; k < fraglen; k++) { pq[k] = qrypos + k; pr[k] = rfnpos + k; }
+                n = fraglen;
+            }
+            if (n < 1) continue;
+            frg3_cov(P, pq, pr, n, v);
+            if (v[15] < 1.0f) continue;
+            /* towards the longer structure (CalcTfmMatrices_DynamicOrientation_Complete) */
+            solve_sums(v, (int)v[15], lq < lr ? 0 : 2, tfm);
+            for (int it = 0; it < 2; it++) {
+                int cw = frg3_window(P, tfm, it == 0, o->window, qrypos, rfnpos, stacksize, pq, pr);
+                frg3_cov(P, pq, pr, cw, v);
+                if (v[15] < 1.0f) continue;
+                if (it == 0) { solve_sums(v, (int)v[15], lq < lr ? 0 : 2, tfm); continue; }
+                solve_sums(v, (int)v[15], 0, tfm);
+                float sc = frg3_progressive(P, tfm, pq, pr, (int)v[15], lq < lr);
+                int slot = nscored % FRG3_NTOP;
+                nscored++;
+                if (0.0f < sc && sbest[slot] < sc) {
+                    sbest[slot] = sc;
+                    memcpy(stfm[slot], tfm, sizeof(tfm));
+                }
+            }
+        }
+    }
+    /* DP scores of the slots' transforms (SaveTopNScoresAndTMsAmongBests with
+     * one thread keeps the slots; ExecDPScore128xKernel skips empty ones) */
+    float dps[FRG3_NTOP];
+    int order[FRG3_NTOP];
+    for (int k = 0; k < FRG3_NTOP; k++) {
+        dps[k] = 0.0f < sbest[k] ? frg3_dpscore(P, stfm[k]) : 0.0f;
+        order[k] = k;
+    }
+    /* the slots by DP score, larger first, lower slot first on ties
+     * (SortBestDPscoresAndTMsAmongDPswifts, MpStageFrg3.h:1150-1250) */
+    for (int a = 1; a < FRG3_NTOP; a++) {
+        int k = order[a], b = a - 1;
+        while (b >= 0 && dps[order[b]] < dps[k]) { order[b + 1] = order[b]; b--; }
+        order[b + 1] = k;
+    }
+    unsigned vskip = 0u;
+    for (int r = 1; r < FRG3_NTOP; r++)
+        if (!(0.0f < dps[order[r]])) vskip |= 1u << r;
+    /* the pair's flag is the first slot's (MpStageFrg3.h:1210-1225) */
+    P->flags = 0.0f < dps[order[0]] ? 0 : CONV_SCOREDP;
+    /* the branches (Refine_tfmaltconfig, MpStageFrg3.cpp:425-467) */
+    float best2 = 0.f;
+    int nbr = o->nbranches < FRG3_NTOP ? o->nbranches : FRG3_NTOP;
+    for (int rci = 0; rci < nbr; rci++) {
+        int k = order[rci];
+        int valid = 0.0f < dps[k];
+        if (!(P->flags & (CONV_LOWTMSC | CONV_SCOREDP)) && valid) {
+            dp_run(P, stfm[k], 1, 0.0f, 0, P->d02);
+            btck_matched(P);
+        } else P->naln = 0;
+        if (P->flags) P->best = 0.f;
+        else refine_stage(P, 1, P->d0, P->d02, 1, 0.f, 1, 0);
+        /* the best branch's result (SECONDARYUPDATE, MpStageBase.h:1250-1280) */
+        if (rci == 0 || best2 < P->best) {
+            best2 = P->best;
+            memcpy(P->tfm_2nd, P->tfm_ib, sizeof(P->tfm_ib));
+        }
+    }
+    free(pq);
+    free(pr);
+    /* DP refinement from the best branch, with a gap cost and without
+     * (MpStageFrg3.h:108-112); the first one skips the fragment variants of
+     * the slots the sorting left empty */
+    P->vskip = vskip;
+    dprefine_t(P, 0, 0, 2, P->tfm_2nd);
+    dprefine(P, 1, 0, 2);
 }
 
 /* ------------------------------------------------------------------------ */
@@ -1123,6 +1581,9 @@ static void run_pair(pairctx* P, char* alndst) {
         dprefine(P, 1, 0, 2);
     }
 
+    /* the spatial-index detailed search (MpBatch.cpp:446-461) */
+    if (!o->nodetailedsearch && !(P->flags & CONV_LOWTMSC)) frg3_stage(P);
+
     /* stage 2, first call: MpStage2.h:63-83 with <false,true,DPSCAN> */
     for (int call = 0; call < 2; call++) {
         int gap0 = call == 1;
@@ -1173,7 +1634,24 @@ int gto_process_block(const gto_opts* o,
                       float* out, float* tfm, float* err,
                       char* alns, const long long* aln_off,
                       char* qss, char* rss, int nthreads) {
+    if (!o->nodetailedsearch) return 2;
+    return gto_process_block_ndx(o, nq, qlen, qx, qy, qz, qrsd, qmol, NULL, NULL,
+                                 nr, rlen, rx, ry, rz, rrsd, rmol, NULL, NULL,
+                                 out, tfm, err, alns, aln_off, qss, rss, nthreads);
+}
+
+int gto_process_block_ndx(const gto_opts* o,
+                          int nq, const int* qlen, const float* qx, const float* qy,
+                          const float* qz, const unsigned char* qrsd, const int* qmol,
+                          const float* const* qnf, const int* const* qni,
+                          int nr, const int* rlen, const float* rx, const float* ry,
+                          const float* rz, const unsigned char* rrsd, const int* rmol,
+                          const float* const* rnf, const int* const* rni,
+                          float* out, float* tfm, float* err,
+                          char* alns, const long long* aln_off,
+                          char* qss, char* rss, int nthreads) {
     if (nq < 1 || nr < 1) return 1;
+    if (!o->nodetailedsearch && (!qnf || !qni || !rnf || !rni)) return 2;
     gtb_gonnet_scores(g_gonnet);
     long long* qoff = (long long*)malloc(sizeof(long long) * (nq + 1));
     long long* roff = (long long*)malloc(sizeof(long long) * (nr + 1));
@@ -1215,6 +1693,13 @@ int gto_process_block(const gto_opts* o,
         P.qs = qss + qoff[qi]; P.rs = rss + roff[ri];
         P.qmol = qmol ? qmol[qi] : 0; P.rmol = rmol ? rmol[ri] : 0;
         P.qmax = qmax; P.qmin = qmin; P.rmax = rmax; P.rmin = rmin;
+        if (!o->nodetailedsearch) {
+            long long a = qoff[qi], b = roff[ri];
+            P.qnx = qnf[0] + a; P.qny = qnf[1] + a; P.qnz = qnf[2] + a;
+            P.qnl = qni[0] + a; P.qnr = qni[1] + a; P.qno = qni[2] + a;
+            P.rnx = rnf[0] + b; P.rny = rnf[1] + b; P.rnz = rnf[2] + b;
+            P.rnl = rni[0] + b; P.rnr = rni[1] + b; P.rno = rni[2] + b;
+        }
         int mx = P.lq > P.lr ? P.lq : P.lr;
         P.aq = (int*)malloc(sizeof(int) * (mx + 1));
         P.ar = (int*)malloc(sizeof(int) * (mx + 1));

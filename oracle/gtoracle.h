@@ -46,6 +46,13 @@ typedef struct {
     int   twotmscore;    /* --2tm-score */
     int   addsearchbyss; /* --add-search-by-ss */
     float presimilarity; /* --pre-similarity (0: off) */
+    /* the spatial-index detailed search (MpStageFrg3) */
+    int   nodetailedsearch; /* --no-detailed-search */
+    int   trigger;       /* --trigger 0..100 (percent) */
+    int   nbranches;     /* --nbranches */
+    float gapcost;       /* --gapcost as the cost: -0.8, -1.2 or -3.0 */
+    int   seedrule;      /* --seedrule as the frame: 0, 64 or 128 */
+    int   window;        /* --window 256..512 */
 } gto_opts;
 
 /* Process a block of nq queries x nr references.
@@ -65,6 +72,20 @@ int gto_process_block(const gto_opts* o,
                       float* out, float* tfm, float* err,
                       char* alns, const long long* aln_off,
                       char* qss, char* rss, int nthreads);
+
+/* The same with the blocks' index trees (the reader's six index fields per
+ * block, structures concatenated like the coordinates: node coordinates,
+ * left and right child, residue), needed when o->nodetailedsearch is 0. */
+int gto_process_block_ndx(const gto_opts* o,
+                          int nq, const int* qlen, const float* qx, const float* qy,
+                          const float* qz, const unsigned char* qrsd, const int* qmol,
+                          const float* const* qnf, const int* const* qni,
+                          int nr, const int* rlen, const float* rx, const float* ry,
+                          const float* rz, const unsigned char* rrsd, const int* rmol,
+                          const float* const* rnf, const int* const* rni,
+                          float* out, float* tfm, float* err,
+                          char* alns, const long long* aln_off,
+                          char* qss, char* rss, int nthreads);
 
 /* single building blocks (exposed for unit tests) */
 void gto_secstr(int len, const float* x, const float* y, const float* z, char* ss);

@@ -36,7 +36,10 @@ class _Opts(ctypes.Structure):
                 ("prescore", ctypes.c_float), ("scorethld", ctypes.c_float),
                 ("symmetric", ctypes.c_int), ("referenced", ctypes.c_int),
                 ("nodeletions", ctypes.c_int), ("twotmscore", ctypes.c_int),
-                ("addsearchbyss", ctypes.c_int), ("presimilarity", ctypes.c_float)]
+                ("addsearchbyss", ctypes.c_int), ("presimilarity", ctypes.c_float),
+                ("nodetailedsearch", ctypes.c_int), ("trigger", ctypes.c_int),
+                ("nbranches", ctypes.c_int), ("gapcost", ctypes.c_float),
+                ("seedrule", ctypes.c_int), ("window", ctypes.c_int)]
 
 
 _lib = None
@@ -58,6 +61,13 @@ def lib():
             fp, fp, fp, ctypes.c_void_p, ctypes.POINTER(ctypes.c_longlong),
             ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int]
         L.gto_process_block.restype = ctypes.c_int
+        L.gto_process_block_ndx.argtypes = [
+            ctypes.POINTER(_Opts),
+            ctypes.c_int, ip, fp, fp, fp, up, ip, ctypes.c_void_p, ctypes.c_void_p,
+            ctypes.c_int, ip, fp, fp, fp, up, ip, ctypes.c_void_p, ctypes.c_void_p,
+            fp, fp, fp, ctypes.c_void_p, ctypes.POINTER(ctypes.c_longlong),
+            ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int]
+        L.gto_process_block_ndx.restype = ctypes.c_int
         L.gto_solve.argtypes = [fp, ctypes.c_int, fp]
         L.gto_solve.restype = ctypes.c_int
         L.gto_secstr.argtypes = [ctypes.c_int, fp, fp, fp, ctypes.c_void_p]
@@ -83,17 +93,32 @@ class OracleResult:
 def opts_from(refinement: int = 0, convergence: int = 2, prescore: float = 0.0,
               scorethld: float = 0.0, depth: int = 2, symmetric: int = 0,
               referenced: int = 0, nodeletions: int = 0, twotmscore: int = 0,
-              addsearchbyss: int = 0, presimilarity: float = 0.0) -> _Opts:
+              addsearchbyss: int = 0, presimilarity: float = 0.0,
+              nodetailedsearch: int = 1, trigger: int = 50, nbranches: int = 5,
+              gapcost: int = 1, seedrule: int = 1, window: int = 256) -> _Opts:
     """Options in the gtalign command line's encoding: --refinement -1 log
     search, 0 coarse, 1 one search (the default), 2 full, 3 full in both final
     phases (the oracle, like the reference, stores code + 1); --depth 0..3
-    (3 = shallow); --2tm-score; --add-search-by-ss; --pre-similarity."""
+    (3 = shallow); --2tm-score; --add-search-by-ss; --pre-similarity; the
+    detailed search: --no-detailed-search, --trigger, --nbranches, --gapcost
+    code (0: -0.8, 1: -1.2, 2: -3.0), --seedrule code (0: fragments, 1: 64-,
+    2: 128-residue local alignment frames), --window."""
     return _Opts(5 if depth == 3 else 1, refinement + 1, depth, convergence,
                  prescore, scorethld, symmetric, referenced, nodeletions, twotmscore,
-                 addsearchbyss, presimilarity)
+                 addsearchbyss, presimilarity, nodetailedsearch, trigger, nbranches,
+                 (-0.8, -1.2, -3.0)[gapcost], (0, 64, 128)[seedrule], window)
 
 
-def process_block(qsoa, rsoa, opts: _Opts, nthreads: int = 0) -> OracleResult:
+def _ndx_ptrs(ndx):
+    """(float* [3], int* [3]) arrays of an index (x, y, z, left, right, residue)."""
+    fa = (ctypes.c_void_p * 3)(*[np.ascontiguousarray(a, np.float32).ctypes.data for a in ndx[:3]])
+    ia = (ctypes.c_void_p * 3)(*[np.ascontiguousarray(a, np.int32).ctypes.data for a in ndx[3:]])
+    return fa, ia
+
+
+def process_block(qsoa, rsoa, opts: _Opts, nthreads: int = 0, qndx=None, rndx=None) -> OracleResult:
+    """qndx/rndx: the blocks' index trees (six arrays each), needed when
+    opts.nodetailedsearch is 0."""
     L = lib()
     nq, nr = qsoa.n, rsoa.n
     out = np.zeros((nq * nr, NOUT), np.float32)
@@ -108,12 +133,20 @@ def process_block(qsoa, rsoa, opts: _Opts, nthreads: int = 0) -> OracleResult:
     rss = np.zeros(rsoa.total, np.uint8)
     if nthreads <= 0:
         nthreads = os.cpu_count() or 1
-    rc = L.gto_process_block(
+    keep = []
+    qf = qi_ = rf = ri_ = None
+    if qndx is not None and rndx is not None:
+        keep = [np.ascontiguousarray(a) for a in list(qndx) + list(rndx)]
+        qf, qi_ = _ndx_ptrs(keep[:6])
+        rf, ri_ = _ndx_ptrs(keep[6:])
+    rc = L.gto_process_block_ndx(
         ctypes.byref(opts),
         nq, _p(qsoa.lens, ctypes.c_int), _p(qsoa.x, ctypes.c_float), _p(qsoa.y, ctypes.c_float),
         _p(qsoa.z, ctypes.c_float), _p(qsoa.rsd, ctypes.c_ubyte), _p(qsoa.mol, ctypes.c_int),
+        qf, qi_,
         nr, _p(rsoa.lens, ctypes.c_int), _p(rsoa.x, ctypes.c_float), _p(rsoa.y, ctypes.c_float),
         _p(rsoa.z, ctypes.c_float), _p(rsoa.rsd, ctypes.c_ubyte), _p(rsoa.mol, ctypes.c_int),
+        rf, ri_,
         _p(out, ctypes.c_float), _p(tfm, ctypes.c_float), _p(err, ctypes.c_float),
         alnbuf.ctypes.data, _p(off, ctypes.c_longlong),
         qss.ctypes.data, rss.ctypes.data, nthreads)

@@ -107,7 +107,25 @@ SETS = {
     # the --speed=13 preset
     "c0_full": (lambda: synth.config0(seed=1, n_refs=1000, qlen=150), ["--no-detailed-search"]),
     "c0_full_s13": (lambda: synth.config0(seed=1, n_refs=1000, qlen=150), ["--speed=13"]),
+    # the spatial-index detailed search: every pair run alone (one query, one
+    # reference per call) on one thread, where the reference's fragment slots
+    # and score-matrix layout are the pair's own
+    "f3_default": (lambda: synth.config0(seed=301, n_refs=60, qlen=150, homolog_frac=0.3),
+                   ["--pre-score=0", "-s", "0"], 1, "perpair"),
+    "f3_speed12": (lambda: synth.config0(seed=302, n_refs=40, qlen=180, homolog_frac=0.3),
+                   ["--speed=12", "--pre-score=0", "-s", "0"], 1, "perpair"),
+    "f3_opts": (lambda: synth.config0(seed=303, n_refs=40, qlen=130, homolog_frac=0.3),
+                ["--speed=7", "--seedrule=0", "--nbranches=3", "--gapcost=2", "--window=512",
+                 "--pre-score=0", "-s", "0"], 1, "perpair"),
 }
+
+
+def run_perpair(wl, opts, threads=1, binary=BIN):
+    """Each reference in a call of its own (every query against it)."""
+    res = {}
+    for r in wl.refs:
+        res.update(run(synth.Workload(wl.queries, [r], wl.seed), opts, threads, binary))
+    return res
 
 
 def run(wl, opts, threads=8, binary=BIN):
@@ -171,14 +189,15 @@ def main():
     for name in names:
         mk, opts = SETS[name][:2]
         threads = SETS[name][2] if len(SETS[name]) > 2 else 8
+        runf = run_perpair if len(SETS[name]) > 3 and SETS[name][3] == "perpair" else run
         wl = mk()
-        res = run(wl, opts, threads, binary)
+        res = runf(wl, opts, threads, binary)
         wl2 = copy.deepcopy(wl)
         rng = np.random.default_rng(7)
         R = synth._rot_random(rng)
         q = wl2.queries[0]
         q.xyz = synth._pdb_round_fast(q.xyz.astype(np.float64) @ R.T + np.array([3.0, -5.0, 7.0]))
-        res2 = run(wl2, opts, threads, binary)
+        res2 = runf(wl2, opts, threads, binary)
         if a.gpu:
             out = {"options": opts, "seed_desc": wl.desc, "results": res,
                    "self_agreement": agreement(res, res2), "binary": "reference GPU build (sm_100a)"}

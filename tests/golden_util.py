@@ -12,7 +12,7 @@ LEVEL_SETS = {-1: "c0_level_m1", 0: "c0_level_0", 1: "c0_level_1", 2: "c0_level_
               3: "c0_level_3"}
 SETS = ["c0_speed13", "c0_default", "c0_filters", "c0_sym_ref_nodel", "c0_shallow", "c0_2tm",
         "c0_ssrr", "c0_presim", "c0_na", "c0_combo"] + \
-    list(LEVEL_SETS.values()) + ["c0_full", "c0_full_s13"]
+    list(LEVEL_SETS.values()) + ["c0_full", "c0_full_s13", "f3_default", "f3_speed12", "f3_opts"]
 # the sets the GPU golden test runs: every set the CUDA library takes (it
 # refuses nucleic-acid pairs) except the combined-options set, which pins
 # the oracle only (each of its options runs on the GPU in the option sets)
@@ -46,12 +46,14 @@ def cli_options(opts):
     """Translate the reference CLI options of a set into oracle/library options."""
     d = dict(refinement=1, convergence=18, prescore=0.4, scorethld=0.5, depth=2,
              symmetric=0, referenced=0, nodeletions=0, twotmscore=0, addsearchbyss=0,
-             presimilarity=0.0)
+             presimilarity=0.0, nodetailedsearch=0 if "--no-detailed-search" not in opts else 1,
+             trigger=50, seedrule=1, nbranches=5, gapcost=1, window=256)
     i = 0
     while i < len(opts):
         o = opts[i]
         if o == "--speed=13":
             d["refinement"], d["convergence"] = 0, 2
+            d["nodetailedsearch"] = 1
         elif o.startswith("--refinement="):
             d["refinement"] = int(o.split("=")[1])
         elif o.startswith("--depth="):
@@ -74,5 +76,34 @@ def cli_options(opts):
             d["addsearchbyss"] = 1
         elif o.startswith("--pre-similarity="):
             d["presimilarity"] = float(o.split("=")[1])
+        elif o.startswith("--speed="):
+            sp = int(o.split("=")[1])
+            d["nodetailedsearch"] = 0
+            d["depth"] = 3 if sp >= 10 else (2 if sp >= 7 else (1 if sp >= 4 else 0))
+            d["trigger"] = (0, 20, 50)[(sp - 1) % 3] if 1 <= sp <= 12 else 0
+            if sp >= 10:
+                d["refinement"], d["convergence"] = 0, 2
+        elif o.startswith("--trigger="):
+            d["trigger"] = int(o.split("=")[1])
+        elif o.startswith("--seedrule="):
+            d["seedrule"] = int(o.split("=")[1])
+        elif o.startswith("--nbranches="):
+            d["nbranches"] = int(o.split("=")[1])
+        elif o.startswith("--gapcost="):
+            d["gapcost"] = int(o.split("=")[1])
+        elif o.startswith("--window="):
+            d["window"] = int(o.split("=")[1])
         i += 1
     return d
+
+
+def oracle_opts(oracle, d):
+    """oracle options from a cli_options dict"""
+    return oracle.opts_from(
+        refinement=d["refinement"], convergence=d["convergence"], prescore=d["prescore"],
+        scorethld=d["scorethld"], symmetric=d["symmetric"], referenced=d["referenced"],
+        nodeletions=d["nodeletions"], depth=d["depth"], twotmscore=d["twotmscore"],
+        addsearchbyss=d["addsearchbyss"], presimilarity=d["presimilarity"],
+        nodetailedsearch=d.get("nodetailedsearch", 1), trigger=d.get("trigger", 50),
+        nbranches=d.get("nbranches", 5), gapcost=d.get("gapcost", 1),
+        seedrule=d.get("seedrule", 1), window=d.get("window", 256))

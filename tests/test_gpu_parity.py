@@ -18,16 +18,16 @@ def _lib_opts(d):
     return Options(refinement=d["refinement"], depth=d.get("depth", 2), convergence=d["convergence"],
                    prescore=d["prescore"], symmetric=d["symmetric"], referenced=d["referenced"],
                    nodeletions=d["nodeletions"], twotmscore=d.get("twotmscore", 0),
-                   addsearchbyss=d.get("addsearchbyss", 0), presimilarity=d.get("presimilarity", 0.0))
+                   addsearchbyss=d.get("addsearchbyss", 0), presimilarity=d.get("presimilarity", 0.0),
+                   nodetailedsearch=d.get("nodetailedsearch", 1), trigger=d.get("trigger", 50),
+                   nbranches=d.get("nbranches", 5), gapcost=d.get("gapcost", 1),
+                   seedrule=d.get("seedrule", 1), window=d.get("window", 256))
 
 
 def _ora_opts(oracle, d):
-    return oracle.opts_from(refinement=d["refinement"], convergence=d["convergence"],
-                            prescore=d["prescore"], scorethld=d["scorethld"], depth=d.get("depth", 2),
-                            symmetric=d["symmetric"], referenced=d["referenced"],
-                            nodeletions=d["nodeletions"], twotmscore=d.get("twotmscore", 0),
-                            addsearchbyss=d.get("addsearchbyss", 0),
-                            presimilarity=d.get("presimilarity", 0.0))
+    return gu.oracle_opts(oracle, dict(d, depth=d.get("depth", 2), twotmscore=d.get("twotmscore", 0),
+                                       addsearchbyss=d.get("addsearchbyss", 0),
+                                       presimilarity=d.get("presimilarity", 0.0)))
 
 
 def assert_same(res, ora, nq, nr):
@@ -43,10 +43,15 @@ def assert_same(res, ora, nq, nr):
 
 
 def run_both(oracle, q, r, d, secstr=False):
-    from gtalign_alpha_b200.api import GTalignB200
+    """The library (gtb_process_block, which builds the index trees itself when
+    the detailed search is on) and the oracle (given the same trees)."""
+    from gtalign_alpha_b200.api import GTalignB200, build_index
     with GTalignB200(0, 0, _lib_opts(d)) as g:
         res = g.process_block(q, r, scorethld=d["scorethld"], secstr=secstr)
-    ora = oracle.process_block(q, r, _ora_opts(oracle, d))
+    qx = rx = None
+    if not d.get("nodetailedsearch", 1):
+        qx, rx = build_index(q), build_index(r)
+    ora = oracle.process_block(q, r, _ora_opts(oracle, d), qndx=qx, rndx=rx)
     return res, ora
 
 
@@ -108,6 +113,16 @@ OPTSETS = {
                  addsearchbyss=1),
     "presim": dict(refinement=1, convergence=6, prescore=0.0, scorethld=0.0, symmetric=0, referenced=0, nodeletions=0,
                    presimilarity=12.0),
+    # the spatial-index detailed search: defaults (--speed 9), --speed 12, and
+    # the fragment seeds with other options
+    "frg3": dict(refinement=1, convergence=6, prescore=0.2, scorethld=0.2, symmetric=0, referenced=0, nodeletions=0,
+                 nodetailedsearch=0),
+    "frg3s12": dict(refinement=0, convergence=2, prescore=0.0, scorethld=0.0, symmetric=0, referenced=0, nodeletions=0,
+                    nodetailedsearch=0, depth=3),
+    "frg3opts": dict(refinement=1, convergence=4, prescore=0.0, scorethld=0.0, symmetric=1, referenced=0, nodeletions=0,
+                     nodetailedsearch=0, trigger=0, seedrule=0, nbranches=3, gapcost=2, window=512),
+    "frg3seed2": dict(refinement=1, convergence=4, prescore=0.0, scorethld=0.0, symmetric=0, referenced=0, nodeletions=0,
+                      nodetailedsearch=0, trigger=20, seedrule=2, nbranches=8, gapcost=0),
 }
 
 

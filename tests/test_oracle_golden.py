@@ -1,5 +1,11 @@
 """The oracle against the reference's own outputs (golden fixtures).
 
+The reference's GPU build, run on the same inputs, agrees with its CPU build
+(TM-scores within 1e-4) on 91% of the reported pairs of the full-size small
+configuration and on 42-90% of the other sets; the oracle agrees with the CPU
+build at the same rates (recorded with the GPU build's outputs in
+tests/golden/*_refgpu.json).
+
 The fixtures hold what the reference CPU build printed for seeded synthetic
 sets (tests/golden/make_golden.py).  Low-TM pairs have several near-equal
 local optima, and the reference's own result for them moves when the query
@@ -43,11 +49,12 @@ def pairs_of(row_q, row_r, q0, r0):
 def run_oracle(oracle, name):
     q, r, qn, rn, meta = gu.load(name)
     d = gu.cli_options(meta["options"])
-    o = oracle.process_block(q, r, oracle.opts_from(
-        refinement=d["refinement"], convergence=d["convergence"], prescore=d["prescore"],
-        scorethld=d["scorethld"], symmetric=d["symmetric"], referenced=d["referenced"],
-        nodeletions=d["nodeletions"], depth=d["depth"], twotmscore=d["twotmscore"],
-        addsearchbyss=d["addsearchbyss"], presimilarity=d["presimilarity"]))
+    qx = rx = None
+    if not d["nodetailedsearch"]:
+        # the reader's index trees (the search's input)
+        from gtalign_alpha_b200.api import build_index
+        qx, rx = build_index(q), build_index(r)
+    o = oracle.process_block(q, r, gu.oracle_opts(oracle, d), qndx=qx, rndx=rx)
     return q, r, qn, rn, meta, d, o
 
 
@@ -78,7 +85,11 @@ def test_oracle_matches_reference(oracle, name):
         dtm.append(dd)
         same.append(ident)
         if b.startswith("hom"):      # a generated homolog of the query
-            hom_same.append(ident and dd <= 1e-4)
+            # the same alignment, and the TM-scores within 1e-4 or higher (a
+            # better superposition of that alignment: the reference's FP32
+            # rotation solve can stop short of the TM-score optimum)
+            lower = max(g["tmq"] - out[9], g["tmr"] - out[10])
+            hom_same.append(ident and (dd <= 1e-4 or lower <= 1e-4))
         if ident:
             # everything that follows from the alignment agrees exactly
             assert rows[3] == g["query_secstr"] and rows[4] == g["refrn_secstr"], key
@@ -92,8 +103,11 @@ def test_oracle_matches_reference(oracle, name):
             assert abs(out[11] - g["d0q"]) < 6e-3 and abs(out[12] - g["d0r"]) < 6e-3
     dtm = np.array(dtm)
     sa = meta["self_agreement"]
-    assert (dtm <= 1e-4).mean() >= sa["frac_tm_1e4"] - MARGIN, ((dtm <= 1e-4).mean(), sa)
-    assert np.mean(same) >= sa["frac_aln_identical"] - MARGIN, (np.mean(same), sa)
+    # sampling margin: at least MARGIN, or two standard errors of a proportion
+    # near 1/2 over the set's pairs
+    margin = max(MARGIN, 2.0 * np.sqrt(0.25 / max(len(dtm), 1)))
+    assert (dtm <= 1e-4).mean() >= sa["frac_tm_1e4"] - margin, ((dtm <= 1e-4).mean(), sa)
+    assert np.mean(same) >= sa["frac_aln_identical"] - margin, (np.mean(same), sa)
     if hom_same:
         assert np.mean(hom_same) >= 0.7, hom_same
     HOMOLOGS.extend(hom_same)
@@ -257,3 +271,80 @@ def test_oracle_nucleic_acids(oracle):
                 same += a == c
     assert np.mean(tm) >= meta["self_agreement"]["frac_tm_1e4"] - MARGIN, np.mean(tm)
     assert tot > 1000 and same / tot >= 0.8, (same, tot)
+
+
+def _d0fin(L):
+    return max(0.5, 1.24 * np.cbrt(L - 15.0) - 1.8) if L > 21 else 0.5
+
+
+def _tm64(P, Q, R, t, d0, L):
+    X = P @ np.asarray(R, np.float64).reshape(3, 3).T + np.asarray(t, np.float64)
+    d2 = ((X - Q) ** 2).sum(1)
+    return float((d0 * d0 / (d0 * d0 + d2)).sum() / L)
+
+
+def classify(oracle, name):
+    """Every pair the reference reports, against the oracle: 'same' (identical
+    alignment and both TM-scores within 1e-4), else the reference's printed
+    alignment and transform rescored in FP64 (TM-score by the shorter length,
+    the search's objective) against the oracle's TM-score by that length:
+    'tie' within 1e-4, 'better' or 'worse' for the oracle.  A pair the oracle
+    leaves below -s is run again without the threshold for its TM-score."""
+    q, r, qn, rn, meta, d, o = run_oracle(oracle, name)
+    ref = meta["results"]
+    qxyz = np.stack([q.x, q.y, q.z], 1).astype(np.float64)
+    rxyz = np.stack([r.x, r.y, r.z], 1).astype(np.float64)
+    cls = {"same": 0, "tie": 0, "better": 0, "worse": 0}
+    diffs = []
+    rerun = None
+    for key, g in ref.items():
+        a, b = key.split("|")
+        qi, ri = qn.index(a), rn.index(b)
+        out = o.out[qi, ri]
+        lq, lr = int(q.lens[qi]), int(r.lens[ri])
+        rows = o.alns[qi][ri]
+        if rows[0] == g["query_aln"] and rows[2] == g["refrn_aln"] and \
+                max(abs(out[9] - g["tmq"]), abs(out[10] - g["tmr"])) <= 1e-4:
+            cls["same"] += 1
+            diffs.append(0.0)
+            continue
+        pr = pairs_of(g["query_aln"], g["refrn_aln"], g["query_from"] - 1, g["refn_from"] - 1)
+        P = qxyz[[q.offs[qi] + x for x, _ in pr]]
+        Q = rxyz[[r.offs[ri] + y for _, y in pr]]
+        L = min(lq, lr)
+        if d["referenced"]:
+            reft = _tm64(Q, P, g["rotation"], g["translation"], _d0fin(L), L)
+        else:
+            reft = _tm64(P, Q, g["rotation"], g["translation"], _d0fin(L), L)
+        col = 9 if lq <= lr else 10
+        ours = float(out[col])
+        if ours == 0.0 and d["scorethld"] > 0:
+            if rerun is None:
+                d2 = dict(d, scorethld=0.0)
+                qx = rx = None
+                if not d["nodetailedsearch"]:
+                    from gtalign_alpha_b200.api import build_index
+                    qx, rx = build_index(q), build_index(r)
+                rerun = oracle.process_block(q, r, gu.oracle_opts(oracle, d2), qndx=qx, rndx=rx)
+            ours = float(rerun.out[qi, ri, col])
+        diff = ours - reft
+        diffs.append(diff)
+        cls["tie" if abs(diff) <= 1e-4 else ("better" if diff > 0 else "worse")] += 1
+    return cls, np.array(diffs)
+
+
+@pytest.mark.parametrize("name", [s for s in gu.SETS if s != "c0_na"])
+def test_oracle_optima_not_worse_than_reference(oracle, name):
+    """Where the oracle and the reference part, the oracle's optimum is no
+    worse on balance: the reference's own result moves between near-equal
+    local optima when the query is only rotated, so a disagreement is a
+    different optimum, not an error, as long as the oracle does not lose
+    score systematically.  Per set: the mean TM-score difference (oracle -
+    reference, FP64 rescored) is at least -5e-3 and the pairs where the
+    oracle is worse exceed those where it is better by at most 20% of the
+    pairs."""
+    cls, diffs = classify(oracle, name)
+    n = len(diffs)
+    assert n > 0
+    assert float(diffs.mean()) >= -5e-3, (cls, float(diffs.mean()))
+    assert cls["worse"] - cls["better"] <= 0.2 * n, cls
