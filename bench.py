@@ -90,6 +90,25 @@ def progress(msg: str) -> None:
     print("[bench %7.1fs] %s" % (time.time() - _T0, msg), file=sys.stderr, flush=True)
 
 
+def lib_options(args, polish: int):
+    """The library's options of the run: --speed 9 (the command line's
+    default, detailed search on) or 13 (--no-detailed-search), -s 0.5."""
+    from gtalign_alpha_b200.api import Options
+    if args.speed == 13:
+        return Options(polish_steps=polish)      # defaults with --no-detailed-search
+    return Options.speed(args.speed, polish_steps=polish)
+
+
+def cli_options(args):
+    """The same options on the reference's command line."""
+    return ["--no-detailed-search"] if args.speed == 13 else ["--speed=%d" % args.speed]
+
+
+def options_text(args) -> str:
+    return ("gtalign defaults with --no-detailed-search, -s 0.5" if args.speed == 13
+            else "gtalign defaults (--speed %d: the spatial-index detailed search on), -s 0.5" % args.speed)
+
+
 def dist_env():
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -300,8 +319,8 @@ def run_ours(args):
     qchunks = [subset(q, np.arange(c * args.qchunk, min(q.n, (c + 1) * args.qchunk))) for c in range(nchunk)]
     qbs = [pack_fields(c) for c in qchunks]
     rb = pack_fields(r)
-    gp = GTalignB200(dev, 0, Options(polish_steps=args.polish_steps))
-    g0 = GTalignB200(dev, 0, Options())
+    gp = GTalignB200(dev, 0, lib_options(args, args.polish_steps))
+    g0 = GTalignB200(dev, 0, lib_options(args, 0))
 
     # resident blocks (uploaded once, used by both handles on this device)
     L.gtb_block_upload.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p)]
@@ -433,7 +452,7 @@ def run_ours(args):
                        "step": "%d queries x %d references%s" % (args.qchunk, args.nrefs,
                                                                  " (split over the ranks)" if ws > 1 else ""),
                        "form": "batched + adjoint polishing (%d steps)" % args.polish_steps,
-                       "options": "gtalign defaults with --no-detailed-search, -s 0.5",
+                       "options": options_text(args),
                        "l2": "inputs larger than L2 (%.0f MB of reference coordinates)" % (12 * r_all.total / 1e6),
                        "parallelism": "dp%d (references split by cost, independent pairs)" % ws},
             "accuracy": {"max_err_tm": max(A["maxerr"][:2]), "max_err_rmsd": A["maxerr"][2],
@@ -485,6 +504,18 @@ def e2e_run(L, g, qbs, rb, qchunks, r, step_pairs, maxpairs, args, ws, rank, dev
             beg[f] = t.data_ptr()
             end[f] = t.data_ptr() + t.numel()
         pin[nm] = (arrs, beg, end)
+    # with the detailed search the reader's index trees travel with the blocks
+    # (made once, as the reader makes them with the blocks)
+    ndx = {}
+    if args.speed != 13:
+        from gtalign_alpha_b200.api import build_index
+        for nm, soa in [("q%d" % c, qc) for c, qc in enumerate(qchunks)] + [("r", r)]:
+            arrs = []
+            for a in build_index(soa):
+                t = torch.empty(a.nbytes, dtype=torch.uint8, pin_memory=True)
+                t.numpy()[:] = a.view(np.uint8).ravel()
+                arrs.append(t)
+            ndx[nm] = (arrs, (ctypes.c_void_p * 6)(*[t.data_ptr() for t in arrs]))
     h_out = torch.empty(maxpairs * 16, dtype=torch.float32, pin_memory=True)
     h_tfm = torch.empty(maxpairs * 12, dtype=torch.float32, pin_memory=True)
     h_err = torch.empty(maxpairs * 4, dtype=torch.float32, pin_memory=True)
@@ -497,8 +528,13 @@ def e2e_run(L, g, qbs, rb, qchunks, r, step_pairs, maxpairs, args, ws, rank, dev
 
     def process(k):
         qk = "q%d" % (k % nchunk)
-        st = L.gtb_process_block(g.handle, ctypes.c_float(0.5), pin[qk][1], pin[qk][2],
-                                 pin["r"][1], pin["r"][2], ctypes.byref(res))
+        if ndx:
+            st = L.gtb_process_block_ndx(g.handle, ctypes.c_float(0.5), pin[qk][1], pin[qk][2],
+                                         ndx[qk][1], pin["r"][1], pin["r"][2], ndx["r"][1],
+                                         ctypes.byref(res))
+        else:
+            st = L.gtb_process_block(g.handle, ctypes.c_float(0.5), pin[qk][1], pin[qk][2],
+                                     pin["r"][1], pin["r"][2], ctypes.byref(res))
         if st != 0:
             raise RuntimeError(L.gtb_last_error(g.handle).decode())
         n = step_pairs[k % nchunk]
@@ -534,6 +570,9 @@ def e2e_run(L, g, qbs, rb, qchunks, r, step_pairs, maxpairs, args, ws, rank, dev
     ms = _max_over_ranks(e2.elapsed_time(e3), ws, dev)
     allpairs = _sum_over_ranks(done, ws, dev)
     h2d = int(np.mean([sum(a.nbytes for a in qb.arrays) for qb in qbs])) + sum(a.nbytes for a in rb.arrays)
+    if ndx:
+        h2d += int(np.mean([sum(t.numel() for t in ndx["q%d" % c][0]) for c in range(nchunk)]))
+        h2d += sum(t.numel() for t in ndx["r"][0])
     d2h = int(np.mean(step_pairs)) * (16 + 12 + 4) * 4 + int(np.mean(d2h_rows))
     return {"value": allpairs / (ms / 1000.0), "unit": UNIT, "h2d_bytes_per_step": h2d,
             "d2h_bytes_per_step": d2h, "ms_per_step": ms / args.steps,
@@ -642,9 +681,18 @@ def ref_binary():
     return p if os.path.exists(p) else None
 
 
-def run_reference_sample(wl, nq: int, nref: int, threads: int):
+# Runs of the reference CPU build that stalled (every thread waiting on a
+# futex, no progress: an intermittent deadlock of its worker threads, seen on
+# about one call in six with 8 threads and 250 references) and were restarted.
+REF_STALLS = {"stalled": 0, "calls": 0}
+REF_CALL_LIMIT_S = 20          # a call of the samples here takes a few seconds
+
+
+def run_reference_sample(wl, nq: int, nref: int, threads: int, args):
     """Time the reference CPU build (or the oracle port) on the first nq
-    queries x nref references of the workload.  Returns (pairs, seconds, kind)."""
+    queries x nref references of the workload.  Returns (pairs, seconds, kind).
+    The time is the build's own "query batch execution time"; a call that
+    stalls is killed after REF_CALL_LIMIT_S and run again (REF_STALLS)."""
     from gtalign_alpha_b200 import synth
     binp = ref_binary()
     sub = synth.Workload(wl.queries[:nq], wl.refs[:nref], wl.seed)
@@ -653,9 +701,19 @@ def run_reference_sample(wl, nq: int, nref: int, threads: int):
         try:
             synth.write_dirs(sub, d + "/q", d + "/r")
             cmd = [binp, "--qrs=" + d + "/q", "--rfs=" + d + "/r", "-o", d + "/out", "--outfmt=1",
-                   "--cpu-threads=%d" % threads, "--cpu-threads-reading=1", "--no-detailed-search",
-                   "--dev-queries-per-chunk=%d" % max(1, nq)]
-            subprocess.run(cmd, capture_output=True, check=True)
+                   "--cpu-threads=%d" % threads, "--cpu-threads-reading=1",
+                   "--dev-queries-per-chunk=%d" % max(1, nq)] + cli_options(args)
+            for attempt in range(5):
+                REF_STALLS["calls"] += 1
+                shutil.rmtree(d + "/out", ignore_errors=True)
+                try:
+                    subprocess.run(cmd, capture_output=True, check=True, timeout=REF_CALL_LIMIT_S)
+                    break
+                except subprocess.TimeoutExpired:
+                    REF_STALLS["stalled"] += 1
+                    progress("reference CPU build stalled; run again (%d)" % REF_STALLS["stalled"])
+            else:
+                raise RuntimeError("the reference CPU build stalled 5 times in a row")
             secs = 0.0
             seen = set()
             for f in os.listdir(d + "/out"):
@@ -671,8 +729,15 @@ def run_reference_sample(wl, nq: int, nref: int, threads: int):
     import pyoracle
     q, r = synth.pack(sub.queries), synth.pack(sub.refs)
     t = time.time()
+    ndx = {}
+    if args.speed != 13:
+        from gtalign_alpha_b200.api import build_index
+        ndx = dict(qndx=build_index(q), rndx=build_index(r))
     pyoracle.process_block(q, r, pyoracle.opts_from(refinement=1, convergence=18, prescore=0.4,
-                                                    scorethld=0.5), nthreads=threads)
+                                                    scorethld=0.5,
+                                                    nodetailedsearch=1 if args.speed == 13 else 0,
+                                                    trigger=(0, 20, 50)[(args.speed - 1) % 3]),
+                           nthreads=threads, **ndx)
     return nq * nref, time.time() - t, "port"
 
 
@@ -692,8 +757,8 @@ def reference_gpu_sample(wl, args, value):
     try:
         synth.write_dirs(sub, d + "/q", d + "/r")
         cmd = [binp, "--qrs=" + d + "/q", "--rfs=" + d + "/r", "-o", d + "/out", "--outfmt=1",
-               "--no-detailed-search", "--dev-queries-per-chunk=%d" % nq, "--dev-N=1",
-               "--cpu-threads-reading=4"]
+               "--dev-queries-per-chunk=%d" % nq, "--dev-N=1",
+               "--cpu-threads-reading=4"] + cli_options(args)
         t0 = time.perf_counter()
         p = subprocess.run(cmd, capture_output=True, timeout=args.refgpu_timeout)
         wall = time.perf_counter() - t0
@@ -708,8 +773,7 @@ def reference_gpu_sample(wl, args, value):
                 secs += t
         v = nq * nref / secs
         return {"value": v, "unit": UNIT, "wall_s": wall, "batch_s": secs,
-                "sample": "%d queries x %d references of the workload, default options with "
-                          "--no-detailed-search" % (nq, nref),
+                "sample": "%d queries x %d references of the workload, %s" % (nq, nref, options_text(args)),
                 "ours_vs_reference_gpu": value / v}
     except subprocess.TimeoutExpired:
         return {"unavailable": "reference GPU build did not finish within %d s" % args.refgpu_timeout}
@@ -753,20 +817,21 @@ def plain_sample(g, L, q, r, npairs: int, seed: int):
 
 def cpu_baseline_sample(wl, args):
     """The reference CPU build over all the workload's queries, each against
-    the first cpu_sample_refs / 8 references (one call per query, as the
+    the first cpu_sample_refs / 4 references (one call per query, as the
     reference arm cycles queries)."""
     threads = os.cpu_count() or 1
     from gtalign_alpha_b200 import synth
-    nref = max(50, args.cpu_sample_refs // 8)
+    nref = max(50, args.cpu_sample_refs // 4)
     pairs, secs, kind = 0, 0.0, "reference"
     for qi in range(len(wl.queries)):
         sub = synth.Workload(wl.queries[qi:qi + 1], wl.refs, wl.seed)
-        p, s, kind = run_reference_sample(sub, 1, nref, threads)
+        p, s, kind = run_reference_sample(sub, 1, nref, threads, args)
         pairs += p
         secs += s
     return {"value": pairs / secs, "unit": UNIT, "cores": threads, "kind": kind, "cpu": cpu_model(),
-            "sample": "each of the %d queries x the first %d references of the workload, default "
-                      "options with --no-detailed-search; %.1f s in all" % (len(wl.queries), nref, secs)}
+            "sample": "each of the %d queries x the first %d references of the workload, %s; "
+                      "%.1f s in all" % (len(wl.queries), nref, options_text(args), secs),
+            "stalled_runs_restarted": dict(REF_STALLS)}
 
 
 def run_reference(args):
@@ -777,12 +842,12 @@ def run_reference(args):
     from gtalign_alpha_b200 import synth
     wl = synth.config1(seed=args.seed, n_queries=args.nqueries, n_refs=args.cpu_sample_refs * 2)
     for _ in range(args.warmup):
-        run_reference_sample(wl, 1, 50, threads)
+        run_reference_sample(wl, 1, 50, threads, args)
     tot_pairs, tot_s, kind = 0, 0.0, "reference"
     for k in range(args.steps):
         qi = k % args.nqueries
         sub = synth.Workload(wl.queries[qi:qi + 1], wl.refs, wl.seed)
-        pairs, secs, kind = run_reference_sample(sub, 1, args.cpu_sample_refs, threads)
+        pairs, secs, kind = run_reference_sample(sub, 1, args.cpu_sample_refs, threads, args)
         tot_pairs += pairs
         tot_s += secs
     v = tot_pairs / tot_s
@@ -791,11 +856,12 @@ def run_reference(args):
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded C-alpha traces)",
             "config": {"workload": "16 queries x %d references (log-normal lengths, median 250)" % args.nrefs,
-                       "options": "gtalign defaults with --no-detailed-search",
+                       "options": options_text(args),
                        "parallelism": "host cores"},
             "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": kind, "cpu": cpu_model(),
                              "sample": "per step 1 query (cycling over the 16) x %d references of the "
-                                       "workload" % args.cpu_sample_refs},
+                                       "workload" % args.cpu_sample_refs,
+                             "stalled_runs_restarted": dict(REF_STALLS)},
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -810,6 +876,8 @@ def main():
     ap.add_argument("--nqueries", type=int, default=16)
     ap.add_argument("--qchunk", type=int, default=2, help="queries per step (the reference's --dev-queries-per-chunk)")
     ap.add_argument("--seed", type=int, default=2)
+    ap.add_argument("--speed", type=int, default=13, choices=[7, 8, 9, 10, 11, 12, 13],
+                    help="the command line's --speed preset (13: --no-detailed-search; 9: its default)")
     ap.add_argument("--cpu-sample-refs", type=int, default=2000)
     ap.add_argument("--polish-steps", type=int, default=5,
                     help="adjoint polishing steps of the headline (batched + adjoint) form")

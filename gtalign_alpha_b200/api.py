@@ -48,7 +48,8 @@ class _COptions(ctypes.Structure):
                 ("addsearchbyss", ctypes.c_int), ("twotmscore", ctypes.c_int),
                 ("polish_steps", ctypes.c_int), ("presimilarity", ctypes.c_float),
                 ("trigger", ctypes.c_int), ("nbranches", ctypes.c_int),
-                ("gapcost", ctypes.c_int), ("seedrule", ctypes.c_int), ("window", ctypes.c_int)]
+                ("gapcost", ctypes.c_int), ("seedrule", ctypes.c_int), ("window", ctypes.c_int),
+                ("clsfilter", ctypes.c_int), ("clscoverage", ctypes.c_float)]
 
 
 class _CResults(ctypes.Structure):
@@ -82,6 +83,8 @@ class Options:
     gapcost: int = 1           # --gapcost code: -0.8, -1.2, -3.0
     seedrule: int = 1          # --seedrule code: fragments, 64-, 128-residue frames
     window: int = 256          # --window
+    clsfilter: int = 0         # 1: a clustering run's prefilter (blocks carry global indices)
+    clscoverage: float = 0.7   # --cls-coverage
 
     @classmethod
     def speed(cls, level: int, **kw) -> "Options":
@@ -105,7 +108,8 @@ class Options:
                          self.symmetric, self.referenced, self.nodeletions,
                          self.nodetailedsearch, self.addsearchbyss, self.twotmscore,
                          self.polish_steps, self.presimilarity, self.trigger, self.nbranches,
-                         self.gapcost, self.seedrule, self.window)
+                         self.gapcost, self.seedrule, self.window, self.clsfilter,
+                         self.clscoverage)
 
 
 _lib = None
@@ -161,8 +165,10 @@ class PackedBlock:
     npos: int
 
 
-def pack_fields(s: SoA) -> PackedBlock:
-    """Lay out a block the way PMBatchStrData does (one array per field)."""
+def pack_fields(s: SoA, types=None) -> PackedBlock:
+    """Lay out a block the way PMBatchStrData does (one array per field).
+    types: the structures' global indices in a clustering run (pps2DType), or
+    None (zeros)."""
     n, N = s.n, s.total
     insch = np.zeros(N, np.int32)
     first = s.offs[s.mol > 0]
@@ -170,7 +176,7 @@ def pack_fields(s: SoA) -> PackedBlock:
     arrays = [
         np.ascontiguousarray(s.lens, np.int32),
         np.ascontiguousarray(s.offs, np.uint32),
-        np.zeros(n, np.int32),
+        np.zeros(n, np.int32) if types is None else np.ascontiguousarray(types, np.int32),
         np.ascontiguousarray(s.x, np.float32),
         np.ascontiguousarray(s.y, np.float32),
         np.ascontiguousarray(s.z, np.float32),
@@ -300,10 +306,13 @@ class GTalignB200:
 
     def process_block(self, queries: SoA, refs: SoA, scorethld: float = 0.5,
                       alignments: bool = True, numerr: bool = True,
-                      secstr: bool = False, qndx=None, rndx=None) -> BlockResult:
+                      secstr: bool = False, qndx=None, rndx=None, qtypes=None,
+                      rtypes=None) -> BlockResult:
         """qndx/rndx (build_index): the blocks' index trees as a reader made
-        them; without them the library builds the same when it needs them."""
-        qb, rb = pack_fields(queries), pack_fields(refs)
+        them; without them the library builds the same when it needs them.
+        qtypes/rtypes: the structures' global indices in a clustering run
+        (Options.clsfilter)."""
+        qb, rb = pack_fields(queries, qtypes), pack_fields(refs, rtypes)
         return self.process_packed(qb, rb, scorethld, alignments, numerr, secstr, qndx=qndx,
                                    rndx=rndx)
 

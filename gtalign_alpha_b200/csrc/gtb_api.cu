@@ -163,6 +163,11 @@ static gtb_status check_options(gtb_handle* h) {
         snprintf(h->err, sizeof(h->err), "--pre-similarity out of range");
         return GTB_ERR_ARG;
     }
+    if (o.clsfilter < 0 || o.clsfilter > 1 ||
+        (o.clsfilter && !(o.clscoverage > 0.f && o.clscoverage <= 1.f))) {
+        snprintf(h->err, sizeof(h->err), "--cls-coverage out of (0,1]");
+        return GTB_ERR_ARG;
+    }
     if (o.polish_steps < 0 || o.polish_steps > 50) {
         snprintf(h->err, sizeof(h->err), "polish_steps %d out of 0..50", o.polish_steps);
         return GTB_ERR_ARG;
@@ -186,6 +191,10 @@ struct DevBlock {
     // index trees (null: none)
     const float *qnx = nullptr, *qny = nullptr, *qnz = nullptr, *rnx = nullptr, *rny = nullptr, *rnz = nullptr;
     const int *qnl = nullptr, *qnr = nullptr, *qno = nullptr, *rnl = nullptr, *rnr = nullptr, *rno = nullptr;
+    // clustering runs: the references' global indices and the end of the
+    // query block's (qrysernrbeg + nqystrs, CuBatch.cu:492-494)
+    const int* rtype = nullptr;
+    int qtypeend = 0;
     std::vector<int> hqlen, hrlen;
 };
 
@@ -264,6 +273,11 @@ static gtb_status run_block(gtb_handle* h, const DevBlock& D, float scorethld,
     // (CuBatch.cu:459-462)
     B.presim = (0.f < o.presimilarity && PRESIM_EDGE < B.qmax && PRESIM_EDGE < B.rmax) ? o.presimilarity : 0.f;
     B.symmetric = o.symmetric; B.nodeletions = o.nodeletions;
+    B.cls = o.clsfilter ? 1 : 0;
+    if (B.cls) {
+        if (!D.rtype) { snprintf(h->err, sizeof(h->err), "a clustering run needs the type field"); return GTB_ERR_ARG; }
+        B.rtype = D.rtype; B.clsqend = D.qtypeend; B.clscov = o.clscoverage;
+    }
     B.f3 = o.nodetailedsearch ? 0 : 1;
     if (B.f3) {
         if (!D.qnx || !D.rnx) {
@@ -611,6 +625,7 @@ struct HostSoA {
     const float *x = nullptr, *y = nullptr, *z = nullptr;
     const int* insch = nullptr;
     const char* rsd = nullptr;
+    const int* type = nullptr;      // global indices of a clustering run (may be null)
     std::vector<int> mol, off;
 };
 
@@ -631,6 +646,7 @@ static gtb_status parse_soa(gtb_handle* h, char* const* beg, char* const* end, H
     S.x = (const float*)beg[GTB_FLD_X]; S.y = (const float*)beg[GTB_FLD_Y]; S.z = (const float*)beg[GTB_FLD_Z];
     S.insch = (const int*)beg[GTB_FLD_INSCHORD];
     S.rsd = beg[GTB_FLD_RSD];
+    S.type = (const int*)beg[GTB_FLD_TYPE];
     S.mol.resize(S.n); S.off.resize(S.n);
     for (int i = 0; i < S.n; i++) {
         int L = S.len[i];
@@ -683,8 +699,9 @@ struct gtb_block {
     int n = 0;
     long long npos = 0;
     std::vector<int> len, off, mol;
+    int typemin = 0;                 // smallest global index (clustering runs)
     char* dbase = nullptr;
-    int *dlen = nullptr, *doff = nullptr, *dmol = nullptr;
+    int *dlen = nullptr, *doff = nullptr, *dmol = nullptr, *dtype = nullptr;
     float *x = nullptr, *y = nullptr, *z = nullptr;
     float4* c4 = nullptr;
     cudaStream_t st = nullptr;       // stream of the allocation and of the free
@@ -744,9 +761,14 @@ static gtb_status upload_block(gtb_handle* h, const HostSoA& S, gtb_block* b,
     b->n = S.n; b->npos = S.npos;
     b->len.assign(S.len, S.len + S.n);
     b->off = S.off; b->mol = S.mol;
+    // a clustering run's global indices (pps2DType; TdDataReader.cpp:736-745)
+    const bool cls = h->opts.clsfilter != 0;
+    if (cls && !S.type) { snprintf(h->err, sizeof(h->err), "a clustering run needs the type field"); return GTB_ERR_ARG; }
+    if (cls) b->typemin = *std::min_element(S.type, S.type + S.n);
     size_t sz = 0;
     auto carve = [&](size_t bytes) { size_t o2 = sz; sz += align256(bytes); return o2; };
     size_t ol = carve(S.n * 4), oo = carve(S.n * 4), om = carve(S.n * 4);
+    size_t ot = cls ? carve(S.n * 4) : 0;
     size_t ox = carve(S.npos * 4), oy = carve(S.npos * 4), oz = carve(S.npos * 4);
     size_t oa = carve(S.npos), os = carve(S.npos);
     size_t o4 = carve(S.npos * 16);
@@ -756,6 +778,10 @@ static gtb_status upload_block(gtb_handle* h, const HostSoA& S, gtb_block* b,
     b->st = st;
     char* d = b->dbase;
     b->dlen = (int*)(d + ol); b->doff = (int*)(d + oo); b->dmol = (int*)(d + om);
+    if (cls) {
+        b->dtype = (int*)(d + ot);
+        CK(cudaMemcpyAsync(b->dtype, S.type, S.n * 4, cudaMemcpyHostToDevice, st));
+    }
     b->x = (float*)(d + ox); b->y = (float*)(d + oy); b->z = (float*)(d + oz);
     b->rsd = (unsigned char*)(d + oa); b->ss = d + os;
     b->c4 = (float4*)(d + o4);
@@ -825,6 +851,7 @@ static DevBlock make_devblock(const gtb_block* Q, const gtb_block* R) {
     D.qa = Q->rsd; D.ra = R->rsd; D.qs = Q->ss; D.rs = R->ss;
     D.qnx = Q->nx; D.qny = Q->ny; D.qnz = Q->nz; D.qnl = Q->nl; D.qnr = Q->nr; D.qno = Q->no;
     D.rnx = R->nx; D.rny = R->ny; D.rnz = R->nz; D.rnl = R->nl; D.rnr = R->nr; D.rno = R->no;
+    D.rtype = R->dtype; D.qtypeend = Q->typemin + Q->n;
     D.hqlen = Q->len; D.hrlen = R->len;
     return D;
 }

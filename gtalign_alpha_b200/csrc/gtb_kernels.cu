@@ -156,13 +156,23 @@ void launch_pack4_structs(float4* out, const float* x, const float* y, const flo
 
 // ---------------------------------------------------------------------------
 // pair initialisation: MpStage1.cpp:28-167
+// the clustering run's prefilter of a pair (CheckMaxCoverage)
+__device__ __forceinline__ bool cls_pass(const Blk& B, int qi, int ri) {
+    const float lq = (float)B.qlen[qi], lr = (float)B.rlen[ri];
+    return B.rtype[ri] < B.clsqend && __fmul_rn(fmaxf(lq, lr), B.clscov) <= fminf(lq, lr);
+}
+
 __global__ void k_init(Blk B, Bat T) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= T.np) return;
     int qi = pair_qi(B, T, i), ri = pair_ri(B, T, i);
-    // with the --pre-similarity screen every pair starts filtered, with no
-    // molecule-type check (custage1.cu:74-82); k_presim releases the ones that pass
-    T.flags[i] = (B.presim > 0.f || B.qmol[qi] != B.rmol[ri]) ? CONV_LOWTMSC : 0;
+    // with the --pre-similarity screen or in a clustering run every pair starts
+    // filtered, with no molecule-type check (custage1.cu:74-82); a clustering
+    // run releases the pairs of its triangle whose lengths can reach the
+    // coverage (CheckMaxCoverage, coverage.cu:28-52), and k_presim then
+    // releases, of the rest, the ones that pass its screen
+    if (B.cls) T.flags[i] = cls_pass(B, qi, ri) ? 0 : CONV_LOWTMSC;
+    else T.flags[i] = (B.presim > 0.f || B.qmol[qi] != B.rmol[ri]) ? CONV_LOWTMSC : 0;
     T.grand[i] = 0.f; T.best[i] = 0.f; T.best0[i] = 0.f; T.rmsd32[i] = -1.f;
     T.seedq[i] = 0; T.seedr[i] = 0; T.naln[i] = 0;
     T.sfndx[i] = T.sfpos[i] = T.sfndx_cur[i] = T.sfpos_cur[i] = 0;
@@ -198,6 +208,7 @@ __global__ void __launch_bounds__(128) k_presim(Blk B, Bat T) {
     const int i = blockIdx.x * 4 + (threadIdx.x >> 5);
     if (i >= T.np) return;                        // the same for the whole warp
     int qi = pair_qi(B, T, i), ri = pair_ri(B, T, i);
+    if (B.cls && cls_pass(B, qi, ri)) return;     // released already (similarity.cu:60-65)
     const int ql = B.qlen[qi], rl = B.rlen[ri];
     const unsigned char* qa = B.qa + B.qoff[qi];
     const unsigned char* ra = B.ra + B.roff[ri];

@@ -57,6 +57,12 @@ struct Blk {
     const int *qnl, *qnr, *qno, *rnl, *rnr, *rno;
     int f3trigger, f3nbranches, f3seedrule, f3window;
     float f3gapcost;
+    // clustering runs: the prefilter of CheckMaxCoverage (cls = 1): the
+    // references' global indices, the end of the query block's, the coverage
+    int cls;
+    const int* rtype;
+    int clsqend;
+    float clscov;
 };
 
 // detailed search: fragment slots, branches per pair at most

@@ -130,9 +130,9 @@ extern "C" gtb_status gtb_process_block_noalloc(int device, const gtb_options* o
         setmsg(errbuf, errlen, "null argument or device out of range (%lld, %lld)", device, MAXDEV);
         return GTB_ERR_ARG;
     }
-    if (!opts->nodetailedsearch) {
-        setmsg(errbuf, errlen, "the spatial-index detailed search is not implemented (%lld %lld)",
-               !opts->nodetailedsearch, 0);
+    if (!opts->nodetailedsearch || opts->clsfilter) {
+        setmsg(errbuf, errlen, "the detailed search (%lld) and the clustering prefilter (%lld) are not implemented here",
+               !opts->nodetailedsearch, (long long)opts->clsfilter);
         return GTB_ERR_UNSUPPORTED;
     }
     if (!(scorethld >= 0.f && scorethld < 1.f) || opts->depth < 0 || opts->depth > 3 ||

@@ -121,6 +121,13 @@ typedef struct {
     int   seedrule;          /* --seedrule 0..2 (fragments, 64- or 128-residue
                                 local alignment frames; default 1) */
     int   window;            /* --window 256..512 (default 256) */
+    /* clustering runs (--cls): every pair starts filtered and is compared
+     * only when the reference's global index (GTB_FLD_TYPE, pps2DType) is below
+     * the end of the query block's (its largest + 1) and the shorter length
+     * is at least clscoverage x the longer (CheckMaxCoverage,
+     * cufilter/coverage.cu:28-52, CuBatch.cu:452-495) */
+    int   clsfilter;         /* 1 in a clustering run */
+    float clscoverage;       /* --cls-coverage (default 0.7) */
 } gtb_options;
 
 /* Result buffers (host memory), sizes for nq queries x nr references with
@@ -252,7 +259,10 @@ gtb_status gtb_polish(gtb_handle* h, int npairs, const long long* off,
  * the call returns.  Results are those of gtb_process_block (records and
  * transforms only).  Blocks that would pair two nucleic-acid structures are
  * refused with GTB_ERR_UNSUPPORTED, as by gtb_process_block (the molecule
- * types are read back from the device before any search work). */
+ * types are read back from the device before any search work), and so are
+ * options with the detailed search on (nodetailedsearch 0) or a clustering
+ * run's prefilter (clsfilter 1): this path carries no index trees and no
+ * global indices. */
 #define GTB_NOALLOC_SCRATCH_BYTES ((size_t)16 << 20)
 #define GTB_NOALLOC_MAX_PAIRS 4096
 

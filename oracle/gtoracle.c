@@ -5,8 +5,13 @@
  * bench.py's cpu_baseline leg; never by the product.
  *
  * A sequential restatement, one query-reference pair at a time, of the
- * reference's CPU stage sequence with --no-detailed-search semantics:
+ * reference's CPU stage sequence:
  *   MpBatch::ProcessBlock           src/libmymp/mpbatch/MpBatch.cpp:208-470
+ *   MpStageFrg3::Run (the spatial-index detailed search, each pair as if alone
+ *     in its chunk on one thread)   src/libmymp/mpstage1/MpStageFrg3.h:80-115,
+ *                                   MpStageFrg3.cpp:35-469,
+ *     ExecDPSSLocal128xKernel       src/libmymp/mpdp/MpDPHub.cpp:1256-1480,
+ *     ExecDPScore128xKernel         src/libmymp/mpdp/MpDPHub.cpp:389-645
  *   MpStage1::Preinitialize1Kernel  src/libmymp/mpstage1/MpStage1.cpp:28-167
  *   MpSecStr::ssk_kernel_helper     src/libmymp/mpss/MpSecStr.cpp:26-118,
  *                                   AassignSecStr src/libmymp/mpss/MpSecStr.h:218-249
@@ -381,6 +386,7 @@ typedef struct {
     const unsigned char *qa, *ra;
     const char *qs, *rs;
     int qmol, rmol;
+    int ri;              /* the reference's index in its block */
     /* chunk-level values */
     int qmax, rmax, qmin, rmin;
     const gto_opts* o;
@@ -1542,8 +1548,19 @@ static void run_pair(pairctx* P, char* alndst) {
      * molecule-type check, and the ones that pass are released
      * (custage1.cu:74-82, MpStage1.cpp:123-128) */
     int presim = 0.0f < o->presimilarity && PRESIM_EDGE < P->qmax && PRESIM_EDGE < P->rmax;
-    P->flags = (presim || P->qmol != P->rmol) ? CONV_LOWTMSC : 0;
-    if (presim && presim_pass(P, o->presimilarity)) P->flags = 0;
+    if (o->clsfilter) {
+        /* a clustering run: every pair starts filtered (CuBatch.cu:452-467) and
+         * is released when the reference's global index precedes the end of
+         * the query block's and the shorter length reaches the coverage of the
+         * longer (coverage.cu:43-51); the screen below only sees the pairs
+         * left filtered (similarity.cu:56-65) */
+        float lq = (float)P->lq, lr = (float)P->lr;
+        float mx = lq < lr ? lr : lq, mn = lq < lr ? lq : lr;
+        int pass = o->clsrtype[P->ri] < o->clsqend && mx * o->clscoverage <= mn;
+        P->flags = pass ? 0 : CONV_LOWTMSC;
+    } else
+        P->flags = (presim || P->qmol != P->rmol) ? CONV_LOWTMSC : 0;
+    if (presim && P->flags && presim_pass(P, o->presimilarity)) P->flags = 0;
     P->grand = P->best = P->best0 = 0.f;
     P->seedq = P->seedr = 0;
     P->naln = 0;
@@ -1692,6 +1709,7 @@ int gto_process_block_ndx(const gto_opts* o,
         P.qa = qrsd + qoff[qi]; P.ra = rrsd + roff[ri];
         P.qs = qss + qoff[qi]; P.rs = rss + roff[ri];
         P.qmol = qmol ? qmol[qi] : 0; P.rmol = rmol ? rmol[ri] : 0;
+        P.ri = ri;
         P.qmax = qmax; P.qmin = qmin; P.rmax = rmax; P.rmin = rmin;
         if (!o->nodetailedsearch) {
             long long a = qoff[qi], b = roff[ri];

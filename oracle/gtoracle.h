@@ -2,8 +2,8 @@
  * gtoracle.h -- CPU oracle for the GTalign per-pair superposition search.
  *
  * TEST INFRASTRUCTURE ONLY.  This is a sequential plain-C restatement of the
- * reference's CPU path (libmymp: MpStage1, MpStage2, MpStageFin, MpDPHub,
- * MpSecStr) used by tests/, __graft_entry__.smoke() and bench.py's
+ * reference's CPU path (libmymp: MpStage1, MpStageFrg3, MpStage2, MpStageFin,
+ * MpDPHub, MpSecStr) used by tests/, __graft_entry__.smoke() and bench.py's
  * cpu_baseline leg as the checker.  The product (gtalign_alpha_b200 and its
  * CUDA library) never links, loads or calls it.
  *
@@ -53,6 +53,13 @@ typedef struct {
     float gapcost;       /* --gapcost as the cost: -0.8, -1.2 or -3.0 */
     int   seedrule;      /* --seedrule as the frame: 0, 64 or 128 */
     int   window;        /* --window 256..512 */
+    /* a clustering run's prefilter (CheckMaxCoverage, cufilter/coverage.cu:28-52):
+     * the references' global indices (pps2DType), the end of the query
+     * block's (qrysernrbeg + nqystrs), --cls-coverage */
+    int   clsfilter;
+    const int* clsrtype;
+    int   clsqend;
+    float clscoverage;
 } gto_opts;
 
 /* Process a block of nq queries x nr references.

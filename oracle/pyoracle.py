@@ -39,7 +39,9 @@ class _Opts(ctypes.Structure):
                 ("addsearchbyss", ctypes.c_int), ("presimilarity", ctypes.c_float),
                 ("nodetailedsearch", ctypes.c_int), ("trigger", ctypes.c_int),
                 ("nbranches", ctypes.c_int), ("gapcost", ctypes.c_float),
-                ("seedrule", ctypes.c_int), ("window", ctypes.c_int)]
+                ("seedrule", ctypes.c_int), ("window", ctypes.c_int),
+                ("clsfilter", ctypes.c_int), ("clsrtype", ctypes.POINTER(ctypes.c_int)),
+                ("clsqend", ctypes.c_int), ("clscoverage", ctypes.c_float)]
 
 
 _lib = None
@@ -95,18 +97,30 @@ def opts_from(refinement: int = 0, convergence: int = 2, prescore: float = 0.0,
               referenced: int = 0, nodeletions: int = 0, twotmscore: int = 0,
               addsearchbyss: int = 0, presimilarity: float = 0.0,
               nodetailedsearch: int = 1, trigger: int = 50, nbranches: int = 5,
-              gapcost: int = 1, seedrule: int = 1, window: int = 256) -> _Opts:
+              gapcost: int = 1, seedrule: int = 1, window: int = 256,
+              cls=None) -> _Opts:
     """Options in the gtalign command line's encoding: --refinement -1 log
     search, 0 coarse, 1 one search (the default), 2 full, 3 full in both final
     phases (the oracle, like the reference, stores code + 1); --depth 0..3
     (3 = shallow); --2tm-score; --add-search-by-ss; --pre-similarity; the
     detailed search: --no-detailed-search, --trigger, --nbranches, --gapcost
     code (0: -0.8, 1: -1.2, 2: -3.0), --seedrule code (0: fragments, 1: 64-,
-    2: 128-residue local alignment frames), --window."""
-    return _Opts(5 if depth == 3 else 1, refinement + 1, depth, convergence,
-                 prescore, scorethld, symmetric, referenced, nodeletions, twotmscore,
-                 addsearchbyss, presimilarity, nodetailedsearch, trigger, nbranches,
-                 (-0.8, -1.2, -3.0)[gapcost], (0, 64, 128)[seedrule], window)
+    2: 128-residue local alignment frames), --window.  cls: a clustering
+    run's prefilter, (the references' global indices, the end of the query
+    block's global indices, --cls-coverage), or None."""
+    o = _Opts(5 if depth == 3 else 1, refinement + 1, depth, convergence,
+              prescore, scorethld, symmetric, referenced, nodeletions, twotmscore,
+              addsearchbyss, presimilarity, nodetailedsearch, trigger, nbranches,
+              (-0.8, -1.2, -3.0)[gapcost], (0, 64, 128)[seedrule], window)
+    if cls is not None:
+        rtype, qend, coverage = cls
+        arr = np.ascontiguousarray(rtype, dtype=np.int32)
+        o.clsfilter = 1
+        o.clsrtype = arr.ctypes.data_as(ctypes.POINTER(ctypes.c_int))
+        o.clsqend = int(qend)
+        o.clscoverage = float(coverage)
+        o._cls_keep = arr          # the array outlives the options
+    return o
 
 
 def _ndx_ptrs(ndx):

@@ -97,9 +97,10 @@ def cli_options(opts):
     return d
 
 
-def oracle_opts(oracle, d):
-    """oracle options from a cli_options dict"""
-    return oracle.opts_from(
+def oracle_opts(oracle, d, cls=None):
+    """oracle options from a cli_options dict (cls: a clustering run's
+    prefilter, as pyoracle.opts_from takes it)"""
+    return oracle.opts_from(cls=cls,
         refinement=d["refinement"], convergence=d["convergence"], prescore=d["prescore"],
         scorethld=d["scorethld"], symmetric=d["symmetric"], referenced=d["referenced"],
         nodeletions=d["nodeletions"], depth=d["depth"], twotmscore=d["twotmscore"],

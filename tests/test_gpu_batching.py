@@ -50,3 +50,27 @@ def test_sub_batches_and_budget_batches_match_small_blocks():
     hom = np.array([n.startswith("hom") for n in names])
     tm = whole.alndata[0, -40:, 9]
     assert hom.sum() > 0 and (tm[hom] > 0.5).mean() > 0.5
+
+
+def test_sharded_search_with_the_gpu_library():
+    """shard.search_sharded with the CUDA library as the per-rank process
+    (world = 1: the plan, the shard and the result placement; ranks > 1 are
+    the gloo test's): records and transforms equal an unsharded call, and a
+    reusable ShardPlan gives the same."""
+    from gtalign_alpha_b200 import synth
+    from gtalign_alpha_b200.api import GTalignB200, Options
+    from gtalign_alpha_b200.shard import ShardPlan, search_sharded
+    wl = synth.config0(seed=51, n_refs=40, qlen=120)
+    q, r = synth.pack(wl.queries), synth.pack(wl.refs)
+    with GTalignB200(0, 0, Options(prescore=0.3)) as g:
+        ref = g.process_block(q, r, scorethld=0.3, alignments=False)
+
+        def fn(qs, rs):
+            res = g.process_block(qs, rs, scorethld=0.3, alignments=False)
+            return res.alndata, res.tfm
+        aln, tfm = search_sharded(q, r, fn, 0, 1)
+        plan = ShardPlan(r, q.lens, 0, 1)
+        aln2, tfm2 = search_sharded(q, r, fn, 0, 1, plan=plan)
+    for a, t in ((aln, tfm), (aln2, tfm2)):
+        assert np.array_equal(a.view(np.uint32), ref.alndata.view(np.uint32))
+        assert np.array_equal(t.view(np.uint32), ref.tfm.view(np.uint32))

@@ -24,10 +24,10 @@ def _lib_opts(d):
                    seedrule=d.get("seedrule", 1), window=d.get("window", 256))
 
 
-def _ora_opts(oracle, d):
+def _ora_opts(oracle, d, cls=None):
     return gu.oracle_opts(oracle, dict(d, depth=d.get("depth", 2), twotmscore=d.get("twotmscore", 0),
                                        addsearchbyss=d.get("addsearchbyss", 0),
-                                       presimilarity=d.get("presimilarity", 0.0)))
+                                       presimilarity=d.get("presimilarity", 0.0)), cls=cls)
 
 
 def assert_same(res, ora, nq, nr):
@@ -139,6 +139,41 @@ def test_multi_query_ragged_lengths(oracle, opt):
     assert_same(res, ora, q.n, r.n)
 
 
+@pytest.mark.parametrize("opt", ["speed13", "presim", "frg3"])
+def test_clustering_prefilter(oracle, opt):
+    """A clustering run in two query blocks over 12 structures: each block
+    compares a reference only when its global index precedes the end of the
+    block's and the shorter length reaches 0.6 of the longer
+    (CheckMaxCoverage), and the --pre-similarity screen sees only the pairs
+    left filtered (and may release them: similarity.cu:56-65); records,
+    transforms and rows bit for bit."""
+    from gtalign_alpha_b200 import synth
+    from gtalign_alpha_b200.api import GTalignB200, build_index
+    rng = np.random.default_rng(11)
+    base = synth.random_chains(rng, [60, 80, 95, 120, 150, 40])
+    chains = base + [synth.homolog(rng, base[k], 0.9, 0.05, "h%d" % k) for k in range(6)]
+    d = dict(OPTSETS[opt])
+    lo = _lib_opts(d)
+    lo.clsfilter, lo.clscoverage = 1, 0.6
+    r = synth.pack(chains)
+    rx = build_index(r) if not d.get("nodetailedsearch", 1) else None
+    released = 0
+    for b in range(2):
+        q = synth.pack(chains[6 * b:6 * b + 6])
+        qt = np.arange(6 * b, 6 * b + 6, dtype=np.int32)
+        rt = np.where(np.arange(12) < 6 * b + 6, np.arange(12), 2**31 - 1).astype(np.int32)
+        with GTalignB200(0, 0, lo) as g:
+            res = g.process_block(q, r, scorethld=d["scorethld"], qtypes=qt, rtypes=rt)
+        qx = build_index(q) if rx is not None else None
+        ora = oracle.process_block(q, r, _ora_opts(oracle, d, cls=(rt, 6 * b + 6, 0.6)),
+                                   qndx=qx, rndx=rx)
+        assert_same(res, ora, q.n, r.n)
+        released += int((res.alndata[..., 9] > 0).sum())
+        if opt != "presim":      # the screen also releases pairs the prefilter left
+            assert (res.alndata[:, 6 * b + 6:, 9] == 0).all()
+    assert released > 12
+
+
 def test_molecule_type_mismatch_is_skipped(oracle):
     """A protein query and a nucleic-acid reference are not compared
     (MpStage1.cpp:143-152): the record keeps its initial values."""
@@ -202,10 +237,17 @@ def test_status_codes():
     from gtalign_alpha_b200.api import GTalignB200, GTBError, Options
     wl = synth.config0(seed=34, n_refs=2, qlen=50)
     q, r = synth.pack(wl.queries), synth.pack(wl.refs)
-    with GTalignB200(0, 0, Options(nodetailedsearch=0)) as g:
+    # the detailed search at --depth 0 or 1 is refused as not supported
+    with GTalignB200(0, 0, Options(nodetailedsearch=0, depth=1)) as g:
         with pytest.raises(GTBError) as e:
             g.process_block(q, r)
         assert e.value.status == 4
+    for bad in (dict(trigger=101), dict(nbranches=0), dict(window=100), dict(gapcost=3),
+                dict(clsfilter=1, clscoverage=0.0), dict(clsfilter=1, clscoverage=1.5)):
+        with GTalignB200(0, 0, Options(nodetailedsearch=0, **bad)) as g:
+            with pytest.raises(GTBError) as e:
+                g.process_block(q, r)
+            assert e.value.status == 1, bad
     with GTalignB200(0, 0, Options(refinement=4)) as g:
         with pytest.raises(GTBError) as e:
             g.process_block(q, r)

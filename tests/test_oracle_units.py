@@ -114,3 +114,31 @@ def test_gonnet_scores_table():
     for c in "BJOUXZ":
         assert (s[ix(c)] == 0).all()
     assert s[ix("W"), ix("W")] == s.max() and s[ix("W"), ix("D")] < 0
+
+
+def test_clustering_prefilter(oracle):
+    """A clustering run's prefilter (CheckMaxCoverage, coverage.cu:28-52):
+    a pair is compared only when the reference's global index precedes the
+    end of the query block's and the shorter length is at least the coverage
+    times the longer; the pairs it compares keep their records, the rest
+    get the filtered pair's record (TM-scores 0)."""
+    from gtalign_alpha_b200 import synth
+    rng = np.random.default_rng(7)
+    base = synth.random_chains(rng, [60, 70, 90, 120])
+    chains = base + [synth.homolog(rng, base[1], 0.8, 0.05, "h1"), synth.homolog(rng, base[3], 0.8, 0.05, "h3")]
+    q = synth.pack(chains[:3])
+    r = synth.pack(chains)
+    rtype = np.array([0, 1, 2, 2**31 - 1, 2**31 - 1, 2**31 - 1], np.int32)
+    rtype[4] = 1          # read as a query in an earlier block
+    plain = oracle.process_block(q, r, oracle.opts_from(refinement=0, convergence=2))
+    cov = 0.7
+    cls = oracle.process_block(q, r, oracle.opts_from(refinement=0, convergence=2,
+                                                     cls=(rtype, 3, cov)))
+    lq, lr = q.lens[:, None].astype(np.float32), r.lens[None, :].astype(np.float32)
+    passes = (rtype[None, :] < 3) & (np.maximum(lq, lr) * np.float32(cov) <= np.minimum(lq, lr))
+    assert passes.any() and (~passes).any()
+    a, b = plain.out, cls.out
+    np.testing.assert_array_equal(a[passes], b[passes])
+    np.testing.assert_array_equal(plain.tfm[passes], cls.tfm[passes])
+    tm = b[~passes][:, 9:11]                # TM-scores by query and reference length
+    assert (tm == 0).all() and (a[~passes][:, 9:11] > 0).all()
