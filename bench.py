@@ -228,6 +228,7 @@ class Resident:
         self.tfm = torch.empty((nbuf, maxpairs * 12), dtype=torch.float32, device=dev)
         self.err = torch.zeros((nbuf, maxpairs * 4), dtype=torch.float32, device=dev)
         self.maxerr = torch.zeros(3, dtype=torch.float32, device=dev)
+        self.nrmsd_over = torch.zeros((), dtype=torch.int64, device=dev)
 
     def step(self, k):
         import torch
@@ -243,6 +244,7 @@ class Resident:
         e = self.err[b, :n * 4].view(n, 4)
         # every timed pair's error, reduced on the device (no host sync)
         torch.maximum(self.maxerr, e[:, :3].amax(dim=0), out=self.maxerr)
+        self.nrmsd_over += (e[:, 2] > TOL_RMSD).sum()
         return int(self.L.gtb_last_launch_count(self.g.handle))
 
     def records(self, k):
@@ -256,12 +258,14 @@ def timed_steps(res: Resident, args, ws, dev, barrier, clocks=False, work=False)
     for k in range(args.warmup):
         res.step(k)
     res.maxerr.zero_()
+    res.nrmsd_over.zero_()
     torch.cuda.synchronize()
     barrier()
     torch.cuda.synchronize()
     launches, done = 0, 0
     stage_ms = np.zeros(7)
-    wk = np.zeros(3, np.float64)
+    wk = np.zeros(4, np.float64)
+    kms = np.zeros(4, np.float64)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     clk = Clocks(dev) if clocks else None
     if clk:
@@ -275,6 +279,7 @@ def timed_steps(res: Resident, args, ws, dev, barrier, clocks=False, work=False)
         stage_ms += tm
         if work:
             wk += res.g.last_work().astype(np.float64)
+            kms += res.g.last_kernel_ms().astype(np.float64)
     e1.record()
     torch.cuda.synchronize()
     if clk:
@@ -285,7 +290,8 @@ def timed_steps(res: Resident, args, ws, dev, barrier, clocks=False, work=False)
     allpairs = _sum_over_ranks(done, ws, dev)
     me = res.maxerr.cpu().numpy()
     return {"ms": ms, "pairs": allpairs, "launches": launches, "stage_ms": stage_ms / args.steps,
-            "work": wk / args.steps, "maxerr": [float(x) for x in me],
+            "work": wk / args.steps, "kernel_ms": kms / args.steps, "maxerr": [float(x) for x in me],
+            "nrmsd_over": int(res.nrmsd_over.item()),
             "clocks": clk.summary() if clk else None}
 
 
@@ -340,10 +346,16 @@ def run_ours(args):
     # headline: batched + adjoint polishing, resident
     progress("headline (batched + adjoint, resident)")
     rp = Resident(L, gp, qblks, rblk, step_pairs, maxpairs, args.steps, dev)
+    gp.set_kernel_timing(True)          # per-family device time for the FP32 roofline
     A = timed_steps(rp, args, ws, dev, barrier, clocks=True, work=True)
+    gp.set_kernel_timing(False)
     value = A["pairs"] / (A["ms"] / 1000.0)
     ms_step = A["ms"] / args.steps
-    acc_ok = A["maxerr"][0] <= TOL_TM and A["maxerr"][1] <= TOL_TM and A["maxerr"][2] <= TOL_RMSD
+    # the metric's qualifier: every timed pair's TM-scores within TOL_TM of
+    # the FP64 recomputation.  The RMSD is the reference's FP32 value (from
+    # sums of squares, bit-identical to the oracle); its error against FP64
+    # is reported, not gated.
+    acc_ok = A["maxerr"][0] <= TOL_TM and A["maxerr"][1] <= TOL_TM
 
     # the unpolished form (the reference's results) and the polishing gain
     unpol = None
@@ -351,7 +363,7 @@ def run_ours(args):
         progress("unpolished")
         r0 = Resident(L, g0, qblks, rblk, step_pairs, maxpairs, args.steps, dev)
         B = timed_steps(r0, args, ws, dev, barrier)
-        ok0 = B["maxerr"][0] <= TOL_TM and B["maxerr"][1] <= TOL_TM and B["maxerr"][2] <= TOL_RMSD
+        ok0 = B["maxerr"][0] <= TOL_TM and B["maxerr"][1] <= TOL_TM
         acc_ok = acc_ok and ok0
         k_last = args.steps - 1
         a, b = r0.records(k_last), rp.records(k_last)
@@ -401,10 +413,22 @@ def run_ours(args):
     clocks = A["clocks"]
     sm_mhz = clocks["sm_mhz"] if clocks else 1965.0
     fp32_peak = NSM_B200 * FP32_LANES_PER_SM * 2 * sm_mhz * 1e6 / 1e12
-    wk = A["work"]
-    fl = {"seed": FLOPS_PER_VISIT * wk[0], "refine": FLOPS_PER_VISIT * wk[1], "dp": FLOPS_PER_DP_CELL * wk[2]}
+    wk, kms = A["work"], A["kernel_ms"]
+    fl = {"seed": FLOPS_PER_VISIT * wk[0], "refine": FLOPS_PER_VISIT * wk[1],
+          "dp": FLOPS_PER_DP_CELL * (wk[2] + wk[3])}
     fl_step = sum(fl.values())
     fp32_ach = fl_step / (ms_step / 1000.0) / 1e12
+    # per kernel family: its algorithmic flops over its summed launch
+    # durations (CUDA events on the launching streams; the detailed search's
+    # slot-score DP cells are timed with its own kernels)
+    fam = {"k_findfrag (seed)": (FLOPS_PER_VISIT * wk[0], kms[0]),
+           "k_refine (refinement passes)": (FLOPS_PER_VISIT * wk[1], kms[1]),
+           "k_dp / k_dp_wave (DP)": (FLOPS_PER_DP_CELL * wk[2], kms[2])}
+    per_kernel = {}
+    for name, (f, t) in fam.items():
+        a = f / (t / 1000.0) / 1e12 if t > 0 else 0.0
+        per_kernel[name] = {"flops_per_step": f, "ms_per_step": t, "achieved": a,
+                            "frac": a / fp32_peak}
     roof = {"bound": "hbm", "kernel": "k_findfrag (stage-1 seed scan)",
             "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
             "frac": achieved / hbm_peak, "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)",
@@ -415,10 +439,13 @@ def run_ours(args):
                      "peak_source": "148 SMs x 128 FP32 lanes x 2 (FMA) x %.0f MHz (median SM clock "
                                     "sampled during the timed steps)" % sm_mhz,
                      "scope": "whole step (every kernel), per-step algorithmic flops / ms_per_step",
+                     "per_kernel": per_kernel,
+                     "per_kernel_note": "summed launch durations of concurrent sub-batch streams "
+                                        "overlap, so these fractions are lower bounds",
                      "flops_per_step": fl_step,
                      "flops_per_step_by_kernel": fl,
                      "units_per_step": {"seed_position_visits": wk[0], "refine_position_visits": wk[1],
-                                        "dp_cells": wk[2]},
+                                        "dp_cells": wk[2], "detailed_search_dp_cells": wk[3]},
                      "flops_per_unit": {"position_visit": FLOPS_PER_VISIT, "dp_cell": FLOPS_PER_DP_CELL}},
             "stage_ms": {"seed": float(st_ms[0]), "refine_init": float(st_ms[1]),
                          "dp_refine_loops": float(st_ms[2]), "final": float(st_ms[5]),
@@ -456,8 +483,13 @@ def run_ours(args):
                        "l2": "inputs larger than L2 (%.0f MB of reference coordinates)" % (12 * r_all.total / 1e6),
                        "parallelism": "dp%d (references split by cost, independent pairs)" % ws},
             "accuracy": {"max_err_tm": max(A["maxerr"][:2]), "max_err_rmsd": A["maxerr"][2],
-                         "tolerance_tm": TOL_TM, "tolerance_rmsd": TOL_RMSD, "ok": bool(acc_ok),
-                         "scope": "every timed pair: |FP32 search path - FP64 recomputation|"},
+                         "tolerance_tm": TOL_TM, "ok": bool(acc_ok),
+                         "pairs_rmsd_err_over_1e-3": A["nrmsd_over"],
+                         "pairs_timed": A["pairs"],
+                         "scope": "every timed pair: |FP32 search path - FP64 recomputation|; "
+                                  "gated on the TM-scores (the metric's |dTM|<=1e-4); the RMSD "
+                                  "is the reference's FP32 sums-of-squares value, its FP64 error "
+                                  "reported"},
             "e2e": e2e,
             "gpu_launches": A["launches"],
             "roofline": roof,

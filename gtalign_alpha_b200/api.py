@@ -143,6 +143,10 @@ def load_library():
     L.gtb_build_index.restype = ctypes.c_int
     L.gtb_last_work.argtypes = [vp, ctypes.POINTER(ctypes.c_ulonglong)]
     L.gtb_last_work.restype = ctypes.c_int
+    L.gtb_set_kernel_timing.argtypes = [vp, ctypes.c_int]
+    L.gtb_set_kernel_timing.restype = ctypes.c_int
+    L.gtb_last_kernel_ms.argtypes = [vp, ctypes.POINTER(ctypes.c_float)]
+    L.gtb_last_kernel_ms.restype = ctypes.c_int
     L.gtb_set_wait_limit.argtypes = [vp, ctypes.c_longlong]
     L.gtb_set_wait_limit.restype = ctypes.c_int
     L.gtb_destroy.argtypes = [vp]
@@ -299,10 +303,22 @@ class GTalignB200:
             raise GTBError(st, "wait limit must be >= 0")
 
     def last_work(self) -> np.ndarray:
-        """Device-counted work of the last call (seed visits, refinement visits, DP cells)."""
-        w = np.zeros(3, np.uint64)
+        """Device-counted work of the last call (seed visits, refinement
+        visits, DP cells, the detailed search's slot-score DP cells)."""
+        w = np.zeros(4, np.uint64)
         self.lib.gtb_last_work(self._h, w.ctypes.data_as(ctypes.POINTER(ctypes.c_ulonglong)))
         return w
+
+    def set_kernel_timing(self, on: bool) -> None:
+        """Per-family device timing of the following calls (gtb_set_kernel_timing)."""
+        self.lib.gtb_set_kernel_timing(self._h, 1 if on else 0)
+
+    def last_kernel_ms(self) -> np.ndarray:
+        """Summed device time (ms) of the last call's seed, refinement, DP
+        and detailed-search launches."""
+        ms = np.zeros(4, np.float32)
+        self.lib.gtb_last_kernel_ms(self._h, ms.ctypes.data_as(ctypes.POINTER(ctypes.c_float)))
+        return ms
 
     def process_block(self, queries: SoA, refs: SoA, scorethld: float = 0.5,
                       alignments: bool = True, numerr: bool = True,

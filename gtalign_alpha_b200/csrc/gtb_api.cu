@@ -39,7 +39,10 @@ struct gtb_handle {
     int* h_flag = nullptr;           // pinned: wavefront error flag per sub-batch
     long long wait_limit = gtb::DP_WAVE_SPIN_DEFAULT;  // spins of a wavefront wait
     unsigned long long* d_work = nullptr;  // device work counters of the last call
-    unsigned long long work[gtb::WK_NKIND] = {0, 0, 0};
+    unsigned long long work[gtb::WK_NKIND] = {0, 0, 0, 0};
+    bool ktime = false;                    // per-family launch timing on
+    gtb::KTimer kt;
+    float kms[gtb::KF_N] = {0, 0, 0, 0};   // its times of the last call
 };
 
 static const int TBL = 65536;
@@ -126,9 +129,19 @@ extern "C" gtb_status gtb_last_timings(const gtb_handle* h, float* ms7) {
     memcpy(ms7, h->timings, sizeof(h->timings));
     return GTB_OK;
 }
-extern "C" gtb_status gtb_last_work(const gtb_handle* h, unsigned long long* w3) {
-    if (!h || !w3) return GTB_ERR_ARG;
-    memcpy(w3, h->work, sizeof(h->work));
+extern "C" gtb_status gtb_last_work(const gtb_handle* h, unsigned long long* w4) {
+    if (!h || !w4) return GTB_ERR_ARG;
+    memcpy(w4, h->work, sizeof(h->work));
+    return GTB_OK;
+}
+extern "C" gtb_status gtb_set_kernel_timing(gtb_handle* h, int on) {
+    if (!h) return GTB_ERR_ARG;
+    h->ktime = on != 0;
+    return GTB_OK;
+}
+extern "C" gtb_status gtb_last_kernel_ms(const gtb_handle* h, float* ms4) {
+    if (!h || !ms4) return GTB_ERR_ARG;
+    memcpy(ms4, h->kms, sizeof(h->kms));
     return GTB_OK;
 }
 extern "C" gtb_status gtb_set_wait_limit(gtb_handle* h, long long spins) {
@@ -301,6 +314,7 @@ static gtb_status run_block(gtb_handle* h, const DevBlock& D, float scorethld,
 
     float tsum[7] = {0, 0, 0, 0, 0, 0, 0};
     h->launches = 0;
+    h->kt.used = 0;                     // pairs of an unfinished earlier call
     cudaError_t lerr = cudaSuccess;     // a launch that failed (cooperative DP)
     // work counters: cleared on the handle's stream, which the sub-batch
     // streams wait for below
@@ -464,6 +478,7 @@ static gtb_status run_block(gtb_handle* h, const DevBlock& D, float scorethld,
             T.vskip_mask = (unsigned*)(base + o_f3v);
         }
         T.work = h->d_work;
+        T.kt = h->ktime ? &h->kt : nullptr;
         T.dw_spin = h->wait_limit;
         T.nff = np; T.ff_pair = nullptr; T.ff_chunk = nullptr; T.ff_nch = nullptr; T.ff_key = nullptr;
         T.rl_nlmax = nlmax; T.rl_long = T.rl_count = T.rl_next = nullptr; T.rl_cand = nullptr;
@@ -603,6 +618,8 @@ static gtb_status run_block(gtb_handle* h, const DevBlock& D, float scorethld,
         p0 = p1;
     }
     memcpy(h->timings, tsum, sizeof(tsum));
+    for (int k = 0; k < gtb::KF_N; k++) h->kms[k] = 0.f;
+    if (h->ktime) CK(h->kt.collect(h->kms));
     {
         unsigned long long wk[gtb::WK_NKIND * gtb::WORK_SLOTS];
         CK(cudaMemcpy(wk, h->d_work, sizeof(wk), cudaMemcpyDeviceToHost));

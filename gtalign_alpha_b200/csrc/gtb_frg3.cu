@@ -534,17 +534,20 @@ __global__ void k_f3_second(Blk B, Bat T, int rci) {
 void launch_frg3(const Blk& B, const Bat& T, cudaStream_t st) {
     const int nb = (T.np + 3) / 4;
     auto plist = [&]() { launch_pair_list(B, T, CONV_LOWTMSC, st); };
-    if (0 < B.f3trigger || B.f3seedrule) {
-        plist();
-        k_f3_localdp<<<nb, 128, 0, st>>>(B, T);
-        if (T.launches) (*T.launches)++;
-    } else plist();
-    k_f3_search<<<(T.np + F3_WARPS - 1) / F3_WARPS, F3_WARPS * 32, 0, st>>>(B, T, B.depth);
-    if (T.launches) (*T.launches)++;
-    launch_f3_dpscore(B, T, st);
+    plist();
     const int nbr = B.f3nbranches < F3_NBMAX ? B.f3nbranches : F3_NBMAX;
-    k_f3_select<<<(T.np + 255) / 256, 256, 0, st>>>(B, T, nbr);
-    if (T.launches) (*T.launches)++;
+    {
+        KtScope kts(T, KF_FRG3, st);
+        if (0 < B.f3trigger || B.f3seedrule) {
+            k_f3_localdp<<<nb, 128, 0, st>>>(B, T);
+            if (T.launches) (*T.launches)++;
+        }
+        k_f3_search<<<(T.np + F3_WARPS - 1) / F3_WARPS, F3_WARPS * 32, 0, st>>>(B, T, B.depth);
+        if (T.launches) (*T.launches)++;
+        launch_f3_dpscore(B, T, st);
+        k_f3_select<<<(T.np + 255) / 256, 256, 0, st>>>(B, T, nbr);
+        if (T.launches) (*T.launches)++;
+    }
     // the branches (Refine_tfmaltconfig, MpStageFrg3.cpp:425-467)
     for (int rci = 0; rci < nbr; rci++) {
         Bat TA = T;

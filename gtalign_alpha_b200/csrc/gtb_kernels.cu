@@ -48,6 +48,41 @@ __device__ __forceinline__ float gonnet(unsigned char a, unsigned char b) {
 
 #define GTB_LAUNCHED(T) do { if ((T).launches) (*(T).launches)++; } while (0)
 
+void KTimer::begin(int f, cudaStream_t st) {
+    if (used + 2 > ev.size()) {
+        for (int k = 0; k < 64; k++) {
+            cudaEvent_t e;
+            if (cudaEventCreate(&e) != cudaSuccess) return;
+            ev.push_back(e);
+        }
+    }
+    if (fam.size() < ev.size() / 2) fam.resize(ev.size() / 2);
+    fam[used / 2] = f;
+    cudaEventRecord(ev[used], st);
+}
+
+void KTimer::end(cudaStream_t st) {
+    if (used + 2 > ev.size()) return;       // begin could not create events
+    cudaEventRecord(ev[used + 1], st);
+    used += 2;
+}
+
+cudaError_t KTimer::collect(float* ms) {
+    cudaError_t e = cudaSuccess;
+    for (size_t k = 0; k + 1 < used; k += 2) {
+        float t = 0.f;
+        cudaError_t r = cudaEventElapsedTime(&t, ev[k], ev[k + 1]);
+        if (r == cudaSuccess) ms[fam[k / 2]] += t;
+        else if (e == cudaSuccess) e = r;
+    }
+    used = 0;
+    return e;
+}
+
+KTimer::~KTimer() {
+    for (cudaEvent_t e : ev) cudaEventDestroy(e);
+}
+
 // algorithmic work counters (Bat::work): one atomic per caller, spread over
 // WORK_SLOTS addresses by CTA
 __device__ __forceinline__ void work_add(const Bat& T, int kind, unsigned long long v) {
@@ -636,6 +671,7 @@ __global__ void k_findfrag_fin(Blk B, Bat T) {
 }
 
 void launch_findfrag(const Blk& B, const Bat& T, cudaStream_t st) {
+    KtScope kts(T, KF_SEED, st);
     if (T.ff_pair) {
         cudaMemsetAsync(T.ff_key, 0, (size_t)T.np * sizeof(unsigned long long), st);
         k_findfrag<<<T.nff, 128, 0, st>>>(B, T);
@@ -1348,6 +1384,7 @@ void launch_refine(int mode, const Blk& B, const Bat& T, cudaStream_t st, bool f
     k_rlist_count<<<nb, 256, 0, st>>>(B, T, mode);
     k_rlist_scan<<<1, 1024, 0, st>>>(T);
     k_rlist_fill<<<nb, 256, 0, st>>>(B, T, mode);
+    KtScope kts(T, KF_REFINE, st);
     if (few) launch_refine_k<32, false>(mode, B, T, st);
     else launch_refine_k<16, false>(mode, B, T, st);
     if (T.launches) (*T.launches) += 4;
@@ -1625,6 +1662,7 @@ void launch_dp(const Blk& B, const Bat& T, int tfmsrc, int gap0, float gcost, in
         k_dlist_fill<<<nb, 256, 0, st>>>(B, T, skipmode);
         if (T.launches) (*T.launches) += 3;
     }
+    KtScope kts(T, KF_DP, st);
     if (T.ndw > 0) {
         cudaMemsetAsync(T.dw_prog, 0, (size_t)T.dw_nprog * sizeof(int), st);
         if (usess == DP_SC_SSRR) launch_dp_wave<0, DP_SC_SSRR>(B, T, tfmsrc, gcost, dpscan, skipmode, st);
@@ -1682,7 +1720,7 @@ __global__ void __launch_bounds__(128) k_f3_dpscore(Blk B, Bat T) {
         float t[12];
 #pragma unroll
         for (int f = 0; f < 12; f++) t[f] = sl[1 + f];
-        if (lane == 0) work_add(T, WK_DPCELL, (unsigned long long)lq * (unsigned long long)lr);
+        if (lane == 0) work_add(T, WK_F3CELL, (unsigned long long)lq * (unsigned long long)lr);
         if (dp_r(lq) == 4)
             dp_pair<4, true, DP_SC_TFM, false, true>(t, d02, 0.f, lq, lr, qx, qy, qz, r4, nullptr,
                                                      nullptr, nullptr, nullptr, row, nullptr, lane,

@@ -1,6 +1,7 @@
 // gtb_kernels.cuh -- kernel-side data layout and launchers of the search.
 #pragma once
 #include <cstdint>
+#include <vector>
 #include <cuda_runtime.h>
 
 namespace gtb {
@@ -112,9 +113,9 @@ struct Bat {
     long long dw_spin;               // spins a wavefront wait makes before it gives up
     long long* launches;             // host counter of kernel launches
     cudaError_t* lerr;               // host: first failed launch (null: not recorded)
-    // device work counters (null: not counted), WORK_SLOTS slots per kind,
-    // summed on the host: position visits of the seed passes, position
-    // visits of the refinement passes, DP cells
+    struct KTimer* kt;               // host: per-family launch timer (null: off)
+    // device work counters (null: not counted), WORK_SLOTS slots per kind
+    // (WorkKind), summed on the host
     unsigned long long* work;
     // detailed search (null when off): per pair the local score matrix
     // (lq x lr bytes, row major, at off_lsm[i]); the 32 fragment slots'
@@ -131,7 +132,31 @@ struct Bat {
     const unsigned* vskip;           // refinement variant skips in force (null: none)
 };
 
-enum WorkKind { WK_SEED = 0, WK_REFINE = 1, WK_DPCELL = 2, WK_NKIND = 3 };
+// position visits of the seed and refinement passes, DP cells, and the DP
+// cells of the detailed search's slot scores
+enum WorkKind { WK_SEED = 0, WK_REFINE = 1, WK_DPCELL = 2, WK_F3CELL = 3, WK_NKIND = 4 };
+
+// Device time of the launches of each kernel family, from an event pair
+// recorded on the launching stream around each launch (host side).  Where
+// sub-batches run concurrently on several streams, a launch's interval also
+// covers the other streams' work that overlapped it.
+enum KernelFamily { KF_SEED = 0, KF_REFINE = 1, KF_DP = 2, KF_FRG3 = 3, KF_N = 4 };
+struct KTimer {
+    std::vector<cudaEvent_t> ev;     // begin/end pairs, created on first use
+    std::vector<int> fam;
+    size_t used = 0;
+    void begin(int f, cudaStream_t st);
+    void end(cudaStream_t st);
+    // adds the elapsed times of the recorded pairs to ms[KF_N] (after they
+    // completed) and starts over
+    cudaError_t collect(float* ms);
+    ~KTimer();
+};
+struct KtScope {                      // begin/end around one launch helper
+    KTimer* k; cudaStream_t st;
+    KtScope(const Bat& T, int f, cudaStream_t s) : k(T.kt), st(s) { if (k) k->begin(f, st); }
+    ~KtScope() { if (k) k->end(st); }
+};
 constexpr int WORK_SLOTS = 64;       // spread over addresses: fewer atomic collisions
 constexpr long long DP_WAVE_SPIN_DEFAULT = 1LL << 24;
 

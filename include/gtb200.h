@@ -45,7 +45,8 @@ enum {
 enum {
     GTB_FLD_LEN = 0,      /* int32 structure length (pps2DLen) */
     GTB_FLD_DIST = 1,     /* uint32 offset of the structure's first residue (pps2DDist) */
-    GTB_FLD_TYPE = 2,     /* int32 (pps2DType, unused here) */
+    GTB_FLD_TYPE = 2,     /* int32 (pps2DType): a clustering run's global
+                             structure index, read only when clsfilter is 1 */
     GTB_FLD_X = 3,        /* float x (pmv2DCoords+0) */
     GTB_FLD_Y = 4,        /* float y */
     GTB_FLD_Z = 5,        /* float z */
@@ -123,7 +124,8 @@ typedef struct {
     int   window;            /* --window 256..512 (default 256) */
     /* clustering runs (--cls): every pair starts filtered and is compared
      * only when the reference's global index (GTB_FLD_TYPE, pps2DType) is below
-     * the end of the query block's (its largest + 1) and the shorter length
+     * the end of the query block's (its smallest + its count: the block's
+     * indices are consecutive, TdClustWriter.h:213-219) and the shorter length
      * is at least clscoverage x the longer (CheckMaxCoverage,
      * cufilter/coverage.cu:28-52, CuBatch.cu:452-495) */
     int   clsfilter;         /* 1 in a clustering run */
@@ -297,11 +299,22 @@ gtb_status gtb_last_timings(const gtb_handle* h, float* ms7);
 
 /* Algorithmic work of the last gtb_process_block / gtb_process_resident
  * call, counted on the device (no reference counterpart; the measurement
- * behind a FP32 roofline): w3[0] position visits of the seed passes (one
+ * behind a FP32 roofline): w4[0] position visits of the seed passes (one
  * visit = one aligned residue pair transformed, scored or added to a
- * covariance in one pass), w3[1] position visits of the refinement passes,
- * w3[2] DP matrix cells. */
-gtb_status gtb_last_work(const gtb_handle* h, unsigned long long* w3);
+ * covariance in one pass), w4[1] position visits of the refinement passes,
+ * w4[2] DP matrix cells, w4[3] DP matrix cells of the detailed search's
+ * fragment-slot scores. */
+gtb_status gtb_last_work(const gtb_handle* h, unsigned long long* w4);
+
+/* Per-family device time (no reference counterpart): with timing on, every
+ * launch of the seed scan, the refinement passes, the DP and the detailed
+ * search's own kernels is bracketed by CUDA events on its stream, and
+ * gtb_last_kernel_ms gives the summed times (ms) of the last call:
+ * ms4[0] seed, [1] refinement, [2] DP, [3] detailed search.  Launches of
+ * concurrent sub-batches overlap, so a sum can exceed the call's span.
+ * Off by default. */
+gtb_status gtb_set_kernel_timing(gtb_handle* h, int on);
+gtb_status gtb_last_kernel_ms(const gtb_handle* h, float* ms4);
 
 /* Spins a bounded wait of the multi-CTA DP makes before it gives up (no
  * reference counterpart; default 2^24).  A wait that gives up ends the call

@@ -74,3 +74,31 @@ def test_sharded_search_with_the_gpu_library():
     for a, t in ((aln, tfm), (aln2, tfm2)):
         assert np.array_equal(a.view(np.uint32), ref.alndata.view(np.uint32))
         assert np.array_equal(t.view(np.uint32), ref.tfm.view(np.uint32))
+
+
+def test_kernel_timing_and_work_counters():
+    """Per-family device times (gtb_set_kernel_timing / gtb_last_kernel_ms)
+    and the device-counted work of a call: every family that ran has time
+    and work, timing off leaves the times at 0, and the results do not
+    depend on the timing."""
+    from gtalign_alpha_b200 import synth
+    from gtalign_alpha_b200.api import GTalignB200, Options
+    wl = synth.config0(seed=41, n_refs=60, qlen=120)
+    q, r = synth.pack(wl.queries), synth.pack(wl.refs)
+    with GTalignB200(0, 0, Options.speed(9)) as g:
+        a = g.process_block(q, r, scorethld=0.0)
+        assert (g.last_kernel_ms() == 0).all()
+        w = g.last_work()
+        assert (w > 0).all(), w
+        g.set_kernel_timing(True)
+        b = g.process_block(q, r, scorethld=0.0)
+        ms = g.last_kernel_ms()
+        assert (ms > 0).all(), ms
+        assert np.array_equal(g.last_work(), w)
+        g.set_kernel_timing(False)
+    assert np.array_equal(a.alndata.view(np.uint32), b.alndata.view(np.uint32))
+    with GTalignB200(0, 0, Options.speed(13)) as g:
+        g.set_kernel_timing(True)
+        g.process_block(q, r, scorethld=0.0)
+        ms, w = g.last_kernel_ms(), g.last_work()
+        assert (ms[:3] > 0).all() and ms[3] == 0 and w[3] == 0
