@@ -429,6 +429,11 @@ def run_ours(args):
         a = f / (t / 1000.0) / 1e12 if t > 0 else 0.0
         per_kernel[name] = {"flops_per_step": f, "ms_per_step": t, "achieved": a,
                             "frac": a / fp32_peak}
+    if kms[3] > 0:
+        # the detailed search's own kernels (local SS alignment, configuration
+        # search, slot scores): time only, their work is not a FP32 count
+        per_kernel["k_f3_* (detailed search)"] = {"ms_per_step": kms[3],
+                                                  "slot_score_dp_cells": wk[3]}
     roof = {"bound": "hbm", "kernel": "k_findfrag (stage-1 seed scan)",
             "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
             "frac": achieved / hbm_peak, "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)",

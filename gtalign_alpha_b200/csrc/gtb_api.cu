@@ -228,6 +228,8 @@ static size_t pair_bytes(int lq, int lr, bool strings, bool f3 = false) {
     b += (size_t)std::min(lq, lr) * 28;                // aligned pairs + coordinates
     if (strings) b += (size_t)5 * (lq + lr + 1);       // alignment rows
     b += 4 * 8 + 12 * 4 * 2 + 16 * 4 + 4 * 4 + 12 * 4 + 64 + 4 + 24;  // state, offsets, work lists
+    if (std::min(lq, lr) >= gtb::RL_LONG_FEW)          // long-pair candidates
+        b += (size_t)gtb::RLW_WARPS * gtb::RLW_CAND * 4 + 12;
     return b;
 }
 
@@ -395,11 +397,12 @@ static gtb_status run_block(gtb_handle* h, const DevBlock& D, float scorethld,
                 for (int k = 0; k < nl; k++) mk[lp[k]] = 1;
             }
         }
-        // pairs that may reach RL_LONG refinement positions (n <= min(lq, lr))
+        // pairs that may reach the long-pair threshold of some refinement
+        // launch (n <= min(lq, lr))
         int nlmax = 0;
         for (int i = 0; i < np; i++) {
             long long p = q0 + i;
-            if (std::min(D.hqlen[p / D.nr], D.hrlen[p % D.nr]) >= gtb::RL_LONG) nlmax++;
+            if (std::min(D.hqlen[p / D.nr], D.hrlen[p % D.nr]) >= gtb::RL_LONG_FEW) nlmax++;
         }
         std::vector<int>& ffi = ffiv[j];
         if (split) {

@@ -25,6 +25,7 @@
 // All floating-point reductions are sequential per thread in forward position
 // order (blocks of BLK positions, Neumaier-compensated), so results do not
 // depend on the launch geometry.
+#include <algorithm>
 #include <type_traits>
 #include "gtb200.h"
 #include "gtb_device.cuh"
@@ -709,7 +710,7 @@ __global__ void k_rlist_count(Blk B, Bat T, int mode) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= T.np) return;
     int n = refine_span(B, T, mode, i);
-    if (n >= RL_LONG && T.rl_long) {           // many warps for this pair
+    if (n >= T.rl_min && T.rl_long) {          // many warps for this pair
         int slot = atomicAdd(T.rl_count, 1);
         if (slot < T.rl_nlmax) { T.rl_long[slot] = i; return; }
     }
@@ -797,7 +798,7 @@ __global__ void k_rlist_fill(Blk B, Bat T, int mode) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= T.np) return;
     int n = refine_span(B, T, mode, i);
-    if (n >= RL_LONG && T.rl_long) return;      // listed by k_rlist_count
+    if (n >= T.rl_min && T.rl_long) return;     // listed by k_rlist_count
     if (n > 0) T.rlist[atomicAdd(&T.rhist[RL_NB - 1 - (n >> RL_SHIFT)], 1)] = i;
 }
 
@@ -1048,16 +1049,21 @@ __device__ __forceinline__ void refine_commit(const Blk& B, const Bat& T, int i,
 // RF_LPP lanes per pair: 16 (two pairs per warp) where most pairs of a
 // batch take part; 32 where few do (after the --pre-score filter), which
 // shortens the launches whose time is that of their slowest pair.
-constexpr int RF_WARPS = 4;
+// Warps per CTA: 4 (1 and 2, with an SM refilling a finished warp's slot at
+// once, measured the same on the benchmark step: the concurrent sub-batch
+// streams fill those slots already).
+constexpr int RF_WARPS_SHORT = 4;
+constexpr int RF_WARPS_LONG = 4;
 
 // LONG: the pairs with at least RL_LONG positions, RLW_CTAS CTAs each; every
 // warp of them takes the pair's variants from one counter in global memory
 // and leaves its best variant as a candidate; k_refine_long_fin picks the
 // pair's winner among them.
+// One slot of a refinement launch: a short pair (slot of the length-sorted
+// list) or, LONG, warp `wlong` of the warps working on long pair `slot`.
 template <int MODE, int RF_LPP, bool LONG>
-__global__ void __launch_bounds__(RF_WARPS * 32) k_refine(Blk B, Bat T) {
-    constexpr int RF_PPW = 32 / RF_LPP;        // pairs per warp
-    constexpr int RF_PAIRS = RF_PPW * RF_WARPS;  // pairs per CTA
+__device__ __forceinline__ void refine_slot(const Blk& B, const Bat& T, int slot, int wlong) {
+    constexpr int RF_WARPS = LONG ? RF_WARPS_LONG : RF_WARPS_SHORT;
     __shared__ float s_last[16 * RF_WARPS * 32];   // previous iteration's sums
     __shared__ float s_tb[12 * RF_WARPS * 32];     // best transform of the current variant
     __shared__ float s_tbest[12 * RF_WARPS * 32];  // best transform over the lane's variants
@@ -1065,9 +1071,6 @@ __global__ void __launch_bounds__(RF_WARPS * 32) k_refine(Blk B, Bat T) {
     const int lane = threadIdx.x & 31;
     const int sub = lane / RF_LPP;
     const unsigned smask = RF_LPP == 32 ? 0xffffffffu : ((1u << (RF_LPP & 31)) - 1u) << (sub * RF_LPP);
-    const int slot = LONG ? (int)(blockIdx.x / RLW_CTAS)
-                          : blockIdx.x * RF_PAIRS + (threadIdx.x >> 5) * RF_PPW + sub;
-    const int wlong = LONG ? (int)(blockIdx.x % RLW_CTAS) * RF_WARPS + (threadIdx.x >> 5) : 0;
     const bool valid = LONG ? slot < *T.rl_count : slot < T.rhist[RL_NB];
     if (__ballot_sync(FULL, valid) == 0) return;
     const int i = valid ? (LONG ? T.rl_long[slot] : T.rlist[slot]) : 0;
@@ -1293,6 +1296,24 @@ __global__ void __launch_bounds__(RF_WARPS * 32) k_refine(Blk B, Bat T) {
         refine_commit<MODE>(B, T, i, lq, lr, havewin, wb, lgbest, wndx, wpos, tbest, str);
 }
 
+// LONG: T.rlw_ctas CTAs per long pair; the grid (a multiple of that) walks
+// the long pairs listed for this launch.
+template <int MODE, int RF_LPP, bool LONG>
+__global__ void __launch_bounds__((LONG ? RF_WARPS_LONG : RF_WARPS_SHORT) * 32) k_refine(Blk B, Bat T) {
+    if (LONG) {
+        const int c = T.rlw_ctas;
+        const int wl = (int)(blockIdx.x % c) * RF_WARPS_LONG + (threadIdx.x >> 5);
+        const int nlong = *T.rl_count;
+        for (int slot = (int)(blockIdx.x / c); slot < nlong; slot += (int)(gridDim.x / c))
+            refine_slot<MODE, RF_LPP, LONG>(B, T, slot, wl);
+    } else {
+        constexpr int RF_PPW = 32 / RF_LPP;        // pairs per warp
+        const int slot = blockIdx.x * (RF_PPW * RF_WARPS_SHORT) + (threadIdx.x >> 5) * RF_PPW +
+                         (int)(threadIdx.x & 31) / RF_LPP;
+        refine_slot<MODE, RF_LPP, LONG>(B, T, slot, 0);
+    }
+}
+
 // the winner of each long pair among its warps' candidates
 template <int MODE>
 __global__ void k_refine_long_fin(Blk B, Bat T) {
@@ -1304,7 +1325,8 @@ __global__ void k_refine_long_fin(Blk B, Bat T) {
     const float* c0 = T.rl_cand + (long long)slot * RLW_WARPS * RLW_CAND;
     float wb = 0.f;
     int wsi = 0x7fffffff, wk = -1;
-    for (int k = lane; k < RLW_WARPS; k += 32) {
+    const int nw = T.rlw_ctas * RF_WARPS_LONG;      // the warps that left candidates
+    for (int k = lane; k < nw; k += 32) {
         float b = c0[k * RLW_CAND];
         int si = __float_as_int(c0[k * RLW_CAND + 1]);
         if (b > 0.f && (wb < b || (wb == b && si < wsi))) { wb = b; wsi = si; wk = k; }
@@ -1326,9 +1348,12 @@ __global__ void k_refine_long_fin(Blk B, Bat T) {
 
 template <int LPP, bool LONG>
 static void launch_refine_k(int mode, const Blk& B, const Bat& T, cudaStream_t st) {
-    const int ng = LONG ? T.rl_nlmax * RLW_CTAS
-                        : (T.np + (32 / LPP) * RF_WARPS - 1) / ((32 / LPP) * RF_WARPS);
-    const int nt = RF_WARPS * 32;
+    constexpr int W = LONG ? RF_WARPS_LONG : RF_WARPS_SHORT;
+    // long pairs: at most RLW_GRID CTAs, T.rlw_ctas per pair at a time
+    const int nslot = LONG ? std::max(1, std::min(T.rl_nlmax, RLW_GRID / T.rlw_ctas)) : 0;
+    const int ng = LONG ? nslot * T.rlw_ctas
+                        : (T.np + (32 / LPP) * W - 1) / ((32 / LPP) * W);
+    const int nt = W * 32;
     switch (mode) {
         case RM_INIT:  k_refine<RM_INIT, LPP, LONG><<<ng, nt, 0, st>>>(B, T); break;
         case RM_DP:    k_refine<RM_DP, LPP, LONG><<<ng, nt, 0, st>>>(B, T); break;
@@ -1341,15 +1366,34 @@ static void launch_refine_k(int mode, const Blk& B, const Bat& T, cudaStream_t s
 }
 
 // The refinement kernels re-read each pair's positions on every pass: ask
-// for the smallest shared-memory carve-out that holds three CTAs (3 x 20 kB
-// of their static arrays), leaving the rest of the SM's 256 kB to L1.
+// for the smallest shared-memory carve-out that holds as many CTAs as their
+// registers allow (static arrays + the 1 kB each CTA reserves), leaving the
+// rest of the SM's 256 kB to L1.
 template <int LPP, bool LONG>
 static void carve_refine() {
+    constexpr int W = LONG ? RF_WARPS_LONG : RF_WARPS_SHORT;
     const void* ks[7] = {(const void*)k_refine<RM_INIT, LPP, LONG>, (const void*)k_refine<RM_DP, LPP, LONG>,
                          (const void*)k_refine<RM_FIN1, LPP, LONG>, (const void*)k_refine<RM_FIN2, LPP, LONG>,
                          (const void*)k_refine<RM_PROD1, LPP, LONG>, (const void*)k_refine<RM_PROD2, LPP, LONG>,
                          (const void*)k_refine<RM_PLOG, LPP, LONG>};
-    for (const void* k : ks) cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, 27);
+    int dev = 0, smem_sm = 0, regs_sm = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
+    cudaDeviceGetAttribute(&regs_sm, cudaDevAttrMaxRegistersPerMultiprocessor, dev);
+    for (const void* k : ks) {
+        cudaFuncAttributes fa{};
+        int carve = 27;
+        if (cudaFuncGetAttributes(&fa, k) == cudaSuccess && smem_sm > 0 && fa.numRegs > 0) {
+            const int warp_regs = (fa.numRegs * 32 + 255) / 256 * 256;   // per-warp allocation unit
+            int ctas = regs_sm / (warp_regs * W);
+            if (ctas > 32) ctas = 32;
+            const long long need = (long long)ctas * ((long long)fa.sharedSizeBytes + 1024);
+            carve = (int)((need * 100 + smem_sm - 1) / smem_sm);
+            if (carve < 1) carve = 1;
+            if (carve > 100) carve = 100;
+        }
+        cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, carve);
+    }
 }
 
 void configure_kernels() {
@@ -1374,7 +1418,14 @@ static void launch_refine_long_fin(int mode, const Blk& B, const Bat& T, cudaStr
     }
 }
 
-void launch_refine(int mode, const Blk& B, const Bat& T, cudaStream_t st, bool few) {
+void launch_refine(int mode, const Blk& B, const Bat& T0, cudaStream_t st, bool few) {
+    // the long-pair path: from RL_LONG positions with RLW_CTAS CTAs where
+    // most pairs take part; where few do (the launches after the --pre-score
+    // filter) a launch lasts as long as its slowest pair, so pairs from
+    // RL_LONG_FEW positions get RLW_CTAS_FEW CTAs
+    Bat T = T0;
+    T.rl_min = few ? RL_LONG_FEW : RL_LONG;
+    T.rlw_ctas = few ? RLW_CTAS_FEW : RLW_CTAS;
     cudaMemsetAsync(T.rhist, 0, (RL_NB + 1) * sizeof(int), st);
     if (T.rl_long) {
         cudaMemsetAsync(T.rl_count, 0, sizeof(int), st);

@@ -12,11 +12,17 @@ namespace gtb {
 // multiple of 16/R; every lane packs the 2-bit directions of its R rows for
 // 16/R consecutive steps into one 32-bit word, words of a strip stored
 // [step / (16/R)][lane].
-// refinement: pairs with at least RL_LONG positions get RLW_CTAS CTAs
+// refinement: pairs with at least RL_LONG positions get RLW_CTAS CTAs of 4
+// warps; in the launches where few pairs take part, pairs with at least
+// RL_LONG_FEW positions get RLW_CTAS_FEW; a long-pair launch has at most
+// RLW_GRID CTAs (they walk the long pairs)
 constexpr int RL_LONG = 1536;
+constexpr int RL_LONG_FEW = 384;
 constexpr int RL_NBUCKET = 65536 >> 4;   // work-list buckets; rhist[RL_NBUCKET] = list length
 constexpr int RLW_CTAS = 16;
-constexpr int RLW_WARPS = RLW_CTAS * 4;
+constexpr int RLW_CTAS_FEW = 4;
+constexpr int RLW_GRID = 1024;
+constexpr int RLW_WARPS = RLW_CTAS * 4;  // candidates per long pair (the most warps)
 constexpr int RLW_CAND = 17;         // floats per warp candidate
 
 constexpr int DP_R4_MIN = 384;
@@ -92,6 +98,7 @@ struct Bat {
     // long pairs of a refinement launch (null: none possible): list, count,
     // per-pair variant counter, per-warp candidates; rl_nlmax = capacity
     int rl_nlmax;
+    int rl_min, rlw_ctas;            // this launch's long-pair threshold and CTAs per long pair
     int *rl_long, *rl_count, *rl_next;
     int plog_round;                  // round of an RM_PLOG launch (0 .. PLOG_ROUNDS-1)
     float* rl_cand;
