@@ -223,7 +223,7 @@ static size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 // score matrix, slots and branches).
 static size_t pair_bytes(int lq, int lr, bool strings, bool f3 = false) {
     size_t b = (size_t)gtb::bt_words(lq, lr) * 4;     // traceback words
-    if (f3) b += (size_t)lq * lr + (size_t)F3_NTOP * 14 * 4 + (size_t)F3_NBMAX * 13 * 4 + 13 * 4 + 8;
+    if (f3) b += (size_t)gtb::f3_region_bytes(lq, lr) + (size_t)F3_NTOP * 14 * 4 + (size_t)F3_NBMAX * 13 * 4 + 13 * 4 + 8;
     b += (size_t)lr * 4;                               // DP row buffer
     b += (size_t)std::min(lq, lr) * 28;                // aligned pairs + coordinates
     if (strings) b += (size_t)5 * (lq + lr + 1);       // alignment rows
@@ -352,7 +352,7 @@ static gtb_status run_block(gtb_handle* h, const DevBlock& D, float scorethld,
             off_row[i + 1] = off_row[i] + lr;
             off_aln[i + 1] = off_aln[i] + std::min(lq, lr);
             off_str[i + 1] = off_str[i] + (strings ? 5LL * (lq + lr + 1) : 0);
-            if (off_lsm) off_lsm[i + 1] = off_lsm[i] + (long long)lq * lr;
+            if (off_lsm) off_lsm[i + 1] = off_lsm[i] + gtb::f3_region_bytes(lq, lr);
             int n1, silo, sihi, prv;
             gtb::seed_range(lq, lr, B.qmax, B.qmin, B.rmax, B.rmin, B.stepinit, n1, silo, sihi, prv);
             int cnt = sihi - silo + 1;

@@ -241,11 +241,12 @@ __device__ void f3_cov(const float* qx, const float* qy, const float* qz, const 
 // MpStageFrg3.h:1270-1440): depth first with a bounded stack, at most 64
 // nodes visited; with ssfilt only residues of secondary structure ss count
 // and one farther than 8 A is none.  Returns the residue or -1.
+// The stack is the lane's column of a shared-memory array (entry q at
+// [q * 32]).
 __device__ int f3_nn(const float* nx, const float* ny, const float* nz, const int* nl,
                      const int* nr, const int* no, const char* sss, int len, bool ssfilt, char ss,
-                     float px, float py, float pz, int stacksize) {
-    int stk_node[F3_MAXSTACK], stk_dim[F3_MAXSTACK];
-    float stk_diff[F3_MAXSTACK];
+                     float px, float py, float pz, int stacksize, unsigned short* stk_node,
+                     float* stk_diff, unsigned char* stk_dim) {
     int sp = 0, nvisited = 0, best = -1, root = len >> 1, dim = 0;
     float bestd = 9.9e6f;
     while (0 < sp || 0 <= root) {
@@ -264,10 +265,9 @@ __device__ int f3_nn(const float* nx, const float* ny, const float* nz, const in
             const float diffc = dim == 0 ? dx : (dim == 1 ? dy : dz);
             if (2 < ++dim) dim = 0;
             if (sp < stacksize) {
-                // (a register array indexed through an unrolled select)
-#pragma unroll
-                for (int q = 0; q < F3_MAXSTACK; q++)
-                    if (q == sp) { stk_node[q] = root; stk_dim[q] = dim; stk_diff[q] = diffc; }
+                stk_node[sp * 32] = (unsigned short)root;    // a node index is below 65536
+                stk_dim[sp * 32] = (unsigned char)dim;
+                stk_diff[sp * 32] = diffc;
                 sp++;
             }
             root = (0.0f < diffc) ? __ldg(nl + root) : __ldg(nr + root);
@@ -276,9 +276,7 @@ __device__ int f3_nn(const float* nx, const float* ny, const float* nz, const in
             float diffc = 0.f;
             while (0 < sp && !cond) {
                 sp--;
-#pragma unroll
-                for (int q = 0; q < F3_MAXSTACK; q++)
-                    if (q == sp) { root = stk_node[q]; dim = stk_dim[q]; diffc = stk_diff[q]; }
+                root = stk_node[sp * 32]; dim = stk_dim[sp * 32]; diffc = stk_diff[sp * 32];
                 cond = __fmul_rn(diffc, diffc) < bestd;
             }
             if (!cond) break;
@@ -303,7 +301,8 @@ struct F3Pair {
 // window slot per lane per round; fills pq/pr (-1: empty), returns the
 // window length.
 __device__ int f3_window(const F3Pair& P, const float* tfm, bool ssfilt, int window, int qrypos,
-                         int rfnpos, int stacksize, int* pq, int* pr, int lane) {
+                         int rfnpos, int stacksize, int* pq, int* pr, int lane, unsigned short* sn,
+                         float* sd, unsigned char* sm) {
     const int lq = P.lq, lr = P.lr;
     int n;
     if (lq < lr) {
@@ -317,7 +316,7 @@ __device__ int f3_window(const F3Pair& P, const float* tfm, bool ssfilt, int win
             float x, y, z;
             xform(tfm, P.qx[q], P.qy[q], P.qz[q], x, y, z);
             const int r = f3_nn(P.rnx, P.rny, P.rnz, P.rnl, P.rnr, P.rno, P.rs, lr, ssfilt, P.qs[q],
-                                x, y, z, stacksize);
+                                x, y, z, stacksize, sn, sd, sm);
             pq[pi] = q;
             pr[pi] = r > 0 ? r : -1;
         }
@@ -332,7 +331,7 @@ __device__ int f3_window(const F3Pair& P, const float* tfm, bool ssfilt, int win
             float x, y, z;
             xform(tfm, P.rx[r], P.ry[r], P.rz[r], x, y, z);
             const int q = f3_nn(P.qnx, P.qny, P.qnz, P.qnl, P.qnr, P.qno, P.qs, lq, ssfilt, P.rs[r],
-                                x, y, z, stacksize);
+                                x, y, z, stacksize, sn, sd, sm);
             pq[pi] = q > 0 ? q : -1;
             pr[pi] = r;
         }
@@ -386,14 +385,23 @@ __device__ __forceinline__ int f3_stacksize(int lq, int lr) {
     return b < F3_MAXSTACK ? b : F3_MAXSTACK;
 }
 
-// A warp per listed pair: every configuration in order; the slot of a scored
-// configuration is the pair's count of them mod 32, and keeps its best.
-__global__ void __launch_bounds__(F3_WARPS * 32) k_f3_search(Blk B, Bat T, int depth) {
+// A CTA per listed pair, its F3_WARPS warps on consecutive configurations
+// (one each per round); a scored configuration's slot is the pair's count
+// of scored configurations before it mod 32, and the slot keeps its best:
+// after each round the round's results are applied in configuration order,
+// as one warp going through the configurations in order would.
+__global__ void __launch_bounds__(F3_WARPS * 32, 3) k_f3_search(Blk B, Bat T, int depth) {
     __shared__ int s_pq[F3_WARPS][F3_MAXWIN], s_pr[F3_WARPS][F3_MAXWIN];
     __shared__ float s_omax[F3_WARPS][F3_HASH], s_ondx[F3_WARPS][F3_HASH];
+    __shared__ unsigned short s_stkn[F3_WARPS][F3_MAXSTACK * 32];
+    __shared__ float s_stkd[F3_WARPS][F3_MAXSTACK * 32];
+    __shared__ unsigned char s_stkm[F3_WARPS][F3_MAXSTACK * 32];
+    // a round's results: per warp and fragment, scored (1) or not, score, transform
+    __shared__ int s_got[F3_WARPS][2];
+    __shared__ float s_res[F3_WARPS][2][13];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    const int slot = blockIdx.x * F3_WARPS + w;
-    if (slot >= T.rhist[RL_NBUCKET]) return;
+    const int slot = blockIdx.x;
+    if (slot >= T.rhist[RL_NBUCKET]) return;       // the same for the whole CTA
     const int i = T.rlist[slot];
     const int qi = pair_q(B, T, i), ri = pair_r(B, T, i);
     F3Pair P;
@@ -413,63 +421,84 @@ __global__ void __launch_bounds__(F3_WARPS * 32) k_f3_search(Blk B, Bat T, int d
     const unsigned char* m = T.lsm + T.off_lsm[i];
     int* pq = s_pq[w];
     int* pr = s_pr[w];
+    unsigned short* sn = s_stkn[w] + lane;
+    float* sd = s_stkd[w] + lane;
+    unsigned char* sm = s_stkm[w] + lane;
     float* slots = T.f3slot + (long long)i * F3_NTOP * 13;
-    for (int k = lane; k < F3_NTOP; k += 32) slots[k * 13] = 0.f;
-    __syncwarp();
+    for (int k = threadIdx.x; k < F3_NTOP; k += blockDim.x) slots[k * 13] = 0.f;
     const float thr = __fdiv_rn((float)B.f3trigger, 100.0f);
     const int seedrule = B.f3seedrule;
     const int qstep = f3_step(depth, lq), rstep = f3_step(depth, lr);
     const int minn = depth == 3 ? 5 : 10;
     int nsy = lq / qstep + 1; if (nsy < minn) nsy = minn;
     int nsx = lr / rstep + 1; if (nsx < minn) nsx = minn;
+    const int nconf = nsy * nsx;
     const int stacksize = f3_stacksize(lq, lr);
     const int f0 = f3_fraglen(lq, lr, 0, 0), f1 = f3_fraglen(lq, lr, 1, 0);
     const int nfr = seedrule ? 1 : 2;
-    int nscored = 0;
-    for (int ys = 0; ys < nsy; ys++)
-    for (int xs = 0; xs < nsx; xs++) {
-        const int qrypos = ys * qstep, rfnpos = xs * rstep;
-        if (lq < qrypos + f0 || lr < rfnpos + f0 || f0 < 1) continue;
-        const bool conv1 = (lq < qrypos + f1 || lr < rfnpos + f1 || f1 < 1);
-        if (0.0f < thr && !f3_similar(m, lq, lr, qrypos, rfnpos, f1, thr, lane)) continue;
-        for (int fi = 0; fi < nfr; fi++) {
-            if (fi == 1 && conv1) continue;
-            const int fraglen = fi == 0 ? f0 : f1;
-            if (lq < qrypos + fraglen || lr < rfnpos + fraglen) continue;
-            float v[16], tfm[12];
-            int n;
-            if (seedrule) {
-                n = f3_seed_local(m, lq, lr, B.f3trigger > 0, f3_fraglen(lq, lr, fi, seedrule),
-                                  qrypos, rfnpos, pq, pr, lane);
-            } else {
-                for (int k = lane; k < fraglen; k += 32) { pq[k] = qrypos + k; pr[k] = rfnpos + k; }
-                __syncwarp();
-                n = fraglen;
-            }
-            if (n < 1) continue;
-            f3_cov(P.qx, P.qy, P.qz, P.rx, P.ry, P.rz, pq, pr, n, v, lane);
-            __syncwarp();
-            if (v[15] < 1.0f) continue;
-            solve_sums(v, lq < lr ? 0 : 2, tfm);
-            for (int it = 0; it < 2; it++) {
-                const int cw = f3_window(P, tfm, it == 0, B.f3window, qrypos, rfnpos, stacksize,
-                                         pq, pr, lane);
-                f3_cov(P.qx, P.qy, P.qz, P.rx, P.ry, P.rz, pq, pr, cw, v, lane);
-                if (v[15] < 1.0f) { __syncwarp(); continue; }
-                if (it == 0) { solve_sums(v, lq < lr ? 0 : 2, tfm); __syncwarp(); continue; }
-                solve_sums(v, 0, tfm);
-                const float sc = f3_progressive(P, tfm, d02, pq, pr, (int)v[15], lq < lr,
-                                                s_omax[w], s_ondx[w], lane);
-                const int k = nscored % F3_NTOP;
-                nscored++;
-                if (lane == 0 && 0.0f < sc && slots[k * 13] < sc) {
-                    slots[k * 13] = sc;
-#pragma unroll
-                    for (int f = 0; f < 12; f++) slots[k * 13 + 1 + f] = tfm[f];
+    int nscored = 0;                              // kept by thread 0
+    for (int c0 = 0; c0 < nconf; c0 += F3_WARPS) {
+        const int c = c0 + w;
+        if (lane < 2) s_got[w][lane] = 0;
+        __syncwarp();
+        if (c < nconf) {
+            const int qrypos = (c / nsx) * qstep, rfnpos = (c % nsx) * rstep;
+            bool go = !(lq < qrypos + f0 || lr < rfnpos + f0 || f0 < 1);
+            const bool conv1 = (lq < qrypos + f1 || lr < rfnpos + f1 || f1 < 1);
+            if (go && 0.0f < thr && !f3_similar(m, lq, lr, qrypos, rfnpos, f1, thr, lane)) go = false;
+            for (int fi = 0; go && fi < nfr; fi++) {
+                if (fi == 1 && conv1) continue;
+                const int fraglen = fi == 0 ? f0 : f1;
+                if (lq < qrypos + fraglen || lr < rfnpos + fraglen) continue;
+                float v[16], tfm[12];
+                int n;
+                if (seedrule) {
+                    n = f3_seed_local(m, lq, lr, B.f3trigger > 0, f3_fraglen(lq, lr, fi, seedrule),
+                                      qrypos, rfnpos, pq, pr, lane);
+                } else {
+                    for (int k = lane; k < fraglen; k += 32) { pq[k] = qrypos + k; pr[k] = rfnpos + k; }
+                    __syncwarp();
+                    n = fraglen;
                 }
+                if (n < 1) continue;
+                f3_cov(P.qx, P.qy, P.qz, P.rx, P.ry, P.rz, pq, pr, n, v, lane);
                 __syncwarp();
+                if (v[15] < 1.0f) continue;
+                solve_sums(v, lq < lr ? 0 : 2, tfm);
+                for (int it = 0; it < 2; it++) {
+                    const int cw = f3_window(P, tfm, it == 0, B.f3window, qrypos, rfnpos, stacksize,
+                                             pq, pr, lane, sn, sd, sm);
+                    f3_cov(P.qx, P.qy, P.qz, P.rx, P.ry, P.rz, pq, pr, cw, v, lane);
+                    if (v[15] < 1.0f) { __syncwarp(); continue; }
+                    if (it == 0) { solve_sums(v, lq < lr ? 0 : 2, tfm); __syncwarp(); continue; }
+                    solve_sums(v, 0, tfm);
+                    const float sc = f3_progressive(P, tfm, d02, pq, pr, (int)v[15], lq < lr,
+                                                    s_omax[w], s_ondx[w], lane);
+                    if (lane == 0) {
+                        s_got[w][fi] = 1;
+                        s_res[w][fi][0] = sc;
+#pragma unroll
+                        for (int f = 0; f < 12; f++) s_res[w][fi][1 + f] = tfm[f];
+                    }
+                    __syncwarp();
+                }
             }
         }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            for (int ww = 0; ww < F3_WARPS; ww++)
+                for (int fi = 0; fi < 2; fi++) {
+                    if (!s_got[ww][fi]) continue;
+                    const int k = nscored % F3_NTOP;
+                    nscored++;
+                    const float sc = s_res[ww][fi][0];
+                    if (0.0f < sc && slots[k * 13] < sc) {
+                        slots[k * 13] = sc;
+                        for (int f = 0; f < 12; f++) slots[k * 13 + 1 + f] = s_res[ww][fi][1 + f];
+                    }
+                }
+        }
+        __syncthreads();
     }
 }
 
@@ -542,7 +571,7 @@ void launch_frg3(const Blk& B, const Bat& T, cudaStream_t st) {
             k_f3_localdp<<<nb, 128, 0, st>>>(B, T);
             if (T.launches) (*T.launches)++;
         }
-        k_f3_search<<<(T.np + F3_WARPS - 1) / F3_WARPS, F3_WARPS * 32, 0, st>>>(B, T, B.depth);
+        k_f3_search<<<T.np, F3_WARPS * 32, 0, st>>>(B, T, B.depth);
         if (T.launches) (*T.launches)++;
         launch_f3_dpscore(B, T, st);
         k_f3_select<<<(T.np + 255) / 256, 256, 0, st>>>(B, T, nbr);

@@ -1744,30 +1744,34 @@ void launch_pair_list(const Blk& B, const Bat& T, int skipmask, cudaStream_t st)
 // Detailed search: the DP scores of a pair's fragment slots
 // (ExecDPScore128xKernel, MpDPHub.cpp:389-645): for every slot with a
 // positive score, the last cell of the gap-0 DP under the slot's transform
-// (search d0), no traceback; 0 for the others.  A warp per listed pair, its
-// slots one after another (they share the pair's row buffer).
+// (search d0), no traceback; 0 for the others.  A warp per (listed pair,
+// slot) item, the items walked by a grid of resident warps in list order
+// (largest pairs first); each slot's DP keeps its strip row in the pair's
+// detailed-search region (the local score matrix is no longer read).
 __global__ void __launch_bounds__(128) k_f3_dpscore(Blk B, Bat T) {
     const int lane = threadIdx.x & 31;
-    const int slot = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-    if (slot >= T.rhist[RL_NB]) return;
-    const int i = T.rlist[slot];
-    int qi = pair_qi(B, T, i), ri = pair_ri(B, T, i);
-    int lq = B.qlen[qi], lr = B.rlen[ri];
-    int ml = lq < lr ? lq : lr;
-    const float d0 = B.t_d0[ml];
-    const float d02 = __fmul_rn(d0, d0);
-    const float* qx = B.qx + B.qoff[qi];
-    const float* qy = B.qy + B.qoff[qi];
-    const float* qz = B.qz + B.qoff[qi];
-    const float4* r4 = B.r4 + B.r4off[ri];
-    float* row = T.row + T.off_row[i];
-    for (int k = 0; k < F3_NTOP; k++) {
+    const long long nitems = (long long)T.rhist[RL_NB] * F3_NTOP;
+    const long long wstride = (long long)gridDim.x * (blockDim.x >> 5);
+    for (long long it = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); it < nitems;
+         it += wstride) {
+        const int i = T.rlist[it / F3_NTOP];
+        const int k = (int)(it % F3_NTOP);
         const float* sl = T.f3slot + ((long long)i * F3_NTOP + k) * 13;
         float* fin = T.f3dps + (long long)i * F3_NTOP + k;
         if (!(0.f < sl[0])) {
             if (lane == 0) *fin = 0.f;
             continue;
         }
+        int qi = pair_qi(B, T, i), ri = pair_ri(B, T, i);
+        int lq = B.qlen[qi], lr = B.rlen[ri];
+        int ml = lq < lr ? lq : lr;
+        const float d0 = B.t_d0[ml];
+        const float d02 = __fmul_rn(d0, d0);
+        const float* qx = B.qx + B.qoff[qi];
+        const float* qy = B.qy + B.qoff[qi];
+        const float* qz = B.qz + B.qoff[qi];
+        const float4* r4 = B.r4 + B.r4off[ri];
+        float* row = (float*)(T.lsm + T.off_lsm[i]) + (long long)k * lr;
         float t[12];
 #pragma unroll
         for (int f = 0; f < 12; f++) t[f] = sl[1 + f];
@@ -1785,7 +1789,13 @@ __global__ void __launch_bounds__(128) k_f3_dpscore(Blk B, Bat T) {
 }
 
 void launch_f3_dpscore(const Blk& B, const Bat& T, cudaStream_t st) {
-    k_f3_dpscore<<<(T.np + 3) / 4, 128, 0, st>>>(B, T);
+    // enough warps to fill the GPU (the kernel walks its items)
+    int dev = 0, nsm = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    const long long need = ((long long)T.np * F3_NTOP + 3) / 4;
+    const int ng = (int)std::min<long long>(need, (long long)nsm * 8);
+    k_f3_dpscore<<<ng > 0 ? ng : 1, 128, 0, st>>>(B, T);
     GTB_LAUNCHED(T);
 }
 

@@ -27,6 +27,14 @@ constexpr int RLW_CAND = 17;         // floats per warp candidate
 
 constexpr int DP_R4_MIN = 384;
 __host__ __device__ inline int dp_r(int lq) { return lq >= DP_R4_MIN ? 4 : 2; }
+// bytes of a pair's detailed-search region: its local score matrix (lq x lr
+// bytes), later the 32 slot DPs' row buffers (32 x lr floats, which the DP
+// writes for every strip); a multiple of 16
+__host__ __device__ inline long long f3_region_bytes(int lq, int lr) {
+    long long b = (long long)lq * lr;
+    if (b < 128LL * lr) b = 128LL * lr;
+    return (b + 15) & ~15LL;
+}
 __host__ __device__ inline long long bt_strip_words(int lr, int R) {
     const int spw = 16 / R;
     return (long long)((lr + 31 + spw - 1) / spw) * 32;
