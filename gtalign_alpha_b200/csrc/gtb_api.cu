@@ -202,8 +202,8 @@ struct DevBlock {
     const unsigned char *qa, *ra;
     char *qs, *rs;
     // index trees (null: none)
-    const float *qnx = nullptr, *qny = nullptr, *qnz = nullptr, *rnx = nullptr, *rny = nullptr, *rnz = nullptr;
-    const int *qnl = nullptr, *qnr = nullptr, *qno = nullptr, *rnl = nullptr, *rnr = nullptr, *rno = nullptr;
+    const float4 *qnd = nullptr, *rnd = nullptr;
+    const int2 *qnc = nullptr, *rnc = nullptr;
     // clustering runs: the references' global indices and the end of the
     // query block's (qrysernrbeg + nqystrs, CuBatch.cu:492-494)
     const int* rtype = nullptr;
@@ -295,12 +295,11 @@ static gtb_status run_block(gtb_handle* h, const DevBlock& D, float scorethld,
     }
     B.f3 = o.nodetailedsearch ? 0 : 1;
     if (B.f3) {
-        if (!D.qnx || !D.rnx) {
+        if (!D.qnd || !D.rnd) {
             snprintf(h->err, sizeof(h->err), "the detailed search needs the blocks' index trees");
             return GTB_ERR_ARG;
         }
-        B.qnx = D.qnx; B.qny = D.qny; B.qnz = D.qnz; B.qnl = D.qnl; B.qnr = D.qnr; B.qno = D.qno;
-        B.rnx = D.rnx; B.rny = D.rny; B.rnz = D.rnz; B.rnl = D.rnl; B.rnr = D.rnr; B.rno = D.rno;
+        B.qnd = D.qnd; B.qnc = D.qnc; B.rnd = D.rnd; B.rnc = D.rnc;
         B.f3trigger = o.trigger; B.f3nbranches = o.nbranches;
         B.f3gapcost = o.gapcost == 0 ? -0.8f : (o.gapcost == 1 ? -1.2f : -3.0f);
         B.f3seedrule = o.seedrule == 0 ? 0 : (o.seedrule == 1 ? 64 : 128);
@@ -730,6 +729,8 @@ struct gtb_block {
     // index trees (null: none): node x, y, z; left, right, residue
     float *nx = nullptr, *ny = nullptr, *nz = nullptr;
     int *nl = nullptr, *nr = nullptr, *no = nullptr;
+    float4* nd = nullptr;            // the trees packed for the walks (launch_pack_nodes)
+    int2* nc = nullptr;
 };
 
 // the detailed search needs the blocks' index trees
@@ -793,6 +794,8 @@ static gtb_status upload_block(gtb_handle* h, const HostSoA& S, gtb_block* b,
     size_t oa = carve(S.npos), os = carve(S.npos);
     size_t o4 = carve(S.npos * 16);
     size_t on = ndx ? carve((size_t)S.npos * 4 * GTB_NNDXFIELDS) : 0;
+    size_t ond = ndx ? carve((size_t)S.npos * 16) : 0;
+    size_t onc = ndx ? carve((size_t)S.npos * 8) : 0;
     // from the device's memory pool (kept between calls), in stream order
     CK(cudaMallocAsync((void**)&b->dbase, sz, st));
     b->st = st;
@@ -810,6 +813,7 @@ static gtb_status upload_block(gtb_handle* h, const HostSoA& S, gtb_block* b,
         int* ni = (int*)(nf + 3 * S.npos);
         b->nx = nf; b->ny = nf + S.npos; b->nz = nf + 2 * S.npos;
         b->nl = ni; b->nr = ni + S.npos; b->no = ni + 2 * S.npos;
+        b->nd = (float4*)(d + ond); b->nc = (int2*)(d + onc);
         void* dst[GTB_NNDXFIELDS] = {b->nx, b->ny, b->nz, b->nl, b->nr, b->no};
         for (int f = 0; f < GTB_NNDXFIELDS; f++)
             CK(cudaMemcpyAsync(dst[f], src[f], (size_t)S.npos * 4, cudaMemcpyHostToDevice, st));
@@ -824,6 +828,9 @@ static gtb_status upload_block(gtb_handle* h, const HostSoA& S, gtb_block* b,
     long long nl = 0;
     launch_pack4(b->c4, b->x, b->y, b->z, S.npos, st);
     launch_secstr(b->ss, b->x, b->y, b->z, b->dlen, b->doff, b->dmol, b->n, st, &nl);
+    if (ndx)
+        launch_pack_nodes(b->nd, b->nc, b->nx, b->ny, b->nz, b->nl, b->nr, b->no, b->doff, b->dlen,
+                          b->ss, S.npos, b->n, st);
     CK(cudaGetLastError());
     return GTB_OK;
 }
@@ -869,8 +876,7 @@ static DevBlock make_devblock(const gtb_block* Q, const gtb_block* R) {
     D.qx = Q->x; D.qy = Q->y; D.qz = Q->z; D.rx = R->x; D.ry = R->y; D.rz = R->z;
     D.q4 = Q->c4; D.r4 = R->c4;
     D.qa = Q->rsd; D.ra = R->rsd; D.qs = Q->ss; D.rs = R->ss;
-    D.qnx = Q->nx; D.qny = Q->ny; D.qnz = Q->nz; D.qnl = Q->nl; D.qnr = Q->nr; D.qno = Q->no;
-    D.rnx = R->nx; D.rny = R->ny; D.rnz = R->nz; D.rnl = R->nl; D.rnr = R->nr; D.rno = R->no;
+    D.qnd = Q->nd; D.qnc = Q->nc; D.rnd = R->nd; D.rnc = R->nc;
     D.rtype = R->dtype; D.qtypeend = Q->typemin + Q->n;
     D.hqlen = Q->len; D.hrlen = R->len;
     return D;

@@ -240,26 +240,28 @@ __device__ void f3_cov(const float* qx, const float* qy, const float* qz, const 
 // Nearest neighbour in a structure's 3-d tree (NNByIndex*,
 // MpStageFrg3.h:1270-1440): depth first with a bounded stack, at most 64
 // nodes visited; with ssfilt only residues of secondary structure ss count
-// and one farther than 8 A is none.  Returns the residue or -1.
-// The stack is the lane's column of a shared-memory array (entry q at
-// [q * 32]).
-__device__ int f3_nn(const float* nx, const float* ny, const float* nz, const int* nl,
-                     const int* nr, const int* no, const char* sss, int len, bool ssfilt, char ss,
-                     float px, float py, float pz, int stacksize, unsigned short* stk_node,
-                     float* stk_diff, unsigned char* stk_dim) {
+// and one farther than 8 A is none.  Returns the residue or -1.  Nodes are
+// packed (k_pack_nodes): nd = (x, y, z, residue | SS << 16), nc = (left,
+// right).  The stack is the lane's column of a shared-memory array (entry q
+// at [q * 32]).
+__device__ int f3_nn(const float4* nd, const int2* nc, int len, bool ssfilt, char ss, float px,
+                     float py, float pz, int stacksize, unsigned short* stk_node, float* stk_diff,
+                     unsigned char* stk_dim) {
     int sp = 0, nvisited = 0, best = -1, root = len >> 1, dim = 0;
     float bestd = 9.9e6f;
     while (0 < sp || 0 <= root) {
         if (0 <= root) {
             nvisited++;
             if (F3_MAXVISIT <= nvisited) break;
-            const int org = __ldg(no + root);
-            const float x = __ldg(nx + root), y = __ldg(ny + root), z = __ldg(nz + root);
-            const float dx = __fsub_rn(x, px), dy = __fsub_rn(y, py), dz = __fsub_rn(z, pz);
+            const float4 n = __ldg(nd + root);
+            const int2 ch = __ldg(nc + root);
+            const int ow = __float_as_int(n.w);
+            const int org = ow & 0xffff;
+            const float dx = __fsub_rn(n.x, px), dy = __fsub_rn(n.y, py), dz = __fsub_rn(n.z, pz);
             const float d2 = __fmaf_rn(dx, dx, __fmaf_rn(dy, dy, __fmul_rn(dz, dz)));
-            if ((best < 0 || d2 < bestd) && (!ssfilt || sss[org] == ss)) {
+            if ((best < 0 || d2 < bestd) && (!ssfilt || (char)(ow >> 16) == ss)) {
                 bestd = d2;
-                best = ssfilt ? org : root;
+                best = org;
             }
             if (bestd == 0.0f) break;
             const float diffc = dim == 0 ? dx : (dim == 1 ? dy : dz);
@@ -270,7 +272,7 @@ __device__ int f3_nn(const float* nx, const float* ny, const float* nz, const in
                 stk_diff[sp * 32] = diffc;
                 sp++;
             }
-            root = (0.0f < diffc) ? __ldg(nl + root) : __ldg(nr + root);
+            root = (0.0f < diffc) ? ch.x : ch.y;
         } else {
             bool cond = false;
             float diffc = 0.f;
@@ -280,11 +282,12 @@ __device__ int f3_nn(const float* nx, const float* ny, const float* nz, const in
                 cond = __fmul_rn(diffc, diffc) < bestd;
             }
             if (!cond) break;
-            root = (0.0f < diffc) ? __ldg(nr + root) : __ldg(nl + root);
+            const int2 ch = __ldg(nc + root);
+            root = (0.0f < diffc) ? ch.y : ch.x;
         }
     }
     if (ssfilt) return F3_SSDST2 < bestd ? -1 : best;
-    return 0 <= best ? __ldg(no + best) : -1;
+    return best;
 }
 
 // per-pair view of the search's inputs
@@ -292,8 +295,8 @@ struct F3Pair {
     int lq, lr;
     const float *qx, *qy, *qz, *rx, *ry, *rz;
     const char *qs, *rs;
-    const float *qnx, *qny, *qnz, *rnx, *rny, *rnz;
-    const int *qnl, *qnr, *qno, *rnl, *rnr, *rno;
+    const float4 *qnd, *rnd;
+    const int2 *qnc, *rnc;
 };
 
 // Neighbours over the window of the shorter structure
@@ -315,8 +318,7 @@ __device__ int f3_window(const F3Pair& P, const float* tfm, bool ssfilt, int win
             const int q = qp + pi;
             float x, y, z;
             xform(tfm, P.qx[q], P.qy[q], P.qz[q], x, y, z);
-            const int r = f3_nn(P.rnx, P.rny, P.rnz, P.rnl, P.rnr, P.rno, P.rs, lr, ssfilt, P.qs[q],
-                                x, y, z, stacksize, sn, sd, sm);
+            const int r = f3_nn(P.rnd, P.rnc, lr, ssfilt, P.qs[q], x, y, z, stacksize, sn, sd, sm);
             pq[pi] = q;
             pr[pi] = r > 0 ? r : -1;
         }
@@ -330,8 +332,7 @@ __device__ int f3_window(const F3Pair& P, const float* tfm, bool ssfilt, int win
             const int r = rp + pi;
             float x, y, z;
             xform(tfm, P.rx[r], P.ry[r], P.rz[r], x, y, z);
-            const int q = f3_nn(P.qnx, P.qny, P.qnz, P.qnl, P.qnr, P.qno, P.qs, lq, ssfilt, P.rs[r],
-                                x, y, z, stacksize, sn, sd, sm);
+            const int q = f3_nn(P.qnd, P.qnc, lq, ssfilt, P.rs[r], x, y, z, stacksize, sn, sd, sm);
             pq[pi] = q > 0 ? q : -1;
             pr[pi] = r;
         }
@@ -344,9 +345,37 @@ __device__ int f3_window(const F3Pair& P, const float* tfm, bool ssfilt, int win
 // MpStageFrg3.h:760-850) over the first cnt window slots: each pair extends
 // the best chain of earlier-partnered pairs kept in a 512-entry table hashed
 // by partner index; lanes share the table scan, lane 0 updates it.
+//
+// When the partner structure has at most F3_HASH residues no two partners
+// share an entry, so an entry only ever rises (to the larger chain score of
+// its own partner) and the scan "best entry with a lower partner" is the
+// running maximum of the entries below the partner's: the table is then
+// kept as prefix maxima (pm[k] = max of entries 0..k), read with one load
+// and raised by every lane for its own entries at or above the partner's.
 __device__ float f3_progressive(const F3Pair& P, const float* tfm, float d02, const int* pq,
                                 const int* pr, int cnt, bool partner_is_r, float* omax,
                                 float* ondx, int lane) {
+    if ((partner_is_r ? P.lr : P.lq) <= F3_HASH) {
+        float* pm = omax;
+        for (int k = lane; k < F3_HASH; k += 32) pm[k] = 0.f;
+        __syncwarp();
+        for (int pi = 0; pi < cnt; pi++) {
+            const int a = pq[pi], b = pr[pi];
+            if (a < 0 || b < 0) continue;          // the same on every lane
+            const float d = dist2_tf(tfm, P.qx[a], P.qy[a], P.qz[a], P.rx[b], P.ry[b], P.rz[b]);
+            const float sco = tmterm(d02, d);
+            if (!(0.f < sco)) continue;
+            const int c = partner_is_r ? b : a;
+            const float mx = c > 0 ? pm[c - 1] : 0.f;
+            const float nsc = __fadd_rn(mx, sco);
+            __syncwarp();
+            for (int k = c + ((lane - c) & 31); k < F3_HASH; k += 32) pm[k] = fmaxf(pm[k], nsc);
+            __syncwarp();
+        }
+        const float mx = pm[F3_HASH - 1];
+        __syncwarp();
+        return mx;
+    }
     for (int k = lane; k < F3_HASH; k += 32) { omax[k] = 0.f; ondx[k] = -1.f; }
     __syncwarp();
     for (int pi = 0; pi < cnt; pi++) {
@@ -410,10 +439,8 @@ __global__ void __launch_bounds__(F3_WARPS * 32, 3) k_f3_search(Blk B, Bat T, in
     P.qx = B.qx + qo; P.qy = B.qy + qo; P.qz = B.qz + qo;
     P.rx = B.rx + ro; P.ry = B.ry + ro; P.rz = B.rz + ro;
     P.qs = B.qs + qo; P.rs = B.rs + ro;
-    P.qnx = B.qnx + qo; P.qny = B.qny + qo; P.qnz = B.qnz + qo;
-    P.qnl = B.qnl + qo; P.qnr = B.qnr + qo; P.qno = B.qno + qo;
-    P.rnx = B.rnx + ro; P.rny = B.rny + ro; P.rnz = B.rnz + ro;
-    P.rnl = B.rnl + ro; P.rnr = B.rnr + ro; P.rno = B.rno + ro;
+    P.qnd = B.qnd + qo; P.qnc = B.qnc + qo;
+    P.rnd = B.rnd + ro; P.rnc = B.rnc + ro;
     const int lq = P.lq, lr = P.lr;
     const int ml = lq < lr ? lq : lr;
     const float d0 = B.t_d0[ml];

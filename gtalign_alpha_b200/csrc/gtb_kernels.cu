@@ -198,6 +198,32 @@ __device__ __forceinline__ bool cls_pass(const Blk& B, int qi, int ri) {
     return B.rtype[ri] < B.clsqend && __fmul_rn(fmaxf(lq, lr), B.clscov) <= fminf(lq, lr);
 }
 
+// a thread per node; the residue index is relative to the structure, its SS
+// byte at the structure's offset + residue
+__global__ void k_pack_nodes(float4* nd, int2* nc, const float* x, const float* y, const float* z,
+                             const int* l, const int* r, const int* o, const int* off,
+                             const int* len, const char* ss, int nstr) {
+    const int s = blockIdx.y;
+    if (s >= nstr) return;
+    const int L = len[s], a = off[s];
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < L; k += gridDim.x * blockDim.x) {
+        const int p = a + k, org = o[p];
+        const unsigned w = (unsigned)org | ((unsigned)(unsigned char)ss[a + org] << 16);
+        nd[p] = make_float4(x[p], y[p], z[p], __uint_as_float(w));
+        nc[p] = make_int2(l[p], r[p]);
+    }
+}
+
+void launch_pack_nodes(float4* nd, int2* nc, const float* x, const float* y, const float* z,
+                       const int* l, const int* r, const int* o, const int* off, const int* len,
+                       const char* ss, long long n, int nstr, cudaStream_t st) {
+    (void)n;
+    for (int s0 = 0; s0 < nstr; s0 += 65535) {
+        const int ns = nstr - s0 < 65535 ? nstr - s0 : 65535;
+        k_pack_nodes<<<dim3(4, ns), 128, 0, st>>>(nd, nc, x, y, z, l, r, o, off + s0, len + s0, ss, ns);
+    }
+}
+
 __global__ void k_init(Blk B, Bat T) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= T.np) return;

@@ -65,11 +65,11 @@ struct Blk {
     int addss;                       // --add-search-by-ss
     float presim;                    // --pre-similarity threshold when the screen runs, else 0
     // the spatial-index detailed search (f3 = 1: on): the structures' index
-    // trees (node x, y, z; left, right child; residue), at the residue offsets
-    // of the coordinates, and its options
+    // trees, packed per node (launch_pack_nodes) at the residue offsets of
+    // the coordinates, and its options
     int f3;
-    const float *qnx, *qny, *qnz, *rnx, *rny, *rnz;
-    const int *qnl, *qnr, *qno, *rnl, *rnr, *rno;
+    const float4 *qnd, *rnd;
+    const int2 *qnc, *rnc;
     int f3trigger, f3nbranches, f3seedrule, f3window;
     float f3gapcost;
     // clustering runs: the prefilter of CheckMaxCoverage (cls = 1): the
@@ -197,6 +197,12 @@ void launch_pack4(float4* out, const float* x, const float* y, const float* z, l
 void launch_pack4_structs(float4* out, const float* x, const float* y, const float* z,
                           const int* off, const int* len, const int* coff, int n,
                           cudaStream_t st);
+// index tree nodes packed for the walks: nd[k] = (x, y, z, residue | SS << 16),
+// nc[k] = (left, right); n positions of a block (ss: the block's secondary
+// structure, computed before)
+void launch_pack_nodes(float4* nd, int2* nc, const float* x, const float* y, const float* z,
+                       const int* l, const int* r, const int* o, const int* off, const int* len,
+                       const char* ss, long long n, int nstr, cudaStream_t st);
 void launch_init(const Blk& B, const Bat& T, cudaStream_t st);
 // the --pre-similarity screen (B.presim > 0): 20 positions kept from the ends
 constexpr int PRESIM_EDGE = 20;
