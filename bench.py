@@ -67,8 +67,8 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 # k_findfrag DRAM read + write per pair (ncu, one seed launch of the benchmark
-# step: profiles/findfrag_c1_2x200000.md)
-FINDFRAG_DRAM_BYTES_PER_PAIR = (102.29e6 + 5.99e6) / 13333
+# step, 66,667 pairs: profiles/findfrag_dram_c1_2x200000.md)
+FINDFRAG_DRAM_BYTES_PER_PAIR = (336.93e6 + 8.44e6) / 66667
 
 METRIC = "pairs/s on 1 B200 at |dTM|<=1e-4; batched+adjoint vs plain; HBM % of peak"
 UNIT = "pairs/s"
@@ -437,7 +437,7 @@ def run_ours(args):
     roof = {"bound": "hbm", "kernel": "k_findfrag (stage-1 seed scan)",
             "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
             "frac": achieved / hbm_peak, "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)",
-            "traffic": traffic, "traffic_unit": "bytes per launch (ncu, one seed launch of the step)",
+            "traffic": traffic, "traffic_unit": "bytes per launch (ncu, one seed launch of the bench step)",
             "algorithmic_bytes_per_launch": algo_bytes / nsub,
             "fp32": {"bound": "fp32 SIMT", "achieved": fp32_ach, "unit": "TFLOP/s",
                      "peak": fp32_peak, "frac": fp32_ach / fp32_peak,

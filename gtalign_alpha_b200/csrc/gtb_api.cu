@@ -396,12 +396,14 @@ static gtb_status run_block(gtb_handle* h, const DevBlock& D, float scorethld,
                 for (int k = 0; k < nl; k++) mk[lp[k]] = 1;
             }
         }
-        // pairs that may reach the long-pair threshold of some refinement
-        // launch (n <= min(lq, lr))
-        int nlmax = 0;
+        // pairs that may reach the long-pair thresholds of the refinement
+        // launches (n <= min(lq, lr)): the first tier and the second
+        int nlmax = 0, nlmax2 = 0;
         for (int i = 0; i < np; i++) {
             long long p = q0 + i;
-            if (std::min(D.hqlen[p / D.nr], D.hrlen[p % D.nr]) >= gtb::RL_LONG_FEW) nlmax++;
+            const int ml = std::min(D.hqlen[p / D.nr], D.hrlen[p % D.nr]);
+            if (ml >= gtb::RL_LONG) nlmax++;
+            else if (ml >= gtb::RL_LONG_FEW) nlmax2++;
         }
         std::vector<int>& ffi = ffiv[j];
         if (split) {
@@ -436,6 +438,8 @@ static gtb_status run_block(gtb_handle* h, const DevBlock& D, float scorethld,
         size_t o_dwe = nl ? carve(sizeof(int)) : 0;
         size_t o_rll = nlmax ? carve((size_t)(2 * nlmax + 1) * sizeof(int)) : 0;
         size_t o_rlc = nlmax ? carve((size_t)nlmax * gtb::RLW_WARPS * gtb::RLW_CAND * sizeof(float)) : 0;
+        size_t o_rll2 = nlmax2 ? carve((size_t)(2 * nlmax2 + 1) * sizeof(int)) : 0;
+        size_t o_rlc2 = nlmax2 ? carve((size_t)nlmax2 * gtb::RLW_WARPS * gtb::RLW_CAND * sizeof(float)) : 0;
         // detailed search: local score matrices, slots, DP scores, branches
         size_t o_lsm = B.f3 ? carve((size_t)std::max<long long>(off_lsm[np], 1)) : 0;
         size_t o_f3s = B.f3 ? carve((size_t)np * F3_NTOP * 13 * sizeof(float)) : 0;
@@ -488,6 +492,12 @@ static gtb_status run_block(gtb_handle* h, const DevBlock& D, float scorethld,
             int* rl = (int*)(base + o_rll);
             T.rl_long = rl; T.rl_next = rl + nlmax; T.rl_count = rl + 2 * nlmax;
             T.rl_cand = (float*)(base + o_rlc);
+        }
+        T.rl_nlmax2 = nlmax2; T.rl_long2 = T.rl_count2 = T.rl_next2 = nullptr; T.rl_cand2 = nullptr;
+        if (nlmax2) {
+            int* rl = (int*)(base + o_rll2);
+            T.rl_long2 = rl; T.rl_next2 = rl + nlmax2; T.rl_count2 = rl + 2 * nlmax2;
+            T.rl_cand2 = (float*)(base + o_rlc2);
         }
         T.ndw = 0; T.dw_nprog = 0; T.dw_item = T.dw_pair = T.dw_G = nullptr; T.dw_soff = nullptr;
         T.dw_mark = nullptr; T.dw_prog = nullptr; T.dw_err = nullptr;

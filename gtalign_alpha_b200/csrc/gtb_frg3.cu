@@ -39,6 +39,11 @@ constexpr int F3_MAXSTACK = 17;
 constexpr float F3_SSDST2 = 64.f;   // an SS-matched neighbour farther than 8 A is none
 constexpr int F3_MAXWIN = 512;      // the largest --window
 constexpr int F3_WARPS = 4;         // warps per CTA of the search
+constexpr int F3_PERWARP = 4;       // configurations per warp in a round of the search
+constexpr int F3_ROUND = F3_WARPS * F3_PERWARP;
+// the search's dynamic shared memory: a round's results (scored flags, then
+// score + transform per configuration and fragment)
+constexpr int F3_ROUND_BYTES = F3_ROUND * 2 * (int)sizeof(int) + F3_ROUND * 2 * 13 * (int)sizeof(float);
 
 __device__ __forceinline__ int pair_q(const Blk& B, const Bat& T, int i) { return (int)((T.p0 + i) / B.nr); }
 __device__ __forceinline__ int pair_r(const Blk& B, const Bat& T, int i) { return (int)((T.p0 + i) % B.nr); }
@@ -414,20 +419,23 @@ __device__ __forceinline__ int f3_stacksize(int lq, int lr) {
     return b < F3_MAXSTACK ? b : F3_MAXSTACK;
 }
 
-// A CTA per listed pair, its F3_WARPS warps on consecutive configurations
-// (one each per round); a scored configuration's slot is the pair's count
-// of scored configurations before it mod 32, and the slot keeps its best:
-// after each round the round's results are applied in configuration order,
-// as one warp going through the configurations in order would.
+// A CTA per listed pair; a round is F3_ROUND consecutive configurations,
+// F3_PERWARP per warp (interleaved, so that cheap and dear ones mix); a
+// scored configuration's slot is the pair's count of scored configurations
+// before it mod 32, and the slot keeps its best: after each round the
+// round's results are applied in configuration order, as one warp going
+// through the configurations in order would.
 __global__ void __launch_bounds__(F3_WARPS * 32, 3) k_f3_search(Blk B, Bat T, int depth) {
     __shared__ int s_pq[F3_WARPS][F3_MAXWIN], s_pr[F3_WARPS][F3_MAXWIN];
     __shared__ float s_omax[F3_WARPS][F3_HASH], s_ondx[F3_WARPS][F3_HASH];
     __shared__ unsigned short s_stkn[F3_WARPS][F3_MAXSTACK * 32];
     __shared__ float s_stkd[F3_WARPS][F3_MAXSTACK * 32];
     __shared__ unsigned char s_stkm[F3_WARPS][F3_MAXSTACK * 32];
-    // a round's results: per warp and fragment, scored (1) or not, score, transform
-    __shared__ int s_got[F3_WARPS][2];
-    __shared__ float s_res[F3_WARPS][2][13];
+    // a round's results (F3_ROUND_BYTES, dynamic): per configuration of the
+    // round and fragment, scored (1) or not; score and transform
+    extern __shared__ float s_dyn[];
+    int* s_got = (int*)s_dyn;
+    float* s_res = s_dyn + F3_ROUND * 2;
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int slot = blockIdx.x;
     if (slot >= T.rhist[RL_NBUCKET]) return;       // the same for the whole CTA
@@ -464,9 +472,31 @@ __global__ void __launch_bounds__(F3_WARPS * 32, 3) k_f3_search(Blk B, Bat T, in
     const int f0 = f3_fraglen(lq, lr, 0, 0), f1 = f3_fraglen(lq, lr, 1, 0);
     const int nfr = seedrule ? 1 : 2;
     int nscored = 0;                              // kept by thread 0
-    for (int c0 = 0; c0 < nconf; c0 += F3_WARPS) {
-        const int c = c0 + w;
-        if (lane < 2) s_got[w][lane] = 0;
+    for (int c0 = 0; c0 < nconf; c0 += F3_ROUND)
+    for (int jj = 0; jj <= F3_PERWARP; jj++) {
+      if (jj == F3_PERWARP) {
+        // the round's results in configuration order
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            for (int rr = 0; rr < F3_ROUND; rr++)
+                for (int fi = 0; fi < 2; fi++) {
+                    if (!s_got[rr * 2 + fi]) continue;
+                    const int k = nscored % F3_NTOP;
+                    nscored++;
+                    const float* res = s_res + (rr * 2 + fi) * 13;
+                    const float sc = res[0];
+                    if (0.0f < sc && slots[k * 13] < sc) {
+                        slots[k * 13] = sc;
+                        for (int f = 0; f < 12; f++) slots[k * 13 + 1 + f] = res[1 + f];
+                    }
+                }
+        }
+        __syncthreads();
+        continue;
+      }
+        const int rix = w + F3_WARPS * jj;        // this configuration's place in the round
+        const int c = c0 + rix;
+        if (lane < 2) s_got[rix * 2 + lane] = 0;
         __syncwarp();
         if (c < nconf) {
             const int qrypos = (c / nsx) * qstep, rfnpos = (c % nsx) * rstep;
@@ -502,30 +532,16 @@ __global__ void __launch_bounds__(F3_WARPS * 32, 3) k_f3_search(Blk B, Bat T, in
                     const float sc = f3_progressive(P, tfm, d02, pq, pr, (int)v[15], lq < lr,
                                                     s_omax[w], s_ondx[w], lane);
                     if (lane == 0) {
-                        s_got[w][fi] = 1;
-                        s_res[w][fi][0] = sc;
+                        float* res = s_res + (rix * 2 + fi) * 13;
+                        s_got[rix * 2 + fi] = 1;
+                        res[0] = sc;
 #pragma unroll
-                        for (int f = 0; f < 12; f++) s_res[w][fi][1 + f] = tfm[f];
+                        for (int f = 0; f < 12; f++) res[1 + f] = tfm[f];
                     }
                     __syncwarp();
                 }
             }
         }
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            for (int ww = 0; ww < F3_WARPS; ww++)
-                for (int fi = 0; fi < 2; fi++) {
-                    if (!s_got[ww][fi]) continue;
-                    const int k = nscored % F3_NTOP;
-                    nscored++;
-                    const float sc = s_res[ww][fi][0];
-                    if (0.0f < sc && slots[k * 13] < sc) {
-                        slots[k * 13] = sc;
-                        for (int f = 0; f < 12; f++) slots[k * 13 + 1 + f] = s_res[ww][fi][1 + f];
-                    }
-                }
-        }
-        __syncthreads();
     }
 }
 
@@ -598,7 +614,9 @@ void launch_frg3(const Blk& B, const Bat& T, cudaStream_t st) {
             k_f3_localdp<<<nb, 128, 0, st>>>(B, T);
             if (T.launches) (*T.launches)++;
         }
-        k_f3_search<<<T.np, F3_WARPS * 32, 0, st>>>(B, T, B.depth);
+        // static arrays (~48 kB) + the round's results go past the default 48 kB
+        cudaFuncSetAttribute(k_f3_search, cudaFuncAttributeMaxDynamicSharedMemorySize, F3_ROUND_BYTES);
+        k_f3_search<<<T.np, F3_WARPS * 32, F3_ROUND_BYTES, st>>>(B, T, B.depth);
         if (T.launches) (*T.launches)++;
         launch_f3_dpscore(B, T, st);
         k_f3_select<<<(T.np + 255) / 256, 256, 0, st>>>(B, T, nbr);

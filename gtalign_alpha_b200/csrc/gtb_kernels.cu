@@ -739,6 +739,9 @@ __global__ void k_rlist_count(Blk B, Bat T, int mode) {
     if (n >= T.rl_min && T.rl_long) {          // many warps for this pair
         int slot = atomicAdd(T.rl_count, 1);
         if (slot < T.rl_nlmax) { T.rl_long[slot] = i; return; }
+    } else if (n >= T.rl_min2 && T.rl_long2) {  // the lower tier
+        int slot = atomicAdd(T.rl_count2, 1);
+        if (slot < T.rl_nlmax2) { T.rl_long2[slot] = i; return; }
     }
     if (n > 0) {
         atomicAdd(&T.rhist[RL_NB - 1 - (n >> RL_SHIFT)], 1);
@@ -824,7 +827,8 @@ __global__ void k_rlist_fill(Blk B, Bat T, int mode) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= T.np) return;
     int n = refine_span(B, T, mode, i);
-    if (n >= T.rl_min && T.rl_long) return;     // listed by k_rlist_count
+    if ((n >= T.rl_min && T.rl_long) || (n >= T.rl_min2 && T.rl_long2))
+        return;                                  // listed by k_rlist_count
     if (n > 0) T.rlist[atomicAdd(&T.rhist[RL_NB - 1 - (n >> RL_SHIFT)], 1)] = i;
 }
 
@@ -1445,17 +1449,24 @@ static void launch_refine_long_fin(int mode, const Blk& B, const Bat& T, cudaStr
 }
 
 void launch_refine(int mode, const Blk& B, const Bat& T0, cudaStream_t st, bool few) {
-    // the long-pair path: from RL_LONG positions with RLW_CTAS CTAs where
-    // most pairs take part; where few do (the launches after the --pre-score
-    // filter) a launch lasts as long as its slowest pair, so pairs from
-    // RL_LONG_FEW positions get RLW_CTAS_FEW CTAs
+    // the long-pair path: from RL_LONG positions with RLW_CTAS CTAs; where
+    // few pairs take part (the launches after the --pre-score filter) a
+    // launch lasts as long as its slowest pair, so there the pairs from
+    // RL_LONG_FEW positions below that get RLW_CTAS_FEW CTAs (second tier)
     Bat T = T0;
-    T.rl_min = few ? RL_LONG_FEW : RL_LONG;
-    T.rlw_ctas = few ? RLW_CTAS_FEW : RLW_CTAS;
+    T.rl_min = RL_LONG;
+    T.rlw_ctas = RLW_CTAS;
+    T.rl_min2 = RL_LONG_FEW;
+    T.rlw_ctas2 = RLW_CTAS_FEW;
+    if (!few) T.rl_long2 = nullptr;
     cudaMemsetAsync(T.rhist, 0, (RL_NB + 1) * sizeof(int), st);
     if (T.rl_long) {
         cudaMemsetAsync(T.rl_count, 0, sizeof(int), st);
         cudaMemsetAsync(T.rl_next, 0, (size_t)T.rl_nlmax * sizeof(int), st);
+    }
+    if (T.rl_long2) {
+        cudaMemsetAsync(T.rl_count2, 0, sizeof(int), st);
+        cudaMemsetAsync(T.rl_next2, 0, (size_t)T.rl_nlmax2 * sizeof(int), st);
     }
     const int nb = (T.np + 255) / 256;
     k_rlist_count<<<nb, 256, 0, st>>>(B, T, mode);
@@ -1468,6 +1479,15 @@ void launch_refine(int mode, const Blk& B, const Bat& T0, cudaStream_t st, bool 
     if (T.rl_long) {
         launch_refine_k<32, true>(mode, B, T, st);
         launch_refine_long_fin(mode, B, T, st);
+        if (T.launches) (*T.launches) += 2;
+    }
+    if (T.rl_long2) {
+        // the second tier through the same kernels, on its own list
+        Bat T2 = T;
+        T2.rl_long = T.rl_long2; T2.rl_count = T.rl_count2; T2.rl_next = T.rl_next2;
+        T2.rl_cand = T.rl_cand2; T2.rl_nlmax = T.rl_nlmax2; T2.rlw_ctas = T.rlw_ctas2;
+        launch_refine_k<32, true>(mode, B, T2, st);
+        launch_refine_long_fin(mode, B, T2, st);
         if (T.launches) (*T.launches) += 2;
     }
 }

@@ -13,9 +13,9 @@ namespace gtb {
 // 16/R consecutive steps into one 32-bit word, words of a strip stored
 // [step / (16/R)][lane].
 // refinement: pairs with at least RL_LONG positions get RLW_CTAS CTAs of 4
-// warps; in the launches where few pairs take part, pairs with at least
-// RL_LONG_FEW positions get RLW_CTAS_FEW; a long-pair launch has at most
-// RLW_GRID CTAs (they walk the long pairs)
+// warps; in the launches where few pairs take part, the pairs below that
+// with at least RL_LONG_FEW positions get RLW_CTAS_FEW; a long-pair launch
+// has at most RLW_GRID CTAs (they walk the long pairs)
 constexpr int RL_LONG = 1536;
 constexpr int RL_LONG_FEW = 384;
 constexpr int RL_NBUCKET = 65536 >> 4;   // work-list buckets; rhist[RL_NBUCKET] = list length
@@ -104,12 +104,19 @@ struct Bat {
     unsigned long long* str_cnt;
     int *rlist, *rhist;              // refinement work list [np], buckets [4097]
     // long pairs of a refinement launch (null: none possible): list, count,
-    // per-pair variant counter, per-warp candidates; rl_nlmax = capacity
+    // per-pair variant counter, per-warp candidates; rl_nlmax = capacity;
+    // this launch's threshold and CTAs per long pair.  The second set (the
+    // same fields with 2) is a lower tier, pairs from rl_min2 positions with
+    // rlw_ctas2 CTAs each, used in the launches after the --pre-score filter
+    // (null rl_long2: no second tier in this launch)
     int rl_nlmax;
-    int rl_min, rlw_ctas;            // this launch's long-pair threshold and CTAs per long pair
+    int rl_min, rlw_ctas;
     int *rl_long, *rl_count, *rl_next;
-    int plog_round;                  // round of an RM_PLOG launch (0 .. PLOG_ROUNDS-1)
     float* rl_cand;
+    int rl_nlmax2, rl_min2, rlw_ctas2;
+    int *rl_long2, *rl_count2, *rl_next2;
+    float* rl_cand2;
+    int plog_round;                  // round of an RM_PLOG launch (0 .. PLOG_ROUNDS-1)
     // seed work items when some pair's offsets are split over several CTAs
     // (null: one CTA per pair): item -> pair, item -> chunk, chunks per pair,
     // per-pair packed (score, variant) maximum
