@@ -38,6 +38,10 @@ references.  Legs of one run:
   compiled for sm_100a from its sources by oracle/Makefile.refgpu) on the
   same B200, over the first query chunk x a sample of the references, timed
   by its "query batch execution time" (the GPU bar for this path).
+* clustering: the all-against-all clustering configuration at 1,000
+  structures (config4's generator): the set aligned against itself with the
+  clustering run's coverage prefilter, linked by gtb_cluster; the
+  reference's GPU build (--cls) on the same structures, wall clock both.
 
 Inputs (about 0.6 GB of coordinates and the pair state) are larger than L2
 between steps.  --impl reference times the reference's own CPU
@@ -91,8 +95,9 @@ def progress(msg: str) -> None:
 
 
 def lib_options(args, polish: int):
-    """The library's options of the run: --speed 9 (the command line's
-    default, detailed search on) or 13 (--no-detailed-search), -s 0.5."""
+    """The library's options of the run: a --speed preset 0..12 (9 is the
+    command line's default, the detailed search on), or 13: the defaults
+    with --no-detailed-search; -s 0.5."""
     from gtalign_alpha_b200.api import Options
     if args.speed == 13:
         return Options(polish_steps=polish)      # defaults with --no-detailed-search
@@ -456,11 +461,14 @@ def run_ours(args):
                          "dp_refine_loops": float(st_ms[2]), "final": float(st_ms[5]),
                          "total": float(st_ms[6])}}
 
-    long_chain = adjoint = cpu = refgpu = None
+    long_chain = adjoint = cpu = refgpu = clustering = None
     if rank == 0 and ws == 1:
         if "refgpu" in legs:
             progress("reference GPU build")
             refgpu = reference_gpu_sample(wl, args, value)
+        if "cluster" in legs:
+            progress("clustering run")
+            clustering = cluster_run(args)
         if "long" in legs:
             progress("long chains")
             long_chain = long_chain_run(gp, args)
@@ -504,6 +512,7 @@ def run_ours(args):
             "adjoint": adjoint,
             "cpu_baseline": cpu,
             "reference_gpu": refgpu,
+            "clustering": clustering,
             "clocks": clocks,
             "workload_gen_s": gen_s,
         }
@@ -770,12 +779,87 @@ def run_reference_sample(wl, nq: int, nref: int, threads: int, args):
     if args.speed != 13:
         from gtalign_alpha_b200.api import build_index
         ndx = dict(qndx=build_index(q), rndx=build_index(r))
-    pyoracle.process_block(q, r, pyoracle.opts_from(refinement=1, convergence=18, prescore=0.4,
-                                                    scorethld=0.5,
-                                                    nodetailedsearch=1 if args.speed == 13 else 0,
-                                                    trigger=(0, 20, 50)[(args.speed - 1) % 3]),
+    lo = lib_options(args, 0)
+    pyoracle.process_block(q, r, pyoracle.opts_from(refinement=lo.refinement, convergence=lo.convergence,
+                                                    prescore=lo.prescore, scorethld=0.5, depth=lo.depth,
+                                                    addsearchbyss=lo.addsearchbyss,
+                                                    nodetailedsearch=lo.nodetailedsearch,
+                                                    trigger=lo.trigger, nbranches=lo.nbranches),
                            nthreads=threads, **ndx)
     return nq * nref, time.time() - t, "port"
+
+
+def cluster_run(args):
+    """The all-against-all clustering configuration at a bounded size: the
+    set of config4 (args.cluster_n structures, log-normal lengths, 30% in
+    families of 10) aligned against itself in query blocks with the
+    clustering run's coverage prefilter, at --speed 13 as the reference
+    recommends for clustering, then linked (complete linkage, TM-score 0.5)
+    by gtb_cluster; and the reference's GPU build on the same structures
+    (--cls over the file list).  Times are wall clock of the whole run
+    (device work, transfers, linkage; for the reference also its reading)."""
+    from gtalign_alpha_b200 import synth
+    from gtalign_alpha_b200.api import GTalignB200, Options, cluster
+    wl = synth.config4(seed=4, n=args.cluster_n)
+    chains = wl.queries
+    n = len(chains)
+    allsoa = synth.pack(chains)
+    types = np.arange(n, dtype=np.int32)
+    rec = np.zeros((n, n, 16), np.float32)
+    qblock = 64
+    with GTalignB200(0, 0, Options.speed(13, clsfilter=1, clscoverage=0.7)) as g:
+        # warm-up on the first block (allocations, kernel load)
+        g.process_block(synth.pack(chains[:qblock]), allsoa, scorethld=0.5, alignments=False,
+                        numerr=False, qtypes=types[:qblock], rtypes=types)
+        t0 = time.perf_counter()
+        compared = 0
+        for q0 in range(0, n, qblock):
+            q1 = min(n, q0 + qblock)
+            res = g.process_block(synth.pack(chains[q0:q1]), allsoa, scorethld=0.5, alignments=False,
+                                  numerr=False, qtypes=types[q0:q1], rtypes=types)
+            rec[q0:q1] = res.alndata
+            compared += int((res.alndata[..., 4] > 0).sum())
+        t1 = time.perf_counter()
+    cl = cluster(rec, allsoa.lens, ids=[c.name for c in chains], linkage=0, threshold=0.5, coverage=0.7)
+    t2 = time.perf_counter()
+    ours = [frozenset(chains[k].name for k in c) for c in cl.clusters]
+    out = {"value": n * n / (t2 - t0), "unit": "candidate pairs/s",
+           "structures": n, "pairs_aligned": compared, "align_s": t1 - t0, "link_s": t2 - t1,
+           "clusters": len(ours),
+           "workload": "config4: %d structures, log-normal lengths (median 220), 30%% in families of 10; "
+                       "--speed 13, --cls-threshold 0.5, complete linkage, coverage 0.7" % n}
+    binp = os.path.join(ROOT, "oracle", "_ref", "gpu", "gtalign")
+    if not os.path.exists(binp):
+        out["reference_gpu"] = {"unavailable": "oracle/_ref/gpu/gtalign not built"}
+        return out
+    d = tempfile.mkdtemp(prefix="gtclsb")
+    try:
+        files = []
+        for c in chains:
+            files.append(os.path.join(d, c.name + ".pdb"))
+            synth.write_pdb(c, files[-1])
+        cmd = [binp, "--cls=" + ",".join(files), "-o", os.path.join(d, "o"), "--speed=13", "--dev-N=1",
+               "--cls-threshold=0.5", "--cls-algorithm=0"]
+        t = time.perf_counter()
+        p = subprocess.run(cmd, capture_output=True, timeout=args.refgpu_timeout)
+        wall = time.perf_counter() - t
+        if p.returncode != 0:
+            out["reference_gpu"] = {"unavailable": "reference --cls run failed (rc %d)" % p.returncode}
+            return out
+        text = open(os.path.join(d, "o", "gtalignclusters.lst")).read().splitlines()
+        last = max(k for k, ln in enumerate(text) if ln.startswith("===="))
+        ref = []
+        for ln in text[last + 1:]:
+            names = [w.split("_")[0] for w in ln.split() if w.startswith("s")]
+            if names:
+                ref.append(frozenset(names))
+        same = sum(len(c) for c in set(ours) & set(ref))
+        out["reference_gpu"] = {"wall_s": wall, "value": n * n / wall, "unit": "candidate pairs/s",
+                                "clusters": len(ref), "structures_in_identical_clusters": same,
+                                "ours_vs_reference_gpu": (n * n / (t2 - t0)) / (n * n / wall)}
+        return out
+    finally:
+        shutil.rmtree(d, ignore_errors=True)
 
 
 def reference_gpu_sample(wl, args, value):
@@ -913,8 +997,9 @@ def main():
     ap.add_argument("--nqueries", type=int, default=16)
     ap.add_argument("--qchunk", type=int, default=2, help="queries per step (the reference's --dev-queries-per-chunk)")
     ap.add_argument("--seed", type=int, default=2)
-    ap.add_argument("--speed", type=int, default=13, choices=[7, 8, 9, 10, 11, 12, 13],
-                    help="the command line's --speed preset (13: --no-detailed-search; 9: its default)")
+    ap.add_argument("--speed", type=int, default=13, choices=list(range(14)),
+                    help="the command line's --speed preset 0..12 (9: its default); 13: its "
+                         "defaults with --no-detailed-search")
     ap.add_argument("--cpu-sample-refs", type=int, default=2000)
     ap.add_argument("--polish-steps", type=int, default=5,
                     help="adjoint polishing steps of the headline (batched + adjoint) form")
@@ -926,8 +1011,10 @@ def main():
     ap.add_argument("--refgpu-refs", type=int, default=10000,
                     help="references in the reference GPU build's sample (x the first query chunk)")
     ap.add_argument("--refgpu-timeout", type=int, default=600)
-    ap.add_argument("--legs", default="unpolished,e2e,plain,long,adjoint,cpu,refgpu",
-                    help="legs besides the headline: unpolished,e2e,plain,long,adjoint,cpu,refgpu")
+    ap.add_argument("--cluster-n", type=int, default=1000,
+                    help="structures of the all-against-all clustering leg")
+    ap.add_argument("--legs", default="unpolished,e2e,plain,long,adjoint,cpu,refgpu,cluster",
+                    help="legs besides the headline: unpolished,e2e,plain,long,adjoint,cpu,refgpu,cluster")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

@@ -91,8 +91,9 @@ class Options:
         """The --speed presets (gtalign.cpp:833-867, gtalign.h:189-208):
         13 = --no-detailed-search --refinement=0 --convergence=2; 10..12 =
         --depth=3 with --trigger 0/20/50, --refinement=0 --convergence=2; 7..9
-        = --depth=2 with --trigger 0/20/50 (9 is the command line's default).
-        The presets at --depth 0 and 1 (0..6) are not available."""
+        = --depth=2 with --trigger 0/20/50 (9 is the command line's default);
+        4..6 = --depth=1 and 1..3 = --depth=0 with --trigger 0/20/50; 0 =
+        --depth=0 --trigger=0 --nbranches=16 --add-search-by-ss."""
         if level == 13:
             return cls(refinement=0, convergence=2, **kw)
         trig = {0: 0, 1: 20, 2: 50}
@@ -101,7 +102,13 @@ class Options:
                        convergence=2, **kw)
         if 7 <= level <= 9:
             return cls(nodetailedsearch=0, depth=2, trigger=trig[level - 7], **kw)
-        raise GTBError(4, "--speed %d (detailed search at --depth 0 or 1) is not available" % level)
+        if 4 <= level <= 6:
+            return cls(nodetailedsearch=0, depth=1, trigger=trig[level - 4], **kw)
+        if 1 <= level <= 3:
+            return cls(nodetailedsearch=0, depth=0, trigger=trig[level - 1], **kw)
+        if level == 0:
+            return cls(nodetailedsearch=0, depth=0, trigger=0, nbranches=16, addsearchbyss=1, **kw)
+        raise GTBError(1, "--speed %d out of 0..13" % level)
 
     def _c(self) -> _COptions:
         return _COptions(self.refinement, self.depth, self.convergence, self.prescore,

@@ -160,13 +160,6 @@ static gtb_status check_options(gtb_handle* h) {
             snprintf(h->err, sizeof(h->err), "detailed-search option out of range");
             return GTB_ERR_ARG;
         }
-        if (o.depth < 2) {
-            // --depth deep/high add the secondary configuration sections
-            // (MpStageFrg3.cpp:196-215, 249-266), not built here
-            snprintf(h->err, sizeof(h->err),
-                     "the detailed search at --depth 0 or 1 is not implemented (use 2 or 3)");
-            return GTB_ERR_UNSUPPORTED;
-        }
     }
     if (o.refinement < GTB_REFINEMENT_LOG || o.refinement > GTB_REFINEMENT_FULLA) {
         snprintf(h->err, sizeof(h->err), "--refinement %d out of -1..3", o.refinement);
@@ -223,7 +216,8 @@ static size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 // score matrix, slots and branches).
 static size_t pair_bytes(int lq, int lr, bool strings, bool f3 = false) {
     size_t b = (size_t)gtb::bt_words(lq, lr) * 4;     // traceback words
-    if (f3) b += (size_t)gtb::f3_region_bytes(lq, lr) + (size_t)F3_NTOP * 14 * 4 + (size_t)F3_NBMAX * 13 * 4 + 13 * 4 + 8;
+    if (f3) b += (size_t)gtb::f3_region_bytes(lq, lr, F3_NSEC) + (size_t)F3_NSEC * (F3_NTOP * 14 * 4 + F3_NBMAX * 13 * 4) +
+                 13 * 4 + 8 + F3_NSEC * 4;
     b += (size_t)lr * 4;                               // DP row buffer
     b += (size_t)std::min(lq, lr) * 28;                // aligned pairs + coordinates
     if (strings) b += (size_t)5 * (lq + lr + 1);       // alignment rows
@@ -301,6 +295,8 @@ static gtb_status run_block(gtb_handle* h, const DevBlock& D, float scorethld,
         }
         B.qnd = D.qnd; B.qnc = D.qnc; B.rnd = D.rnd; B.rnc = D.rnc;
         B.f3trigger = o.trigger; B.f3nbranches = o.nbranches;
+        // configuration sections (MpStageFrg3.cpp:204-212, 403-404)
+        B.f3nsec = o.depth <= 0 ? 3 : (o.depth <= 1 ? 2 : 1);
         B.f3gapcost = o.gapcost == 0 ? -0.8f : (o.gapcost == 1 ? -1.2f : -3.0f);
         B.f3seedrule = o.seedrule == 0 ? 0 : (o.seedrule == 1 ? 64 : 128);
         B.f3window = o.window;
@@ -351,7 +347,7 @@ static gtb_status run_block(gtb_handle* h, const DevBlock& D, float scorethld,
             off_row[i + 1] = off_row[i] + lr;
             off_aln[i + 1] = off_aln[i] + std::min(lq, lr);
             off_str[i + 1] = off_str[i] + (strings ? 5LL * (lq + lr + 1) : 0);
-            if (off_lsm) off_lsm[i + 1] = off_lsm[i] + gtb::f3_region_bytes(lq, lr);
+            if (off_lsm) off_lsm[i + 1] = off_lsm[i] + gtb::f3_region_bytes(lq, lr, B.f3nsec);
             int n1, silo, sihi, prv;
             gtb::seed_range(lq, lr, B.qmax, B.qmin, B.rmax, B.rmin, B.stepinit, n1, silo, sihi, prv);
             int cnt = sihi - silo + 1;
@@ -435,19 +431,20 @@ static gtb_status run_block(gtb_handle* h, const DevBlock& D, float scorethld,
         size_t o_dw = nl ? carve(dwv.size() * sizeof(int)) : 0;
         size_t o_dws = nl ? carve((size_t)nl * sizeof(long long)) : 0;
         size_t o_dwp = nl ? carve((size_t)dnprog * sizeof(int)) : 0;
-        size_t o_dwe = nl ? carve(sizeof(int)) : 0;
+        size_t o_dwe = carve(sizeof(int));      // wavefront error flag (multi-CTA and CTA waves)
         size_t o_rll = nlmax ? carve((size_t)(2 * nlmax + 1) * sizeof(int)) : 0;
         size_t o_rlc = nlmax ? carve((size_t)nlmax * gtb::RLW_WARPS * gtb::RLW_CAND * sizeof(float)) : 0;
         size_t o_rll2 = nlmax2 ? carve((size_t)(2 * nlmax2 + 1) * sizeof(int)) : 0;
         size_t o_rlc2 = nlmax2 ? carve((size_t)nlmax2 * gtb::RLW_WARPS * gtb::RLW_CAND * sizeof(float)) : 0;
         // detailed search: local score matrices, slots, DP scores, branches
         size_t o_lsm = B.f3 ? carve((size_t)std::max<long long>(off_lsm[np], 1)) : 0;
-        size_t o_f3s = B.f3 ? carve((size_t)np * F3_NTOP * 13 * sizeof(float)) : 0;
-        size_t o_f3d = B.f3 ? carve((size_t)np * F3_NTOP * sizeof(float)) : 0;
-        size_t o_f3a = B.f3 ? carve((size_t)np * F3_NBMAX * 12 * sizeof(float)) : 0;
-        size_t o_f3o = B.f3 ? carve((size_t)np * F3_NBMAX) : 0;
+        const size_t nsl = (size_t)B.f3nsec * F3_NTOP, nbr = (size_t)B.f3nsec * F3_NBMAX;
+        size_t o_f3s = B.f3 ? carve((size_t)np * nsl * 13 * sizeof(float)) : 0;
+        size_t o_f3d = B.f3 ? carve((size_t)np * nsl * sizeof(float)) : 0;
+        size_t o_f3a = B.f3 ? carve((size_t)np * nbr * 12 * sizeof(float)) : 0;
+        size_t o_f3o = B.f3 ? carve((size_t)np * nbr) : 0;
         size_t o_f32 = B.f3 ? carve((size_t)np * 13 * sizeof(float)) : 0;
-        size_t o_f3v = B.f3 ? carve((size_t)np * sizeof(unsigned)) : 0;
+        size_t o_f3v = B.f3 ? carve((size_t)np * F3_NSEC * sizeof(unsigned)) : 0;
         char* base = nullptr;
         CK(cudaMallocAsync((void**)&base, sz, st));
         Bat T{};
@@ -482,6 +479,7 @@ static gtb_status run_block(gtb_handle* h, const DevBlock& D, float scorethld,
             T.tfm_2nd = (float*)(base + o_f32);
             T.best2 = T.tfm_2nd + (size_t)np * 12;
             T.vskip_mask = (unsigned*)(base + o_f3v);
+            T.f3br = (int)nbr;
         }
         T.work = h->d_work;
         T.kt = h->ktime ? &h->kt : nullptr;
@@ -500,7 +498,10 @@ static gtb_status run_block(gtb_handle* h, const DevBlock& D, float scorethld,
             T.rl_cand2 = (float*)(base + o_rlc2);
         }
         T.ndw = 0; T.dw_nprog = 0; T.dw_item = T.dw_pair = T.dw_G = nullptr; T.dw_soff = nullptr;
-        T.dw_mark = nullptr; T.dw_prog = nullptr; T.dw_err = nullptr;
+        T.dw_mark = nullptr; T.dw_prog = nullptr;
+        T.dw_err = (int*)(base + o_dwe);
+        T.dp_kc = gtb::DP_CTA_PAIRS;
+        CK(cudaMemsetAsync(T.dw_err, 0, sizeof(int), st));
         h->h_flag[evset] = 0;
         if (nl) {
             int* dw = (int*)(base + o_dw);
@@ -509,11 +510,9 @@ static gtb_status run_block(gtb_handle* h, const DevBlock& D, float scorethld,
             T.dw_mark = (const unsigned char*)(dw + 2 * nitw + 2 * nl);
             T.dw_soff = (const long long*)(base + o_dws);
             T.dw_prog = (int*)(base + o_dwp);
-            T.dw_err = (int*)(base + o_dwe);
             CK(cudaMemcpyAsync(dw, dwv.data(), dwv.size() * sizeof(int), cudaMemcpyHostToDevice, st));
             CK(cudaMemcpyAsync(base + o_dws, dwsv[j].data(), (size_t)nl * sizeof(long long),
                                cudaMemcpyHostToDevice, st));
-            CK(cudaMemsetAsync(T.dw_err, 0, sizeof(int), st));
         }
         CK(cudaMemcpyAsync(offs, off_bt, (B.f3 ? 5 : 4) * (size_t)(np + 1) * sizeof(long long),
                            cudaMemcpyHostToDevice, st));
@@ -535,7 +534,7 @@ static gtb_status run_block(gtb_handle* h, const DevBlock& D, float scorethld,
             CK(cudaMemcpyAsync(h_tfm + q0 * 12, T.tfm_gr, (size_t)np * 12 * sizeof(float), cudaMemcpyDefault, st));
         if (h_err)
             CK(cudaMemcpyAsync(h_err + q0 * 4, T.err, (size_t)np * 4 * sizeof(float), cudaMemcpyDefault, st));
-        if (nl) CK(cudaMemcpyAsync(h->h_flag + evset, T.dw_err, sizeof(int), cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(h->h_flag + evset, T.dw_err, sizeof(int), cudaMemcpyDeviceToHost, st));
         if (strings) {
             // read after the batch: only the bytes the rows took
             strbat.push_back({base, q0, np, T.str_off, T.str_cnt, T.str});

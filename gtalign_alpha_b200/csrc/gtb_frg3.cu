@@ -36,6 +36,7 @@ constexpr int F3_HASH = 512;        // CUSF_TBSP_INDEX_SCORE_POSLIMIT2
 constexpr int F3_SIMROWS = 96;      // MPSF_TBSP_LOCAL_SIMILARITY_YDIM x 3
 constexpr int F3_SIMCOLS = 128;     // MPSF_TBSP_LOCAL_SIMILARITY_XDIM
 constexpr int F3_MAXSTACK = 17;
+constexpr int F3_LENTHR = 150;      // MpStageFrg3.cpp:48: longer structures thin the sections
 constexpr float F3_SSDST2 = 64.f;   // an SS-matched neighbour farther than 8 A is none
 constexpr int F3_MAXWIN = 512;      // the largest --window
 constexpr int F3_WARPS = 4;         // warps per CTA of the search
@@ -459,8 +460,9 @@ __global__ void __launch_bounds__(F3_WARPS * 32, 3) k_f3_search(Blk B, Bat T, in
     unsigned short* sn = s_stkn[w] + lane;
     float* sd = s_stkd[w] + lane;
     unsigned char* sm = s_stkm[w] + lane;
-    float* slots = T.f3slot + (long long)i * F3_NTOP * 13;
-    for (int k = threadIdx.x; k < F3_NTOP; k += blockDim.x) slots[k * 13] = 0.f;
+    const int nsec = B.f3nsec;
+    float* slots = T.f3slot + (long long)i * nsec * F3_NTOP * 13;
+    for (int k = threadIdx.x; k < nsec * F3_NTOP; k += blockDim.x) slots[k * 13] = 0.f;
     const float thr = __fdiv_rn((float)B.f3trigger, 100.0f);
     const int seedrule = B.f3seedrule;
     const int qstep = f3_step(depth, lq), rstep = f3_step(depth, lr);
@@ -478,18 +480,33 @@ __global__ void __launch_bounds__(F3_WARPS * 32, 3) k_f3_search(Blk B, Bat T, in
         // the round's results in configuration order
         __syncthreads();
         if (threadIdx.x == 0) {
-            for (int rr = 0; rr < F3_ROUND; rr++)
+            for (int rr = 0; rr < F3_ROUND; rr++) {
+                // the sections this configuration feeds: section 0 all; at
+                // --depth 1 and 0 sections 1 and 2 those on every second /
+                // third grid row and column of a structure longer than
+                // F3_LENTHR (sec2met, sec3met: MpStageFrg3.cpp:204-212)
+                const int cc = c0 + rr, ys = cc / nsx, xs = cc % nsx;
+                const bool sec1 = nsec > 1 && (lq <= F3_LENTHR || (ys & 1) == 0) &&
+                                  (lr <= F3_LENTHR || (xs & 1) == 0);
+                const bool sec2 = nsec > 2 && (lq <= F3_LENTHR || ys % 3 == 0) &&
+                                  (lr <= F3_LENTHR || xs % 3 == 0);
                 for (int fi = 0; fi < 2; fi++) {
                     if (!s_got[rr * 2 + fi]) continue;
                     const int k = nscored % F3_NTOP;
                     nscored++;
                     const float* res = s_res + (rr * 2 + fi) * 13;
                     const float sc = res[0];
-                    if (0.0f < sc && slots[k * 13] < sc) {
-                        slots[k * 13] = sc;
-                        for (int f = 0; f < 12; f++) slots[k * 13 + 1 + f] = res[1 + f];
+                    if (!(0.0f < sc)) continue;
+                    for (int sec = 0; sec < nsec; sec++) {
+                        if ((sec == 1 && !sec1) || (sec == 2 && !sec2)) continue;
+                        float* sl = slots + (sec * F3_NTOP + k) * 13;
+                        if (sl[0] < sc) {
+                            sl[0] = sc;
+                            for (int f = 0; f < 12; f++) sl[1 + f] = res[1 + f];
+                        }
                     }
                 }
+            }
         }
         __syncthreads();
         continue;
@@ -546,38 +563,45 @@ __global__ void __launch_bounds__(F3_WARPS * 32, 3) k_f3_search(Blk B, Bat T, in
 }
 
 // ---------------------------------------------------------------------------
-// 3. The slots by DP score (SortBestDPscoresAndTMsAmongDPswifts,
+// 3. Per section, the slots by DP score (SortBestDPscoresAndTMsAmongDPswifts,
 // MpStageFrg3.h:1150-1250), larger first, lower slot first on ties: the
-// pair's flag becomes the first slot's (SCOREDP when no slot scored), the
-// first --nbranches are the branches, and the next DP refinement skips the
-// refinement variants 1..31 whose rank holds no score.  A thread per pair.
+// pair's flag becomes section 0's first slot's (SCOREDP when no slot scored),
+// the first --nbranches of each section are its branches (branch index =
+// section * nbranches + rank), and the next DP refinement skips refinement
+// variant section * 32 + rank when that rank holds no score (section 0's
+// rank 0 being the pair's flag).  A thread per pair.
 __global__ void k_f3_select(Blk B, Bat T, int nbranches) {
     const int slot = blockIdx.x * blockDim.x + threadIdx.x;
     if (slot >= T.rhist[RL_NBUCKET]) return;
     const int i = T.rlist[slot];
-    const float* dps = T.f3dps + (long long)i * F3_NTOP;
-    float d[F3_NTOP];
-    int order[F3_NTOP];
-    for (int k = 0; k < F3_NTOP; k++) { d[k] = dps[k]; order[k] = k; }
-    for (int a = 1; a < F3_NTOP; a++) {
-        const int k = order[a];
-        int b = a - 1;
-        while (b >= 0 && d[order[b]] < d[k]) { order[b + 1] = order[b]; b--; }
-        order[b + 1] = k;
-    }
-    unsigned vs = 0u;
-    for (int r = 1; r < F3_NTOP; r++)
-        if (!(0.0f < d[order[r]])) vs |= 1u << r;
-    T.vskip_mask[i] = vs;
-    T.flags[i] = 0.0f < d[order[0]] ? 0 : CONV_SCOREDP;
-    for (int r = 0; r < nbranches; r++) {
-        const int k = order[r];
-        const bool ok = 0.0f < d[k];
-        T.f3ok[(long long)i * F3_NBMAX + r] = ok ? 1 : 0;
-        if (ok) {
-            const float* src = T.f3slot + ((long long)i * F3_NTOP + k) * 13 + 1;
-            float* dst = T.f3alt + ((long long)i * F3_NBMAX + r) * 12;
-            for (int f = 0; f < 12; f++) dst[f] = src[f];
+    const int nsec = B.f3nsec;
+    for (int sec = 0; sec < F3_NSEC; sec++) {
+        if (sec >= nsec) { T.vskip_mask[(long long)i * F3_NSEC + sec] = 0u; continue; }
+        const float* dps = T.f3dps + ((long long)i * nsec + sec) * F3_NTOP;
+        float d[F3_NTOP];
+        int order[F3_NTOP];
+        for (int k = 0; k < F3_NTOP; k++) { d[k] = dps[k]; order[k] = k; }
+        for (int a = 1; a < F3_NTOP; a++) {
+            const int k = order[a];
+            int b = a - 1;
+            while (b >= 0 && d[order[b]] < d[k]) { order[b + 1] = order[b]; b--; }
+            order[b + 1] = k;
+        }
+        unsigned vs = 0u;
+        for (int r = sec == 0 ? 1 : 0; r < F3_NTOP; r++)
+            if (!(0.0f < d[order[r]])) vs |= 1u << r;
+        T.vskip_mask[(long long)i * F3_NSEC + sec] = vs;
+        if (sec == 0) T.flags[i] = 0.0f < d[order[0]] ? 0 : CONV_SCOREDP;
+        for (int r = 0; r < nbranches; r++) {
+            const int k = order[r];
+            const bool ok = 0.0f < d[k];
+            const long long br = (long long)i * T.f3br + sec * nbranches + r;
+            T.f3ok[br] = ok ? 1 : 0;
+            if (ok) {
+                const float* src = T.f3slot + (((long long)i * nsec + sec) * F3_NTOP + k) * 13 + 1;
+                float* dst = T.f3alt + br * 12;
+                for (int f = 0; f < 12; f++) dst[f] = src[f];
+            }
         }
     }
 }
@@ -622,8 +646,11 @@ void launch_frg3(const Blk& B, const Bat& T, cudaStream_t st) {
         k_f3_select<<<(T.np + 255) / 256, 256, 0, st>>>(B, T, nbr);
         if (T.launches) (*T.launches)++;
     }
-    // the branches (Refine_tfmaltconfig, MpStageFrg3.cpp:425-467)
-    for (int rci = 0; rci < nbr; rci++) {
+    // the branches, section by section (Refine_tfmaltconfig,
+    // MpStageFrg3.cpp:425-467); at --depth 1 and 0 each branch's refinement
+    // is followed by a DP under its iteration-best transform and a
+    // refinement of that alignment (MpStageFrg3.cpp:452-466)
+    for (int rci = 0; rci < B.f3nsec * nbr; rci++) {
         Bat TA = T;
         TA.alt_rci = rci;
         launch_dp(B, TA, DP_TFM_ALT, 1, 0.0f, 0, 0, 0, st);
@@ -632,6 +659,14 @@ void launch_frg3(const Blk& B, const Bat& T, cudaStream_t st) {
         plist();
         k_f3_second<<<(T.np + 255) / 256, 256, 0, st>>>(B, T, rci);
         if (T.launches) (*T.launches)++;
+        if (B.depth <= 1) {
+            launch_dp(B, T, DP_TFM_IBEST, 1, 0.0f, 0, 0, 0, st);
+            launch_btck(B, T, 0, st);
+            launch_refine(RM_DP, B, T, st, true);
+            plist();
+            k_f3_second<<<(T.np + 255) / 256, 256, 0, st>>>(B, T, rci);
+            if (T.launches) (*T.launches)++;
+        }
     }
     // DP refinement from the best branch, with a gap cost (its refinements
     // skipping the variants the slots rule out) and without

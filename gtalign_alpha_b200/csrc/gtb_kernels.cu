@@ -94,13 +94,13 @@ __device__ __forceinline__ void work_add(const Bat& T, int kind, unsigned long l
 // the transform a DP of pair i uses (DpTfm)
 __device__ __forceinline__ const float* dp_tfm(const Bat& T, int i, int tfmsrc) {
     if (tfmsrc == DP_TFM_GRAND) return T.tfm_gr + i * 12;
-    if (tfmsrc == DP_TFM_ALT) return T.f3alt + ((long long)i * F3_NBMAX + T.alt_rci) * 12;
+    if (tfmsrc == DP_TFM_ALT) return T.f3alt + ((long long)i * T.f3br + T.alt_rci) * 12;
     if (tfmsrc == DP_TFM_2ND) return T.tfm_2nd + i * 12;
     return T.tfm_ib + i * 12;
 }
 // the detailed search's branch T.alt_rci of pair i is empty
 __device__ __forceinline__ bool alt_empty(const Bat& T, int i) {
-    return T.f3ok && T.alt_rci >= 0 && !T.f3ok[(long long)i * F3_NBMAX + T.alt_rci];
+    return T.f3ok && T.alt_rci >= 0 && !T.f3ok[(long long)i * T.f3br + T.alt_rci];
 }
 
 __device__ __forceinline__ int pair_qi(const Blk& B, const Bat& T, int i) {
@@ -1211,7 +1211,8 @@ __device__ __forceinline__ void refine_slot(const Blk& B, const Bat& T, int slot
                 if (kv < V.total) {
                     int fl, kf;
                     variants_get(V, vk, n, kv, si, vndx, vpos, fl, kf);
-                    if (MODE == RM_DP && T.vskip && si < 32 && ((T.vskip[i] >> si) & 1u)) {
+                    if (MODE == RM_DP && T.vskip && si < 32 * F3_NSEC &&
+                        ((T.vskip[(long long)i * F3_NSEC + (si >> 5)] >> (si & 31)) & 1u)) {
                         need = true;       // a variant the detailed search's slots rule out
                     } else {
                         kind = PK_FRAG; k0 = kf; k1 = kf + fl;
@@ -1644,12 +1645,22 @@ __device__ __forceinline__ bool dp_pair(const float* t, float d02, float gcost, 
     return true;
 }
 
+// The DP work list (k_dlist_*, largest matrices first): its first dp_kc
+// pairs take a CTA each, whose 4 warps run the pair's strips as a wavefront
+// (strip s on warp s mod 4, each strip waiting with a bounded spin until the
+// previous one has published the row values it reads, the counters in
+// shared memory); the other pairs take a warp each.
 template <int GAP0, int SC>
 __global__ void __launch_bounds__(128) k_dp(Blk B, Bat T, int tfmsrc, float gcost, int dpscan,
                                             int skipmode) {
-    const int lane = threadIdx.x & 31;
-    const int slot = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-    if (slot >= T.rhist[RL_NB]) return;            // the DP work list (k_dlist_*)
+    __shared__ int s_prog[DP_CTA_MAXSTRIPS];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int len = T.rhist[RL_NB];
+    const int dkc = T.dw_err ? T.dp_kc : 0;
+    const int kc = dkc < len ? dkc : len;
+    const bool cta = (int)blockIdx.x < kc;
+    const int slot = cta ? (int)blockIdx.x : kc + ((int)blockIdx.x - kc) * (blockDim.x >> 5) + w;
+    if (slot >= len) return;                       // never for a CTA of the first kind
     const int i = T.rlist[slot];
     int qi = pair_qi(B, T, i), ri = pair_ri(B, T, i);
     int lq = B.qlen[qi], lr = B.rlen[ri];
@@ -1672,7 +1683,23 @@ __global__ void __launch_bounds__(128) k_dp(Blk B, Bat T, int tfmsrc, float gcos
     unsigned* bt = T.bt + T.off_bt[i];
     const unsigned char* qa = B.qa + B.qoff[qi];
     const unsigned char* ra = B.ra + B.roff[ri];
-    if (lane == 0) work_add(T, WK_DPCELL, (unsigned long long)lq * (unsigned long long)lr);
+    if (cta) {
+        if (lane == 0 && w == 0) work_add(T, WK_DPCELL, (unsigned long long)lq * (unsigned long long)lr);
+        if (dp_strips(lq) > 1) {
+            for (int k = threadIdx.x; k < DP_CTA_MAXSTRIPS; k += blockDim.x) s_prog[k] = 0;
+            __syncthreads();
+            if (dp_r(lq) == 4)
+                dp_pair<4, GAP0 != 0, SC, true>(t, d02, gcost, lq, lr, qx, qy, qz, r4, qs, rs, qa, ra, row,
+                                                bt, lane, w, blockDim.x >> 5, s_prog, T.dw_err, T.dw_spin);
+            else
+                dp_pair<2, GAP0 != 0, SC, true>(t, d02, gcost, lq, lr, qx, qy, qz, r4, qs, rs, qa, ra, row,
+                                                bt, lane, w, blockDim.x >> 5, s_prog, T.dw_err, T.dw_spin);
+            return;
+        }
+        if (w != 0) return;                        // one strip: one warp
+    } else if (lane == 0) {
+        work_add(T, WK_DPCELL, (unsigned long long)lq * (unsigned long long)lr);
+    }
     if (dp_r(lq) == 4)
         dp_pair<4, GAP0 != 0, SC, false>(t, d02, gcost, lq, lr, qx, qy, qz, r4, qs, rs, qa, ra, row, bt, lane);
     else
@@ -1769,7 +1796,8 @@ void launch_dp(const Blk& B, const Bat& T, int tfmsrc, int gap0, float gcost, in
         else launch_dp_wave<1, DP_SC_TFMSS>(B, T, tfmsrc, gcost, dpscan, skipmode, st);
         GTB_LAUNCHED(T);
     }
-    const int nb = (T.np + 3) / 4;
+    // dp_kc CTAs for the largest listed pairs, then a warp per pair
+    const int nb = (T.dw_err ? T.dp_kc : 0) + (T.np + 3) / 4;
     if (usess == DP_SC_SSRR) k_dp<0, DP_SC_SSRR><<<nb, 128, 0, st>>>(B, T, tfmsrc, gcost, dpscan, skipmode);
     else if (gap0 && !usess) k_dp<1, DP_SC_TFM><<<nb, 128, 0, st>>>(B, T, tfmsrc, gcost, dpscan, skipmode);
     else if (!gap0 && !usess) k_dp<0, DP_SC_TFM><<<nb, 128, 0, st>>>(B, T, tfmsrc, gcost, dpscan, skipmode);
@@ -1796,14 +1824,15 @@ void launch_pair_list(const Blk& B, const Bat& T, int skipmask, cudaStream_t st)
 // detailed-search region (the local score matrix is no longer read).
 __global__ void __launch_bounds__(128) k_f3_dpscore(Blk B, Bat T) {
     const int lane = threadIdx.x & 31;
-    const long long nitems = (long long)T.rhist[RL_NB] * F3_NTOP;
+    const int nsl = B.f3nsec * F3_NTOP;          // slots per pair
+    const long long nitems = (long long)T.rhist[RL_NB] * nsl;
     const long long wstride = (long long)gridDim.x * (blockDim.x >> 5);
     for (long long it = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); it < nitems;
          it += wstride) {
-        const int i = T.rlist[it / F3_NTOP];
-        const int k = (int)(it % F3_NTOP);
-        const float* sl = T.f3slot + ((long long)i * F3_NTOP + k) * 13;
-        float* fin = T.f3dps + (long long)i * F3_NTOP + k;
+        const int i = T.rlist[it / nsl];
+        const int k = (int)(it % nsl);
+        const float* sl = T.f3slot + ((long long)i * nsl + k) * 13;
+        float* fin = T.f3dps + (long long)i * nsl + k;
         if (!(0.f < sl[0])) {
             if (lane == 0) *fin = 0.f;
             continue;
@@ -1839,7 +1868,7 @@ void launch_f3_dpscore(const Blk& B, const Bat& T, cudaStream_t st) {
     int dev = 0, nsm = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-    const long long need = ((long long)T.np * F3_NTOP + 3) / 4;
+    const long long need = ((long long)T.np * B.f3nsec * F3_NTOP + 3) / 4;
     const int ng = (int)std::min<long long>(need, (long long)nsm * 8);
     k_f3_dpscore<<<ng > 0 ? ng : 1, 128, 0, st>>>(B, T);
     GTB_LAUNCHED(T);

@@ -28,11 +28,11 @@ constexpr int RLW_CAND = 17;         // floats per warp candidate
 constexpr int DP_R4_MIN = 384;
 __host__ __device__ inline int dp_r(int lq) { return lq >= DP_R4_MIN ? 4 : 2; }
 // bytes of a pair's detailed-search region: its local score matrix (lq x lr
-// bytes), later the 32 slot DPs' row buffers (32 x lr floats, which the DP
-// writes for every strip); a multiple of 16
-__host__ __device__ inline long long f3_region_bytes(int lq, int lr) {
+// bytes), later the slot DPs' row buffers (32 per section, lr floats each,
+// which the DP writes for every strip); a multiple of 16
+__host__ __device__ inline long long f3_region_bytes(int lq, int lr, int nsec) {
     long long b = (long long)lq * lr;
-    if (b < 128LL * lr) b = 128LL * lr;
+    if (b < 128LL * nsec * lr) b = 128LL * nsec * lr;
     return (b + 15) & ~15LL;
 }
 __host__ __device__ inline long long bt_strip_words(int lr, int R) {
@@ -67,7 +67,7 @@ struct Blk {
     // the spatial-index detailed search (f3 = 1: on): the structures' index
     // trees, packed per node (launch_pack_nodes) at the residue offsets of
     // the coordinates, and its options
-    int f3;
+    int f3, f3nsec;                  // f3nsec: configuration sections (1..F3_NSEC)
     const float4 *qnd, *rnd;
     const int2 *qnc, *rnc;
     int f3trigger, f3nbranches, f3seedrule, f3window;
@@ -80,9 +80,11 @@ struct Blk {
     float clscov;
 };
 
-// detailed search: fragment slots, branches per pair at most
+// detailed search: fragment slots per configuration section, branches per
+// section at most, sections at most (--depth 0: 3, 1: 2, else 1)
 constexpr int F3_NTOP = 32;
 constexpr int F3_NBMAX = 16;
+constexpr int F3_NSEC = 3;
 
 // Batch of consecutive pairs p0 .. p0+np-1 of a block (pair = qi*nr + ri).
 struct Bat {
@@ -133,6 +135,9 @@ struct Bat {
     const unsigned char* dw_mark;
     int *dw_prog, *dw_err;
     long long dw_spin;               // spins a wavefront wait makes before it gives up
+    // the first dp_kc pairs of a DP work list (the largest matrices) run as a
+    // wavefront over the 4 warps of a CTA each (0: none; needs dw_err)
+    int dp_kc;
     long long* launches;             // host counter of kernel launches
     cudaError_t* lerr;               // host: first failed launch (null: not recorded)
     struct KTimer* kt;               // host: per-family launch timer (null: off)
@@ -140,16 +145,18 @@ struct Bat {
     // (WorkKind), summed on the host
     unsigned long long* work;
     // detailed search (null when off): per pair the local score matrix
-    // (lq x lr bytes, row major, at off_lsm[i]); the 32 fragment slots'
-    // score and transform ([np][32][13]); their DP scores ([np][32]); the
-    // branches' transforms and validity ([np][F3_NBMAX][12], [np][F3_NBMAX]);
-    // the best branch's transform and score; the refinement variants (1..31)
-    // the next DP refinement skips
+    // (lq x lr bytes, row major, at off_lsm[i]); the fragment slots' score
+    // and transform, 32 per section ([np][f3nsec * 32][13]); their DP scores
+    // ([np][f3nsec * 32]); the branches' transforms and validity, f3br =
+    // f3nsec * F3_NBMAX per pair ([np][f3br][12], [np][f3br]); the best
+    // branch's transform and score; the refinement variants (1..95, three
+    // words per pair) the next DP refinement skips
     const long long* off_lsm;
     unsigned char* lsm;
     float *f3slot, *f3dps, *f3alt, *tfm_2nd, *best2;
     unsigned char* f3ok;
     unsigned* vskip_mask;
+    int f3br;
     int alt_rci;                     // DP/traceback of branch alt_rci (-1: none)
     const unsigned* vskip;           // refinement variant skips in force (null: none)
 };
@@ -181,6 +188,8 @@ struct KtScope {                      // begin/end around one launch helper
 };
 constexpr int WORK_SLOTS = 64;       // spread over addresses: fewer atomic collisions
 constexpr long long DP_WAVE_SPIN_DEFAULT = 1LL << 24;
+constexpr int DP_CTA_PAIRS = 592;    // dp_kc of the library's runs: 4 CTAs per SM
+constexpr int DP_CTA_MAXSTRIPS = 512;   // strips of a 65,535-residue query at 4 rows per lane
 
 // DP cell scores (launch_dp's usess): TM term under a transform, + SS, or the
 // --add-search-by-ss score (SS + Gonnet, no transform)

@@ -349,6 +349,36 @@ def config1(seed: int = 2, n_queries: int = 16, n_refs: int = 200_000,
     return Workload(queries, refs, seed, f"config1 seed={seed}", hom)
 
 
+def config4(seed: int = 4, n: int = 20_000, family_frac: float = 0.3,
+            family_size: int = 10) -> Workload:
+    """The all-against-all clustering set: ``n`` structures, log-normal
+    lengths (median 220, sigma_log 0.6) clipped to 40..1,200; ``family_frac``
+    of them in families of ``family_size`` (a random chain and noisy copies,
+    sigma 0.5-3 A, <=10% indels), placed at random positions; names
+    s0000000.. in list order.  The structures are returned as ``queries``
+    (a clustering run aligns the set against itself)."""
+    rng = np.random.default_rng(seed)
+    lens = np.clip(np.round(rng.lognormal(math.log(220.0), 0.6, size=n)), 40, 1200).astype(int)
+    chains = random_chains(rng, lens, "s")
+    nfam = int(family_frac * n) // family_size
+    pos = rng.permutation(n)
+    hom = [-1] * n
+    k = 0
+    for f in range(nfam):
+        base = chains[int(pos[k])]
+        hom[int(pos[k])] = f
+        k += 1
+        for _ in range(family_size - 1):
+            ri = int(pos[k])
+            chains[ri] = homolog(rng, base, float(rng.uniform(0.5, 3.0)),
+                                 float(rng.uniform(0.0, 0.10)), "s")
+            hom[ri] = f
+            k += 1
+    for i, c in enumerate(chains):
+        c.name = "s%07d" % i
+    return Workload(chains, [], seed, f"config4 seed={seed} n={n}", hom)
+
+
 def _rot_small(rng: np.random.Generator, max_deg: float) -> np.ndarray:
     """Rotation by a uniform angle in [0, max_deg] about a random axis."""
     ax = rng.normal(size=3)

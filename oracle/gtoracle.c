@@ -406,12 +406,13 @@ typedef struct {
     float err[GTO_NERR];
     float d0, d02, d82, d0fin, d0s;
     /* detailed search: the structures' index trees, the best transform among
-     * its refined branches, and the refinement variants (1..31) the first DP
-     * refinement after it skips (the fragment slots its sorting left empty) */
+     * its refined branches, and the refinement variants (1..95: the three
+     * sections' slots) the first DP refinement after it skips (the fragment
+     * slots its sorting left without a DP score) */
     const float *qnx, *qny, *qnz, *rnx, *rny, *rnz;
     const int *qnl, *qnr, *qno, *rnl, *rnr, *rno;
     float tfm_2nd[12];
-    unsigned vskip;
+    unsigned vskip[3];
 } pairctx;
 
 static void tfm_identity(float* t) { memset(t, 0, 12 * sizeof(float)); t[0] = t[4] = t[8] = 1.f; }
@@ -606,7 +607,7 @@ static void refine_stage(pairctx* P, int dpmode, float d0, float d02, int chk,
     float wbest = 0.f, wtfm[12];
     int wsi = -1, wndx = 0, wpos = 0;
     for (int si = 0; si < nloc && nrange > 0; si++) {
-        if (dpmode == 1 && si < 32 && ((P->vskip >> si) & 1u)) continue;
+        if (dpmode == 1 && si < 96 && ((P->vskip[si >> 5] >> (si & 31)) & 1u)) continue;
         int sfragfct = si / FRAG_NSUB, sfragndx = si % FRAG_NSUB;
         int fraglen = frag_length(nrange, sfragndx);
         if (fraglen < 1) continue;
@@ -845,7 +846,7 @@ static void dprefine_t(pairctx* P, int gap0, int prescreen, int maxit, const flo
     /* InitScoresKernel<INITOPT_CONVFLAG_SCOREDP> over every slot
      * (MpStage1.cpp:510): the pair's flag and the fragment slots' flags */
     P->flags &= ~CONV_SCOREDP;
-    P->vskip = 0u;
+    P->vskip[0] = P->vskip[1] = P->vskip[2] = 0u;
 }
 
 static void dprefine(pairctx* P, int gap0, int prescreen, int maxit) {
@@ -859,6 +860,8 @@ static void dprefine(pairctx* P, int gap0, int prescreen, int maxit) {
 /* its thread's running count of them; its memory alignment of the local    */
 /* score matrix follows the chunk layout).                                   */
 #define FRG3_NTOP 32            /* CUS1_TBSP_DPSCORE_TOP_N */
+#define FRG3_NSEC 3             /* CUS1_TBSP_DPSCORE_TOP_N_MAX_CONFIGS: slot sections */
+#define FRG3_LENTHR 150         /* MpStageFrg3.cpp:48 */
 #define FRG3_MAXVISIT 64        /* CUSF_TBSP_INDEX_SCORE_MAXDEPTH */
 #define FRG3_HASH 512           /* CUSF_TBSP_INDEX_SCORE_POSLIMIT2 */
 #define FRG3_SIMROWS 96         /* MPSF_TBSP_LOCAL_SIMILARITY_YDIM x 3 */
@@ -1185,8 +1188,14 @@ static void frg3_stage(pairctx* P) {
     unsigned char* m = P->bt;          /* the local score matrix; DP scores below keep it */
     if (0.0f < thr || seedrule) frg3_localdp(P, o->gapcost, m);
 
-    float sbest[FRG3_NTOP], stfm[FRG3_NTOP][12];
-    for (int k = 0; k < FRG3_NTOP; k++) sbest[k] = 0.f;
+    /* the slots of the configuration sections: section 0 takes every scored
+     * configuration; at --depth 1 and 0 sections 1 and 2 take those on every
+     * second / third grid row and column of a structure longer than 150
+     * (sec2met / sec3met, MpStageFrg3.cpp:204-212), in the same slot */
+    const int nsec = o->depth <= 0 ? 3 : (o->depth <= 1 ? 2 : 1);
+    float sbest[FRG3_NSEC][FRG3_NTOP], stfm[FRG3_NSEC][FRG3_NTOP][12];
+    for (int s = 0; s < FRG3_NSEC; s++)
+        for (int k = 0; k < FRG3_NTOP; k++) sbest[s][k] = 0.f;
     int nscored = 0;
     int qstep = frg3_step(o->depth, lq), rstep = frg3_step(o->depth, lr);
     int minn = o->depth == 3 ? 5 : 10;
@@ -1198,6 +1207,12 @@ static void frg3_stage(pairctx* P) {
     for (int ys = 0; ys < nsy; ys++)
     for (int xs = 0; xs < nsx; xs++) {
         int qrypos = ys * qstep, rfnpos = xs * rstep;
+        int secmet[FRG3_NSEC];
+        secmet[0] = 1;
+        secmet[1] = o->depth <= 1 && (lq <= FRG3_LENTHR || (ys & 1) == 0) &&
+                    (lr <= FRG3_LENTHR || (xs & 1) == 0);
+        secmet[2] = o->depth <= 0 && (lq <= FRG3_LENTHR || ys % 3 == 0) &&
+                    (lr <= FRG3_LENTHR || xs % 3 == 0);
         /* CalcLocalSimilarity2_frg2: flags of the two fragment lengths */
         if (lq < qrypos + f0 || lr < rfnpos + f0 || f0 < 1) continue;
         int conv1 = (lq < qrypos + f1 || lr < rfnpos + f1 || f1 < 1);
@@ -1229,49 +1244,64 @@ static void frg3_stage(pairctx* P) {
                 float sc = frg3_progressive(P, tfm, pq, pr, (int)v[15], lq < lr);
                 int slot = nscored % FRG3_NTOP;
                 nscored++;
-                if (0.0f < sc && sbest[slot] < sc) {
-                    sbest[slot] = sc;
-                    memcpy(stfm[slot], tfm, sizeof(tfm));
-                }
+                /* SaveBestScoreAndTM_Complete and Save2ndryScoreAndTM_Complete
+                 * (MpStageFrg3.h:887-915): a positive score above the slot's */
+                for (int s = 0; s < nsec; s++)
+                    if (secmet[s] && 0.0f < sc && sbest[s][slot] < sc) {
+                        sbest[s][slot] = sc;
+                        memcpy(stfm[s][slot], tfm, sizeof(tfm));
+                    }
             }
         }
     }
-    /* DP scores of the slots' transforms (SaveTopNScoresAndTMsAmongBests with
-     * one thread keeps the slots; ExecDPScore128xKernel skips empty ones) */
-    float dps[FRG3_NTOP];
-    int order[FRG3_NTOP];
-    for (int k = 0; k < FRG3_NTOP; k++) {
-        dps[k] = 0.0f < sbest[k] ? frg3_dpscore(P, stfm[k]) : 0.0f;
-        order[k] = k;
+    /* DP scores of the slots' transforms (SaveTopNScoresAndTMsAmong(Secondary)
+     * Bests with one thread keep the slots; ExecDPScore128xKernel skips empty
+     * ones), then per section the slots by DP score, larger first, lower slot
+     * first on ties (SortBestDPscoresAndTMsAmongDPswifts, MpStageFrg3.h:
+     * 1150-1250): a slot rank without a score flags refinement variant
+     * section * 32 + rank, section 0's first rank being the pair's flag */
+    float dps[FRG3_NSEC][FRG3_NTOP];
+    int order[FRG3_NSEC][FRG3_NTOP];
+    unsigned vskip[3] = {0u, 0u, 0u};   /* in force only in the DP refinement after the branches */
+    for (int s = 0; s < nsec; s++) {
+        for (int k = 0; k < FRG3_NTOP; k++) {
+            dps[s][k] = 0.0f < sbest[s][k] ? frg3_dpscore(P, stfm[s][k]) : 0.0f;
+            order[s][k] = k;
+        }
+        for (int a = 1; a < FRG3_NTOP; a++) {
+            int k = order[s][a], b = a - 1;
+            while (b >= 0 && dps[s][order[s][b]] < dps[s][k]) { order[s][b + 1] = order[s][b]; b--; }
+            order[s][b + 1] = k;
+        }
+        for (int r = s == 0 ? 1 : 0; r < FRG3_NTOP; r++)
+            if (!(0.0f < dps[s][order[s][r]])) vskip[s] |= 1u << r;
     }
-    /* the slots by DP score, larger first, lower slot first on ties
-     * (SortBestDPscoresAndTMsAmongDPswifts, MpStageFrg3.h:1150-1250) */
-    for (int a = 1; a < FRG3_NTOP; a++) {
-        int k = order[a], b = a - 1;
-        while (b >= 0 && dps[order[b]] < dps[k]) { order[b + 1] = order[b]; b--; }
-        order[b + 1] = k;
-    }
-    unsigned vskip = 0u;
-    for (int r = 1; r < FRG3_NTOP; r++)
-        if (!(0.0f < dps[order[r]])) vskip |= 1u << r;
-    /* the pair's flag is the first slot's (MpStageFrg3.h:1210-1225) */
-    P->flags = 0.0f < dps[order[0]] ? 0 : CONV_SCOREDP;
-    /* the branches (Refine_tfmaltconfig, MpStageFrg3.cpp:425-467) */
+    /* the pair's flag is section 0's first slot's (MpStageFrg3.h:1210-1225) */
+    P->flags = 0.0f < dps[0][order[0][0]] ? 0 : CONV_SCOREDP;
+    /* the branches, section by section (Refine_tfmaltconfig,
+     * MpStageFrg3.cpp:425-467); at --depth 1 and 0 each branch's refinement
+     * is followed by one more DP under its iteration-best transform and a
+     * refinement of that alignment */
     float best2 = 0.f;
     int nbr = o->nbranches < FRG3_NTOP ? o->nbranches : FRG3_NTOP;
-    for (int rci = 0; rci < nbr; rci++) {
-        int k = order[rci];
-        int valid = 0.0f < dps[k];
-        if (!(P->flags & (CONV_LOWTMSC | CONV_SCOREDP)) && valid) {
-            dp_run(P, stfm[k], 1, 0.0f, 0, P->d02);
-            btck_matched(P);
-        } else P->naln = 0;
-        if (P->flags) P->best = 0.f;
-        else refine_stage(P, 1, P->d0, P->d02, 1, 0.f, 1, 0);
-        /* the best branch's result (SECONDARYUPDATE, MpStageBase.h:1250-1280) */
-        if (rci == 0 || best2 < P->best) {
-            best2 = P->best;
-            memcpy(P->tfm_2nd, P->tfm_ib, sizeof(P->tfm_ib));
+    for (int rci = 0; rci < nsec * nbr; rci++) {
+        int s = rci / nbr, k = order[s][rci % nbr];
+        int valid = 0.0f < dps[s][k];
+        for (int pass = 0; pass < (o->depth <= 1 ? 2 : 1); pass++) {
+            if (!(P->flags & (CONV_LOWTMSC | CONV_SCOREDP)) && (valid || pass == 1)) {
+                float t[12];
+                memcpy(t, pass == 0 ? stfm[s][k] : P->tfm_ib, sizeof(t));
+                dp_run(P, t, 1, 0.0f, 0, P->d02);
+                btck_matched(P);
+            } else P->naln = 0;
+            if (P->flags) P->best = 0.f;
+            else refine_stage(P, 1, P->d0, P->d02, 1, 0.f, 1, 0);
+            /* the best branch's result (SECONDARYUPDATE, MpStageBase.h:1250-1280):
+             * unconditional for the first branch */
+            if (rci == 0 || best2 < P->best) {
+                best2 = P->best;
+                memcpy(P->tfm_2nd, P->tfm_ib, sizeof(P->tfm_ib));
+            }
         }
     }
     free(pq);
@@ -1279,7 +1309,7 @@ static void frg3_stage(pairctx* P) {
     /* DP refinement from the best branch, with a gap cost and without
      * (MpStageFrg3.h:108-112); the first one skips the fragment variants of
      * the slots the sorting left empty */
-    P->vskip = vskip;
+    memcpy(P->vskip, vskip, sizeof(vskip));
     dprefine_t(P, 0, 0, 2, P->tfm_2nd);
     dprefine(P, 1, 0, 2);
 }

@@ -38,6 +38,10 @@ NAME = re.compile(r"clsf\d\dm\d\d")
 SETS = {
     "cls_complete": dict(seed=51, families=8, members=5, sigma=0.9, indel=0.04, linkage=0, threshold=0.5),
     "cls_single": dict(seed=52, families=6, members=6, sigma=1.2, indel=0.06, linkage=1, threshold=0.5),
+    # members drawn from 1.0 to 3.0 A of noise, so that some fall near or out
+    # of the threshold
+    "cls_mixed_single": dict(seed=53, families=6, members=5, sigma=1.0, sigma_hi=3.0, indel=0.05,
+                             linkage=1, threshold=0.5),
 }
 
 
@@ -52,7 +56,10 @@ def structures(p):
     for f, b in enumerate(base):
         out.append(synth.Chain(b.xyz, b.seq, "clsf%02dm%02d" % (f, 0)))
         for m in range(1, p["members"]):
-            h = synth.homolog(rng, b, p["sigma"], p["indel"], "clsf%02dm%02d" % (f, m))
+            sigma = p["sigma"]
+            if "sigma_hi" in p:
+                sigma = float(rng.uniform(p["sigma"], p["sigma_hi"]))
+            h = synth.homolog(rng, b, sigma, p["indel"], "clsf%02dm%02d" % (f, m))
             out.append(h)
     return out
 
@@ -74,11 +81,19 @@ def run_reference(p, chains, workdir):
         raise RuntimeError("reference --cls run failed: %s" % r.stderr[-2000:])
     clusters = []
     with open(os.path.join(odir, "gtalignclusters.lst")) as f:
-        for line in f:
-            names = NAME.findall(line)
-            if names:
-                clusters.append(names)
-    return clusters, " ".join(cmd[1:])
+        text = f.read()
+    lines = text.splitlines()
+    # the cluster lines follow the last rule of '=' under the header (which
+    # lists the command line and the structures clustered)
+    last = max(k for k, ln in enumerate(lines) if ln.startswith("===="))
+    for line in lines[last + 1:]:
+        names = []
+        for nm in NAME.findall(line):      # a name may occur in a member's path and id
+            if nm not in names:
+                names.append(nm)
+        if names:
+            clusters.append(names)
+    return clusters, " ".join(cmd[1:]), text
 
 
 def main():
@@ -90,9 +105,11 @@ def main():
         p = SETS[name]
         chains = structures(p)
         with tempfile.TemporaryDirectory(prefix="gtcls") as wd:
-            clusters, cmd = run_reference(p, chains, wd)
+            clusters, cmd, text = run_reference(p, chains, wd)
         seen = sorted(n for c in clusters for n in c)
         if seen != sorted(c.name for c in chains):
+            with open(os.path.join(a.outdir, name + ".lst"), "w") as f:
+                f.write(text)
             raise RuntimeError("%s: the clusters do not list every structure once" % name)
         cmd = cmd.replace(os.path.dirname(cmd.split("--cls=")[1].split(",")[0]) + "/", "")
         rec = {"params": p, "command": cmd, "clusters": clusters,

@@ -117,6 +117,15 @@ SETS = {
     "f3_opts": (lambda: synth.config0(seed=303, n_refs=40, qlen=130, homolog_frac=0.3),
                 ["--speed=7", "--seedrule=0", "--nbranches=3", "--gapcost=2", "--window=512",
                  "--pre-score=0", "-s", "0"], 1, "perpair"),
+    # --depth 1 and 0 (the secondary configuration sections and the extra DP
+    # of each branch): --speed 6 and 3 (trigger 50), --speed 0 (trigger 0,
+    # 16 branches, --add-search-by-ss)
+    "f3_speed6": (lambda: synth.config0(seed=304, n_refs=40, qlen=170, homolog_frac=0.3),
+                  ["--speed=6", "--pre-score=0", "-s", "0"], 1, "perpair"),
+    "f3_speed3": (lambda: synth.config0(seed=305, n_refs=40, qlen=160, homolog_frac=0.3),
+                  ["--speed=3", "--pre-score=0", "-s", "0"], 1, "perpair"),
+    "f3_speed0": (lambda: synth.config0(seed=306, n_refs=24, qlen=155, homolog_frac=0.3),
+                  ["--speed=0", "--pre-score=0", "-s", "0"], 1, "perpair"),
 }
 
 

@@ -12,7 +12,8 @@ LEVEL_SETS = {-1: "c0_level_m1", 0: "c0_level_0", 1: "c0_level_1", 2: "c0_level_
               3: "c0_level_3"}
 SETS = ["c0_speed13", "c0_default", "c0_filters", "c0_sym_ref_nodel", "c0_shallow", "c0_2tm",
         "c0_ssrr", "c0_presim", "c0_na", "c0_combo"] + \
-    list(LEVEL_SETS.values()) + ["c0_full", "c0_full_s13", "f3_default", "f3_speed12", "f3_opts"]
+    list(LEVEL_SETS.values()) + ["c0_full", "c0_full_s13", "f3_default", "f3_speed12", "f3_opts",
+                                 "f3_speed6", "f3_speed3", "f3_speed0"]
 # the sets the GPU golden test runs: every set the CUDA library takes (it
 # refuses nucleic-acid pairs) except the combined-options set, which pins
 # the oracle only (each of its options runs on the GPU in the option sets)
@@ -83,6 +84,8 @@ def cli_options(opts):
             d["trigger"] = (0, 20, 50)[(sp - 1) % 3] if 1 <= sp <= 12 else 0
             if sp >= 10:
                 d["refinement"], d["convergence"] = 0, 2
+            if sp == 0:
+                d["nbranches"], d["addsearchbyss"] = 16, 1
         elif o.startswith("--trigger="):
             d["trigger"] = int(o.split("=")[1])
         elif o.startswith("--seedrule="):

@@ -123,6 +123,13 @@ OPTSETS = {
                      nodetailedsearch=0, trigger=0, seedrule=0, nbranches=3, gapcost=2, window=512),
     "frg3seed2": dict(refinement=1, convergence=4, prescore=0.0, scorethld=0.0, symmetric=0, referenced=0, nodeletions=0,
                       nodetailedsearch=0, trigger=20, seedrule=2, nbranches=8, gapcost=0),
+    # --depth 1 and 0: the secondary configuration sections and the extra DP
+    # of every branch (--speed 5, and --speed 0 with its 16 branches and
+    # --add-search-by-ss)
+    "frg3d1": dict(refinement=1, convergence=4, prescore=0.2, scorethld=0.2, symmetric=0, referenced=0, nodeletions=0,
+                   nodetailedsearch=0, depth=1, trigger=20),
+    "frg3d0": dict(refinement=1, convergence=4, prescore=0.0, scorethld=0.0, symmetric=0, referenced=0, nodeletions=0,
+                   nodetailedsearch=0, depth=0, trigger=0, nbranches=16, addsearchbyss=1),
 }
 
 
@@ -237,11 +244,6 @@ def test_status_codes():
     from gtalign_alpha_b200.api import GTalignB200, GTBError, Options
     wl = synth.config0(seed=34, n_refs=2, qlen=50)
     q, r = synth.pack(wl.queries), synth.pack(wl.refs)
-    # the detailed search at --depth 0 or 1 is refused as not supported
-    with GTalignB200(0, 0, Options(nodetailedsearch=0, depth=1)) as g:
-        with pytest.raises(GTBError) as e:
-            g.process_block(q, r)
-        assert e.value.status == 4
     for bad in (dict(trigger=101), dict(nbranches=0), dict(window=100), dict(gapcost=3),
                 dict(clsfilter=1, clscoverage=0.0), dict(clsfilter=1, clscoverage=1.5)):
         with GTalignB200(0, 0, Options(nodetailedsearch=0, **bad)) as g:
