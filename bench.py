@@ -812,19 +812,19 @@ def cluster_run(args):
         g.process_block(synth.pack(chains[:qblock]), allsoa, scorethld=0.5, alignments=False,
                         numerr=False, qtypes=types[:qblock], rtypes=types)
         t0 = time.perf_counter()
-        compared = 0
+        reported = 0
         for q0 in range(0, n, qblock):
             q1 = min(n, q0 + qblock)
             res = g.process_block(synth.pack(chains[q0:q1]), allsoa, scorethld=0.5, alignments=False,
                                   numerr=False, qtypes=types[q0:q1], rtypes=types)
             rec[q0:q1] = res.alndata
-            compared += int((res.alndata[..., 4] > 0).sum())
+            reported += int((res.alndata[..., 4] > 0).sum())
         t1 = time.perf_counter()
     cl = cluster(rec, allsoa.lens, ids=[c.name for c in chains], linkage=0, threshold=0.5, coverage=0.7)
     t2 = time.perf_counter()
     ours = [frozenset(chains[k].name for k in c) for c in cl.clusters]
     out = {"value": n * n / (t2 - t0), "unit": "candidate pairs/s",
-           "structures": n, "pairs_aligned": compared, "align_s": t1 - t0, "link_s": t2 - t1,
+           "structures": n, "pairs_reported": reported, "align_s": t1 - t0, "link_s": t2 - t1,
            "clusters": len(ours),
            "workload": "config4: %d structures, log-normal lengths (median 220), 30%% in families of 10; "
                        "--speed 13, --cls-threshold 0.5, complete linkage, coverage 0.7" % n}
