@@ -316,8 +316,9 @@ gtb_status gtb_last_work(const gtb_handle* h, unsigned long long* w4);
 gtb_status gtb_set_kernel_timing(gtb_handle* h, int on);
 gtb_status gtb_last_kernel_ms(const gtb_handle* h, float* ms4);
 
-/* Spins a bounded wait of the multi-CTA DP makes before it gives up (no
- * reference counterpart; default 2^24).  A wait that gives up ends the call
+/* Spins a bounded wait of the wavefront DPs (a long pair's strips over
+ * several CTAs, or a large pair's over the warps of one CTA) makes before it
+ * gives up (no reference counterpart; default 2^24).  A wait that gives up ends the call
  * with GTB_ERR_CUDA and a message; the handle stays usable.  Small values
  * make the waits give up early, which is how the failure path is tested. */
 gtb_status gtb_set_wait_limit(gtb_handle* h, long long spins);
