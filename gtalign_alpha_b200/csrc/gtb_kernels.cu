@@ -1522,7 +1522,10 @@ __device__ __forceinline__ bool dp_pair(const float* t, float d02, float gcost, 
                                         float* row, unsigned* bt, int lane, int s_first = 0,
                                         int s_step = 1, volatile int* prog = nullptr,
                                         volatile int* err = nullptr,
-                                        long long spin = DP_WAVE_SPIN_DEFAULT, float* fin = nullptr) {
+                                        long long spin = DP_WAVE_SPIN_DEFAULT, float* fin = nullptr,
+                                        bool cta_wave = false) {
+    // cta_wave: the strips' warps share one CTA, so the row values and the
+    // progress counters need ordering at CTA scope only
     constexpr bool usess = SC == DP_SC_TFMSS, ssrr = SC == DP_SC_SSRR;
     constexpr float BND = ssrr ? DPSS_C : 0.f;   // the matrix border
     constexpr int ROWS = 32 * R, SPW = 16 / R;
@@ -1567,7 +1570,8 @@ __device__ __forceinline__ bool dp_pair(const float* t, float d02, float gcost, 
                     }
                 }
                 __syncwarp();
-                __threadfence();
+                if (cta_wave) __threadfence_block();
+                else __threadfence();
                 if (*err) return false;
             }
             if ((g * SPW & 31) == 0) {            // the previous strip's last row, 32 columns
@@ -1636,7 +1640,8 @@ __device__ __forceinline__ bool dp_pair(const float* t, float d02, float gcost, 
             else steps(std::true_type{});
             if (!SCOREONLY) bts[g * 32] = acc;
             if (WAVE && lane == 31) {
-                __threadfence();              // this group's row values before the count
+                if (cta_wave) __threadfence_block();   // this group's row values before the count
+                else __threadfence();
                 prog[s] = (g + 1) * SPW;
             }
         }
@@ -1690,10 +1695,12 @@ __global__ void __launch_bounds__(128) k_dp(Blk B, Bat T, int tfmsrc, float gcos
             __syncthreads();
             if (dp_r(lq) == 4)
                 dp_pair<4, GAP0 != 0, SC, true>(t, d02, gcost, lq, lr, qx, qy, qz, r4, qs, rs, qa, ra, row,
-                                                bt, lane, w, blockDim.x >> 5, s_prog, T.dw_err, T.dw_spin);
+                                                bt, lane, w, blockDim.x >> 5, s_prog, T.dw_err, T.dw_spin,
+                                                nullptr, true);
             else
                 dp_pair<2, GAP0 != 0, SC, true>(t, d02, gcost, lq, lr, qx, qy, qz, r4, qs, rs, qa, ra, row,
-                                                bt, lane, w, blockDim.x >> 5, s_prog, T.dw_err, T.dw_spin);
+                                                bt, lane, w, blockDim.x >> 5, s_prog, T.dw_err, T.dw_spin,
+                                                nullptr, true);
             return;
         }
         if (w != 0) return;                        // one strip: one warp
