@@ -33,6 +33,8 @@ struct gtb_handle {
     // so the short, narrow launches at the end of one overlap the others
     static const int NSUB = 3;
     cudaStream_t sub[NSUB] = {};
+    cudaStream_t aux[NSUB] = {};     // per sub-batch stream: a refinement's long pairs
+    cudaEvent_t fork[NSUB] = {}, join[NSUB] = {};
     static const int NWAVE = 2;      // sub-batches per stream and batch
     cudaEvent_t sev[NWAVE * NSUB][8] = {};  // stage events per sub-batch
     int dw_cap = 0;                  // CTAs the wavefront DP keeps resident
@@ -91,6 +93,11 @@ extern "C" gtb_status gtb_create(int device, size_t mem_bytes, const gtb_options
     h->sub[0] = h->st;
     for (int j = 1; j < gtb_handle::NSUB; j++)
         CK(cudaStreamCreateWithFlags(&h->sub[j], cudaStreamNonBlocking));
+    for (int j = 0; j < gtb_handle::NSUB; j++) {
+        CK(cudaStreamCreateWithFlags(&h->aux[j], cudaStreamNonBlocking));
+        CK(cudaEventCreateWithFlags(&h->fork[j], cudaEventDisableTiming));
+        CK(cudaEventCreateWithFlags(&h->join[j], cudaEventDisableTiming));
+    }
     for (int j = 0; j < gtb_handle::NWAVE * gtb_handle::NSUB; j++)
         for (int k = 0; k < 8; k++) CK(cudaEventCreate(&h->sev[j][k]));
     std::vector<float> a(TBL), b(TBL), c(TBL);
@@ -117,6 +124,11 @@ extern "C" void gtb_destroy(gtb_handle* h) {
         for (int k = 0; k < 8; k++) if (h->sev[j][k]) cudaEventDestroy(h->sev[j][k]);
     for (int j = 1; j < gtb_handle::NSUB; j++)
         if (h->sub[j]) cudaStreamDestroy(h->sub[j]);
+    for (int j = 0; j < gtb_handle::NSUB; j++) {
+        if (h->aux[j]) cudaStreamDestroy(h->aux[j]);
+        if (h->fork[j]) cudaEventDestroy(h->fork[j]);
+        if (h->join[j]) cudaEventDestroy(h->join[j]);
+    }
     if (h->st) cudaStreamDestroy(h->st);
     if (h->h_flag) cudaFreeHost(h->h_flag);
     delete h;
@@ -483,6 +495,7 @@ static gtb_status run_block(gtb_handle* h, const DevBlock& D, float scorethld,
         }
         T.work = h->d_work;
         T.kt = h->ktime ? &h->kt : nullptr;
+        T.st2 = h->aux[j]; T.evfork = h->fork[j]; T.evjoin = h->join[j];
         T.dw_spin = h->wait_limit;
         T.nff = np; T.ff_pair = nullptr; T.ff_chunk = nullptr; T.ff_nch = nullptr; T.ff_key = nullptr;
         T.rl_nlmax = nlmax; T.rl_long = T.rl_count = T.rl_next = nullptr; T.rl_cand = nullptr;

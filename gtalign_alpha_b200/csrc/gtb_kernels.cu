@@ -1473,13 +1473,21 @@ void launch_refine(int mode, const Blk& B, const Bat& T0, cudaStream_t st, bool 
     k_rlist_count<<<nb, 256, 0, st>>>(B, T, mode);
     k_rlist_scan<<<1, 1024, 0, st>>>(T);
     k_rlist_fill<<<nb, 256, 0, st>>>(B, T, mode);
-    KtScope kts(T, KF_REFINE, st);
+    // the long pairs on the second stream, beside the short ones (both read
+    // the lists built above; they write disjoint pairs)
+    const bool fork = T.st2 && (T.rl_long || T.rl_long2);
+    cudaStream_t sl = fork ? T.st2 : st;
+    KtScope kts(T, KF_REFINE, st);   // on st, after the join: both streams' time
+    if (fork) {
+        cudaEventRecord(T.evfork, st);
+        cudaStreamWaitEvent(T.st2, T.evfork, 0);
+    }
     if (few) launch_refine_k<32, false>(mode, B, T, st);
     else launch_refine_k<16, false>(mode, B, T, st);
     if (T.launches) (*T.launches) += 4;
     if (T.rl_long) {
-        launch_refine_k<32, true>(mode, B, T, st);
-        launch_refine_long_fin(mode, B, T, st);
+        launch_refine_k<32, true>(mode, B, T, sl);
+        launch_refine_long_fin(mode, B, T, sl);
         if (T.launches) (*T.launches) += 2;
     }
     if (T.rl_long2) {
@@ -1487,9 +1495,13 @@ void launch_refine(int mode, const Blk& B, const Bat& T0, cudaStream_t st, bool 
         Bat T2 = T;
         T2.rl_long = T.rl_long2; T2.rl_count = T.rl_count2; T2.rl_next = T.rl_next2;
         T2.rl_cand = T.rl_cand2; T2.rl_nlmax = T.rl_nlmax2; T2.rlw_ctas = T.rlw_ctas2;
-        launch_refine_k<32, true>(mode, B, T2, st);
-        launch_refine_long_fin(mode, B, T2, st);
+        launch_refine_k<32, true>(mode, B, T2, sl);
+        launch_refine_long_fin(mode, B, T2, sl);
         if (T.launches) (*T.launches) += 2;
+    }
+    if (fork) {
+        cudaEventRecord(T.evjoin, T.st2);
+        cudaStreamWaitEvent(st, T.evjoin, 0);
     }
 }
 

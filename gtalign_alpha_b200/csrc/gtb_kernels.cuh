@@ -119,6 +119,10 @@ struct Bat {
     int *rl_long2, *rl_count2, *rl_next2;
     float* rl_cand2;
     int plog_round;                  // round of an RM_PLOG launch (0 .. PLOG_ROUNDS-1)
+    // host: a second stream for a refinement launch's long pairs, which then
+    // run beside its short pairs (fork and join events; null: one stream)
+    cudaStream_t st2;
+    cudaEvent_t evfork, evjoin;
     // seed work items when some pair's offsets are split over several CTAs
     // (null: one CTA per pair): item -> pair, item -> chunk, chunks per pair,
     // per-pair packed (score, variant) maximum
