@@ -13,6 +13,10 @@ loops -> final superposition/production scores) over one query chunk (2
 queries, the reference's --dev-queries-per-chunk default) x all 200,000
 references.  Legs of one run:
 
+* autotune (before any timing, --autotune 1): gtb_autotune picks the launch
+  shapes (seed offsets per CTA, CTAs per long refinement pair, DP pairs per
+  CTA wavefront, pairs per sub-batch) on the first step's block; every
+  handle then uses them.  They change no result.
 * value (headline): the batched form with adjoint polishing of the final
   transforms (5 projected-gradient steps), structure blocks resident in HBM
   (gtb_process_resident, results left on the device).  The per-pair numeric
@@ -348,6 +352,17 @@ def run_ours(args):
     maxpairs = max(step_pairs)
     legs = set(args.legs.split(","))
 
+    # launch shapes picked by the library's autotuner on the first step's
+    # block (outside the timed region), then used by every handle
+    tuning = None
+    if args.autotune:
+        progress("autotune (launch shapes, on the first step's block)")
+        t0 = time.time()
+        best, tms, tried = gp.autotune(qblks[0], rblk, scorethld=0.5, trials=1)
+        g0.set_tuning(best)
+        tuning = {"picked": best.as_dict(), "ms_per_call": tms, "s": time.time() - t0,
+                  "tried": [dict(t, ms=round(m, 2)) for t, m in tried]}
+
     # headline: batched + adjoint polishing, resident
     progress("headline (batched + adjoint, resident)")
     rp = Resident(L, gp, qblks, rblk, step_pairs, maxpairs, args.steps, dev)
@@ -494,7 +509,9 @@ def run_ours(args):
                        "form": "batched + adjoint polishing (%d steps)" % args.polish_steps,
                        "options": options_text(args),
                        "l2": "inputs larger than L2 (%.0f MB of reference coordinates)" % (12 * r_all.total / 1e6),
-                       "parallelism": "dp%d (references split by cost, independent pairs)" % ws},
+                       "parallelism": "dp%d (references split by cost, independent pairs)" % ws,
+                       "launch_shapes": tuning["picked"] if tuning else "defaults (--autotune 0)"},
+            "autotune": tuning,
             "accuracy": {"max_err_tm": max(A["maxerr"][:2]), "max_err_rmsd": A["maxerr"][2],
                          "tolerance_tm": TOL_TM, "ok": bool(acc_ok),
                          "pairs_rmsd_err_over_1e-3": A["nrmsd_over"],
@@ -997,6 +1014,8 @@ def main():
     ap.add_argument("--nqueries", type=int, default=16)
     ap.add_argument("--qchunk", type=int, default=2, help="queries per step (the reference's --dev-queries-per-chunk)")
     ap.add_argument("--seed", type=int, default=2)
+    ap.add_argument("--autotune", type=int, default=1,
+                    help="pick the launch shapes with gtb_autotune before the timed steps (0: defaults)")
     ap.add_argument("--speed", type=int, default=13, choices=list(range(14)),
                     help="the command line's --speed preset 0..12 (9: its default); 13: its "
                          "defaults with --no-detailed-search")

@@ -58,6 +58,19 @@ class _CResults(ctypes.Structure):
                 ("qss", ctypes.c_void_p), ("rss", ctypes.c_void_p)]
 
 
+class Tuning(ctypes.Structure):
+    """Launch shapes of a handle (gtb_tuning); none changes a result."""
+    _fields_ = [("seed_chunk", ctypes.c_int), ("refine_long_ctas", ctypes.c_int),
+                ("dp_cta_pairs", ctypes.c_int), ("sub_pairs", ctypes.c_int)]
+
+    def as_dict(self) -> dict:
+        return {f: int(getattr(self, f)) for f, _ in self._fields_}
+
+
+class _CTuningTrial(ctypes.Structure):
+    _fields_ = [("t", Tuning), ("ms", ctypes.c_float)]
+
+
 @dataclass
 class Options:
     """Per-pair computation options, with the gtalign command line's codes.
@@ -158,6 +171,20 @@ def load_library():
     L.gtb_set_wait_limit.restype = ctypes.c_int
     L.gtb_destroy.argtypes = [vp]
     L.gtb_destroy.restype = None
+    L.gtb_block_upload.argtypes = [vp, vp, vp, ctypes.POINTER(vp)]
+    L.gtb_block_upload.restype = ctypes.c_int
+    L.gtb_block_free.argtypes = [vp, vp]
+    L.gtb_block_free.restype = None
+    L.gtb_process_resident.argtypes = [vp, ctypes.c_float, vp, vp, vp, vp, vp]
+    L.gtb_process_resident.restype = ctypes.c_int
+    L.gtb_get_tuning.argtypes = [vp, ctypes.POINTER(Tuning)]
+    L.gtb_get_tuning.restype = ctypes.c_int
+    L.gtb_set_tuning.argtypes = [vp, ctypes.POINTER(Tuning)]
+    L.gtb_set_tuning.restype = ctypes.c_int
+    L.gtb_autotune.argtypes = [vp, ctypes.c_float, vp, vp, ctypes.c_int, ctypes.POINTER(Tuning),
+                               ctypes.POINTER(ctypes.c_float), ctypes.POINTER(_CTuningTrial),
+                               ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
+    L.gtb_autotune.restype = ctypes.c_int
     L.gtb_tm_adjoint.argtypes = [vp, ctypes.c_int, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp]
     L.gtb_tm_adjoint.restype = ctypes.c_int
     L.gtb_polish.argtypes = [vp, ctypes.c_int, vp, vp, vp, vp, vp, vp, ctypes.c_int, vp, vp, vp]
@@ -327,6 +354,48 @@ class GTalignB200:
         self.lib.gtb_last_kernel_ms(self._h, ms.ctypes.data_as(ctypes.POINTER(ctypes.c_float)))
         return ms
 
+    def get_tuning(self) -> Tuning:
+        t = Tuning()
+        self.lib.gtb_get_tuning(self._h, ctypes.byref(t))
+        return t
+
+    def set_tuning(self, t: Optional[Tuning] = None, **fields) -> None:
+        """Set the launch shapes: a Tuning, or fields changed from the
+        current one (seed_chunk=..., refine_long_ctas=..., ...)."""
+        t2 = self.get_tuning() if t is None else Tuning(**t.as_dict())
+        for k, v in fields.items():
+            if k not in t2.as_dict():
+                raise GTBError(1, "no tuning field %r" % k)
+            setattr(t2, k, int(v))
+        st = self.lib.gtb_set_tuning(self._h, ctypes.byref(t2))
+        if st != 0:
+            raise GTBError(st, self.lib.gtb_last_error(self._h).decode())
+
+    def upload(self, blk: PackedBlock) -> "ResidentBlock":
+        """A block copied to the device once (gtb_block_upload)."""
+        h = ctypes.c_void_p()
+        st = self.lib.gtb_block_upload(self._h, blk.beg, blk.end, ctypes.byref(h))
+        if st != 0:
+            raise GTBError(st, self.lib.gtb_last_error(self._h).decode())
+        return ResidentBlock(self, h, blk.n)
+
+    def autotune(self, queries: "ResidentBlock", refs: "ResidentBlock", scorethld: float = 0.5,
+                 trials: int = 1, nlog: int = 32):
+        """Pick the launch shapes for this workload (gtb_autotune; the blocks
+        are ResidentBlocks or gtb_block handles): returns
+        (the tuning left set, its ms per call, [(tuning dict, ms) tried])."""
+        best = Tuning()
+        ms = ctypes.c_float()
+        log = (_CTuningTrial * nlog)()
+        nl = ctypes.c_int()
+        qh, rh = getattr(queries, "h", queries), getattr(refs, "h", refs)
+        st = self.lib.gtb_autotune(self._h, float(scorethld), qh, rh, int(trials),
+                                   ctypes.byref(best), ctypes.byref(ms), log, nlog,
+                                   ctypes.byref(nl))
+        if st != 0:
+            raise GTBError(st, self.lib.gtb_last_error(self._h).decode())
+        return best, float(ms.value), [(log[k].t.as_dict(), float(log[k].ms)) for k in range(nl.value)]
+
     def process_block(self, queries: SoA, refs: SoA, scorethld: float = 0.5,
                       alignments: bool = True, numerr: bool = True,
                       secstr: bool = False, qndx=None, rndx=None, qtypes=None,
@@ -381,6 +450,24 @@ class GTalignB200:
                            alns, qb.arrays[0].copy(), rb.arrays[0].copy(), rb.arrays[1].copy(),
                            qss, rss, int(self.lib.gtb_last_launch_count(self._h)), tms,
                            self.last_work())
+
+
+class ResidentBlock:
+    """A block on the device (GTalignB200.upload); free it before the handle."""
+
+    def __init__(self, g: GTalignB200, h: ctypes.c_void_p, n: int):
+        self.g, self.h, self.n = g, h, n
+
+    def free(self) -> None:
+        if self.h:
+            self.g.lib.gtb_block_free(self.g.handle, self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.free()
 
 
 class _CClusterOptions(ctypes.Structure):

@@ -12,6 +12,7 @@
 #include <string>
 #include <vector>
 #include <algorithm>
+#include <chrono>
 #include <cuda_runtime.h>
 
 #include "gtb200.h"
@@ -45,6 +46,8 @@ struct gtb_handle {
     bool ktime = false;                    // per-family launch timing on
     gtb::KTimer kt;
     float kms[gtb::KF_N] = {0, 0, 0, 0};   // its times of the last call
+    // launch shapes (gtb_set_tuning / gtb_autotune)
+    gtb_tuning tn{gtb::FF_CHUNK, gtb::RLW_CTAS, gtb::DP_CTA_PAIRS, 16384};
 };
 
 static const int TBL = 65536;
@@ -363,7 +366,8 @@ static gtb_status run_block(gtb_handle* h, const DevBlock& D, float scorethld,
             int n1, silo, sihi, prv;
             gtb::seed_range(lq, lr, B.qmax, B.qmin, B.rmax, B.rmin, B.stepinit, n1, silo, sihi, prv);
             int cnt = sihi - silo + 1;
-            int nch = cnt > gtb::FF_CHUNK ? (cnt + gtb::FF_CHUNK - 1) / gtb::FF_CHUNK : 1;
+            const int chunk = h->tn.seed_chunk;
+            int nch = cnt > chunk ? (cnt + chunk - 1) / chunk : 1;
             ffn[i] = nch;
             nitems += nch;
             split = split || nch > 1;
@@ -513,7 +517,9 @@ static gtb_status run_block(gtb_handle* h, const DevBlock& D, float scorethld,
         T.ndw = 0; T.dw_nprog = 0; T.dw_item = T.dw_pair = T.dw_G = nullptr; T.dw_soff = nullptr;
         T.dw_mark = nullptr; T.dw_prog = nullptr;
         T.dw_err = (int*)(base + o_dwe);
-        T.dp_kc = gtb::DP_CTA_PAIRS;
+        T.dp_kc = h->tn.dp_cta_pairs;
+        T.ff_span = h->tn.seed_chunk;
+        T.rlw_ctas = h->tn.refine_long_ctas;
         CK(cudaMemsetAsync(T.dw_err, 0, sizeof(int), st));
         h->h_flag[evset] = 0;
         if (nl) {
@@ -589,12 +595,12 @@ static gtb_status run_block(gtb_handle* h, const DevBlock& D, float scorethld,
             snprintf(h->err, sizeof(h->err), "pair (%lld) needs %zu bytes > budget %zu", p0, used, budget);
             return GTB_ERR_NOMEM;
         }
-        // split into sub-batches of at least 16k pairs, in up to two waves
+        // split into sub-batches of at least tn.sub_pairs pairs, in up to two waves
         // over the streams: the narrow stage-2 launches of the first wave
         // overlap the wide stage-1 launches of the second
         long long nb = p1 - p0;
         int nsub = (int)std::min<long long>(gtb_handle::NWAVE * gtb_handle::NSUB,
-                                            std::max<long long>(1, nb / 16384));
+                                            std::max<long long>(1, nb / h->tn.sub_pairs));
         long long q0 = p0;
         for (int j = 0; j < nsub; j++) {
             long long q1 = p0 + nb * (j + 1) / nsub;
@@ -916,6 +922,106 @@ extern "C" gtb_status gtb_process_resident(gtb_handle* h, float scorethld, const
     CK(cudaSetDevice(h->dev));
     DevBlock D = make_devblock(queries, refs);
     return run_block(h, D, scorethld, d_alndata, d_tfm, d_numerr, nullptr);
+}
+
+// ---------------------------------------------------------------------------
+// Launch shapes and their autotuner.
+
+static bool tuning_ok(const gtb_tuning& t) {
+    return t.seed_chunk >= 128 && t.seed_chunk <= 65536 && t.refine_long_ctas >= 1 &&
+           t.refine_long_ctas <= gtb::RLW_CTAS && t.dp_cta_pairs >= 0 &&
+           t.dp_cta_pairs <= 65536 && t.sub_pairs >= 1024 && t.sub_pairs <= (1 << 30);
+}
+
+extern "C" gtb_status gtb_get_tuning(const gtb_handle* h, gtb_tuning* t) {
+    if (!h || !t) return GTB_ERR_ARG;
+    *t = h->tn;
+    return GTB_OK;
+}
+
+extern "C" gtb_status gtb_set_tuning(gtb_handle* h, const gtb_tuning* t) {
+    if (!h || !t) return GTB_ERR_ARG;
+    if (!tuning_ok(*t)) {
+        snprintf(h->err, sizeof(h->err), "tuning field out of range");
+        return GTB_ERR_ARG;
+    }
+    h->tn = *t;
+    return GTB_OK;
+}
+
+extern "C" gtb_status gtb_autotune(gtb_handle* h, float scorethld, const gtb_block* queries,
+                                   const gtb_block* refs, int trials, gtb_tuning* best,
+                                   float* best_ms, gtb_tuning_trial* log, int nlog,
+                                   int* nlogged) {
+    if (!h) return GTB_ERR_ARG;
+    h->err[0] = 0;
+    if (nlogged) *nlogged = 0;
+    if (!queries || !refs || trials < 1 || (nlog > 0 && !log) || !tuning_ok(h->tn)) {
+        snprintf(h->err, sizeof(h->err), "autotune: bad arguments");
+        return GTB_ERR_ARG;
+    }
+    const long long np = (long long)queries->n * refs->n;
+    if (np <= 0) {
+        snprintf(h->err, sizeof(h->err), "autotune: empty block");
+        return GTB_ERR_ARG;
+    }
+    CK(cudaSetDevice(h->dev));
+    // the calls' records go to scratch buffers freed on every return
+    struct Scratch {
+        float *rec = nullptr, *tfm = nullptr;
+        ~Scratch() { if (rec) cudaFree(rec); if (tfm) cudaFree(tfm); }
+    } sc;
+    CK(cudaMalloc((void**)&sc.rec, (size_t)np * GTB_NOUT * sizeof(float)));
+    CK(cudaMalloc((void**)&sc.tfm, (size_t)np * 12 * sizeof(float)));
+    const gtb_tuning start = h->tn;
+    int nl = 0;
+    // the least time of `trials` calls under t, after one untimed call
+    auto time_one = [&](const gtb_tuning& t, float& ms) -> gtb_status {
+        h->tn = t;
+        gtb_status s = gtb_process_resident(h, scorethld, queries, refs, sc.rec, sc.tfm, nullptr);
+        ms = 3.0e38f;
+        for (int k = 0; s == GTB_OK && k < trials; k++) {
+            auto t0 = std::chrono::steady_clock::now();
+            s = gtb_process_resident(h, scorethld, queries, refs, sc.rec, sc.tfm, nullptr);
+            auto t1 = std::chrono::steady_clock::now();
+            ms = std::min(ms, std::chrono::duration<float, std::milli>(t1 - t0).count());
+        }
+        if (s == GTB_OK && nl < nlog) log[nl++] = gtb_tuning_trial{t, ms};
+        return s;
+    };
+    gtb_tuning cur = start;
+    float curms = 0.f;
+    gtb_status s = time_one(cur, curms);
+    // one field at a time: its candidates with the others as they stand
+    static const int c_seed[] = {256, 512, 1024, 2048};
+    static const int c_rlw[] = {4, 8, 16};
+    static const int c_dpk[] = {0, 296, 592, 1184};
+    static const int c_sub[] = {8192, 16384, 32768};
+    struct Field { int gtb_tuning::*f; const int* c; int n; };
+    const Field fields[] = {{&gtb_tuning::seed_chunk, c_seed, 4},
+                            {&gtb_tuning::refine_long_ctas, c_rlw, 3},
+                            {&gtb_tuning::dp_cta_pairs, c_dpk, 4},
+                            {&gtb_tuning::sub_pairs, c_sub, 3}};
+    for (const Field& fd : fields) {
+        const int v0 = cur.*(fd.f);
+        for (int k = 0; s == GTB_OK && k < fd.n; k++) {
+            if (fd.c[k] == v0) continue;
+            gtb_tuning t = cur;
+            t.*(fd.f) = fd.c[k];
+            float ms = 0.f;
+            s = time_one(t, ms);
+            if (s == GTB_OK && ms < 0.98f * curms) { cur = t; curms = ms; }
+        }
+    }
+    if (nlogged) *nlogged = nl;
+    if (s != GTB_OK) {
+        h->tn = start;
+        return s;
+    }
+    h->tn = cur;
+    if (best) *best = cur;
+    if (best_ms) *best_ms = curms;
+    return GTB_OK;
 }
 
 extern "C" gtb_status gtb_process_block(gtb_handle* h, float scorethld,

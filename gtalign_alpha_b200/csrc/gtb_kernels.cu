@@ -602,8 +602,9 @@ __global__ void __launch_bounds__(128) k_findfrag(Blk B, Bat T) {
     // this CTA's share of the offsets
     int s0 = silo, s1 = sihi;
     if (nch > 1) {
-        s0 = silo + c * FF_CHUNK;
-        s1 = s0 + FF_CHUNK - 1 < sihi ? s0 + FF_CHUNK - 1 : sihi;
+        const int chunk = T.ff_span > 0 ? T.ff_span : FF_CHUNK;
+        s0 = silo + c * chunk;
+        s1 = s0 + chunk - 1 < sihi ? s0 + chunk - 1 : sihi;
     }
     float d0 = B.t_d0[ml];
     float d02 = __fmul_rn(d0, d0);
@@ -1450,13 +1451,13 @@ static void launch_refine_long_fin(int mode, const Blk& B, const Bat& T, cudaStr
 }
 
 void launch_refine(int mode, const Blk& B, const Bat& T0, cudaStream_t st, bool few) {
-    // the long-pair path: from RL_LONG positions with RLW_CTAS CTAs; where
+    // the long-pair path: from RL_LONG positions with T0.rlw_ctas CTAs; where
     // few pairs take part (the launches after the --pre-score filter) a
     // launch lasts as long as its slowest pair, so there the pairs from
     // RL_LONG_FEW positions below that get RLW_CTAS_FEW CTAs (second tier)
     Bat T = T0;
     T.rl_min = RL_LONG;
-    T.rlw_ctas = RLW_CTAS;
+    T.rlw_ctas = T0.rlw_ctas > 0 && T0.rlw_ctas <= RLW_CTAS ? T0.rlw_ctas : RLW_CTAS;
     T.rl_min2 = RL_LONG_FEW;
     T.rlw_ctas2 = RLW_CTAS_FEW;
     if (!few) T.rl_long2 = nullptr;

@@ -110,7 +110,8 @@ struct Bat {
     // this launch's threshold and CTAs per long pair.  The second set (the
     // same fields with 2) is a lower tier, pairs from rl_min2 positions with
     // rlw_ctas2 CTAs each, used in the launches after the --pre-score filter
-    // (null rl_long2: no second tier in this launch)
+    // (null rl_long2: no second tier in this launch).  The caller's rlw_ctas
+    // is the first tier's CTAs per pair (0: RLW_CTAS)
     int rl_nlmax;
     int rl_min, rlw_ctas;
     int *rl_long, *rl_count, *rl_next;
@@ -142,6 +143,7 @@ struct Bat {
     // the first dp_kc pairs of a DP work list (the largest matrices) run as a
     // wavefront over the 4 warps of a CTA each (0: none; needs dw_err)
     int dp_kc;
+    int ff_span;                     // seed offsets per CTA of a split pair (0: FF_CHUNK)
     long long* launches;             // host counter of kernel launches
     cudaError_t* lerr;               // host: first failed launch (null: not recorded)
     struct KTimer* kt;               // host: per-family launch timer (null: off)

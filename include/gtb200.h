@@ -323,6 +323,43 @@ gtb_status gtb_last_kernel_ms(const gtb_handle* h, float* ms4);
  * make the waits give up early, which is how the failure path is tested. */
 gtb_status gtb_set_wait_limit(gtb_handle* h, long long spins);
 
+/* Launch shapes of a handle (no reference counterpart: the reference fixes
+ * its launch configurations at compile time).  None of them changes a
+ * result, only how the work is spread over the SMs and streams. */
+typedef struct {
+    int seed_chunk;        /* seed offsets per CTA; a pair with more is split
+                              over several CTAs (128..65536; default 512) */
+    int refine_long_ctas;  /* CTAs per pair of the refinement's long-pair tier
+                              (pairs from 1,536 positions; 1..16; default 16) */
+    int dp_cta_pairs;      /* pairs of each DP launch (its largest matrices)
+                              run as a wavefront over a CTA's warps
+                              (0..65536; default 592, 4 per SM) */
+    int sub_pairs;         /* pairs per concurrent sub-batch, at least
+                              (1024..2^30; default 16384) */
+} gtb_tuning;
+gtb_status gtb_get_tuning(const gtb_handle* h, gtb_tuning* t);
+/* GTB_ERR_ARG (the handle's tuning unchanged) when a field is out of range. */
+gtb_status gtb_set_tuning(gtb_handle* h, const gtb_tuning* t);
+
+/* Autotuner: times gtb_process_resident on two resident blocks (a sample of
+ * the caller's workload, or the workload itself) for candidate launch
+ * shapes, one field at a time from the handle's current tuning (seed_chunk
+ * 256/512/1024/2048, refine_long_ctas 4/8/16, dp_cta_pairs 0/296/592/1184,
+ * sub_pairs 8192/16384/32768); a candidate replaces the field's value only
+ * when its time, the least of `trials` calls after one untimed call, is
+ * below 98% of the best so far.  Leaves the winner set on the handle and
+ * returns it in *best and its time in *best_ms (either may be NULL).
+ * `log`, when not NULL, receives up to `nlog` entries (the tuning tried
+ * and its ms) and *nlogged their count.  Host wall time around the calls,
+ * which synchronise; the results written by the calls are discarded. */
+typedef struct {
+    gtb_tuning t;
+    float ms;
+} gtb_tuning_trial;
+gtb_status gtb_autotune(gtb_handle* h, float scorethld, const gtb_block* queries,
+                        const gtb_block* refs, int trials, gtb_tuning* best, float* best_ms,
+                        gtb_tuning_trial* log, int nlog, int* nlogged);
+
 void gtb_destroy(gtb_handle* h);
 
 /* Clustering of n structures from the records of their all-against-all

@@ -73,13 +73,16 @@ def test_pack_fields_layout():
 
 
 def test_python_structs_match_the_c_header(tmp_path):
-    """The ctypes mirrors of gtb_options and gtb_results have the C header's
-    field offsets and sizes (compiled with the host C compiler)."""
+    """The ctypes mirrors of gtb_options, gtb_results, gtb_tuning and
+    gtb_tuning_trial have the C header's field offsets and sizes (compiled
+    with the host C compiler)."""
     import subprocess
-    from gtalign_alpha_b200.api import _COptions, _CResults
+    from gtalign_alpha_b200.api import _COptions, _CResults, Tuning, _CTuningTrial
+    structs = (("gtb_options", _COptions), ("gtb_results", _CResults), ("gtb_tuning", Tuning),
+               ("gtb_tuning_trial", _CTuningTrial))
     src = tmp_path / "layout.c"
     lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "gtb200.h"', "int main(void) {"]
-    for cname, py in (("gtb_options", _COptions), ("gtb_results", _CResults)):
+    for cname, py in structs:
         lines.append('printf("%s size %%zu\\n", sizeof(%s));' % (cname, cname))
         for fname, _ in py._fields_:
             lines.append('printf("%s.%s %%zu\\n", offsetof(%s, %s));' % (cname, fname, cname, fname))
@@ -88,7 +91,21 @@ def test_python_structs_match_the_c_header(tmp_path):
     exe = tmp_path / "layout"
     subprocess.check_call(["gcc", "-I", os.path.join(ROOT, "include"), "-o", str(exe), str(src)])
     got = dict(l.rsplit(" ", 1) for l in subprocess.check_output([str(exe)]).decode().splitlines())
-    for cname, py in (("gtb_options", _COptions), ("gtb_results", _CResults)):
+    for cname, py in structs:
         assert int(got[cname + " size"]) == ctypes.sizeof(py), cname
         for fname, _ in py._fields_:
             assert int(got["%s.%s" % (cname, fname)]) == getattr(py, fname).offset, (cname, fname)
+
+
+def test_options_and_tuning_mirrors_build_on_the_host():
+    """Options (keyword fields, speed presets) and Tuning convert to their C
+    structs without a device."""
+    from gtalign_alpha_b200.api import Options, Tuning
+    o = Options(polish_steps=2, prescore=0.3)
+    c = o._c()
+    assert c.polish_steps == 2 and abs(c.prescore - 0.3) < 1e-7
+    assert Options.speed(9)._c().nodetailedsearch == 0
+    assert Options.speed(13)._c().nodetailedsearch == 1
+    t = Tuning(256, 8, 0, 8192)
+    assert t.as_dict() == dict(seed_chunk=256, refine_long_ctas=8, dp_cta_pairs=0, sub_pairs=8192)
+    assert Tuning(**t.as_dict()).as_dict() == t.as_dict()
