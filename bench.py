@@ -46,6 +46,9 @@ references.  Legs of one run:
   structures (config4's generator): the set aligned against itself with the
   clustering run's coverage prefilter, linked by gtb_cluster; the
   reference's GPU build (--cls) on the same structures, wall clock both.
+* default_options: gtalign's default options (--speed 9, the spatial-index
+  detailed search on) on the same workload, --defaults-steps steps over the
+  first query chunks, and the reference's GPU build at those options.
 
 Inputs (about 0.6 GB of coordinates and the pair state) are larger than L2
 between steps.  --impl reference times the reference's own CPU
@@ -428,7 +431,8 @@ def run_ours(args):
     algo_bytes = 12 * r.total + 12 * q.total / nchunk + 64 * step_pairs_avg
     seed_ms = float(st_ms[0])
     achieved = algo_bytes / (seed_ms / 1000.0) / 1e9 if seed_ms > 0 else 0.0
-    nsub = max(1, min(6, int(step_pairs_avg) // 16384))
+    sub_pairs = tuning["picked"]["sub_pairs"] if tuning else 16384
+    nsub = max(1, min(6, int(step_pairs_avg) // sub_pairs))
     traffic = FINDFRAG_DRAM_BYTES_PER_PAIR * step_pairs_avg / nsub
     clocks = A["clocks"]
     sm_mhz = clocks["sm_mhz"] if clocks else 1965.0
@@ -476,11 +480,14 @@ def run_ours(args):
                          "dp_refine_loops": float(st_ms[2]), "final": float(st_ms[5]),
                          "total": float(st_ms[6])}}
 
-    long_chain = adjoint = cpu = refgpu = clustering = None
+    long_chain = adjoint = cpu = refgpu = clustering = defaults = None
     if rank == 0 and ws == 1:
         if "refgpu" in legs:
             progress("reference GPU build")
             refgpu = reference_gpu_sample(wl, args, value)
+        if "defaults" in legs and args.speed == 13:
+            progress("default options (--speed 9)")
+            defaults = defaults_run(L, args, wl, qbs, rb, step_pairs, maxpairs, dev, legs)
         if "cluster" in legs:
             progress("clustering run")
             clustering = cluster_run(args)
@@ -529,6 +536,7 @@ def run_ours(args):
             "adjoint": adjoint,
             "cpu_baseline": cpu,
             "reference_gpu": refgpu,
+            "default_options": defaults,
             "clustering": clustering,
             "clocks": clocks,
             "workload_gen_s": gen_s,
@@ -879,6 +887,48 @@ def cluster_run(args):
         shutil.rmtree(d, ignore_errors=True)
 
 
+def defaults_run(L, args, wl, qbs, rb, step_pairs, maxpairs, dev, legs):
+    """gtalign's default options (--speed 9: the spatial-index detailed search
+    on) on the headline workload, one GPU: a handle of its own (the blocks
+    uploaded again, with their index trees), one warm-up step, then
+    --defaults-steps resident polished steps over the first query chunks,
+    every timed pair's TM-score error checked; and the reference's GPU build
+    at the same options on its sample."""
+    import copy
+    from gtalign_alpha_b200.api import GTalignB200
+    a9 = copy.copy(args)
+    a9.speed, a9.steps, a9.warmup = 9, args.defaults_steps, 1
+    g9 = GTalignB200(dev, 0, lib_options(a9, args.polish_steps))
+    blks = []
+    try:
+        t0 = time.time()
+        for pk in list(qbs) + [rb]:
+            blk = ctypes.c_void_p()
+            st = L.gtb_block_upload(g9.handle, pk.beg, pk.end, ctypes.byref(blk))
+            if st != 0:
+                raise RuntimeError(L.gtb_last_error(g9.handle).decode())
+            blks.append(blk)
+        upload_s = time.time() - t0
+        res = Resident(L, g9, blks[:-1], blks[-1], step_pairs, maxpairs, a9.steps, dev)
+        D = timed_steps(res, a9, 1, dev, lambda: None)
+        v = D["pairs"] / (D["ms"] / 1000.0)
+        out = {"value": v, "unit": UNIT, "ms_per_step": D["ms"] / a9.steps, "steps": a9.steps,
+               "options": options_text(a9), "form": "batched + adjoint polishing (%d steps), resident"
+               % args.polish_steps, "max_err_tm": max(D["maxerr"][:2]),
+               "ok": bool(max(D["maxerr"][:2]) <= TOL_TM),
+               "upload_and_index_s": upload_s,
+               "note": "the first query chunks only (they hold the longest queries); the "
+                       "headline's 8 steps cover all 16"}
+        if "refgpu" in legs:
+            progress("reference GPU build at the default options")
+            out["reference_gpu"] = reference_gpu_sample(wl, a9, v)
+        return out
+    finally:
+        for blk in blks:
+            L.gtb_block_free(g9.handle, blk)
+        g9.close()
+
+
 def reference_gpu_sample(wl, args, value):
     """The reference's GPU build on this device: the first query chunk (2
     queries) x the first refgpu_refs references of the workload, default
@@ -1032,8 +1082,11 @@ def main():
     ap.add_argument("--refgpu-timeout", type=int, default=600)
     ap.add_argument("--cluster-n", type=int, default=1000,
                     help="structures of the all-against-all clustering leg")
-    ap.add_argument("--legs", default="unpolished,e2e,plain,long,adjoint,cpu,refgpu,cluster",
-                    help="legs besides the headline: unpolished,e2e,plain,long,adjoint,cpu,refgpu,cluster")
+    ap.add_argument("--legs", default="unpolished,e2e,plain,long,adjoint,cpu,refgpu,cluster,defaults",
+                    help="legs besides the headline: unpolished,e2e,plain,long,adjoint,cpu,refgpu,"
+                         "cluster,defaults")
+    ap.add_argument("--defaults-steps", type=int, default=2,
+                    help="timed steps of the default-options leg (--speed 9)")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

@@ -1896,6 +1896,11 @@ void launch_f3_dpscore(const Blk& B, const Bat& T, cudaStream_t st) {
 
 // ---------------------------------------------------------------------------
 // traceback: MpDPHub.cpp:1515-1660 (plain) and 1699-1905 (constrained)
+constexpr int BTCK_AHEAD = 4;     // step groups the traceback loads ahead
+__device__ __forceinline__ void bt_prefetch(const unsigned* p) {
+    asm volatile("prefetch.global.L1 [%0];" ::"l"(p));
+}
+
 __global__ void k_btck(Blk B, Bat T, int constrained) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= T.np) return;
@@ -1923,9 +1928,35 @@ __global__ void k_btck(Blk B, Bat T, int constrained) {
         for (int f = 0; f < 12; f++) t[f] = T.tfm_gr[i * 12 + f];
     }
     int y = lq - 1, x = lr - 1, n = 0;
+    // The walk is a chain of dependent loads.  The 32 words of a (strip, step
+    // group) are one 128-byte line and the path only moves to lower groups and
+    // strips, so each new group starts the loads of the BTCK_AHEAD groups
+    // below it (and, near a strip's top, of the previous strip's groups the
+    // path enters next); the last word read is kept.
+    long long cwi = -1;
+    unsigned w = 0;
+    int cs = -1, cg = -1, prevs = -1;
     while (x >= 0 && y >= 0) {
         int yy = y % rows, l = yy / R, tt = x + l;
-        unsigned w = bt[(long long)(y / rows) * sw + (tt / spw) * 32 + l];
+        const int s = y / rows, g = tt / spw;
+        const long long wi = (long long)s * sw + (long long)g * 32 + l;
+        if (wi != cwi) {
+            if (s != cs) {              // a new strip (or the start): its next groups
+                for (int k = 1; k <= BTCK_AHEAD && g - k >= 0; k++)
+                    bt_prefetch(bt + (long long)s * sw + (long long)(g - k) * 32);
+            } else if (g != cg && g >= BTCK_AHEAD) {
+                bt_prefetch(bt + (long long)s * sw + (long long)(g - BTCK_AHEAD) * 32);
+            }
+            cs = s; cg = g;
+            if (l <= 2 && s > 0 && prevs != s) {
+                const int gp = (x + 31) / spw;
+                for (int k = 0; k < BTCK_AHEAD && gp - k >= 0; k++)
+                    bt_prefetch(bt + (long long)(s - 1) * sw + (long long)(gp - k) * 32);
+                prevs = s;
+            }
+            w = bt[wi];
+            cwi = wi;
+        }
         int b = (int)((w >> (2 * R * (tt % spw) + 2 * (yy % R))) & 3u);
         if (b == BT_UP) { y--; continue; }
         if (b == BT_LEFT) { x--; continue; }
