@@ -30,7 +30,8 @@ references.  Legs of one run:
   layout) inside the timed region.
 * plain: the same kernels at one pair per call (1 query x 1 reference).
 * long_chain: the long-chain configuration (8 assembly pairs of
-  5,000-37,860 residues, one call per pair) with alignment rows.
+  5,000-37,860 residues, one call per pair) with alignment rows; the
+  reference's GPU build on the 12,000 and 37,860 pairs.
 * adjoint: 1,000,000 fixed-alignment pairs (lengths U(60,600)) polished
   with 10 projected-gradient steps of the TM-score adjoint.
 * roofline: the HBM roofline of the stage-1 seed scan, and the FP32 SIMT
@@ -675,10 +676,60 @@ def long_chain_run(g, args):
         per.append({"length": int(lengths[i]), "wall_s": wall, "tm_q": float(rec[9]), "tm_r": float(rec[10]),
                     "rmsd": float(rec[8]), "aligned": int(rec[4]),
                     "err_tm": float(res.numerr[0, 0, :2].max()), "err_rmsd": float(res.numerr[0, 0, 2])})
-    return {"value": q.n / tot, "unit": "pairs/s", "total_s": tot, "pairs": per,
-            "form": "batched + adjoint polishing (%d steps), alignment rows" % args.polish_steps,
-            "published_reference": "GTalign on a T4: 65.12 s for a 37,860-residue pair (other "
-                                   "structures, other GPU; not comparable as a ratio)"}
+    out = {"value": q.n / tot, "unit": "pairs/s", "total_s": tot, "pairs": per,
+           "form": "batched + adjoint polishing (%d steps), alignment rows" % args.polish_steps,
+           "published_reference": "GTalign on a T4: 65.12 s for a 37,860-residue pair (other "
+                                  "structures, other GPU; not comparable as a ratio)"}
+    if "refgpu" in args.legs.split(",") and args.long_refgpu_lengths:
+        progress("reference GPU build on long chains")
+        pick = {int(x) for x in args.long_refgpu_lengths.split(",")}
+        out["reference_gpu"] = [long_chain_reference_gpu(wl.queries[i], wl.refs[i], per[i], args)
+                                for i in range(q.n) if lengths[i] in pick]
+    return out
+
+
+def long_chain_reference_gpu(qc, rc, ours, args):
+    """The reference's GPU build on one long pair (the same structures as PDB
+    files; --dev-max-length and --dev-queries-total-length-per-chunk raised
+    to the pair's length so that it is not skipped): its query batch
+    execution time and wall time against this library's wall time for the
+    pair (which includes the host copies and alignment rows)."""
+    from gtalign_alpha_b200 import synth
+    binp = os.path.join(ROOT, "oracle", "_ref", "gpu", "gtalign")
+    if not os.path.exists(binp):
+        return {"unavailable": "oracle/_ref/gpu/gtalign not built (make -f oracle/Makefile.refgpu)"}
+    L = max(qc.length, rc.length)
+    d = tempfile.mkdtemp(prefix="gtreflong")
+    try:
+        qf, rf = os.path.join(d, "q.pdb"), os.path.join(d, "r.pdb")
+        synth.write_pdb(qc, qf)
+        synth.write_pdb(rc, rf)
+        cmd = [binp, "--qrs=" + qf, "--rfs=" + rf, "-o", d + "/out", "--outfmt=1", "--dev-N=1",
+               "--dev-max-length=%d" % L, "--dev-queries-total-length-per-chunk=%d" % L,
+               "-s", "0"] + cli_options(args)
+        t0 = time.perf_counter()
+        p = subprocess.run(cmd, capture_output=True, timeout=args.refgpu_timeout)
+        wall = time.perf_counter() - t0
+        if p.returncode != 0:
+            return {"length": ours["length"],
+                    "unavailable": "reference GPU build exited %d: %s" % (p.returncode, p.stderr.decode()[-300:])}
+        secs, tmq = 0.0, None
+        for f in os.listdir(d + "/out"):
+            J = json.load(open(os.path.join(d, "out", f)))["gtalign_search"]
+            secs += J["search_statistics"]["query_batch_execution_time"]
+            for h in J["search_results"]:
+                tmq = float(h["hit_record"]["alignment"]["tmscore_query"])
+        if tmq is None:
+            return {"length": ours["length"], "wall_s": wall,
+                    "unavailable": "no alignment reported (stderr: %s)" % p.stderr.decode()[-300:]}
+        return {"length": ours["length"], "wall_s": wall, "batch_s": secs, "tm_q": tmq,
+                "ours_wall_s": ours["wall_s"], "ours_tm_q": ours["tm_q"],
+                "reference_batch_over_ours_wall": secs / ours["wall_s"] if ours["wall_s"] > 0 else None}
+    except subprocess.TimeoutExpired:
+        return {"length": ours["length"],
+                "unavailable": "reference GPU build did not finish within %d s" % args.refgpu_timeout}
+    finally:
+        shutil.rmtree(d, ignore_errors=True)
 
 
 def adjoint_pairs(npairs: int, steps: int, nbase: int = 50_000):
@@ -1080,6 +1131,8 @@ def main():
     ap.add_argument("--refgpu-refs", type=int, default=10000,
                     help="references in the reference GPU build's sample (x the first query chunk)")
     ap.add_argument("--refgpu-timeout", type=int, default=600)
+    ap.add_argument("--long-refgpu-lengths", default="12000,37860",
+                    help="long-chain pairs also run through the reference's GPU build (empty: none)")
     ap.add_argument("--cluster-n", type=int, default=1000,
                     help="structures of the all-against-all clustering leg")
     ap.add_argument("--legs", default="unpolished,e2e,plain,long,adjoint,cpu,refgpu,cluster,defaults",

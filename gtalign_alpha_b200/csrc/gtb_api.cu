@@ -238,7 +238,7 @@ static size_t pair_bytes(int lq, int lr, bool strings, bool f3 = false) {
     if (strings) b += (size_t)5 * (lq + lr + 1);       // alignment rows
     b += 4 * 8 + 12 * 4 * 2 + 16 * 4 + 4 * 4 + 12 * 4 + 64 + 4 + 24;  // state, offsets, work lists
     if (std::min(lq, lr) >= gtb::RL_LONG_FEW)          // long-pair candidates
-        b += (size_t)gtb::RLW_WARPS * gtb::RLW_CAND * 4 + 12;
+        b += (size_t)gtb::RLW_CTAS_MAX * gtb::RLW_CTA_WARPS * gtb::RLW_CAND * 4 + 12;
     return b;
 }
 
@@ -449,9 +449,12 @@ static gtb_status run_block(gtb_handle* h, const DevBlock& D, float scorethld,
         size_t o_dwp = nl ? carve((size_t)dnprog * sizeof(int)) : 0;
         size_t o_dwe = carve(sizeof(int));      // wavefront error flag (multi-CTA and CTA waves)
         size_t o_rll = nlmax ? carve((size_t)(2 * nlmax + 1) * sizeof(int)) : 0;
-        size_t o_rlc = nlmax ? carve((size_t)nlmax * gtb::RLW_WARPS * gtb::RLW_CAND * sizeof(float)) : 0;
+        // CTAs per long pair of each tier (more when few pairs are long)
+        const int ctasA = gtb::rlw_ctas_for(h->tn.refine_long_ctas, nlmax);
+        const int ctasB = gtb::rlw_ctas_for(gtb::RLW_CTAS_FEW, nlmax2);
+        size_t o_rlc = nlmax ? carve((size_t)nlmax * ctasA * gtb::RLW_CTA_WARPS * gtb::RLW_CAND * sizeof(float)) : 0;
         size_t o_rll2 = nlmax2 ? carve((size_t)(2 * nlmax2 + 1) * sizeof(int)) : 0;
-        size_t o_rlc2 = nlmax2 ? carve((size_t)nlmax2 * gtb::RLW_WARPS * gtb::RLW_CAND * sizeof(float)) : 0;
+        size_t o_rlc2 = nlmax2 ? carve((size_t)nlmax2 * ctasB * gtb::RLW_CTA_WARPS * gtb::RLW_CAND * sizeof(float)) : 0;
         // detailed search: local score matrices, slots, DP scores, branches
         size_t o_lsm = B.f3 ? carve((size_t)std::max<long long>(off_lsm[np], 1)) : 0;
         const size_t nsl = (size_t)B.f3nsec * F3_NTOP, nbr = (size_t)B.f3nsec * F3_NBMAX;
@@ -519,7 +522,8 @@ static gtb_status run_block(gtb_handle* h, const DevBlock& D, float scorethld,
         T.dw_err = (int*)(base + o_dwe);
         T.dp_kc = h->tn.dp_cta_pairs;
         T.ff_span = h->tn.seed_chunk;
-        T.rlw_ctas = h->tn.refine_long_ctas;
+        T.rlw_ctas = ctasA;
+        T.rlw_ctas2 = ctasB;
         CK(cudaMemsetAsync(T.dw_err, 0, sizeof(int), st));
         h->h_flag[evset] = 0;
         if (nl) {

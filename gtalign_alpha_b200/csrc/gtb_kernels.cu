@@ -1032,6 +1032,104 @@ __device__ __forceinline__ float lane_pass(const PairGeom& G, int kind, int k0, 
               : lane_pass_t<false, false, false>(G, kind, k0, k1, tfm, d02, chk, d82, thr, m3on, v, m3out, pl);
 }
 
+// One pass of a variant that the 32 lanes of a warp share (the long pairs'
+// refinement when few pairs are long).  Lane L sums the positions of block
+// cb + L (blocks of BLK positions, the absolute blocks of lane_pass_t) in
+// position order, exactly as lane_pass_t sums a block; the block partials
+// then go through shared memory and lane f folds field f of every block in
+// block order (the same Neumaier folds, the same closing fold), so the sums,
+// the score and the three smallest distances equal lane_pass_t's bit for
+// bit.  Every lane returns the results.  sm: 32 x 17 floats of this warp.
+__device__ float wide_pass(const PairGeom& G, int kind, int k0, int k1, const float* tfm,
+                           float d02, int chk, float d82, float thr, int m3on, float* v,
+                           float& m3out, int lane, float* sm) {
+    const unsigned FULL = 0xffffffffu;
+    const bool frag = kind == PK_FRAG;
+    const bool scr = kind == PK_SCORE || kind == PK_GSCORE;
+    const bool cov = kind == PK_SCORE || kind == PK_EXT;
+    const bool trk = kind == PK_SCORE && m3on;
+    const int n = kind == PK_IDLE ? 0 : (frag ? k1 : G.n);
+    const int bfirst = frag ? (k0 & ~(BLK - 1)) / BLK : 0;
+    const int nblk = (n + BLK - 1) / BLK;
+    float fs = 0.f, fc = 0.f;                  // lane f < 16: field f's compensated total
+    float m1 = LARGEDST, m2 = LARGEDST, m3 = LARGEDST;
+    int cnt = 0;
+    for (int cb = bfirst; cb < nblk; cb += 32) {
+        const int b = cb + lane;
+        float part[16];
+#pragma unroll
+        for (int f = 0; f < 16; f++) part[f] = 0.f;
+        if (b < nblk) {
+            const int p0 = b * BLK, p1 = p0 + BLK < n ? p0 + BLK : n;
+            for (int k = p0; k < p1; k++) {
+                float qx, qy, qz, rx, ry, rz;
+                G.at(k, qx, qy, qz, rx, ry, rz);
+                float d = dist2_tf(tfm, qx, qy, qz, rx, ry, rz);
+                if (scr) part[15] = __fadd_rn(part[15], (!chk || d <= d82) ? tmterm(d02, d) : 0.f);
+                if (trk) {
+                    bool c1 = d < m1, c2 = d < m2, c3 = d < m3;
+                    m3 = c2 ? m2 : (c3 ? d : m3);
+                    m2 = c1 ? m1 : (c2 ? d : m2);
+                    m1 = c1 ? d : m1;
+                }
+                bool inc = frag ? (k0 <= k) : (cov && d <= thr);
+                const float ax = inc ? qx : 0.f, ay = inc ? qy : 0.f, az = inc ? qz : 0.f;
+                const float bx = inc ? rx : 0.f, by = inc ? ry : 0.f, bz = inc ? rz : 0.f;
+                part[0] = __fmaf_rn(ax, bx, part[0]); part[1] = __fmaf_rn(ax, by, part[1]);
+                part[2] = __fmaf_rn(ax, bz, part[2]); part[3] = __fmaf_rn(ay, bx, part[3]);
+                part[4] = __fmaf_rn(ay, by, part[4]); part[5] = __fmaf_rn(ay, bz, part[5]);
+                part[6] = __fmaf_rn(az, bx, part[6]); part[7] = __fmaf_rn(az, by, part[7]);
+                part[8] = __fmaf_rn(az, bz, part[8]);
+                part[9] = __fadd_rn(part[9], ax); part[10] = __fadd_rn(part[10], ay);
+                part[11] = __fadd_rn(part[11], az); part[12] = __fadd_rn(part[12], bx);
+                part[13] = __fadd_rn(part[13], by); part[14] = __fadd_rn(part[14], bz);
+                cnt += inc ? 1 : 0;
+            }
+        }
+        __syncwarp();
+#pragma unroll
+        for (int f = 0; f < 16; f++) sm[lane * 17 + f] = part[f];
+        __syncwarp();
+        if (lane < 16) {
+            const int nb = nblk - cb < 32 ? nblk - cb : 32;
+            for (int L = 0; L < nb; L++) {
+                float bb = sm[L * 17 + lane];
+                nfold(fs, fc, bb);
+            }
+        }
+    }
+    // the closing fold of lane_pass_t (score) and of CovAcc::final (sums)
+    if (lane < 16) {
+        float z = 0.f;
+        nfold(fs, fc, z);
+    }
+    const float tot = __fadd_rn(fs, fc);
+#pragma unroll
+    for (int f = 0; f < 15; f++) v[f] = __shfl_sync(FULL, tot, f);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) cnt += __shfl_xor_sync(FULL, cnt, o);
+    v[15] = (float)cnt;
+    // the three smallest distances of the pass (a multiset: merging the
+    // lanes' three smallest gives the same three as one sweep)
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const float o1 = __shfl_xor_sync(FULL, m1, o), o2 = __shfl_xor_sync(FULL, m2, o),
+                    o3 = __shfl_xor_sync(FULL, m3, o);
+        const float x[3] = {o1, o2, o3};
+#pragma unroll
+        for (int e = 0; e < 3; e++) {
+            const float d = x[e];
+            bool c1 = d < m1, c2 = d < m2, c3 = d < m3;
+            m3 = c2 ? m2 : (c3 ? d : m3);
+            m2 = c1 ? m1 : (c2 ? d : m2);
+            m1 = c1 ? d : m1;
+        }
+    }
+    m3out = m3;
+    __syncwarp();
+    return __shfl_sync(FULL, tot, 15);
+}
+
 // The pair's result of a refinement launch (MpStage1.cpp:700-716 and the
 // final/production copies): winner score, transform and fragment, or the
 // "nothing scored" outputs.  tb: the winner's transform, stride tstr.
@@ -1084,7 +1182,7 @@ __device__ __forceinline__ void refine_commit(const Blk& B, const Bat& T, int i,
 // once, measured the same on the benchmark step: the concurrent sub-batch
 // streams fill those slots already).
 constexpr int RF_WARPS_SHORT = 4;
-constexpr int RF_WARPS_LONG = 4;
+constexpr int RF_WARPS_LONG = RLW_CTA_WARPS;
 
 // LONG: the pairs with at least RL_LONG positions, RLW_CTAS CTAs each; every
 // warp of them takes the pair's variants from one counter in global memory
@@ -1092,9 +1190,13 @@ constexpr int RF_WARPS_LONG = 4;
 // pair's winner among them.
 // One slot of a refinement launch: a short pair (slot of the length-sorted
 // list) or, LONG, warp `wlong` of the warps working on long pair `slot`.
-template <int MODE, int RF_LPP, bool LONG>
+// WIDE (long pairs only): a warp works on one variant at a time, its lanes
+// sharing the passes (wide_pass); otherwise every lane has a variant.
+template <int MODE, int RF_LPP, bool LONG, bool WIDE = false>
 __device__ __forceinline__ void refine_slot(const Blk& B, const Bat& T, int slot, int wlong) {
     constexpr int RF_WARPS = LONG ? RF_WARPS_LONG : RF_WARPS_SHORT;
+    static_assert(!WIDE || (LONG && RF_LPP == 32), "a wide pass is a long pair's warp");
+    __shared__ float s_wide[WIDE ? 17 * RF_WARPS * 32 : 1];   // block partials of wide passes
     __shared__ float s_last[16 * RF_WARPS * 32];   // previous iteration's sums
     __shared__ float s_tb[12 * RF_WARPS * 32];     // best transform of the current variant
     __shared__ float s_tbest[12 * RF_WARPS * 32];  // best transform over the lane's variants
@@ -1198,7 +1300,25 @@ __device__ __forceinline__ void refine_slot(const Blk& B, const Bat& T, int slot
     unsigned long long vis = 0;                   // position visits of this lane's passes
     for (;;) {
         const unsigned nm = __ballot_sync(FULL, need) & smask;
-        if (nm) {
+        if (WIDE && nm) {                         // one variant for the whole warp
+            int base = 0;
+            if (lane == 0) base = atomicAdd(T.rl_next + slot, 1);
+            const int kv = __shfl_sync(FULL, base, 0);
+            need = false;
+            kind = PK_IDLE;
+            if (kv < V.total) {
+                int fl, kf;
+                variants_get(V, vk, n, kv, si, vndx, vpos, fl, kf);
+                if (MODE == RM_DP && T.vskip && si < 32 * F3_NSEC &&
+                    ((T.vskip[(long long)i * F3_NSEC + (si >> 5)] >> (si & 31)) & 1u)) {
+                    need = true;
+                } else {
+                    kind = PK_FRAG; k0 = kf; k1 = kf + fl;
+                    best = best_init; cit = 0;
+                }
+            }
+            if (need) continue;                   // a skipped variant: the next one
+        } else if (nm) {
             if (LONG) {                           // the pair's counter, shared by its warps
                 int base = 0;
                 if (lane == 0) base = atomicAdd(T.rl_next + slot, __popc(nm));
@@ -1228,9 +1348,12 @@ __device__ __forceinline__ void refine_slot(const Blk& B, const Bat& T, int slot
             break;
         }
         float v[16], m3;
-        const float sc = lane_pass(G, kind, k0, k1, tfm, pd02, pchk, d82, thr, m3mode, v, m3,
-                                   lane % RF_LPP);
-        vis += kind == PK_IDLE ? 0u : (kind == PK_FRAG ? (unsigned)(k1 - k0) : (unsigned)n);
+        const float sc = WIDE ? wide_pass(G, kind, k0, k1, tfm, pd02, pchk, d82, thr, m3mode, v, m3,
+                                          lane, s_wide + (threadIdx.x >> 5) * 32 * 17)
+                              : lane_pass(G, kind, k0, k1, tfm, pd02, pchk, d82, thr, m3mode, v, m3,
+                                          lane % RF_LPP);
+        if (!WIDE || lane == 0)
+            vis += kind == PK_IDLE ? 0u : (kind == PK_FRAG ? (unsigned)(k1 - k0) : (unsigned)n);
         bool havev = false, done = false;
         if (kind == PK_FRAG) {
             if (v[15] < 1.0f) done = true;
@@ -1313,7 +1436,7 @@ __device__ __forceinline__ void refine_slot(const Blk& B, const Bat& T, int slot
     if (!valid) return;
     if (LONG) {
         if (lane == wl) {
-            float* c = T.rl_cand + ((long long)slot * RLW_WARPS + wlong) * RLW_CAND;
+            float* c = T.rl_cand + ((long long)slot * (T.rlw_ctas * RF_WARPS_LONG) + wlong) * RLW_CAND;
             c[0] = havewin ? wb : 0.f;
             c[1] = __int_as_float(wsi);
             c[2] = lgbest;
@@ -1330,14 +1453,14 @@ __device__ __forceinline__ void refine_slot(const Blk& B, const Bat& T, int slot
 
 // LONG: T.rlw_ctas CTAs per long pair; the grid (a multiple of that) walks
 // the long pairs listed for this launch.
-template <int MODE, int RF_LPP, bool LONG>
+template <int MODE, int RF_LPP, bool LONG, bool WIDE = false>
 __global__ void __launch_bounds__((LONG ? RF_WARPS_LONG : RF_WARPS_SHORT) * 32) k_refine(Blk B, Bat T) {
     if (LONG) {
         const int c = T.rlw_ctas;
         const int wl = (int)(blockIdx.x % c) * RF_WARPS_LONG + (threadIdx.x >> 5);
         const int nlong = *T.rl_count;
         for (int slot = (int)(blockIdx.x / c); slot < nlong; slot += (int)(gridDim.x / c))
-            refine_slot<MODE, RF_LPP, LONG>(B, T, slot, wl);
+            refine_slot<MODE, RF_LPP, LONG, WIDE>(B, T, slot, wl);
     } else {
         constexpr int RF_PPW = 32 / RF_LPP;        // pairs per warp
         const int slot = blockIdx.x * (RF_PPW * RF_WARPS_SHORT) + (threadIdx.x >> 5) * RF_PPW +
@@ -1354,7 +1477,7 @@ __global__ void k_refine_long_fin(Blk B, Bat T) {
     const int slot = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
     if (slot >= *T.rl_count) return;
     const int i = T.rl_long[slot];
-    const float* c0 = T.rl_cand + (long long)slot * RLW_WARPS * RLW_CAND;
+    const float* c0 = T.rl_cand + (long long)slot * (T.rlw_ctas * RF_WARPS_LONG) * RLW_CAND;
     float wb = 0.f;
     int wsi = 0x7fffffff, wk = -1;
     const int nw = T.rlw_ctas * RF_WARPS_LONG;      // the warps that left candidates
@@ -1378,7 +1501,7 @@ __global__ void k_refine_long_fin(Blk B, Bat T) {
                         __float_as_int(c[4]), c + 5, 1);
 }
 
-template <int LPP, bool LONG>
+template <int LPP, bool LONG, bool WIDE = false>
 static void launch_refine_k(int mode, const Blk& B, const Bat& T, cudaStream_t st) {
     constexpr int W = LONG ? RF_WARPS_LONG : RF_WARPS_SHORT;
     // long pairs: at most RLW_GRID CTAs, T.rlw_ctas per pair at a time
@@ -1387,13 +1510,13 @@ static void launch_refine_k(int mode, const Blk& B, const Bat& T, cudaStream_t s
                         : (T.np + (32 / LPP) * W - 1) / ((32 / LPP) * W);
     const int nt = W * 32;
     switch (mode) {
-        case RM_INIT:  k_refine<RM_INIT, LPP, LONG><<<ng, nt, 0, st>>>(B, T); break;
-        case RM_DP:    k_refine<RM_DP, LPP, LONG><<<ng, nt, 0, st>>>(B, T); break;
-        case RM_FIN1:  k_refine<RM_FIN1, LPP, LONG><<<ng, nt, 0, st>>>(B, T); break;
-        case RM_FIN2:  k_refine<RM_FIN2, LPP, LONG><<<ng, nt, 0, st>>>(B, T); break;
-        case RM_PROD1: k_refine<RM_PROD1, LPP, LONG><<<ng, nt, 0, st>>>(B, T); break;
-        case RM_PROD2: k_refine<RM_PROD2, LPP, LONG><<<ng, nt, 0, st>>>(B, T); break;
-        case RM_PLOG:  k_refine<RM_PLOG, LPP, LONG><<<ng, nt, 0, st>>>(B, T); break;
+        case RM_INIT:  k_refine<RM_INIT, LPP, LONG, WIDE><<<ng, nt, 0, st>>>(B, T); break;
+        case RM_DP:    k_refine<RM_DP, LPP, LONG, WIDE><<<ng, nt, 0, st>>>(B, T); break;
+        case RM_FIN1:  k_refine<RM_FIN1, LPP, LONG, WIDE><<<ng, nt, 0, st>>>(B, T); break;
+        case RM_FIN2:  k_refine<RM_FIN2, LPP, LONG, WIDE><<<ng, nt, 0, st>>>(B, T); break;
+        case RM_PROD1: k_refine<RM_PROD1, LPP, LONG, WIDE><<<ng, nt, 0, st>>>(B, T); break;
+        case RM_PROD2: k_refine<RM_PROD2, LPP, LONG, WIDE><<<ng, nt, 0, st>>>(B, T); break;
+        case RM_PLOG:  k_refine<RM_PLOG, LPP, LONG, WIDE><<<ng, nt, 0, st>>>(B, T); break;
     }
 }
 
@@ -1401,13 +1524,13 @@ static void launch_refine_k(int mode, const Blk& B, const Bat& T, cudaStream_t s
 // for the smallest shared-memory carve-out that holds as many CTAs as their
 // registers allow (static arrays + the 1 kB each CTA reserves), leaving the
 // rest of the SM's 256 kB to L1.
-template <int LPP, bool LONG>
+template <int LPP, bool LONG, bool WIDE = false>
 static void carve_refine() {
     constexpr int W = LONG ? RF_WARPS_LONG : RF_WARPS_SHORT;
-    const void* ks[7] = {(const void*)k_refine<RM_INIT, LPP, LONG>, (const void*)k_refine<RM_DP, LPP, LONG>,
-                         (const void*)k_refine<RM_FIN1, LPP, LONG>, (const void*)k_refine<RM_FIN2, LPP, LONG>,
-                         (const void*)k_refine<RM_PROD1, LPP, LONG>, (const void*)k_refine<RM_PROD2, LPP, LONG>,
-                         (const void*)k_refine<RM_PLOG, LPP, LONG>};
+    const void* ks[7] = {(const void*)k_refine<RM_INIT, LPP, LONG, WIDE>, (const void*)k_refine<RM_DP, LPP, LONG, WIDE>,
+                         (const void*)k_refine<RM_FIN1, LPP, LONG, WIDE>, (const void*)k_refine<RM_FIN2, LPP, LONG, WIDE>,
+                         (const void*)k_refine<RM_PROD1, LPP, LONG, WIDE>, (const void*)k_refine<RM_PROD2, LPP, LONG, WIDE>,
+                         (const void*)k_refine<RM_PLOG, LPP, LONG, WIDE>};
     int dev = 0, smem_sm = 0, regs_sm = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
@@ -1432,6 +1555,7 @@ void configure_kernels() {
     carve_refine<16, false>();
     carve_refine<32, false>();
     carve_refine<32, true>();
+    carve_refine<32, true, true>();
     float gs[GTB_GONNET_NA * GTB_GONNET_NA];
     gtb_gonnet_scores(gs);
     cudaMemcpyToSymbol(g_gonnet, gs, sizeof(gs));
@@ -1457,9 +1581,9 @@ void launch_refine(int mode, const Blk& B, const Bat& T0, cudaStream_t st, bool 
     // RL_LONG_FEW positions below that get RLW_CTAS_FEW CTAs (second tier)
     Bat T = T0;
     T.rl_min = RL_LONG;
-    T.rlw_ctas = T0.rlw_ctas > 0 && T0.rlw_ctas <= RLW_CTAS ? T0.rlw_ctas : RLW_CTAS;
+    T.rlw_ctas = T0.rlw_ctas > 0 && T0.rlw_ctas <= RLW_CTAS_MAX ? T0.rlw_ctas : RLW_CTAS;
     T.rl_min2 = RL_LONG_FEW;
-    T.rlw_ctas2 = RLW_CTAS_FEW;
+    T.rlw_ctas2 = T0.rlw_ctas2 > 0 && T0.rlw_ctas2 <= RLW_CTAS_MAX ? T0.rlw_ctas2 : RLW_CTAS_FEW;
     if (!few) T.rl_long2 = nullptr;
     cudaMemsetAsync(T.rhist, 0, (RL_NB + 1) * sizeof(int), st);
     if (T.rl_long) {
@@ -1487,7 +1611,8 @@ void launch_refine(int mode, const Blk& B, const Bat& T0, cudaStream_t st, bool 
     else launch_refine_k<16, false>(mode, B, T, st);
     if (T.launches) (*T.launches) += 4;
     if (T.rl_long) {
-        launch_refine_k<32, true>(mode, B, T, sl);
+        if (T.rl_nlmax <= RLW_WIDE_MAX) launch_refine_k<32, true, true>(mode, B, T, sl);
+        else launch_refine_k<32, true>(mode, B, T, sl);
         launch_refine_long_fin(mode, B, T, sl);
         if (T.launches) (*T.launches) += 2;
     }
@@ -1518,8 +1643,8 @@ void launch_refine(int mode, const Blk& B, const Bat& T0, cudaStream_t st, bool 
 // WAVE: the strips of one pair are shared by several CTAs (strip s by CTA
 // s mod s_step); a strip waits, with a bounded spin, until the previous one
 // has published the steps whose last-row values it is about to read
-// (`prog`: steps done per strip), and publishes its own progress after each
-// group of steps.  Returns false when a wait gave up (error flag set).
+// (`prog`: steps done per strip), and publishes its own progress every 32
+// steps.  Returns false when a wait gave up (error flag set).
 // SC, the cell score: DP_SC_TFM (TM-score term under t), DP_SC_TFMSS (plus 0.5
 // for equal secondary structure), DP_SC_SSRR (the --add-search-by-ss DP,
 // dpssw_btck.cu:280-330: 1 for equal secondary structure + 0.2 x the Gonnet
@@ -1652,8 +1777,11 @@ __device__ __forceinline__ bool dp_pair(const float* t, float d02, float gcost, 
             if (full && g * SPW >= 31 && (g + 1) * SPW <= lr) steps(std::false_type{});
             else steps(std::true_type{});
             if (!SCOREONLY) bts[g * 32] = acc;
-            if (WAVE && lane == 31) {
-                if (cta_wave) __threadfence_block();   // this group's row values before the count
+            // the next strip reads its row values 32 steps at a time, so the
+            // count is published at every 32nd step (and the last): one fence
+            // per 32 steps instead of per group
+            if (WAVE && lane == 31 && ((((g + 1) * SPW) & 31) == 0 || g == ngrp - 1)) {
+                if (cta_wave) __threadfence_block();   // the row values before the count
                 else __threadfence();
                 prog[s] = (g + 1) * SPW;
             }

@@ -15,15 +15,29 @@ namespace gtb {
 // refinement: pairs with at least RL_LONG positions get RLW_CTAS CTAs of 4
 // warps; in the launches where few pairs take part, the pairs below that
 // with at least RL_LONG_FEW positions get RLW_CTAS_FEW; a long-pair launch
-// has at most RLW_GRID CTAs (they walk the long pairs)
+// has at most RLW_GRID CTAs (they walk the long pairs).  When a sub-batch
+// has few pairs of a tier, each gets more CTAs (rlw_ctas_for), up to
+// RLW_CTAS_MAX: a lone long pair has variants for many more warps.
 constexpr int RL_LONG = 1536;
 constexpr int RL_LONG_FEW = 384;
 constexpr int RL_NBUCKET = 65536 >> 4;   // work-list buckets; rhist[RL_NBUCKET] = list length
 constexpr int RLW_CTAS = 16;
 constexpr int RLW_CTAS_FEW = 4;
 constexpr int RLW_GRID = 1024;
-constexpr int RLW_WARPS = RLW_CTAS * 4;  // candidates per long pair (the most warps)
+constexpr int RLW_CTAS_MAX = 256;
+constexpr int RLW_CTA_WARPS = 4;     // warps of a long-pair CTA (one candidate each)
+// a sub-batch with at most this many pairs in the first long-pair tier runs
+// them with a variant per warp (its lanes share each pass) instead of a
+// variant per lane: too few variants to fill the lanes otherwise
+constexpr int RLW_WIDE_MAX = 64;
 constexpr int RLW_CAND = 17;         // floats per warp candidate
+// CTAs per pair of a long-pair tier with `nlong` possible pairs: `base`, or
+// as many as fill RLW_GRID CTAs, at most RLW_CTAS_MAX
+inline int rlw_ctas_for(int base, int nlong) {
+    int c = nlong > 0 ? RLW_GRID / nlong : RLW_GRID;
+    c = c > base ? c : base;
+    return c < RLW_CTAS_MAX ? c : RLW_CTAS_MAX;
+}
 
 constexpr int DP_R4_MIN = 384;
 __host__ __device__ inline int dp_r(int lq) { return lq >= DP_R4_MIN ? 4 : 2; }

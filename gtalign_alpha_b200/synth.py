@@ -271,17 +271,18 @@ def na_moved_copy(rng: np.random.Generator, tmpl: Chain, sigma: float, name: str
 def write_pdb(ch: Chain, path: str) -> None:
     """Write a PDB file the reference reader accepts: C-alpha atoms of a
     protein, or C3' atoms of a nucleic acid (residue names "  A" etc., which
-    the reader takes for nucleotides)."""
+    the reader takes for nucleotides).  Residue numbers run 1..9999 and start
+    over (the field has four columns), so consecutive residues always differ."""
     lines = []
     for i in range(ch.length):
         x, y, z = (float(v) for v in ch.xyz[i])
         if ch.na:
             lines.append("ATOM  %5d  C3'   %s A%4d    %8.3f%8.3f%8.3f  1.00  0.00           C\n"
-                         % (i + 1, chr(int(ch.seq[i])), i + 1, x, y, z))
+                         % (i + 1, chr(int(ch.seq[i])), i % 9999 + 1, x, y, z))
             continue
         res = AA3[chr(int(ch.seq[i]))]
         lines.append("ATOM  %5d  CA  %3s A%4d    %8.3f%8.3f%8.3f  1.00  0.00           C\n"
-                     % (i + 1, res, i + 1, x, y, z))
+                     % (i + 1, res, i % 9999 + 1, x, y, z))
     lines.append("TER\nEND\n")
     with open(path, "w") as f:
         f.writelines(lines)

@@ -330,7 +330,10 @@ typedef struct {
     int seed_chunk;        /* seed offsets per CTA; a pair with more is split
                               over several CTAs (128..65536; default 512) */
     int refine_long_ctas;  /* CTAs per pair of the refinement's long-pair tier
-                              (pairs from 1,536 positions; 1..16; default 16) */
+                              (pairs from 1,536 positions; 1..16; default 16);
+                              raised, up to 256, where a sub-batch has so few
+                              such pairs that their launch would have fewer
+                              than 1,024 CTAs */
     int dp_cta_pairs;      /* pairs of each DP launch (its largest matrices)
                               run as a wavefront over a CTA's warps
                               (0..65536; default 592, 4 per SM) */
