@@ -995,7 +995,10 @@ extern "C" gtb_status gtb_autotune(gtb_handle* h, float scorethld, const gtb_blo
     };
     gtb_tuning cur = start;
     float curms = 0.f;
-    gtb_status s = time_one(cur, curms);
+    // one more untimed call first: the device's clocks and memory pool settle
+    // during the first calls, which would otherwise count against the start
+    gtb_status s = gtb_process_resident(h, scorethld, queries, refs, sc.rec, sc.tfm, nullptr);
+    if (s == GTB_OK) s = time_one(cur, curms);
     // one field at a time: its candidates with the others as they stand
     static const int c_seed[] = {256, 512, 1024, 2048};
     static const int c_rlw[] = {4, 8, 16};

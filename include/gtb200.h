@@ -349,8 +349,8 @@ gtb_status gtb_set_tuning(gtb_handle* h, const gtb_tuning* t);
  * shapes, one field at a time from the handle's current tuning (seed_chunk
  * 256/512/1024/2048, refine_long_ctas 4/8/16, dp_cta_pairs 0/296/592/1184,
  * sub_pairs 8192/16384/32768); a candidate replaces the field's value only
- * when its time, the least of `trials` calls after one untimed call, is
- * below 98% of the best so far.  Leaves the winner set on the handle and
+ * when its time, the least of `trials` calls after one untimed call (two
+ * for the starting tuning), is below 98% of the best so far.  Leaves the winner set on the handle and
  * returns it in *best and its time in *best_ms (either may be NULL).
  * `log`, when not NULL, receives up to `nlog` entries (the tuning tried
  * and its ms) and *nlogged their count.  Host wall time around the calls,
