@@ -50,6 +50,8 @@ references.  Legs of one run:
 * default_options: gtalign's default options (--speed 9, the spatial-index
   detailed search on) on the same workload, --defaults-steps steps over the
   first query chunks, and the reference's GPU build at those options.
+* reader: the host PDB reader (gtb_read_pdb) on the first --reader-files
+  references written as files, all host threads.
 
 Inputs (about 0.6 GB of coordinates and the pair state) are larger than L2
 between steps.  --impl reference times the reference's own CPU
@@ -481,8 +483,11 @@ def run_ours(args):
                          "dp_refine_loops": float(st_ms[2]), "final": float(st_ms[5]),
                          "total": float(st_ms[6])}}
 
-    long_chain = adjoint = cpu = refgpu = clustering = defaults = None
+    long_chain = adjoint = cpu = refgpu = clustering = defaults = reader = None
     if rank == 0 and ws == 1:
+        if "reader" in legs:
+            progress("host reader")
+            reader = reader_run(wl, args, r_all)
         if "refgpu" in legs:
             progress("reference GPU build")
             refgpu = reference_gpu_sample(wl, args, value)
@@ -538,6 +543,7 @@ def run_ours(args):
             "cpu_baseline": cpu,
             "reference_gpu": refgpu,
             "default_options": defaults,
+            "reader": reader,
             "clustering": clustering,
             "clocks": clocks,
             "workload_gen_s": gen_s,
@@ -938,6 +944,37 @@ def cluster_run(args):
         shutil.rmtree(d, ignore_errors=True)
 
 
+def reader_run(wl, args, r_all):
+    """The host reader (gtb_read_pdb): the first --reader-files references
+    of the workload written as PDB files, then read back on every host
+    thread (the files just written, so from the page cache); files,
+    residues and bytes per second, and the time the whole reference set
+    would take at that rate."""
+    from gtalign_alpha_b200 import synth
+    from gtalign_alpha_b200.api import read_pdb
+    nf = min(args.reader_files, len(wl.refs))
+    d = tempfile.mkdtemp(prefix="gtreader")
+    try:
+        paths = []
+        for i in range(nf):
+            paths.append(os.path.join(d, "r%06d.pdb" % i))
+            synth.write_pdb(wl.refs[i], paths[-1])
+        nbytes = sum(os.path.getsize(p) for p in paths)
+        read_pdb(paths[:64])                                  # library and threads warm
+        t0 = time.perf_counter()
+        rb = read_pdb(paths, threads=0)
+        dt = time.perf_counter() - t0
+        ok = rb.soa.n == nf and int(rb.soa.total) == int(sum(c.length for c in wl.refs[:nf]))
+        return {"value": nf / dt, "unit": "files/s", "residues_per_s": rb.soa.total / dt,
+                "mb_per_s": nbytes / dt / 1e6, "threads": os.cpu_count(), "files": nf,
+                "all_structures_read": bool(ok),
+                "reference_set_s_at_this_rate": r_all.n / (nf / dt),
+                "sample": "the first %d references of the workload as PDB files (%.0f MB), "
+                          "page cache warm" % (nf, nbytes / 1e6)}
+    finally:
+        shutil.rmtree(d, ignore_errors=True)
+
+
 def defaults_run(L, args, wl, qbs, rb, step_pairs, maxpairs, dev, legs):
     """gtalign's default options (--speed 9: the spatial-index detailed search
     on) on the headline workload, one GPU: a handle of its own (the blocks
@@ -1135,9 +1172,11 @@ def main():
                     help="long-chain pairs also run through the reference's GPU build (empty: none)")
     ap.add_argument("--cluster-n", type=int, default=1000,
                     help="structures of the all-against-all clustering leg")
-    ap.add_argument("--legs", default="unpolished,e2e,plain,long,adjoint,cpu,refgpu,cluster,defaults",
+    ap.add_argument("--legs", default="unpolished,e2e,plain,long,adjoint,cpu,refgpu,cluster,defaults,reader",
                     help="legs besides the headline: unpolished,e2e,plain,long,adjoint,cpu,refgpu,"
-                         "cluster,defaults")
+                         "cluster,defaults,reader")
+    ap.add_argument("--reader-files", type=int, default=4000,
+                    help="PDB files of the host-reader leg")
     ap.add_argument("--defaults-steps", type=int, default=2,
                     help="timed steps of the default-options leg (--speed 9)")
     args = ap.parse_args()

@@ -470,6 +470,83 @@ class ResidentBlock:
         self.free()
 
 
+class _CReaderOptions(ctypes.Structure):
+    _fields_ = [("ter", ctypes.c_int), ("split", ctypes.c_int), ("hetatm", ctypes.c_int),
+                ("mol", ctypes.c_int), ("aatom", ctypes.c_char * 5), ("natom", ctypes.c_char * 5),
+                ("minlen", ctypes.c_int), ("maxlen", ctypes.c_int)]
+
+
+@dataclass
+class ReadBlock:
+    """Structures read by read_pdb: the block as a SoA (for process_block),
+    its reference-layout fields as read (PackedBlock, for process_packed and
+    gtb_block_upload) and each structure's description."""
+    soa: SoA
+    packed: PackedBlock
+    descriptions: list
+
+
+def read_pdb(paths, ter: int = 3, split: int = 0, hetatm: bool = False, mol: int = 2,
+             aatom: str = " CA ", natom: str = " C3'", minlen: int = 20, maxlen: int = 65535,
+             threads: int = 0) -> ReadBlock:
+    """Read PDB files (plain or gzip) into one block (gtb_read_pdb), with the
+    reference's interpretation options (--ter, --split, --hetatm, --mol,
+    --aatom, --natom, --dev-min-length, --dev-max-length).  Host code."""
+    L = load_library()
+    L.gtb_read_pdb.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(_CReaderOptions),
+                               ctypes.c_int, ctypes.POINTER(ctypes.c_void_p), ctypes.c_char_p,
+                               ctypes.c_size_t]
+    L.gtb_read_pdb.restype = ctypes.c_int
+    L.gtb_structs_size.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int),
+                                   ctypes.POINTER(ctypes.c_longlong)]
+    L.gtb_structs_fields.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+    L.gtb_structs_description.argtypes = [ctypes.c_void_p, ctypes.c_int]
+    L.gtb_structs_description.restype = ctypes.c_char_p
+    L.gtb_structs_free.argtypes = [ctypes.c_void_p]
+    L.gtb_structs_free.restype = None
+    if len(aatom) != 4 or len(natom) != 4:
+        raise GTBError(1, "atom names have 4 characters")
+    o = _CReaderOptions(int(ter), int(split), int(bool(hetatm)), int(mol), aatom.encode(),
+                        natom.encode(), int(minlen), int(maxlen))
+    enc = [os.fsencode(p) for p in paths]
+    arr = (ctypes.c_char_p * max(1, len(enc)))(*enc)
+    h = ctypes.c_void_p()
+    err = ctypes.create_string_buffer(512)
+    st = L.gtb_read_pdb(ctypes.cast(arr, ctypes.c_void_p), len(enc), ctypes.byref(o), int(threads),
+                        ctypes.byref(h), err, 512)
+    if st != 0:
+        raise GTBError(st, err.value.decode())
+    try:
+        ns, npos = ctypes.c_int(), ctypes.c_longlong()
+        L.gtb_structs_size(h, ctypes.byref(ns), ctypes.byref(npos))
+        beg = (ctypes.c_void_p * NFIELDS)()
+        end = (ctypes.c_void_p * NFIELDS)()
+        L.gtb_structs_fields(h, beg, end)
+        dtypes = [np.int32, np.uint32, np.int32, np.float32, np.float32, np.float32, np.int32,
+                  np.int32, np.uint8, np.uint8]
+        arrays = []
+        for f, dt in enumerate(dtypes):
+            nb = (end[f] or 0) - (beg[f] or 0)
+            a = np.empty(nb // np.dtype(dt).itemsize, dt)
+            if nb:
+                ctypes.memmove(a.ctypes.data, beg[f], nb)
+            arrays.append(a)
+        desc = [L.gtb_structs_description(h, i).decode() for i in range(ns.value)]
+    finally:
+        L.gtb_structs_free(h)
+    pb = (ctypes.c_void_p * NFIELDS)()
+    pe = (ctypes.c_void_p * NFIELDS)()
+    for f, a in enumerate(arrays):
+        pb[f] = a.ctypes.data
+        pe[f] = a.ctypes.data + a.nbytes
+    packed = PackedBlock(arrays, pb, pe, ns.value, int(npos.value))
+    lens, offs = arrays[0], arrays[1].astype(np.int32)
+    first = arrays[6][offs] if ns.value else np.zeros(0, np.int32)
+    soa = SoA(lens.copy(), offs, arrays[3].copy(), arrays[4].copy(), arrays[5].copy(),
+              arrays[8].copy(), (first > 0).astype(np.int32))
+    return ReadBlock(soa, packed, desc)
+
+
 class _CClusterOptions(ctypes.Structure):
     _fields_ = [("linkage", ctypes.c_int), ("measure", ctypes.c_int),
                 ("threshold", ctypes.c_float), ("coverage", ctypes.c_float),

@@ -10,7 +10,7 @@ ROOT = os.path.dirname(PKG)
 CSRC = os.path.join(PKG, "csrc")
 LIB = os.path.join(PKG, "libgtb200.so")
 SOURCES = ["gtb_kernels.cu", "gtb_api.cu", "gtb_adjoint.cu", "gtb_noalloc.cu", "gtb_cluster.cu",
-           "gtb_index.cpp", "gtb_frg3.cu"]
+           "gtb_index.cpp", "gtb_frg3.cu", "gtb_reader.cpp"]
 HEADERS = ["gtb_device.cuh", "gtb_kernels.cuh", "gtb_gonnet.h"]
 
 NVCC_FLAGS = [
@@ -53,7 +53,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
         subprocess.check_call(cmd)
         objs.append(obj)
     tmp = LIB + ".tmp"
-    cmd = [nvcc(), "-shared", "-gencode", "arch=compute_100a,code=sm_100a", "-o", tmp] + objs + ["-lcudart"]
+    cmd = [nvcc(), "-shared", "-gencode", "arch=compute_100a,code=sm_100a", "-o", tmp] + objs + ["-lcudart", "-lz"]
     subprocess.check_call(cmd)
     os.replace(tmp, LIB)
     return LIB

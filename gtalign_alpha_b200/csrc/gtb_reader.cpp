@@ -1,0 +1,376 @@
+// gtb_reader.cpp -- host reader and packer: PDB structure files (plain or
+// gzip-compressed) into one block of the reference's SoA fields, the input of
+// gtb_process_block / gtb_block_upload.  Host code; files are parsed in
+// parallel on host threads and packed in file order.
+//
+// The record loop follows FlexDataRead::ReadDataPDB
+// (src/libgenp/gdats/FlexDataRead.cpp:285-560) step for step, including its
+// byte-offset line handling (myfiler.h:56-64: a skip of `by` bytes moves
+// past the end of the line it lands in, so a record shorter than the skip
+// also skips the next line), because the structures a file yields depend on
+// it: the --ter / --split rules, the alternate-location filter (' ' or 'A'),
+// ATOM (and, with --hetatm, HETATM) records of the --aatom / --natom atom,
+// the --mol molecule-type vote, the --dev-min-length / --dev-max-length
+// limits (PMBatchStrData.h:368-415, 440-460) and the description format
+// (PMBatchStrData.h:525-545).  Residue codes: ResName2Code
+// (src/libutil/alpha.cpp:65-75, 115-143).  Field values as AddOneResidue
+// writes them (PM2DVectorFields.h:40-41, 96-115): per residue
+// (insertion code << 16 | chain id << 8 | chain order), negated for protein
+// residues; per structure the length, the offset of its first residue and
+// the molecule-type vote (pps2DType outside clustering runs).
+// PDBx/mmCIF files are not read (GTB_ERR_UNSUPPORTED).
+
+#include <zlib.h>
+
+#include <algorithm>
+#include <atomic>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "gtb200.h"
+
+namespace {
+
+enum { TER_EOF = 0, TER_END = 1, TER_END_CHAIN = 2, TER_TER_END_CHAIN = 3 };
+enum { SPLIT_NONE = 0, SPLIT_MODEL = 1, SPLIT_CHAIN = 2 };
+
+// one-letter code of a residue name (3 characters at p)
+char res_code(const char* p) {
+    static const char* const names[] = {
+        "ALA", "DAL", "ASX", "CYS", "DCY", "ASP", "DAS", "GLU", "DGL", "PHE", "DPN", "GLY",
+        "HIS", "DHI", "ILE", "DIL", "LYS", "DLY", "LEU", "DLE", "MET", "MED", "MSE", "ASN",
+        "DSG", "PYL", "PRO", "DPR", "GLN", "DGN", "ARG", "DAR", "SER", "DSN", "THR", "DTH",
+        "SEC", "VAL", "DVA", "TRP", "DTR", "TYR", "DTY", "GLX"};
+    static const char codes[] = "AABCCDDEEFFGHHIIKKLLMMMNNOPPQQRRSSTTUVVWWYYZ";
+    for (size_t k = 0; k < sizeof(names) / sizeof(names[0]); k++)
+        if (p[0] == names[k][0] && p[1] == names[k][1] && p[2] == names[k][2]) return codes[k];
+    // names of one or two characters (nucleotides): the letter itself
+    if (p[0] == ' ') {
+        if (p[1] == ' ') return p[2] == ' ' ? 'X' : p[2];
+        return p[2] == ' ' ? p[1] : 'X';
+    }
+    return p[1] == ' ' ? p[0] : 'X';
+}
+
+struct Structure {
+    std::string desc;
+    std::vector<float> x, y, z;
+    std::vector<int> insch, resnum;
+    std::vector<char> rsd;
+    int moltype = 0;
+    void clear() {
+        x.clear(); y.clear(); z.clear(); insch.clear(); resnum.clear(); rsd.clear();
+    }
+};
+
+struct FileResult {
+    std::vector<Structure> strs;
+    std::string err;          // empty: read
+    int unsupported = 0;
+};
+
+bool read_all(const char* path, std::string& buf, std::string& err) {
+    gzFile f = gzopen(path, "rb");     // reads plain files as they are
+    if (!f) { err = std::string("cannot open ") + path; return false; }
+    buf.clear();
+    char tmp[1 << 16];
+    for (;;) {
+        int n = gzread(f, tmp, sizeof(tmp));
+        if (n < 0) { int e = 0; err = std::string(path) + ": " + gzerror(f, &e); gzclose(f); return false; }
+        if (n == 0) break;
+        buf.append(tmp, (size_t)n);
+    }
+    gzclose(f);
+    return true;
+}
+
+// the leading integer / number of a fixed-width field, as std::stoi / std::stof
+// read it (leading blanks skipped, trailing characters ignored); false: none
+bool field_int(const char* p, int w, int& v) {
+    std::string s(p, (size_t)w);
+    const char* c = s.c_str();
+    char* e = nullptr;
+    long r = std::strtol(c, &e, 10);
+    if (e == c) return false;
+    v = (int)r;
+    return true;
+}
+bool field_float(const char* p, int w, float& v) {
+    std::string s(p, (size_t)w);
+    const char* c = s.c_str();
+    char* e = nullptr;
+    float r = std::strtof(c, &e);
+    if (e == c) return false;
+    v = r;
+    return true;
+}
+
+void parse_pdb(const std::string& path, const std::string& data, const gtb_reader_options& o,
+               FileResult& out) {
+    const size_t terlnwidth = 26, sfflnwidth = 54, sffmodlnwidth = 12;
+    const int ter = o.ter, split = o.split;
+    const bool usechid = !(ter == TER_EOF && (split == SPLIT_NONE || split == SPLIT_MODEL));
+    const bool usemodn = !(ter == TER_EOF && split == SPLIT_NONE);
+    const char* data0 = data.data();
+    const size_t datlen = data.size();
+    size_t cur = 0;
+    auto incposnl = [&](size_t by) {
+        cur += by;
+        size_t p = cur;
+        while (p < datlen && data0[p] != '\n' && data0[p] != '\r') p++;
+        while (p < datlen && (data0[p] == '\n' || data0[p] == '\r')) p++;
+        cur = p;
+    };
+    int moltype = 0;
+    char chord = 0, prevchid = 0, prevchidx = 0;
+    std::string model, modelprev;
+    Structure s;
+    bool stop = false;          // file closed (the reader's Eof)
+    // FinalizeCrntStructure: 0 written, 1 empty, 2 short, 3 (never: too long
+    // structures are dropped while being added)
+    auto finalize = [&](char chain, const std::string& mdl) -> int {
+        const int n = (int)s.x.size();
+        int code = 0;
+        if (n < 1) code = 1;
+        else if (n < o.minlen) code = 2;
+        else {
+            std::string d = path;
+            if (usechid && chain) d += std::string(" Chn:") + chain;
+            if (usemodn && !mdl.empty()) d += " (M:" + mdl + ")";
+            s.desc = d;
+            s.moltype = moltype;
+            out.strs.push_back(s);
+        }
+        s.clear();
+        return code;
+    };
+    // a record's bytes past the end of the data read as zeros
+    auto at = [&](size_t k) -> char { return k < datlen ? data0[k] : '\0'; };
+    auto cmp = [&](size_t k, const char* lit) {
+        for (size_t i = 0; lit[i]; i++) if (at(k + i) != lit[i]) return false;
+        return true;
+    };
+    while (!stop && cur < datlen) {
+        const size_t p = cur;
+        const size_t datwidth = datlen - p;
+        if (datwidth < 3) { incposnl(0); continue; }
+        if (!s.x.empty()) {
+            if ((ter >= TER_END && cmp(p, "END")) || (ter >= TER_TER_END_CHAIN && cmp(p, "TER"))) {
+                stop = true;
+                break;
+            }
+        }
+        if (split > SPLIT_NONE && cmp(p, "END")) {
+            prevchid = 0;
+            incposnl(3);
+            continue;
+        }
+        if (cmp(p, "MODEL ") && datwidth > sffmodlnwidth) {
+            std::string m;
+            for (size_t i = 10; i < 14 && at(p + i) != '\n' && at(p + i) != '\r'; i++)
+                if (at(p + i) != ' ' && at(p + i) != '\t') m += at(p + i);
+            model = m;                  // at most the 4 characters of columns 11-14
+            incposnl(sffmodlnwidth);
+            continue;
+        }
+        if (datwidth < sfflnwidth || (at(p + 16) != ' ' && at(p + 16) != 'A')) {
+            incposnl(0);
+            continue;
+        }
+        if (!cmp(p, "ATOM  ") && (!o.hetatm || !cmp(p, "HETATM"))) {
+            incposnl(cmp(p, "TER") ? terlnwidth : sfflnwidth);
+            continue;
+        }
+        const bool isa = std::memcmp(data0 + p + 12, o.aatom, 4) == 0;
+        const bool isn = std::memcmp(data0 + p + 12, o.natom, 4) == 0;
+        if (!isa && !isn) {
+            incposnl(sfflnwidth);
+            continue;
+        }
+        const char chid = data0[p + 21], insc = data0[p + 26];
+        const char resd = res_code(data0 + p + 17);
+        int resnum = 0;
+        float c[3];
+        if (!field_int(data0 + p + 22, 4, resnum) || !field_float(data0 + p + 30, 8, c[0]) ||
+            !field_float(data0 + p + 38, 8, c[1]) || !field_float(data0 + p + 46, 8, c[2])) {
+            out.err = path + ": failed to read residue data";
+            return;
+        }
+        if (prevchid != chid) {
+            const bool cond1 = ter >= TER_END_CHAIN;
+            const bool cond2 = split == SPLIT_CHAIN || (prevchid == 0 && split == SPLIT_MODEL);
+            if (!s.x.empty() && (cond1 || cond2)) {
+                chord = 0;
+                const int code = finalize(prevchidx, modelprev);
+                if (code == 1) return;             // empty: the file is done
+                if (cond1) return;
+                moltype = 0;
+            }
+            modelprev = model;
+            prevchid = prevchidx = chid;
+            chord++;
+        }
+        int restype;
+        if (o.mol == 0) restype = -1;
+        else if (o.mol == 1) restype = 1;
+        else restype = (data0[p + 17] == ' ' && (data0[p + 18] == ' ' || data0[p + 18] == 'D')) ? 1 : -1;
+        moltype += restype;
+        // the length limits compare the residues stored before this one
+        // (PMBatchStrData.h:377-385)
+        const int nprev = (int)s.x.size();
+        if ((o.maxlen > 0 && o.maxlen < nprev) || 65535 < nprev) {
+            s.clear();                             // too long: dropped, the file is done
+            return;
+        }
+        int v = (int)((((unsigned)(unsigned char)insc & 0xffu) << 16) |
+                      (((unsigned)(unsigned char)chid & 0xffu) << 8) | ((unsigned)(unsigned char)chord & 0xffu));
+        v = std::abs(v);
+        if (restype <= 0) v = -v;
+        s.x.push_back(c[0]); s.y.push_back(c[1]); s.z.push_back(c[2]);
+        s.insch.push_back(v);
+        s.resnum.push_back(resnum);
+        s.rsd.push_back(resd);
+        incposnl(sfflnwidth);
+    }
+    finalize(prevchidx, modelprev);
+}
+
+bool looks_like_cif(const std::string& d) {
+    size_t k = 0;
+    while (k < d.size() && (d[k] == ' ' || d[k] == '\t' || d[k] == '\n' || d[k] == '\r')) k++;
+    return d.compare(k, 5, "data_") == 0;
+}
+
+}  // namespace
+
+struct gtb_structs {
+    std::vector<Structure> strs;
+    std::vector<int> len, type, insch, resnum;
+    std::vector<unsigned> dist;
+    std::vector<float> x, y, z;
+    std::vector<char> rsd, ss;
+    std::string err;
+};
+
+extern "C" void gtb_reader_default_options(gtb_reader_options* o) {
+    if (!o) return;
+    std::memset(o, 0, sizeof(*o));
+    o->ter = TER_TER_END_CHAIN;
+    o->split = SPLIT_NONE;
+    o->hetatm = 0;
+    o->mol = 2;
+    std::memcpy(o->aatom, " CA ", 5);
+    std::memcpy(o->natom, " C3'", 5);
+    o->minlen = 20;
+    o->maxlen = 65535;
+}
+
+extern "C" gtb_status gtb_read_pdb(const char* const* paths, int npaths,
+                                   const gtb_reader_options* opts, int nthreads,
+                                   gtb_structs** out, char* err, size_t errlen) {
+    auto fail = [&](gtb_status st, const std::string& m) {
+        if (err && errlen) std::snprintf(err, errlen, "%s", m.c_str());
+        return st;
+    };
+    if (!out || npaths < 0 || (npaths > 0 && !paths)) return fail(GTB_ERR_ARG, "bad arguments");
+    *out = nullptr;
+    gtb_reader_options o;
+    if (opts) o = *opts;
+    else gtb_reader_default_options(&o);
+    if (o.ter < 0 || o.ter > 3 || o.split < 0 || o.split > 2 || o.mol < 0 || o.mol > 2 ||
+        o.minlen < 1 || o.maxlen < 0 || o.maxlen > 65535)
+        return fail(GTB_ERR_ARG, "reader option out of range");
+    for (int i = 0; i < npaths; i++)
+        if (!paths[i]) return fail(GTB_ERR_ARG, "null path");
+    std::vector<FileResult> res((size_t)npaths);
+    int nt = nthreads > 0 ? nthreads : (int)std::thread::hardware_concurrency();
+    if (nt < 1) nt = 1;
+    if (nt > npaths) nt = npaths > 0 ? npaths : 1;
+    std::atomic<int> next{0};
+    auto work = [&]() {
+        std::string buf;
+        for (int i = next++; i < npaths; i = next++) {
+            FileResult& r = res[(size_t)i];
+            if (!read_all(paths[i], buf, r.err)) continue;
+            if (looks_like_cif(buf)) { r.unsupported = 1; continue; }
+            parse_pdb(paths[i], buf, o, r);
+        }
+    };
+    std::vector<std::thread> th;
+    for (int t = 1; t < nt; t++) th.emplace_back(work);
+    work();
+    for (auto& t : th) t.join();
+    for (int i = 0; i < npaths; i++) {
+        if (res[(size_t)i].unsupported)
+            return fail(GTB_ERR_UNSUPPORTED, std::string(paths[i]) + ": PDBx/mmCIF input is not read here");
+        if (!res[(size_t)i].err.empty()) return fail(GTB_ERR_ARG, res[(size_t)i].err);
+    }
+    gtb_structs* b = new gtb_structs();
+    size_t ns = 0, np = 0;
+    for (auto& r : res) {
+        ns += r.strs.size();
+        for (auto& s : r.strs) np += s.x.size();
+    }
+    b->strs.reserve(ns);
+    b->len.reserve(ns); b->dist.reserve(ns); b->type.reserve(ns);
+    b->x.reserve(np); b->y.reserve(np); b->z.reserve(np);
+    b->insch.reserve(np); b->resnum.reserve(np); b->rsd.reserve(np);
+    for (auto& r : res)
+        for (auto& s : r.strs) {
+            b->len.push_back((int)s.x.size());
+            b->dist.push_back((unsigned)b->x.size());
+            b->type.push_back(s.moltype);
+            b->x.insert(b->x.end(), s.x.begin(), s.x.end());
+            b->y.insert(b->y.end(), s.y.begin(), s.y.end());
+            b->z.insert(b->z.end(), s.z.begin(), s.z.end());
+            b->insch.insert(b->insch.end(), s.insch.begin(), s.insch.end());
+            b->resnum.insert(b->resnum.end(), s.resnum.begin(), s.resnum.end());
+            b->rsd.insert(b->rsd.end(), s.rsd.begin(), s.rsd.end());
+            Structure meta;
+            meta.desc = s.desc;
+            meta.moltype = s.moltype;
+            b->strs.push_back(std::move(meta));
+            s.clear();
+        }
+    b->ss.assign(b->x.size(), 0);
+    *out = b;
+    return GTB_OK;
+}
+
+extern "C" gtb_status gtb_structs_size(const gtb_structs* b, int* nstr, long long* npos) {
+    if (!b) return GTB_ERR_ARG;
+    if (nstr) *nstr = (int)b->len.size();
+    if (npos) *npos = (long long)b->x.size();
+    return GTB_OK;
+}
+
+extern "C" gtb_status gtb_structs_fields(gtb_structs* b, char** pmbeg, char** pmend) {
+    if (!b || !pmbeg || !pmend) return GTB_ERR_ARG;
+    auto set = [&](int f, void* p, size_t bytes) {
+        pmbeg[f] = (char*)p;
+        pmend[f] = (char*)p + bytes;
+    };
+    const size_t n = b->len.size(), N = b->x.size();
+    set(GTB_FLD_LEN, b->len.data(), n * sizeof(int));
+    set(GTB_FLD_DIST, b->dist.data(), n * sizeof(unsigned));
+    set(GTB_FLD_TYPE, b->type.data(), n * sizeof(int));
+    set(GTB_FLD_X, b->x.data(), N * sizeof(float));
+    set(GTB_FLD_Y, b->y.data(), N * sizeof(float));
+    set(GTB_FLD_Z, b->z.data(), N * sizeof(float));
+    set(GTB_FLD_INSCHORD, b->insch.data(), N * sizeof(int));
+    set(GTB_FLD_RESNUM, b->resnum.data(), N * sizeof(int));
+    set(GTB_FLD_RSD, b->rsd.data(), N);
+    set(GTB_FLD_SS, b->ss.data(), N);
+    return GTB_OK;
+}
+
+extern "C" const char* gtb_structs_description(const gtb_structs* b, int i) {
+    if (!b || i < 0 || (size_t)i >= b->strs.size()) return nullptr;
+    return b->strs[(size_t)i].desc.c_str();
+}
+
+extern "C" void gtb_structs_free(gtb_structs* b) { delete b; }

@@ -365,6 +365,40 @@ gtb_status gtb_autotune(gtb_handle* h, float scorethld, const gtb_block* queries
 
 void gtb_destroy(gtb_handle* h);
 
+/* Host reader and packer (replaces, for callers without the reference's
+ * reader, FlexDataRead::ReadDataPDB + PMBatchStrData::AddOneResidue /
+ * FinalizeCrntStructure, src/libgenp/gdats/FlexDataRead.cpp:285-560,
+ * PMBatchStrData.h:368-545): PDB files, plain or gzip-compressed, parsed on
+ * `nthreads` host threads (0: all cores) into one block of the SoA fields
+ * above, structures in file order, as the reference's reader produces them
+ * under the same interpretation options.  PDBx/mmCIF files are refused
+ * (GTB_ERR_UNSUPPORTED).  Host code; needs no device. */
+typedef struct {
+    int ter;          /* --ter: 0 end of file, 1 ENDMDL/END, 2 + chain change,
+                         3 + TER (default 3) */
+    int split;        /* --split: 0 none, 1 each MODEL, 2 each chain (default 0) */
+    int hetatm;       /* --hetatm: HETATM records too (default 0) */
+    int mol;          /* --mol: 0 protein, 1 nucleic acid, 2 by residue name (default 2) */
+    char aatom[5];    /* --aatom, 4 characters (default " CA ") */
+    char natom[5];    /* --natom, 4 characters (default " C3'") */
+    int minlen;       /* --dev-min-length: shorter structures are dropped (default 20) */
+    int maxlen;       /* --dev-max-length: longer ones are dropped (default 65535;
+                         the reference's default for references is 4000) */
+} gtb_reader_options;
+typedef struct gtb_structs gtb_structs;
+void gtb_reader_default_options(gtb_reader_options* o);
+/* err: a message of at most errlen bytes on failure (may be NULL). */
+gtb_status gtb_read_pdb(const char* const* paths, int npaths, const gtb_reader_options* opts,
+                        int nthreads, gtb_structs** out, char* err, size_t errlen);
+gtb_status gtb_structs_size(const gtb_structs* b, int* nstr, long long* npos);
+/* The block's GTB_NFIELDS field pointers (the pmbeg/pmend arrays that
+ * gtb_process_block and gtb_block_upload take), valid until gtb_structs_free. */
+gtb_status gtb_structs_fields(gtb_structs* b, char** pmbeg, char** pmend);
+/* Structure i's description: the path, " Chn:<id>" and " (M:<model>)" as the
+ * reference's reader forms it (PMBatchStrData.h:525-545). */
+const char* gtb_structs_description(const gtb_structs* b, int i);
+void gtb_structs_free(gtb_structs* b);
+
 /* Clustering of n structures from the records of their all-against-all
  * block (queries = references = the n structures, record (q, i) at
  * (q*n + i)*GTB_NOUT), as the reference's clustering writer does it

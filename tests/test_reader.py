@@ -1,0 +1,128 @@
+"""The host reader (gtb_read_pdb) against the reference's own reader.
+
+tests/golden/reader_cases.json holds, for each interpretation option set,
+the structures the reference's CPU build read from a set of crafted PDB
+files (description, length, sequence; tests/golden/make_reader_golden.py):
+chains split or joined by TER / END / ENDMDL / chain changes, models,
+alternate locations, HETATM residues, insertion codes, a nucleic-acid
+chain, unknown residue names, a chain below the minimum length, short
+records, lengths around --dev-max-length.  The reader must yield exactly
+those structures.  Host code: no device needed.
+"""
+import gzip
+import json
+import os
+import shutil
+import sys
+
+import numpy as np
+import pytest
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(HERE, "golden"))
+
+FIX = os.path.join(HERE, "golden", "reader_cases.json")
+
+
+def _opts(flags):
+    kw = {}
+    for f in flags:
+        if f == "--hetatm":
+            kw["hetatm"] = True
+        elif f.startswith("--dev-max-length="):
+            kw["maxlen"] = int(f.split("=")[1])
+        else:
+            k, v = f[2:].split("=")
+            kw[k] = int(v)
+    return kw
+
+
+@pytest.fixture(scope="module")
+def cases(tmp_path_factory):
+    import make_reader_golden as mrg
+    d = str(tmp_path_factory.mktemp("reader"))
+    names = mrg.write_cases(d)
+    return d, names
+
+
+@pytest.mark.parametrize("key", ["default", "hetatm", "ter0", "ter1", "ter2", "split1", "split2",
+                                 "split2ter1", "ter0max100"])
+def test_reader_reads_what_the_reference_reads(cases, key):
+    from gtalign_alpha_b200.api import read_pdb
+    fx = json.load(open(FIX))
+    d, names = cases
+    assert names == fx["files"]
+    rb = read_pdb([os.path.join(d, n) for n in names], threads=3, **_opts(fx["sets"][key]["options"]))
+    s = rb.soa
+    ours = []
+    for i, desc in enumerate(rb.descriptions):
+        o, n = int(s.offs[i]), int(s.lens[i])
+        seq = bytes(s.rsd[o:o + n]).decode()
+        ours.append([os.path.relpath(desc, d), n, seq])
+    assert sorted(ours) == sorted([list(t) for t in fx["sets"][key]["structures"]])
+
+
+def test_reader_round_trip_and_layout(tmp_path):
+    """Chains written by synth.write_pdb (one file each, one gzip-compressed)
+    come back with their coordinates (to the file's 3 decimals), residue
+    letters, lengths and offsets; the packed fields have the reference's
+    layout (per-residue insertion/chain/order value negated for protein)."""
+    from gtalign_alpha_b200 import synth
+    from gtalign_alpha_b200.api import read_pdb
+    rng = np.random.default_rng(5)
+    chains = synth.random_chains(rng, [35, 120, 60, 250], "r")
+    paths = []
+    for k, c in enumerate(chains):
+        p = str(tmp_path / ("s%d.pdb" % k))
+        synth.write_pdb(c, p)
+        if k == 1:
+            with open(p, "rb") as f, gzip.open(p + ".gz", "wb") as g:
+                shutil.copyfileobj(f, g)
+            p += ".gz"
+        paths.append(p)
+    for threads in (1, 4):
+        rb = read_pdb(paths, threads=threads)
+        s = rb.soa
+        assert s.n == 4 and list(s.lens) == [c.length for c in chains]
+        assert list(s.offs) == list(np.cumsum([0] + [c.length for c in chains])[:-1])
+        xyz = np.stack([s.x, s.y, s.z], 1)
+        ref = np.concatenate([c.xyz for c in chains]).astype(np.float32)
+        assert np.abs(xyz - np.round(ref.astype(np.float64), 3)).max() < 1e-4
+        assert bytes(s.rsd).decode() == "".join(bytes(c.seq).decode() for c in chains)
+        assert (s.mol == 0).all()
+        pk = rb.packed
+        assert pk.n == 4 and pk.npos == s.total
+        insch = pk.arrays[6]
+        assert (insch < 0).all()                      # protein residues
+        assert ((-insch >> 8) & 0xff == ord("A")).all() and ((-insch) & 0xff == 1).all()
+        assert rb.descriptions[0] == paths[0] + " Chn:A"
+
+
+def test_reader_refuses_mmcif_and_missing_files(tmp_path):
+    from gtalign_alpha_b200.api import GTBError, read_pdb
+    p = tmp_path / "x.cif"
+    p.write_text("data_1ABC\nloop_\n_atom_site.group_PDB\n")
+    with pytest.raises(GTBError) as e:
+        read_pdb([str(p)])
+    assert e.value.status == 4
+    with pytest.raises(GTBError) as e:
+        read_pdb([str(tmp_path / "nope.pdb")])
+    assert e.value.status == 1
+    with pytest.raises(GTBError):
+        read_pdb([str(p)], ter=7)
+
+
+def test_reader_length_limits(tmp_path):
+    """--dev-min-length drops shorter structures; --dev-max-length drops a
+    structure once more residues than the limit are stored before the next
+    one (the reference's comparison, which admits one residue above it)."""
+    from gtalign_alpha_b200 import synth
+    from gtalign_alpha_b200.api import read_pdb
+    rng = np.random.default_rng(6)
+    paths = []
+    for k, n in enumerate((19, 20, 100, 101, 102)):
+        c = synth.random_chains(rng, [n], "m")[0]
+        paths.append(str(tmp_path / ("m%d.pdb" % k)))
+        synth.write_pdb(c, paths[-1])
+    rb = read_pdb(paths, maxlen=100)
+    assert list(rb.soa.lens) == [20, 100, 101]
