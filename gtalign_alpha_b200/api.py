@@ -473,7 +473,7 @@ class ResidentBlock:
 class _CReaderOptions(ctypes.Structure):
     _fields_ = [("ter", ctypes.c_int), ("split", ctypes.c_int), ("hetatm", ctypes.c_int),
                 ("mol", ctypes.c_int), ("aatom", ctypes.c_char * 5), ("natom", ctypes.c_char * 5),
-                ("minlen", ctypes.c_int), ("maxlen", ctypes.c_int)]
+                ("minlen", ctypes.c_int), ("maxlen", ctypes.c_int), ("infmt", ctypes.c_int)]
 
 
 @dataclass
@@ -488,10 +488,11 @@ class ReadBlock:
 
 def read_pdb(paths, ter: int = 3, split: int = 0, hetatm: bool = False, mol: int = 2,
              aatom: str = " CA ", natom: str = " C3'", minlen: int = 20, maxlen: int = 65535,
-             threads: int = 0) -> ReadBlock:
-    """Read PDB files (plain or gzip) into one block (gtb_read_pdb), with the
-    reference's interpretation options (--ter, --split, --hetatm, --mol,
-    --aatom, --natom, --dev-min-length, --dev-max-length).  Host code."""
+             infmt: int = 0, threads: int = 0) -> ReadBlock:
+    """Read PDB and PDBx/mmCIF files (plain or gzip) into one block
+    (gtb_read_pdb), with the reference's interpretation options (--ter,
+    --split, --hetatm, --mol, --aatom, --natom, --dev-min-length,
+    --dev-max-length, --infmt).  Host code."""
     L = load_library()
     L.gtb_read_pdb.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(_CReaderOptions),
                                ctypes.c_int, ctypes.POINTER(ctypes.c_void_p), ctypes.c_char_p,
@@ -507,7 +508,7 @@ def read_pdb(paths, ter: int = 3, split: int = 0, hetatm: bool = False, mol: int
     if len(aatom) != 4 or len(natom) != 4:
         raise GTBError(1, "atom names have 4 characters")
     o = _CReaderOptions(int(ter), int(split), int(bool(hetatm)), int(mol), aatom.encode(),
-                        natom.encode(), int(minlen), int(maxlen))
+                        natom.encode(), int(minlen), int(maxlen), int(infmt))
     enc = [os.fsencode(p) for p in paths]
     arr = (ctypes.c_char_p * max(1, len(enc)))(*enc)
     h = ctypes.c_void_p()

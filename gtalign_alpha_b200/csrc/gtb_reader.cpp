@@ -18,7 +18,13 @@
 // (insertion code << 16 | chain id << 8 | chain order), negated for protein
 // residues; per structure the length, the offset of its first residue and
 // the molecule-type vote (pps2DType outside clustering runs).
-// PDBx/mmCIF files are not read (GTB_ERR_UNSUPPORTED).
+// PDBx/mmCIF files follow FlexDataRead::ReadDataCIF (FlexDataRead.cpp:553-
+// 930): the _atom_site loop's columns, tokens of a record's first 128
+// characters, the model / chain changes as structure ends.  The format comes
+// from the file name as InputFilelist::GetFileTypeFromFilename decides it
+// (InputFilelist.h:147-174: .cif / .cif.gz are PDBx/mmCIF, anything else
+// PDB, unless the --infmt option says which); files under 10 bytes are
+// skipped (InputFilelist.h AddFile); tar archives are refused.
 
 #include <zlib.h>
 
@@ -239,10 +245,211 @@ void parse_pdb(const std::string& path, const std::string& data, const gtb_reade
     finalize(prevchidx, modelprev);
 }
 
-bool looks_like_cif(const std::string& d) {
-    size_t k = 0;
-    while (k < d.size() && (d[k] == ' ' || d[k] == '\t' || d[k] == '\n' || d[k] == '\r')) k++;
-    return d.compare(k, 5, "data_") == 0;
+// the _atom_site columns the reader uses (FlexDataRead.h's field indices)
+enum CifField { CF_GROUP, CF_ATOM, CF_ALT, CF_COMP, CF_LASYM, CF_LSEQ, CF_INS, CF_X, CF_Y, CF_Z,
+                CF_ASEQ, CF_AASYM, CF_MODEL, CF_SET, CF_N };
+
+void parse_cif(const std::string& path, const std::string& data, const gtb_reader_options& o,
+               FileResult& out) {
+    const size_t maxlnwidth = 128, sfflnwidth = 54;
+    const int ter = o.ter, split = o.split;
+    const bool usechid = !(ter == TER_EOF && (split == SPLIT_NONE || split == SPLIT_MODEL));
+    const bool usemodn = !(ter == TER_EOF && split == SPLIT_NONE);
+    // the trimmed atom names
+    auto trim = [](const char* a) {
+        std::string t(a, strnlen(a, 4));
+        size_t b = t.find_first_not_of(' '), e = t.find_last_not_of(' ');
+        return b == std::string::npos ? std::string() : t.substr(b, e - b + 1);
+    };
+    const std::string satom = trim(o.aatom), natom = trim(o.natom);
+    const char* d0 = data.data();
+    const size_t datlen = data.size();
+    auto at = [&](size_t k) -> char { return k < datlen ? d0[k] : '\0'; };
+    size_t cur = 0;
+    auto incposnl = [&](size_t by) {
+        cur += by;
+        size_t p = cur;
+        while (p < datlen && d0[p] != '\n' && d0[p] != '\r') p++;
+        while (p < datlen && (d0[p] == '\n' || d0[p] == '\r')) p++;
+        cur = p;
+    };
+    int fld[CF_N];
+    auto reset = [&]() { for (int& f : fld) f = -1; };
+    reset();
+    auto pre = [&](size_t p, size_t dw, const char* lit) {
+        const size_t n = std::strlen(lit);
+        if (dw < n) return false;
+        for (size_t i = 0; i < n; i++) if (at(p + i) != lit[i]) return false;
+        return true;
+    };
+    auto isspc = [](char c) { return c == ' ' || c == '\t' || c == '\n' || c == '\r' || c == '\v' || c == '\f'; };
+    auto set_field = [&](size_t p, size_t dw, int ndx) {
+        if (pre(p, dw, "group_PDB")) fld[CF_GROUP] = ndx;
+        else if (pre(p, dw, "label_atom_id")) fld[CF_ATOM] = ndx;
+        else if (pre(p, dw, "label_alt_id")) fld[CF_ALT] = ndx;
+        else if (pre(p, dw, "label_comp_id")) fld[CF_COMP] = ndx;
+        else if (pre(p, dw, "label_asym_id")) fld[CF_LASYM] = ndx;
+        else if (pre(p, dw, "label_seq_id")) fld[CF_LSEQ] = ndx;
+        else if (pre(p, dw, "pdbx_PDB_ins_code")) fld[CF_INS] = ndx;
+        else if (pre(p, dw, "Cartn_x") && isspc(at(p + 7))) fld[CF_X] = ndx;
+        else if (pre(p, dw, "Cartn_y") && isspc(at(p + 7))) fld[CF_Y] = ndx;
+        else if (pre(p, dw, "Cartn_z") && isspc(at(p + 7))) fld[CF_Z] = ndx;
+        else if (pre(p, dw, "auth_seq_id")) fld[CF_ASEQ] = ndx;
+        else if (pre(p, dw, "auth_asym_id")) fld[CF_AASYM] = ndx;
+        else if (pre(p, dw, "pdbx_PDB_model_num")) fld[CF_MODEL] = ndx;
+        if (0 <= fld[CF_GROUP] && 0 <= fld[CF_ATOM] && 0 <= fld[CF_COMP] &&
+            (0 <= fld[CF_AASYM] || 0 <= fld[CF_LASYM]) && (0 <= fld[CF_ASEQ] || 0 <= fld[CF_LSEQ]) &&
+            0 <= fld[CF_X] && 0 <= fld[CF_Y] && 0 <= fld[CF_Z])
+            fld[CF_SET] = 1;
+    };
+    // the atom name token matches `atom` (an opening quote skipped)
+    auto check_atom = [&](size_t pt, const std::string& atom) {
+        if (at(pt) == '"') pt++;
+        for (size_t i = 0; i < atom.size(); i++) if (atom[i] != at(pt++)) return false;
+        const char c = at(pt);
+        return c == '"' || c == ' ' || c == '\t' || c == '\n' || c == '\r';
+    };
+    std::string modelprev(4, '\0'), chainprev(5, '\0'), model, chain;
+    int loop = -1, moltype = 0;
+    char chord = 0;
+    Structure s;
+    auto finalize = [&](const std::string& ch, const std::string& mdl) -> int {
+        const int n = (int)s.x.size();
+        int code = 0;
+        if (n < 1) code = 1;
+        else if (n < o.minlen) code = 2;
+        else {
+            std::string d = path;
+            if (usechid && ch.size() && ch[0]) d += " Chn:" + ch;
+            if (usemodn && mdl.size() && mdl[0]) d += " (M:" + mdl + ")";
+            s.desc = d;
+            s.moltype = moltype;
+            out.strs.push_back(s);
+        }
+        s.clear();
+        return code;
+    };
+    std::vector<size_t> tk, te;
+    tk.reserve(maxlnwidth); te.reserve(maxlnwidth);
+    while (cur < datlen) {
+        const size_t pbeg = cur;
+        size_t p = pbeg;
+        const size_t datwidth = datlen - p;
+        if (datwidth < 5 || d0[p] == '#') { reset(); incposnl(0); continue; }
+        if (pre(p, datwidth, "loop_")) { reset(); loop = 0; incposnl(5); continue; }
+        if (0 <= loop && (datwidth < 11 || !pre(p, datwidth, "_atom_site."))) loop = -1;
+        if (0 <= loop) { set_field(p + 11, datwidth - 11, loop++); incposnl(11); continue; }
+        if (fld[CF_SET] <= 0) { incposnl(0); continue; }
+        // tokens of the record's first maxlnwidth characters
+        tk.clear(); te.clear();
+        for (const size_t pmax = p + maxlnwidth; p < datlen && p < pmax && d0[p] != '\n' && d0[p] != '\r';) {
+            for (; p < datlen && p < pmax && (d0[p] == ' ' || d0[p] == '\t'); p++) {}
+            tk.push_back(p);
+            for (; p < datlen && p < pmax && d0[p] != ' ' && d0[p] != '\t' && d0[p] != '\n' && d0[p] != '\r'; p++) {}
+            te.push_back(p);
+        }
+        const int nt = (int)tk.size();
+        auto skip = [&]() { incposnl(p - pbeg); };
+        if (nt < 1 || datwidth < sfflnwidth) { skip(); continue; }
+        auto tok = [&](int f) { return tk[(size_t)fld[f]]; };
+        auto toklen = [&](int f) { return te[(size_t)fld[f]] - tk[(size_t)fld[f]]; };
+        if (nt <= fld[CF_GROUP] || (!pre(tok(CF_GROUP), datlen - tok(CF_GROUP), "ATOM") &&
+                                    (!o.hetatm || !pre(tok(CF_GROUP), datlen - tok(CF_GROUP), "HETATM")))) {
+            skip(); continue;
+        }
+        if (0 <= fld[CF_ALT] && (nt <= fld[CF_ALT] || (at(tok(CF_ALT)) != '.' && at(tok(CF_ALT)) != 'A'))) {
+            skip(); continue;
+        }
+        if (nt <= fld[CF_ATOM] || (!check_atom(tok(CF_ATOM), satom) && !check_atom(tok(CF_ATOM), natom))) {
+            skip(); continue;
+        }
+        if (nt <= fld[CF_X] || nt <= fld[CF_Y] || nt <= fld[CF_Z] || nt <= fld[CF_LSEQ] ||
+            nt <= fld[CF_LASYM] || nt <= fld[CF_COMP]) {
+            skip(); continue;
+        }
+        int fa = CF_LASYM;
+        if (0 <= fld[CF_AASYM] && fld[CF_AASYM] < nt) fa = CF_AASYM;
+        if (toklen(fa) < 1) { out.err = path + ": invalid PDBx/mmCIF file format"; return; }
+        chain.assign(d0 + tok(fa), toklen(fa));
+        char chid = chain[0];
+        if (chid == '.') chid = ' ';
+        char insc = ' ';
+        if (0 <= fld[CF_INS] && fld[CF_INS] < nt) insc = at(tok(CF_INS));
+        if (insc == '?') insc = ' ';
+        char nm[3] = {at(tok(CF_COMP)), at(tok(CF_COMP) + 1), at(tok(CF_COMP) + 2)};
+        const char resd = res_code(nm);
+        int fs = CF_LSEQ;
+        if (0 <= fld[CF_ASEQ] && fld[CF_ASEQ] < nt) fs = CF_ASEQ;
+        int resnum = 0;
+        float c[3];
+        if (!field_int(d0 + tok(fs), (int)toklen(fs), resnum) ||
+            !field_float(d0 + tok(CF_X), (int)toklen(CF_X), c[0]) ||
+            !field_float(d0 + tok(CF_Y), (int)toklen(CF_Y), c[1]) ||
+            !field_float(d0 + tok(CF_Z), (int)toklen(CF_Z), c[2])) {
+            out.err = path + ": failed to read residue data";
+            return;
+        }
+        bool seteof = false, fin = false;
+        if (0 <= fld[CF_MODEL] && fld[CF_MODEL] < nt) {
+            model.assign(d0 + tok(CF_MODEL), toklen(CF_MODEL));
+            if (model != modelprev) {
+                if (ter >= TER_END) { fin = true; seteof = true; }
+                if (split > SPLIT_NONE) fin = true;
+            }
+        }
+        if (chain != chainprev) {
+            if (ter >= TER_END_CHAIN) { fin = true; seteof = true; }
+            if (split >= SPLIT_CHAIN) fin = true;
+            chord++;
+        }
+        if (fin && !s.x.empty()) {
+            chord = 1;
+            const int code = finalize(chainprev, modelprev);
+            if (code == 1) return;
+            if (seteof) return;
+            moltype = 0;
+        }
+        modelprev = model;
+        chainprev = chain;
+        int restype;
+        if (o.mol == 0) restype = -1;
+        else if (o.mol == 1) restype = 1;
+        else restype = (toklen(CF_COMP) < 2 || at(tok(CF_COMP)) == 'D') ? 1 : -1;
+        moltype += restype;
+        const int nprev = (int)s.x.size();
+        if ((o.maxlen > 0 && o.maxlen < nprev) || 65535 < nprev) { s.clear(); return; }
+        int v = (int)((((unsigned)(unsigned char)insc & 0xffu) << 16) |
+                      (((unsigned)(unsigned char)chid & 0xffu) << 8) | ((unsigned)(unsigned char)chord & 0xffu));
+        v = std::abs(v);
+        if (restype <= 0) v = -v;
+        s.x.push_back(c[0]); s.y.push_back(c[1]); s.z.push_back(c[2]);
+        s.insch.push_back(v);
+        s.resnum.push_back(resnum);
+        s.rsd.push_back(resd);
+        skip();
+    }
+    finalize(chainprev, modelprev);
+}
+
+bool ends_with(const std::string& a, const char* b) {
+    const size_t n = std::strlen(b);
+    return n < a.size() && a.compare(a.size() - n, n, b) == 0;
+}
+
+// 0 PDB, 1 PDBx/mmCIF, 2 tar (refused)
+int file_format(const std::string& name, int infmt) {
+    if (ends_with(name, ".gz")) {
+        if (infmt == 1) return 0;
+        if (infmt == 2) return 1;
+        if (ends_with(name, ".pdb.gz") || ends_with(name, ".ent.gz")) return 0;
+        if (ends_with(name, ".cif.gz")) return 1;
+        return 0;
+    }
+    if (ends_with(name, ".tar")) return 2;
+    if (infmt == 1) return 0;
+    if (infmt == 2) return 1;
+    if (ends_with(name, ".cif")) return 1;
+    return 0;
 }
 
 }  // namespace
@@ -267,6 +474,7 @@ extern "C" void gtb_reader_default_options(gtb_reader_options* o) {
     std::memcpy(o->natom, " C3'", 5);
     o->minlen = 20;
     o->maxlen = 65535;
+    o->infmt = 0;
 }
 
 extern "C" gtb_status gtb_read_pdb(const char* const* paths, int npaths,
@@ -282,8 +490,13 @@ extern "C" gtb_status gtb_read_pdb(const char* const* paths, int npaths,
     if (opts) o = *opts;
     else gtb_reader_default_options(&o);
     if (o.ter < 0 || o.ter > 3 || o.split < 0 || o.split > 2 || o.mol < 0 || o.mol > 2 ||
-        o.minlen < 1 || o.maxlen < 0 || o.maxlen > 65535)
+        o.minlen < 1 || o.maxlen < 0 || o.maxlen > 65535 || o.infmt < 0 || o.infmt > 2)
         return fail(GTB_ERR_ARG, "reader option out of range");
+    // the command line's combinations (gtalign.cpp:693-709)
+    if (o.split == SPLIT_MODEL && o.ter != TER_EOF)
+        return fail(GTB_ERR_ARG, "--split=1 is only compatible with --ter=0");
+    if (o.split == SPLIT_CHAIN && o.ter >= TER_END_CHAIN)
+        return fail(GTB_ERR_ARG, "--split=2 is only compatible with --ter=0|1");
     for (int i = 0; i < npaths; i++)
         if (!paths[i]) return fail(GTB_ERR_ARG, "null path");
     std::vector<FileResult> res((size_t)npaths);
@@ -295,9 +508,18 @@ extern "C" gtb_status gtb_read_pdb(const char* const* paths, int npaths,
         std::string buf;
         for (int i = next++; i < npaths; i = next++) {
             FileResult& r = res[(size_t)i];
+            const int fmt = file_format(paths[i], o.infmt);
+            if (fmt == 2) { r.unsupported = 1; continue; }
+            FILE* f = std::fopen(paths[i], "rb");
+            if (f) {
+                std::fseek(f, 0, SEEK_END);
+                const long sz = std::ftell(f);
+                std::fclose(f);
+                if (sz >= 0 && sz < 10) continue;          // too small to list
+            }
             if (!read_all(paths[i], buf, r.err)) continue;
-            if (looks_like_cif(buf)) { r.unsupported = 1; continue; }
-            parse_pdb(paths[i], buf, o, r);
+            if (fmt == 1) parse_cif(paths[i], buf, o, r);
+            else parse_pdb(paths[i], buf, o, r);
         }
     };
     std::vector<std::thread> th;
@@ -306,7 +528,7 @@ extern "C" gtb_status gtb_read_pdb(const char* const* paths, int npaths,
     for (auto& t : th) t.join();
     for (int i = 0; i < npaths; i++) {
         if (res[(size_t)i].unsupported)
-            return fail(GTB_ERR_UNSUPPORTED, std::string(paths[i]) + ": PDBx/mmCIF input is not read here");
+            return fail(GTB_ERR_UNSUPPORTED, std::string(paths[i]) + ": tar archives are not read here");
         if (!res[(size_t)i].err.empty()) return fail(GTB_ERR_ARG, res[(size_t)i].err);
     }
     gtb_structs* b = new gtb_structs();

@@ -367,16 +367,18 @@ void gtb_destroy(gtb_handle* h);
 
 /* Host reader and packer (replaces, for callers without the reference's
  * reader, FlexDataRead::ReadDataPDB + PMBatchStrData::AddOneResidue /
- * FinalizeCrntStructure, src/libgenp/gdats/FlexDataRead.cpp:285-560,
- * PMBatchStrData.h:368-545): PDB files, plain or gzip-compressed, parsed on
+ * FinalizeCrntStructure, src/libgenp/gdats/FlexDataRead.cpp:285-930,
+ * PMBatchStrData.h:368-545): PDB and PDBx/mmCIF files, plain or
+ * gzip-compressed, parsed on
  * `nthreads` host threads (0: all cores) into one block of the SoA fields
  * above, structures in file order, as the reference's reader produces them
- * under the same interpretation options.  PDBx/mmCIF files are refused
+ * under the same interpretation options.  Tar archives are refused
  * (GTB_ERR_UNSUPPORTED).  Host code; needs no device. */
 typedef struct {
     int ter;          /* --ter: 0 end of file, 1 ENDMDL/END, 2 + chain change,
                          3 + TER (default 3) */
-    int split;        /* --split: 0 none, 1 each MODEL, 2 each chain (default 0) */
+    int split;        /* --split: 0 none, 1 each MODEL (with ter 0), 2 each chain
+                         (with ter 0 or 1) (default 0) */
     int hetatm;       /* --hetatm: HETATM records too (default 0) */
     int mol;          /* --mol: 0 protein, 1 nucleic acid, 2 by residue name (default 2) */
     char aatom[5];    /* --aatom, 4 characters (default " CA ") */
@@ -384,6 +386,8 @@ typedef struct {
     int minlen;       /* --dev-min-length: shorter structures are dropped (default 20) */
     int maxlen;       /* --dev-max-length: longer ones are dropped (default 65535;
                          the reference's default for references is 4000) */
+    int infmt;        /* --infmt: 0 by the file name (.cif, .cif.gz: PDBx/mmCIF;
+                         else PDB), 1 PDB, 2 PDBx/mmCIF (default 0) */
 } gtb_reader_options;
 typedef struct gtb_structs gtb_structs;
 void gtb_reader_default_options(gtb_reader_options* o);

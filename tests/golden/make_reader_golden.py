@@ -72,6 +72,46 @@ def chain_lines(rng, n, chain, start=1, rec_of=None, alts=None, icodes=None, nam
     return out
 
 
+CIF_COLS = ["group_PDB", "id", "type_symbol", "label_atom_id", "label_alt_id", "label_comp_id",
+            "label_asym_id", "label_entity_id", "label_seq_id", "pdbx_PDB_ins_code", "Cartn_x",
+            "Cartn_y", "Cartn_z", "occupancy", "B_iso_or_equiv", "auth_seq_id", "auth_asym_id",
+            "pdbx_PDB_model_num"]
+
+
+def cif_file(rows, cols=CIF_COLS, pad=1):
+    """A PDBx/mmCIF text with one _atom_site loop; rows are dicts of column
+    values ('.' where absent); `pad` spaces between tokens."""
+    out = ["data_TEST\n", "#\n", "_entry.id TEST\n", "#\n", "loop_\n"]
+    out += ["_atom_site.%s \n" % c for c in cols]
+    for r in rows:
+        out.append((" " * pad).join(str(r.get(c, ".")) for c in cols) + "\n")
+    out.append("#\n")
+    return out
+
+
+def cif_chain(rng, n, label_asym, auth_asym, model=1, seq0=1, rec_of=None, alts=None,
+              icodes=None, names=None, atomname="CA", extra_atoms=False):
+    c = synth.random_chains(rng, [n], "c")[0]
+    rows = []
+    for i in range(n):
+        res = names[i] if names else AA3[int(rng.integers(0, 20))]
+        base = {"group_PDB": rec_of(i) if rec_of else "ATOM", "type_symbol": "C",
+                "label_comp_id": res, "label_asym_id": label_asym, "label_entity_id": 1,
+                "label_seq_id": seq0 + i, "pdbx_PDB_ins_code": icodes[i] if icodes else "?",
+                "occupancy": "1.00", "B_iso_or_equiv": "0.00", "auth_seq_id": seq0 + i,
+                "auth_asym_id": auth_asym, "pdbx_PDB_model_num": model}
+        if extra_atoms:
+            rows.append(dict(base, label_atom_id="N", label_alt_id=".",
+                             Cartn_x="%.3f" % (c.xyz[i][0] + 1), Cartn_y="%.3f" % c.xyz[i][1],
+                             Cartn_z="%.3f" % c.xyz[i][2]))
+        for alt in (alts(i) if alts else ["."]):
+            sh = 0.0 if alt in ".A" else 0.4
+            rows.append(dict(base, label_atom_id=atomname, label_alt_id=alt,
+                             Cartn_x="%.3f" % (c.xyz[i][0] + sh), Cartn_y="%.3f" % c.xyz[i][1],
+                             Cartn_z="%.3f" % c.xyz[i][2]))
+    return rows
+
+
 def ter_line(full=True):
     return "TER     999      ALA A 999                                                      \n" if full else "TER\n"
 
@@ -107,7 +147,30 @@ def write_cases(d: str) -> list:
     files["l_blank_chain.pdb"] = chain_lines(rng, 40, " ") + ["END\n"]
     for n in (100, 101, 102):                # around --dev-max-length=100
         files["m_len%d.pdb" % n] = chain_lines(rng, n, "A") + ["END\n"]
+    # PDBx/mmCIF
+    files["n_cif_plain.cif"] = cif_file(cif_chain(rng, 70, "A", "A", extra_atoms=True))
+    files["o_cif_two_chains.cif"] = cif_file(cif_chain(rng, 50, "A", "X") + cif_chain(rng, 40, "B", "Y"))
+    files["p_cif_models.cif"] = cif_file(cif_chain(rng, 45, "A", "A", model=1) +
+                                         cif_chain(rng, 45, "A", "A", model=2))
+    files["q_cif_altloc_hetatm.cif"] = cif_file(cif_chain(
+        rng, 60, "A", "A", alts=lambda i: ["A", "B"] if 5 <= i < 9 else (["C"] if i == 12 else ["."]),
+        rec_of=lambda i: "HETATM" if 30 <= i < 34 else "ATOM",
+        names=[("MSE" if 30 <= i < 34 else ("DAL" if i == 40 else AA3[i % 20])) for i in range(60)]))
+    files["r_cif_rna.cif"] = cif_file(cif_chain(rng, 40, "A", "A", atomname='"C3\'"',
+                                                names=["ACGU"[i % 4] for i in range(40)]))
+    files["s_cif_icodes_label_only.cif"] = cif_file(
+        cif_chain(rng, 35, "A", "A", icodes=[("B" if i % 6 == 2 else "?") for i in range(35)]),
+        cols=[c for c in CIF_COLS if not c.startswith("auth_")])
+    # tokens past a record's 128th character are not read: with wide spacing
+    # the chain, number and model come from the label columns or not at all
+    files["t_cif_wide.cif"] = cif_file(cif_chain(rng, 30, "A", "Z", model=3), pad=7)
+    files["u_cif.gz"] = cif_file(cif_chain(rng, 25, "A", "A"))     # .gz without .cif: read as PDB
     for name, lines in files.items():
+        if name.endswith(".gz"):
+            import gzip
+            with gzip.open(os.path.join(d, name), "wt") as f:
+                f.writelines(lines)
+            continue
         with open(os.path.join(d, name), "w") as f:
             f.writelines(lines)
     return sorted(files)

@@ -98,18 +98,24 @@ def test_reader_round_trip_and_layout(tmp_path):
         assert rb.descriptions[0] == paths[0] + " Chn:A"
 
 
-def test_reader_refuses_mmcif_and_missing_files(tmp_path):
+def test_reader_refuses_tar_and_missing_files(tmp_path):
     from gtalign_alpha_b200.api import GTBError, read_pdb
     p = tmp_path / "x.cif"
     p.write_text("data_1ABC\nloop_\n_atom_site.group_PDB\n")
+    assert read_pdb([str(p)]).soa.n == 0                  # no complete atom table
+    t = tmp_path / "x.tar"
+    t.write_bytes(b"0" * 1024)
     with pytest.raises(GTBError) as e:
-        read_pdb([str(p)])
+        read_pdb([str(t)])
     assert e.value.status == 4
     with pytest.raises(GTBError) as e:
         read_pdb([str(tmp_path / "nope.pdb")])
     assert e.value.status == 1
     with pytest.raises(GTBError):
         read_pdb([str(p)], ter=7)
+    for bad in (dict(split=1, ter=1), dict(split=2, ter=2), dict(split=2)):   # the CLI's rules
+        with pytest.raises(GTBError):
+            read_pdb([str(p)], **bad)
 
 
 def test_reader_length_limits(tmp_path):
