@@ -73,13 +73,13 @@ def test_pack_fields_layout():
 
 
 def test_python_structs_match_the_c_header(tmp_path):
-    """The ctypes mirrors of gtb_options, gtb_results, gtb_tuning and
-    gtb_tuning_trial have the C header's field offsets and sizes (compiled
-    with the host C compiler)."""
+    """The ctypes mirrors of gtb_options, gtb_results, gtb_tuning,
+    gtb_tuning_trial and gtb_reader_options have the C header's field offsets
+    and sizes (compiled with the host C compiler)."""
     import subprocess
-    from gtalign_alpha_b200.api import _COptions, _CResults, Tuning, _CTuningTrial
+    from gtalign_alpha_b200.api import _COptions, _CReaderOptions, _CResults, Tuning, _CTuningTrial
     structs = (("gtb_options", _COptions), ("gtb_results", _CResults), ("gtb_tuning", Tuning),
-               ("gtb_tuning_trial", _CTuningTrial))
+               ("gtb_tuning_trial", _CTuningTrial), ("gtb_reader_options", _CReaderOptions))
     src = tmp_path / "layout.c"
     lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "gtb200.h"', "int main(void) {"]
     for cname, py in structs:
