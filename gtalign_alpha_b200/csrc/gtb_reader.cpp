@@ -24,7 +24,11 @@
 // from the file name as InputFilelist::GetFileTypeFromFilename decides it
 // (InputFilelist.h:147-174: .cif / .cif.gz are PDBx/mmCIF, anything else
 // PDB, unless the --infmt option says which); files under 10 bytes are
-// skipped (InputFilelist.h AddFile); tar archives are refused.
+// skipped (InputFilelist.h AddFile).  Tar archives are read entry by entry
+// as InputFilelist::AddFilesFromTAR lists them (InputFilelist.cpp:95-200:
+// regular files of 10 bytes to 128 MB, a bad header checksum ends the list,
+// each entry's format from its name, gzip entries inflated), the
+// description being "<archive>:<entry>" (FlexDataRead.h:219-222).
 
 #include <zlib.h>
 
@@ -76,8 +80,18 @@ struct Structure {
 struct FileResult {
     std::vector<Structure> strs;
     std::string err;          // empty: read
-    int unsupported = 0;
 };
+
+bool read_raw(const char* path, std::string& buf) {
+    FILE* f = std::fopen(path, "rb");
+    if (!f) return false;
+    buf.clear();
+    char tmp[1 << 16];
+    size_t n;
+    while ((n = std::fread(tmp, 1, sizeof(tmp), f)) > 0) buf.append(tmp, n);
+    std::fclose(f);
+    return true;
+}
 
 bool read_all(const char* path, std::string& buf, std::string& err) {
     gzFile f = gzopen(path, "rb");     // reads plain files as they are
@@ -431,6 +445,62 @@ void parse_cif(const std::string& path, const std::string& data, const gtb_reade
     finalize(chainprev, modelprev);
 }
 
+// gzip data in memory -> out
+bool gunzip(const std::string& in, std::string& out) {
+    z_stream zs;
+    std::memset(&zs, 0, sizeof(zs));
+    if (inflateInit2(&zs, 16 + MAX_WBITS) != Z_OK) return false;
+    zs.next_in = (Bytef*)in.data();
+    zs.avail_in = (uInt)in.size();
+    out.clear();
+    char tmp[1 << 16];
+    int rc = Z_OK;
+    while (rc == Z_OK) {
+        zs.next_out = (Bytef*)tmp;
+        zs.avail_out = sizeof(tmp);
+        rc = inflate(&zs, Z_NO_FLUSH);
+        if (rc != Z_OK && rc != Z_STREAM_END) { inflateEnd(&zs); return false; }
+        out.append(tmp, sizeof(tmp) - zs.avail_out);
+        if (rc == Z_OK && zs.avail_in == 0 && zs.avail_out != 0) break;   // truncated input
+    }
+    inflateEnd(&zs);
+    return true;
+}
+
+struct TarEntry { std::string name; size_t pos, size; };
+
+// the regular-file entries of a tar archive (as AddFilesFromTAR lists them)
+bool tar_entries(const std::string& tar, std::vector<TarEntry>& ents) {
+    const size_t HS = 512;
+    auto oct = [&](size_t at, int w) {
+        size_t r = 0;
+        const char* h = tar.data() + at;
+        for (; !('0' <= *h && *h <= '7') && 0 < w; h++, w--) {}
+        for (; ('0' <= *h && *h <= '7') && 0 < w; h++, w--) r = 8 * r + (size_t)(*h - '0');
+        return r;
+    };
+    size_t pos = 0;
+    for (;;) {
+        if (pos + HS > tar.size()) return pos == tar.size();    // ill-formed unless at the end
+        const unsigned char* h = (const unsigned char*)tar.data() + pos;
+        int sum = 0, sumfld = 0;
+        for (size_t n = 0; n < HS; n++) sum += h[n];
+        for (size_t n = 148; n < 156; n++) sumfld += h[n];
+        if (sum == 0) return true;                              // the end marker
+        const int chk = (int)oct(pos + 148, 8);
+        if (sum - sumfld + 8 * 32 != chk) return true;          // corrupted: the list ends
+        const int type = (int)h[156];
+        const size_t size = oct(pos + 124, 12);
+        const size_t start = pos + HS;
+        pos = start + (size + 511) / 512 * 512;
+        if (type != '0' && type != 0) continue;
+        if (size < 10 || size > ((size_t)128 << 20)) continue;
+        if (start + size > tar.size()) return false;
+        std::string name((const char*)h, strnlen((const char*)h, 100));
+        ents.push_back({name, start, size});
+    }
+}
+
 bool ends_with(const std::string& a, const char* b) {
     const size_t n = std::strlen(b);
     return n < a.size() && a.compare(a.size() - n, n, b) == 0;
@@ -509,7 +579,27 @@ extern "C" gtb_status gtb_read_pdb(const char* const* paths, int npaths,
         for (int i = next++; i < npaths; i = next++) {
             FileResult& r = res[(size_t)i];
             const int fmt = file_format(paths[i], o.infmt);
-            if (fmt == 2) { r.unsupported = 1; continue; }
+            if (fmt == 2) {
+                std::string tar, ent;
+                if (!read_raw(paths[i], tar)) { r.err = std::string("cannot read ") + paths[i]; continue; }
+                std::vector<TarEntry> ents;
+                if (!tar_entries(tar, ents)) { r.err = std::string(paths[i]) + ": ill-formed tar archive"; continue; }
+                for (const TarEntry& e : ents) {
+                    const int efmt = file_format(e.name, o.infmt);
+                    if (efmt == 2) continue;
+                    std::string raw = tar.substr(e.pos, e.size);
+                    if (ends_with(e.name, ".gz")) {
+                        if (!gunzip(raw, ent)) { r.err = std::string(paths[i]) + ":" + e.name + ": bad gzip data"; break; }
+                    } else {
+                        ent.swap(raw);
+                    }
+                    const std::string desc = std::string(paths[i]) + ":" + e.name;
+                    if (efmt == 1) parse_cif(desc, ent, o, r);
+                    else parse_pdb(desc, ent, o, r);
+                    if (!r.err.empty()) break;
+                }
+                continue;
+            }
             FILE* f = std::fopen(paths[i], "rb");
             if (f) {
                 std::fseek(f, 0, SEEK_END);
@@ -526,11 +616,8 @@ extern "C" gtb_status gtb_read_pdb(const char* const* paths, int npaths,
     for (int t = 1; t < nt; t++) th.emplace_back(work);
     work();
     for (auto& t : th) t.join();
-    for (int i = 0; i < npaths; i++) {
-        if (res[(size_t)i].unsupported)
-            return fail(GTB_ERR_UNSUPPORTED, std::string(paths[i]) + ": tar archives are not read here");
+    for (int i = 0; i < npaths; i++)
         if (!res[(size_t)i].err.empty()) return fail(GTB_ERR_ARG, res[(size_t)i].err);
-    }
     gtb_structs* b = new gtb_structs();
     size_t ns = 0, np = 0;
     for (auto& r : res) {

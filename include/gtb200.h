@@ -372,8 +372,8 @@ void gtb_destroy(gtb_handle* h);
  * gzip-compressed, parsed on
  * `nthreads` host threads (0: all cores) into one block of the SoA fields
  * above, structures in file order, as the reference's reader produces them
- * under the same interpretation options.  Tar archives are refused
- * (GTB_ERR_UNSUPPORTED).  Host code; needs no device. */
+ * under the same interpretation options; tar archives are read entry by
+ * entry (descriptions "<archive>:<entry>").  Host code; needs no device. */
 typedef struct {
     int ter;          /* --ter: 0 end of file, 1 ENDMDL/END, 2 + chain change,
                          3 + TER (default 3) */

@@ -112,6 +112,11 @@ def cif_chain(rng, n, label_asym, auth_asym, model=1, seq0=1, rec_of=None, alts=
     return rows
 
 
+def _gz(b: bytes) -> bytes:
+    import gzip
+    return gzip.compress(b, mtime=0)
+
+
 def ter_line(full=True):
     return "TER     999      ALA A 999                                                      \n" if full else "TER\n"
 
@@ -165,6 +170,24 @@ def write_cases(d: str) -> list:
     # the chain, number and model come from the label columns or not at all
     files["t_cif_wide.cif"] = cif_file(cif_chain(rng, 30, "A", "Z", model=3), pad=7)
     files["u_cif.gz"] = cif_file(cif_chain(rng, 25, "A", "A"))     # .gz without .cif: read as PDB
+    # a tar archive: a PDB, a PDBx/mmCIF and a gzip-compressed PDB entry, a
+    # directory entry and a file under 10 bytes
+    tar_entries = [("t1.pdb", "".join(chain_lines(rng, 33, "A") + ["END\n"]).encode()),
+                   ("sub/t2.cif", "".join(cif_file(cif_chain(rng, 28, "B", "B"))).encode()),
+                   ("t3.pdb.gz", _gz("".join(chain_lines(rng, 41, "C") + ["END\n"]).encode())),
+                   ("tiny.pdb", b"END\n")]
+    import io
+    import tarfile
+    with tarfile.open(os.path.join(d, "v_archive.tar"), "w", format=tarfile.USTAR_FORMAT) as t:
+        di = tarfile.TarInfo("sub")
+        di.type = tarfile.DIRTYPE
+        di.mtime = 0
+        t.addfile(di)
+        for name, data in tar_entries:
+            ti = tarfile.TarInfo(name)
+            ti.size = len(data)
+            ti.mtime = 0
+            t.addfile(ti, io.BytesIO(data))
     for name, lines in files.items():
         if name.endswith(".gz"):
             import gzip
@@ -173,7 +196,7 @@ def write_cases(d: str) -> list:
             continue
         with open(os.path.join(d, name), "w") as f:
             f.writelines(lines)
-    return sorted(files)
+    return sorted(list(files) + ["v_archive.tar"])
 
 
 def run_reference(d: str, opts: list) -> list:
