@@ -672,6 +672,7 @@ def long_chain_run(g, args):
     g.process_block(synth.pack(warm.queries), synth.pack(warm.refs), scorethld=0.5)
     per = []
     tot = 0.0
+    g.set_kernel_timing(True)       # the per-family split of each pair's device time
     for i in range(q.n):
         qi, ri = subset(q, np.array([i])), subset(r, np.array([i]))
         t0 = time.perf_counter()
@@ -679,9 +680,12 @@ def long_chain_run(g, args):
         wall = time.perf_counter() - t0
         tot += wall
         rec = res.alndata[0, 0]
+        kms = g.last_kernel_ms()
         per.append({"length": int(lengths[i]), "wall_s": wall, "tm_q": float(rec[9]), "tm_r": float(rec[10]),
                     "rmsd": float(rec[8]), "aligned": int(rec[4]),
-                    "err_tm": float(res.numerr[0, 0, :2].max()), "err_rmsd": float(res.numerr[0, 0, 2])})
+                    "err_tm": float(res.numerr[0, 0, :2].max()), "err_rmsd": float(res.numerr[0, 0, 2]),
+                    "kernel_ms": {"seed": float(kms[0]), "refine": float(kms[1]), "dp": float(kms[2])}})
+    g.set_kernel_timing(False)
     out = {"value": q.n / tot, "unit": "pairs/s", "total_s": tot, "pairs": per,
            "form": "batched + adjoint polishing (%d steps), alignment rows" % args.polish_steps,
            "published_reference": "GTalign on a T4: 65.12 s for a 37,860-residue pair (other "
