@@ -111,20 +111,49 @@ bool read_all(const char* path, std::string& buf, std::string& err) {
 // the leading integer / number of a fixed-width field, as std::stoi / std::stof
 // read it (leading blanks skipped, trailing characters ignored); false: none
 bool field_int(const char* p, int w, int& v) {
-    std::string s(p, (size_t)w);
-    const char* c = s.c_str();
+    char s[32];
+    const int n = w < 31 ? w : 31;
+    std::memcpy(s, p, (size_t)n);
+    s[n] = 0;
     char* e = nullptr;
-    long r = std::strtol(c, &e, 10);
-    if (e == c) return false;
+    long r = std::strtol(s, &e, 10);
+    if (e == s) return false;
     v = (int)r;
     return true;
 }
 bool field_float(const char* p, int w, float& v) {
-    std::string s(p, (size_t)w);
-    const char* c = s.c_str();
+    // the common form, [blanks][sign]digits[.digits] with at most 9 digits and
+    // 6 decimals: m / 10^d in double is the correctly rounded quotient (both
+    // exact in double; Clinger's fast path), and its rounding to float is the
+    // correctly rounded float of the decimal (a decimal of at most 6 places
+    // lies at least ulp/(2*10^6) from any float midpoint it is not equal to,
+    // far beyond the double's error), so this equals strtof
+    int k = 0;
+    while (k < w && (p[k] == ' ' || p[k] == '\t')) k++;
+    bool neg = false;
+    if (k < w && (p[k] == '-' || p[k] == '+')) { neg = p[k] == '-'; k++; }
+    long long m = 0;
+    int nd = 0, dec = -1, j = k;
+    for (; j < w; j++) {
+        const char c = p[j];
+        if (c >= '0' && c <= '9') { m = m * 10 + (c - '0'); nd++; if (dec >= 0) dec++; }
+        else if (c == '.' && dec < 0) dec = 0;
+        else break;
+    }
+    const bool end = j == w || p[j] == ' ' || p[j] == '\t' || p[j] == '\n' || p[j] == '\r';
+    if (nd > 0 && nd <= 9 && dec <= 6 && end) {
+        static const double p10[7] = {1e0, 1e1, 1e2, 1e3, 1e4, 1e5, 1e6};
+        const double q = (double)m / p10[dec < 0 ? 0 : dec];
+        v = (float)(neg ? -q : q);
+        return true;
+    }
+    char s[32];
+    const int n = w < 31 ? w : 31;
+    std::memcpy(s, p, (size_t)n);
+    s[n] = 0;
     char* e = nullptr;
-    float r = std::strtof(c, &e);
-    if (e == c) return false;
+    float r = std::strtof(s, &e);
+    if (e == s) return false;
     v = r;
     return true;
 }

@@ -131,3 +131,50 @@ def test_reader_length_limits(tmp_path):
         synth.write_pdb(c, paths[-1])
     rb = read_pdb(paths, maxlen=100)
     assert list(rb.soa.lens) == [20, 100, 101]
+
+
+def test_coordinate_parser_equals_strtof(tmp_path):
+    """The reader's fast decimal path gives strtof's float for every
+    coordinate a PDB record can hold (-999.999 .. 9999.999 in steps of
+    0.001, the "%8.3f" field) and for random decimals of up to 6 places and
+    9 digits (compiled with the host compiler around the reader's source)."""
+    import subprocess
+    src = tmp_path / "fp.cpp"
+    src.write_text(r'''
+#include "%s"
+#include <random>
+int main() {
+    char buf[32];
+    long bad = 0, n = 0;
+    for (long m = -999999; m <= 9999999; m++) {
+        std::snprintf(buf, sizeof buf, "%%8.3f", m / 1000.0);
+        float a = 0.f, b = std::strtof(buf, nullptr);
+        if (!field_float(buf, 8, a) || std::memcmp(&a, &b, 4) != 0) bad++;
+        n++;
+    }
+    std::mt19937_64 g(7);
+    for (int k = 0; k < 3000000; k++) {
+        int d = (int)(g() %% 7), nd = 1 + (int)(g() %% 9);
+        if (d > nd) d = nd;
+        long long m = (long long)(g() %% 1000000000ULL);
+        long long lim = 1; for (int i = 0; i < nd; i++) lim *= 10;
+        m %%= lim;
+        char digits[16];
+        std::snprintf(digits, sizeof digits, "%%0*lld", nd, m);
+        std::string s = (g() & 1) ? "-" : " ";
+        s += std::string(digits, (size_t)(nd - d));
+        if (d) s += "." + std::string(digits + nd - d, (size_t)d);
+        float a = 0.f, b = std::strtof(s.c_str(), nullptr);
+        if (!field_float(s.c_str(), (int)s.size(), a) || std::memcmp(&a, &b, 4) != 0) bad++;
+        n++;
+    }
+    std::printf("%%ld %%ld\n", n, bad);
+    return bad != 0;
+}
+''' % os.path.join(os.path.dirname(HERE), "gtalign_alpha_b200", "csrc", "gtb_reader.cpp"))
+    exe = tmp_path / "fp"
+    subprocess.check_call(["g++", "-O2", "-std=c++17", "-I", os.path.join(os.path.dirname(HERE), "include"),
+                           "-o", str(exe), str(src), "-lz", "-lpthread"])
+    out = subprocess.run([str(exe)], capture_output=True, text=True)
+    n, bad = (int(x) for x in out.stdout.split())
+    assert n > 13_000_000 and bad == 0, out.stdout
