@@ -56,8 +56,17 @@ char res_code(const char* p) {
         "DSG", "PYL", "PRO", "DPR", "GLN", "DGN", "ARG", "DAR", "SER", "DSN", "THR", "DTH",
         "SEC", "VAL", "DVA", "TRP", "DTR", "TYR", "DTY", "GLX"};
     static const char codes[] = "AABCCDDEEFFGHHIIKKLLMMMNNOPPQQRRSSTTUVVWWYYZ";
-    for (size_t k = 0; k < sizeof(names) / sizeof(names[0]); k++)
-        if (p[0] == names[k][0] && p[1] == names[k][1] && p[2] == names[k][2]) return codes[k];
+    // the names are three capital letters: a 26^3 table, built once
+    static const std::vector<char> table = []() {
+        std::vector<char> t(26 * 26 * 26, 0);
+        for (size_t k = 0; k < sizeof(names) / sizeof(names[0]); k++)
+            t[(size_t)((names[k][0] - 'A') * 676 + (names[k][1] - 'A') * 26 + (names[k][2] - 'A'))] = codes[k];
+        return t;
+    }();
+    if (p[0] >= 'A' && p[0] <= 'Z' && p[1] >= 'A' && p[1] <= 'Z' && p[2] >= 'A' && p[2] <= 'Z') {
+        const char c = table[(size_t)((p[0] - 'A') * 676 + (p[1] - 'A') * 26 + (p[2] - 'A'))];
+        if (c) return c;
+    }
     // names of one or two characters (nucleotides): the letter itself
     if (p[0] == ' ') {
         if (p[1] == ' ') return p[2] == ' ' ? 'X' : p[2];
@@ -111,6 +120,19 @@ bool read_all(const char* path, std::string& buf, std::string& err) {
 // the leading integer / number of a fixed-width field, as std::stoi / std::stof
 // read it (leading blanks skipped, trailing characters ignored); false: none
 bool field_int(const char* p, int w, int& v) {
+    // the common form: [blanks][sign] up to 9 digits
+    int k = 0;
+    while (k < w && (p[k] == ' ' || p[k] == '\t' || p[k] == '\n' || p[k] == '\r' ||
+                     p[k] == '\v' || p[k] == '\f')) k++;
+    bool neg = false;
+    if (k < w && (p[k] == '-' || p[k] == '+')) { neg = p[k] == '-'; k++; }
+    int nd = 0;
+    long r0 = 0;
+    for (; k < w && p[k] >= '0' && p[k] <= '9' && nd < 10; k++, nd++) r0 = r0 * 10 + (p[k] - '0');
+    if (nd > 0 && nd <= 9 && !(k < w && p[k] >= '0' && p[k] <= '9')) {
+        v = (int)(neg ? -r0 : r0);
+        return true;
+    }
     char s[32];
     const int n = w < 31 ? w : 31;
     std::memcpy(s, p, (size_t)n);
@@ -178,6 +200,9 @@ void parse_pdb(const std::string& path, const std::string& data, const gtb_reade
     char chord = 0, prevchid = 0, prevchidx = 0;
     std::string model, modelprev;
     Structure s;
+    const size_t guess = data.size() / 81 + 1;  // a residue per 80-column record, at most
+    s.x.reserve(guess); s.y.reserve(guess); s.z.reserve(guess);
+    s.insch.reserve(guess); s.resnum.reserve(guess); s.rsd.reserve(guess);
     bool stop = false;          // file closed (the reader's Eof)
     // FinalizeCrntStructure: 0 written, 1 empty, 2 short, 3 (never: too long
     // structures are dropped while being added)
@@ -636,7 +661,13 @@ extern "C" gtb_status gtb_read_pdb(const char* const* paths, int npaths,
                 std::fclose(f);
                 if (sz >= 0 && sz < 10) continue;          // too small to list
             }
-            if (!read_all(paths[i], buf, r.err)) continue;
+            // gzip by the name, as the reference decides it; other files as they are
+            if (ends_with(paths[i], ".gz")) {
+                if (!read_all(paths[i], buf, r.err)) continue;
+            } else if (!read_raw(paths[i], buf)) {
+                r.err = std::string("cannot open ") + paths[i];
+                continue;
+            }
             if (fmt == 1) parse_cif(paths[i], buf, o, r);
             else parse_pdb(paths[i], buf, o, r);
         }

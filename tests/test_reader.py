@@ -137,7 +137,9 @@ def test_coordinate_parser_equals_strtof(tmp_path):
     """The reader's fast decimal path gives strtof's float for every
     coordinate a PDB record can hold (-999.999 .. 9999.999 in steps of
     0.001, the "%8.3f" field) and for random decimals of up to 6 places and
-    9 digits (compiled with the host compiler around the reader's source)."""
+    9 digits, and its integer path strtol's value for every "%4d" residue
+    number and a few odd fields (compiled with the host compiler around the
+    reader's source)."""
     import subprocess
     src = tmp_path / "fp.cpp"
     src.write_text(r'''
@@ -166,6 +168,21 @@ int main() {
         if (d) s += "." + std::string(digits + nd - d, (size_t)d);
         float a = 0.f, b = std::strtof(s.c_str(), nullptr);
         if (!field_float(s.c_str(), (int)s.size(), a) || std::memcmp(&a, &b, 4) != 0) bad++;
+        n++;
+    }
+    for (long m = -999; m <= 9999; m++) {                 // the "%%4d" residue number field
+        std::snprintf(buf, sizeof buf, "%%4ld", m);
+        int a = 0;
+        long b = std::strtol(buf, nullptr, 10);
+        if (!field_int(buf, 4, a) || a != (int)b) bad++;
+        n++;
+    }
+    for (const char* t : {"  1A", " -0 ", "+12 ", "    ", " x12", "1234", "\t 7\t"}) {
+        int a = 0;
+        char* e = nullptr;
+        long b = std::strtol(t, &e, 10);
+        const bool ok = field_int(t, 4, a);
+        if (ok != (e != t) || (ok && a != (int)b)) bad++;
         n++;
     }
     std::printf("%%ld %%ld\n", n, bad);
