@@ -38,6 +38,7 @@ OPTSETS = {
     "split2": ["--split=2", "--ter=0"],
     "split2ter1": ["--split=2", "--ter=1"],
     "ter0max100": ["--ter=0", "--dev-max-length=100"],
+    "aatom_n": ["--aatom= N  "],
 }
 
 AA3 = ["ALA", "ARG", "ASN", "ASP", "CYS", "GLN", "GLU", "GLY", "HIS", "ILE", "LEU", "LYS",

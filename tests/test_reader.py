@@ -32,6 +32,8 @@ def _opts(flags):
             kw["hetatm"] = True
         elif f.startswith("--dev-max-length="):
             kw["maxlen"] = int(f.split("=")[1])
+        elif f.startswith("--aatom="):
+            kw["aatom"] = f[len("--aatom="):]
         else:
             k, v = f[2:].split("=")
             kw[k] = int(v)
@@ -47,7 +49,7 @@ def cases(tmp_path_factory):
 
 
 @pytest.mark.parametrize("key", ["default", "hetatm", "ter0", "ter1", "ter2", "split1", "split2",
-                                 "split2ter1", "ter0max100"])
+                                 "split2ter1", "ter0max100", "aatom_n"])
 def test_reader_reads_what_the_reference_reads(cases, key):
     from gtalign_alpha_b200.api import read_pdb
     fx = json.load(open(FIX))
