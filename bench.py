@@ -42,7 +42,9 @@ references.  Legs of one run:
 * reference_gpu: the reference's own GPU build (oracle/_ref/gpu/gtalign,
   compiled for sm_100a from its sources by oracle/Makefile.refgpu) on the
   same B200, over the first query chunk x a sample of the references, timed
-  by its "query batch execution time" (the GPU bar for this path).
+  by its "query batch execution time" (the GPU bar for this path); and
+  from_files: the same sample's files read by this library's reader and
+  aligned, wall clock against the reference process's.
 * clustering: the all-against-all clustering configuration at 1,000
   structures (config4's generator): the set aligned against itself with the
   clustering run's coverage prefilter, linked by gtb_cluster; the
@@ -1021,6 +1023,33 @@ def defaults_run(L, args, wl, qbs, rb, step_pairs, maxpairs, dev, legs):
         g9.close()
 
 
+def from_files_run(d, args, ref_wall):
+    """The reference GPU build's sample the way a user runs it, from the
+    structure files to the results, this library's way: the host reader
+    (gtb_read_pdb) on the same query and reference files, then one
+    gtb_process_block call with alignment rows (the reference's results,
+    unpolished; no output files written).  Host wall time from the first
+    file read to the results in host memory; the handle is created before."""
+    import glob
+    from gtalign_alpha_b200.api import GTalignB200, read_pdb
+    try:
+        qf = sorted(glob.glob(os.path.join(d, "q", "*.pdb")))
+        rf = sorted(glob.glob(os.path.join(d, "r", "*.pdb")))
+        with GTalignB200(0, 0, lib_options(args, 0)) as g:
+            read_pdb(qf)                                   # the reader's first call
+            t0 = time.perf_counter()
+            q = read_pdb(qf, maxlen=65535)
+            r = read_pdb(rf, maxlen=65535)
+            res = g.process_packed(q.packed, r.packed, scorethld=0.5, alignments=True)
+            wall = time.perf_counter() - t0
+        return {"wall_s": wall, "pairs": q.soa.n * r.soa.n, "reported": int((res.alndata[..., 9] > 0).sum()),
+                "reference_wall_s": ref_wall, "reference_wall_over_ours": ref_wall / wall,
+                "scope": "ours: read the files, align, results and alignment rows in host memory; "
+                         "reference: its whole process (reading, device setup, search, JSON output)"}
+    except Exception as e:                                 # a missing piece must not lose the line
+        return {"unavailable": "%s: %s" % (type(e).__name__, str(e)[:200])}
+
+
 def reference_gpu_sample(wl, args, value):
     """The reference's GPU build on this device: the first query chunk (2
     queries) x the first refgpu_refs references of the workload, default
@@ -1052,9 +1081,11 @@ def reference_gpu_sample(wl, args, value):
                 seen.add(t)
                 secs += t
         v = nq * nref / secs
-        return {"value": v, "unit": UNIT, "wall_s": wall, "batch_s": secs,
-                "sample": "%d queries x %d references of the workload, %s" % (nq, nref, options_text(args)),
-                "ours_vs_reference_gpu": value / v}
+        out = {"value": v, "unit": UNIT, "wall_s": wall, "batch_s": secs,
+               "sample": "%d queries x %d references of the workload, %s" % (nq, nref, options_text(args)),
+               "ours_vs_reference_gpu": value / v}
+        out["from_files"] = from_files_run(d, args, wall)
+        return out
     except subprocess.TimeoutExpired:
         return {"unavailable": "reference GPU build did not finish within %d s" % args.refgpu_timeout}
     finally:
