@@ -437,6 +437,11 @@ void parse_cif(const std::string& path, const std::string& data, const gtb_reade
         }
         int fa = CF_LASYM;
         if (0 <= fld[CF_AASYM] && fld[CF_AASYM] < nt) fa = CF_AASYM;
+        int fs = CF_LSEQ;
+        if (0 <= fld[CF_ASEQ] && fld[CF_ASEQ] < nt) fs = CF_ASEQ;
+        // a record without the chain or number column it would read (the
+        // table has only the other form, past this record's tokens): skipped
+        if (fld[fa] < 0 || fld[fs] < 0) { skip(); continue; }
         if (toklen(fa) < 1) { out.err = path + ": invalid PDBx/mmCIF file format"; return; }
         chain.assign(d0 + tok(fa), toklen(fa));
         char chid = chain[0];
@@ -446,8 +451,6 @@ void parse_cif(const std::string& path, const std::string& data, const gtb_reade
         if (insc == '?') insc = ' ';
         char nm[3] = {at(tok(CF_COMP)), at(tok(CF_COMP) + 1), at(tok(CF_COMP) + 2)};
         const char resd = res_code(nm);
-        int fs = CF_LSEQ;
-        if (0 <= fld[CF_ASEQ] && fld[CF_ASEQ] < nt) fs = CF_ASEQ;
         int resnum = 0;
         float c[3];
         if (!field_int(d0 + tok(fs), (int)toklen(fs), resnum) ||

@@ -197,3 +197,34 @@ int main() {
     out = subprocess.run([str(exe)], capture_output=True, text=True)
     n, bad = (int(x) for x in out.stdout.split())
     assert n > 13_000_000 and bad == 0, out.stdout
+
+
+def test_reader_survives_truncated_and_garbage_files(cases, tmp_path):
+    """Every crafted file cut at random offsets, and random bytes under each
+    file name form, read without a crash (structures or a status code)."""
+    from gtalign_alpha_b200.api import GTBError, read_pdb
+    d, names = cases
+    rng = np.random.default_rng(17)
+    paths = []
+    for k in range(120):
+        src = os.path.join(d, names[k % len(names)])
+        data = open(src, "rb").read()
+        cut = int(rng.integers(0, len(data) + 1))
+        ext = os.path.splitext(names[k % len(names)])[1]
+        p = str(tmp_path / ("cut%03d%s" % (k, ext)))
+        with open(p, "wb") as f:
+            f.write(data[:cut])
+        paths.append(p)
+    for k, ext in enumerate([".pdb", ".cif", ".gz", ".tar", ".ent"] * 6):
+        p = str(tmp_path / ("rnd%03d%s" % (k, ext)))
+        with open(p, "wb") as f:
+            f.write(rng.integers(0, 256, int(rng.integers(0, 3000)), dtype=np.uint8).tobytes())
+        paths.append(p)
+    ok = 0
+    for p in paths:
+        try:
+            read_pdb([p])
+            ok += 1
+        except GTBError:
+            pass
+    assert ok > 60
