@@ -39,6 +39,8 @@ OPTSETS = {
     "split2ter1": ["--split=2", "--ter=1"],
     "ter0max100": ["--ter=0", "--dev-max-length=100"],
     "aatom_n": ["--aatom= N  "],
+    "infmt_pdb": ["--infmt=1"],
+    "infmt_cif": ["--infmt=2"],
 }
 
 AA3 = ["ALA", "ARG", "ASN", "ASP", "CYS", "GLN", "GLU", "GLY", "HIS", "ILE", "LEU", "LYS",

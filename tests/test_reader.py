@@ -49,7 +49,8 @@ def cases(tmp_path_factory):
 
 
 @pytest.mark.parametrize("key", ["default", "hetatm", "ter0", "ter1", "ter2", "split1", "split2",
-                                 "split2ter1", "ter0max100", "aatom_n"])
+                                 "split2ter1", "ter0max100", "aatom_n", "infmt_pdb",
+                                 "infmt_cif"])
 def test_reader_reads_what_the_reference_reads(cases, key):
     from gtalign_alpha_b200.api import read_pdb
     fx = json.load(open(FIX))
