@@ -489,7 +489,10 @@ def run_ours(args):
     if rank == 0 and ws == 1:
         if "reader" in legs:
             progress("host reader")
-            reader = reader_run(wl, args, r_all)
+            try:
+                reader = reader_run(wl, args, r_all)
+            except Exception as e:                   # a host-side leg must not lose the line
+                reader = {"unavailable": "%s: %s" % (type(e).__name__, str(e)[:200])}
         if "refgpu" in legs:
             progress("reference GPU build")
             refgpu = reference_gpu_sample(wl, args, value)
