@@ -698,8 +698,15 @@ def long_chain_run(g, args):
     if "refgpu" in args.legs.split(",") and args.long_refgpu_lengths:
         progress("reference GPU build on long chains")
         pick = {int(x) for x in args.long_refgpu_lengths.split(",")}
-        out["reference_gpu"] = [long_chain_reference_gpu(wl.queries[i], wl.refs[i], per[i], args)
-                                for i in range(q.n) if lengths[i] in pick]
+        out["reference_gpu"] = []
+        for i in range(q.n):
+            if lengths[i] not in pick:
+                continue
+            try:
+                out["reference_gpu"].append(long_chain_reference_gpu(wl.queries[i], wl.refs[i], per[i], args))
+            except Exception as e:                   # a comparison must not lose the line
+                out["reference_gpu"].append({"length": int(lengths[i]),
+                                             "unavailable": "%s: %s" % (type(e).__name__, str(e)[:200])})
     return out
 
 
